@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark of the DMOLP partitioning hot path on B200: label-propagation traversed edges per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rmat22] [--impl ours|reference]
+
+A step is one phase-2 run (the fixed number of LP iterations of the workload) from the phase-1 partition,
+on a graph resident in HBM.  Traversed edges (TE) per iteration = sum of degrees over the previous window,
+over the candidates and over the selected window, plus all arcs for the statistics pass; the same count
+the oracle and the reference harness report.
+
+One JSON line on stdout (rank 0).  With --gpus N (launched under torchrun) every rank runs the same
+workload on its own GPU: the path does not shard a single graph, so N GPUs are N independent replicas.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # R-MAT scale 22, edge factor 16, (.57,.19,.19,.05), seed 7, k = 32, 30 LP iterations
+    "rmat22": dict(kind="rmat", scale=22, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=7, k=32, theta=10000,
+                   iters=30),
+    "rmat22-k16": dict(kind="rmat", scale=22, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=7, k=16, theta=10000,
+                       iters=30),
+    "rmat22-k64": dict(kind="rmat", scale=22, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=7, k=64, theta=10000,
+                       iters=30),
+    # 3-D k-NN (k=12), 55,476 points, k = 8, 20 LP iterations
+    "knn-c0": dict(kind="knn", n=55476, dim=3, knn=12, seed=1, k=8, theta=1000, iters=20),
+}
+
+
+def describe(w: dict) -> str:
+    if w["kind"] == "rmat":
+        return (f"R-MAT scale {w['scale']} edge factor {w['edge_factor']} ({w['a']},{w['b']},{w['c']}) seed "
+                f"{w['seed']}, symmetrised, k={w['k']}, theta={w['theta']}, {w['iters']} LP iterations")
+    return f"3-D kNN n={w['n']} knn={w['knn']} seed {w['seed']}, k={w['k']}, {w['iters']} LP iterations"
+
+
+def make_graph(w: dict):
+    from dmolp_b200 import graphs
+
+    if w["kind"] == "rmat":
+        return graphs.rmat(w["scale"], w["edge_factor"], w["a"], w["b"], w["c"], seed=w["seed"])
+    return graphs.knn(w["n"], w["dim"], w["knn"], w["seed"])
+
+
+def measured_peaks() -> tuple[float, str]:
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200", "-i",
+                 str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def traffic_from_profiles(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/ncu_traffic.json)."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))
+        return d.get(workload, {}).get(kernel)
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------------------------------- our arm
+def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | None:
+    import torch
+
+    from dmolp_b200.partitioner import Partitioner
+
+    torch.cuda.set_device(local_rank)
+    g = make_graph(w)
+    p = Partitioner(local_rank)
+    p.upload(g)
+    m1 = p.phase1(w["k"], w["theta"])
+    labels1 = p.labels()
+    p.lib.dmolp_labels_save(p.ctx)
+    stream = torch.cuda.ExternalStream(p.lib.dmolp_stream(p.ctx), device=torch.device("cuda", local_rank))
+
+    def step():
+        p._check(p.lib.dmolp_labels_restore(p.ctx))
+        return p.phase2(w["k"], mode="fixed", iterations=w["iters"], records=False)
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    t_end = time.time() + 1.0  # keep the GPU busy ~1 s before warm-up so the clock samples see load
+    while time.time() < t_end:
+        step()
+    for _ in range(args.warmup):
+        step()
+    p.lib.dmolp_set_profiling(p.ctx, 1)
+    launches0 = p.kernel_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    te = 0
+    last = None
+    for _ in range(args.steps):
+        last = step()
+        te += last.traversed_edges
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = p.kernel_launches() - launches0
+    elapsed = e0.elapsed_time(e1) / 1e3
+    prof = {}
+    for kid, name in ((0, "lp_scan"), (1, "stats")):
+        import ctypes
+
+        ms, n, by = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
+        p.lib.dmolp_kernel_profile(p.ctx, kid, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(by))
+        prof[name] = dict(ms=ms.value, launches=n.value, bytes=by.value)
+    p.lib.dmolp_set_profiling(p.ctx, 0)
+    final_labels = p.labels()
+
+    # ---- end to end through the public API, host buffers in pinned memory ----
+    off_h = torch.from_numpy(g.offsets).pin_memory()
+    col_h = torch.from_numpy(g.indices).pin_memory()
+    raw_h = torch.from_numpy(g.raw_deg()).pin_memory()
+    lab_h = torch.from_numpy(labels1).pin_memory()
+    out_h = torch.empty_like(lab_h).pin_memory()
+    import ctypes
+
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    q0 = torch.cuda.Event(enable_timing=True)
+    q1 = torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    e2e_te = 0
+    for _ in range(e2e_steps):
+        p._check(p.lib.dmolp_graph_upload(p.ctx, g.num_vertices, g.num_arcs, ctypes.c_void_p(off_h.data_ptr()),
+                                          ctypes.c_void_p(col_h.data_ptr()), ctypes.c_void_p(raw_h.data_ptr())))
+        p._check(p.lib.dmolp_labels_set(p.ctx, ctypes.c_void_p(lab_h.data_ptr())))
+        r = p.phase2(w["k"], mode="fixed", iterations=w["iters"], records=False)
+        e2e_te += r.traversed_edges
+        p._check(p.lib.dmolp_labels_get(p.ctx, ctypes.c_void_p(out_h.data_ptr())))
+    q1.record(stream)
+    torch.cuda.synchronize()
+    e2e_wall = time.perf_counter() - t0
+    e2e_elapsed = q0.elapsed_time(q1) / 1e3
+    assert np.array_equal(out_h.numpy(), final_labels), "end-to-end labels differ from the resident run"
+    h2d = g.offsets.nbytes + g.indices.nbytes + g.raw_deg().nbytes + labels1.nbytes
+    d2h = labels1.nbytes
+
+    t_max = elapsed
+    e2e_max = e2e_elapsed
+    if dist:
+        t = torch.tensor([elapsed, e2e_elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max, e2e_max = float(t[0]), float(t[1])
+    p.close()
+    if rank != 0:
+        return None
+
+    peak, peak_kind = measured_peaks()
+    dom = max(prof, key=lambda k: prof[k]["ms"])
+    d = prof[dom]
+    per_launch_bytes = d["bytes"] / max(1, d["launches"])
+    per_launch_s = d["ms"] / 1e3 / max(1, d["launches"])
+    achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else None
+    line = {
+        "metric": "LP traversed edges/s",
+        "value": te * world / t_max,
+        "unit": "TE/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int32",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": describe(w), "k": w["k"], "iterations": w["iters"], "mode": "fixed",
+                   "label_cap": "reference (min(k,32))", "num_vertices": g.num_vertices, "num_arcs": g.num_arcs,
+                   "te_per_step": te // args.steps, "edge_cut": last.edge_cut,
+                   "vertex_balance": last.vertex_balance, "edge_balance": last.edge_balance,
+                   "phase1_gpu_ms": m1.gpu_ms, "phase1_initial_edge_cut": m1.initial_edge_cut,
+                   "l2": "inputs larger than L2 (CSR arcs %.0f MB)" % (g.indices.nbytes / 1e6),
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_te * world / e2e_max, "unit": "TE/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "wall_s": e2e_wall, "steps": e2e_steps},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                     "traffic": traffic_from_profiles(dom, args.workload),
+                     "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": per_launch_s * 1e3,
+                     "kernels": prof},
+        "clocks": clocks,
+    }
+    return line
+
+
+# ------------------------------------------------------------------------------------------- CPU baselines
+def reference_cpu_run(g, labels1, w, repeats: int, iters: int, threads: int, timeout: float = 900):
+    """The reference's own phase-2 code (oracle/_ref, built from its sources) on the host cores."""
+    import oracle
+
+    with tempfile.TemporaryDirectory() as td:
+        from dmolp_b200 import graphs
+
+        txt = os.path.join(td, "g.txt")
+        graphs.write_adjtext(g, txt)
+        lab = os.path.join(td, "labels1.bin")
+        labels1.astype(np.int32).tofile(lab)
+        cmd = [oracle.REF_HARNESS, txt, str(w["k"]), str(w["theta"]), "--out", os.path.join(td, "o"), "--mode",
+               "fixed", "--iters", str(iters), "--threads", str(threads), "--labels-in", lab, "--no-seed-dump",
+               "--repeat", str(repeats)]
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        pr = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
+        if pr.returncode != 0:
+            raise RuntimeError(pr.stderr[-1000:])
+        reps = [json.loads(l) for l in pr.stdout.splitlines() if l.startswith("{\"repeat\"")]
+        if not reps:
+            reps = [json.loads(pr.stdout.splitlines()[-1])]
+            reps[0]["repeat"] = 0
+        return reps
+
+
+def port_cpu_run(g, labels1, w, iters: int):
+    import oracle
+
+    t0 = time.perf_counter()
+    o = oracle.phase2(g.offsets, g.indices, labels1, w["k"], "fixed", iters)
+    return dict(lp_seconds=time.perf_counter() - t0, te_total=o.res.te_total)
+
+
+def cpu_baseline(g, labels1, w, args) -> dict:
+    import oracle
+
+    threads = os.cpu_count() or 1
+    iters = args.cpu_sample_iters
+    sample = f"LP iteration{'s' if iters > 1 else ''} 1..{iters} of {w['iters']} on the full graph"
+    if oracle.reference_available():
+        reps = reference_cpu_run(g, labels1, w, 1, iters, threads)
+        r = reps[-1]
+        return {"value": r["te_total"] / r["lp_seconds"], "unit": "TE/s", "cores": threads, "kind": "reference",
+                "sample": sample, "seconds": r["lp_seconds"]}
+    r = port_cpu_run(g, labels1, w, iters)
+    return {"value": r["te_total"] / r["lp_seconds"], "unit": "TE/s", "cores": 1, "kind": "port",
+            "sample": sample, "seconds": r["lp_seconds"]}
+
+
+def run_reference_arm(args, w) -> dict:
+    """--impl reference: the reference's own implementation of the path on this box's host cores."""
+    import oracle
+
+    g = make_graph(w)
+    # phase-1 labels from the oracle (the reference's phase 1 is undefined on R-MAT: fewer seeds than parts)
+    labels1 = oracle.phase1(g.offsets, g.indices, g.raw_deg(), w["k"], w["theta"]).labels
+    threads = os.cpu_count() or 1
+    iters = args.cpu_sample_iters
+    sample = f"per step: LP iteration{'s' if iters > 1 else ''} 1..{iters} of {w['iters']} on the full graph"
+    if oracle.reference_available():
+        reps = reference_cpu_run(g, labels1, w, args.warmup + args.steps, iters, threads, timeout=3600)
+        kind, cores = "reference", threads
+    else:
+        reps = [dict(port_cpu_run(g, labels1, w, iters), repeat=i) for i in range(args.warmup + args.steps)]
+        kind, cores = "port", 1
+    timed = [r for r in reps if r["repeat"] >= args.warmup] or reps
+    secs = sum(r["lp_seconds"] for r in timed)
+    te = sum(r["te_total"] for r in timed)
+    value = te / secs
+    return {
+        "impl": "reference", "metric": "LP traversed edges/s", "value": value, "unit": "TE/s", "n_gpus": args.gpus,
+        "steps": len(timed), "warmup": args.warmup, "ms_per_step": secs / len(timed) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": describe(w), "k": w["k"], "iterations": w["iters"], "mode": "fixed",
+                   "num_vertices": g.num_vertices, "num_arcs": g.num_arcs},
+        "cpu_baseline": {"value": value, "unit": "TE/s", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "TE/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="rmat22", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-iters", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        print(json.dumps(run_reference_arm(args, w)), flush=True)
+        return
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    line = run_ours(args, w, rank, world, local_rank, dist)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0 and line is not None:
+        if world == 1 and not args.no_cpu_baseline:
+            g = make_graph(w)
+            import oracle
+
+            labels1 = oracle.phase1(g.offsets, g.indices, g.raw_deg(), w["k"], w["theta"]).labels
+            try:
+                line["cpu_baseline"] = cpu_baseline(g, labels1, w, args)
+            except Exception as e:  # report, do not hide
+                line["cpu_baseline"] = {"error": str(e)[:300]}
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,88 @@
+"""ctypes declarations of include/dmolp_b200.h."""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_double, c_int, c_int32, c_int64, c_uint64, c_void_p
+
+DMOLP_OK = 0
+DMOLP_ERR_ARG = 1
+DMOLP_ERR_CUDA = 2
+DMOLP_ERR_NOMEM = 3
+DMOLP_ERR_STATE = 4
+DMOLP_ERR_BAD_LABELS = 5
+DMOLP_ERR_NO_GPU = 6
+MODE_REF = 0
+MODE_FIXED = 1
+CAP_REF = 0
+CAP_FULL = 1
+MAX_K = 1024
+
+# every function the header declares (checked by the CPU test suite against the built library)
+EXPORTS = [
+    "dmolp_last_error", "dmolp_create", "dmolp_destroy", "dmolp_graph_upload", "dmolp_phase1", "dmolp_lp_run",
+    "dmolp_metrics", "dmolp_labels_get", "dmolp_labels_set", "dmolp_window_select", "dmolp_lp_apply",
+    "dmolp_lp_history", "dmolp_device_labels", "dmolp_kernel_launches", "dmolp_adjtext_load",
+    "dmolp_adjtext_error", "dmolp_host_graph_nv", "dmolp_host_graph_narcs", "dmolp_host_graph_offsets",
+    "dmolp_host_graph_indices", "dmolp_host_graph_raw_degree", "dmolp_host_graph_free", "dmolp_stream",
+    "dmolp_labels_save", "dmolp_labels_restore", "dmolp_set_profiling", "dmolp_kernel_profile",
+]
+
+
+class Phase1Info(ctypes.Structure):
+    _fields_ = [("initial_edge_cut", c_int64), ("initial_vertex_balance", c_double),
+                ("initial_edge_balance", c_double), ("num_seeds_found", c_int32), ("rounds", c_int32),
+                ("num_hubs", c_int64), ("traversed_edges", c_uint64), ("gpu_ms", c_double)]
+
+
+class LpConfig(ctypes.Structure):
+    _fields_ = [("mode", c_int32), ("iterations", c_int32), ("cap", c_int32), ("flags", c_int32)]
+
+
+class LpResult(ctypes.Structure):
+    _fields_ = [("edge_cut", c_int64), ("vertex_balance", c_double), ("edge_balance", c_double),
+                ("iterations_run", c_int32), ("stop_reason", c_int32), ("traversed_edges", c_uint64),
+                ("total_vertices", c_int64), ("total_edges", c_int64), ("gpu_ms", c_double)]
+
+
+class LpRecord(ctypes.Structure):
+    _fields_ = [("iteration", c_int32), ("window", c_int32), ("candidates", c_int32), ("changes", c_int32),
+                ("boundary", c_int32), ("pad", c_int32), ("edge_cut", c_int64), ("te_prev", c_uint64), ("te_cand", c_uint64), ("te_sel", c_uint64),
+                ("te_stats", c_uint64)]
+
+
+def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
+    vp = c_void_p
+    lib.dmolp_last_error.restype = c_char_p
+    lib.dmolp_last_error.argtypes = []
+    lib.dmolp_create.argtypes = [c_int, POINTER(vp)]
+    lib.dmolp_destroy.argtypes = [vp]
+    lib.dmolp_graph_upload.argtypes = [vp, c_int64, c_int64, vp, vp, vp]
+    lib.dmolp_phase1.argtypes = [vp, c_int, c_int, vp, vp, vp, POINTER(Phase1Info)]
+    lib.dmolp_lp_run.argtypes = [vp, c_int, POINTER(LpConfig), POINTER(LpResult), vp, c_int]
+    lib.dmolp_metrics.argtypes = [vp, c_int, POINTER(c_int64), vp, vp]
+    lib.dmolp_labels_get.argtypes = [vp, vp]
+    lib.dmolp_labels_set.argtypes = [vp, vp]
+    lib.dmolp_window_select.argtypes = [vp, c_int, c_int, vp, vp, c_int64, vp, POINTER(c_int64)]
+    lib.dmolp_lp_apply.argtypes = [vp, c_int, c_int, vp, vp, c_int64, vp, vp, POINTER(c_int64)]
+    lib.dmolp_lp_history.argtypes = [vp, c_int, c_int, vp, vp]
+    lib.dmolp_device_labels.argtypes = [vp, POINTER(vp)]
+    lib.dmolp_kernel_launches.argtypes = [vp]
+    lib.dmolp_kernel_launches.restype = c_int64
+    lib.dmolp_adjtext_load.argtypes = [c_char_p, POINTER(vp)]
+    lib.dmolp_adjtext_error.restype = c_char_p
+    lib.dmolp_adjtext_error.argtypes = []
+    for f in ("dmolp_host_graph_nv", "dmolp_host_graph_narcs"):
+        getattr(lib, f).argtypes = [vp]
+        getattr(lib, f).restype = c_int64
+    for f in ("dmolp_host_graph_offsets", "dmolp_host_graph_indices", "dmolp_host_graph_raw_degree"):
+        getattr(lib, f).argtypes = [vp]
+        getattr(lib, f).restype = vp
+    lib.dmolp_host_graph_free.argtypes = [vp]
+    lib.dmolp_host_graph_free.restype = None
+    lib.dmolp_stream.argtypes = [vp]
+    lib.dmolp_stream.restype = vp
+    lib.dmolp_labels_save.argtypes = [vp]
+    lib.dmolp_labels_restore.argtypes = [vp]
+    lib.dmolp_set_profiling.argtypes = [vp, c_int]
+    lib.dmolp_kernel_profile.argtypes = [vp, c_int, POINTER(c_double), POINTER(c_int64), POINTER(c_double)]
+    return lib

@@ -1,0 +1,113 @@
+// Device-resident state of one dmolp context (layout in HBM) and the small control blocks the
+// iteration kernels share.  Everything is allocated once per graph upload; the LP loop allocates nothing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace dmolp {
+
+// Per-iteration counters of the LP loop (one instance, reset by the first kernel of each iteration).
+struct LpCounters {
+    int ncand;        // candidates appended this iteration (t >= 2)
+    int nbnd;         // boundary candidates (selection records)
+    int nwin[2];      // window (selected set) sizes, double-buffered by iteration parity
+    int nactive[2];   // radix-select active lists
+    int nchanged;     // selected vertices whose label changed
+    int pad;
+    unsigned long long cut_arcs;  // full stats pass: arcs whose endpoint labels differ
+};
+
+// Loop control shared by the iteration kernels.
+struct LpControl {
+    int stopped;        // set at the end of the iteration that met a stopping rule; later kernels return
+    int stop_now;       // stopping rule met in the current iteration (1 empty, 2 no change, 3 converged)
+    int skip_stats;     // current iteration runs no statistics pass
+    int conv;           // consecutive iterations with relative cut change < 3 %
+    long long prev_cut; // last computed edge cut
+    int iters_run;
+    int stop_reason;
+    int error;          // 1 = odd cut-arc count or invalid label (the reference aborts)
+    int mode;           // DMOLP_LP_MODE_*
+};
+
+// One LP iteration record as kept on the device.
+struct LpRecordDev {
+    int iteration, window, candidates, changes;
+    int boundary, pad;
+    long long edge_cut;
+    unsigned long long te_prev, te_cand, te_sel, te_stats;
+};
+
+struct Buffers {
+    // graph
+    int64_t *off = nullptr;   // [nv+1]
+    int32_t *col = nullptr;   // [narcs]
+    int32_t *rawdeg = nullptr;// [nv]
+    int32_t *label = nullptr; // [nv]
+    // LP scratch
+    int32_t *stamp = nullptr; // [nv] iteration stamp of candidate marking
+    int32_t *cand = nullptr;  // [nv]
+    int32_t *win[2] = {nullptr, nullptr};  // [nv] each
+    int32_t *bv = nullptr, *bown = nullptr, *bnew = nullptr;  // [nv] boundary records
+    uint64_t *bkey = nullptr;  // [nv]
+    uint8_t *bsel = nullptr;   // [nv]
+    int32_t *active[2] = {nullptr, nullptr};  // [nv] radix-select active lists
+    // per-part arrays (DMOLP_MAX_K)
+    unsigned int *hist = nullptr;        // [MAX_K * 256]
+    int32_t *need = nullptr;             // [MAX_K]
+    int32_t *sel_below = nullptr;        // [MAX_K]
+    int32_t *keep_digit = nullptr;       // [MAX_K]
+    int32_t *npart = nullptr;            // [MAX_K] records per segment
+    unsigned long long *vc = nullptr;    // [MAX_K] vertex counts
+    unsigned long long *intra = nullptr; // [MAX_K] intra-part arcs
+    long long *psize = nullptr;          // [MAX_K] phase-1 part sizes
+    double *tpen = nullptr;              // [MAX_K] 1 + penalty
+    double *RE = nullptr;                // [MAX_K]
+    double *penhist = nullptr;           // [kMaxIter * MAX_K]
+    long long *cnthist = nullptr;        // [kMaxIter * 2 * MAX_K]
+    double *logtab = nullptr;            // [kMaxIter + 1] log(t)
+    double *ratiotab = nullptr;          // [kMaxIter + 1] exp(-t/5)
+    LpCounters *cnt = nullptr;
+    LpControl *ctrl = nullptr;
+    LpRecordDev *rec = nullptr;          // [kMaxIter]
+    // phase 1 scratch (aliases LP scratch where lifetimes do not overlap)
+    uint8_t *covered = nullptr;          // [nv]
+    int32_t *hubs = nullptr;             // [nv]
+    uint8_t *hub_used = nullptr;         // [nv]
+    int32_t *claim = nullptr;            // [nv]
+    unsigned long long *best = nullptr;  // [1] packed hub argmax
+    int *p1cnt = nullptr;                // [8] phase-1 counters
+    unsigned long long *p1te = nullptr;  // [1]
+};
+
+}  // namespace dmolp
+
+struct dmolp_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    int64_t nv = 0, narcs = 0;
+    int64_t maxdeg = 0, maxraw = 0;
+    int ibits = 1, dbits = 1, rbits = 1;  // bits for ids, CSR degree, raw degree
+    bool has_graph = false;
+    std::vector<int32_t> h_rawdeg;        // host copy for the hub sort
+    dmolp::Buffers b;
+    std::vector<void *> allocations;
+    long long launches = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int32_t *saved_labels = nullptr;  // dmolp_labels_save
+    // optional kernel timing (dmolp_set_profiling)
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_events;  // pairs, in launch order
+    std::vector<int> prof_kind;            // kernel id per pair
+    std::vector<int> prof_iter;            // LP iteration per pair
+    double prof_ms[2] = {0, 0};
+    long long prof_launches[2] = {0, 0};
+    double prof_bytes[2] = {0, 0};
+};

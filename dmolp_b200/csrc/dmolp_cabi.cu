@@ -1,0 +1,763 @@
+// C-ABI entry points (include/dmolp_b200.h): context, resident graph, phase 1, phase 2, metrics.
+//
+// Host-side steps that decide ORDER-dependent results stay on the host, in the reference's exact form:
+// the hub sort (an unstable std::sort over vertices V-1..0, src/phase1/init.cpp:139-177) and the first-seed
+// scan (init.cpp:179-187).  Everything that touches the graph's arcs runs on the device.
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dmolp_b200.h"
+#include "kernels.cuh"
+
+using namespace dmolp;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define DMOLP_CUDA(call)                                                                              \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return fail(e_ == cudaErrorMemoryAllocation ? DMOLP_ERR_NOMEM : DMOLP_ERR_CUDA,           \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+
+int bits_for(int64_t x) {
+    int b = 1;
+    while (b < 62 && (int64_t(1) << b) <= x) ++b;
+    return b;
+}
+
+template <typename T>
+int dalloc(dmolp_ctx *c, T **p, size_t n) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DMOLP_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    c->allocations.push_back(q);
+    *p = (T *)q;
+    return DMOLP_OK;
+}
+
+void free_all(dmolp_ctx *c) {
+    for (void *p : c->allocations) cudaFree(p);
+    c->allocations.clear();
+    c->saved_labels = nullptr;
+    c->b = Buffers();
+    c->has_graph = false;
+}
+
+int check_launch(dmolp_ctx *c) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(DMOLP_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    (void)c;
+    return DMOLP_OK;
+}
+
+int sync(dmolp_ctx *c) {
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return fail(DMOLP_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+    return check_launch(c);
+}
+
+// The reference's balance = max over parts of count / expected (src/phase2/phase2.cpp:426-432).
+void balances(const std::vector<long long> &vc, const std::vector<long long> &ec, int k, double *vb, double *eb,
+              int64_t *tv_out, int64_t *te_out) {
+    long long tv = 0, te = 0;
+    for (int p = 0; p < k; ++p) {
+        tv += vc[p];
+        te += ec[p];
+    }
+    const double ev = (double)tv / k;
+    const double ee = te > 0 ? (double)te / k : 1.0;
+    double mv = 0.0, me = 0.0;
+    for (int p = 0; p < k; ++p) {
+        const double rv = ev > 0 ? (double)vc[p] / ev : 1.0;
+        const double re = ee > 0 ? (double)ec[p] / ee : 1.0;
+        mv = std::max(mv, rv);
+        me = std::max(me, re);
+    }
+    *vb = mv;
+    *eb = me;
+    if (tv_out) *tv_out = tv;
+    if (te_out) *te_out = te;
+}
+
+// Fused cut/balance pass over the resident labels; fills host copies.  Returns the status.
+int run_stats(dmolp_ctx *c, int k, unsigned long long *cut_arcs, std::vector<long long> &vc,
+              std::vector<long long> &intra, int *bad) {
+    lp_reset_stats(c, k, nullptr);
+    lp_stats(c, k, nullptr, nullptr);
+    std::vector<unsigned long long> hv(k), hi(k);
+    LpCounters cn;
+    LpControl ctl;
+    DMOLP_CUDA(cudaMemcpyAsync(hv.data(), c->b.vc, k * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(hi.data(), c->b.intra, k * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                               c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(&cn, c->b.cnt, sizeof(cn), cudaMemcpyDeviceToHost, c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(&ctl, c->b.ctrl, sizeof(ctl), cudaMemcpyDeviceToHost, c->stream));
+    int st = sync(c);
+    if (st) return st;
+    vc.assign(k, 0);
+    intra.assign(k, 0);
+    for (int p = 0; p < k; ++p) {
+        vc[p] = (long long)hv[p];
+        intra[p] = (long long)hi[p];
+    }
+    *cut_arcs = cn.cut_arcs;
+    *bad = ctl.error;
+    return DMOLP_OK;
+}
+
+// src/phase1/init.cpp:139-177 (see the comment at the top of this file).
+std::vector<int> find_hubs(const std::vector<int32_t> &raw) {
+    const int64_t nv = (int64_t)raw.size();
+    std::vector<std::pair<int, int>> sd;
+    sd.reserve(nv);
+    for (int64_t v = nv - 1; v >= 0; --v) sd.emplace_back((int)v, raw[v]);
+    std::sort(sd.begin(), sd.end(),
+              [](const std::pair<int, int> &a, const std::pair<int, int> &b) { return a.second < b.second; });
+    const int N = (int)sd.size();
+    std::vector<int> hubs;
+    if (N < 2) return hubs;
+    std::vector<double> cum(N);
+    double total = 0.0, run = 0.0;
+    for (int i = 0; i < N; ++i) {
+        total += sd[i].second;
+        run += sd[i].second;
+        cum[i] = run;
+    }
+    for (int i = 0; i < N; ++i) cum[i] /= total;
+    const double inv_n = 1.0 / N;
+    const double x1 = N * inv_n, y1 = cum[N - 1];
+    const double x0 = (N - 1) * inv_n, y0 = cum[N - 2];
+    const double slope = (y1 - y0) / (x1 - x0);
+    const double x_int = x1 - y1 / slope;
+    for (int i = N - 1; i >= 0; --i) {
+        if ((i + 1) * inv_n > x_int) hubs.push_back(sd[i].first);
+        else break;
+    }
+    return hubs;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *dmolp_last_error(void) { return g_err.c_str(); }
+
+int dmolp_create(int device, dmolp_ctx **out) {
+    if (!out) return fail(DMOLP_ERR_ARG, "out is null");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(DMOLP_ERR_NO_GPU, "no CUDA device");
+    }
+    if (device < 0 || device >= n) return fail(DMOLP_ERR_ARG, "device index out of range");
+    DMOLP_CUDA(cudaSetDevice(device));
+    dmolp_ctx *c = new dmolp_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(DMOLP_ERR_CUDA, std::string("stream/event: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return DMOLP_OK;
+}
+
+int dmolp_destroy(dmolp_ctx *c) {
+    if (!c) return DMOLP_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_all(c);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return DMOLP_OK;
+}
+
+int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *off, const int32_t *col,
+                       const int32_t *raw) {
+    if (!c) return fail(DMOLP_ERR_ARG, "null context");
+    if (nv < 0 || nv > 0x7ffffffe || narcs < 0 || (!off && nv >= 0) || (!col && narcs > 0))
+        return fail(DMOLP_ERR_ARG, "bad graph sizes or null arrays");
+    if (off[0] != 0 || off[nv] != narcs) return fail(DMOLP_ERR_ARG, "offsets must start at 0 and end at narcs");
+    // Validate on the host: every device access below is then in bounds.
+    int bad = 0;
+    int64_t maxdeg = 0, maxraw = 0;
+#pragma omp parallel for reduction(| : bad) reduction(max : maxdeg, maxraw) schedule(static)
+    for (int64_t v = 0; v < nv; ++v) {
+        const int64_t d = off[v + 1] - off[v];
+        if (d < 0 || d > 0x7fffffff) bad |= 1;
+        maxdeg = std::max(maxdeg, d);
+        if (raw) {
+            if (raw[v] < 0) bad |= 4;
+            maxraw = std::max(maxraw, (int64_t)raw[v]);
+        }
+    }
+    if (!raw) maxraw = maxdeg;
+    if (!bad) {
+#pragma omp parallel for reduction(| : bad) schedule(static)
+        for (int64_t j = 0; j < narcs; ++j)
+            if ((uint32_t)col[j] >= (uint64_t)nv) bad |= 2;
+    }
+    if (bad & 1) return fail(DMOLP_ERR_ARG, "offsets are not non-decreasing");
+    if (bad & 2) return fail(DMOLP_ERR_ARG, "a neighbour id is outside [0, nv)");
+    if (bad & 4) return fail(DMOLP_ERR_ARG, "negative raw degree");
+
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    DMOLP_CUDA(cudaStreamSynchronize(c->stream));
+    free_all(c);
+    c->nv = nv;
+    c->narcs = narcs;
+    c->maxdeg = maxdeg;
+    c->maxraw = maxraw;
+    c->ibits = bits_for(nv > 0 ? nv - 1 : 0);
+    c->dbits = bits_for(maxdeg);
+    c->rbits = bits_for(maxraw);
+    c->h_rawdeg.resize(nv);
+    for (int64_t v = 0; v < nv; ++v) c->h_rawdeg[v] = raw ? raw[v] : (int32_t)(off[v + 1] - off[v]);
+
+    Buffers &b = c->b;
+    const size_t n = (size_t)nv + 1;
+    int st = DMOLP_OK;
+#define ALLOC(ptr, count) \
+    if ((st = dalloc(c, &(ptr), (count))) != DMOLP_OK) { free_all(c); return st; }
+    ALLOC(b.off, n);
+    ALLOC(b.col, (size_t)narcs);
+    ALLOC(b.rawdeg, n);
+    ALLOC(b.label, n);
+    ALLOC(b.stamp, n);
+    ALLOC(b.cand, n);
+    ALLOC(b.win[0], n);
+    ALLOC(b.win[1], n);
+    ALLOC(b.bv, n);
+    ALLOC(b.bown, n);
+    ALLOC(b.bnew, n);
+    ALLOC(b.bkey, n);
+    ALLOC(b.bsel, n);
+    ALLOC(b.active[0], n);
+    ALLOC(b.active[1], n);
+    ALLOC(b.hist, (size_t)DMOLP_MAX_K * kRadix);
+    ALLOC(b.need, DMOLP_MAX_K);
+    ALLOC(b.sel_below, DMOLP_MAX_K);
+    ALLOC(b.keep_digit, DMOLP_MAX_K);
+    ALLOC(b.npart, DMOLP_MAX_K);
+    ALLOC(b.vc, DMOLP_MAX_K);
+    ALLOC(b.intra, DMOLP_MAX_K);
+    ALLOC(b.psize, DMOLP_MAX_K);
+    ALLOC(b.tpen, DMOLP_MAX_K);
+    ALLOC(b.RE, DMOLP_MAX_K);
+    ALLOC(b.penhist, (size_t)kMaxIter * DMOLP_MAX_K);
+    ALLOC(b.cnthist, (size_t)kMaxIter * 2 * DMOLP_MAX_K);
+    ALLOC(b.logtab, kMaxIter + 1);
+    ALLOC(b.ratiotab, kMaxIter + 1);
+    ALLOC(b.cnt, 1);
+    ALLOC(b.ctrl, 1);
+    ALLOC(b.rec, kMaxIter);
+    ALLOC(b.covered, n);
+    ALLOC(b.hubs, n);
+    ALLOC(b.hub_used, n);
+    ALLOC(b.best, 1);
+    ALLOC(b.p1cnt, 8);
+    ALLOC(b.p1te, 1);
+#undef ALLOC
+    b.claim = b.stamp;  // phase 1 and the LP loop never run at the same time
+    DMOLP_CUDA(cudaMemcpyAsync(b.off, off, n * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+    if (narcs)
+        DMOLP_CUDA(cudaMemcpyAsync(b.col, col, (size_t)narcs * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(b.rawdeg, c->h_rawdeg.data(), (size_t)nv * sizeof(int32_t), cudaMemcpyHostToDevice,
+                               c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.label, 0, n * sizeof(int32_t), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.hist, 0, (size_t)DMOLP_MAX_K * kRadix * sizeof(unsigned int), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.ctrl, 0, sizeof(LpControl), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.cnt, 0, sizeof(LpCounters), c->stream));
+    // log(t) and e^(-t/5) with the host's libm, as the reference computes them (phase2.cpp:199,
+    // gpu_lp_boundary.cu:244)
+    std::vector<double> lt(kMaxIter + 1, 0.0), rt(kMaxIter + 1, 1.0);
+    for (int t = 1; t <= kMaxIter; ++t) {
+        lt[t] = std::log((double)t);
+        rt[t] = std::exp((-t) / (5.0));
+    }
+    DMOLP_CUDA(cudaMemcpyAsync(b.logtab, lt.data(), lt.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(b.ratiotab, rt.data(), rt.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    int s2 = sync(c);
+    if (s2) return s2;
+    c->has_graph = true;
+    return DMOLP_OK;
+}
+
+int dmolp_labels_get(dmolp_ctx *c, int32_t *labels) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (!labels && c->nv) return fail(DMOLP_ERR_ARG, "null labels");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    DMOLP_CUDA(cudaMemcpyAsync(labels, c->b.label, (size_t)c->nv * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    return sync(c);
+}
+
+int dmolp_labels_set(dmolp_ctx *c, const int32_t *labels) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (!labels && c->nv) return fail(DMOLP_ERR_ARG, "null labels");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    DMOLP_CUDA(cudaMemcpyAsync(c->b.label, labels, (size_t)c->nv * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    return sync(c);
+}
+
+int dmolp_device_labels(dmolp_ctx *c, int32_t **labels_device) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    *labels_device = c->b.label;
+    return DMOLP_OK;
+}
+
+int64_t dmolp_kernel_launches(const dmolp_ctx *c) { return c ? c->launches : 0; }
+
+void *dmolp_stream(dmolp_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int dmolp_labels_save(dmolp_ctx *c) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    if (!c->saved_labels) {
+        int st = dalloc(c, &c->saved_labels, (size_t)c->nv + 1);
+        if (st) return st;
+    }
+    DMOLP_CUDA(cudaMemcpyAsync(c->saved_labels, c->b.label, (size_t)c->nv * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                               c->stream));
+    return DMOLP_OK;
+}
+
+int dmolp_labels_restore(dmolp_ctx *c) {
+    if (!c || !c->has_graph || !c->saved_labels) return fail(DMOLP_ERR_STATE, "no saved labels");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    DMOLP_CUDA(cudaMemcpyAsync(c->b.label, c->saved_labels, (size_t)c->nv * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                               c->stream));
+    return DMOLP_OK;
+}
+
+int dmolp_set_profiling(dmolp_ctx *c, int enable) {
+    if (!c) return fail(DMOLP_ERR_ARG, "null context");
+    c->profiling = enable != 0;
+    for (int i = 0; i < 2; ++i) {
+        c->prof_ms[i] = 0;
+        c->prof_launches[i] = 0;
+        c->prof_bytes[i] = 0;
+    }
+    return DMOLP_OK;
+}
+
+int dmolp_kernel_profile(dmolp_ctx *c, int kernel, double *total_ms, int64_t *launches, double *bytes) {
+    if (!c || kernel < 0 || kernel > 1) return fail(DMOLP_ERR_ARG, "bad context or kernel id");
+    if (total_ms) *total_ms = c->prof_ms[kernel];
+    if (launches) *launches = c->prof_launches[kernel];
+    if (bytes) *bytes = c->prof_bytes[kernel];
+    return DMOLP_OK;
+}
+
+int dmolp_metrics(dmolp_ctx *c, int k, int64_t *edge_cut, int64_t *vertex_counts, int64_t *edge_counts) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (k < 1 || k > DMOLP_MAX_K) return fail(DMOLP_ERR_ARG, "k out of range");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    unsigned long long arcs = 0;
+    std::vector<long long> vc, intra;
+    int bad = 0;
+    int st = run_stats(c, k, &arcs, vc, intra, &bad);
+    if (st) return st;
+    if (edge_cut) *edge_cut = (int64_t)(arcs >> 1);
+    for (int p = 0; p < k; ++p) {
+        if (vertex_counts) vertex_counts[p] = vc[p];
+        if (edge_counts) edge_counts[p] = intra[p] / 2;
+    }
+    if (bad || (arcs & 1ull)) return fail(DMOLP_ERR_BAD_LABELS, "label outside [0,k) or odd cut-arc count");
+    return DMOLP_OK;
+}
+
+int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *vertex_counts, int64_t *edge_counts,
+                 dmolp_phase1_info *info) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (k < 1 || k > DMOLP_MAX_K) return fail(DMOLP_ERR_ARG, "k out of range [1, 1024]");
+    if (theta < 1)
+        return fail(DMOLP_ERR_ARG, "theta must be >= 1 (with theta = 0 the reference expands nothing and never ends)");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    Buffers &b = c->b;
+    const int64_t nv = c->nv;
+    dmolp_phase1_info inf;
+    std::memset(&inf, 0, sizeof(inf));
+    DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
+
+    // ---- hubs and first seed on the host (order-dependent; see the top of this file) ----
+    std::vector<int> hubs = find_hubs(c->h_rawdeg);
+    std::pair<int, int> first(-1, -1);
+    for (int64_t v = nv - 1; v >= 0; --v) {  // init.cpp:179-187, including its id-vs-degree tie test
+        const int d = c->h_rawdeg[v];
+        if (d > first.second || (d == first.second && (int)v < first.second)) first = std::make_pair((int)v, d);
+    }
+    inf.num_hubs = (int64_t)hubs.size();
+    std::vector<int> seeds;
+    std::vector<char> used(hubs.size(), 0);
+    if (nv > 0) seeds.push_back(first.first);
+    auto hub_index = [&](int s) -> int64_t {
+        auto it = std::find(hubs.begin(), hubs.end(), s);
+        return it == hubs.end() ? -1 : (int64_t)(it - hubs.begin());
+    };
+    DMOLP_CUDA(cudaMemsetAsync(b.p1te, 0, sizeof(unsigned long long), c->stream));
+    if (nv > 0 && !hubs.empty() && k > 1) {
+        DMOLP_CUDA(cudaMemcpyAsync(b.hubs, hubs.data(), hubs.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                   c->stream));
+        DMOLP_CUDA(cudaMemsetAsync(b.hub_used, 0, hubs.size(), c->stream));
+        DMOLP_CUDA(cudaMemsetAsync(b.covered, 0, (size_t)nv, c->stream));
+        int64_t fi = hub_index(first.first);
+        if (fi >= 0) {
+            used[fi] = 1;
+            DMOLP_CUDA(cudaMemsetAsync(b.hub_used + fi, 1, 1, c->stream));
+        }
+        size_t balls = 0;
+        for (int p = 1; p < k; ++p) {  // seed.cpp:206-226
+            for (; balls < seeds.size(); ++balls) p1_mark_ball(c, seeds[balls]);
+            p1_hub_argmax(c, (int64_t)hubs.size());
+            unsigned long long best = 0;
+            DMOLP_CUDA(cudaMemcpyAsync(&best, b.best, sizeof(best), cudaMemcpyDeviceToHost, c->stream));
+            int st = sync(c);
+            if (st) return st;
+            if (best == 0) break;
+            const int64_t idx = (int64_t)(0xffffffffu - (unsigned)(best & 0xffffffffull));
+            seeds.push_back(hubs[idx]);
+            used[idx] = 1;
+            DMOLP_CUDA(cudaMemsetAsync(b.hub_used + idx, 1, 1, c->stream));
+        }
+    }
+    inf.num_seeds_found = (int32_t)seeds.size();
+    // Seed completion (the reference reads past its seed vector here, partition.cpp:347): unused hubs by
+    // raw degree (first in hub order on ties), then other vertices by raw degree (lowest id on ties).
+    if ((int64_t)seeds.size() < k && nv > 0) {
+        std::vector<char> is_seed(nv, 0);
+        for (int s : seeds) is_seed[s] = 1;
+        while ((int)seeds.size() < k) {
+            int bestv = -1, bd = -1;
+            for (size_t i = 0; i < hubs.size(); ++i)
+                if (!used[i] && c->h_rawdeg[hubs[i]] > bd) {
+                    bd = c->h_rawdeg[hubs[i]];
+                    bestv = hubs[i];
+                }
+            if (bestv == -1)
+                for (int64_t v = 0; v < nv; ++v)
+                    if (!is_seed[v] && c->h_rawdeg[v] > bd) {
+                        bd = c->h_rawdeg[v];
+                        bestv = (int)v;
+                    }
+            if (bestv == -1) break;
+            seeds.push_back(bestv);
+            is_seed[bestv] = 1;
+            int64_t hi = hub_index(bestv);
+            if (hi >= 0) used[hi] = 1;
+        }
+    }
+    std::vector<int32_t> seedk(k, -1);
+    for (int p = 0; p < k && p < (int)seeds.size(); ++p) seedk[p] = seeds[p];
+    if (seeds_out) std::copy(seedk.begin(), seedk.end(), seeds_out);
+
+    // ---- growth rounds (partition.cpp:335-604) ----
+    p1_init_labels(c);
+    DMOLP_CUDA(cudaMemsetAsync(b.psize, 0, DMOLP_MAX_K * sizeof(long long), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.npart, 0, DMOLP_MAX_K * sizeof(int32_t), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.p1cnt, 0, 8 * sizeof(int), c->stream));
+    // seeds go through the need[] buffer as staging (k ints)
+    DMOLP_CUDA(cudaMemcpyAsync(b.need, seedk.data(), k * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    p1_set_seeds(c, b.need, k);
+    int cur = 0, rounds = 0;
+    std::vector<long long> psize(k);
+    while (nv > 0) {
+        int cnt[8];
+        DMOLP_CUDA(cudaMemcpyAsync(cnt, b.p1cnt, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+        DMOLP_CUDA(cudaMemcpyAsync(psize.data(), b.psize, k * sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+        int st = sync(c);
+        if (st) return st;
+        if (cnt[3] >= nv) break;
+        if (cnt[0] == 0) {  // every frontier empty: all unlabelled vertices go to the smallest part
+            int best = 0;
+            for (int p = 1; p < k; ++p)
+                if (psize[p] < psize[best]) best = p;
+            p1_fallback(c, best, cur);
+        }
+        p1_round(c, k, theta, cur);
+        cur ^= 1;
+        ++rounds;
+    }
+    inf.rounds = rounds;
+
+    // ---- initial metrics (phase1.cpp:83-153) ----
+    unsigned long long arcs = 0;
+    std::vector<long long> vc, intra;
+    int bad = 0;
+    int st = run_stats(c, k, &arcs, vc, intra, &bad);
+    if (st) return st;
+    DMOLP_CUDA(cudaEventRecord(c->ev1, c->stream));
+    unsigned long long te = 0;
+    DMOLP_CUDA(cudaMemcpyAsync(&te, b.p1te, sizeof(te), cudaMemcpyDeviceToHost, c->stream));
+    st = sync(c);
+    if (st) return st;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    inf.gpu_ms = ms;
+    inf.traversed_edges = te;
+    inf.initial_edge_cut = (int64_t)(arcs / 2);
+    const double ev = (double)nv / k;
+    double mv = 0;
+    for (int p = 0; p < k; ++p) mv = std::max(mv, vc[p] / ev);
+    double tot = 0;
+    std::vector<long long> ec(k);
+    for (int p = 0; p < k; ++p) {
+        ec[p] = intra[p] / 2;
+        tot += (double)ec[p];
+    }
+    const double ee = tot / k;
+    double me = 0;
+    for (int p = 0; p < k; ++p) me = std::max(me, ec[p] / ee);
+    inf.initial_vertex_balance = mv;
+    inf.initial_edge_balance = me;
+    for (int p = 0; p < k; ++p) {
+        if (vertex_counts) vertex_counts[p] = vc[p];
+        if (edge_counts) edge_counts[p] = ec[p];
+    }
+    if (info) *info = inf;
+    if (bad) return fail(DMOLP_ERR_BAD_LABELS, "phase 1 left a label outside [0,k)");
+    return DMOLP_OK;
+}
+
+int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_result *res, dmolp_lp_record *records,
+                 int max_records) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (k < 1 || k > DMOLP_MAX_K) return fail(DMOLP_ERR_ARG, "k out of range [1, 1024]");
+    if (!cfg) return fail(DMOLP_ERR_ARG, "null config");
+    if (cfg->mode != DMOLP_LP_MODE_REF && cfg->mode != DMOLP_LP_MODE_FIXED) return fail(DMOLP_ERR_ARG, "bad mode");
+    if (cfg->mode == DMOLP_LP_MODE_FIXED && (cfg->iterations < 0 || cfg->iterations > kMaxIter))
+        return fail(DMOLP_ERR_ARG, "iterations must be in [0, 500]");
+    if (cfg->cap != DMOLP_LP_CAP_REF && cfg->cap != DMOLP_LP_CAP_FULL) return fail(DMOLP_ERR_ARG, "bad cap");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    Buffers &b = c->b;
+    LpLaunch L;
+    L.k = k;
+    L.eff = cfg->cap == DMOLP_LP_CAP_FULL ? k : std::min(k, 32);
+    L.mode = cfg->mode;
+    const int max_iter = cfg->mode == DMOLP_LP_MODE_REF ? kMaxIter : cfg->iterations;
+
+    DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.stamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
+    lp_reset_stats(c, k, nullptr);
+    lp_stats(c, k, nullptr, nullptr);
+    lp_init_end(c, cfg->mode);
+    int st = check_launch(c);
+    if (st) return st;
+    int stopped = 0;
+    for (int t = 1; t <= max_iter; ++t) {
+        lp_iteration(c, L, t);
+        if (cfg->mode == DMOLP_LP_MODE_REF && (t % 8) == 0) {
+            DMOLP_CUDA(cudaMemcpyAsync(&stopped, &b.ctrl->stopped, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            st = sync(c);
+            if (st) return st;
+            if (stopped) break;
+        }
+    }
+    DMOLP_CUDA(cudaEventRecord(c->ev1, c->stream));
+    LpControl ctl;
+    DMOLP_CUDA(cudaMemcpyAsync(&ctl, b.ctrl, sizeof(ctl), cudaMemcpyDeviceToHost, c->stream));
+    std::vector<unsigned long long> hv(k), hi(k);
+    DMOLP_CUDA(cudaMemcpyAsync(hv.data(), b.vc, k * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(hi.data(), b.intra, k * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    std::vector<LpRecordDev> recs(kMaxIter);
+    DMOLP_CUDA(cudaMemcpyAsync(recs.data(), b.rec, kMaxIter * sizeof(LpRecordDev), cudaMemcpyDeviceToHost, c->stream));
+    st = sync(c);
+    if (st) return st;
+    if (ctl.error) return fail(DMOLP_ERR_BAD_LABELS, "label outside [0,k) or odd cut-arc count");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    std::vector<long long> vc(k), ec(k);
+    for (int p = 0; p < k; ++p) {
+        vc[p] = (long long)hv[p];
+        ec[p] = (long long)(hi[p] / 2);
+    }
+    if (c->profiling) {
+        // algorithmic bytes per launch: scan = 8 B per neighbour arc (id + label) + 20 B per candidate (two
+        // offsets, own label) + 4 B per listed candidate + 21 B per boundary record; stats = 8 B per arc +
+        // 20 B per vertex
+        for (size_t i = 0; i < c->prof_kind.size(); ++i) {
+            const int t = c->prof_iter[i], kind = c->prof_kind[i];
+            if (t > ctl.iters_run) continue;
+            const LpRecordDev &d = recs[t - 1];
+            double bytes = 0;
+            if (kind == 0) {
+                const double ncand = t == 1 ? (double)c->nv : (double)d.candidates;
+                bytes = 8.0 * (double)d.te_cand + 20.0 * ncand + (t > 1 ? 4.0 * ncand : 0.0) + 21.0 * d.boundary;
+            } else {
+                if (d.te_stats == 0) continue;  // statistics skipped this iteration
+                bytes = 8.0 * (double)c->narcs + 20.0 * (double)c->nv;
+            }
+            float ems = 0;
+            cudaEventElapsedTime(&ems, c->prof_events[2 * i], c->prof_events[2 * i + 1]);
+            c->prof_ms[kind] += ems;
+            c->prof_launches[kind] += 1;
+            c->prof_bytes[kind] += bytes;
+        }
+        for (cudaEvent_t e : c->prof_events) cudaEventDestroy(e);
+        c->prof_events.clear();
+        c->prof_kind.clear();
+        c->prof_iter.clear();
+    }
+    dmolp_lp_result r;
+    std::memset(&r, 0, sizeof(r));
+    r.edge_cut = ctl.prev_cut;
+    r.iterations_run = ctl.iters_run;
+    r.stop_reason = ctl.stop_reason;
+    balances(vc, ec, k, &r.vertex_balance, &r.edge_balance, &r.total_vertices, &r.total_edges);
+    r.gpu_ms = ms;
+    for (int i = 0; i < ctl.iters_run; ++i) {
+        const LpRecordDev &d = recs[i];
+        r.traversed_edges += d.te_prev + d.te_cand + d.te_sel + d.te_stats;
+        if (records && i < max_records) {
+            dmolp_lp_record &o = records[i];
+            o.iteration = d.iteration;
+            o.window = d.window;
+            o.candidates = d.candidates < 0 ? (int32_t)c->nv : d.candidates;
+            o.changes = d.changes;
+            o.boundary = d.boundary;
+            o.reserved = 0;
+            o.edge_cut = d.edge_cut;
+            o.te_prev = d.te_prev;
+            o.te_cand = d.te_cand;
+            o.te_sel = d.te_sel;
+            o.te_stats = d.te_stats;
+        }
+    }
+    if (res) *res = r;
+    return DMOLP_OK;
+}
+
+// Per-iteration history of the last dmolp_lp_run: penalties[iters][k] and counts[iters][2k] (vertex counts,
+// then intra-part edge counts).  Not part of the reference interface; used by the parity tests.
+int dmolp_lp_history(dmolp_ctx *c, int k, int iters, double *penalties, int64_t *counts) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (k < 1 || k > DMOLP_MAX_K || iters < 0 || iters > kMaxIter) return fail(DMOLP_ERR_ARG, "bad k/iters");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    std::vector<double> ph((size_t)iters * DMOLP_MAX_K);
+    std::vector<long long> ch((size_t)iters * 2 * DMOLP_MAX_K);
+    if (iters) {
+        DMOLP_CUDA(cudaMemcpyAsync(ph.data(), c->b.penhist, ph.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                   c->stream));
+        DMOLP_CUDA(cudaMemcpyAsync(ch.data(), c->b.cnthist, ch.size() * sizeof(long long), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    }
+    int st = sync(c);
+    if (st) return st;
+    for (int t = 0; t < iters; ++t)
+        for (int p = 0; p < k; ++p) {
+            if (penalties) penalties[(size_t)t * k + p] = ph[(size_t)t * DMOLP_MAX_K + p];
+            if (counts) {
+                counts[(size_t)t * 2 * k + p] = ch[(size_t)t * 2 * DMOLP_MAX_K + p];
+                counts[(size_t)t * 2 * k + k + p] = ch[(size_t)t * 2 * DMOLP_MAX_K + DMOLP_MAX_K + p];
+            }
+        }
+    return DMOLP_OK;
+}
+
+int dmolp_window_select(dmolp_ctx *c, int k, int iteration, const double *RE, const int32_t *prev, int64_t nprev,
+                        int32_t *out, int64_t *nout) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (k < 1 || k > DMOLP_MAX_K || iteration < 1 || iteration > kMaxIter || !RE || !out || !nout || nprev < 0 ||
+        (nprev && !prev))
+        return fail(DMOLP_ERR_ARG, "bad arguments");
+    // keep only in-range previous vertices, deduplicated (gpu_lp_boundary.cu:210 skips the others)
+    std::vector<int32_t> pv;
+    pv.reserve(nprev);
+    for (int64_t i = 0; i < nprev; ++i)
+        if (prev[i] >= 0 && prev[i] < c->nv) pv.push_back(prev[i]);
+    std::sort(pv.begin(), pv.end());
+    pv.erase(std::unique(pv.begin(), pv.end()), pv.end());
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    {  // the selection indexes per-label arrays by label: check every label is in [0,k) first
+        unsigned long long arcs = 0;
+        std::vector<long long> vc, intra;
+        int bad = 0;
+        int st0 = run_stats(c, k, &arcs, vc, intra, &bad);
+        if (st0) return st0;
+        if (bad) return fail(DMOLP_ERR_BAD_LABELS, "label outside [0,k)");
+    }
+    const int t = iteration;
+    Buffers &b = c->b;
+    DMOLP_CUDA(cudaMemsetAsync(b.stamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
+    if (!pv.empty())
+        DMOLP_CUDA(cudaMemcpyAsync(b.win[(t - 1) & 1], pv.data(), pv.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                   c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(b.RE, RE, k * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    lp_window_from_list(c, k, t, b.RE, (int)pv.size());
+    LpCounters cn;
+    DMOLP_CUDA(cudaMemcpyAsync(&cn, b.cnt, sizeof(cn), cudaMemcpyDeviceToHost, c->stream));
+    int st = sync(c);
+    if (st) return st;
+    const int n = cn.nwin[t & 1];
+    if (n)
+        DMOLP_CUDA(cudaMemcpyAsync(out, b.win[t & 1], (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    st = sync(c);
+    if (st) return st;
+    std::sort(out, out + n);
+    *nout = n;
+    return DMOLP_OK;
+}
+
+int dmolp_lp_apply(dmolp_ctx *c, int k, int cap, const double *penalty, const int32_t *window, int64_t nwindow,
+                   int32_t *changed_nodes, int32_t *changed_labels, int64_t *nchanged) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (k < 1 || k > DMOLP_MAX_K || !penalty || nwindow < 0 || (nwindow && !window) || !nchanged)
+        return fail(DMOLP_ERR_ARG, "bad arguments");
+    if (cap != DMOLP_LP_CAP_REF && cap != DMOLP_LP_CAP_FULL) return fail(DMOLP_ERR_ARG, "bad cap");
+    std::vector<int32_t> w;
+    w.reserve(nwindow);
+    for (int64_t i = 0; i < nwindow; ++i)
+        if (window[i] >= 0 && window[i] < c->nv) w.push_back(window[i]);
+    std::sort(w.begin(), w.end());
+    w.erase(std::unique(w.begin(), w.end()), w.end());
+    std::vector<double> tp(k);
+    for (int p = 0; p < k; ++p) tp[p] = 1.0 + penalty[p];
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    Buffers &b = c->b;
+    const int n = (int)w.size();
+    if (n) DMOLP_CUDA(cudaMemcpyAsync(b.cand, w.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(b.tpen, tp.data(), k * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const int eff = cap == DMOLP_LP_CAP_FULL ? k : std::min(k, 32);
+    lp_apply_list(c, k, eff, n);
+    std::vector<int32_t> bv(n), bo(n), bn(n);
+    if (n) {
+        DMOLP_CUDA(cudaMemcpyAsync(bv.data(), b.bv, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        DMOLP_CUDA(cudaMemcpyAsync(bo.data(), b.bown, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        DMOLP_CUDA(cudaMemcpyAsync(bn.data(), b.bnew, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    }
+    int st = sync(c);
+    if (st) return st;
+    int64_t m = 0;
+    for (int i = 0; i < n; ++i)
+        if (bn[i] != bo[i]) {
+            if (changed_nodes) changed_nodes[m] = bv[i];
+            if (changed_labels) changed_labels[m] = bn[i];
+            ++m;
+        }
+    *nchanged = m;
+    return DMOLP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,38 @@
+// Host-side launchers of the DMOLP kernels (one translation unit per kernel family).
+#pragma once
+
+#include "device_state.cuh"
+
+namespace dmolp {
+
+// ---- segmented radix select (select_kernels.cu) ----
+// Records i < *n_dev carry a segment seg[i] in [0,nseg) and a 64-bit key whose top bit is below
+// `keybits`; keys are unique.  For every segment p, marks sel[i] = 1 on the need[p] records with the
+// smallest keys (need[] is consumed).  sel[] must be zero on entry.  `stopped` (may be null) turns the
+// launches into no-ops once it is non-zero.
+void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, const int *n_dev, int nseg, int keybits,
+                     uint8_t *sel, const int *stopped);
+
+// ---- LP loop (lp_kernels.cu) ----
+struct LpLaunch {
+    int k;
+    int eff;       // labels scored: min(k,32) or k
+    int mode;      // DMOLP_LP_MODE_*
+};
+void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped);
+void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip);
+void lp_init_end(dmolp_ctx *c, int mode);
+void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t);
+// one-off pieces used by dmolp_window_select / dmolp_lp_apply
+void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int nprev);
+void lp_apply_list(dmolp_ctx *c, int k, int eff, int n);
+
+// ---- phase 1 (seed_kernels.cu) ----
+void p1_mark_ball(dmolp_ctx *c, int seed);
+void p1_hub_argmax(dmolp_ctx *c, int64_t nhubs);
+void p1_init_labels(dmolp_ctx *c);
+void p1_set_seeds(dmolp_ctx *c, const int32_t *seeds_dev, int nseeds);
+void p1_fallback(dmolp_ctx *c, int best_part, int cur);
+void p1_round(dmolp_ctx *c, int k, int theta, int cur);
+
+}  // namespace dmolp

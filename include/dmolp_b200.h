@@ -1,0 +1,182 @@
+/*
+ * dmolp_b200.h -- C-ABI of the B200-native DMOLP partitioning path (libdmolp_b200.so).
+ *
+ * One context owns one CUDA device, one stream and a graph resident in HBM (int64 offsets, int32
+ * neighbour ids, int32 labels).  Every entry point returns a status code (DMOLP_OK == 0) and never aborts;
+ * dmolp_last_error() describes the last failure on the calling thread.  All pointers are HOST pointers
+ * unless the name says _device.  Calls on one context must come from one host thread at a time.
+ *
+ * The reference (DMOLP, C++/MPI/CUDA) has no C-ABI; each entry point below names the reference interface
+ * it replaces (paths relative to the reference tree).  The reference's C++ signatures themselves are
+ * provided on top of this ABI by libdmolp_dropin.so.
+ */
+#ifndef DMOLP_B200_H
+#define DMOLP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define DMOLP_OK 0
+#define DMOLP_ERR_ARG 1            /* bad argument (size, k, theta, null pointer) */
+#define DMOLP_ERR_CUDA 2           /* a CUDA runtime call failed */
+#define DMOLP_ERR_NOMEM 3          /* device or host allocation failed */
+#define DMOLP_ERR_STATE 4          /* call out of order (e.g. no graph uploaded) */
+#define DMOLP_ERR_BAD_LABELS 5     /* a label outside [0,k) or an odd cut-arc count: where the reference
+                                      calls MPI_Abort (src/phase2/phase2.cpp:239-250) */
+#define DMOLP_ERR_NO_GPU 6         /* no CUDA device */
+
+/* ---- modes ---- */
+#define DMOLP_LP_MODE_REF 0        /* the reference's loop: at most 500 iterations, stops on an empty
+                                      window, on zero changes, or after 10 consecutive iterations whose
+                                      edge-cut change is below 3 % (src/phase2/phase2.cpp:263-416) */
+#define DMOLP_LP_MODE_FIXED 1      /* exactly `iterations` iterations, no early stop */
+#define DMOLP_LP_CAP_REF 0         /* score labels < min(k,32), as boundaryLPKernel_unified does
+                                      (src/phase2/gpu_lp_boundary.cu:360) */
+#define DMOLP_LP_CAP_FULL 1        /* score every label < k (extension; its own oracle) */
+
+#define DMOLP_MAX_K 1024
+
+typedef struct dmolp_ctx dmolp_ctx;
+
+typedef struct {
+    int64_t initial_edge_cut;      /* Phase1Metrics::initial_edge_cut  (include/graph_types.h:277) */
+    double initial_vertex_balance; /* Phase1Metrics::initial_vertex_balance */
+    double initial_edge_balance;   /* Phase1Metrics::initial_edge_balance */
+    int32_t num_seeds_found;       /* seeds found by the reference rule (the rest by seed completion) */
+    int32_t rounds;                /* expansion rounds */
+    int64_t num_hubs;
+    uint64_t traversed_edges;      /* arcs read by ball marking + expansion */
+    double gpu_ms;                 /* device time of the phase (CUDA events) */
+} dmolp_phase1_info;
+
+typedef struct {
+    int32_t mode;                  /* DMOLP_LP_MODE_* */
+    int32_t iterations;            /* DMOLP_LP_MODE_FIXED: iterations to run */
+    int32_t cap;                   /* DMOLP_LP_CAP_* */
+    int32_t flags;                 /* reserved, 0 */
+} dmolp_lp_config;
+
+typedef struct {
+    int64_t edge_cut;              /* PartitioningMetrics::edge_cut (include/graph_types.h:313) */
+    double vertex_balance;
+    double edge_balance;
+    int32_t iterations_run;
+    int32_t stop_reason;           /* 0 limit, 1 empty window, 2 no changes, 3 converged */
+    uint64_t traversed_edges;      /* sum over iterations of the four traversed-edge terms */
+    int64_t total_vertices;
+    int64_t total_edges;
+    double gpu_ms;                 /* device time of the LP loop (CUDA events) */
+} dmolp_lp_result;
+
+typedef struct {                   /* one per LP iteration */
+    int32_t iteration;
+    int32_t window;                /* selected boundary vertices */
+    int32_t candidates;
+    int32_t changes;
+    int32_t boundary;              /* boundary candidates (before the per-label selection) */
+    int32_t reserved;
+    int64_t edge_cut;
+    uint64_t te_prev, te_cand, te_sel, te_stats;
+} dmolp_lp_record;
+
+const char *dmolp_last_error(void);
+
+/* Create a context on CUDA device `device`.  Replaces the device set-up of allocateGPU
+ * (src/main.cpp:25-121), which picks local_rank % device_count. */
+int dmolp_create(int device, dmolp_ctx **out);
+int dmolp_destroy(dmolp_ctx *ctx);
+
+/* Copy a CSR graph to the device and keep it resident.  offsets[nv+1] (int64), indices[narcs] (int32,
+ * 0 <= id < nv), raw_degree[nv] (the per-line token count phase 1 sorts by; NULL = CSR degree).
+ * Replaces the per-iteration subgraph allocation and copies of runBoundaryLPOnGPU_SubgraphUnified
+ * (src/phase2/gpu_lp_boundary.cu:456-471) and the Graph built by build_local_graph_and_ghosts
+ * (src/phase1/partition.cpp:182). */
+int dmolp_graph_upload(dmolp_ctx *ctx, int64_t nv, int64_t narcs, const int64_t *offsets, const int32_t *indices,
+                       const int32_t *raw_degree);
+
+/* Phase 1: hubs, first seed, seeds, theta-limited multi-source BFS growth, initial metrics.  Leaves the
+ * labels on the device.  seeds_out[k], vertex_counts[k], edge_counts[k] may be NULL.
+ * Replaces find_hub_nodes / find_first_seed (src/phase1/init.cpp:139-187), find_seeds
+ * (src/phase1/seed.cpp:192), partition_expansion (src/phase1/partition.cpp:323) and the metrics of
+ * run_phase1 (src/phase1/phase1.cpp:83-153). */
+int dmolp_phase1(dmolp_ctx *ctx, int k, int theta, int32_t *seeds_out, int64_t *vertex_counts,
+                 int64_t *edge_counts, dmolp_phase1_info *info);
+
+/* Phase 2: boundary label propagation with balance penalties on the resident labels.
+ * records[max_records] (may be NULL) receives one entry per iteration.
+ * Replaces run_phase2 (src/phase2/phase2.cpp:256-449). */
+int dmolp_lp_run(dmolp_ctx *ctx, int k, const dmolp_lp_config *cfg, dmolp_lp_result *res, dmolp_lp_record *records,
+                 int max_records);
+
+/* The fused edge-cut / balance reduction on the resident labels: cut = arcs with different labels / 2,
+ * vertex_counts[p], edge_counts[p] = intra-part arcs / 2.  Replaces computeEdgeCut and
+ * computePartitionStats (src/phase2/phase2.cpp:55-117, 214-253). */
+int dmolp_metrics(dmolp_ctx *ctx, int k, int64_t *edge_cut, int64_t *vertex_counts, int64_t *edge_counts);
+
+/* Resident labels <-> host (int32[nv]). */
+int dmolp_labels_get(dmolp_ctx *ctx, int32_t *labels);
+int dmolp_labels_set(dmolp_ctx *ctx, const int32_t *labels);
+
+/* One boundary-window selection on the resident graph and labels, from an explicit previous window.
+ * RE[k] as calculatePenalties returns it; iteration is 1-based.  out[] needs room for nv entries; the
+ * selected set is returned in ascending id order.  Replaces expandBoundaryNodes
+ * (src/phase2/gpu_lp_boundary.cu:185-305). */
+int dmolp_window_select(dmolp_ctx *ctx, int k, int iteration, const double *RE, const int32_t *prev, int64_t nprev,
+                        int32_t *out, int64_t *nout);
+
+/* One synchronous LP update of `window` with the given penalties; labels of moved vertices are changed
+ * on the device and reported (changed_nodes/changed_labels need room for nwindow entries).  Replaces
+ * runBoundaryLPOnGPU_Streaming / _SubgraphUnified and boundaryLPKernel_unified
+ * (src/phase2/gpu_lp_boundary.cu:327-565). */
+int dmolp_lp_apply(dmolp_ctx *ctx, int k, int cap, const double *penalty, const int32_t *window, int64_t nwindow,
+                   int32_t *changed_nodes, int32_t *changed_labels, int64_t *nchanged);
+
+/* Per-iteration history of the last dmolp_lp_run: penalties[iters*k] (the penalty vector each iteration
+ * used) and counts[iters*2k] (vertex counts then intra-part edge counts after each iteration).  No
+ * reference counterpart: calculatePenalties' vectors and computePartitionStats' counts are internal there
+ * (src/phase2/phase2.cpp:297, 393); exposed for bitwise parity checks. */
+int dmolp_lp_history(dmolp_ctx *ctx, int k, int iters, double *penalties, int64_t *counts);
+
+/* Device pointers of the resident arrays (for callers that keep data on the GPU). */
+int dmolp_device_labels(dmolp_ctx *ctx, int32_t **labels_device);
+
+/* The CUDA stream every kernel of this context runs on (a cudaStream_t), e.g. to record timing events on it. */
+void *dmolp_stream(dmolp_ctx *ctx);
+
+/* Keep a device-side copy of the current labels / copy it back (device to device, on the context's stream).
+ * No reference counterpart: lets a caller rerun phase 2 from the same start without a host round trip. */
+int dmolp_labels_save(dmolp_ctx *ctx);
+int dmolp_labels_restore(dmolp_ctx *ctx);
+
+/* Optional per-kernel timing: when enabled, dmolp_lp_run brackets its fused scan and statistics kernels with
+ * CUDA events and accumulates their device time and algorithmic bytes (read with dmolp_kernel_profile).
+ * kernel: 0 = boundary/decision scan, 1 = cut/balance statistics pass.  No reference counterpart. */
+int dmolp_set_profiling(dmolp_ctx *ctx, int enable);
+int dmolp_kernel_profile(dmolp_ctx *ctx, int kernel, double *total_ms, int64_t *launches, double *bytes);
+
+/* ---- host-side graph loading (no device work) ----
+ * Parse the reference's adjacency text: first line V, line i+1 = neighbour ids of vertex i.  Produces the
+ * CSR the reference builds (rows sorted and de-duplicated, self-loops kept) and the raw per-line token
+ * count.  Replaces load_graph (src/phase1/init.cpp:25-100) and the CSR construction of
+ * build_local_graph_and_ghosts (src/phase1/partition.cpp:227-262). */
+typedef struct dmolp_host_graph dmolp_host_graph;
+int dmolp_adjtext_load(const char *path, dmolp_host_graph **out);
+const char *dmolp_adjtext_error(void);
+int64_t dmolp_host_graph_nv(const dmolp_host_graph *g);
+int64_t dmolp_host_graph_narcs(const dmolp_host_graph *g);
+const int64_t *dmolp_host_graph_offsets(const dmolp_host_graph *g);
+const int32_t *dmolp_host_graph_indices(const dmolp_host_graph *g);
+const int32_t *dmolp_host_graph_raw_degree(const dmolp_host_graph *g);
+void dmolp_host_graph_free(dmolp_host_graph *g);
+
+/* Number of kernel launches this context has issued (all entry points). */
+int64_t dmolp_kernel_launches(const dmolp_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
