@@ -148,10 +148,11 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
         return p.phase2(w["k"], mode="fixed", iterations=w["iters"], records=False)
 
     sampler = ClockSampler(local_rank)
-    sampler.start()
-    t_end = time.time() + 1.0  # keep the GPU busy ~1 s before warm-up so the clock samples see load
-    while time.time() < t_end:
-        step()
+    if not args.quick:
+        sampler.start()
+        t_end = time.time() + 1.0  # keep the GPU busy ~1 s before warm-up so the clock samples see load
+        while time.time() < t_end:
+            step()
     for _ in range(args.warmup):
         step()
     p.lib.dmolp_set_profiling(p.ctx, 1)
@@ -171,11 +172,11 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    clocks = sampler.stop()
+    clocks = sampler.stop() if not args.quick else None
     launches = p.kernel_launches() - launches0
     elapsed = e0.elapsed_time(e1) / 1e3
     prof = {}
-    for kid, name in ((0, "lp_scan"), (1, "stats")):
+    for kid, name in ((0, "boundary_test"), (1, "lp_decide"), (2, "window_mark"), (3, "cut_update")):
         import ctypes
 
         ms, n, by = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
@@ -184,6 +185,16 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
     p.lib.dmolp_set_profiling(p.ctx, 0)
     final_labels = p.labels()
 
+    rec_step = p.phase2(w["k"], mode="fixed", iterations=w["iters"], records=True) if args.records else None
+    if rec_step is not None:
+        for r in rec_step.records:
+            print(json.dumps({f: getattr(r, f) for f, _ in r._fields_}), file=sys.stderr)
+        p._check(p.lib.dmolp_labels_restore(p.ctx))
+        p.phase2(w["k"], mode="fixed", iterations=w["iters"], records=False)
+    if args.quick:
+        p.close()
+        return {"metric": "LP traversed edges/s", "value": te / elapsed, "unit": "TE/s", "ms_per_step":
+                elapsed / args.steps * 1e3, "quick": True, "kernels": prof, "gpu_launches": int(launches)}
     # ---- end to end through the public API, host buffers in pinned memory ----
     off_h = torch.from_numpy(g.offsets).pin_memory()
     col_h = torch.from_numpy(g.indices).pin_memory()
@@ -354,6 +365,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-iters", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="timed steps only: no clock soak, e2e or CPU baseline")
+    ap.add_argument("--records", action="store_true", help="print one step's per-iteration records to stderr")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", "0"))
@@ -379,7 +392,7 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0 and line is not None:
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and not args.quick:
             g = make_graph(w)
             import oracle
 

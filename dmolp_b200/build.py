@@ -86,8 +86,6 @@ def build_cuda(force: bool = False, ptxas_log: list[str] | None = None) -> str:
 def build_dropin(force: bool = False) -> str:
     out = os.path.join(LIB, "libdmolp_dropin.so")
     srcs = [os.path.join(CSRC, s) for s in DROPIN_SOURCES]
-    if not all(os.path.exists(s) for s in srcs):
-        return ""
     deps = srcs + [os.path.join(CSRC, "dropin_types.hpp"),
                    os.path.join(INCLUDE, "dmolp_b200.h"), os.path.join(LIB, "libdmolp_b200.so")]
     if force or _newer(out, deps):

@@ -25,6 +25,7 @@ EXPORTS = [
     "dmolp_adjtext_error", "dmolp_host_graph_nv", "dmolp_host_graph_narcs", "dmolp_host_graph_offsets",
     "dmolp_host_graph_indices", "dmolp_host_graph_raw_degree", "dmolp_host_graph_free", "dmolp_stream",
     "dmolp_labels_save", "dmolp_labels_restore", "dmolp_set_profiling", "dmolp_kernel_profile",
+    "dmolp_find_seeds", "dmolp_expand_partitions", "dmolp_current_device",
 ]
 
 
@@ -46,14 +47,15 @@ class LpResult(ctypes.Structure):
 
 class LpRecord(ctypes.Structure):
     _fields_ = [("iteration", c_int32), ("window", c_int32), ("candidates", c_int32), ("changes", c_int32),
-                ("boundary", c_int32), ("pad", c_int32), ("edge_cut", c_int64), ("te_prev", c_uint64), ("te_cand", c_uint64), ("te_sel", c_uint64),
-                ("te_stats", c_uint64)]
+                ("boundary", c_int32), ("reserved", c_int32), ("edge_cut", c_int64), ("te_prev", c_uint64),
+                ("te_cand", c_uint64), ("te_sel", c_uint64), ("te_stats", c_uint64), ("arcs_read", c_uint64)]
 
 
 def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     vp = c_void_p
     lib.dmolp_last_error.restype = c_char_p
     lib.dmolp_last_error.argtypes = []
+    lib.dmolp_current_device.argtypes = []
     lib.dmolp_create.argtypes = [c_int, POINTER(vp)]
     lib.dmolp_destroy.argtypes = [vp]
     lib.dmolp_graph_upload.argtypes = [vp, c_int64, c_int64, vp, vp, vp]
@@ -84,5 +86,7 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_labels_save.argtypes = [vp]
     lib.dmolp_labels_restore.argtypes = [vp]
     lib.dmolp_set_profiling.argtypes = [vp, c_int]
+    lib.dmolp_find_seeds.argtypes = [vp, c_int, c_int32, vp, c_int64, vp, POINTER(c_int32)]
+    lib.dmolp_expand_partitions.argtypes = [vp, c_int, c_int, vp, c_int32, POINTER(c_int32)]
     lib.dmolp_kernel_profile.argtypes = [vp, c_int, POINTER(c_double), POINTER(c_int64), POINTER(c_double)]
     return lib

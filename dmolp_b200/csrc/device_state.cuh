@@ -5,22 +5,31 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
 
 namespace dmolp {
 
-// Per-iteration counters of the LP loop (one instance, reset by the first kernel of each iteration).
+// Degree classes of the bucketed kernels: thread per vertex, warp per vertex, block per vertex.
+constexpr int kSmallDeg = 16;    // deg <= 16: one thread walks the row
+constexpr int kLargeDeg = 4096;  // deg > 4096: one block walks the row
+constexpr int kChunk = 4096;     // row chunk of the window-marking kernel
+
+// Per-iteration counters of the LP loop (reset by the first kernel of each iteration).
 struct LpCounters {
-    int ncand;        // candidates appended this iteration (t >= 2)
+    int ncand;        // candidates this iteration (t >= 2)
     int nbnd;         // boundary candidates (selection records)
     int nwin[2];      // window (selected set) sizes, double-buffered by iteration parity
     int nactive[2];   // radix-select active lists
-    int nchanged;     // selected vertices whose label changed
+    int nchanged;     // selected vertices whose label changed (movers)
+    int ndec[3];      // selected vertices per decision class
+    int nchunk;       // queued row chunks of the marking kernel
     int pad;
-    unsigned long long cut_arcs;  // full stats pass: arcs whose endpoint labels differ
+    unsigned long long cut_arcs;   // arcs whose endpoint labels differ (kept current incrementally)
 };
 
 // Loop control shared by the iteration kernels.
@@ -42,23 +51,30 @@ struct LpRecordDev {
     int boundary, pad;
     long long edge_cut;
     unsigned long long te_prev, te_cand, te_sel, te_stats;
+    // arcs the kernels actually read: boundary test (early exit), decisions, incremental update
+    unsigned long long arcs_bnd, arcs_dec, arcs_upd;
 };
 
 struct Buffers {
     // graph
-    int64_t *off = nullptr;   // [nv+1]
-    int32_t *col = nullptr;   // [narcs]
-    int32_t *rawdeg = nullptr;// [nv]
-    int32_t *label = nullptr; // [nv]
+    int64_t *off = nullptr;    // [nv+1]
+    int32_t *col = nullptr;    // [narcs]
+    int32_t *rawdeg = nullptr; // [nv]
+    int32_t *label = nullptr;  // [nv]
+    int32_t *bucket[3] = {nullptr, nullptr, nullptr};  // vertex ids of each degree class (deg >= 1), ascending
     // LP scratch
-    int32_t *stamp = nullptr; // [nv] iteration stamp of candidate marking
-    int32_t *cand = nullptr;  // [nv]
-    int32_t *win[2] = {nullptr, nullptr};  // [nv] each
+    int32_t *stamp = nullptr;  // [nv] iteration stamp of candidate marking
+    int32_t *cand = nullptr;   // [nv] phase-1 claimed list / stand-alone window list
+    int32_t *win[2] = {nullptr, nullptr};  // [nv] each: selected window of the iteration (by parity)
     int32_t *bv = nullptr, *bown = nullptr, *bnew = nullptr;  // [nv] boundary records
     uint64_t *bkey = nullptr;  // [nv]
     uint8_t *bsel = nullptr;   // [nv]
+    int32_t *dec[3] = {nullptr, nullptr, nullptr};  // [nv] each: selected vertices per decision class
+    int32_t *newlab = nullptr; // [nv] new label of a mover in the current iteration, else -1
+    int32_t *mov = nullptr;    // [nv] movers of the current iteration
+    int2 *chunkq = nullptr;    // [chunk_cap] (vertex, first arc) of queued row chunks
     int32_t *active[2] = {nullptr, nullptr};  // [nv] radix-select active lists
-    // per-part arrays (DMOLP_MAX_K)
+    // per-part arrays (DMOLP_MAX_K); vc / intra hold signed values in two's complement
     unsigned int *hist = nullptr;        // [MAX_K * 256]
     int32_t *need = nullptr;             // [MAX_K]
     int32_t *sel_below = nullptr;        // [MAX_K]
@@ -76,14 +92,15 @@ struct Buffers {
     LpCounters *cnt = nullptr;
     LpControl *ctrl = nullptr;
     LpRecordDev *rec = nullptr;          // [kMaxIter]
-    // phase 1 scratch (aliases LP scratch where lifetimes do not overlap)
+    // phase 1 scratch
     uint8_t *covered = nullptr;          // [nv]
     int32_t *hubs = nullptr;             // [nv]
     uint8_t *hub_used = nullptr;         // [nv]
-    int32_t *claim = nullptr;            // [nv]
+    int32_t *claim = nullptr;            // [nv] (aliases stamp)
     unsigned long long *best = nullptr;  // [1] packed hub argmax
     int *p1cnt = nullptr;                // [8] phase-1 counters
     unsigned long long *p1te = nullptr;  // [1]
+    int *flag = nullptr;                 // [1] scratch flag (symmetry check)
 };
 
 }  // namespace dmolp
@@ -95,6 +112,9 @@ struct dmolp_ctx {
     int64_t nv = 0, narcs = 0;
     int64_t maxdeg = 0, maxraw = 0;
     int ibits = 1, dbits = 1, rbits = 1;  // bits for ids, CSR degree, raw degree
+    int nb[3] = {0, 0, 0};                // vertices per degree class
+    int64_t chunk_cap = 0;
+    bool symmetric = false;               // every arc (u,v) has its reverse: incremental statistics apply
     bool has_graph = false;
     std::vector<int32_t> h_rawdeg;        // host copy for the hub sort
     dmolp::Buffers b;
@@ -102,12 +122,26 @@ struct dmolp_ctx {
     long long launches = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int32_t *saved_labels = nullptr;  // dmolp_labels_save
-    // optional kernel timing (dmolp_set_profiling)
+    // optional kernel timing (dmolp_set_profiling): event pairs around timed kernels
+    struct ProfEvents {
+        std::vector<cudaEvent_t> ev;  // pairs, in launch order
+        std::vector<int> kind, iter;  // kernel id and LP iteration per pair
+    };
+    // captured LP iteration graphs, keyed by (k, eff, mode, first iteration, iteration count, profiling);
+    // a profiling graph owns the events recorded by its event-record nodes
+    struct GraphEntry {
+        cudaGraphExec_t exec = nullptr;
+        long long kernels = 0;
+        ProfEvents prof;
+    };
+    std::map<std::tuple<int, int, int, int, int, int>, GraphEntry> graphs;
+    bool use_graphs = true;
+    bool capturing = false;
+    ProfEvents capture_prof;               // events created while capturing a profiling graph
     bool profiling = false;
-    std::vector<cudaEvent_t> prof_events;  // pairs, in launch order
-    std::vector<int> prof_kind;            // kernel id per pair
-    std::vector<int> prof_iter;            // LP iteration per pair
-    double prof_ms[2] = {0, 0};
-    long long prof_launches[2] = {0, 0};
-    double prof_bytes[2] = {0, 0};
+    ProfEvents prof_pending;               // pairs to read after the run
+    std::vector<char> prof_owned;          // per pending pair: destroy after reading (direct launches)
+    double prof_ms[4] = {0, 0, 0, 0};
+    long long prof_launches[4] = {0, 0, 0, 0};
+    double prof_bytes[4] = {0, 0, 0, 0};
 };

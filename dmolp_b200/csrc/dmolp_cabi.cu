@@ -53,7 +53,16 @@ int dalloc(dmolp_ctx *c, T **p, size_t n) {
     return DMOLP_OK;
 }
 
+void drop_graphs(dmolp_ctx *c) {
+    for (auto &kv : c->graphs) {
+        cudaGraphExecDestroy(kv.second.exec);
+        for (cudaEvent_t e : kv.second.prof.ev) cudaEventDestroy(e);
+    }
+    c->graphs.clear();
+}
+
 void free_all(dmolp_ctx *c) {
+    drop_graphs(c);
     for (void *p : c->allocations) cudaFree(p);
     c->allocations.clear();
     c->saved_labels = nullptr;
@@ -154,11 +163,56 @@ std::vector<int> find_hubs(const std::vector<int32_t> &raw) {
     return hubs;
 }
 
+// Capture (once) and launch the iterations [t0, t0+cnt) of an LP run as one CUDA graph.
+int run_block_graph(dmolp_ctx *c, const LpLaunch &L, int t0, int cnt) {
+    const auto key = std::make_tuple(L.k, L.eff, L.mode, t0, cnt, c->profiling ? 1 : 0);
+    auto it = c->graphs.find(key);
+    if (it == c->graphs.end()) {
+        cudaGraph_t g = nullptr;
+        dmolp_ctx::GraphEntry ge;
+        const long long before = c->launches;
+        DMOLP_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->capturing = true;
+        c->capture_prof = dmolp_ctx::ProfEvents();
+        for (int t = t0; t < t0 + cnt; ++t) lp_iteration(c, L, t);
+        c->capturing = false;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        ge.kernels = c->launches - before;
+        ge.prof = c->capture_prof;
+        c->launches = before;
+        if (e != cudaSuccess) return fail(DMOLP_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&ge.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(DMOLP_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        it = c->graphs.emplace(key, ge).first;
+    }
+    DMOLP_CUDA(cudaGraphLaunch(it->second.exec, c->stream));
+    c->launches += it->second.kernels;
+    const dmolp_ctx::ProfEvents &pe = it->second.prof;
+    for (size_t i = 0; i < pe.kind.size(); ++i) {
+        c->prof_pending.ev.push_back(pe.ev[2 * i]);
+        c->prof_pending.ev.push_back(pe.ev[2 * i + 1]);
+        c->prof_pending.kind.push_back(pe.kind[i]);
+        c->prof_pending.iter.push_back(pe.iter[i]);
+        c->prof_owned.push_back(0);
+    }
+    return DMOLP_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
 const char *dmolp_last_error(void) { return g_err.c_str(); }
+
+int dmolp_current_device(void) {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return d;
+}
 
 int dmolp_create(int device, dmolp_ctx **out) {
     if (!out) return fail(DMOLP_ERR_ARG, "out is null");
@@ -202,9 +256,9 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
         return fail(DMOLP_ERR_ARG, "bad graph sizes or null arrays");
     if (off[0] != 0 || off[nv] != narcs) return fail(DMOLP_ERR_ARG, "offsets must start at 0 and end at narcs");
     // Validate on the host: every device access below is then in bounds.
-    int bad = 0;
+    int bad = 0, unsorted = 0;
     int64_t maxdeg = 0, maxraw = 0;
-#pragma omp parallel for reduction(| : bad) reduction(max : maxdeg, maxraw) schedule(static)
+#pragma omp parallel for reduction(| : bad, unsorted) reduction(max : maxdeg, maxraw) schedule(static)
     for (int64_t v = 0; v < nv; ++v) {
         const int64_t d = off[v + 1] - off[v];
         if (d < 0 || d > 0x7fffffff) bad |= 1;
@@ -219,6 +273,15 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
 #pragma omp parallel for reduction(| : bad) schedule(static)
         for (int64_t j = 0; j < narcs; ++j)
             if ((uint32_t)col[j] >= (uint64_t)nv) bad |= 2;
+    }
+    if (!bad) {  // rows strictly increasing: a precondition of the symmetry test
+#pragma omp parallel for reduction(| : unsorted) schedule(dynamic, 4096)
+        for (int64_t v = 0; v < nv; ++v)
+            for (int64_t j = off[v] + 1; j < off[v + 1]; ++j)
+                if (col[j] <= col[j - 1]) {
+                    unsorted = 1;
+                    break;
+                }
     }
     if (bad & 1) return fail(DMOLP_ERR_ARG, "offsets are not non-decreasing");
     if (bad & 2) return fail(DMOLP_ERR_ARG, "a neighbour id is outside [0, nv)");
@@ -236,6 +299,15 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     c->rbits = bits_for(maxraw);
     c->h_rawdeg.resize(nv);
     for (int64_t v = 0; v < nv; ++v) c->h_rawdeg[v] = raw ? raw[v] : (int32_t)(off[v + 1] - off[v]);
+    // degree classes (isolated vertices belong to none: they are never on a boundary)
+    std::vector<int32_t> bl[3];
+    for (int64_t v = 0; v < nv; ++v) {
+        const int64_t d = off[v + 1] - off[v];
+        if (d == 0) continue;
+        bl[d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2)].push_back((int32_t)v);
+    }
+    for (int i = 0; i < 3; ++i) c->nb[i] = (int)bl[i].size();
+    c->chunk_cap = narcs / kChunk + 2;
 
     Buffers &b = c->b;
     const size_t n = (size_t)nv + 1;
@@ -280,6 +352,14 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     ALLOC(b.best, 1);
     ALLOC(b.p1cnt, 8);
     ALLOC(b.p1te, 1);
+    ALLOC(b.flag, 1);
+    for (int i = 0; i < 3; ++i) {
+        ALLOC(b.bucket[i], bl[i].size());
+        ALLOC(b.dec[i], n);
+    }
+    ALLOC(b.newlab, n);
+    ALLOC(b.mov, n);
+    ALLOC(b.chunkq, (size_t)c->chunk_cap);
 #undef ALLOC
     b.claim = b.stamp;  // phase 1 and the LP loop never run at the same time
     DMOLP_CUDA(cudaMemcpyAsync(b.off, off, n * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
@@ -291,6 +371,24 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     DMOLP_CUDA(cudaMemsetAsync(b.hist, 0, (size_t)DMOLP_MAX_K * kRadix * sizeof(unsigned int), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.ctrl, 0, sizeof(LpControl), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.cnt, 0, sizeof(LpCounters), c->stream));
+    for (int i = 0; i < 3; ++i)
+        if (!bl[i].empty())
+            DMOLP_CUDA(cudaMemcpyAsync(b.bucket[i], bl[i].data(), bl[i].size() * sizeof(int32_t),
+                                       cudaMemcpyHostToDevice, c->stream));
+    lp_fill(c, b.newlab, (int64_t)n, -1);
+    select_prepare();
+    // every arc has its reverse (checked on the device): the LP loop may update its statistics from the
+    // movers alone
+    c->symmetric = false;
+    if (!unsorted && nv > 0) {
+        DMOLP_CUDA(cudaMemsetAsync(b.flag, 0, sizeof(int), c->stream));
+        lp_check_symmetric(c);
+        int missing = 1;
+        DMOLP_CUDA(cudaMemcpyAsync(&missing, b.flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        int s1 = sync(c);
+        if (s1) return s1;
+        c->symmetric = missing == 0;
+    }
     // log(t) and e^(-t/5) with the host's libm, as the reference computes them (phase2.cpp:199,
     // gpu_lp_boundary.cu:244)
     std::vector<double> lt(kMaxIter + 1, 0.0), rt(kMaxIter + 1, 1.0);
@@ -355,7 +453,7 @@ int dmolp_labels_restore(dmolp_ctx *c) {
 int dmolp_set_profiling(dmolp_ctx *c, int enable) {
     if (!c) return fail(DMOLP_ERR_ARG, "null context");
     c->profiling = enable != 0;
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < 4; ++i) {
         c->prof_ms[i] = 0;
         c->prof_launches[i] = 0;
         c->prof_bytes[i] = 0;
@@ -364,7 +462,7 @@ int dmolp_set_profiling(dmolp_ctx *c, int enable) {
 }
 
 int dmolp_kernel_profile(dmolp_ctx *c, int kernel, double *total_ms, int64_t *launches, double *bytes) {
-    if (!c || kernel < 0 || kernel > 1) return fail(DMOLP_ERR_ARG, "bad context or kernel id");
+    if (!c || kernel < 0 || kernel > 3) return fail(DMOLP_ERR_ARG, "bad context or kernel id");
     if (total_ms) *total_ms = c->prof_ms[kernel];
     if (launches) *launches = c->prof_launches[kernel];
     if (bytes) *bytes = c->prof_bytes[kernel];
@@ -389,96 +487,82 @@ int dmolp_metrics(dmolp_ctx *c, int k, int64_t *edge_cut, int64_t *vertex_counts
     return DMOLP_OK;
 }
 
-int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *vertex_counts, int64_t *edge_counts,
-                 dmolp_phase1_info *info) {
-    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
-    if (k < 1 || k > DMOLP_MAX_K) return fail(DMOLP_ERR_ARG, "k out of range [1, 1024]");
-    if (theta < 1)
-        return fail(DMOLP_ERR_ARG, "theta must be >= 1 (with theta = 0 the reference expands nothing and never ends)");
-    DMOLP_CUDA(cudaSetDevice(c->device));
+// Seeds by the reference rule (seed.cpp:138-242) from a given hub list and first seed; no completion.
+static int find_seeds_impl(dmolp_ctx *c, int k, int first, const std::vector<int> &hubs, std::vector<int> &seeds) {
     Buffers &b = c->b;
     const int64_t nv = c->nv;
-    dmolp_phase1_info inf;
-    std::memset(&inf, 0, sizeof(inf));
-    DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
-
-    // ---- hubs and first seed on the host (order-dependent; see the top of this file) ----
-    std::vector<int> hubs = find_hubs(c->h_rawdeg);
-    std::pair<int, int> first(-1, -1);
-    for (int64_t v = nv - 1; v >= 0; --v) {  // init.cpp:179-187, including its id-vs-degree tie test
-        const int d = c->h_rawdeg[v];
-        if (d > first.second || (d == first.second && (int)v < first.second)) first = std::make_pair((int)v, d);
+    seeds.clear();
+    if (nv <= 0) return DMOLP_OK;
+    seeds.push_back(first);
+    if (hubs.empty() || k <= 1) return DMOLP_OK;
+    DMOLP_CUDA(cudaMemcpyAsync(b.hubs, hubs.data(), hubs.size() * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.hub_used, 0, hubs.size(), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.covered, 0, (size_t)nv, c->stream));
+    auto fi = std::find(hubs.begin(), hubs.end(), first);
+    if (fi != hubs.end()) DMOLP_CUDA(cudaMemsetAsync(b.hub_used + (fi - hubs.begin()), 1, 1, c->stream));
+    size_t balls = 0;
+    for (int p = 1; p < k; ++p) {  // seed.cpp:206-226
+        for (; balls < seeds.size(); ++balls) p1_mark_ball(c, seeds[balls]);
+        p1_hub_argmax(c, (int64_t)hubs.size());
+        unsigned long long best = 0;
+        DMOLP_CUDA(cudaMemcpyAsync(&best, b.best, sizeof(best), cudaMemcpyDeviceToHost, c->stream));
+        int st = sync(c);
+        if (st) return st;
+        if (best == 0) break;
+        const int64_t idx = (int64_t)(0xffffffffu - (unsigned)(best & 0xffffffffull));
+        seeds.push_back(hubs[idx]);
+        DMOLP_CUDA(cudaMemsetAsync(b.hub_used + idx, 1, 1, c->stream));
     }
-    inf.num_hubs = (int64_t)hubs.size();
-    std::vector<int> seeds;
-    std::vector<char> used(hubs.size(), 0);
-    if (nv > 0) seeds.push_back(first.first);
-    auto hub_index = [&](int s) -> int64_t {
+    return DMOLP_OK;
+}
+
+// Seed completion: where the reference rule found fewer than k seeds the reference reads past its seed
+// vector (partition.cpp:347).  Remaining seeds: unused hubs by raw degree (first in hub order on ties),
+// then other vertices by raw degree (lowest id on ties).
+static void complete_seeds(dmolp_ctx *c, int k, const std::vector<int> &hubs, std::vector<int> &seeds) {
+    const int64_t nv = c->nv;
+    if ((int64_t)seeds.size() >= k || nv <= 0) return;
+    std::vector<char> used(hubs.size(), 0), is_seed(nv, 0);
+    for (int s : seeds) {
+        is_seed[s] = 1;
         auto it = std::find(hubs.begin(), hubs.end(), s);
-        return it == hubs.end() ? -1 : (int64_t)(it - hubs.begin());
-    };
-    DMOLP_CUDA(cudaMemsetAsync(b.p1te, 0, sizeof(unsigned long long), c->stream));
-    if (nv > 0 && !hubs.empty() && k > 1) {
-        DMOLP_CUDA(cudaMemcpyAsync(b.hubs, hubs.data(), hubs.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
-                                   c->stream));
-        DMOLP_CUDA(cudaMemsetAsync(b.hub_used, 0, hubs.size(), c->stream));
-        DMOLP_CUDA(cudaMemsetAsync(b.covered, 0, (size_t)nv, c->stream));
-        int64_t fi = hub_index(first.first);
-        if (fi >= 0) {
-            used[fi] = 1;
-            DMOLP_CUDA(cudaMemsetAsync(b.hub_used + fi, 1, 1, c->stream));
-        }
-        size_t balls = 0;
-        for (int p = 1; p < k; ++p) {  // seed.cpp:206-226
-            for (; balls < seeds.size(); ++balls) p1_mark_ball(c, seeds[balls]);
-            p1_hub_argmax(c, (int64_t)hubs.size());
-            unsigned long long best = 0;
-            DMOLP_CUDA(cudaMemcpyAsync(&best, b.best, sizeof(best), cudaMemcpyDeviceToHost, c->stream));
-            int st = sync(c);
-            if (st) return st;
-            if (best == 0) break;
-            const int64_t idx = (int64_t)(0xffffffffu - (unsigned)(best & 0xffffffffull));
-            seeds.push_back(hubs[idx]);
-            used[idx] = 1;
-            DMOLP_CUDA(cudaMemsetAsync(b.hub_used + idx, 1, 1, c->stream));
-        }
+        if (it != hubs.end()) used[it - hubs.begin()] = 1;
     }
-    inf.num_seeds_found = (int32_t)seeds.size();
-    // Seed completion (the reference reads past its seed vector here, partition.cpp:347): unused hubs by
-    // raw degree (first in hub order on ties), then other vertices by raw degree (lowest id on ties).
-    if ((int64_t)seeds.size() < k && nv > 0) {
-        std::vector<char> is_seed(nv, 0);
-        for (int s : seeds) is_seed[s] = 1;
-        while ((int)seeds.size() < k) {
-            int bestv = -1, bd = -1;
-            for (size_t i = 0; i < hubs.size(); ++i)
-                if (!used[i] && c->h_rawdeg[hubs[i]] > bd) {
-                    bd = c->h_rawdeg[hubs[i]];
-                    bestv = hubs[i];
+    while ((int)seeds.size() < k) {
+        int bestv = -1, bd = -1;
+        int64_t bi = -1;
+        for (size_t i = 0; i < hubs.size(); ++i)
+            if (!used[i] && c->h_rawdeg[hubs[i]] > bd) {
+                bd = c->h_rawdeg[hubs[i]];
+                bestv = hubs[i];
+                bi = (int64_t)i;
+            }
+        if (bestv == -1)
+            for (int64_t v = 0; v < nv; ++v)
+                if (!is_seed[v] && c->h_rawdeg[v] > bd) {
+                    bd = c->h_rawdeg[v];
+                    bestv = (int)v;
                 }
-            if (bestv == -1)
-                for (int64_t v = 0; v < nv; ++v)
-                    if (!is_seed[v] && c->h_rawdeg[v] > bd) {
-                        bd = c->h_rawdeg[v];
-                        bestv = (int)v;
-                    }
-            if (bestv == -1) break;
-            seeds.push_back(bestv);
-            is_seed[bestv] = 1;
-            int64_t hi = hub_index(bestv);
-            if (hi >= 0) used[hi] = 1;
+        if (bestv == -1) break;
+        seeds.push_back(bestv);
+        is_seed[bestv] = 1;
+        if (bi >= 0) used[bi] = 1;
+        else {
+            auto it = std::find(hubs.begin(), hubs.end(), bestv);
+            if (it != hubs.end()) used[it - hubs.begin()] = 1;
         }
     }
-    std::vector<int32_t> seedk(k, -1);
-    for (int p = 0; p < k && p < (int)seeds.size(); ++p) seedk[p] = seeds[p];
-    if (seeds_out) std::copy(seedk.begin(), seedk.end(), seeds_out);
+}
 
-    // ---- growth rounds (partition.cpp:335-604) ----
+// Growth rounds (partition.cpp:335-604); seedk[p] = -1 for a part without a seed.
+static int expand_impl(dmolp_ctx *c, int k, int theta, const std::vector<int32_t> &seedk, int *rounds_out) {
+    Buffers &b = c->b;
+    const int64_t nv = c->nv;
     p1_init_labels(c);
     DMOLP_CUDA(cudaMemsetAsync(b.psize, 0, DMOLP_MAX_K * sizeof(long long), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.npart, 0, DMOLP_MAX_K * sizeof(int32_t), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.p1cnt, 0, 8 * sizeof(int), c->stream));
-    // seeds go through the need[] buffer as staging (k ints)
+    // the seeds go through the need[] buffer as staging (k ints)
     DMOLP_CUDA(cudaMemcpyAsync(b.need, seedk.data(), k * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
     p1_set_seeds(c, b.need, k);
     int cur = 0, rounds = 0;
@@ -500,13 +584,94 @@ int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *ve
         cur ^= 1;
         ++rounds;
     }
+    *rounds_out = rounds;
+    return DMOLP_OK;
+}
+
+static int check_seed_args(dmolp_ctx *c, int k) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (k < 1 || k > DMOLP_MAX_K) return fail(DMOLP_ERR_ARG, "k out of range [1, 1024]");
+    return DMOLP_OK;
+}
+
+int dmolp_find_seeds(dmolp_ctx *c, int k, int32_t first_seed, const int32_t *hubs, int64_t nhubs, int32_t *seeds_out,
+                     int32_t *nseeds) {
+    int st = check_seed_args(c, k);
+    if (st) return st;
+    if (nhubs < 0 || (nhubs && !hubs) || !seeds_out || !nseeds) return fail(DMOLP_ERR_ARG, "bad arguments");
+    if (c->nv > 0 && (first_seed < 0 || first_seed >= c->nv)) return fail(DMOLP_ERR_ARG, "first seed out of range");
+    for (int64_t i = 0; i < nhubs; ++i)
+        if (hubs[i] < 0 || hubs[i] >= c->nv) return fail(DMOLP_ERR_ARG, "hub id out of range");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    DMOLP_CUDA(cudaMemsetAsync(c->b.p1te, 0, sizeof(unsigned long long), c->stream));
+    std::vector<int> hv(hubs, hubs + nhubs), seeds;
+    st = find_seeds_impl(c, k, first_seed, hv, seeds);
+    if (st) return st;
+    for (size_t i = 0; i < seeds.size(); ++i) seeds_out[i] = seeds[i];
+    *nseeds = (int32_t)seeds.size();
+    return DMOLP_OK;
+}
+
+int dmolp_expand_partitions(dmolp_ctx *c, int k, int theta, const int32_t *seeds, int32_t nseeds, int32_t *rounds) {
+    int st = check_seed_args(c, k);
+    if (st) return st;
+    if (theta < 1) return fail(DMOLP_ERR_ARG, "theta must be >= 1 (with theta = 0 the reference never ends)");
+    if (nseeds < 0 || (nseeds && !seeds)) return fail(DMOLP_ERR_ARG, "bad seeds");
+    std::vector<int32_t> seedk(k, -1);
+    std::vector<char> seen(c->nv, 0);
+    for (int p = 0; p < k && p < nseeds; ++p) {
+        if (seeds[p] < 0 || seeds[p] >= c->nv) return fail(DMOLP_ERR_ARG, "seed out of range");
+        if (seen[seeds[p]]) return fail(DMOLP_ERR_ARG, "a vertex is the seed of two parts");
+        seen[seeds[p]] = 1;
+        seedk[p] = seeds[p];
+    }
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    int r = 0;
+    st = expand_impl(c, k, theta, seedk, &r);
+    if (rounds) *rounds = r;
+    return st;
+}
+
+int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *vertex_counts, int64_t *edge_counts,
+                 dmolp_phase1_info *info) {
+    int st = check_seed_args(c, k);
+    if (st) return st;
+    if (theta < 1)
+        return fail(DMOLP_ERR_ARG, "theta must be >= 1 (with theta = 0 the reference expands nothing and never ends)");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    Buffers &b = c->b;
+    const int64_t nv = c->nv;
+    dmolp_phase1_info inf;
+    std::memset(&inf, 0, sizeof(inf));
+    DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
+
+    // ---- hubs and first seed on the host (order-dependent; see the top of this file) ----
+    std::vector<int> hubs = find_hubs(c->h_rawdeg);
+    std::pair<int, int> first(-1, -1);
+    for (int64_t v = nv - 1; v >= 0; --v) {  // init.cpp:179-187, including its id-vs-degree tie test
+        const int d = c->h_rawdeg[v];
+        if (d > first.second || (d == first.second && (int)v < first.second)) first = std::make_pair((int)v, d);
+    }
+    inf.num_hubs = (int64_t)hubs.size();
+    DMOLP_CUDA(cudaMemsetAsync(b.p1te, 0, sizeof(unsigned long long), c->stream));
+    std::vector<int> seeds;
+    st = find_seeds_impl(c, k, first.first, hubs, seeds);
+    if (st) return st;
+    inf.num_seeds_found = (int32_t)seeds.size();
+    complete_seeds(c, k, hubs, seeds);
+    std::vector<int32_t> seedk(k, -1);
+    for (int p = 0; p < k && p < (int)seeds.size(); ++p) seedk[p] = seeds[p];
+    if (seeds_out) std::copy(seedk.begin(), seedk.end(), seeds_out);
+    int rounds = 0;
+    st = expand_impl(c, k, theta, seedk, &rounds);
+    if (st) return st;
     inf.rounds = rounds;
 
     // ---- initial metrics (phase1.cpp:83-153) ----
     unsigned long long arcs = 0;
     std::vector<long long> vc, intra;
     int bad = 0;
-    int st = run_stats(c, k, &arcs, vc, intra, &bad);
+    st = run_stats(c, k, &arcs, vc, intra, &bad);
     if (st) return st;
     DMOLP_CUDA(cudaEventRecord(c->ev1, c->stream));
     unsigned long long te = 0;
@@ -566,9 +731,18 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     int st = check_launch(c);
     if (st) return st;
     int stopped = 0;
-    for (int t = 1; t <= max_iter; ++t) {
-        lp_iteration(c, L, t);
-        if (cfg->mode == DMOLP_LP_MODE_REF && (t % 8) == 0) {
+    // Iterations in blocks: FIXED mode one block of all iterations, REF mode blocks of 8 with a check of
+    // the stop flag in between.  Each block is captured into a CUDA graph once and replayed afterwards.
+    const int block = cfg->mode == DMOLP_LP_MODE_REF ? 8 : std::max(1, max_iter);
+    for (int t0 = 1; t0 <= max_iter; t0 += block) {
+        const int cnt = std::min(block, max_iter - t0 + 1);
+        if (c->use_graphs) {
+            st = run_block_graph(c, L, t0, cnt);
+            if (st) return st;
+        } else {
+            for (int t = t0; t < t0 + cnt; ++t) lp_iteration(c, L, t);
+        }
+        if (cfg->mode == DMOLP_LP_MODE_REF && t0 + cnt <= max_iter) {
             DMOLP_CUDA(cudaMemcpyAsync(&stopped, &b.ctrl->stopped, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             st = sync(c);
             if (st) return st;
@@ -594,31 +768,37 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
         ec[p] = (long long)(hi[p] / 2);
     }
     if (c->profiling) {
-        // algorithmic bytes per launch: scan = 8 B per neighbour arc (id + label) + 20 B per candidate (two
-        // offsets, own label) + 4 B per listed candidate + 21 B per boundary record; stats = 8 B per arc +
-        // 20 B per vertex
-        for (size_t i = 0; i < c->prof_kind.size(); ++i) {
-            const int t = c->prof_iter[i], kind = c->prof_kind[i];
-            if (t > ctl.iters_run) continue;
-            const LpRecordDev &d = recs[t - 1];
-            double bytes = 0;
-            if (kind == 0) {
-                const double ncand = t == 1 ? (double)c->nv : (double)d.candidates;
-                bytes = 8.0 * (double)d.te_cand + 20.0 * ncand + (t > 1 ? 4.0 * ncand : 0.0) + 21.0 * d.boundary;
-            } else {
-                if (d.te_stats == 0) continue;  // statistics skipped this iteration
-                bytes = 8.0 * (double)c->narcs + 20.0 * (double)c->nv;
-            }
+        // Algorithmic bytes per launch of the design (ids and labels are 4 B, offsets 8 B):
+        //  bnd    : bucket ids (+ stamps after t = 1) of every vertex with arcs, offsets + own label of each
+        //           candidate, id + label of each arc read before the first differing one, 21 B per record
+        //  decide : list id + offsets + own label per selected vertex, id + label per arc, 8 B per mover
+        //  mark   : list id + offsets per window vertex, id read + stamp write per arc
+        //  update : offsets + labels per mover, id + label + pending label per arc
+        const double nbk = (double)c->nb[0] + c->nb[1] + c->nb[2];
+        dmolp_ctx::ProfEvents &pe = c->prof_pending;
+        for (size_t i = 0; i < pe.kind.size(); ++i) {
+            const int t = pe.iter[i], kind = pe.kind[i];
             float ems = 0;
-            cudaEventElapsedTime(&ems, c->prof_events[2 * i], c->prof_events[2 * i + 1]);
-            c->prof_ms[kind] += ems;
-            c->prof_launches[kind] += 1;
-            c->prof_bytes[kind] += bytes;
+            if (t <= ctl.iters_run && cudaEventElapsedTime(&ems, pe.ev[2 * i], pe.ev[2 * i + 1]) == cudaSuccess) {
+                const LpRecordDev &d = recs[t - 1];
+                const double ncand = t == 1 ? nbk : (double)d.candidates;
+                double bytes = 0;
+                if (kind == 0) bytes = 4.0 * nbk * (t > 1 ? 2 : 1) + 20.0 * ncand + 8.0 * (double)d.arcs_bnd + 21.0 * d.boundary;
+                else if (kind == 1) bytes = 24.0 * d.window + 8.0 * (double)d.arcs_dec + 8.0 * d.changes;
+                else if (kind == 2) bytes = (t > 1 ? 20.0 * recs[t - 2].window : 0.0) + 8.0 * (double)d.te_prev;
+                else bytes = 28.0 * d.changes + 12.0 * (double)d.arcs_upd;
+                c->prof_ms[kind] += ems;
+                c->prof_launches[kind] += 1;
+                c->prof_bytes[kind] += bytes;
+            }
+            cudaGetLastError();
+            if (c->prof_owned[i]) {
+                cudaEventDestroy(pe.ev[2 * i]);
+                cudaEventDestroy(pe.ev[2 * i + 1]);
+            }
         }
-        for (cudaEvent_t e : c->prof_events) cudaEventDestroy(e);
-        c->prof_events.clear();
-        c->prof_kind.clear();
-        c->prof_iter.clear();
+        c->prof_pending = dmolp_ctx::ProfEvents();
+        c->prof_owned.clear();
     }
     dmolp_lp_result r;
     std::memset(&r, 0, sizeof(r));
@@ -638,6 +818,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
             o.changes = d.changes;
             o.boundary = d.boundary;
             o.reserved = 0;
+            o.arcs_read = d.arcs_bnd + d.arcs_dec + d.arcs_upd + (i > 0 ? d.te_prev : 0);
             o.edge_cut = d.edge_cut;
             o.te_prev = d.te_prev;
             o.te_cand = d.te_cand;
@@ -741,21 +922,22 @@ int dmolp_lp_apply(dmolp_ctx *c, int k, int cap, const double *penalty, const in
     DMOLP_CUDA(cudaMemcpyAsync(b.tpen, tp.data(), k * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     const int eff = cap == DMOLP_LP_CAP_FULL ? k : std::min(k, 32);
     lp_apply_list(c, k, eff, n);
-    std::vector<int32_t> bv(n), bo(n), bn(n);
-    if (n) {
-        DMOLP_CUDA(cudaMemcpyAsync(bv.data(), b.bv, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-        DMOLP_CUDA(cudaMemcpyAsync(bo.data(), b.bown, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-        DMOLP_CUDA(cudaMemcpyAsync(bn.data(), b.bnew, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-    }
+    LpCounters cn;
+    DMOLP_CUDA(cudaMemcpyAsync(&cn, b.cnt, sizeof(cn), cudaMemcpyDeviceToHost, c->stream));
     int st = sync(c);
     if (st) return st;
-    int64_t m = 0;
-    for (int i = 0; i < n; ++i)
-        if (bn[i] != bo[i]) {
-            if (changed_nodes) changed_nodes[m] = bv[i];
-            if (changed_labels) changed_labels[m] = bn[i];
-            ++m;
-        }
+    const int m = cn.nchanged;
+    std::vector<int32_t> mv(m), ml(m);
+    if (m) {
+        DMOLP_CUDA(cudaMemcpyAsync(mv.data(), b.bv, m * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        DMOLP_CUDA(cudaMemcpyAsync(ml.data(), b.bnew, m * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    }
+    st = sync(c);
+    if (st) return st;
+    for (int i = 0; i < m; ++i) {
+        if (changed_nodes) changed_nodes[i] = mv[i];
+        if (changed_labels) changed_labels[i] = ml[i];
+    }
     *nchanged = m;
     return DMOLP_OK;
 }

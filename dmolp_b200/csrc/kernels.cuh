@@ -12,6 +12,7 @@ namespace dmolp {
 // launches into no-ops once it is non-zero.
 void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, const int *n_dev, int nseg, int keybits,
                      uint8_t *sel, const int *stopped);
+void select_prepare();  // kernel attributes; call once before any capture
 
 // ---- LP loop (lp_kernels.cu) ----
 struct LpLaunch {
@@ -19,6 +20,8 @@ struct LpLaunch {
     int eff;       // labels scored: min(k,32) or k
     int mode;      // DMOLP_LP_MODE_*
 };
+void lp_check_symmetric(dmolp_ctx *c);  // sets *b.flag when an arc has no reverse
+void lp_fill(dmolp_ctx *c, int32_t *p, int64_t n, int32_t v);
 void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped);
 void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip);
 void lp_init_end(dmolp_ctx *c, int mode);

@@ -1,19 +1,25 @@
 // Phase-2 label propagation on the resident CSR.  One iteration t (1-based) is a fixed sequence of
-// launches with device-side counts, so it needs no host round trip and can be enqueued ahead or captured:
+// launches with device-side counts, so a whole run is captured once into a CUDA graph and replayed:
 //
-//   begin      penalties from the last statistics (calculatePenalties, src/phase2/phase2.cpp:158-209),
-//              counter reset
-//   cand       candidates = previous window plus its neighbours, deduplicated by an iteration stamp
-//              (expandBoundaryNodes, src/phase2/gpu_lp_boundary.cu:195-240); at t = 1 every vertex
-//   scan       one pass over each candidate's neighbours computing BOTH the boundary test
-//              (gpu_lp_boundary.cu:251-270) and the penalised-argmax decision of boundaryLPKernel_unified
-//              (gpu_lp_boundary.cu:354-426); boundary candidates become selection records
-//   need/select  per label, the ceil(e^(-t/5) n) records with the smallest (degree asc|desc, id) key
-//              (gpu_lp_boundary.cu:244, 277-301), by segmented radix select
-//   commit     selected records become the next window; moved vertices take their new label (Jacobi:
-//              every decision read the labels as they were at the start of the iteration)
-//   mid/stats/end  the fused edge-cut + balance pass (computePartitionStats / computeEdgeCut,
-//              phase2.cpp:55-117, 214-253) and the stopping rules of run_phase2 (phase2.cpp:309-415)
+//   begin    penalties from the current statistics (calculatePenalties, src/phase2/phase2.cpp:158-209);
+//            counter reset
+//   mark     stamp the previous window and its neighbours with t (expandBoundaryNodes' candidate set,
+//            src/phase2/gpu_lp_boundary.cu:195-240); rows longer than kChunk are split into queued chunks
+//   bnd      degree-bucketed boundary test of every stamped vertex (thread / warp / block per vertex),
+//            stopping at the first differently-labelled neighbour (gpu_lp_boundary.cu:251-270); a
+//            boundary vertex becomes a selection record keyed (degree asc|desc by RE[label], id)
+//   need/select  per label the ceil(e^(-t/5) n) smallest keys (gpu_lp_boundary.cu:244, 277-301)
+//   split    selected vertices form the next window and are routed to a decision class
+//   decide   boundaryLPKernel_unified's rule (gpu_lp_boundary.cu:354-426) for the selected vertices only:
+//            thread per vertex (deg <= 16, pairwise counts), warp per vertex (shared histogram), block per
+//            vertex (deg > 4096); a changed label is parked in newlab[] (Jacobi: nothing moves yet)
+//   update   (symmetric graphs) edge cut, per-part intra arcs and vertex counts change only through the
+//            movers' arcs: each arc is re-scored with both endpoints' old and new labels, weighted 2 when
+//            the neighbour stays (its reverse arc is not visited) and 1 when it moves too.  Asymmetric
+//            graphs run the full statistics pass instead (computePartitionStats / computeEdgeCut,
+//            phase2.cpp:55-117, 214-253).
+//   apply    movers take their new labels
+//   end      the stopping rules of run_phase2 (phase2.cpp:309-415) and the iteration record
 //
 // Floating point: penalties and scores use __d*_rn intrinsics, which the compiler never contracts into
 // FMAs, so every value is the IEEE double of the reference's expression in its evaluation order.
@@ -27,9 +33,45 @@ namespace {
 
 constexpr int kGridPerSm = 4;
 
+__device__ __forceinline__ int tiekey(int c) { return (c & ~31) | (int)brev5((unsigned)c & 31u); }
+
+__device__ __forceinline__ long long sll(unsigned long long x) { return (long long)x; }
+
+// Better (score desc, tie key asc).
+__device__ __forceinline__ bool better(double s, int key, double bs, int bkey) {
+    return s > bs || (s == bs && key < bkey);
+}
+
+// Visit neighbour ids col[s..e) with the lanes of a warp: scalar head up to a 16-byte boundary, 128-bit
+// loads for the body, scalar tail.  f(u) is called per neighbour; after each step `stop()` (evaluated
+// warp-uniformly) may end the walk early.  Returns the number of arcs the warp read.
+template <typename F, typename S>
+__device__ __forceinline__ int64_t warp_row(const int32_t *__restrict__ col, int64_t s, int64_t e, int lane, F f,
+                                            S stop) {
+    int64_t a = (s + 3) & ~int64_t(3);
+    if (a > e) a = e;
+    if (s + lane < a) f(__ldg(col + s + lane));
+    int64_t read = a - s;
+    if (stop()) return read;
+    const int64_t qe = e >> 2;  // body: int4 words [a/4, e/4)
+    const int4 *c4 = reinterpret_cast<const int4 *>(col);
+    for (int64_t q = (a >> 2) + lane, q0 = a >> 2; q0 < qe; q += 32, q0 += 32) {
+        if (q < qe) {
+            const int4 x = __ldcs(c4 + q);
+            f(x.x);
+            f(x.y);
+            f(x.z);
+            f(x.w);
+        }
+        read += 4 * (qe - q0 < 32 ? qe - q0 : (int64_t)32);
+        if (stop()) return read;
+    }
+    const int64_t t0 = a > (qe << 2) ? a : (qe << 2);
+    if (t0 + lane < e) f(__ldg(col + t0 + lane));
+    return read + (e - t0);
+}
+
 // ------------------------------------------------------------------------------------ begin
-// Single block.  Thread 0 computes the penalties sequentially (k <= 1024 values); the block resets the
-// per-iteration counters.
 __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
     LpControl *ctl = b.ctrl;
     if (ctl->stopped) return;
@@ -40,29 +82,31 @@ __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
         cn->nbnd = 0;
         cn->nwin[t & 1] = 0;
         cn->nchanged = 0;
+        cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
+        cn->nchunk = 0;
         ctl->stop_now = 0;
         ctl->skip_stats = 0;
         LpRecordDev &r = b.rec[t - 1];
         r.iteration = t;
-        r.window = r.candidates = r.changes = 0;
-        r.boundary = 0;
+        r.window = r.candidates = r.changes = r.boundary = 0;
         r.edge_cut = ctl->prev_cut;
         r.te_prev = t == 1 ? (unsigned long long)narcs : 0ull;
         r.te_cand = r.te_sel = r.te_stats = 0;
+        r.arcs_bnd = r.arcs_dec = r.arcs_upd = 0;
 
         // ---- statistics -> expected values (phase2.cpp:110-115) ----
         long long tv = 0, te = 0;
         for (int p = 0; p < k; ++p) {
-            tv += (long long)b.vc[p];
-            te += (long long)(b.intra[p] / 2);
+            tv += sll(b.vc[p]);
+            te += sll(b.intra[p]) / 2;
         }
         const double ev = __ddiv_rn((double)tv, (double)k);
         const double ee = te > 0 ? __ddiv_rn((double)te, (double)k) : 1.0;
         // ---- calculatePenalties (phase2.cpp:166-203) ----
         double rv_mean = 0.0, re_mean = 0.0;
         for (int p = 0; p < k; ++p) {
-            const double rv = ev > 0 ? __ddiv_rn((double)(long long)b.vc[p], ev) : 1.0;
-            const double re = ee > 0 ? __ddiv_rn((double)(long long)(b.intra[p] / 2), ee) : 1.0;
+            const double rv = ev > 0 ? __ddiv_rn((double)sll(b.vc[p]), ev) : 1.0;
+            const double re = ee > 0 ? __ddiv_rn((double)(sll(b.intra[p]) / 2), ee) : 1.0;
             b.RE[p] = re;
             b.tpen[p] = rv;  // RV kept here until the penalties overwrite it below
             rv_mean = __dadd_rn(rv_mean, rv);
@@ -93,10 +137,10 @@ __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
     }
 }
 
-// ------------------------------------------------------------------------------------ cand
-// Warp per vertex of the previous window: stamp the vertex and its neighbours with t; a vertex whose stamp
-// changes is appended once.
-__global__ void k_lp_cand(Buffers b, int t, int nv) {
+// ------------------------------------------------------------------------------------ mark
+// Warp per vertex of the previous window: stamp it and its first kChunk neighbours; the rest of a long row
+// is queued in kChunk pieces for k_mark_chunks.
+__global__ void k_mark(Buffers b, int t) {
     if (b.ctrl->stopped) return;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
@@ -106,99 +150,149 @@ __global__ void k_lp_cand(Buffers b, int t, int nv) {
     for (int i = gw; i < n; i += nw) {
         const int v = prev[i];
         const int64_t s = b.off[v], e = b.off[v + 1];
-        if (lane == 0) te += (unsigned long long)(e - s);
-        {
-            bool fresh = false;
-            if (lane == 0) fresh = atomicExch(&b.stamp[v], t) != t;
-            const int slot = warp_append(&b.cnt->ncand, fresh);
-            if (fresh) b.cand[slot] = v;
-        }
-        for (int64_t j0 = s; j0 < e; j0 += 32) {
-            const int64_t j = j0 + lane;
-            bool fresh = false;
-            int u = 0;
-            if (j < e) {
-                u = ld_stream(b.col + j);
-                fresh = atomicExch(&b.stamp[u], t) != t;
+        if (lane == 0) {
+            b.stamp[v] = t;
+            te += (unsigned long long)(e - s);
+            for (int64_t c = s + kChunk; c < e; c += kChunk) {
+                const int q = atomicAdd(&b.cnt->nchunk, 1);
+                b.chunkq[q] = make_int2(v, (int)(c - s));
             }
-            const int slot = warp_append(&b.cnt->ncand, fresh);
-            if (fresh) b.cand[slot] = u;
         }
+        const int64_t e1 = e - s > kChunk ? s + kChunk : e;
+        warp_row(b.col, s, e1, lane, [&](int u) { b.stamp[u] = t; }, [] { return false; });
     }
     te = warp_sum_u64(te);
     if (lane == 0 && te) atomicAdd(&b.rec[t - 1].te_prev, te);
 }
 
-// ------------------------------------------------------------------------------------ scan
-// Warp per candidate.  Each warp owns an `eff`-entry shared histogram of neighbour labels.  One read of the
-// neighbour labels gives the boundary flag (any neighbour labelled differently) and the decision:
-//   score[c] = count[c] > 0 ? count[c] * (1 + penalty[c]) : 0          for c < eff
-//   M = max score; among labels scoring M the reference's shuffle tree keeps the one whose 5-bit
-//   bit-reversed lane index is smallest (earlier 32-label chunk first when eff > 32);
-//   new label = M > (own < eff ? count[own] : -1e300) ? that label : own.
-__global__ void k_lp_scan(Buffers b, int t, int all, int nv, int eff, int ibits, int maxdeg) {
+__global__ void k_mark_chunks(Buffers b, int t) {
     if (b.ctrl->stopped) return;
-    extern __shared__ int shist[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    int *h = shist + wib * eff;
+    const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    const int n = all ? nv : b.cnt->ncand;
-    unsigned long long te = 0;
+    const int n = b.cnt->nchunk;
     for (int i = gw; i < n; i += nw) {
-        const int v = all ? i : b.cand[i];
-        const int own = b.label[v];
-        const int64_t s = b.off[v], e = b.off[v + 1];
-        for (int c = lane; c < eff; c += 32) h[c] = 0;
-        __syncwarp();
-        bool diff = false;
-        for (int64_t j = s + lane; j < e; j += 32) {
-            const int lu = b.label[ld_stream(b.col + j)];
-            diff |= (lu != own);
-            if ((unsigned)lu < (unsigned)eff) atomicAdd(&h[lu], 1);
+        const int2 q = b.chunkq[i];
+        const int64_t s = b.off[q.x] + q.y, rowe = b.off[q.x + 1];
+        const int64_t e = rowe - s > kChunk ? s + kChunk : rowe;
+        warp_row(b.col, s, e, lane, [&](int u) { b.stamp[u] = t; }, [] { return false; });
+    }
+}
+
+// ------------------------------------------------------------------------------------ bnd
+struct BndArgs {
+    int t, all, ibits, maxdeg;
+    int nb0, nb1, nb2;
+    int g0, g1;  // block split: [0,g0) thread class, [g0,g0+g1) warp class, rest block class
+};
+
+__device__ __forceinline__ uint64_t sel_key(const Buffers &b, int own, int deg, int v, int ibits, int maxdeg) {
+    const uint64_t dk = b.RE[own] > 1.0 ? (uint64_t)(maxdeg - deg) : (uint64_t)deg;
+    return (dk << ibits) | (uint64_t)v;
+}
+
+__device__ __forceinline__ void put_record(const Buffers &b, int idx, int v, int own, uint64_t key) {
+    b.bv[idx] = v;
+    b.bown[idx] = own;
+    b.bkey[idx] = key;
+    b.bsel[idx] = 0;
+    atomicAdd(&b.npart[own], 1);
+}
+
+__global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a) {
+    if (b.ctrl->stopped) return;
+    const int lane = threadIdx.x & 31;
+    unsigned long long te = 0, rd = 0, nc = 0;
+    if ((int)blockIdx.x < a.g0) {
+        // ---- thread per vertex (deg <= kSmallDeg) ----
+        const int n = a.nb0;
+        for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += a.g0 * blockDim.x) {
+            const int i = i0 + threadIdx.x;
+            bool isb = false;
+            int v = 0, own = 0, deg = 0;
+            if (i < n) {
+                v = b.bucket[0][i];
+                if (a.all || b.stamp[v] == a.t) {
+                    own = b.label[v];
+                    const int64_t s = b.off[v];
+                    deg = (int)(b.off[v + 1] - s);
+                    ++nc;
+                    te += deg;
+                    int j = 0;
+                    for (; j < deg; ++j)
+                        if (b.label[__ldg(b.col + s + j)] != own) {
+                            isb = true;
+                            ++j;
+                            break;
+                        }
+                    rd += j;
+                }
+            }
+            const int slot = warp_append(&b.cnt->nbnd, isb);
+            if (isb) put_record(b, slot, v, own, sel_key(b, own, deg, v, a.ibits, a.maxdeg));
         }
-        __syncwarp();
-        if (lane == 0) te += (unsigned long long)(e - s);
-        if (__any_sync(DMOLP_FULL_MASK, diff)) {
-            double best = -DBL_MAX;
-            int bkey = 0x7fffffff, blab = -1;
-            for (int c = lane; c < eff; c += 32) {
-                const int cnt = h[c];
-                const double sc = cnt > 0 ? __dmul_rn((double)cnt, b.tpen[c]) : 0.0;
-                const int key = (c & ~31) | (int)brev5((unsigned)c & 31u);
-                if (sc > best || (sc == best && key < bkey)) {
-                    best = sc;
-                    bkey = key;
-                    blab = c;
-                }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ob = __shfl_xor_sync(DMOLP_FULL_MASK, best, o);
-                const int ok = __shfl_xor_sync(DMOLP_FULL_MASK, bkey, o);
-                const int ol = __shfl_xor_sync(DMOLP_FULL_MASK, blab, o);
-                if (ob > best || (ob == best && ok < bkey)) {
-                    best = ob;
-                    bkey = ok;
-                    blab = ol;
-                }
-            }
+    } else if ((int)blockIdx.x < a.g0 + a.g1) {
+        // ---- warp per vertex ----
+        const int wpb = blockDim.x >> 5;
+        const int gw = ((int)blockIdx.x - a.g0) * wpb + (threadIdx.x >> 5), nw = a.g1 * wpb;
+        for (int i = gw; i < a.nb1; i += nw) {
+            const int v = b.bucket[1][i];
+            if (!a.all && b.stamp[v] != a.t) continue;
+            const int own = b.label[v];
+            const int64_t s = b.off[v], e = b.off[v + 1];
+            bool diff = false;
+            const int64_t r = warp_row(b.col, s, e, lane, [&](int u) { diff |= (b.label[u] != own); },
+                                       [&] { return __any_sync(DMOLP_FULL_MASK, diff); });
             if (lane == 0) {
-                const double own_raw = (unsigned)own < (unsigned)eff ? (double)h[own] : -1e300;
-                const int nl = best > own_raw ? blab : own;
+                ++nc;
+                te += (unsigned long long)(e - s);
+                rd += (unsigned long long)r;
+            }
+            if (__any_sync(DMOLP_FULL_MASK, diff) && lane == 0) {
                 const int idx = atomicAdd(&b.cnt->nbnd, 1);
-                const int deg = (int)(e - s);
-                const uint64_t dk = b.RE[own] > 1.0 ? (uint64_t)(maxdeg - deg) : (uint64_t)deg;
-                b.bv[idx] = v;
-                b.bown[idx] = own;
-                b.bnew[idx] = nl;
-                b.bkey[idx] = (dk << ibits) | (uint64_t)v;
-                b.bsel[idx] = 0;
-                atomicAdd(&b.npart[own], 1);
+                put_record(b, idx, v, own, sel_key(b, own, (int)(e - s), v, a.ibits, a.maxdeg));
             }
         }
-        __syncwarp();
+    } else {
+        // ---- block per vertex (deg > kLargeDeg) ----
+        const int gb = (int)blockIdx.x - a.g0 - a.g1, nbk = (int)gridDim.x - a.g0 - a.g1;
+        for (int i = gb; i < a.nb2; i += nbk) {
+            const int v = b.bucket[2][i];
+            if (!a.all && b.stamp[v] != a.t) continue;
+            const int own = b.label[v];
+            const int64_t s = b.off[v], e = b.off[v + 1];
+            bool diff = false;
+            int64_t j0 = s;
+            for (; j0 < e; j0 += blockDim.x * 4) {
+                for (int q = 0; q < 4; ++q) {
+                    const int64_t j = j0 + q * blockDim.x + threadIdx.x;
+                    if (j < e) diff |= (b.label[__ldcs(b.col + j)] != own);
+                }
+                if (__syncthreads_or(diff)) {
+                    j0 += blockDim.x * 4;
+                    break;
+                }
+            }
+            const bool isb = __syncthreads_or(diff);
+            if (threadIdx.x == 0) {
+                ++nc;
+                te += (unsigned long long)(e - s);
+                rd += (unsigned long long)((j0 < e ? j0 : e) - s);
+                if (isb) {
+                    const int idx = atomicAdd(&b.cnt->nbnd, 1);
+                    put_record(b, idx, v, own, sel_key(b, own, (int)(e - s), v, a.ibits, a.maxdeg));
+                }
+            }
+            __syncthreads();
+        }
     }
     te = warp_sum_u64(te);
-    if (lane == 0 && te) atomicAdd(&b.rec[t - 1].te_cand, te);
+    rd = warp_sum_u64(rd);
+    nc = warp_sum_u64(nc);
+    if (lane == 0) {
+        if (te) atomicAdd(&b.rec[a.t - 1].te_cand, te);
+        if (rd) atomicAdd(&b.rec[a.t - 1].arcs_bnd, rd);
+        if (nc) atomicAdd(&b.cnt->ncand, (int)nc);
+    }
 }
 
 // ------------------------------------------------------------------------------------ need
@@ -213,102 +307,343 @@ __global__ void k_lp_need(Buffers b, int k, int t) {
     }
 }
 
-// ------------------------------------------------------------------------------------ commit
-__global__ void k_lp_commit(Buffers b, int t, int apply) {
+// ------------------------------------------------------------------------------------ split
+// Selected records: next window (for marking) and decision class.  A vertex whose own label is not scored
+// (>= eff) goes to the warp class, whose histogram also sees absent labels.
+__global__ void k_split(Buffers b, int t, int eff) {
     if (b.ctrl->stopped) return;
     const int n = b.cnt->nbnd;
     int32_t *win = b.win[t & 1];
     unsigned long long te = 0;
     for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
         const int i = i0 + threadIdx.x;
-        bool take = false, moved = false;
-        int v = 0;
-        if (i < n && b.bsel[i]) {
-            take = true;
+        const bool take = i < n && b.bsel[i];
+        int v = 0, cls = -1;
+        if (take) {
             v = b.bv[i];
-            te += (unsigned long long)(b.off[v + 1] - b.off[v]);
-            const int nl = b.bnew[i];
-            if (apply && nl != b.bown[i]) {
-                b.label[v] = nl;
-                moved = true;
-            }
+            const int deg = (int)(b.off[v + 1] - b.off[v]);
+            te += (unsigned long long)deg;
+            cls = deg > kLargeDeg ? 2 : ((deg > kSmallDeg || b.bown[i] >= eff) ? 1 : 0);
         }
         const int slot = warp_append(&b.cnt->nwin[t & 1], take);
         if (take) win[slot] = v;
-        warp_append(&b.cnt->nchanged, moved);
+        for (int c = 0; c < 3; ++c) {
+            const int s2 = warp_append(&b.cnt->ndec[c], cls == c);
+            if (cls == c) b.dec[c][s2] = v;
+        }
     }
     te = warp_sum_u64(te);
     if ((threadIdx.x & 31) == 0 && te) atomicAdd(&b.rec[t - 1].te_sel, te);
 }
 
-// ------------------------------------------------------------------------------------ mid
-// Decides whether this iteration runs the statistics pass (run_phase2's breaks at phase2.cpp:309 and 387
-// come before the statistics), and clears the accumulators for it.
-__global__ void k_lp_mid(Buffers b, int k, int t) {
-    LpControl *ctl = b.ctrl;
-    if (ctl->stopped) return;
-    __shared__ int s_skip;
-    if (threadIdx.x == 0) {
-        LpRecordDev &r = b.rec[t - 1];
-        r.window = b.cnt->nwin[t & 1];
-        r.candidates = t == 1 ? -1 : b.cnt->ncand;
-        r.changes = b.cnt->nchanged;
-        r.boundary = b.cnt->nbnd;
-        int skip = 0;
-        if (r.window == 0) {
-            skip = 1;
-            if (ctl->mode == DMOLP_LP_MODE_REF) ctl->stop_now = 1;
-        } else if (r.changes == 0 && ctl->mode == DMOLP_LP_MODE_REF) {
-            skip = 1;
-            ctl->stop_now = 2;
-        }
-        ctl->skip_stats = skip;
-        if (!skip) b.cnt->cut_arcs = 0;
-        s_skip = skip;
-    }
-    __syncthreads();
-    if (!s_skip)
-        for (int p = threadIdx.x; p < k; p += blockDim.x) {
-            b.vc[p] = 0;
-            b.intra[p] = 0;
-        }
+// ------------------------------------------------------------------------------------ decide
+struct DecArgs {
+    int t, eff;
+    int g0, g1;  // block split as in BndArgs
+};
+
+__device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
+    b.newlab[v] = nl;
+    const int q = atomicAdd(&b.cnt->nchanged, 1);
+    b.mov[q] = v;
 }
 
-// ------------------------------------------------------------------------------------ stats
-// The fused edge-cut / balance pass: per vertex its label count, its same-label arcs and its cut arcs.
-// Warp per vertex; per-block shared accumulators per label.
-__global__ void k_stats(Buffers b, int k, int nv, const int *stopped, const int *skip) {
-    if ((stopped && *stopped) || (skip && *skip)) return;
-    extern __shared__ unsigned long long sacc[];  // [2k]: vertex counts, intra arcs
-    unsigned long long *svc = sacc, *sin = sacc + k;
+__global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
+    if (b.ctrl->stopped) return;
+    extern __shared__ int shist[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int eff = a.eff;
+    unsigned long long rd = 0;
+    if ((int)blockIdx.x < a.g0) {
+        // ---- thread per vertex: deg <= 16 and own label < eff; only present labels can beat the own raw
+        //      count (an absent label scores 0 <= count[own]) ----
+        const int n = b.cnt->ndec[0];
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += a.g0 * blockDim.x) {
+            const int v = b.dec[0][i];
+            const int own = b.label[v];
+            const int64_t s = b.off[v];
+            const int deg = (int)(b.off[v + 1] - s);
+            int l[kSmallDeg];
+#pragma unroll
+            for (int j = 0; j < kSmallDeg; ++j) l[j] = j < deg ? b.label[__ldg(b.col + s + j)] : -1;
+            rd += deg;
+            int own_cnt = 0;
+            double best = -DBL_MAX;
+            int bkey = 0x7fffffff, blab = -1;
+#pragma unroll
+            for (int j = 0; j < kSmallDeg; ++j) {
+                own_cnt += (l[j] == own);
+                const int c = l[j];
+                if ((unsigned)c < (unsigned)eff) {
+                    int cnt = 0;
+#pragma unroll
+                    for (int q = 0; q < kSmallDeg; ++q) cnt += (l[q] == c);
+                    const double sc = __dmul_rn((double)cnt, b.tpen[c]);
+                    const int key = tiekey(c);
+                    if (better(sc, key, best, bkey)) {
+                        best = sc;
+                        bkey = key;
+                        blab = c;
+                    }
+                }
+            }
+            if (blab >= 0 && best > (double)own_cnt && blab != own) park_move(b, v, blab);
+        }
+    } else if ((int)blockIdx.x < a.g0 + a.g1) {
+        // ---- warp per vertex: shared histogram of the scored labels ----
+        int *h = shist + wib * eff;
+        const int wpb = blockDim.x >> 5;
+        const int gw = ((int)blockIdx.x - a.g0) * wpb + wib, nw = a.g1 * wpb;
+        const int n = b.cnt->ndec[1];
+        for (int i = gw; i < n; i += nw) {
+            const int v = b.dec[1][i];
+            const int own = b.label[v];
+            const int64_t s = b.off[v], e = b.off[v + 1];
+            for (int c = lane; c < eff; c += 32) h[c] = 0;
+            __syncwarp();
+            warp_row(b.col, s, e, lane, [&](int u) {
+                const int lu = b.label[u];
+                if ((unsigned)lu < (unsigned)eff) atomicAdd(&h[lu], 1);
+            }, [] { return false; });
+            __syncwarp();
+            double best = -DBL_MAX;
+            int bkey = 0x7fffffff, blab = -1;
+            for (int c = lane; c < eff; c += 32) {
+                const int cnt = h[c];
+                const double sc = cnt > 0 ? __dmul_rn((double)cnt, b.tpen[c]) : 0.0;
+                const int key = tiekey(c);
+                if (better(sc, key, best, bkey)) {
+                    best = sc;
+                    bkey = key;
+                    blab = c;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(DMOLP_FULL_MASK, best, o);
+                const int ok = __shfl_xor_sync(DMOLP_FULL_MASK, bkey, o);
+                const int ol = __shfl_xor_sync(DMOLP_FULL_MASK, blab, o);
+                if (better(ob, ok, best, bkey)) {
+                    best = ob;
+                    bkey = ok;
+                    blab = ol;
+                }
+            }
+            if (lane == 0) {
+                rd += (unsigned long long)(e - s);
+                const double own_raw = (unsigned)own < (unsigned)eff ? (double)h[own] : -1e300;
+                const int nl = best > own_raw ? blab : own;
+                if (nl != own) park_move(b, v, nl);
+            }
+            __syncwarp();
+        }
+    } else {
+        // ---- block per vertex: one shared histogram per block ----
+        __shared__ double s_best[kWarpsPerBlock];
+        __shared__ int s_key[kWarpsPerBlock], s_lab[kWarpsPerBlock];
+        const int gb = (int)blockIdx.x - a.g0 - a.g1, nbk = (int)gridDim.x - a.g0 - a.g1;
+        const int n = b.cnt->ndec[2];
+        for (int i = gb; i < n; i += nbk) {
+            const int v = b.dec[2][i];
+            const int own = b.label[v];
+            const int64_t s = b.off[v], e = b.off[v + 1];
+            for (int c = threadIdx.x; c < eff; c += blockDim.x) shist[c] = 0;
+            __syncthreads();
+            for (int64_t j = s + threadIdx.x; j < e; j += blockDim.x) {
+                const int lu = b.label[__ldcs(b.col + j)];
+                if ((unsigned)lu < (unsigned)eff) atomicAdd(&shist[lu], 1);
+            }
+            __syncthreads();
+            double best = -DBL_MAX;
+            int bkey = 0x7fffffff, blab = -1;
+            for (int c = threadIdx.x; c < eff; c += blockDim.x) {
+                const int cnt = shist[c];
+                const double sc = cnt > 0 ? __dmul_rn((double)cnt, b.tpen[c]) : 0.0;
+                const int key = tiekey(c);
+                if (better(sc, key, best, bkey)) {
+                    best = sc;
+                    bkey = key;
+                    blab = c;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(DMOLP_FULL_MASK, best, o);
+                const int ok = __shfl_xor_sync(DMOLP_FULL_MASK, bkey, o);
+                const int ol = __shfl_xor_sync(DMOLP_FULL_MASK, blab, o);
+                if (better(ob, ok, best, bkey)) {
+                    best = ob;
+                    bkey = ok;
+                    blab = ol;
+                }
+            }
+            if (lane == 0) {
+                s_best[wib] = best;
+                s_key[wib] = bkey;
+                s_lab[wib] = blab;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int w = 1; w < kWarpsPerBlock; ++w)
+                    if (better(s_best[w], s_key[w], best, bkey)) {
+                        best = s_best[w];
+                        bkey = s_key[w];
+                        blab = s_lab[w];
+                    }
+                rd += (unsigned long long)(e - s);
+                const double own_raw = (unsigned)own < (unsigned)eff ? (double)shist[own] : -1e300;
+                const int nl = best > own_raw ? blab : own;
+                if (nl != own) park_move(b, v, nl);
+            }
+            __syncthreads();
+        }
+    }
+    rd = warp_sum_u64(rd);
+    if (lane == 0 && rd) atomicAdd(&b.rec[a.t - 1].arcs_dec, rd);
+}
+
+// ------------------------------------------------------------------------------------ update
+// Warp per mover v (old label a = label[v], new label c = newlab[v]).  For each arc (v,u), with u's old
+// label lo = label[u] and new label ln (newlab[u] if u moves, else lo), the arc leaves the cut count
+// [a != lo] and the intra count of a if a == lo, and enters them with (c, ln).  Weight 2 when u stays:
+// the reverse arc (u,v) changes the same way but is never visited; weight 1 when u moves (or u == v):
+// (u,v) is visited from u's side.  Vertex counts move by one.
+__global__ void k_update(Buffers b, int k, int t) {
+    if (b.ctrl->stopped) return;
+    extern __shared__ unsigned long long sacc[];  // [2k]: vertex-count deltas, intra-arc deltas
     for (int p = threadIdx.x; p < 2 * k; p += blockDim.x) sacc[p] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int n = b.cnt->nchanged;
+    long long dcut = 0;
+    unsigned long long rd = 0;
+    for (int i = gw; i < n; i += nw) {
+        const int v = b.mov[i];
+        const int a = b.label[v], c = b.newlab[v];
+        const int64_t s = b.off[v], e = b.off[v + 1];
+        long long in_c = 0, out_a = 0, dc = 0;
+        warp_row(b.col, s, e, lane, [&](int u) {
+            const int lo = b.label[u];
+            const int nu = b.newlab[u];
+            const int ln = nu >= 0 ? nu : lo;
+            const int w = nu >= 0 ? 1 : 2;
+            dc += w * ((int)(c != ln) - (int)(a != lo));
+            in_c += w * (int)(c == ln);
+            out_a += w * (int)(a == lo);
+        }, [] { return false; });
+        for (int o = 16; o > 0; o >>= 1) {
+            in_c += __shfl_xor_sync(DMOLP_FULL_MASK, in_c, o);
+            out_a += __shfl_xor_sync(DMOLP_FULL_MASK, out_a, o);
+        }
+        dcut += dc;
+        if (lane == 0) {
+            rd += (unsigned long long)(e - s);
+            atomicAdd(&sacc[a], (unsigned long long)(-1ll));
+            atomicAdd(&sacc[c], 1ull);
+            if (in_c) atomicAdd(&sacc[k + c], (unsigned long long)in_c);
+            if (out_a) atomicAdd(&sacc[k + a], (unsigned long long)(-out_a));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) dcut += __shfl_xor_sync(DMOLP_FULL_MASK, dcut, o);
+    rd = warp_sum_u64(rd);
+    if (lane == 0) {
+        if (dcut) atomicAdd(&b.cnt->cut_arcs, (unsigned long long)dcut);
+        if (rd) atomicAdd(&b.rec[t - 1].arcs_upd, rd);
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < k; p += blockDim.x) {
+        if (sacc[p]) atomicAdd(&b.vc[p], sacc[p]);
+        if (sacc[k + p]) atomicAdd(&b.intra[p], sacc[k + p]);
+    }
+}
+
+// Movers take their labels.
+__global__ void k_apply(Buffers b) {
+    if (b.ctrl->stopped) return;
+    const int n = b.cnt->nchanged;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int v = b.mov[i];
+        b.label[v] = b.newlab[v];
+        b.newlab[v] = -1;
+    }
+}
+
+// ------------------------------------------------------------------------------------ stats
+// The fused edge-cut / balance pass over all vertices: label counts (all vertices, coalesced), and per
+// degree class the same-label and cut arcs.  Block ranges: [0,gv) vertex counts, then the three classes.
+struct StatsArgs {
+    int k, nv, gv, g0, g1, nb0, nb1, nb2;
+};
+
+__global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int *stopped, const int *skip) {
+    if ((stopped && *stopped) || (skip && *skip)) return;
+    extern __shared__ unsigned long long sacc[];  // [2k]: vertex counts, intra arcs
+    const int k = a.k;
+    unsigned long long *svc = sacc, *sin = sacc + k;
+    for (int p = threadIdx.x; p < 2 * k; p += blockDim.x) sacc[p] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     unsigned long long cut = 0;
     bool bad = false;
-    for (int v = gw; v < nv; v += nw) {
-        const int lv = b.label[v];
-        const int64_t s = b.off[v], e = b.off[v + 1];
-        unsigned int same = 0, diff = 0;
-        for (int64_t j = s + lane; j < e; j += 32) {
-            const int lu = b.label[ld_stream(b.col + j)];
-            bad |= (unsigned)lu >= (unsigned)k;
-            same += (lu == lv);
-            diff += (lu != lv);
+    const int bx = blockIdx.x;
+    if (bx < a.gv) {
+        for (int v = bx * blockDim.x + threadIdx.x; v < a.nv; v += a.gv * blockDim.x) {
+            const int lv = b.label[v];
+            if ((unsigned)lv < (unsigned)k) atomicAdd(&svc[lv], 1ull);
+            else bad = true;
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            same += __shfl_xor_sync(DMOLP_FULL_MASK, same, o);
-            diff += __shfl_xor_sync(DMOLP_FULL_MASK, diff, o);
-        }
-        if (lane == 0) {
-            if ((unsigned)lv < (unsigned)k) {
-                atomicAdd(&svc[lv], 1ull);
-                if (same) atomicAdd(&sin[lv], (unsigned long long)same);
-            } else {
-                bad = true;
+    } else if (bx < a.gv + a.g0) {
+        for (int i = (bx - a.gv) * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
+            const int v = b.bucket[0][i];
+            const int lv = b.label[v];
+            const int64_t s = b.off[v], e = b.off[v + 1];
+            unsigned int same = 0, diff = 0;
+            for (int64_t j = s; j < e; ++j) {
+                const int lu = b.label[__ldg(b.col + j)];
+                bad |= (unsigned)lu >= (unsigned)k;
+                same += (lu == lv);
+                diff += (lu != lv);
             }
             cut += diff;
+            if (same && (unsigned)lv < (unsigned)k) atomicAdd(&sin[lv], (unsigned long long)same);
+        }
+    } else if (bx < a.gv + a.g0 + a.g1) {
+        const int wpb = blockDim.x >> 5;
+        const int gw = (bx - a.gv - a.g0) * wpb + wib, nw = a.g1 * wpb;
+        for (int i = gw; i < a.nb1; i += nw) {
+            const int v = b.bucket[1][i];
+            const int lv = b.label[v];
+            unsigned int same = 0, diff = 0;
+            warp_row(b.col, b.off[v], b.off[v + 1], lane, [&](int u) {
+                const int lu = b.label[u];
+                bad |= (unsigned)lu >= (unsigned)k;
+                same += (lu == lv);
+                diff += (lu != lv);
+            }, [] { return false; });
+            for (int o = 16; o > 0; o >>= 1) {
+                same += __shfl_xor_sync(DMOLP_FULL_MASK, same, o);
+                diff += __shfl_xor_sync(DMOLP_FULL_MASK, diff, o);
+            }
+            if (lane == 0) {
+                cut += diff;
+                if (same && (unsigned)lv < (unsigned)k) atomicAdd(&sin[lv], (unsigned long long)same);
+            }
+        }
+    } else {
+        const int gb = bx - a.gv - a.g0 - a.g1, nbk = (int)gridDim.x - a.gv - a.g0 - a.g1;
+        for (int i = gb; i < a.nb2; i += nbk) {
+            const int v = b.bucket[2][i];
+            const int lv = b.label[v];
+            const int64_t s = b.off[v], e = b.off[v + 1];
+            unsigned int same = 0, diff = 0;
+            for (int64_t j = s + threadIdx.x; j < e; j += blockDim.x) {
+                const int lu = b.label[__ldcs(b.col + j)];
+                bad |= (unsigned)lu >= (unsigned)k;
+                same += (lu == lv);
+                diff += (lu != lv);
+            }
+            cut += diff;
+            for (int o = 16; o > 0; o >>= 1) same += __shfl_xor_sync(DMOLP_FULL_MASK, same, o);
+            if (lane == 0 && same && (unsigned)lv < (unsigned)k) atomicAdd(&sin[lv], (unsigned long long)same);
         }
     }
     cut = warp_sum_u64(cut);
@@ -322,12 +657,25 @@ __global__ void k_stats(Buffers b, int k, int nv, const int *stopped, const int 
 }
 
 // ------------------------------------------------------------------------------------ end
-__global__ void k_lp_end(Buffers b, int k, int t, long long narcs) {
+__global__ void k_lp_end(Buffers b, int k, int t, long long narcs, int mode) {
     LpControl *ctl = b.ctrl;
     if (ctl->stopped) return;
+    LpCounters *cn = b.cnt;
     LpRecordDev &r = b.rec[t - 1];
-    if (!ctl->skip_stats) {
-        const unsigned long long arcs = b.cnt->cut_arcs;
+    r.window = cn->nwin[t & 1];
+    r.candidates = t == 1 ? -1 : cn->ncand;
+    r.changes = cn->nchanged;
+    r.boundary = cn->nbnd;
+    bool stats = true;
+    if (r.window == 0) {
+        stats = false;
+        if (mode == DMOLP_LP_MODE_REF) ctl->stop_now = 1;
+    } else if (r.changes == 0 && mode == DMOLP_LP_MODE_REF) {
+        stats = false;
+        ctl->stop_now = 2;
+    }
+    if (stats) {
+        const unsigned long long arcs = cn->cut_arcs;
         r.te_stats = (unsigned long long)narcs;
         if ((arcs & 1ull) || ctl->error) {
             ctl->error = 1;
@@ -339,20 +687,41 @@ __global__ void k_lp_end(Buffers b, int k, int t, long long narcs) {
             if (delta < 0.03) ctl->conv += 1;
             else ctl->conv = 0;
             ctl->prev_cut = cur;
-            if (ctl->mode == DMOLP_LP_MODE_REF && ctl->conv >= 10) ctl->stop_now = 3;
+            if (mode == DMOLP_LP_MODE_REF && ctl->conv >= 10) ctl->stop_now = 3;
         }
     }
     r.edge_cut = ctl->prev_cut;
     long long *ch = b.cnthist + (size_t)(t - 1) * 2 * DMOLP_MAX_K;
     for (int p = 0; p < k; ++p) {
-        ch[p] = (long long)b.vc[p];
-        ch[DMOLP_MAX_K + p] = (long long)(b.intra[p] / 2);
+        ch[p] = sll(b.vc[p]);
+        ch[DMOLP_MAX_K + p] = sll(b.intra[p]) / 2;
     }
     ctl->iters_run = t;
     if (ctl->stop_now) {
         ctl->stopped = 1;
         ctl->stop_reason = ctl->stop_now;
     }
+}
+
+// Asymmetric graphs: decide whether the full statistics pass runs (the reference skips it on an empty
+// window and, with its stopping rules, on zero changes) and clear its accumulators.
+__global__ void k_lp_mid(Buffers b, int k, int t, int mode) {
+    LpControl *ctl = b.ctrl;
+    if (ctl->stopped) return;
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) {
+        const int win = b.cnt->nwin[t & 1], ch = b.cnt->nchanged;
+        const int skip = (win == 0) || (ch == 0 && mode == DMOLP_LP_MODE_REF);
+        ctl->skip_stats = skip;
+        if (!skip) b.cnt->cut_arcs = 0;
+        s_skip = skip;
+    }
+    __syncthreads();
+    if (!s_skip)
+        for (int p = threadIdx.x; p < k; p += blockDim.x) {
+            b.vc[p] = 0;
+            b.intra[p] = 0;
+        }
 }
 
 __global__ void k_lp_init_end(Buffers b, int mode) {
@@ -374,116 +743,191 @@ __global__ void k_lp_init_end(Buffers b, int mode) {
     }
 }
 
-__global__ void k_reset_stats(Buffers b, int k, const int *stopped) {
-    if (stopped && *stopped) return;
+__global__ void k_reset_stats(Buffers b, int k, int clear_error) {
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
         b.vc[p] = 0;
         b.intra[p] = 0;
     }
     if (threadIdx.x == 0) {
         b.cnt->cut_arcs = 0;
-        if (!stopped) b.ctrl->error = 0;
+        if (clear_error) b.ctrl->error = 0;
     }
 }
 
-// ---- single-call pieces (dmolp_window_select / dmolp_lp_apply) ----
-
-// Records for an explicit window list (already in b.cand, count in cnt->ncand): decisions only.
-__global__ void k_apply_scan(Buffers b, int n, int eff) {
-    extern __shared__ int shist[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    int *h = shist + wib * eff;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    for (int i = gw; i < n; i += nw) {
-        const int v = b.cand[i];
-        const int own = b.label[v];
-        const int64_t s = b.off[v], e = b.off[v + 1];
-        for (int c = lane; c < eff; c += 32) h[c] = 0;
-        __syncwarp();
-        for (int64_t j = s + lane; j < e; j += 32) {
-            const int lu = b.label[b.col[j]];
-            if ((unsigned)lu < (unsigned)eff) atomicAdd(&h[lu], 1);
-        }
-        __syncwarp();
-        double best = -DBL_MAX;
-        int bkey = 0x7fffffff, blab = -1;
-        for (int c = lane; c < eff; c += 32) {
-            const int cnt = h[c];
-            const double sc = cnt > 0 ? __dmul_rn((double)cnt, b.tpen[c]) : 0.0;
-            const int key = (c & ~31) | (int)brev5((unsigned)c & 31u);
-            if (sc > best || (sc == best && key < bkey)) {
-                best = sc;
-                bkey = key;
-                blab = c;
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob = __shfl_xor_sync(DMOLP_FULL_MASK, best, o);
-            const int ok = __shfl_xor_sync(DMOLP_FULL_MASK, bkey, o);
-            const int ol = __shfl_xor_sync(DMOLP_FULL_MASK, blab, o);
-            if (ob > best || (ob == best && ok < bkey)) {
-                best = ob;
-                bkey = ok;
-                blab = ol;
-            }
-        }
-        if (lane == 0) {
-            const double own_raw = (unsigned)own < (unsigned)eff ? (double)h[own] : -1e300;
-            b.bnew[i] = best > own_raw ? blab : own;
-            b.bown[i] = own;
-            b.bv[i] = v;
-        }
-        __syncwarp();
-    }
-}
-
-__global__ void k_apply_commit(Buffers b, int n) {
-    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
-        const int i = i0 + threadIdx.x;
-        bool moved = false;
-        if (i < n && b.bnew[i] != b.bown[i]) {
-            b.label[b.bv[i]] = b.bnew[i];
-            moved = true;
-        }
-        const int slot = warp_append(&b.cnt->nchanged, moved);
-        if (moved) b.win[0][slot] = i;  // index into bv/bnew of the moved record
-    }
-}
-
-__global__ void k_zero_counters(Buffers b) {
-    b.cnt->ncand = 0;
-    b.cnt->nbnd = 0;
-    b.cnt->nwin[0] = b.cnt->nwin[1] = 0;
-    b.cnt->nchanged = 0;
-}
-
-// Set-up of a stand-alone window selection: the caller's previous window is in win[(t-1)&1].
+// ---- stand-alone pieces (dmolp_window_select / dmolp_lp_apply) ----
 __global__ void k_ws_begin(Buffers b, int k, int t, int nprev) {
     for (int p = threadIdx.x; p < k; p += blockDim.x) b.npart[p] = 0;
     if (threadIdx.x == 0) {
-        b.cnt->ncand = 0;
-        b.cnt->nbnd = 0;
-        b.cnt->nchanged = 0;
-        b.cnt->nwin[(t - 1) & 1] = nprev;
-        b.cnt->nwin[t & 1] = 0;
+        LpCounters *cn = b.cnt;
+        cn->ncand = cn->nbnd = cn->nchanged = cn->nchunk = 0;
+        cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
+        cn->nwin[(t - 1) & 1] = nprev;
+        cn->nwin[t & 1] = 0;
         b.ctrl->stopped = 0;
         LpRecordDev &r = b.rec[t - 1];
         r.te_prev = r.te_cand = r.te_sel = r.te_stats = 0;
+        r.arcs_bnd = r.arcs_dec = r.arcs_upd = 0;
     }
+}
+
+// An explicit window (n vertices in b.cand) sorted into decision classes.
+__global__ void k_classify(Buffers b, int n, int eff) {
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        int cls = -1, v = 0;
+        if (i < n) {
+            v = b.cand[i];
+            const int deg = (int)(b.off[v + 1] - b.off[v]);
+            const int own = b.label[v];
+            cls = deg > kLargeDeg ? 2 : ((deg > kSmallDeg || (unsigned)own >= (unsigned)eff) ? 1 : 0);
+        }
+        for (int c = 0; c < 3; ++c) {
+            const int s2 = warp_append(&b.cnt->ndec[c], cls == c);
+            if (cls == c) b.dec[c][s2] = v;
+        }
+    }
+}
+
+__global__ void k_zero_small(Buffers b) {
+    LpCounters *cn = b.cnt;
+    cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
+    cn->nchanged = 0;
+    b.ctrl->stopped = 0;
+}
+
+// Movers of dmolp_lp_apply as (vertex, label) pairs into bv/bnew.
+__global__ void k_collect_moves(Buffers b) {
+    const int n = b.cnt->nchanged;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int v = b.mov[i];
+        b.bv[i] = v;
+        b.bnew[i] = b.newlab[v];
+    }
+}
+
+// Warp per vertex u: every arc (u,v) must have its reverse, found by binary search in v's (strictly
+// increasing) row; a missing one sets the flag.
+__global__ void k_symcheck(Buffers b, int nv) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    bool missing = false;
+    for (int u = gw; u < nv; u += nw) {
+        for (int64_t j = b.off[u] + lane; j < b.off[u + 1]; j += 32) {
+            const int v = b.col[j];
+            int64_t lo = b.off[v], hi = b.off[v + 1];
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (b.col[mid] < u) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo >= b.off[v + 1] || b.col[lo] != u) missing = true;
+        }
+    }
+    if (__any_sync(DMOLP_FULL_MASK, missing) && lane == 0) *b.flag = 1;
+}
+
+__global__ void k_fill_int(int32_t *p, int64_t n, int32_t v) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = v;
 }
 
 int grid_for(dmolp_ctx *c) { return c->num_sms * kGridPerSm; }
 
+int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+BndArgs bnd_args(dmolp_ctx *c, int t, int all) {
+    BndArgs a;
+    a.t = t;
+    a.all = all;
+    a.ibits = c->ibits;
+    a.maxdeg = (int)c->maxdeg;
+    a.nb0 = c->nb[0];
+    a.nb1 = c->nb[1];
+    a.nb2 = c->nb[2];
+    const int cap = c->num_sms * 8;
+    a.g0 = clampi((c->nb[0] + 255) / 256, 1, cap);
+    a.g1 = clampi((c->nb[1] + 7) / 8, 1, cap);
+    return a;
+}
+
+int bnd_grid(dmolp_ctx *c, const BndArgs &a) { return a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
+
+DecArgs dec_args(dmolp_ctx *c, int t, int eff) {
+    DecArgs a;
+    a.t = t;
+    a.eff = eff;
+    a.g0 = c->num_sms * 2;
+    a.g1 = c->num_sms * 4;
+    return a;
+}
+
+int dec_grid(dmolp_ctx *c, const DecArgs &a) { return a.g0 + a.g1 + c->num_sms; }
+
+size_t dec_smem(int eff) { return (size_t)kWarpsPerBlock * eff * sizeof(int); }
+
+StatsArgs stats_args(dmolp_ctx *c, int k) {
+    StatsArgs a;
+    a.k = k;
+    a.nv = (int)c->nv;
+    const int cap = c->num_sms * 8;
+    a.gv = clampi((int)((c->nv + 255) / 256), 1, c->num_sms * 2);
+    a.g0 = clampi((c->nb[0] + 255) / 256, 1, cap);
+    a.g1 = clampi((c->nb[1] + 7) / 8, 1, cap);
+    a.nb0 = c->nb[0];
+    a.nb1 = c->nb[1];
+    a.nb2 = c->nb[2];
+    return a;
+}
+
+int stats_grid(dmolp_ctx *c, const StatsArgs &a) { return a.gv + a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
+
+// Optional timing of one kernel launch (dmolp_set_profiling): an event pair around it on the same stream.
+// While a graph is being captured the records become event-record nodes of the graph, which owns them.
+struct ProfScope {
+    dmolp_ctx *c;
+    cudaEvent_t e1 = nullptr;
+    ProfScope(dmolp_ctx *c_, int kind, int t) : c(c_) {
+        if (!c->profiling) return;
+        cudaEvent_t e0;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        dmolp_ctx::ProfEvents &pe = c->capturing ? c->capture_prof : c->prof_pending;
+        pe.ev.push_back(e0);
+        pe.ev.push_back(e1);
+        pe.kind.push_back(kind);
+        pe.iter.push_back(t);
+        if (!c->capturing) c->prof_owned.push_back(1);
+        record(e0);
+    }
+    void record(cudaEvent_t e) {
+        if (c->capturing) cudaEventRecordWithFlags(e, c->stream, cudaEventRecordExternal);
+        else cudaEventRecord(e, c->stream);
+    }
+    ~ProfScope() {
+        if (e1) record(e1);
+    }
+};
+
 }  // namespace
 
+void lp_check_symmetric(dmolp_ctx *c) {
+    k_symcheck<<<grid_for(c), kBlock, 0, c->stream>>>(c->b, (int)c->nv);
+    c->launches++;
+}
+
+void lp_fill(dmolp_ctx *c, int32_t *p, int64_t n, int32_t v) {
+    k_fill_int<<<grid_for(c), kBlock, 0, c->stream>>>(p, n, v);
+    c->launches++;
+}
+
 void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped) {
-    k_reset_stats<<<1, 256, 0, c->stream>>>(c->b, k, stopped);
+    k_reset_stats<<<1, 256, 0, c->stream>>>(c->b, k, stopped == nullptr);
     c->launches++;
 }
 
 void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip) {
-    k_stats<<<grid_for(c), kBlock, 2 * k * sizeof(unsigned long long), c->stream>>>(c->b, k, (int)c->nv, stopped,
-                                                                                     skip);
+    const StatsArgs a = stats_args(c, k);
+    k_stats<<<stats_grid(c, a), kBlock, 2 * k * sizeof(unsigned long long), c->stream>>>(c->b, a, stopped, skip);
     c->launches++;
 }
 
@@ -492,79 +936,81 @@ void lp_init_end(dmolp_ctx *c, int mode) {
     c->launches++;
 }
 
-// Optional timing of one kernel launch (dmolp_set_profiling): an event pair around it on the same stream.
-struct ProfScope {
-    dmolp_ctx *c;
-    int kind, t;
-    cudaEvent_t e1 = nullptr;
-    ProfScope(dmolp_ctx *c_, int kind_, int t_) : c(c_), kind(kind_), t(t_) {
-        if (!c->profiling) return;
-        cudaEvent_t e0;
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        cudaEventRecord(e0, c->stream);
-        c->prof_events.push_back(e0);
-        c->prof_events.push_back(e1);
-        c->prof_kind.push_back(kind);
-        c->prof_iter.push_back(t);
-    }
-    ~ProfScope() {
-        if (e1) cudaEventRecord(e1, c->stream);
-    }
-};
-
 void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     Buffers &b = c->b;
     const int grid = grid_for(c);
     const int *stopped = &b.ctrl->stopped;
     k_lp_begin<<<1, 256, 0, c->stream>>>(b, L.k, t, (long long)c->narcs);
-    if (t > 1) k_lp_cand<<<grid, kBlock, 0, c->stream>>>(b, t, (int)c->nv);
-    const size_t smem = (size_t)kWarpsPerBlock * L.eff * sizeof(int);
+    c->launches += 1;
+    if (t > 1) {
+        ProfScope ps(c, 2, t);
+        k_mark<<<grid, kBlock, 0, c->stream>>>(b, t);
+        k_mark_chunks<<<grid, kBlock, 0, c->stream>>>(b, t);
+        c->launches += 2;
+    }
     {
         ProfScope ps(c, 0, t);
-        k_lp_scan<<<grid, kBlock, smem, c->stream>>>(b, t, t == 1, (int)c->nv, L.eff, c->ibits, (int)c->maxdeg);
+        const BndArgs a = bnd_args(c, t, t == 1);
+        k_bnd<<<bnd_grid(c, a), kBlock, 0, c->stream>>>(b, a);
     }
     k_lp_need<<<1, 256, 0, c->stream>>>(b, L.k, t);
-    c->launches += t > 1 ? 4 : 3;
+    c->launches += 2;
     select_smallest(c, b.bown, b.bkey, &b.cnt->nbnd, L.k, c->dbits + c->ibits, b.bsel, stopped);
-    k_lp_commit<<<grid, kBlock, 0, c->stream>>>(b, t, 1);
-    k_lp_mid<<<1, 256, 0, c->stream>>>(b, L.k, t);
+    k_split<<<grid, kBlock, 0, c->stream>>>(b, t, L.eff);
     {
         ProfScope ps(c, 1, t);
-        k_stats<<<grid, kBlock, 2 * L.k * sizeof(unsigned long long), c->stream>>>(b, L.k, (int)c->nv, stopped,
-                                                                                    &b.ctrl->skip_stats);
+        const DecArgs d = dec_args(c, t, L.eff);
+        k_decide<<<dec_grid(c, d), kBlock, dec_smem(L.eff), c->stream>>>(b, d);
     }
-    k_lp_end<<<1, 1, 0, c->stream>>>(b, L.k, t, (long long)c->narcs);
-    c->launches += 4;
-}
-
-// The window of dmolp_window_select: prev list in win[(t-1)&1] with count n; RE in b.RE.
-void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int nprev) {
-    (void)RE_dev;  // already copied to b.RE by the caller
-    Buffers &b = c->b;
-    const int grid = grid_for(c);
-    k_ws_begin<<<1, 256, 0, c->stream>>>(b, k, t, nprev);
-    k_lp_cand<<<grid, kBlock, 0, c->stream>>>(b, t, (int)c->nv);
-    // the scan's decisions are not used here (eff = 1 keeps its histogram tiny); only its records are
-    const size_t smem = (size_t)kWarpsPerBlock * 1 * sizeof(int);
-    k_lp_scan<<<grid, kBlock, smem, c->stream>>>(b, t, 0, (int)c->nv, 1, c->ibits, (int)c->maxdeg);
-    k_lp_need<<<1, 256, 0, c->stream>>>(b, k, t);
-    c->launches += 4;
-    select_smallest(c, b.bown, b.bkey, &b.cnt->nbnd, k, c->dbits + c->ibits, b.bsel, nullptr);
-    k_lp_commit<<<grid, kBlock, 0, c->stream>>>(b, t, 0);
+    c->launches += 2;
+    if (c->symmetric) {
+        {
+            ProfScope ps(c, 3, t);
+            k_update<<<grid, kBlock, 2 * L.k * sizeof(unsigned long long), c->stream>>>(b, L.k, t);
+        }
+        k_apply<<<grid, kBlock, 0, c->stream>>>(b);
+        c->launches += 2;
+    } else {
+        k_apply<<<grid, kBlock, 0, c->stream>>>(b);
+        k_lp_mid<<<1, 256, 0, c->stream>>>(b, L.k, t, L.mode);
+        const StatsArgs a = stats_args(c, L.k);
+        k_stats<<<stats_grid(c, a), kBlock, 2 * L.k * sizeof(unsigned long long), c->stream>>>(b, a, stopped,
+                                                                                                &b.ctrl->skip_stats);
+        c->launches += 3;
+    }
+    k_lp_end<<<1, 1, 0, c->stream>>>(b, L.k, t, (long long)c->narcs, L.mode);
     c->launches += 1;
 }
 
-// Decisions + commit for an explicit list already in b.cand (n entries), penalties in b.tpen.
+// dmolp_window_select: previous window in win[(t-1)&1] (nprev entries), RE in b.RE, stamps cleared.
+void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int nprev) {
+    (void)RE_dev;
+    Buffers &b = c->b;
+    const int grid = grid_for(c);
+    k_ws_begin<<<1, 256, 0, c->stream>>>(b, k, t, nprev);
+    k_mark<<<grid, kBlock, 0, c->stream>>>(b, t);
+    k_mark_chunks<<<grid, kBlock, 0, c->stream>>>(b, t);
+    const BndArgs a = bnd_args(c, t, 0);
+    k_bnd<<<bnd_grid(c, a), kBlock, 0, c->stream>>>(b, a);
+    k_lp_need<<<1, 256, 0, c->stream>>>(b, k, t);
+    c->launches += 5;
+    select_smallest(c, b.bown, b.bkey, &b.cnt->nbnd, k, c->dbits + c->ibits, b.bsel, nullptr);
+    k_split<<<grid, kBlock, 0, c->stream>>>(b, t, DMOLP_MAX_K);
+    c->launches += 1;
+}
+
+// dmolp_lp_apply: window in b.cand (n entries), penalties in b.tpen; movers reported in bv/bnew.
 void lp_apply_list(dmolp_ctx *c, int k, int eff, int n) {
     (void)k;
     Buffers &b = c->b;
     const int grid = grid_for(c);
-    k_zero_counters<<<1, 1, 0, c->stream>>>(b);
-    const size_t smem = (size_t)kWarpsPerBlock * eff * sizeof(int);
-    k_apply_scan<<<grid, kBlock, smem, c->stream>>>(b, n, eff);
-    k_apply_commit<<<grid, kBlock, 0, c->stream>>>(b, n);
-    c->launches += 3;
+    k_zero_small<<<1, 1, 0, c->stream>>>(b);
+    k_classify<<<grid, kBlock, 0, c->stream>>>(b, n, eff);
+    const DecArgs d = dec_args(c, 1, eff);
+    k_decide<<<dec_grid(c, d), kBlock, dec_smem(eff), c->stream>>>(b, d);
+    k_collect_moves<<<grid, kBlock, 0, c->stream>>>(b);
+    k_apply<<<grid, kBlock, 0, c->stream>>>(b);
+    c->launches += 5;
 }
 
 }  // namespace dmolp

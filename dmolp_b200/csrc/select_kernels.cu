@@ -131,7 +131,6 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
     const int grid = c->num_sms * 4;
     const size_t smem = nseg <= kSmemSegMax ? (size_t)nseg * kRadix * sizeof(unsigned int) : 0;
     int *nact = &c->b.cnt->nactive[0];
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_sel_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     for (int pass = 0; pass < npass; ++pass) {
         const int shift = top - kRadixBits * (pass + 1);
         const int32_t *in_list = pass == 0 ? nullptr : c->b.active[(pass - 1) & 1];
@@ -145,6 +144,11 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
                                                      c->b.keep_digit, sel, out_list, out_n, stopped);
         c->launches += 4;
     }
+}
+
+void select_prepare() {
+    cudaFuncSetAttribute(k_sel_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kSmemSegMax * kRadix * sizeof(unsigned int)));
 }
 
 }  // namespace dmolp

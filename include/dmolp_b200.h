@@ -80,10 +80,14 @@ typedef struct {                   /* one per LP iteration */
     int32_t boundary;              /* boundary candidates (before the per-label selection) */
     int32_t reserved;
     int64_t edge_cut;
-    uint64_t te_prev, te_cand, te_sel, te_stats;
+    uint64_t te_prev, te_cand, te_sel, te_stats;  /* traversed-edge terms of the reference's loop */
+    uint64_t arcs_read;            /* arcs this implementation actually read in the iteration */
 } dmolp_lp_record;
 
 const char *dmolp_last_error(void);
+
+/* The calling thread's current CUDA device (0 when none is set). */
+int dmolp_current_device(void);
 
 /* Create a context on CUDA device `device`.  Replaces the device set-up of allocateGPU
  * (src/main.cpp:25-121), which picks local_rank % device_count. */
@@ -105,6 +109,16 @@ int dmolp_graph_upload(dmolp_ctx *ctx, int64_t nv, int64_t narcs, const int64_t 
  * run_phase1 (src/phase1/phase1.cpp:83-153). */
 int dmolp_phase1(dmolp_ctx *ctx, int k, int theta, int32_t *seeds_out, int64_t *vertex_counts,
                  int64_t *edge_counts, dmolp_phase1_info *info);
+
+/* The two halves of phase 1, for callers that supply their own hubs / seeds.
+ * dmolp_find_seeds: up to k seeds by the reference rule -- the first seed, then repeatedly the first unused
+ * hub (in the given order) of maximum raw degree outside the radius-2 balls of the seeds so far; stops
+ * early when none is left, as find_seeds does (src/phase1/seed.cpp:192-242).  seeds_out needs k entries.
+ * dmolp_expand_partitions: theta-limited multi-source BFS growth from seeds[0..nseeds) (part p grows from
+ * seeds[p]; parts >= nseeds start empty), labels left on the device (src/phase1/partition.cpp:323-604). */
+int dmolp_find_seeds(dmolp_ctx *ctx, int k, int32_t first_seed, const int32_t *hubs, int64_t nhubs, int32_t *seeds_out,
+                     int32_t *nseeds);
+int dmolp_expand_partitions(dmolp_ctx *ctx, int k, int theta, const int32_t *seeds, int32_t nseeds, int32_t *rounds);
 
 /* Phase 2: boundary label propagation with balance penalties on the resident labels.
  * records[max_records] (may be NULL) receives one entry per iteration.
@@ -154,7 +168,8 @@ int dmolp_labels_restore(dmolp_ctx *ctx);
 
 /* Optional per-kernel timing: when enabled, dmolp_lp_run brackets its fused scan and statistics kernels with
  * CUDA events and accumulates their device time and algorithmic bytes (read with dmolp_kernel_profile).
- * kernel: 0 = boundary/decision scan, 1 = cut/balance statistics pass.  No reference counterpart. */
+ * kernel: 0 = boundary test, 1 = LP decisions, 2 = window marking, 3 = incremental cut/balance update.
+ * No reference counterpart. */
 int dmolp_set_profiling(dmolp_ctx *ctx, int enable);
 int dmolp_kernel_profile(dmolp_ctx *ctx, int kernel, double *total_ms, int64_t *launches, double *bytes);
 
