@@ -176,7 +176,8 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
     launches = p.kernel_launches() - launches0
     elapsed = e0.elapsed_time(e1) / 1e3
     prof = {}
-    for kid, name in ((0, "boundary_test"), (1, "lp_decide"), (2, "window_mark"), (3, "cut_update")):
+    for kid, name in ((0, "boundary_test"), (1, "lp_decide"), (2, "window_mark"), (3, "cut_update"),
+                      (4, "window_select")):
         import ctypes
 
         ms, n, by = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
@@ -185,7 +186,10 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
     p.lib.dmolp_set_profiling(p.ctx, 0)
     final_labels = p.labels()
 
-    rec_step = p.phase2(w["k"], mode="fixed", iterations=w["iters"], records=True) if args.records else None
+    rec_step = None
+    if args.records:
+        p._check(p.lib.dmolp_labels_restore(p.ctx))
+        rec_step = p.phase2(w["k"], mode="fixed", iterations=w["iters"], records=True)
     if rec_step is not None:
         for r in rec_step.records:
             print(json.dumps({f: getattr(r, f) for f, _ in r._fields_}), file=sys.stderr)

@@ -89,8 +89,10 @@ def build_dropin(force: bool = False) -> str:
     deps = srcs + [os.path.join(CSRC, "dropin_types.hpp"),
                    os.path.join(INCLUDE, "dmolp_b200.h"), os.path.join(LIB, "libdmolp_b200.so")]
     if force or _newer(out, deps):
-        _run([CXX, *HOST_FLAGS, "-fopenmp", "-shared", "-I", INCLUDE, "-I", CSRC, "-o", out, *srcs,
-              "-L", LIB, "-ldmolp_b200", "-Wl,-rpath,$ORIGIN"])
+        cuda_lib = os.path.join(CUDA_HOME, "lib64")
+        _run([CXX, *HOST_FLAGS, "-fopenmp", "-shared", "-I", INCLUDE, "-I", CSRC, "-I", os.path.join(CUDA_HOME, "include"),
+              "-o", out, *srcs, "-L", LIB, "-ldmolp_b200", "-L", cuda_lib, "-lcudart", "-Wl,-rpath,$ORIGIN",
+              "-Wl,-rpath," + cuda_lib])
     return out
 
 

@@ -28,7 +28,7 @@ struct LpCounters {
     int nchanged;     // selected vertices whose label changed (movers)
     int ndec[3];      // selected vertices per decision class
     int nchunk;       // queued row chunks of the marking kernel
-    int pad;
+    int npos;         // selection record slots: one per vertex with arcs (fixed per graph)
     unsigned long long cut_arcs;   // arcs whose endpoint labels differ (kept current incrementally)
 };
 
@@ -61,14 +61,16 @@ struct Buffers {
     int32_t *col = nullptr;    // [narcs]
     int32_t *rawdeg = nullptr; // [nv]
     int32_t *label = nullptr;  // [nv]
-    int32_t *bucket[3] = {nullptr, nullptr, nullptr};  // vertex ids of each degree class (deg >= 1), ascending
+    int32_t *ball = nullptr;   // vertex ids with arcs, by degree class then ascending id; position = record slot
+    int32_t *bucket[3] = {nullptr, nullptr, nullptr};  // the three classes inside ball
     // LP scratch
     int32_t *stamp = nullptr;  // [nv] iteration stamp of candidate marking
     int32_t *cand = nullptr;   // [nv] phase-1 claimed list / stand-alone window list
     int32_t *win[2] = {nullptr, nullptr};  // [nv] each: selected window of the iteration (by parity)
-    int32_t *bv = nullptr, *bown = nullptr, *bnew = nullptr;  // [nv] boundary records
-    uint64_t *bkey = nullptr;  // [nv]
-    uint8_t *bsel = nullptr;   // [nv]
+    int32_t *bv = nullptr, *bnew = nullptr;  // [nv] mover pairs of dmolp_lp_apply; phase-1 records
+    int32_t *bown = nullptr;   // [nv] record slot: own label of a boundary vertex, -1 otherwise
+    uint64_t *bkey = nullptr;  // [nv] record slot: selection key
+    uint8_t *bsel = nullptr;   // [nv] record slot: selected
     int32_t *dec[3] = {nullptr, nullptr, nullptr};  // [nv] each: selected vertices per decision class
     int32_t *newlab = nullptr; // [nv] new label of a mover in the current iteration, else -1
     int32_t *mov = nullptr;    // [nv] movers of the current iteration
@@ -141,7 +143,7 @@ struct dmolp_ctx {
     bool profiling = false;
     ProfEvents prof_pending;               // pairs to read after the run
     std::vector<char> prof_owned;          // per pending pair: destroy after reading (direct launches)
-    double prof_ms[4] = {0, 0, 0, 0};
-    long long prof_launches[4] = {0, 0, 0, 0};
-    double prof_bytes[4] = {0, 0, 0, 0};
+    double prof_ms[5] = {0, 0, 0, 0, 0};
+    long long prof_launches[5] = {0, 0, 0, 0, 0};
+    double prof_bytes[5] = {0, 0, 0, 0, 0};
 };

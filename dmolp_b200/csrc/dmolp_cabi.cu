@@ -353,10 +353,11 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     ALLOC(b.p1cnt, 8);
     ALLOC(b.p1te, 1);
     ALLOC(b.flag, 1);
-    for (int i = 0; i < 3; ++i) {
-        ALLOC(b.bucket[i], bl[i].size());
-        ALLOC(b.dec[i], n);
-    }
+    ALLOC(b.ball, bl[0].size() + bl[1].size() + bl[2].size());
+    b.bucket[0] = b.ball;
+    b.bucket[1] = b.ball + bl[0].size();
+    b.bucket[2] = b.bucket[1] + bl[1].size();
+    for (int i = 0; i < 3; ++i) ALLOC(b.dec[i], n);
     ALLOC(b.newlab, n);
     ALLOC(b.mov, n);
     ALLOC(b.chunkq, (size_t)c->chunk_cap);
@@ -375,6 +376,9 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
         if (!bl[i].empty())
             DMOLP_CUDA(cudaMemcpyAsync(b.bucket[i], bl[i].data(), bl[i].size() * sizeof(int32_t),
                                        cudaMemcpyHostToDevice, c->stream));
+    const int npos = c->nb[0] + c->nb[1] + c->nb[2];
+    DMOLP_CUDA(cudaMemcpyAsync(&b.cnt->npos, &npos, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.bown, 0xff, n * sizeof(int32_t), c->stream));  // all record slots empty
     lp_fill(c, b.newlab, (int64_t)n, -1);
     select_prepare();
     // every arc has its reverse (checked on the device): the LP loop may update its statistics from the
@@ -453,7 +457,7 @@ int dmolp_labels_restore(dmolp_ctx *c) {
 int dmolp_set_profiling(dmolp_ctx *c, int enable) {
     if (!c) return fail(DMOLP_ERR_ARG, "null context");
     c->profiling = enable != 0;
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < 5; ++i) {
         c->prof_ms[i] = 0;
         c->prof_launches[i] = 0;
         c->prof_bytes[i] = 0;
@@ -462,7 +466,7 @@ int dmolp_set_profiling(dmolp_ctx *c, int enable) {
 }
 
 int dmolp_kernel_profile(dmolp_ctx *c, int kernel, double *total_ms, int64_t *launches, double *bytes) {
-    if (!c || kernel < 0 || kernel > 3) return fail(DMOLP_ERR_ARG, "bad context or kernel id");
+    if (!c || kernel < 0 || kernel > 4) return fail(DMOLP_ERR_ARG, "bad context or kernel id");
     if (total_ms) *total_ms = c->prof_ms[kernel];
     if (launches) *launches = c->prof_launches[kernel];
     if (bytes) *bytes = c->prof_bytes[kernel];
@@ -774,6 +778,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
         //  decide : list id + offsets + own label per selected vertex, id + label per arc, 8 B per mover
         //  mark   : list id + offsets per window vertex, id read + stamp write per arc
         //  update : offsets + labels per mover, id + label + pending label per arc
+        //  select : label + key of every record slot, read by the first histogram and partition pass
         const double nbk = (double)c->nb[0] + c->nb[1] + c->nb[2];
         dmolp_ctx::ProfEvents &pe = c->prof_pending;
         for (size_t i = 0; i < pe.kind.size(); ++i) {
@@ -783,10 +788,12 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
                 const LpRecordDev &d = recs[t - 1];
                 const double ncand = t == 1 ? nbk : (double)d.candidates;
                 double bytes = 0;
-                if (kind == 0) bytes = 4.0 * nbk * (t > 1 ? 2 : 1) + 20.0 * ncand + 8.0 * (double)d.arcs_bnd + 21.0 * d.boundary;
+                if (kind == 0)
+                bytes = (t > 1 ? 8.0 : 4.0) * nbk + 5.0 * nbk + 20.0 * ncand + 8.0 * (double)d.arcs_bnd + 8.0 * d.boundary;
                 else if (kind == 1) bytes = 24.0 * d.window + 8.0 * (double)d.arcs_dec + 8.0 * d.changes;
                 else if (kind == 2) bytes = (t > 1 ? 20.0 * recs[t - 2].window : 0.0) + 8.0 * (double)d.te_prev;
-                else bytes = 28.0 * d.changes + 12.0 * (double)d.arcs_upd;
+                else if (kind == 3) bytes = 28.0 * d.changes + 12.0 * (double)d.arcs_upd;
+            else bytes = 24.0 * nbk + (double)d.window;  // select: first digit pass over every record slot
                 c->prof_ms[kind] += ems;
                 c->prof_launches[kind] += 1;
                 c->prof_bytes[kind] += bytes;

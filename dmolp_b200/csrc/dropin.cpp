@@ -4,7 +4,8 @@
 // partitioning path on the B200 kernels.
 //
 // Scope: one process, one GPU (mpi_size must be 1; there are then no ghost vertices).  The device is the
-// one current when a context is first needed (the reference's allocateGPU sets it before phase 2).
+// caller's current one when a context is first needed (the reference's allocateGPU sets it before phase 2),
+// read through the shared CUDA runtime.
 // Environment knobs (not in the reference): DMOLP_LP_ITERATIONS=N runs exactly N LP iterations instead of
 // the reference's stopping rules; DMOLP_LP_LABEL_CAP=full scores every label < k instead of min(k,32).
 //
@@ -25,6 +26,8 @@
 #include <utility>
 #include <vector>
 
+#include <cuda_runtime_api.h>
+
 #include "dmolp_b200.h"
 #include "dropin_types.hpp"
 
@@ -40,6 +43,16 @@ void check(int rc, const char *what) {
     if (rc != DMOLP_OK) throw std::runtime_error(std::string(what) + ": " + dmolp_last_error());
 }
 
+// The caller's current device, read through the shared CUDA runtime its own code (allocateGPU) uses.
+int caller_device() {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) {
+        cudaGetLastError();
+        d = 0;
+    }
+    return d;
+}
+
 void require_single_rank(int mpi_size, const char *fn) {
     if (mpi_size != 1)
         throw std::runtime_error(std::string(fn) + ": this build runs one process on one GPU (mpi_size must be 1)");
@@ -53,7 +66,7 @@ struct Resident {
     int64_t nv = 0;
 
     void ensure_ctx() {
-        if (!ctx) check(dmolp_create(dmolp_current_device(), &ctx), "dmolp_create");
+        if (!ctx) check(dmolp_create(caller_device(), &ctx), "dmolp_create");
     }
     void upload(const std::vector<int64_t> &off, const std::vector<int> &col, const std::vector<int> *raw) {
         ensure_ctx();

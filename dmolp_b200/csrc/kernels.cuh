@@ -6,8 +6,8 @@
 namespace dmolp {
 
 // ---- segmented radix select (select_kernels.cu) ----
-// Records i < *n_dev carry a segment seg[i] in [0,nseg) and a 64-bit key whose top bit is below
-// `keybits`; keys are unique.  For every segment p, marks sel[i] = 1 on the need[p] records with the
+// Records i < *n_dev carry a segment seg[i] in [0,nseg) (or -1: an empty slot, ignored) and a 64-bit key
+// whose top bit is below `keybits`; keys are unique.  For every segment p, marks sel[i] = 1 on the need[p] records with the
 // smallest keys (need[] is consumed).  sel[] must be zero on entry.  `stopped` (may be null) turns the
 // launches into no-ops once it is non-zero.
 void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, const int *n_dev, int nseg, int keybits,

@@ -138,6 +138,11 @@ __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
 }
 
 // ------------------------------------------------------------------------------------ mark
+// Hubs sit in many rows: reading the stamp first saves most of the (L2) stores.
+__device__ __forceinline__ void stamp_once(const Buffers &b, int u, int t) {
+    if (b.stamp[u] != t) b.stamp[u] = t;
+}
+
 // Warp per vertex of the previous window: stamp it and its first kChunk neighbours; the rest of a long row
 // is queued in kChunk pieces for k_mark_chunks.
 __global__ void k_mark(Buffers b, int t) {
@@ -159,7 +164,7 @@ __global__ void k_mark(Buffers b, int t) {
             }
         }
         const int64_t e1 = e - s > kChunk ? s + kChunk : e;
-        warp_row(b.col, s, e1, lane, [&](int u) { b.stamp[u] = t; }, [] { return false; });
+        warp_row(b.col, s, e1, lane, [&](int u) { stamp_once(b, u, t); }, [] { return false; });
     }
     te = warp_sum_u64(te);
     if (lane == 0 && te) atomicAdd(&b.rec[t - 1].te_prev, te);
@@ -174,7 +179,7 @@ __global__ void k_mark_chunks(Buffers b, int t) {
         const int2 q = b.chunkq[i];
         const int64_t s = b.off[q.x] + q.y, rowe = b.off[q.x + 1];
         const int64_t e = rowe - s > kChunk ? s + kChunk : rowe;
-        warp_row(b.col, s, e, lane, [&](int u) { b.stamp[u] = t; }, [] { return false; });
+        warp_row(b.col, s, e, lane, [&](int u) { stamp_once(b, u, t); }, [] { return false; });
     }
 }
 
@@ -190,97 +195,118 @@ __device__ __forceinline__ uint64_t sel_key(const Buffers &b, int own, int deg, 
     return (dk << ibits) | (uint64_t)v;
 }
 
-__device__ __forceinline__ void put_record(const Buffers &b, int idx, int v, int own, uint64_t key) {
-    b.bv[idx] = v;
-    b.bown[idx] = own;
-    b.bkey[idx] = key;
-    b.bsel[idx] = 0;
-    atomicAdd(&b.npart[own], 1);
+// Record slot pos (the vertex's position in ball): own label and key of a boundary vertex, -1 otherwise.
+// No global append: every slot is rewritten each iteration.
+__device__ __forceinline__ void put_slot(const Buffers &b, int pos, bool isb, int own, uint64_t key) {
+    b.bown[pos] = isb ? own : -1;
+    if (isb) b.bkey[pos] = key;
+    b.bsel[pos] = 0;
 }
 
-__global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a) {
+__global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
     if (b.ctrl->stopped) return;
+    extern __shared__ int s_npart[];  // [k] boundary records per label in this block
+    for (int p = threadIdx.x; p < k; p += blockDim.x) s_npart[p] = 0;
+    __syncthreads();
     const int lane = threadIdx.x & 31;
-    unsigned long long te = 0, rd = 0, nc = 0;
+    unsigned long long te = 0, rd = 0, nc = 0, nbd = 0;
     if ((int)blockIdx.x < a.g0) {
         // ---- thread per vertex (deg <= kSmallDeg) ----
-        const int n = a.nb0;
-        for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += a.g0 * blockDim.x) {
-            const int i = i0 + threadIdx.x;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
+            const int v = b.bucket[0][i];
             bool isb = false;
-            int v = 0, own = 0, deg = 0;
-            if (i < n) {
-                v = b.bucket[0][i];
-                if (a.all || b.stamp[v] == a.t) {
-                    own = b.label[v];
-                    const int64_t s = b.off[v];
-                    deg = (int)(b.off[v + 1] - s);
-                    ++nc;
-                    te += deg;
-                    int j = 0;
-                    for (; j < deg; ++j)
-                        if (b.label[__ldg(b.col + s + j)] != own) {
-                            isb = true;
-                            ++j;
-                            break;
-                        }
-                    rd += j;
-                }
+            int own = 0, deg = 0;
+            if (a.all || b.stamp[v] == a.t) {
+                own = b.label[v];
+                const int64_t s = b.off[v];
+                deg = (int)(b.off[v + 1] - s);
+                ++nc;
+                te += deg;
+                int j = 0;
+                for (; j < deg; ++j)
+                    if (b.label[__ldg(b.col + s + j)] != own) {
+                        isb = true;
+                        ++j;
+                        break;
+                    }
+                rd += j;
             }
-            const int slot = warp_append(&b.cnt->nbnd, isb);
-            if (isb) put_record(b, slot, v, own, sel_key(b, own, deg, v, a.ibits, a.maxdeg));
+            if (isb) {
+                ++nbd;
+                atomicAdd(&s_npart[own], 1);
+            }
+            put_slot(b, i, isb, own, isb ? sel_key(b, own, deg, v, a.ibits, a.maxdeg) : 0);
         }
     } else if ((int)blockIdx.x < a.g0 + a.g1) {
         // ---- warp per vertex ----
         const int wpb = blockDim.x >> 5;
         const int gw = ((int)blockIdx.x - a.g0) * wpb + (threadIdx.x >> 5), nw = a.g1 * wpb;
         for (int i = gw; i < a.nb1; i += nw) {
+            const int pos = a.nb0 + i;
             const int v = b.bucket[1][i];
-            if (!a.all && b.stamp[v] != a.t) continue;
-            const int own = b.label[v];
-            const int64_t s = b.off[v], e = b.off[v + 1];
-            bool diff = false;
-            const int64_t r = warp_row(b.col, s, e, lane, [&](int u) { diff |= (b.label[u] != own); },
-                                       [&] { return __any_sync(DMOLP_FULL_MASK, diff); });
-            if (lane == 0) {
-                ++nc;
-                te += (unsigned long long)(e - s);
-                rd += (unsigned long long)r;
+            bool isb = false;
+            int own = 0;
+            int64_t s = 0, e = 0;
+            if (a.all || b.stamp[v] == a.t) {
+                own = b.label[v];
+                s = b.off[v];
+                e = b.off[v + 1];
+                bool diff = false;
+                const int64_t r = warp_row(b.col, s, e, lane, [&](int u) { diff |= (b.label[u] != own); },
+                                           [&] { return __any_sync(DMOLP_FULL_MASK, diff); });
+                isb = __any_sync(DMOLP_FULL_MASK, diff);
+                if (lane == 0) {
+                    ++nc;
+                    te += (unsigned long long)(e - s);
+                    rd += (unsigned long long)r;
+                }
             }
-            if (__any_sync(DMOLP_FULL_MASK, diff) && lane == 0) {
-                const int idx = atomicAdd(&b.cnt->nbnd, 1);
-                put_record(b, idx, v, own, sel_key(b, own, (int)(e - s), v, a.ibits, a.maxdeg));
+            if (lane == 0) {
+                if (isb) {
+                    ++nbd;
+                    atomicAdd(&s_npart[own], 1);
+                }
+                put_slot(b, pos, isb, own, isb ? sel_key(b, own, (int)(e - s), v, a.ibits, a.maxdeg) : 0);
             }
         }
     } else {
         // ---- block per vertex (deg > kLargeDeg) ----
         const int gb = (int)blockIdx.x - a.g0 - a.g1, nbk = (int)gridDim.x - a.g0 - a.g1;
         for (int i = gb; i < a.nb2; i += nbk) {
+            const int pos = a.nb0 + a.nb1 + i;
             const int v = b.bucket[2][i];
-            if (!a.all && b.stamp[v] != a.t) continue;
-            const int own = b.label[v];
-            const int64_t s = b.off[v], e = b.off[v + 1];
-            bool diff = false;
-            int64_t j0 = s;
-            for (; j0 < e; j0 += blockDim.x * 4) {
-                for (int q = 0; q < 4; ++q) {
-                    const int64_t j = j0 + q * blockDim.x + threadIdx.x;
-                    if (j < e) diff |= (b.label[__ldcs(b.col + j)] != own);
+            const bool cand = a.all || b.stamp[v] == a.t;
+            bool isb = false;
+            int own = 0;
+            int64_t s = 0, e = 0, j0 = 0;
+            if (cand) {  // block-uniform
+                own = b.label[v];
+                s = b.off[v];
+                e = b.off[v + 1];
+                bool diff = false;
+                for (j0 = s; j0 < e; j0 += blockDim.x * 4) {
+                    for (int q = 0; q < 4; ++q) {
+                        const int64_t j = j0 + q * blockDim.x + threadIdx.x;
+                        if (j < e) diff |= (b.label[__ldcs(b.col + j)] != own);
+                    }
+                    if (__syncthreads_or(diff)) {
+                        j0 += blockDim.x * 4;
+                        break;
+                    }
                 }
-                if (__syncthreads_or(diff)) {
-                    j0 += blockDim.x * 4;
-                    break;
-                }
+                isb = __syncthreads_or(diff);
             }
-            const bool isb = __syncthreads_or(diff);
             if (threadIdx.x == 0) {
-                ++nc;
-                te += (unsigned long long)(e - s);
-                rd += (unsigned long long)((j0 < e ? j0 : e) - s);
-                if (isb) {
-                    const int idx = atomicAdd(&b.cnt->nbnd, 1);
-                    put_record(b, idx, v, own, sel_key(b, own, (int)(e - s), v, a.ibits, a.maxdeg));
+                if (cand) {
+                    ++nc;
+                    te += (unsigned long long)(e - s);
+                    rd += (unsigned long long)((j0 < e ? j0 : e) - s);
                 }
+                if (isb) {
+                    ++nbd;
+                    atomicAdd(&s_npart[own], 1);
+                }
+                put_slot(b, pos, isb, own, isb ? sel_key(b, own, (int)(e - s), v, a.ibits, a.maxdeg) : 0);
             }
             __syncthreads();
         }
@@ -288,11 +314,16 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a) {
     te = warp_sum_u64(te);
     rd = warp_sum_u64(rd);
     nc = warp_sum_u64(nc);
+    nbd = warp_sum_u64(nbd);
     if (lane == 0) {
         if (te) atomicAdd(&b.rec[a.t - 1].te_cand, te);
         if (rd) atomicAdd(&b.rec[a.t - 1].arcs_bnd, rd);
         if (nc) atomicAdd(&b.cnt->ncand, (int)nc);
+        if (nbd) atomicAdd(&b.cnt->nbnd, (int)nbd);
     }
+    __syncthreads();
+    for (int p = threadIdx.x; p < k; p += blockDim.x)
+        if (s_npart[p]) atomicAdd(&b.npart[p], s_npart[p]);
 }
 
 // ------------------------------------------------------------------------------------ need
@@ -308,11 +339,29 @@ __global__ void k_lp_need(Buffers b, int k, int t) {
 }
 
 // ------------------------------------------------------------------------------------ split
-// Selected records: next window (for marking) and decision class.  A vertex whose own label is not scored
-// (>= eff) goes to the warp class, whose histogram also sees absent labels.
-__global__ void k_split(Buffers b, int t, int eff) {
+// Append under a predicate with one global atomic per block: every thread of the block must call it with
+// the same trip count.  s_tmp: two shared ints.
+__device__ __forceinline__ int block_append(int *gctr, bool pred, int *s_tmp) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_tmp[0] = 0;
+    __syncthreads();
+    const unsigned m = __ballot_sync(DMOLP_FULL_MASK, pred);
+    const int lane = threadIdx.x & 31;
+    int wb = 0;
+    if (lane == 0 && m) wb = atomicAdd(&s_tmp[0], __popc(m));
+    wb = __shfl_sync(DMOLP_FULL_MASK, wb, 0);
+    __syncthreads();
+    if (threadIdx.x == 0) s_tmp[1] = s_tmp[0] ? atomicAdd(gctr, s_tmp[0]) : 0;
+    __syncthreads();
+    return pred ? s_tmp[1] + wb + __popc(m & ((1u << lane) - 1)) : -1;
+}
+
+// Selected record slots: next window (for marking) and decision class.  A vertex whose own label is not
+// scored (>= eff) goes to the warp class, whose histogram also sees absent labels.
+__global__ void __launch_bounds__(256) k_split(Buffers b, int t, int eff) {
     if (b.ctrl->stopped) return;
-    const int n = b.cnt->nbnd;
+    __shared__ int s_tmp[2];
+    const int n = b.cnt->npos;
     int32_t *win = b.win[t & 1];
     unsigned long long te = 0;
     for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
@@ -320,15 +369,15 @@ __global__ void k_split(Buffers b, int t, int eff) {
         const bool take = i < n && b.bsel[i];
         int v = 0, cls = -1;
         if (take) {
-            v = b.bv[i];
+            v = b.ball[i];
             const int deg = (int)(b.off[v + 1] - b.off[v]);
             te += (unsigned long long)deg;
             cls = deg > kLargeDeg ? 2 : ((deg > kSmallDeg || b.bown[i] >= eff) ? 1 : 0);
         }
-        const int slot = warp_append(&b.cnt->nwin[t & 1], take);
+        const int slot = block_append(&b.cnt->nwin[t & 1], take, s_tmp);
         if (take) win[slot] = v;
         for (int c = 0; c < 3; ++c) {
-            const int s2 = warp_append(&b.cnt->ndec[c], cls == c);
+            const int s2 = block_append(&b.cnt->ndec[c], cls == c, s_tmp);
             if (cls == c) b.dec[c][s2] = v;
         }
     }
@@ -348,11 +397,75 @@ __device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
     b.mov[q] = v;
 }
 
+// Lane-private label counters of one warp for labels < 32: lane L counts label c in
+// h[c*32 + ((L + c) & 31)].  Increments need no atomics and hit distinct banks for lanes sharing a label;
+// the sum over row c (lane c, rotated start) is bank-conflict free as well.
+__device__ __forceinline__ void priv_zero(int *h, int eff, int lane) {
+    for (int c = 0; c < eff; ++c) h[c * 32 + ((lane + c) & 31)] = 0;
+}
+__device__ __forceinline__ int priv_total(const int *h, int eff, int lane) {
+    int t = 0;
+    if (lane < eff)
+        for (int j = 0; j < 32; ++j) t += h[lane * 32 + ((j + lane) & 31)];
+    return t;
+}
+
+// Count labels < eff of the arcs [s, e) into the calling warp's histogram: lane-private counters (eff <= 32,
+// h has 32*32 ints) or a shared histogram h[eff] with one atomic per group of equal labels (__match_any).
+__device__ __forceinline__ int64_t warp_count(const Buffers &b, int64_t s, int64_t e, int lane, int eff, int *h) {
+    if (eff <= 32) {
+        return warp_row(b.col, s, e, lane, [&](int u) {
+            const int lu = b.label[u];
+            if ((unsigned)lu < (unsigned)eff) h[lu * 32 + ((lane + lu) & 31)] += 1;
+        }, [] { return false; });
+    }
+    for (int64_t j0 = s; j0 < e; j0 += 32) {
+        const int64_t j = j0 + lane;
+        const int lu = j < e ? b.label[__ldcs(b.col + j)] : -1;
+        const bool ok = (unsigned)lu < (unsigned)eff;
+        const unsigned m = __match_any_sync(DMOLP_FULL_MASK, ok ? lu : -(lane + 1));
+        if (ok && lane == __ffs(m) - 1) atomicAdd(&h[lu], __popc(m));
+    }
+    return e - s;
+}
+
+// Warp argmax over labels < eff given per-label counts: lanes hold the counts of labels lane, lane+32, ...
+// through cnt_of(c).  Returns (best score, best label) in every lane; (score desc, tie key asc).
+template <typename C>
+__device__ __forceinline__ void warp_argmax(int eff, const double *tpen, int lane, C cnt_of, double &best,
+                                            int &blab) {
+    best = -DBL_MAX;
+    int bkey = 0x7fffffff;
+    blab = -1;
+    for (int c = lane; c < eff; c += 32) {
+        const int cnt = cnt_of(c);
+        const double sc = cnt > 0 ? __dmul_rn((double)cnt, tpen[c]) : 0.0;
+        const int key = tiekey(c);
+        if (better(sc, key, best, bkey)) {
+            best = sc;
+            bkey = key;
+            blab = c;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(DMOLP_FULL_MASK, best, o);
+        const int ok = __shfl_xor_sync(DMOLP_FULL_MASK, bkey, o);
+        const int ol = __shfl_xor_sync(DMOLP_FULL_MASK, blab, o);
+        if (better(ob, ok, best, bkey)) {
+            best = ob;
+            bkey = ok;
+            blab = ol;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
     if (b.ctrl->stopped) return;
-    extern __shared__ int shist[];
+    extern __shared__ int shist[];  // eff <= 32: 8 warps x 32x32 private counters + 8x32 totals; else 8 x eff
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int eff = a.eff;
+    const bool priv = eff <= 32;
+    int *h = shist + wib * (priv ? 1024 : eff);
     unsigned long long rd = 0;
     if ((int)blockIdx.x < a.g0) {
         // ---- thread per vertex: deg <= 16 and own label < eff; only present labels can beat the own raw
@@ -390,8 +503,7 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
             if (blab >= 0 && best > (double)own_cnt && blab != own) park_move(b, v, blab);
         }
     } else if ((int)blockIdx.x < a.g0 + a.g1) {
-        // ---- warp per vertex: shared histogram of the scored labels ----
-        int *h = shist + wib * eff;
+        // ---- warp per vertex ----
         const int wpb = blockDim.x >> 5;
         const int gw = ((int)blockIdx.x - a.g0) * wpb + wib, nw = a.g1 * wpb;
         const int n = b.cnt->ndec[1];
@@ -399,99 +511,68 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
             const int v = b.dec[1][i];
             const int own = b.label[v];
             const int64_t s = b.off[v], e = b.off[v + 1];
-            for (int c = lane; c < eff; c += 32) h[c] = 0;
+            if (priv) priv_zero(h, eff, lane);
+            else
+                for (int c = lane; c < eff; c += 32) h[c] = 0;
             __syncwarp();
-            warp_row(b.col, s, e, lane, [&](int u) {
-                const int lu = b.label[u];
-                if ((unsigned)lu < (unsigned)eff) atomicAdd(&h[lu], 1);
-            }, [] { return false; });
+            warp_count(b, s, e, lane, eff, h);
             __syncwarp();
-            double best = -DBL_MAX;
-            int bkey = 0x7fffffff, blab = -1;
-            for (int c = lane; c < eff; c += 32) {
-                const int cnt = h[c];
-                const double sc = cnt > 0 ? __dmul_rn((double)cnt, b.tpen[c]) : 0.0;
-                const int key = tiekey(c);
-                if (better(sc, key, best, bkey)) {
-                    best = sc;
-                    bkey = key;
-                    blab = c;
-                }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ob = __shfl_xor_sync(DMOLP_FULL_MASK, best, o);
-                const int ok = __shfl_xor_sync(DMOLP_FULL_MASK, bkey, o);
-                const int ol = __shfl_xor_sync(DMOLP_FULL_MASK, blab, o);
-                if (better(ob, ok, best, bkey)) {
-                    best = ob;
-                    bkey = ok;
-                    blab = ol;
-                }
+            double best;
+            int blab, own_cnt;
+            if (priv) {
+                const int cnt = priv_total(h, eff, lane);
+                warp_argmax(eff, b.tpen, lane, [&](int) { return cnt; }, best, blab);
+                own_cnt = __shfl_sync(DMOLP_FULL_MASK, cnt, own & 31);
+            } else {
+                warp_argmax(eff, b.tpen, lane, [&](int c) { return h[c]; }, best, blab);
+                own_cnt = (unsigned)own < (unsigned)eff ? h[own] : 0;
             }
             if (lane == 0) {
                 rd += (unsigned long long)(e - s);
-                const double own_raw = (unsigned)own < (unsigned)eff ? (double)h[own] : -1e300;
+                const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
                 const int nl = best > own_raw ? blab : own;
                 if (nl != own) park_move(b, v, nl);
             }
             __syncwarp();
         }
     } else {
-        // ---- block per vertex: one shared histogram per block ----
-        __shared__ double s_best[kWarpsPerBlock];
-        __shared__ int s_key[kWarpsPerBlock], s_lab[kWarpsPerBlock];
+        // ---- block per vertex (deg > kLargeDeg): each warp counts one contiguous eighth of the row ----
+        int *tot = shist + kWarpsPerBlock * 1024;  // [8][32] per-warp totals (eff <= 32)
         const int gb = (int)blockIdx.x - a.g0 - a.g1, nbk = (int)gridDim.x - a.g0 - a.g1;
         const int n = b.cnt->ndec[2];
         for (int i = gb; i < n; i += nbk) {
             const int v = b.dec[2][i];
             const int own = b.label[v];
             const int64_t s = b.off[v], e = b.off[v + 1];
-            for (int c = threadIdx.x; c < eff; c += blockDim.x) shist[c] = 0;
+            if (priv) priv_zero(h, eff, lane);
+            else
+                for (int c = threadIdx.x; c < eff; c += blockDim.x) shist[c] = 0;
             __syncthreads();
-            for (int64_t j = s + threadIdx.x; j < e; j += blockDim.x) {
-                const int lu = b.label[__ldcs(b.col + j)];
-                if ((unsigned)lu < (unsigned)eff) atomicAdd(&shist[lu], 1);
-            }
+            const int64_t len = e - s, per = ((len + kWarpsPerBlock - 1) / kWarpsPerBlock + 3) & ~int64_t(3);
+            const int64_t ws = s + wib * per < e ? s + wib * per : e;
+            const int64_t we = ws + per < e ? ws + per : e;
+            warp_count(b, ws, we, lane, eff, priv ? h : shist);
+            __syncwarp();
+            if (priv) tot[wib * 32 + lane] = priv_total(h, eff, lane);
             __syncthreads();
-            double best = -DBL_MAX;
-            int bkey = 0x7fffffff, blab = -1;
-            for (int c = threadIdx.x; c < eff; c += blockDim.x) {
-                const int cnt = shist[c];
-                const double sc = cnt > 0 ? __dmul_rn((double)cnt, b.tpen[c]) : 0.0;
-                const int key = tiekey(c);
-                if (better(sc, key, best, bkey)) {
-                    best = sc;
-                    bkey = key;
-                    blab = c;
+            if (wib == 0) {
+                double best;
+                int blab, own_cnt;
+                if (priv) {
+                    int cnt = 0;
+                    for (int w = 0; w < kWarpsPerBlock; ++w) cnt += tot[w * 32 + lane];
+                    warp_argmax(eff, b.tpen, lane, [&](int) { return cnt; }, best, blab);
+                    own_cnt = __shfl_sync(DMOLP_FULL_MASK, cnt, own & 31);
+                } else {
+                    warp_argmax(eff, b.tpen, lane, [&](int c) { return shist[c]; }, best, blab);
+                    own_cnt = (unsigned)own < (unsigned)eff ? shist[own] : 0;
                 }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ob = __shfl_xor_sync(DMOLP_FULL_MASK, best, o);
-                const int ok = __shfl_xor_sync(DMOLP_FULL_MASK, bkey, o);
-                const int ol = __shfl_xor_sync(DMOLP_FULL_MASK, blab, o);
-                if (better(ob, ok, best, bkey)) {
-                    best = ob;
-                    bkey = ok;
-                    blab = ol;
+                if (lane == 0) {
+                    rd += (unsigned long long)(e - s);
+                    const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
+                    const int nl = best > own_raw ? blab : own;
+                    if (nl != own) park_move(b, v, nl);
                 }
-            }
-            if (lane == 0) {
-                s_best[wib] = best;
-                s_key[wib] = bkey;
-                s_lab[wib] = blab;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                for (int w = 1; w < kWarpsPerBlock; ++w)
-                    if (better(s_best[w], s_key[w], best, bkey)) {
-                        best = s_best[w];
-                        bkey = s_key[w];
-                        blab = s_lab[w];
-                    }
-                rd += (unsigned long long)(e - s);
-                const double own_raw = (unsigned)own < (unsigned)eff ? (double)shist[own] : -1e300;
-                const int nl = best > own_raw ? blab : own;
-                if (nl != own) park_move(b, v, nl);
             }
             __syncthreads();
         }
@@ -863,7 +944,10 @@ DecArgs dec_args(dmolp_ctx *c, int t, int eff) {
 
 int dec_grid(dmolp_ctx *c, const DecArgs &a) { return a.g0 + a.g1 + c->num_sms; }
 
-size_t dec_smem(int eff) { return (size_t)kWarpsPerBlock * eff * sizeof(int); }
+size_t dec_smem(int eff) {
+    return eff <= 32 ? (size_t)(kWarpsPerBlock * 1024 + kWarpsPerBlock * 32) * sizeof(int)
+                     : (size_t)kWarpsPerBlock * eff * sizeof(int);
+}
 
 StatsArgs stats_args(dmolp_ctx *c, int k) {
     StatsArgs a;
@@ -951,11 +1035,14 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     {
         ProfScope ps(c, 0, t);
         const BndArgs a = bnd_args(c, t, t == 1);
-        k_bnd<<<bnd_grid(c, a), kBlock, 0, c->stream>>>(b, a);
+        k_bnd<<<bnd_grid(c, a), kBlock, L.k * sizeof(int), c->stream>>>(b, a, L.k);
     }
     k_lp_need<<<1, 256, 0, c->stream>>>(b, L.k, t);
     c->launches += 2;
-    select_smallest(c, b.bown, b.bkey, &b.cnt->nbnd, L.k, c->dbits + c->ibits, b.bsel, stopped);
+    {
+        ProfScope ps(c, 4, t);
+        select_smallest(c, b.bown, b.bkey, &b.cnt->npos, L.k, c->dbits + c->ibits, b.bsel, stopped);
+    }
     k_split<<<grid, kBlock, 0, c->stream>>>(b, t, L.eff);
     {
         ProfScope ps(c, 1, t);
@@ -991,10 +1078,10 @@ void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int n
     k_mark<<<grid, kBlock, 0, c->stream>>>(b, t);
     k_mark_chunks<<<grid, kBlock, 0, c->stream>>>(b, t);
     const BndArgs a = bnd_args(c, t, 0);
-    k_bnd<<<bnd_grid(c, a), kBlock, 0, c->stream>>>(b, a);
+    k_bnd<<<bnd_grid(c, a), kBlock, k * sizeof(int), c->stream>>>(b, a, k);
     k_lp_need<<<1, 256, 0, c->stream>>>(b, k, t);
     c->launches += 5;
-    select_smallest(c, b.bown, b.bkey, &b.cnt->nbnd, k, c->dbits + c->ibits, b.bsel, nullptr);
+    select_smallest(c, b.bown, b.bkey, &b.cnt->npos, k, c->dbits + c->ibits, b.bsel, nullptr);
     k_split<<<grid, kBlock, 0, c->stream>>>(b, t, DMOLP_MAX_K);
     c->launches += 1;
 }

@@ -29,6 +29,7 @@ __global__ void k_sel_hist(const int32_t *__restrict__ seg, const uint64_t *__re
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int r = list ? list[i] : i;
         const int p = seg[r];
+        if (p < 0) continue;  // empty record slot
         const int d = (int)((key[r] >> shift) & (kRadix - 1));
         if (use_smem) atomicAdd(&shist[p * kRadix + d], 1u);
         else atomicAdd(&ghist[p * kRadix + d], 1u);
@@ -111,9 +112,11 @@ __global__ void k_sel_partition(const int32_t *__restrict__ seg, const uint64_t 
         if (i < n) {
             r = list ? list[i] : i;
             const int p = seg[r];
-            const int d = (int)((key[r] >> shift) & (kRadix - 1));
-            if (d < sel_below[p]) sel[r] = 1;
-            else keep = (d == keep_digit[p]);
+            if (p >= 0) {  // skip empty record slots
+                const int d = (int)((key[r] >> shift) & (kRadix - 1));
+                if (d < sel_below[p]) sel[r] = 1;
+                else keep = (d == keep_digit[p]);
+            }
         }
         const int slot = warp_append(nout, keep);
         if (keep) out[slot] = r;

@@ -168,7 +168,8 @@ int dmolp_labels_restore(dmolp_ctx *ctx);
 
 /* Optional per-kernel timing: when enabled, dmolp_lp_run brackets its fused scan and statistics kernels with
  * CUDA events and accumulates their device time and algorithmic bytes (read with dmolp_kernel_profile).
- * kernel: 0 = boundary test, 1 = LP decisions, 2 = window marking, 3 = incremental cut/balance update.
+ * kernel: 0 = boundary test, 1 = LP decisions, 2 = window marking, 3 = incremental cut/balance update,
+ * 4 = per-label window selection (all radix-select launches of an iteration).
  * No reference counterpart. */
 int dmolp_set_profiling(dmolp_ctx *ctx, int enable);
 int dmolp_kernel_profile(dmolp_ctx *ctx, int kernel, double *total_ms, int64_t *launches, double *bytes);
