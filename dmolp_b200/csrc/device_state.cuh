@@ -43,6 +43,10 @@ struct LpControl {
     int stop_reason;
     int error;          // 1 = odd cut-arc count or invalid label (the reference aborts)
     int mode;           // DMOLP_LP_MODE_*
+    int pull;           // next iteration finds candidates by pulling (rows scanned for a window member)
+    int sel_done;       // radix select: blocks finished the current histogram
+    int sel_open;       // radix select: segments still needing records
+    int sel_pass;       // radix select: the pass whose digit decisions are current
 };
 
 // One LP iteration record as kept on the device.
@@ -64,7 +68,8 @@ struct Buffers {
     int32_t *ball = nullptr;   // vertex ids with arcs, by degree class then ascending id; position = record slot
     int32_t *bucket[3] = {nullptr, nullptr, nullptr};  // the three classes inside ball
     // LP scratch
-    int32_t *stamp = nullptr;  // [nv] iteration stamp of candidate marking
+    int32_t *stamp = nullptr;  // [nv] iteration stamp of candidate marking (push)
+    int32_t *sstamp = nullptr; // [nv] iteration stamp of the selected window (pull)
     int32_t *cand = nullptr;   // [nv] phase-1 claimed list / stand-alone window list
     int32_t *win[2] = {nullptr, nullptr};  // [nv] each: selected window of the iteration (by parity)
     int32_t *bv = nullptr, *bnew = nullptr;  // [nv] mover pairs of dmolp_lp_apply; phase-1 records

@@ -319,6 +319,7 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     ALLOC(b.rawdeg, n);
     ALLOC(b.label, n);
     ALLOC(b.stamp, n);
+    ALLOC(b.sstamp, n);
     ALLOC(b.cand, n);
     ALLOC(b.win[0], n);
     ALLOC(b.win[1], n);
@@ -729,6 +730,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
 
     DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.stamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.sstamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
     lp_reset_stats(c, k, nullptr);
     lp_stats(c, k, nullptr, nullptr);
     lp_init_end(c, cfg->mode);

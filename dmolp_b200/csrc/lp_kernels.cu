@@ -146,7 +146,7 @@ __device__ __forceinline__ void stamp_once(const Buffers &b, int u, int t) {
 // Warp per vertex of the previous window: stamp it and its first kChunk neighbours; the rest of a long row
 // is queued in kChunk pieces for k_mark_chunks.
 __global__ void k_mark(Buffers b, int t) {
-    if (b.ctrl->stopped) return;
+    if (b.ctrl->stopped || b.ctrl->pull) return;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     const int32_t *prev = b.win[(t - 1) & 1];
@@ -203,33 +203,45 @@ __device__ __forceinline__ void put_slot(const Buffers &b, int pos, bool isb, in
     b.bsel[pos] = 0;
 }
 
+// Candidacy: t = 1 every vertex; push mode stamp[v] == t (set by k_mark); pull mode v is in the previous
+// window (sstamp == t-1) or has a neighbour that is, found while the same row walk looks for a
+// differently-labelled neighbour.  The walk stops once both answers are known.
 __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
     if (b.ctrl->stopped) return;
     extern __shared__ int s_npart[];  // [k] boundary records per label in this block
     for (int p = threadIdx.x; p < k; p += blockDim.x) s_npart[p] = 0;
     __syncthreads();
+    const bool pull = !a.all && b.ctrl->pull;
+    const int tp = a.t - 1;
     const int lane = threadIdx.x & 31;
     unsigned long long te = 0, rd = 0, nc = 0, nbd = 0;
     if ((int)blockIdx.x < a.g0) {
         // ---- thread per vertex (deg <= kSmallDeg) ----
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
             const int v = b.bucket[0][i];
+            bool cand = a.all || (pull ? b.sstamp[v] == tp : b.stamp[v] == a.t);
             bool isb = false;
             int own = 0, deg = 0;
-            if (a.all || b.stamp[v] == a.t) {
+            if (cand || pull) {
                 own = b.label[v];
                 const int64_t s = b.off[v];
                 deg = (int)(b.off[v + 1] - s);
-                ++nc;
-                te += deg;
                 int j = 0;
-                for (; j < deg; ++j)
-                    if (b.label[__ldg(b.col + s + j)] != own) {
-                        isb = true;
+                for (; j < deg; ++j) {
+                    const int u = __ldg(b.col + s + j);
+                    if (!cand && b.sstamp[u] == tp) cand = true;
+                    if (b.label[u] != own) isb = true;
+                    if (cand && isb) {
                         ++j;
                         break;
                     }
+                }
                 rd += j;
+                isb = isb && cand;
+                if (cand) {
+                    ++nc;
+                    te += deg;
+                }
             }
             if (isb) {
                 ++nbd;
@@ -244,21 +256,30 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
         for (int i = gw; i < a.nb1; i += nw) {
             const int pos = a.nb0 + i;
             const int v = b.bucket[1][i];
-            bool isb = false;
+            const bool cand0 = a.all || (pull ? b.sstamp[v] == tp : b.stamp[v] == a.t);
+            bool isb = false, cand = cand0;
             int own = 0;
             int64_t s = 0, e = 0;
-            if (a.all || b.stamp[v] == a.t) {
+            if (cand0 || pull) {  // warp-uniform
                 own = b.label[v];
                 s = b.off[v];
                 e = b.off[v + 1];
-                bool diff = false;
-                const int64_t r = warp_row(b.col, s, e, lane, [&](int u) { diff |= (b.label[u] != own); },
-                                           [&] { return __any_sync(DMOLP_FULL_MASK, diff); });
-                isb = __any_sync(DMOLP_FULL_MASK, diff);
+                bool diff = false, fs = false;
+                const int64_t r = warp_row(b.col, s, e, lane, [&](int u) {
+                    if (!cand0) fs |= (b.sstamp[u] == tp);
+                    diff |= (b.label[u] != own);
+                }, [&] {
+                    const bool c = cand0 || __any_sync(DMOLP_FULL_MASK, fs);
+                    return __any_sync(DMOLP_FULL_MASK, diff) && c;
+                });
+                cand = cand0 || __any_sync(DMOLP_FULL_MASK, fs);
+                isb = cand && __any_sync(DMOLP_FULL_MASK, diff);
                 if (lane == 0) {
-                    ++nc;
-                    te += (unsigned long long)(e - s);
                     rd += (unsigned long long)r;
+                    if (cand) {
+                        ++nc;
+                        te += (unsigned long long)(e - s);
+                    }
                 }
             }
             if (lane == 0) {
@@ -275,32 +296,38 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
         for (int i = gb; i < a.nb2; i += nbk) {
             const int pos = a.nb0 + a.nb1 + i;
             const int v = b.bucket[2][i];
-            const bool cand = a.all || b.stamp[v] == a.t;
-            bool isb = false;
+            const bool cand0 = a.all || (pull ? b.sstamp[v] == tp : b.stamp[v] == a.t);
+            bool isb = false, cand = cand0;
             int own = 0;
             int64_t s = 0, e = 0, j0 = 0;
-            if (cand) {  // block-uniform
+            if (cand0 || pull) {  // block-uniform
                 own = b.label[v];
                 s = b.off[v];
                 e = b.off[v + 1];
-                bool diff = false;
+                bool diff = false, fs = false;
                 for (j0 = s; j0 < e; j0 += blockDim.x * 4) {
                     for (int q = 0; q < 4; ++q) {
                         const int64_t j = j0 + q * blockDim.x + threadIdx.x;
-                        if (j < e) diff |= (b.label[__ldcs(b.col + j)] != own);
+                        if (j < e) {
+                            const int u = __ldcs(b.col + j);
+                            if (!cand0) fs |= (b.sstamp[u] == tp);
+                            diff |= (b.label[u] != own);
+                        }
                     }
-                    if (__syncthreads_or(diff)) {
+                    const bool c = cand0 || __syncthreads_or(fs);
+                    if (__syncthreads_or(diff) && c) {
                         j0 += blockDim.x * 4;
                         break;
                     }
                 }
-                isb = __syncthreads_or(diff);
+                cand = cand0 || __syncthreads_or(fs);
+                isb = cand && __syncthreads_or(diff);
             }
             if (threadIdx.x == 0) {
+                if (cand0 || pull) rd += (unsigned long long)((j0 < e ? j0 : e) - s);
                 if (cand) {
                     ++nc;
                     te += (unsigned long long)(e - s);
-                    rd += (unsigned long long)((j0 < e ? j0 : e) - s);
                 }
                 if (isb) {
                     ++nbd;
@@ -370,6 +397,7 @@ __global__ void __launch_bounds__(256) k_split(Buffers b, int t, int eff) {
         int v = 0, cls = -1;
         if (take) {
             v = b.ball[i];
+            b.sstamp[v] = t;
             const int deg = (int)(b.off[v + 1] - b.off[v]);
             te += (unsigned long long)deg;
             cls = deg > kLargeDeg ? 2 : ((deg > kSmallDeg || b.bown[i] >= eff) ? 1 : 0);
@@ -738,7 +766,7 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
 }
 
 // ------------------------------------------------------------------------------------ end
-__global__ void k_lp_end(Buffers b, int k, int t, long long narcs, int mode) {
+__global__ void k_lp_end(Buffers b, int k, int t, long long narcs, int mode, int symmetric) {
     LpControl *ctl = b.ctrl;
     if (ctl->stopped) return;
     LpCounters *cn = b.cnt;
@@ -778,6 +806,9 @@ __global__ void k_lp_end(Buffers b, int k, int t, long long narcs, int mode) {
         ch[DMOLP_MAX_K + p] = sll(b.intra[p]) / 2;
     }
     ctl->iters_run = t;
+    // the next iteration pulls when pushing would walk more than a quarter of all arcs (pulling finds the
+    // same candidates only when every arc has its reverse)
+    ctl->pull = symmetric && r.te_sel * 4ull > (unsigned long long)narcs;
     if (ctl->stop_now) {
         ctl->stopped = 1;
         ctl->stop_reason = ctl->stop_now;
@@ -814,6 +845,7 @@ __global__ void k_lp_init_end(Buffers b, int mode) {
     ctl->stop_reason = 0;
     ctl->stop_now = 0;
     ctl->skip_stats = 0;
+    ctl->pull = 0;
     ctl->prev_cut = (long long)(arcs >> 1);
     if ((arcs & 1ull) || ctl->error) {
         ctl->error = 1;
@@ -845,6 +877,7 @@ __global__ void k_ws_begin(Buffers b, int k, int t, int nprev) {
         cn->nwin[(t - 1) & 1] = nprev;
         cn->nwin[t & 1] = 0;
         b.ctrl->stopped = 0;
+        b.ctrl->pull = 0;
         LpRecordDev &r = b.rec[t - 1];
         r.te_prev = r.te_cand = r.te_sel = r.te_stats = 0;
         r.arcs_bnd = r.arcs_dec = r.arcs_upd = 0;
@@ -1065,7 +1098,7 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
                                                                                                 &b.ctrl->skip_stats);
         c->launches += 3;
     }
-    k_lp_end<<<1, 1, 0, c->stream>>>(b, L.k, t, (long long)c->narcs, L.mode);
+    k_lp_end<<<1, 1, 0, c->stream>>>(b, L.k, t, (long long)c->narcs, L.mode, c->symmetric ? 1 : 0);
     c->launches += 1;
 }
 
