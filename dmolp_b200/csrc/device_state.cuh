@@ -18,6 +18,7 @@ namespace dmolp {
 constexpr int kSmallDeg = 16;    // deg <= 16: one thread walks the row
 constexpr int kLargeDeg = 4096;  // deg > 4096: one block walks the row
 constexpr int kChunk = 4096;     // row chunk of the window-marking kernel
+constexpr int kHubChunk = 2048;  // row chunk of the decisions of deg > kLargeDeg vertices
 
 // Per-iteration counters of the LP loop (reset by the first kernel of each iteration).
 struct LpCounters {
@@ -28,6 +29,7 @@ struct LpCounters {
     int nchanged;     // selected vertices whose label changed (movers)
     int ndec[3];      // selected vertices per decision class
     int nchunk;       // queued row chunks of the marking kernel
+    int nhubq;        // queued row chunks of the hub decisions
     int npos;         // selection record slots: one per vertex with arcs (fixed per graph)
     unsigned long long cut_arcs;   // arcs whose endpoint labels differ (kept current incrementally)
 };
@@ -80,6 +82,8 @@ struct Buffers {
     int32_t *newlab = nullptr; // [nv] new label of a mover in the current iteration, else -1
     int32_t *mov = nullptr;    // [nv] movers of the current iteration
     int2 *chunkq = nullptr;    // [chunk_cap] (vertex, first arc) of queued row chunks
+    int2 *hubq = nullptr;      // [hubq_cap] (hub index, first arc) of queued hub-decision chunks
+    int32_t *hh = nullptr;     // [nb[2] * MAX_K] per-hub label counts of the current decisions
     int32_t *active[2] = {nullptr, nullptr};  // [nv] radix-select active lists
     // per-part arrays (DMOLP_MAX_K); vc / intra hold signed values in two's complement
     unsigned int *hist = nullptr;        // [MAX_K * 256]
@@ -120,7 +124,7 @@ struct dmolp_ctx {
     int64_t maxdeg = 0, maxraw = 0;
     int ibits = 1, dbits = 1, rbits = 1;  // bits for ids, CSR degree, raw degree
     int nb[3] = {0, 0, 0};                // vertices per degree class
-    int64_t chunk_cap = 0;
+    int64_t chunk_cap = 0, hubq_cap = 0;
     bool symmetric = false;               // every arc (u,v) has its reverse: incremental statistics apply
     bool has_graph = false;
     std::vector<int32_t> h_rawdeg;        // host copy for the hub sort

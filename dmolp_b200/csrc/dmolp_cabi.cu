@@ -201,6 +201,10 @@ int run_block_graph(dmolp_ctx *c, const LpLaunch &L, int t0, int cnt) {
 
 }  // namespace
 
+namespace dmolp {
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace dmolp
+
 extern "C" {
 
 const char *dmolp_last_error(void) { return g_err.c_str(); }
@@ -308,6 +312,7 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     }
     for (int i = 0; i < 3; ++i) c->nb[i] = (int)bl[i].size();
     c->chunk_cap = narcs / kChunk + 2;
+    c->hubq_cap = narcs / kHubChunk + (int64_t)bl[2].size() + 2;
 
     Buffers &b = c->b;
     const size_t n = (size_t)nv + 1;
@@ -362,6 +367,8 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     ALLOC(b.newlab, n);
     ALLOC(b.mov, n);
     ALLOC(b.chunkq, (size_t)c->chunk_cap);
+    ALLOC(b.hubq, (size_t)c->hubq_cap);
+    ALLOC(b.hh, bl[2].size() * (size_t)DMOLP_MAX_K);
 #undef ALLOC
     b.claim = b.stamp;  // phase 1 and the LP loop never run at the same time
     DMOLP_CUDA(cudaMemcpyAsync(b.off, off, n * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));

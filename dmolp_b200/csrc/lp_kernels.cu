@@ -84,13 +84,15 @@ __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
         cn->nchanged = 0;
         cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
         cn->nchunk = 0;
+        cn->nhubq = 0;
         ctl->stop_now = 0;
         ctl->skip_stats = 0;
         LpRecordDev &r = b.rec[t - 1];
         r.iteration = t;
         r.window = r.candidates = r.changes = r.boundary = 0;
         r.edge_cut = ctl->prev_cut;
-        r.te_prev = t == 1 ? (unsigned long long)narcs : 0ull;
+        // sum of degrees over the previous window = the previous iteration's selected window
+        r.te_prev = t == 1 ? (unsigned long long)narcs : b.rec[t - 2].te_sel;
         r.te_cand = r.te_sel = r.te_stats = 0;
         r.arcs_bnd = r.arcs_dec = r.arcs_upd = 0;
 
@@ -151,13 +153,11 @@ __global__ void k_mark(Buffers b, int t) {
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     const int32_t *prev = b.win[(t - 1) & 1];
     const int n = b.cnt->nwin[(t - 1) & 1];
-    unsigned long long te = 0;
     for (int i = gw; i < n; i += nw) {
         const int v = prev[i];
         const int64_t s = b.off[v], e = b.off[v + 1];
         if (lane == 0) {
             b.stamp[v] = t;
-            te += (unsigned long long)(e - s);
             for (int64_t c = s + kChunk; c < e; c += kChunk) {
                 const int q = atomicAdd(&b.cnt->nchunk, 1);
                 b.chunkq[q] = make_int2(v, (int)(c - s));
@@ -166,8 +166,6 @@ __global__ void k_mark(Buffers b, int t) {
         const int64_t e1 = e - s > kChunk ? s + kChunk : e;
         warp_row(b.col, s, e1, lane, [&](int u) { stamp_once(b, u, t); }, [] { return false; });
     }
-    te = warp_sum_u64(te);
-    if (lane == 0 && te) atomicAdd(&b.rec[t - 1].te_prev, te);
 }
 
 __global__ void k_mark_chunks(Buffers b, int t) {
@@ -216,7 +214,8 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
     const int lane = threadIdx.x & 31;
     unsigned long long te = 0, rd = 0, nc = 0, nbd = 0;
     if ((int)blockIdx.x < a.g0) {
-        // ---- thread per vertex (deg <= kSmallDeg) ----
+        // ---- thread per vertex (deg <= kSmallDeg): every neighbour id is loaded first, then their labels
+        //      (and window stamps), so a row costs two dependent round trips instead of one per arc ----
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
             const int v = b.bucket[0][i];
             bool cand = a.all || (pull ? b.sstamp[v] == tp : b.stamp[v] == a.t);
@@ -226,17 +225,18 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
                 own = b.label[v];
                 const int64_t s = b.off[v];
                 deg = (int)(b.off[v + 1] - s);
-                int j = 0;
-                for (; j < deg; ++j) {
-                    const int u = __ldg(b.col + s + j);
-                    if (!cand && b.sstamp[u] == tp) cand = true;
-                    if (b.label[u] != own) isb = true;
-                    if (cand && isb) {
-                        ++j;
-                        break;
+                int u[kSmallDeg];
+#pragma unroll
+                for (int j = 0; j < kSmallDeg; ++j) u[j] = j < deg ? __ldg(b.col + s + j) : 0;
+                bool fs = false;
+#pragma unroll
+                for (int j = 0; j < kSmallDeg; ++j)
+                    if (j < deg) {
+                        isb |= b.label[u[j]] != own;
+                        if (pull && !cand) fs |= b.sstamp[u[j]] == tp;
                     }
-                }
-                rd += j;
+                rd += deg;
+                cand = cand || fs;
                 isb = isb && cand;
                 if (cand) {
                     ++nc;
@@ -564,49 +564,75 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
             __syncwarp();
         }
     } else {
-        // ---- block per vertex (deg > kLargeDeg): each warp counts one contiguous eighth of the row ----
-        int *tot = shist + kWarpsPerBlock * 1024;  // [8][32] per-warp totals (eff <= 32)
-        const int gb = (int)blockIdx.x - a.g0 - a.g1, nbk = (int)gridDim.x - a.g0 - a.g1;
-        const int n = b.cnt->ndec[2];
-        for (int i = gb; i < n; i += nbk) {
-            const int v = b.dec[2][i];
-            const int own = b.label[v];
-            const int64_t s = b.off[v], e = b.off[v + 1];
+        // ---- hubs (deg > kLargeDeg): warp per queued row chunk; counts go to the hub's row of hh ----
+        const int wpb = blockDim.x >> 5;
+        const int gw = ((int)blockIdx.x - a.g0 - a.g1) * wpb + wib, nw = ((int)gridDim.x - a.g0 - a.g1) * wpb;
+        const int n = b.cnt->nhubq;
+        for (int q = gw; q < n; q += nw) {
+            const int2 ch = b.hubq[q];
+            const int v = b.dec[2][ch.x];
+            const int64_t s = b.off[v] + ch.y, rowe = b.off[v + 1];
+            const int64_t e = rowe - s > kHubChunk ? s + kHubChunk : rowe;
             if (priv) priv_zero(h, eff, lane);
             else
-                for (int c = threadIdx.x; c < eff; c += blockDim.x) shist[c] = 0;
-            __syncthreads();
-            const int64_t len = e - s, per = ((len + kWarpsPerBlock - 1) / kWarpsPerBlock + 3) & ~int64_t(3);
-            const int64_t ws = s + wib * per < e ? s + wib * per : e;
-            const int64_t we = ws + per < e ? ws + per : e;
-            warp_count(b, ws, we, lane, eff, priv ? h : shist);
+                for (int c = lane; c < eff; c += 32) h[c] = 0;
             __syncwarp();
-            if (priv) tot[wib * 32 + lane] = priv_total(h, eff, lane);
-            __syncthreads();
-            if (wib == 0) {
-                double best;
-                int blab, own_cnt;
-                if (priv) {
-                    int cnt = 0;
-                    for (int w = 0; w < kWarpsPerBlock; ++w) cnt += tot[w * 32 + lane];
-                    warp_argmax(eff, b.tpen, lane, [&](int) { return cnt; }, best, blab);
-                    own_cnt = __shfl_sync(DMOLP_FULL_MASK, cnt, own & 31);
-                } else {
-                    warp_argmax(eff, b.tpen, lane, [&](int c) { return shist[c]; }, best, blab);
-                    own_cnt = (unsigned)own < (unsigned)eff ? shist[own] : 0;
-                }
-                if (lane == 0) {
-                    rd += (unsigned long long)(e - s);
-                    const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
-                    const int nl = best > own_raw ? blab : own;
-                    if (nl != own) park_move(b, v, nl);
-                }
+            warp_count(b, s, e, lane, eff, h);
+            __syncwarp();
+            int32_t *row = b.hh + (size_t)ch.x * DMOLP_MAX_K;
+            if (priv) {
+                const int cnt = priv_total(h, eff, lane);
+                if (cnt) atomicAdd(&row[lane], cnt);
+            } else {
+                for (int c = lane; c < eff; c += 32)
+                    if (h[c]) atomicAdd(&row[c], h[c]);
             }
-            __syncthreads();
+            if (lane == 0) rd += (unsigned long long)(e - s);
+            __syncwarp();
         }
     }
     rd = warp_sum_u64(rd);
     if (lane == 0 && rd) atomicAdd(&b.rec[a.t - 1].arcs_dec, rd);
+}
+
+// Hub decisions, before k_decide: clear each hub's count row and queue its row in kHubChunk pieces.
+__global__ void k_hub_prep(Buffers b, int eff) {
+    if (b.ctrl->stopped) return;
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int n = b.cnt->ndec[2];
+    for (int i = gw; i < n; i += nw) {
+        const int v = b.dec[2][i];
+        int32_t *row = b.hh + (size_t)i * DMOLP_MAX_K;
+        for (int c = lane; c < eff; c += 32) row[c] = 0;
+        const int64_t deg = b.off[v + 1] - b.off[v];
+        const int nch = (int)((deg + kHubChunk - 1) / kHubChunk);
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&b.cnt->nhubq, nch);
+        base = __shfl_sync(DMOLP_FULL_MASK, base, 0);
+        for (int c = lane; c < nch; c += 32) b.hubq[base + c] = make_int2(i, c * kHubChunk);
+    }
+}
+
+// Hub decisions, after k_decide: warp per hub, argmax over its summed counts.
+__global__ void k_hub_final(Buffers b, int eff) {
+    if (b.ctrl->stopped) return;
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int n = b.cnt->ndec[2];
+    for (int i = gw; i < n; i += nw) {
+        const int v = b.dec[2][i];
+        const int own = b.label[v];
+        const int32_t *row = b.hh + (size_t)i * DMOLP_MAX_K;
+        double best;
+        int blab;
+        warp_argmax(eff, b.tpen, lane, [&](int c) { return row[c]; }, best, blab);
+        if (lane == 0) {
+            const double own_raw = (unsigned)own < (unsigned)eff ? (double)row[own] : -1e300;
+            const int nl = best > own_raw ? blab : own;
+            if (nl != own) park_move(b, v, nl);
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------ update
@@ -905,6 +931,7 @@ __global__ void k_classify(Buffers b, int n, int eff) {
 __global__ void k_zero_small(Buffers b) {
     LpCounters *cn = b.cnt;
     cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
+    cn->nhubq = 0;
     cn->nchanged = 0;
     b.ctrl->stopped = 0;
 }
@@ -975,7 +1002,7 @@ DecArgs dec_args(dmolp_ctx *c, int t, int eff) {
     return a;
 }
 
-int dec_grid(dmolp_ctx *c, const DecArgs &a) { return a.g0 + a.g1 + c->num_sms; }
+int dec_grid(dmolp_ctx *c, const DecArgs &a) { return a.g0 + a.g1 + c->num_sms * 2; }
 
 size_t dec_smem(int eff) {
     return eff <= 32 ? (size_t)(kWarpsPerBlock * 1024 + kWarpsPerBlock * 32) * sizeof(int)
@@ -997,6 +1024,17 @@ StatsArgs stats_args(dmolp_ctx *c, int k) {
 }
 
 int stats_grid(dmolp_ctx *c, const StatsArgs &a) { return a.gv + a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
+
+// The LP decisions of the selected window: hub row chunks queued, the three classes counted / decided,
+// hub argmaxes last.
+void launch_decide(dmolp_ctx *c, int t, int eff) {
+    Buffers &b = c->b;
+    k_hub_prep<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff);
+    const DecArgs d = dec_args(c, t, eff);
+    k_decide<<<dec_grid(c, d), kBlock, dec_smem(eff), c->stream>>>(b, d);
+    k_hub_final<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff);
+    c->launches += 3;
+}
 
 // Optional timing of one kernel launch (dmolp_set_profiling): an event pair around it on the same stream.
 // While a graph is being captured the records become event-record nodes of the graph, which owns them.
@@ -1079,10 +1117,9 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     k_split<<<grid, kBlock, 0, c->stream>>>(b, t, L.eff);
     {
         ProfScope ps(c, 1, t);
-        const DecArgs d = dec_args(c, t, L.eff);
-        k_decide<<<dec_grid(c, d), kBlock, dec_smem(L.eff), c->stream>>>(b, d);
+        launch_decide(c, t, L.eff);
     }
-    c->launches += 2;
+    c->launches += 1;
     if (c->symmetric) {
         {
             ProfScope ps(c, 3, t);
@@ -1126,11 +1163,10 @@ void lp_apply_list(dmolp_ctx *c, int k, int eff, int n) {
     const int grid = grid_for(c);
     k_zero_small<<<1, 1, 0, c->stream>>>(b);
     k_classify<<<grid, kBlock, 0, c->stream>>>(b, n, eff);
-    const DecArgs d = dec_args(c, 1, eff);
-    k_decide<<<dec_grid(c, d), kBlock, dec_smem(eff), c->stream>>>(b, d);
+    launch_decide(c, 1, eff);
     k_collect_moves<<<grid, kBlock, 0, c->stream>>>(b);
     k_apply<<<grid, kBlock, 0, c->stream>>>(b);
-    c->launches += 5;
+    c->launches += 4;
 }
 
 }  // namespace dmolp

@@ -118,13 +118,22 @@ __global__ void __launch_bounds__(kHistThreads) k_sel_hist(SelArgs a) {
         for (int i = threadIdx.x; i < a.nseg * kRadix; i += blockDim.x) shist[i] = 0;
         __syncthreads();
     }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int r = a.list ? a.list[i] : i;
-        const int p = a.seg[r];
-        if (p < 0) continue;  // empty record slot
-        const int d = (int)((a.key[r] >> a.shift) & (kRadix - 1));
-        if (use_smem) atomicAdd(&shist[p * kRadix + d], 1u);
-        else atomicAdd(&a.ghist[p * kRadix + d], 1u);
+    // Keys crowd into few bins (a digit of small degrees is mostly 0): lanes with the same bin are merged
+    // with __match_any_sync and add once.
+    const int lane = threadIdx.x & 31;
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        int bin = -(lane + 1);  // unique non-bin value for idle lanes and empty slots
+        if (i < n) {
+            const int r = a.list ? a.list[i] : i;
+            const int p = a.seg[r];
+            if (p >= 0) bin = p * kRadix + (int)((a.key[r] >> a.shift) & (kRadix - 1));
+        }
+        const unsigned m = __match_any_sync(DMOLP_FULL_MASK, bin);
+        if (bin >= 0 && lane == __ffs(m) - 1) {
+            if (use_smem) atomicAdd(&shist[bin], (unsigned)__popc(m));
+            else atomicAdd(&a.ghist[bin], (unsigned)__popc(m));
+        }
     }
     if (use_smem) {
         __syncthreads();
