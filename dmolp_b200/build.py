@@ -31,7 +31,8 @@ GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", *GENCODE, "-Xcompiler", "-fPIC,-fno-fast-math,-ffp-contract=off",
               "--expt-relaxed-constexpr", "-Xptxas", "-v"]
 
-CUDA_SOURCES = ["dmolp_cabi.cu", "lp_kernels.cu", "seed_kernels.cu", "select_kernels.cu", "adjtext.cpp"]
+CUDA_SOURCES = ["dmolp_cabi.cu", "lp_kernels.cu", "seed_kernels.cu", "select_kernels.cu", "adjtext.cpp",
+                "noalloc.cu"]
 CUDA_HEADERS = ["common.cuh", "device_state.cuh", "kernels.cuh"]
 DROPIN_SOURCES = ["dropin.cpp"]
 

@@ -25,7 +25,7 @@ EXPORTS = [
     "dmolp_adjtext_error", "dmolp_host_graph_nv", "dmolp_host_graph_narcs", "dmolp_host_graph_offsets",
     "dmolp_host_graph_indices", "dmolp_host_graph_raw_degree", "dmolp_host_graph_free", "dmolp_stream",
     "dmolp_labels_save", "dmolp_labels_restore", "dmolp_set_profiling", "dmolp_kernel_profile",
-    "dmolp_find_seeds", "dmolp_expand_partitions", "dmolp_current_device",
+    "dmolp_find_seeds", "dmolp_expand_partitions", "dmolp_current_device", "dmolp_metrics_noalloc",
 ]
 
 
@@ -88,5 +88,6 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_set_profiling.argtypes = [vp, c_int]
     lib.dmolp_find_seeds.argtypes = [vp, c_int, c_int32, vp, c_int64, vp, POINTER(c_int32)]
     lib.dmolp_expand_partitions.argtypes = [vp, c_int, c_int, vp, c_int32, POINTER(c_int32)]
+    lib.dmolp_metrics_noalloc.argtypes = [c_int, c_int64, vp, vp, vp, c_int, vp, POINTER(c_int64), vp, vp]
     lib.dmolp_kernel_profile.argtypes = [vp, c_int, POINTER(c_double), POINTER(c_int64), POINTER(c_double)]
     return lib

@@ -189,6 +189,21 @@ const int32_t *dmolp_host_graph_indices(const dmolp_host_graph *g);
 const int32_t *dmolp_host_graph_raw_degree(const dmolp_host_graph *g);
 void dmolp_host_graph_free(dmolp_host_graph *g);
 
+/* The fused edge-cut / balance reduction without any device allocation.  No counterpart in the reference.
+ * For callers that cannot let a library allocate device memory -- e.g. a process whose GPU memory belongs to
+ * another allocator (a framework's caching pool, or a server that reserves all memory at start-up) -- this
+ * entry point needs no context: the caller passes its CSR and labels as DEVICE pointers (offsets[nv+1],
+ * indices[], labels[nv] on `device`, ids in [0,nv)) and a stream (NULL = the legacy default stream) and gets
+ * the results in HOST memory, as dmolp_metrics returns them.  Its only scratch is a file-scope device array
+ * of 2*DMOLP_NOALLOC_MAX_K+2 64-bit counters (16 KiB), held by every GPU that loads the library until exit;
+ * k above DMOLP_NOALLOC_MAX_K is rejected with DMOLP_ERR_ARG.  Every call shares that array and clears the
+ * part it uses first; calls that overlap on the GPU race.  The first call on a device looks up the array's
+ * address with that device current; make it before any stream capture.  Errors: dmolp_last_error(). */
+#define DMOLP_NOALLOC_MAX_K 1024
+int dmolp_metrics_noalloc(int device, int64_t nv, const int64_t *offsets_device, const int32_t *indices_device,
+                          const int32_t *labels_device, int k, void *stream, int64_t *edge_cut, int64_t *vertex_counts,
+                          int64_t *edge_counts);
+
 /* Number of kernel launches this context has issued (all entry points). */
 int64_t dmolp_kernel_launches(const dmolp_ctx *ctx);
 
