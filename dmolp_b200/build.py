@@ -33,7 +33,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", *GENCODE, "-Xcompiler", "-fPIC,-
 
 CUDA_SOURCES = ["dmolp_cabi.cu", "lp_kernels.cu", "seed_kernels.cu", "select_kernels.cu", "adjtext.cpp",
                 "noalloc.cu"]
-CUDA_HEADERS = ["common.cuh", "device_state.cuh", "kernels.cuh"]
+CUDA_HEADERS = ["common.cuh", "device_state.cuh", "kernels.cuh", "lp_device.cuh"]
 DROPIN_SOURCES = ["dropin.cpp"]
 
 

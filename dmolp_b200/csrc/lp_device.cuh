@@ -1,0 +1,111 @@
+// Device helpers shared by the single-graph LP kernels and the batched LP kernel.
+#pragma once
+
+#include <cfloat>
+
+#include "device_state.cuh"
+
+namespace dmolp {
+
+__device__ __forceinline__ int tiekey(int c) { return (c & ~31) | (int)brev5((unsigned)c & 31u); }
+
+__device__ __forceinline__ long long sll(unsigned long long x) { return (long long)x; }
+
+// Better (score desc, tie key asc).
+__device__ __forceinline__ bool better(double s, int key, double bs, int bkey) {
+    return s > bs || (s == bs && key < bkey);
+}
+
+// Visit neighbour ids col[s..e) with the lanes of a warp: scalar head up to a 16-byte boundary, 128-bit
+// loads for the body, scalar tail.  f(u) is called per neighbour; after each step `stop()` (evaluated
+// warp-uniformly) may end the walk early.  Returns the number of arcs the warp read.
+template <typename F, typename S>
+__device__ __forceinline__ int64_t warp_row(const int32_t *__restrict__ col, int64_t s, int64_t e, int lane, F f,
+                                            S stop) {
+    int64_t a = (s + 3) & ~int64_t(3);
+    if (a > e) a = e;
+    if (s + lane < a) f(__ldg(col + s + lane));
+    int64_t read = a - s;
+    if (stop()) return read;
+    const int64_t qe = e >> 2;  // body: int4 words [a/4, e/4)
+    const int4 *c4 = reinterpret_cast<const int4 *>(col);
+    for (int64_t q = (a >> 2) + lane, q0 = a >> 2; q0 < qe; q += 32, q0 += 32) {
+        if (q < qe) {
+            const int4 x = __ldcs(c4 + q);
+            f(x.x);
+            f(x.y);
+            f(x.z);
+            f(x.w);
+        }
+        read += 4 * (qe - q0 < 32 ? qe - q0 : (int64_t)32);
+        if (stop()) return read;
+    }
+    const int64_t t0 = a > (qe << 2) ? a : (qe << 2);
+    if (t0 + lane < e) f(__ldg(col + t0 + lane));
+    return read + (e - t0);
+}
+
+// Lane-private label counters of one warp for labels < 32: lane L counts label c in
+// h[c*32 + ((L + c) & 31)].  Increments need no atomics and hit distinct banks for lanes sharing a label;
+// the sum over row c (lane c, rotated start) is bank-conflict free as well.
+__device__ __forceinline__ void priv_zero(int *h, int eff, int lane) {
+    for (int c = 0; c < eff; ++c) h[c * 32 + ((lane + c) & 31)] = 0;
+}
+__device__ __forceinline__ int priv_total(const int *h, int eff, int lane) {
+    int t = 0;
+    if (lane < eff)
+        for (int j = 0; j < 32; ++j) t += h[lane * 32 + ((j + lane) & 31)];
+    return t;
+}
+
+// Count labels < eff of the arcs [s, e) into the calling warp's histogram: lane-private counters (eff <= 32,
+// h has 32*32 ints) or a shared histogram h[eff] with one atomic per group of equal labels (__match_any).
+__device__ __forceinline__ int64_t warp_count(const int32_t *__restrict__ col, const int32_t *__restrict__ label,
+                                              int64_t s, int64_t e, int lane, int eff, int *h) {
+    if (eff <= 32) {
+        return warp_row(col, s, e, lane, [&](int u) {
+            const int lu = label[u];
+            if ((unsigned)lu < (unsigned)eff) h[lu * 32 + ((lane + lu) & 31)] += 1;
+        }, [] { return false; });
+    }
+    for (int64_t j0 = s; j0 < e; j0 += 32) {
+        const int64_t j = j0 + lane;
+        const int lu = j < e ? label[__ldcs(col + j)] : -1;
+        const bool ok = (unsigned)lu < (unsigned)eff;
+        const unsigned m = __match_any_sync(DMOLP_FULL_MASK, ok ? lu : -(lane + 1));
+        if (ok && lane == __ffs(m) - 1) atomicAdd(&h[lu], __popc(m));
+    }
+    return e - s;
+}
+
+// Warp argmax over labels < eff given per-label counts: lanes hold the counts of labels lane, lane+32, ...
+// through cnt_of(c).  Returns (best score, best label) in every lane; (score desc, tie key asc).
+template <typename C>
+__device__ __forceinline__ void warp_argmax(int eff, const double *tpen, int lane, C cnt_of, double &best,
+                                            int &blab) {
+    best = -DBL_MAX;
+    int bkey = 0x7fffffff;
+    blab = -1;
+    for (int c = lane; c < eff; c += 32) {
+        const int cnt = cnt_of(c);
+        const double sc = cnt > 0 ? __dmul_rn((double)cnt, tpen[c]) : 0.0;
+        const int key = tiekey(c);
+        if (better(sc, key, best, bkey)) {
+            best = sc;
+            bkey = key;
+            blab = c;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(DMOLP_FULL_MASK, best, o);
+        const int ok = __shfl_xor_sync(DMOLP_FULL_MASK, bkey, o);
+        const int ol = __shfl_xor_sync(DMOLP_FULL_MASK, blab, o);
+        if (better(ob, ok, best, bkey)) {
+            best = ob;
+            bkey = ok;
+            blab = ol;
+        }
+    }
+}
+
+}  // namespace dmolp

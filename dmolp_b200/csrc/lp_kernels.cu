@@ -27,49 +27,12 @@
 
 #include "../../include/dmolp_b200.h"
 #include "kernels.cuh"
+#include "lp_device.cuh"
 
 namespace dmolp {
 namespace {
 
 constexpr int kGridPerSm = 4;
-
-__device__ __forceinline__ int tiekey(int c) { return (c & ~31) | (int)brev5((unsigned)c & 31u); }
-
-__device__ __forceinline__ long long sll(unsigned long long x) { return (long long)x; }
-
-// Better (score desc, tie key asc).
-__device__ __forceinline__ bool better(double s, int key, double bs, int bkey) {
-    return s > bs || (s == bs && key < bkey);
-}
-
-// Visit neighbour ids col[s..e) with the lanes of a warp: scalar head up to a 16-byte boundary, 128-bit
-// loads for the body, scalar tail.  f(u) is called per neighbour; after each step `stop()` (evaluated
-// warp-uniformly) may end the walk early.  Returns the number of arcs the warp read.
-template <typename F, typename S>
-__device__ __forceinline__ int64_t warp_row(const int32_t *__restrict__ col, int64_t s, int64_t e, int lane, F f,
-                                            S stop) {
-    int64_t a = (s + 3) & ~int64_t(3);
-    if (a > e) a = e;
-    if (s + lane < a) f(__ldg(col + s + lane));
-    int64_t read = a - s;
-    if (stop()) return read;
-    const int64_t qe = e >> 2;  // body: int4 words [a/4, e/4)
-    const int4 *c4 = reinterpret_cast<const int4 *>(col);
-    for (int64_t q = (a >> 2) + lane, q0 = a >> 2; q0 < qe; q += 32, q0 += 32) {
-        if (q < qe) {
-            const int4 x = __ldcs(c4 + q);
-            f(x.x);
-            f(x.y);
-            f(x.z);
-            f(x.w);
-        }
-        read += 4 * (qe - q0 < 32 ? qe - q0 : (int64_t)32);
-        if (stop()) return read;
-    }
-    const int64_t t0 = a > (qe << 2) ? a : (qe << 2);
-    if (t0 + lane < e) f(__ldg(col + t0 + lane));
-    return read + (e - t0);
-}
 
 // ------------------------------------------------------------------------------------ begin
 __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
@@ -214,8 +177,8 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
     const int lane = threadIdx.x & 31;
     unsigned long long te = 0, rd = 0, nc = 0, nbd = 0;
     if ((int)blockIdx.x < a.g0) {
-        // ---- thread per vertex (deg <= kSmallDeg): every neighbour id is loaded first, then their labels
-        //      (and window stamps), so a row costs two dependent round trips instead of one per arc ----
+        // ---- thread per vertex (deg <= kSmallDeg): every neighbour id is loaded first, then labels (and
+        //      window stamps) in independent groups of 4 ----
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
             const int v = b.bucket[0][i];
             bool cand = a.all || (pull ? b.sstamp[v] == tp : b.stamp[v] == a.t);
@@ -228,14 +191,22 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
                 int u[kSmallDeg];
 #pragma unroll
                 for (int j = 0; j < kSmallDeg; ++j) u[j] = j < deg ? __ldg(b.col + s + j) : 0;
+                // groups of 4 neighbours: their label (and window-stamp) gathers are independent; stop once
+                // both the boundary and the candidacy answers are known
                 bool fs = false;
+                int j = 0;
 #pragma unroll
-                for (int j = 0; j < kSmallDeg; ++j)
-                    if (j < deg) {
-                        isb |= b.label[u[j]] != own;
-                        if (pull && !cand) fs |= b.sstamp[u[j]] == tp;
-                    }
-                rd += deg;
+                for (int j0 = 0; j0 < kSmallDeg; j0 += 4) {
+                    if (j0 >= deg || (isb && (cand || fs))) break;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (j0 + q < deg) {
+                            isb |= b.label[u[j0 + q]] != own;
+                            if (!cand && !fs) fs |= b.sstamp[u[j0 + q]] == tp;
+                        }
+                    j = j0 + 4 < deg ? j0 + 4 : deg;
+                }
+                rd += j;
                 cand = cand || fs;
                 isb = isb && cand;
                 if (cand) {
@@ -425,68 +396,6 @@ __device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
     b.mov[q] = v;
 }
 
-// Lane-private label counters of one warp for labels < 32: lane L counts label c in
-// h[c*32 + ((L + c) & 31)].  Increments need no atomics and hit distinct banks for lanes sharing a label;
-// the sum over row c (lane c, rotated start) is bank-conflict free as well.
-__device__ __forceinline__ void priv_zero(int *h, int eff, int lane) {
-    for (int c = 0; c < eff; ++c) h[c * 32 + ((lane + c) & 31)] = 0;
-}
-__device__ __forceinline__ int priv_total(const int *h, int eff, int lane) {
-    int t = 0;
-    if (lane < eff)
-        for (int j = 0; j < 32; ++j) t += h[lane * 32 + ((j + lane) & 31)];
-    return t;
-}
-
-// Count labels < eff of the arcs [s, e) into the calling warp's histogram: lane-private counters (eff <= 32,
-// h has 32*32 ints) or a shared histogram h[eff] with one atomic per group of equal labels (__match_any).
-__device__ __forceinline__ int64_t warp_count(const Buffers &b, int64_t s, int64_t e, int lane, int eff, int *h) {
-    if (eff <= 32) {
-        return warp_row(b.col, s, e, lane, [&](int u) {
-            const int lu = b.label[u];
-            if ((unsigned)lu < (unsigned)eff) h[lu * 32 + ((lane + lu) & 31)] += 1;
-        }, [] { return false; });
-    }
-    for (int64_t j0 = s; j0 < e; j0 += 32) {
-        const int64_t j = j0 + lane;
-        const int lu = j < e ? b.label[__ldcs(b.col + j)] : -1;
-        const bool ok = (unsigned)lu < (unsigned)eff;
-        const unsigned m = __match_any_sync(DMOLP_FULL_MASK, ok ? lu : -(lane + 1));
-        if (ok && lane == __ffs(m) - 1) atomicAdd(&h[lu], __popc(m));
-    }
-    return e - s;
-}
-
-// Warp argmax over labels < eff given per-label counts: lanes hold the counts of labels lane, lane+32, ...
-// through cnt_of(c).  Returns (best score, best label) in every lane; (score desc, tie key asc).
-template <typename C>
-__device__ __forceinline__ void warp_argmax(int eff, const double *tpen, int lane, C cnt_of, double &best,
-                                            int &blab) {
-    best = -DBL_MAX;
-    int bkey = 0x7fffffff;
-    blab = -1;
-    for (int c = lane; c < eff; c += 32) {
-        const int cnt = cnt_of(c);
-        const double sc = cnt > 0 ? __dmul_rn((double)cnt, tpen[c]) : 0.0;
-        const int key = tiekey(c);
-        if (better(sc, key, best, bkey)) {
-            best = sc;
-            bkey = key;
-            blab = c;
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(DMOLP_FULL_MASK, best, o);
-        const int ok = __shfl_xor_sync(DMOLP_FULL_MASK, bkey, o);
-        const int ol = __shfl_xor_sync(DMOLP_FULL_MASK, blab, o);
-        if (better(ob, ok, best, bkey)) {
-            best = ob;
-            bkey = ok;
-            blab = ol;
-        }
-    }
-}
-
 __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
     if (b.ctrl->stopped) return;
     extern __shared__ int shist[];  // eff <= 32: 8 warps x 32x32 private counters + 8x32 totals; else 8 x eff
@@ -543,7 +452,7 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
             else
                 for (int c = lane; c < eff; c += 32) h[c] = 0;
             __syncwarp();
-            warp_count(b, s, e, lane, eff, h);
+            warp_count(b.col, b.label, s, e, lane, eff, h);
             __syncwarp();
             double best;
             int blab, own_cnt;
@@ -577,7 +486,7 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
             else
                 for (int c = lane; c < eff; c += 32) h[c] = 0;
             __syncwarp();
-            warp_count(b, s, e, lane, eff, h);
+            warp_count(b.col, b.label, s, e, lane, eff, h);
             __syncwarp();
             int32_t *row = b.hh + (size_t)ch.x * DMOLP_MAX_K;
             if (priv) {
