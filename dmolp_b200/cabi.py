@@ -26,7 +26,11 @@ EXPORTS = [
     "dmolp_host_graph_indices", "dmolp_host_graph_raw_degree", "dmolp_host_graph_free", "dmolp_stream",
     "dmolp_labels_save", "dmolp_labels_restore", "dmolp_set_profiling", "dmolp_kernel_profile",
     "dmolp_find_seeds", "dmolp_expand_partitions", "dmolp_current_device", "dmolp_metrics_noalloc",
+    "dmolp_batch_create", "dmolp_batch_destroy", "dmolp_batch_upload", "dmolp_batch_labels_set",
+    "dmolp_batch_labels_get", "dmolp_batch_device_labels", "dmolp_batch_stream", "dmolp_batch_lp_run",
+    "dmolp_batch_autotune", "dmolp_batch_counts",
 ]
+BATCH_MAX_K = 64
 
 
 class Phase1Info(ctypes.Structure):
@@ -49,6 +53,17 @@ class LpRecord(ctypes.Structure):
     _fields_ = [("iteration", c_int32), ("window", c_int32), ("candidates", c_int32), ("changes", c_int32),
                 ("boundary", c_int32), ("reserved", c_int32), ("edge_cut", c_int64), ("te_prev", c_uint64),
                 ("te_cand", c_uint64), ("te_sel", c_uint64), ("te_stats", c_uint64), ("arcs_read", c_uint64)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("block_threads", c_int32), ("thread_row_max", c_int32), ("blocks_per_sm", c_int32),
+                ("reserved", c_int32)]
+
+
+class BatchResult(ctypes.Structure):
+    _fields_ = [("edge_cut", c_int64), ("traversed_edges", c_uint64), ("arcs_read", c_uint64),
+                ("vertex_balance", c_double), ("edge_balance", c_double), ("iterations_run", c_int32),
+                ("stop_reason", c_int32), ("status", c_int32), ("changes", c_int32)]
 
 
 def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
@@ -90,4 +105,15 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_expand_partitions.argtypes = [vp, c_int, c_int, vp, c_int32, POINTER(c_int32)]
     lib.dmolp_metrics_noalloc.argtypes = [c_int, c_int64, vp, vp, vp, c_int, vp, POINTER(c_int64), vp, vp]
     lib.dmolp_kernel_profile.argtypes = [vp, c_int, POINTER(c_double), POINTER(c_int64), POINTER(c_double)]
+    lib.dmolp_batch_create.argtypes = [c_int, POINTER(vp)]
+    lib.dmolp_batch_destroy.argtypes = [vp]
+    lib.dmolp_batch_upload.argtypes = [vp, c_int32, vp, vp, vp, vp]
+    lib.dmolp_batch_labels_set.argtypes = [vp, vp]
+    lib.dmolp_batch_labels_get.argtypes = [vp, vp]
+    lib.dmolp_batch_device_labels.argtypes = [vp, POINTER(vp)]
+    lib.dmolp_batch_stream.argtypes = [vp]
+    lib.dmolp_batch_stream.restype = vp
+    lib.dmolp_batch_lp_run.argtypes = [vp, POINTER(LpConfig), POINTER(BatchTuning), vp, POINTER(c_double)]
+    lib.dmolp_batch_autotune.argtypes = [vp, POINTER(LpConfig), POINTER(BatchTuning), POINTER(c_double)]
+    lib.dmolp_batch_counts.argtypes = [vp, c_int32, vp, vp]
     return lib

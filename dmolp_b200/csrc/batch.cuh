@@ -1,0 +1,48 @@
+// Batched LP: device-side instance table and kernel arguments (batch_kernels.cu), used by batch_cabi.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/dmolp_b200.h"
+#include "common.cuh"
+
+namespace dmolp {
+namespace batch {
+
+constexpr int kBatchMaxK = DMOLP_BATCH_MAX_K;
+constexpr int kStampStride = 512;  // > the longest run (kMaxIter iterations)
+
+struct Inst {
+    int64_t vbase;   // first vertex of the instance in the union graph
+    int64_t narcs;   // arcs of the instance
+    int32_t nv, k;
+    int32_t maxdeg, ibits, dbits, symmetric;
+};
+
+struct Out {
+    long long edge_cut, te, arcs, visits;
+    int iterations, stop_reason, status, changes;
+};
+
+struct Args {
+    const int64_t *off;
+    const int32_t *col;
+    int32_t *label, *newlab, *cstamp;
+    int32_t *l_cand, *l_bnd, *l_act, *l_win0, *l_win1;  // per-instance slices at vbase
+    const Inst *inst;
+    const int32_t *order;
+    int ninst;
+    int *next, *stamp_base;
+    Out *out;
+    long long *counts;  // [ninst][2 * kBatchMaxK]: vertex counts, intra-part edges
+    const double *logtab, *ratiotab;
+    int mode, iters, cap;
+};
+
+int occupancy(int nt, int td);
+bool launch(const Args &a, int nt, int td, int grid, cudaStream_t s);
+void prepare(const int64_t *off, int32_t *col, Inst *inst, int ninst, int *next, int *err, int grid, cudaStream_t s);
+
+}  // namespace batch
+}  // namespace dmolp

@@ -108,4 +108,62 @@ __device__ __forceinline__ void warp_argmax(int eff, const double *tpen, int lan
     }
 }
 
+// calculatePenalties (src/phase2/phase2.cpp:158-209) by one warp, with the reference's operation order:
+// per-part ratios and penalties in parallel, the means and variances summed in part order by lane 0.
+// vc_of(p) = vertices of part p, ec_of(p) = its intra-part edges (arcs / 2); logt = log(iteration).
+// Writes RE[p] and tpen[p] = 1 + penalty[p] (the kernel's score factor), and penalty[p] to pen_out if given.
+template <typename VC, typename EC>
+__device__ __forceinline__ void warp_penalties(int k, VC vc_of, EC ec_of, double logt, double *RE, double *tpen,
+                                               double *pen_out) {
+    const int lane = threadIdx.x & 31;
+    long long tv = 0, te = 0;
+    for (int p = lane; p < k; p += 32) {
+        tv += vc_of(p);
+        te += ec_of(p);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        tv += __shfl_xor_sync(DMOLP_FULL_MASK, tv, o);
+        te += __shfl_xor_sync(DMOLP_FULL_MASK, te, o);
+    }
+    const double ev = __ddiv_rn((double)tv, (double)k);
+    const double ee = te > 0 ? __ddiv_rn((double)te, (double)k) : 1.0;
+    for (int p = lane; p < k; p += 32) {
+        RE[p] = ee > 0 ? __ddiv_rn((double)ec_of(p), ee) : 1.0;
+        tpen[p] = ev > 0 ? __ddiv_rn((double)vc_of(p), ev) : 1.0;  // RV until the penalties overwrite it
+    }
+    __syncwarp();
+    double imb_rv = 0.0, imb_re = 0.0;
+    if (lane == 0) {
+        double rv_mean = 0.0, re_mean = 0.0;
+        for (int p = 0; p < k; ++p) {
+            rv_mean = __dadd_rn(rv_mean, tpen[p]);
+            re_mean = __dadd_rn(re_mean, RE[p]);
+        }
+        rv_mean = __ddiv_rn(rv_mean, (double)k);
+        re_mean = __ddiv_rn(re_mean, (double)k);
+        double rv_var = 0.0, re_var = 0.0;
+        for (int p = 0; p < k; ++p) {
+            const double dv = __dsub_rn(tpen[p], rv_mean), de = __dsub_rn(RE[p], re_mean);
+            rv_var = __dadd_rn(rv_var, __dmul_rn(dv, dv));
+            re_var = __dadd_rn(re_var, __dmul_rn(de, de));
+        }
+        rv_var = __ddiv_rn(rv_var, (double)k);
+        re_var = __ddiv_rn(re_var, (double)k);
+        const double total_var = __dadd_rn(rv_var, re_var);
+        imb_rv = total_var > 0 ? __ddiv_rn(rv_var, total_var) : 0.0;
+        imb_re = total_var > 0 ? __ddiv_rn(re_var, total_var) : 0.0;
+    }
+    imb_rv = __shfl_sync(DMOLP_FULL_MASK, imb_rv, 0);
+    imb_re = __shfl_sync(DMOLP_FULL_MASK, imb_re, 0);
+    const double g = __dadd_rn(1.0, logt);
+    for (int p = lane; p < k; p += 32) {
+        const double grv = __dmul_rn(__dsub_rn(1.0, tpen[p]), g);
+        const double gre = __dmul_rn(__dsub_rn(1.0, RE[p]), g);
+        const double pen = __dadd_rn(__dmul_rn(imb_rv, grv), __dmul_rn(imb_re, gre));
+        if (pen_out) pen_out[p] = pen;
+        tpen[p] = __dadd_rn(1.0, pen);
+    }
+    __syncwarp();
+}
+
 }  // namespace dmolp

@@ -58,48 +58,11 @@ __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
         r.te_prev = t == 1 ? (unsigned long long)narcs : b.rec[t - 2].te_sel;
         r.te_cand = r.te_sel = r.te_stats = 0;
         r.arcs_bnd = r.arcs_dec = r.arcs_upd = 0;
-
-        // ---- statistics -> expected values (phase2.cpp:110-115) ----
-        long long tv = 0, te = 0;
-        for (int p = 0; p < k; ++p) {
-            tv += sll(b.vc[p]);
-            te += sll(b.intra[p]) / 2;
-        }
-        const double ev = __ddiv_rn((double)tv, (double)k);
-        const double ee = te > 0 ? __ddiv_rn((double)te, (double)k) : 1.0;
-        // ---- calculatePenalties (phase2.cpp:166-203) ----
-        double rv_mean = 0.0, re_mean = 0.0;
-        for (int p = 0; p < k; ++p) {
-            const double rv = ev > 0 ? __ddiv_rn((double)sll(b.vc[p]), ev) : 1.0;
-            const double re = ee > 0 ? __ddiv_rn((double)(sll(b.intra[p]) / 2), ee) : 1.0;
-            b.RE[p] = re;
-            b.tpen[p] = rv;  // RV kept here until the penalties overwrite it below
-            rv_mean = __dadd_rn(rv_mean, rv);
-            re_mean = __dadd_rn(re_mean, re);
-        }
-        rv_mean = __ddiv_rn(rv_mean, (double)k);
-        re_mean = __ddiv_rn(re_mean, (double)k);
-        double rv_var = 0.0, re_var = 0.0;
-        for (int p = 0; p < k; ++p) {
-            const double dv = __dsub_rn(b.tpen[p], rv_mean), de = __dsub_rn(b.RE[p], re_mean);
-            rv_var = __dadd_rn(rv_var, __dmul_rn(dv, dv));
-            re_var = __dadd_rn(re_var, __dmul_rn(de, de));
-        }
-        rv_var = __ddiv_rn(rv_var, (double)k);
-        re_var = __ddiv_rn(re_var, (double)k);
-        const double total_var = __dadd_rn(rv_var, re_var);
-        const double imb_rv = total_var > 0 ? __ddiv_rn(rv_var, total_var) : 0.0;
-        const double imb_re = total_var > 0 ? __ddiv_rn(re_var, total_var) : 0.0;
-        const double g = __dadd_rn(1.0, b.logtab[t]);
-        double *ph = b.penhist + (size_t)(t - 1) * DMOLP_MAX_K;
-        for (int p = 0; p < k; ++p) {
-            const double grv = __dmul_rn(__dsub_rn(1.0, b.tpen[p]), g);
-            const double gre = __dmul_rn(__dsub_rn(1.0, b.RE[p]), g);
-            const double pen = __dadd_rn(__dmul_rn(imb_rv, grv), __dmul_rn(imb_re, gre));
-            ph[p] = pen;
-            b.tpen[p] = __dadd_rn(1.0, pen);  // the kernel's score factor (1.0 + penalty[c])
-        }
     }
+    // ---- statistics -> expected values and calculatePenalties (phase2.cpp:110-115, 158-209) ----
+    if (threadIdx.x < 32)
+        warp_penalties(k, [&](int p) { return sll(b.vc[p]); }, [&](int p) { return sll(b.intra[p]) / 2; },
+                       b.logtab[t], b.RE, b.tpen, b.penhist + (size_t)(t - 1) * DMOLP_MAX_K);
 }
 
 // ------------------------------------------------------------------------------------ mark

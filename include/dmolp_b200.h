@@ -207,6 +207,60 @@ int dmolp_metrics_noalloc(int device, int64_t nv, const int64_t *offsets_device,
 /* Number of kernel launches this context has issued (all entry points). */
 int64_t dmolp_kernel_launches(const dmolp_ctx *ctx);
 
+/* ---------------------------------------------------------------------------------------------------------
+ * Batched phase 2: many independent graphs, each with its own part count, partitioned by one persistent
+ * kernel launch replayed from a captured CUDA graph.  No counterpart in the reference, which partitions one
+ * graph per run; every instance follows run_phase2 (src/phase2/phase2.cpp:256-449) exactly as dmolp_lp_run
+ * does and ends with the same labels, cut and counts as a single-graph run on the same graph and labels.
+ * ------------------------------------------------------------------------------------------------------- */
+#define DMOLP_BATCH_MAX_K 64
+
+typedef struct dmolp_batch dmolp_batch;
+
+typedef struct {                   /* the launch shape; the autotuner picks it */
+    int32_t block_threads;         /* threads per CTA: 256, 512 or 1024 */
+    int32_t thread_row_max;        /* rows of at most this many arcs are walked by one thread: 8 or 16 */
+    int32_t blocks_per_sm;         /* resident CTAs per SM (0 = as many as fit) */
+    int32_t reserved;
+} dmolp_batch_tuning;
+
+typedef struct {                   /* one per instance */
+    int64_t edge_cut;
+    uint64_t traversed_edges;      /* the same four terms as dmolp_lp_result */
+    uint64_t arcs_read;            /* arcs this implementation read */
+    double vertex_balance, edge_balance;
+    int32_t iterations_run;
+    int32_t stop_reason;
+    int32_t status;                /* DMOLP_OK, or DMOLP_ERR_BAD_LABELS for labels outside [0,k) */
+    int32_t changes;               /* moves over all iterations */
+} dmolp_batch_result;
+
+int dmolp_batch_create(int device, dmolp_batch **out);
+int dmolp_batch_destroy(dmolp_batch *b);
+
+/* The batch as one union CSR: instance i owns vertices [vstart[i], vstart[i+1]) and their rows of
+ * offsets[] (int64, nv+1 entries, offsets[0] = 0); indices[] hold ids LOCAL to the instance (0-based).
+ * parts[i] = k of instance i in [1, DMOLP_BATCH_MAX_K].  nv < 2^31.  Resets the labels to 0. */
+int dmolp_batch_upload(dmolp_batch *b, int32_t ninst, const int64_t *vstart, const int64_t *offsets,
+                       const int32_t *indices, const int32_t *parts);
+/* Labels of all instances, int32[nv] in union order, values in [0, parts[i]). */
+int dmolp_batch_labels_set(dmolp_batch *b, const int32_t *labels);
+int dmolp_batch_labels_get(dmolp_batch *b, int32_t *labels);
+int dmolp_batch_device_labels(dmolp_batch *b, int32_t **labels);  /* device pointer to the labels */
+void *dmolp_batch_stream(dmolp_batch *b);              /* the batch's cudaStream_t */
+
+/* Phase 2 on every instance (cfg as for dmolp_lp_run).  tune NULL: the autotuned shape if
+ * dmolp_batch_autotune ran, else a default.  results[ninst] (may be NULL); gpu_ms (may be NULL) = device time
+ * of the launch.  An instance with labels outside [0,k) is left unchanged, its status says so, and the call
+ * returns DMOLP_ERR_BAD_LABELS after all others ran. */
+int dmolp_batch_lp_run(dmolp_batch *b, const dmolp_lp_config *cfg, const dmolp_batch_tuning *tune,
+                       dmolp_batch_result *results, double *gpu_ms);
+/* Times every launch shape on the uploaded batch and its current labels (restored after each trial) and
+ * keeps the fastest for later runs.  best / best_ms may be NULL. */
+int dmolp_batch_autotune(dmolp_batch *b, const dmolp_lp_config *cfg, dmolp_batch_tuning *best, double *best_ms);
+/* Per-part vertex counts and intra-part edge counts of instance i after the last run (k entries each). */
+int dmolp_batch_counts(dmolp_batch *b, int32_t inst, int64_t *vertex_counts, int64_t *edge_counts);
+
 #ifdef __cplusplus
 }
 #endif
