@@ -39,10 +39,17 @@ WORKLOADS = {
                        iters=30),
     # 3-D k-NN (k=12), 55,476 points, k = 8, 20 LP iterations
     "knn-c0": dict(kind="knn", n=55476, dim=3, knn=12, seed=1, k=8, theta=1000, iters=20),
+    # 2048 graphs, V log-uniform in [1K, 200K], half k-NN 2-D/3-D (k_nn 8..14), half preferential attachment
+    # (m 4..8), k uniform in 2..64; phase 2 with the reference's stopping rules from phase-1 partitions
+    "batch2048": dict(kind="batch", n=2048, seed=11, vmin=1000, vmax=200_000, theta=1000),
 }
 
 
 def describe(w: dict) -> str:
+    if w["kind"] == "batch":
+        return (f"{w['n']} graphs, V log-uniform in [{w['vmin']}, {w['vmax']}], half 2-D/3-D k-NN (k_nn 8-14), "
+                f"half preferential attachment (m 4-8), k uniform in 2..64, seed {w['seed']}, phase-1 theta "
+                f"{w['theta']}, phase 2 with the reference's stopping rules")
     if w["kind"] == "rmat":
         return (f"R-MAT scale {w['scale']} edge factor {w['edge_factor']} ({w['a']},{w['b']},{w['c']}) seed "
                 f"{w['seed']}, symmetrised, k={w['k']}, theta={w['theta']}, {w['iters']} LP iterations")
@@ -280,8 +287,135 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
     return line
 
 
+# ------------------------------------------------------------------------------------------- batched
+def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | None:
+    """Graphs per second of phase 2 over a batch of independent graphs: the batched persistent launch
+    against the single-graph path run on one instance after another (the plain method), from the same
+    phase-1 partitions; every instance must end with identical labels either way."""
+    import torch
+
+    from dmolp_b200.batch import Batch, random_instances, union
+    from dmolp_b200.partitioner import Partitioner
+
+    torch.cuda.set_device(local_rank)
+    n = w["n"]
+    t0 = time.perf_counter()
+    inst = random_instances(n, seed=w["seed"] + 1000 * rank, vmin=w["vmin"], vmax=w["vmax"])
+    gen_s = time.perf_counter() - t0
+    arrays = union(inst)
+    nv_tot, na_tot = int(arrays[0][-1]), int(arrays[1][-1])
+
+    # ---- phase 1 (single-graph path) for every instance: the starting partitions ----
+    p = Partitioner(local_rank)
+    lab1, p1_ms = [], 0.0
+    t0 = time.perf_counter()
+    for it in inst:
+        p.upload(it.graph)
+        m1 = p.phase1(it.k, w["theta"])
+        p1_ms += m1.gpu_ms
+        lab1.append(p.labels())
+    p1_wall = time.perf_counter() - t0
+
+    # ---- plain: phase 2 of the single-graph path, one instance after another ----
+    ns = n if args.plain_sample <= 0 else min(n, args.plain_sample)
+    plain_ms, plain_wall, plain_labels, plain_cut = 0.0, 0.0, [], 0
+    for it, l1 in zip(inst[:ns], lab1[:ns]):
+        p.upload(it.graph)
+        p.set_labels(l1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m2 = p.phase2(it.k, mode="ref", records=False)
+        plain_labels.append(p.labels())
+        plain_wall += time.perf_counter() - t0
+        plain_ms += m2.gpu_ms
+        plain_cut += m2.edge_cut
+    p.close()
+
+    # ---- batched ----
+    b = Batch(local_rank)
+    b.upload(arrays=arrays)
+    b.set_labels(lab1)
+    t0 = time.perf_counter()
+    tune = b.autotune("ref", 0, "ref")
+    tune_s = time.perf_counter() - t0
+    b.save_labels()
+    for _ in range(max(1, args.warmup)):
+        b.restore_labels()
+        b.run("ref", results=False)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.steps):
+        b.restore_labels()
+        ms.append(b.run("ref", results=False)[1])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    b.restore_labels()
+    res, one_ms = b.run("ref", results=True)
+    final = b.split(b.labels())
+    identical = all(np.array_equal(final[i], plain_labels[i]) for i in range(ns))
+    batch_cut = sum(r["edge_cut"] for r in res[:ns])
+    elapsed = sum(ms) / 1e3
+    by = sum(8.0 * r["arcs_read"] + 20.0 * r["vertex_visits"] for r in res)
+
+    # ---- end to end: host arrays in, labels and results out ----
+    pinned = [torch.from_numpy(a).pin_memory().numpy() for a in arrays]
+    lab_h = torch.from_numpy(np.concatenate(lab1)).pin_memory().numpy()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.upload(arrays=pinned)
+    b.tuning = {k: tune[k] for k in ("block_threads", "thread_row_max", "blocks_per_sm", "reserved")}
+    b.set_labels(lab_h)
+    res2, _ = b.run("ref", results=True)
+    out = b.labels()
+    e2e_s = time.perf_counter() - t0
+    assert np.array_equal(out, np.concatenate(final)), "end-to-end labels differ"
+    b.close()
+
+    t_max = elapsed
+    if dist:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t[0])
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peaks()
+    per_launch_s = elapsed / max(1, len(ms))
+    achieved = by / per_launch_s / 1e9
+    plain_gps = ns / (plain_ms / 1e3)
+    value = n * args.steps * world / t_max
+    return {
+        "metric": "phase-2 graphs/s (batched)", "value": value, "unit": "graphs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generators)",
+        "config": {"workload": describe(w), "instances": n, "num_vertices": nv_tot, "num_arcs": na_tot,
+                   "mode": "ref", "label_cap": "reference (min(k,32))", "tuning": tune,
+                   "autotune_s": tune_s, "generate_s": gen_s,
+                   "plain": {"instances_timed": ns, "graphs_per_s_device": plain_gps,
+                             "graphs_per_s_wall": ns / plain_wall, "lp_ms_device": plain_ms},
+                   "speedup_vs_plain_device": value / world / plain_gps,
+                   "identical_labels_to_plain": identical, "edge_cut_sum_batched": batch_cut,
+                   "edge_cut_sum_plain": plain_cut,
+                   "phase1_single_graph_ms_device": p1_ms, "phase1_single_graph_wall_s": p1_wall,
+                   "iterations_mean": float(np.mean([r["iterations_run"] for r in res])),
+                   "l2": "batch CSR %.0f MB > L2" % (na_tot * 4 / 1e6), "parallelism": f"replicas x{world}"},
+        "e2e": {"value": n * world / e2e_s, "unit": "graphs/s", "wall_s": e2e_s,
+                "h2d_bytes_per_step": int(sum(a.nbytes for a in arrays) + lab_h.nbytes),
+                "d2h_bytes_per_step": int(lab_h.nbytes)},
+        "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "hbm", "kernel": "k_batch_lp", "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic_from_profiles("k_batch_lp", args.workload),
+                     "algorithmic_bytes_per_launch": by, "avg_launch_ms": per_launch_s * 1e3},
+    }
+
+
 # ------------------------------------------------------------------------------------------- CPU baselines
-def reference_cpu_run(g, labels1, w, repeats: int, iters: int, threads: int, timeout: float = 900):
+def reference_cpu_run(g, labels1, w, repeats: int, iters: int, threads: int, timeout: float = 900,
+                      mode: str = "fixed"):
     """The reference's own phase-2 code (oracle/_ref, built from its sources) on the host cores."""
     import oracle
 
@@ -293,7 +427,7 @@ def reference_cpu_run(g, labels1, w, repeats: int, iters: int, threads: int, tim
         lab = os.path.join(td, "labels1.bin")
         labels1.astype(np.int32).tofile(lab)
         cmd = [oracle.REF_HARNESS, txt, str(w["k"]), str(w["theta"]), "--out", os.path.join(td, "o"), "--mode",
-               "fixed", "--iters", str(iters), "--threads", str(threads), "--labels-in", lab, "--no-seed-dump",
+               mode, "--iters", str(iters), "--threads", str(threads), "--labels-in", lab, "--no-seed-dump",
                "--repeat", str(repeats)]
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         pr = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
@@ -373,6 +507,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="timed steps only: no clock soak, e2e or CPU baseline")
     ap.add_argument("--records", action="store_true", help="print one step's per-iteration records to stderr")
+    ap.add_argument("--plain-sample", type=int, default=0,
+                    help="batched workload: instances timed on the single-graph path (0 = all)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", "0"))
@@ -393,12 +529,12 @@ def main():
         torch.cuda.set_device(local_rank)
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
-    line = run_ours(args, w, rank, world, local_rank, dist)
+    line = (run_batch if w["kind"] == "batch" else run_ours)(args, w, rank, world, local_rank, dist)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0 and line is not None:
-        if world == 1 and not args.no_cpu_baseline and not args.quick:
+        if world == 1 and not args.no_cpu_baseline and not args.quick and w["kind"] != "batch":
             g = make_graph(w)
             import oracle
 

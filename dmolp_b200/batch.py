@@ -142,6 +142,12 @@ class Batch:
     def split(self, union_array: np.ndarray) -> list[np.ndarray]:
         return [union_array[self.vstart[i]:self.vstart[i + 1]] for i in range(self.num_instances)]
 
+    def save_labels(self) -> None:
+        self._check(self.lib.dmolp_batch_labels_save(self.h))
+
+    def restore_labels(self) -> None:
+        self._check(self.lib.dmolp_batch_labels_restore(self.h))
+
     def device_labels(self) -> int:
         p = c_void_p()
         self._check(self.lib.dmolp_batch_device_labels(self.h, byref(p)))
@@ -159,7 +165,8 @@ class Batch:
             results: bool = True):
         """Phase 2 on every instance.  Returns (list of per-instance dicts or None, device ms)."""
         cfg = self._cfg(mode, iterations, cap)
-        t = cabi.BatchTuning(**tuning) if tuning else None
+        shape = tuning or self.tuning  # an explicit shape, else the tuned (or cached) one, else the default
+        t = cabi.BatchTuning(**shape) if shape else None
         res = (cabi.BatchResult * self.num_instances)() if results else None
         ms = c_double()
         rc = self.lib.dmolp_batch_lp_run(self.h, byref(cfg), byref(t) if t else None, res, byref(ms))

@@ -28,7 +28,7 @@ EXPORTS = [
     "dmolp_find_seeds", "dmolp_expand_partitions", "dmolp_current_device", "dmolp_metrics_noalloc",
     "dmolp_batch_create", "dmolp_batch_destroy", "dmolp_batch_upload", "dmolp_batch_labels_set",
     "dmolp_batch_labels_get", "dmolp_batch_device_labels", "dmolp_batch_stream", "dmolp_batch_lp_run",
-    "dmolp_batch_autotune", "dmolp_batch_counts",
+    "dmolp_batch_autotune", "dmolp_batch_counts", "dmolp_batch_labels_save", "dmolp_batch_labels_restore",
 ]
 BATCH_MAX_K = 64
 
@@ -62,7 +62,7 @@ class BatchTuning(ctypes.Structure):
 
 class BatchResult(ctypes.Structure):
     _fields_ = [("edge_cut", c_int64), ("traversed_edges", c_uint64), ("arcs_read", c_uint64),
-                ("vertex_balance", c_double), ("edge_balance", c_double), ("iterations_run", c_int32),
+                ("vertex_visits", c_uint64), ("vertex_balance", c_double), ("edge_balance", c_double), ("iterations_run", c_int32),
                 ("stop_reason", c_int32), ("status", c_int32), ("changes", c_int32)]
 
 
@@ -116,4 +116,6 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_batch_lp_run.argtypes = [vp, POINTER(LpConfig), POINTER(BatchTuning), vp, POINTER(c_double)]
     lib.dmolp_batch_autotune.argtypes = [vp, POINTER(LpConfig), POINTER(BatchTuning), POINTER(c_double)]
     lib.dmolp_batch_counts.argtypes = [vp, c_int32, vp, vp]
+    lib.dmolp_batch_labels_save.argtypes = [vp]
+    lib.dmolp_batch_labels_restore.argtypes = [vp]
     return lib

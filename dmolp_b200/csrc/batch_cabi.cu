@@ -330,6 +330,20 @@ int dmolp_batch_labels_get(dmolp_batch *b, int32_t *labels) {
     return bsync(b);
 }
 
+int dmolp_batch_labels_save(dmolp_batch *b) {
+    if (!b || !b->has_graph) return fail(DMOLP_ERR_STATE, "no batch uploaded");
+    BCUDA(cudaSetDevice(b->device));
+    BCUDA(cudaMemcpyAsync(b->saved, b->a.label, b->nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, b->stream));
+    return DMOLP_OK;
+}
+
+int dmolp_batch_labels_restore(dmolp_batch *b) {
+    if (!b || !b->has_graph) return fail(DMOLP_ERR_STATE, "no batch uploaded");
+    BCUDA(cudaSetDevice(b->device));
+    BCUDA(cudaMemcpyAsync(b->a.label, b->saved, b->nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, b->stream));
+    return DMOLP_OK;
+}
+
 int dmolp_batch_device_labels(dmolp_batch *b, int32_t **labels) {
     if (!b || !b->has_graph) return fail(DMOLP_ERR_STATE, "no batch uploaded");
     if (!labels) return fail(DMOLP_ERR_ARG, "null output");
@@ -368,6 +382,7 @@ int dmolp_batch_lp_run(dmolp_batch *b, const dmolp_lp_config *cfg, const dmolp_b
         r.edge_cut = o.edge_cut;
         r.traversed_edges = (uint64_t)o.te;
         r.arcs_read = (uint64_t)o.arcs;
+        r.vertex_visits = (uint64_t)o.visits;
         r.iterations_run = o.iterations;
         r.stop_reason = o.stop_reason;
         r.status = o.status;

@@ -228,6 +228,7 @@ typedef struct {                   /* one per instance */
     int64_t edge_cut;
     uint64_t traversed_edges;      /* the same four terms as dmolp_lp_result */
     uint64_t arcs_read;            /* arcs this implementation read */
+    uint64_t vertex_visits;        /* vertex rows this implementation opened (offsets + own label) */
     double vertex_balance, edge_balance;
     int32_t iterations_run;
     int32_t stop_reason;
@@ -246,6 +247,8 @@ int dmolp_batch_upload(dmolp_batch *b, int32_t ninst, const int64_t *vstart, con
 /* Labels of all instances, int32[nv] in union order, values in [0, parts[i]). */
 int dmolp_batch_labels_set(dmolp_batch *b, const int32_t *labels);
 int dmolp_batch_labels_get(dmolp_batch *b, int32_t *labels);
+int dmolp_batch_labels_save(dmolp_batch *b);     /* device-side copy of the labels ... */
+int dmolp_batch_labels_restore(dmolp_batch *b);  /* ... put back (the autotuner overwrites the copy) */
 int dmolp_batch_device_labels(dmolp_batch *b, int32_t **labels);  /* device pointer to the labels */
 void *dmolp_batch_stream(dmolp_batch *b);              /* the batch's cudaStream_t */
 
