@@ -29,6 +29,10 @@ EXPORTS = [
     "dmolp_batch_create", "dmolp_batch_destroy", "dmolp_batch_upload", "dmolp_batch_labels_set",
     "dmolp_batch_labels_get", "dmolp_batch_device_labels", "dmolp_batch_stream", "dmolp_batch_lp_run",
     "dmolp_batch_autotune", "dmolp_batch_counts", "dmolp_batch_labels_save", "dmolp_batch_labels_restore",
+    "dmolp_mpnn_num_params", "dmolp_mpnn_create", "dmolp_mpnn_destroy", "dmolp_mpnn_set_params",
+    "dmolp_mpnn_get_params", "dmolp_mpnn_features", "dmolp_mpnn_set_features", "dmolp_mpnn_forward",
+    "dmolp_mpnn_prepare_training", "dmolp_mpnn_backward", "dmolp_mpnn_train_step", "dmolp_mpnn_decode",
+    "dmolp_batch_propose",
 ]
 BATCH_MAX_K = 64
 
@@ -118,4 +122,18 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_batch_counts.argtypes = [vp, c_int32, vp, vp]
     lib.dmolp_batch_labels_save.argtypes = [vp]
     lib.dmolp_batch_labels_restore.argtypes = [vp]
+    lib.dmolp_mpnn_num_params.argtypes = []
+    lib.dmolp_mpnn_num_params.restype = c_int64
+    lib.dmolp_mpnn_create.argtypes = [c_int, POINTER(vp)]
+    lib.dmolp_mpnn_destroy.argtypes = [vp]
+    lib.dmolp_mpnn_set_params.argtypes = [vp, vp]
+    lib.dmolp_mpnn_get_params.argtypes = [vp, vp]
+    lib.dmolp_mpnn_features.argtypes = [vp, vp, vp]
+    lib.dmolp_mpnn_set_features.argtypes = [vp, vp, vp]
+    lib.dmolp_mpnn_forward.argtypes = [vp, vp, vp]
+    lib.dmolp_mpnn_prepare_training.argtypes = [vp, vp]
+    lib.dmolp_mpnn_backward.argtypes = [vp, vp, vp, vp]
+    lib.dmolp_mpnn_train_step.argtypes = [vp, vp, vp, ctypes.c_float, POINTER(c_double)]
+    lib.dmolp_mpnn_decode.argtypes = [vp, vp, vp, vp]
+    lib.dmolp_batch_propose.argtypes = [vp, vp, vp]
     return lib

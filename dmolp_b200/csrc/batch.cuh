@@ -40,6 +40,20 @@ struct Args {
     int mode, iters, cap;
 };
 
+// What the other device modules (the learned proposal) need of a resident batch.
+struct View {
+    const int64_t *off;
+    const int32_t *col;
+    int32_t *label;
+    const Inst *inst;
+    const int32_t *order;
+    int ninst;
+    int64_t nv, narcs;
+    cudaStream_t stream;
+    int num_sms, device;
+};
+bool view(dmolp_batch *b, View *v);  // false when nothing is uploaded
+
 int occupancy(int nt, int td);
 bool launch(const Args &a, int nt, int td, int grid, cudaStream_t s);
 void prepare(const int64_t *off, int32_t *col, Inst *inst, int ninst, int *next, int *err, int grid, cudaStream_t s);

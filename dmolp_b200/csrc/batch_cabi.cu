@@ -155,6 +155,26 @@ void balance(const long long *vc, const long long *ec, int k, double *vb, double
 
 }  // namespace
 
+namespace dmolp {
+namespace batch {
+bool view(dmolp_batch *b, View *v) {
+    if (!b || !b->has_graph) return false;
+    v->off = b->a.off;
+    v->col = b->a.col;
+    v->label = b->a.label;
+    v->inst = b->inst;
+    v->order = b->order;
+    v->ninst = b->ninst;
+    v->nv = b->nv;
+    v->narcs = b->narcs;
+    v->stream = b->stream;
+    v->num_sms = b->num_sms;
+    v->device = b->device;
+    return true;
+}
+}  // namespace batch
+}  // namespace dmolp
+
 extern "C" {
 
 int dmolp_batch_create(int device, dmolp_batch **out) {

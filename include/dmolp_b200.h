@@ -261,6 +261,45 @@ int dmolp_batch_lp_run(dmolp_batch *b, const dmolp_lp_config *cfg, const dmolp_b
 /* Times every launch shape on the uploaded batch and its current labels (restored after each trial) and
  * keeps the fastest for later runs.  best / best_ms may be NULL. */
 int dmolp_batch_autotune(dmolp_batch *b, const dmolp_lp_config *cfg, dmolp_batch_tuning *best, double *best_ms);
+/* ---------------------------------------------------------------------------------------------------------
+ * Learned initial partition (no counterpart in the reference, whose phase 1 is BFS / hub seeding): a 3-layer
+ * mean-aggregation message-passing network, Z = [H | mean over neighbours of H] @ W + b per layer, widths
+ * 16 -> 64 -> 64 -> 16, BF16 weights and activations with FP32 accumulation on the tensor cores.  Inputs per
+ * vertex: degree / mean degree, log(1 + degree), 8 random-walk features (log landing probabilities of lazy
+ * walks from 8 farthest-point anchors, standardised per graph) and k / 64.  The 16-wide output embedding is
+ * turned into k balanced labels per graph by recursive coordinate bisection.  Trained with an
+ * edge-contrastive loss on final partitions of the plain method.  Works on a dmolp_batch; a graph the
+ * proposal cannot serve (fewer vertices than parts, a non-finite embedding, an empty part) is flagged so the
+ * caller seeds it with phase 1 instead.
+ * ------------------------------------------------------------------------------------------------------- */
+typedef struct dmolp_mpnn dmolp_mpnn;
+
+int64_t dmolp_mpnn_num_params(void);           /* length of the flat FP32 parameter vector */
+int dmolp_mpnn_create(int device, dmolp_mpnn **out);  /* Glorot-uniform weights from a fixed seed */
+int dmolp_mpnn_destroy(dmolp_mpnn *m);
+/* Parameters, flat FP32: per layer W [K x N] row-major then b [N]; K = 32, 128, 128; N = 64, 64, 16.
+ * Setting them resets the optimiser state. */
+int dmolp_mpnn_set_params(dmolp_mpnn *m, const float *params);
+int dmolp_mpnn_get_params(dmolp_mpnn *m, float *params);
+/* Input features of the batch's graphs, computed on the device; features[nv*16] (may be NULL) receives
+ * them before the BF16 rounding.  dmolp_mpnn_set_features installs features given by the caller instead. */
+int dmolp_mpnn_features(dmolp_mpnn *m, dmolp_batch *b, float *features);
+int dmolp_mpnn_set_features(dmolp_mpnn *m, dmolp_batch *b, const float *features);
+/* Forward pass on the current features; embedding[nv*16] (may be NULL). */
+int dmolp_mpnn_forward(dmolp_mpnn *m, dmolp_batch *b, float *embedding);
+/* Training needs the activations of every layer: call this before the features of a training batch. */
+int dmolp_mpnn_prepare_training(dmolp_mpnn *m, dmolp_batch *b);
+/* Backward of the last forward pass for an upstream gradient d_embedding[nv*16]; grads[num_params] out. */
+int dmolp_mpnn_backward(dmolp_mpnn *m, dmolp_batch *b, const float *d_embedding, float *grads);
+/* One Adam step (lr; beta 0.9 / 0.999) on the edge-contrastive loss against target labels target[nv]:
+ * mean over arcs (v,u) of |z_v - z_u|^2 when the targets agree, max(0, 1 - |z_v - z_u|^2) otherwise. */
+int dmolp_mpnn_train_step(dmolp_mpnn *m, dmolp_batch *b, const int32_t *target, float lr, double *loss);
+/* Labels from an embedding (NULL = the last forward pass) into the batch's labels; status[ninst] (may be
+ * NULL): 0 = proposal used, 1 = not usable (the graph keeps labels 0 and needs phase-1 seeding). */
+int dmolp_mpnn_decode(dmolp_mpnn *m, dmolp_batch *b, const float *embedding, int32_t *status);
+/* Features + forward + decode. */
+int dmolp_batch_propose(dmolp_batch *b, dmolp_mpnn *m, int32_t *status);
+
 /* Per-part vertex counts and intra-part edge counts of instance i after the last run (k entries each). */
 int dmolp_batch_counts(dmolp_batch *b, int32_t inst, int64_t *vertex_counts, int64_t *edge_counts);
 

@@ -195,3 +195,35 @@ def test_window_select_and_lp_apply_match_oracle(golden_cases, part):
         nodes, labs = part.lp_apply(k, pen, window)
         assert len(nodes) == t["changes"]
     assert np.array_equal(part.labels(), golden_arrays(name)["labels2_fixed"])
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built")
+def test_reference_gpu_kernel_agrees(part):
+    """The reference's own CUDA path (boundaryLPKernel_unified built unmodified for sm_100a, driven by its
+    run_phase2 loop) against the oracle and this build, on the same graphs and phase-1 labels."""
+    import os
+    import tempfile
+
+    from dmolp_b200 import graphs
+
+    rng = np.random.default_rng(77)
+    with tempfile.TemporaryDirectory() as td:
+        for trial in range(3):
+            n = int(rng.integers(800, 4000))
+            g = graphs.knn(n, int(rng.integers(2, 4)), int(rng.integers(6, 13)), int(rng.integers(1, 1000)))
+            k = int(rng.integers(2, 40))
+            o1 = oracle.phase1(g.offsets, g.indices, g.raw_deg(), k, 100)
+            txt = os.path.join(td, f"g{trial}.txt")
+            graphs.write_adjtext(g, txt)
+            lab = os.path.join(td, f"l{trial}.bin")
+            o1.labels.astype(np.int32).tofile(lab)
+            r = oracle.run_reference(txt, k, 100, os.path.join(td, f"o{trial}"), mode="fixed", iters=10, gpu=True,
+                                     labels_in=lab, seed_dump=False, timeout=600)
+            o2 = oracle.phase2(g.offsets, g.indices, o1.labels, k, "fixed", 10)
+            assert np.array_equal(r["labels2"], o2.labels), trial
+            assert r["result"]["edge_cut"] == o2.res.edge_cut
+            part.upload(g)
+            part.set_labels(o1.labels)
+            m = part.phase2(k, mode="fixed", iterations=10)
+            assert np.array_equal(part.labels(), r["labels2"]), trial
+            assert m.edge_cut == r["result"]["edge_cut"]
