@@ -24,7 +24,7 @@ namespace dmolp {
 namespace mpnn {
 namespace {
 
-constexpr uint32_t kWaitLimit = 1u << 24;  // polls of an mbarrier before a GEMM gives up (>> any real MMA)
+constexpr uint32_t kWaitLimit = 1u << 20;  // polls of an mbarrier before a GEMM gives up (>> any real MMA)
 
 __device__ __forceinline__ uint4 zero4() { return make_uint4(0, 0, 0, 0); }
 
@@ -197,7 +197,7 @@ __global__ void k_agg_bwd(const int64_t *__restrict__ off, const int32_t *__rest
         for (int64_t j = s; j < e; ++j) {
             const int v = __ldg(col + j);
             const int64_t dv = off[v + 1] - off[v];
-            const float inv = (float)(1.0 / (double)dv);
+            const float inv = dv > 0 ? (float)(1.0 / (double)dv) : 0.f;
             const float2 x = *reinterpret_cast<const float2 *>(dC + (size_t)v * 128 + 64 + 2 * lane);
             a0 = __fadd_rn(a0, __fmul_rn(x.x, inv));
             a1 = __fadd_rn(a1, __fmul_rn(x.y, inv));
