@@ -42,6 +42,8 @@ WORKLOADS = {
     # 2048 graphs, V log-uniform in [1K, 200K], half k-NN 2-D/3-D (k_nn 8..14), half preferential attachment
     # (m 4..8), k uniform in 2..64; phase 2 with the reference's stopping rules from phase-1 partitions
     "batch2048": dict(kind="batch", n=2048, seed=11, vmin=1000, vmax=200_000, theta=1000),
+    # the same mix, 256 graphs (profiling and quick checks)
+    "batch256": dict(kind="batch", n=256, seed=11, vmin=1000, vmax=200_000, theta=1000),
 }
 
 
@@ -415,8 +417,9 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
 
 # ------------------------------------------------------------------------------------------- CPU baselines
 def reference_cpu_run(g, labels1, w, repeats: int, iters: int, threads: int, timeout: float = 900,
-                      mode: str = "fixed"):
-    """The reference's own phase-2 code (oracle/_ref, built from its sources) on the host cores."""
+                      mode: str = "fixed", gpu: bool = False):
+    """The reference's own phase-2 code (oracle/_ref, built from its sources) on the host cores; with gpu=True
+    its own CUDA path (boundaryLPKernel_unified, built unmodified for sm_100a) instead of the CPU kernel."""
     import oracle
 
     with tempfile.TemporaryDirectory() as td:
@@ -428,7 +431,7 @@ def reference_cpu_run(g, labels1, w, repeats: int, iters: int, threads: int, tim
         labels1.astype(np.int32).tofile(lab)
         cmd = [oracle.REF_HARNESS, txt, str(w["k"]), str(w["theta"]), "--out", os.path.join(td, "o"), "--mode",
                mode, "--iters", str(iters), "--threads", str(threads), "--labels-in", lab, "--no-seed-dump",
-               "--repeat", str(repeats)]
+               "--repeat", str(repeats)] + (["--gpu"] if gpu else [])
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         pr = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
         if pr.returncode != 0:
@@ -457,8 +460,16 @@ def cpu_baseline(g, labels1, w, args) -> dict:
     if oracle.reference_available():
         reps = reference_cpu_run(g, labels1, w, 1, iters, threads)
         r = reps[-1]
-        return {"value": r["te_total"] / r["lp_seconds"], "unit": "TE/s", "cores": threads, "kind": "reference",
-                "sample": sample, "seconds": r["lp_seconds"]}
+        out = {"value": r["te_total"] / r["lp_seconds"], "unit": "TE/s", "cores": threads, "kind": "reference",
+               "sample": sample, "seconds": r["lp_seconds"]}
+        try:  # the reference's own GPU path on the same B200, same sample
+            rg = reference_cpu_run(g, labels1, w, 1, iters, threads, gpu=True)[-1]
+            out["reference_gpu"] = {"value": rg["te_total"] / rg["lp_seconds"], "unit": "TE/s", "sample": sample,
+                                    "seconds": rg["lp_seconds"],
+                                    "kind": "reference run_phase2 loop with its boundaryLPKernel_unified (sm_100a)"}
+        except Exception as e:  # report, do not hide
+            out["reference_gpu"] = {"error": str(e)[:300]}
+        return out
     r = port_cpu_run(g, labels1, w, iters)
     return {"value": r["te_total"] / r["lp_seconds"], "unit": "TE/s", "cores": 1, "kind": "port",
             "sample": sample, "seconds": r["lp_seconds"]}
