@@ -325,6 +325,7 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     ALLOC(b.label, n);
     ALLOC(b.stamp, n);
     ALLOC(b.sstamp, n);
+    ALLOC(b.ndiff, n);
     ALLOC(b.cand, n);
     ALLOC(b.win[0], n);
     ALLOC(b.win[1], n);
@@ -738,6 +739,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.stamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.sstamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.ndiff, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
     lp_reset_stats(c, k, nullptr);
     lp_stats(c, k, nullptr, nullptr);
     lp_init_end(c, cfg->mode);
@@ -782,8 +784,9 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     }
     if (c->profiling) {
         // Algorithmic bytes per launch of the design (ids and labels are 4 B, offsets 8 B):
-        //  bnd    : bucket ids (+ stamps after t = 1) of every vertex with arcs, offsets + own label of each
-        //           candidate, id + label of each arc read before the first differing one, 21 B per record
+        //  bnd    : record slot (ball id, stamp, selection flag) of every vertex with arcs, offsets +
+        //           boundary count of each candidate, id + window stamp per arc of a pull-mode walk, own
+        //           label per boundary record
         //  decide : list id + offsets + own label per selected vertex, id + label per arc, 8 B per mover
         //  mark   : list id + offsets per window vertex, id read + stamp write per arc
         //  update : offsets + labels per mover, id + label + pending label per arc

@@ -128,8 +128,10 @@ __device__ __forceinline__ void put_slot(const Buffers &b, int pos, bool isb, in
 }
 
 // Candidacy: t = 1 every vertex; push mode stamp[v] == t (set by k_mark); pull mode v is in the previous
-// window (sstamp == t-1) or has a neighbour that is, found while the same row walk looks for a
-// differently-labelled neighbour.  The walk stops once both answers are known.
+// window (sstamp == t-1) or has a neighbour that is.  A candidate is on the boundary when it has a
+// differently-labelled neighbour: ndiff[v] > 0, a count kept exact by the statistics pass and by k_update
+// (symmetric graphs) or by the full pass after every move (other graphs).  So only pull-mode candidacy
+// walks rows; at t = 1 and in push mode every record slot costs a handful of per-vertex reads.
 __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
     if (b.ctrl->stopped) return;
     extern __shared__ int s_npart[];  // [k] boundary records per label in this block
@@ -139,135 +141,92 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
     const int tp = a.t - 1;
     const int lane = threadIdx.x & 31;
     unsigned long long te = 0, rd = 0, nc = 0, nbd = 0;
-    if ((int)blockIdx.x < a.g0) {
-        // ---- thread per vertex (deg <= kSmallDeg): every neighbour id is loaded first, then labels (and
-        //      window stamps) in independent groups of 4 ----
+    auto finish = [&](int pos, int v, bool cand, int deg) {
+        const bool isb = cand && b.ndiff[v] > 0;
+        int own = 0;
+        if (cand) {
+            ++nc;
+            te += (unsigned long long)deg;
+        }
+        if (isb) {
+            own = b.label[v];
+            ++nbd;
+            atomicAdd(&s_npart[own], 1);
+        }
+        put_slot(b, pos, isb, own, isb ? sel_key(b, own, deg, v, a.ibits, a.maxdeg) : 0);
+    };
+    if (!pull) {
+        // ---- every record slot, thread per slot ----
+        const int n = a.nb0 + a.nb1 + a.nb2;
+        for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += gridDim.x * blockDim.x) {
+            const int v = b.ball[pos];
+            const bool cand = a.all || b.stamp[v] == a.t;
+            finish(pos, v, cand, cand ? (int)(b.off[v + 1] - b.off[v]) : 0);
+        }
+    } else if ((int)blockIdx.x < a.g0) {
+        // ---- pull, thread per vertex (deg <= kSmallDeg): window stamps of the row, 4 at a time ----
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
             const int v = b.bucket[0][i];
-            bool cand = a.all || (pull ? b.sstamp[v] == tp : b.stamp[v] == a.t);
-            bool isb = false;
-            int own = 0, deg = 0;
-            if (cand || pull) {
-                own = b.label[v];
-                const int64_t s = b.off[v];
-                deg = (int)(b.off[v + 1] - s);
-                int u[kSmallDeg];
-#pragma unroll
-                for (int j = 0; j < kSmallDeg; ++j) u[j] = j < deg ? __ldg(b.col + s + j) : 0;
-                // groups of 4 neighbours: their label (and window-stamp) gathers are independent; stop once
-                // both the boundary and the candidacy answers are known
-                bool fs = false;
+            bool cand = b.sstamp[v] == tp;
+            const int64_t s = b.off[v];
+            const int deg = (int)(b.off[v + 1] - s);
+            if (!cand) {
                 int j = 0;
-#pragma unroll
-                for (int j0 = 0; j0 < kSmallDeg; j0 += 4) {
-                    if (j0 >= deg || (isb && (cand || fs))) break;
+                for (; j < deg && !cand; j += 4) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q)
-                        if (j0 + q < deg) {
-                            isb |= b.label[u[j0 + q]] != own;
-                            if (!cand && !fs) fs |= b.sstamp[u[j0 + q]] == tp;
-                        }
-                    j = j0 + 4 < deg ? j0 + 4 : deg;
+                        if (j + q < deg) cand |= b.sstamp[__ldg(b.col + s + j + q)] == tp;
                 }
-                rd += j;
-                cand = cand || fs;
-                isb = isb && cand;
-                if (cand) {
-                    ++nc;
-                    te += deg;
-                }
+                rd += (unsigned long long)(j < deg ? j : deg);
             }
-            if (isb) {
-                ++nbd;
-                atomicAdd(&s_npart[own], 1);
-            }
-            put_slot(b, i, isb, own, isb ? sel_key(b, own, deg, v, a.ibits, a.maxdeg) : 0);
+            finish(i, v, cand, deg);
         }
     } else if ((int)blockIdx.x < a.g0 + a.g1) {
-        // ---- warp per vertex ----
+        // ---- pull, warp per vertex ----
         const int wpb = blockDim.x >> 5;
         const int gw = ((int)blockIdx.x - a.g0) * wpb + (threadIdx.x >> 5), nw = a.g1 * wpb;
         for (int i = gw; i < a.nb1; i += nw) {
             const int pos = a.nb0 + i;
             const int v = b.bucket[1][i];
-            const bool cand0 = a.all || (pull ? b.sstamp[v] == tp : b.stamp[v] == a.t);
-            bool isb = false, cand = cand0;
-            int own = 0;
-            int64_t s = 0, e = 0;
-            if (cand0 || pull) {  // warp-uniform
-                own = b.label[v];
-                s = b.off[v];
-                e = b.off[v + 1];
-                bool diff = false, fs = false;
-                const int64_t r = warp_row(b.col, s, e, lane, [&](int u) {
-                    if (!cand0) fs |= (b.sstamp[u] == tp);
-                    diff |= (b.label[u] != own);
-                }, [&] {
-                    const bool c = cand0 || __any_sync(DMOLP_FULL_MASK, fs);
-                    return __any_sync(DMOLP_FULL_MASK, diff) && c;
-                });
-                cand = cand0 || __any_sync(DMOLP_FULL_MASK, fs);
-                isb = cand && __any_sync(DMOLP_FULL_MASK, diff);
-                if (lane == 0) {
-                    rd += (unsigned long long)r;
-                    if (cand) {
-                        ++nc;
-                        te += (unsigned long long)(e - s);
-                    }
-                }
+            const bool cand0 = b.sstamp[v] == tp;
+            const int64_t s = b.off[v], e = b.off[v + 1];
+            bool cand = cand0;
+            if (!cand0) {  // warp-uniform
+                bool fs = false;
+                const int64_t r = warp_row(b.col, s, e, lane, [&](int u) { fs |= (b.sstamp[u] == tp); },
+                                           [&] { return __any_sync(DMOLP_FULL_MASK, fs); });
+                cand = __any_sync(DMOLP_FULL_MASK, fs);
+                if (lane == 0) rd += (unsigned long long)r;
             }
-            if (lane == 0) {
-                if (isb) {
-                    ++nbd;
-                    atomicAdd(&s_npart[own], 1);
-                }
-                put_slot(b, pos, isb, own, isb ? sel_key(b, own, (int)(e - s), v, a.ibits, a.maxdeg) : 0);
-            }
+            if (lane == 0) finish(pos, v, cand, (int)(e - s));
         }
     } else {
-        // ---- block per vertex (deg > kLargeDeg) ----
+        // ---- pull, block per vertex (deg > kLargeDeg) ----
         const int gb = (int)blockIdx.x - a.g0 - a.g1, nbk = (int)gridDim.x - a.g0 - a.g1;
         for (int i = gb; i < a.nb2; i += nbk) {
             const int pos = a.nb0 + a.nb1 + i;
             const int v = b.bucket[2][i];
-            const bool cand0 = a.all || (pull ? b.sstamp[v] == tp : b.stamp[v] == a.t);
-            bool isb = false, cand = cand0;
-            int own = 0;
-            int64_t s = 0, e = 0, j0 = 0;
-            if (cand0 || pull) {  // block-uniform
-                own = b.label[v];
-                s = b.off[v];
-                e = b.off[v + 1];
-                bool diff = false, fs = false;
+            const bool cand0 = b.sstamp[v] == tp;
+            const int64_t s = b.off[v], e = b.off[v + 1];
+            bool cand = cand0;
+            int64_t j0 = s;
+            if (!cand0) {  // block-uniform
                 for (j0 = s; j0 < e; j0 += blockDim.x * 4) {
+                    bool fs = false;
                     for (int q = 0; q < 4; ++q) {
                         const int64_t j = j0 + q * blockDim.x + threadIdx.x;
-                        if (j < e) {
-                            const int u = __ldcs(b.col + j);
-                            if (!cand0) fs |= (b.sstamp[u] == tp);
-                            diff |= (b.label[u] != own);
-                        }
+                        if (j < e) fs |= (b.sstamp[__ldcs(b.col + j)] == tp);
                     }
-                    const bool c = cand0 || __syncthreads_or(fs);
-                    if (__syncthreads_or(diff) && c) {
+                    if (__syncthreads_or(fs)) {
+                        cand = true;
                         j0 += blockDim.x * 4;
                         break;
                     }
                 }
-                cand = cand0 || __syncthreads_or(fs);
-                isb = cand && __syncthreads_or(diff);
             }
             if (threadIdx.x == 0) {
-                if (cand0 || pull) rd += (unsigned long long)((j0 < e ? j0 : e) - s);
-                if (cand) {
-                    ++nc;
-                    te += (unsigned long long)(e - s);
-                }
-                if (isb) {
-                    ++nbd;
-                    atomicAdd(&s_npart[own], 1);
-                }
-                put_slot(b, pos, isb, own, isb ? sel_key(b, own, (int)(e - s), v, a.ibits, a.maxdeg) : 0);
+                if (!cand0) rd += (unsigned long long)((j0 < e ? j0 : e) - s);
+                finish(pos, v, cand, (int)(e - s));
             }
             __syncthreads();
         }
@@ -528,6 +487,7 @@ __global__ void k_update(Buffers b, int k, int t) {
         const int a = b.label[v], c = b.newlab[v];
         const int64_t s = b.off[v], e = b.off[v + 1];
         long long in_c = 0, out_a = 0, dc = 0;
+        int dv = 0;
         warp_row(b.col, s, e, lane, [&](int u) {
             const int lo = b.label[u];
             const int nu = b.newlab[u];
@@ -536,11 +496,18 @@ __global__ void k_update(Buffers b, int k, int t) {
             dc += w * ((int)(c != ln) - (int)(a != lo));
             in_c += w * (int)(c == ln);
             out_a += w * (int)(a == lo);
+            // differently-labelled neighbour counts: arc (u,v) seen from u; arc (v,u) from v when u stays
+            // (a moving u updates v's count from its own row)
+            const int du = (int)(ln != c) - (int)(lo != a);
+            if (du) atomicAdd(&b.ndiff[u], du);
+            if (nu < 0) dv += (int)(c != lo) - (int)(a != lo);
         }, [] { return false; });
         for (int o = 16; o > 0; o >>= 1) {
             in_c += __shfl_xor_sync(DMOLP_FULL_MASK, in_c, o);
             out_a += __shfl_xor_sync(DMOLP_FULL_MASK, out_a, o);
+            dv += __shfl_xor_sync(DMOLP_FULL_MASK, dv, o);
         }
+        if (lane == 0 && dv) atomicAdd(&b.ndiff[v], dv);
         dcut += dc;
         if (lane == 0) {
             rd += (unsigned long long)(e - s);
@@ -611,6 +578,7 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
                 diff += (lu != lv);
             }
             cut += diff;
+            b.ndiff[v] = (int)diff;
             if (same && (unsigned)lv < (unsigned)k) atomicAdd(&sin[lv], (unsigned long long)same);
         }
     } else if (bx < a.gv + a.g0 + a.g1) {
@@ -632,10 +600,12 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
             }
             if (lane == 0) {
                 cut += diff;
+                b.ndiff[v] = (int)diff;
                 if (same && (unsigned)lv < (unsigned)k) atomicAdd(&sin[lv], (unsigned long long)same);
             }
         }
     } else {
+        __shared__ unsigned int s_diff[8];
         const int gb = bx - a.gv - a.g0 - a.g1, nbk = (int)gridDim.x - a.gv - a.g0 - a.g1;
         for (int i = gb; i < a.nb2; i += nbk) {
             const int v = b.bucket[2][i];
@@ -649,8 +619,19 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
                 diff += (lu != lv);
             }
             cut += diff;
-            for (int o = 16; o > 0; o >>= 1) same += __shfl_xor_sync(DMOLP_FULL_MASK, same, o);
+            for (int o = 16; o > 0; o >>= 1) {
+                same += __shfl_xor_sync(DMOLP_FULL_MASK, same, o);
+                diff += __shfl_xor_sync(DMOLP_FULL_MASK, diff, o);
+            }
             if (lane == 0 && same && (unsigned)lv < (unsigned)k) atomicAdd(&sin[lv], (unsigned long long)same);
+            if (lane == 0) s_diff[wib] = diff;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned int t = 0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_diff[w];
+                b.ndiff[v] = (int)t;
+            }
+            __syncthreads();
         }
     }
     cut = warp_sum_u64(cut);
