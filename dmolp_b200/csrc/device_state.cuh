@@ -16,6 +16,8 @@ namespace dmolp {
 
 // Degree classes of the bucketed kernels: thread per vertex, warp per vertex, block per vertex.
 constexpr int kSmallDeg = 16;    // deg <= 16: one thread walks the row
+constexpr int kDecSmall = 32;    // LP decisions: rows of at most 32 arcs are counted by one thread ...
+constexpr int kDecSmallK = 64;   // ... when at most 64 labels are scored (byte counters in shared memory)
 constexpr int kLargeDeg = 4096;  // deg > 4096: one block walks the row
 constexpr int kChunk = 4096;     // row chunk of the window-marking kernel
 constexpr int kHubChunk = 2048;  // row chunk of the decisions of deg > kLargeDeg vertices

@@ -276,6 +276,14 @@ __device__ __forceinline__ int block_append(int *gctr, bool pred, int *s_tmp) {
     return pred ? s_tmp[1] + wb + __popc(m & ((1u << lane) - 1)) : -1;
 }
 
+// Decision class of a selected vertex: 0 thread (short row, own label scored, at most kDecSmallK labels),
+// 1 warp, 2 hub (row split into chunks).  A vertex whose own label is not scored goes to the warp class,
+// whose histogram also sees absent labels.
+__device__ __forceinline__ int dec_class(int deg, int own, int eff) {
+    if (deg > kLargeDeg) return 2;
+    return (deg > kDecSmall || (unsigned)own >= (unsigned)eff || eff > kDecSmallK) ? 1 : 0;
+}
+
 // Selected record slots: next window (for marking) and decision class.  A vertex whose own label is not
 // scored (>= eff) goes to the warp class, whose histogram also sees absent labels.
 __global__ void __launch_bounds__(256) k_split(Buffers b, int t, int eff) {
@@ -293,7 +301,7 @@ __global__ void __launch_bounds__(256) k_split(Buffers b, int t, int eff) {
             b.sstamp[v] = t;
             const int deg = (int)(b.off[v + 1] - b.off[v]);
             te += (unsigned long long)deg;
-            cls = deg > kLargeDeg ? 2 : ((deg > kSmallDeg || b.bown[i] >= eff) ? 1 : 0);
+            cls = dec_class(deg, b.bown[i], eff);
         }
         const int slot = block_append(&b.cnt->nwin[t & 1], take, s_tmp);
         if (take) win[slot] = v;
@@ -327,38 +335,46 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
     int *h = shist + wib * (priv ? 1024 : eff);
     unsigned long long rd = 0;
     if ((int)blockIdx.x < a.g0) {
-        // ---- thread per vertex: deg <= 16 and own label < eff; only present labels can beat the own raw
-        //      count (an absent label scores 0 <= count[own]) ----
+        // ---- thread per vertex: deg <= kDecSmall, own label scored, eff <= kDecSmallK.  Label counts are
+        //      bytes in this thread's column of shared memory (word w of thread t at shist[w * 256 + t]: four
+        //      labels per word, conflict-free); a 64-bit mask lists the labels seen, and only those are scored
+        //      -- an absent label scores 0 <= count[own] and cannot win ----
+        uint32_t *cw = reinterpret_cast<uint32_t *>(shist) + threadIdx.x;
+        for (int w = 0; w < kDecSmallK / 4; ++w) cw[w * kBlock] = 0u;
         const int n = b.cnt->ndec[0];
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += a.g0 * blockDim.x) {
             const int v = b.dec[0][i];
             const int own = b.label[v];
             const int64_t s = b.off[v];
             const int deg = (int)(b.off[v + 1] - s);
-            int l[kSmallDeg];
-#pragma unroll
-            for (int j = 0; j < kSmallDeg; ++j) l[j] = j < deg ? b.label[__ldg(b.col + s + j)] : -1;
             rd += deg;
-            int own_cnt = 0;
+            unsigned long long seen = 0ull;
+            for (int j = 0; j < deg; j += 4) {
+                int l[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) l[q] = j + q < deg ? b.label[__ldg(b.col + s + j + q)] : -1;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if ((unsigned)l[q] < (unsigned)eff) {
+                        cw[(l[q] >> 2) * kBlock] += 1u << ((l[q] & 3) * 8);
+                        seen |= 1ull << l[q];
+                    }
+            }
+            const int own_cnt = (int)((cw[(own >> 2) * kBlock] >> ((own & 3) * 8)) & 0xFFu);
             double best = -DBL_MAX;
             int bkey = 0x7fffffff, blab = -1;
-#pragma unroll
-            for (int j = 0; j < kSmallDeg; ++j) {
-                own_cnt += (l[j] == own);
-                const int c = l[j];
-                if ((unsigned)c < (unsigned)eff) {
-                    int cnt = 0;
-#pragma unroll
-                    for (int q = 0; q < kSmallDeg; ++q) cnt += (l[q] == c);
-                    const double sc = __dmul_rn((double)cnt, b.tpen[c]);
-                    const int key = tiekey(c);
-                    if (better(sc, key, best, bkey)) {
-                        best = sc;
-                        bkey = key;
-                        blab = c;
-                    }
+            for (unsigned long long m = seen; m; m &= m - 1) {
+                const int c = __ffsll((long long)m) - 1;
+                const int cnt = (int)((cw[(c >> 2) * kBlock] >> ((c & 3) * 8)) & 0xFFu);
+                const double sc = __dmul_rn((double)cnt, b.tpen[c]);
+                const int key = tiekey(c);
+                if (better(sc, key, best, bkey)) {
+                    best = sc;
+                    bkey = key;
+                    blab = c;
                 }
             }
+            for (unsigned long long m = seen; m; m &= m - 1) cw[((__ffsll((long long)m) - 1) >> 2) * kBlock] = 0u;
             if (blab >= 0 && best > (double)own_cnt && blab != own) park_move(b, v, blab);
         }
     } else if ((int)blockIdx.x < a.g0 + a.g1) {
@@ -772,7 +788,7 @@ __global__ void k_classify(Buffers b, int n, int eff) {
             v = b.cand[i];
             const int deg = (int)(b.off[v + 1] - b.off[v]);
             const int own = b.label[v];
-            cls = deg > kLargeDeg ? 2 : ((deg > kSmallDeg || (unsigned)own >= (unsigned)eff) ? 1 : 0);
+            cls = dec_class(deg, own, eff);
         }
         for (int c = 0; c < 3; ++c) {
             const int s2 = warp_append(&b.cnt->ndec[c], cls == c);
@@ -858,8 +874,10 @@ DecArgs dec_args(dmolp_ctx *c, int t, int eff) {
 int dec_grid(dmolp_ctx *c, const DecArgs &a) { return a.g0 + a.g1 + c->num_sms * 2; }
 
 size_t dec_smem(int eff) {
-    return eff <= 32 ? (size_t)(kWarpsPerBlock * 1024 + kWarpsPerBlock * 32) * sizeof(int)
-                     : (size_t)kWarpsPerBlock * eff * sizeof(int);
+    const size_t warp = eff <= 32 ? (size_t)(kWarpsPerBlock * 1024 + kWarpsPerBlock * 32) * sizeof(int)
+                                  : (size_t)kWarpsPerBlock * eff * sizeof(int);
+    const size_t thread = (size_t)(kDecSmallK / 4) * kBlock * sizeof(uint32_t);  // byte counters
+    return warp > thread ? warp : thread;
 }
 
 StatsArgs stats_args(dmolp_ctx *c, int k) {
