@@ -29,6 +29,7 @@ struct Args {
     const int64_t *off;
     const int32_t *col;
     int32_t *label, *newlab, *cstamp;
+    int32_t *ndiff;  // neighbours with another label, exact at every iteration start
     int32_t *l_cand, *l_bnd, *l_act, *l_win0, *l_win1;  // per-instance slices at vbase
     const Inst *inst;
     const int32_t *order;

@@ -233,7 +233,7 @@ int dmolp_batch_upload(dmolp_batch *b, int32_t ninst, const int64_t *vstart, con
     BCUDA(cudaStreamSynchronize(b->stream));
     free_all(b);
     Args &a = b->a;
-    int32_t *label = nullptr, *newlab = nullptr, *cstamp = nullptr, *lc = nullptr, *lb = nullptr, *la = nullptr,
+    int32_t *label = nullptr, *newlab = nullptr, *cstamp = nullptr, *ndiff = nullptr, *lc = nullptr, *lb = nullptr, *la = nullptr,
             *w0 = nullptr, *w1 = nullptr, *col = nullptr, *order = nullptr, *saved = nullptr;
     int64_t *off = nullptr;
     Inst *inst = nullptr;
@@ -246,6 +246,7 @@ int dmolp_batch_upload(dmolp_batch *b, int32_t ninst, const int64_t *vstart, con
     BTRY(balloc(b, &label, nv));
     BTRY(balloc(b, &newlab, nv));
     BTRY(balloc(b, &cstamp, nv));
+    BTRY(balloc(b, &ndiff, nv));
     BTRY(balloc(b, &lc, nv));
     BTRY(balloc(b, &lb, nv));
     BTRY(balloc(b, &la, nv));
@@ -291,6 +292,7 @@ int dmolp_batch_upload(dmolp_batch *b, int32_t ninst, const int64_t *vstart, con
     BCUDA(cudaMemsetAsync(label, 0, nv * sizeof(int32_t), s));
     BCUDA(cudaMemsetAsync(newlab, 0xff, nv * sizeof(int32_t), s));
     BCUDA(cudaMemsetAsync(cstamp, 0, nv * sizeof(int32_t), s));
+    BCUDA(cudaMemsetAsync(ndiff, 0, nv * sizeof(int32_t), s));
     BCUDA(cudaMemsetAsync(ctr, 0, 4 * sizeof(int), s));
     prepare(off, col, inst, ninst, ctr, ctr + 2, b->num_sms * 4, s);
     BTRY(bsync(b));
@@ -306,6 +308,7 @@ int dmolp_batch_upload(dmolp_batch *b, int32_t ninst, const int64_t *vstart, con
     a.label = label;
     a.newlab = newlab;
     a.cstamp = cstamp;
+    a.ndiff = ndiff;
     a.l_cand = lc;
     a.l_bnd = lb;
     a.l_act = la;

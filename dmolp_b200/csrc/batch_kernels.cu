@@ -105,6 +105,7 @@ __device__ void full_stats(const Args &a, const Inst &I, Smem<NT> &sm) {
               atomicAdd((unsigned long long *)&sm.vc[lv], 1ull);
               if (same) atomicAdd((unsigned long long *)&sm.intra[lv], (unsigned long long)same);
               cut += diff;
+              a.ndiff[v] = diff;
           },
           [&](int v, int64_t s, int64_t e) {
               const int lv = a.label[v];
@@ -125,6 +126,7 @@ __device__ void full_stats(const Args &a, const Inst &I, Smem<NT> &sm) {
                       atomicAdd((unsigned long long *)&sm.vc[lv], 1ull);
                       if (same) atomicAdd((unsigned long long *)&sm.intra[lv], (unsigned long long)same);
                       cut += diff;
+                      a.ndiff[v] = diff;
                   }
               }
           });
@@ -211,50 +213,29 @@ __device__ void run_instance(const Args &a, const int ii, Smem<NT> &sm) {
                   });
             __syncthreads();
         }
-        // ---- boundary test: a neighbour with another label (gpu_lp_boundary.cu:216-236) ----
+        // ---- boundary test: a neighbour with another label (gpu_lp_boundary.cu:216-236), i.e. ndiff > 0 ----
         {
             const int n = t == 1 ? I.nv : sm.ncand;
             unsigned long long tec = 0;
-            visit(a, n, [&](int i) { return t == 1 ? (int)I.vbase + i : cand[i]; },
-                  [&](int, int64_t s, int64_t e) { return e - s > TD; },
-                  [&](bool act, int v, int64_t s, int64_t e) {
-                      bool isb = false;
-                      int own = 0;
-                      if (act) {
-                          own = a.label[v];
-                          tec += (unsigned long long)(e - s);
-                          ++visits;
-                          int64_t j = s;
-                          for (; j < e; ++j)
-                              if (a.label[__ldg(a.col + j)] != own) {
-                                  isb = true;
-                                  ++j;
-                                  break;
-                              }
-                          arcs += (unsigned long long)(j - s);
-                      }
-                      const int slot = warp_push(&sm.nbnd, isb);
-                      if (isb) {
-                          bnd[slot] = v;
-                          atomicAdd(&sm.bcnt[own], 1);
-                      }
-                  },
-                  [&](int v, int64_t s, int64_t e) {
-                      const int own = a.label[v];
-                      bool f = false;
-                      const int64_t rd = warp_row(a.col, s, e, lane, [&](int u) { f |= a.label[u] != own; },
-                                                  [&] { return __any_sync(DMOLP_FULL_MASK, f); });
-                      const bool isb = __any_sync(DMOLP_FULL_MASK, f);
-                      if (lane == 0) {
-                          tec += (unsigned long long)(e - s);
-                          ++visits;
-                          arcs += (unsigned long long)rd;
-                          if (isb) {
-                              bnd[atomicAdd(&sm.nbnd, 1)] = v;
-                              atomicAdd(&sm.bcnt[own], 1);
-                          }
-                      }
-                  });
+            for (int i0 = (int)(threadIdx.x & ~31u); i0 < n; i0 += blockDim.x) {
+                const int i = i0 + lane;
+                bool isb = false;
+                int own = 0, v = 0;
+                if (i < n) {
+                    v = t == 1 ? (int)I.vbase + i : cand[i];
+                    tec += (unsigned long long)(a.off[v + 1] - a.off[v]);
+                    ++visits;
+                    if (a.ndiff[v] > 0) {
+                        isb = true;
+                        own = a.label[v];
+                    }
+                }
+                const int slot = warp_push(&sm.nbnd, isb);
+                if (isb) {
+                    bnd[slot] = v;
+                    atomicAdd(&sm.bcnt[own], 1);
+                }
+            }
             tec = warp_sum_u64(tec);
             if (lane == 0 && tec) atomicAdd(&sm.te_cand, tec);
         }
@@ -454,7 +435,9 @@ __device__ void run_instance(const Args &a, const int ii, Smem<NT> &sm) {
         // ---- incremental cut / balance update from the movers (symmetric graphs) ----
         if (I.symmetric && nmov > 0) {
             long long dcut = 0;
-            auto upd = [&](int v, int u, long long &dc, long long &in_c, long long &out_a) {
+            // cut / intra counts, and the differently-labelled neighbour counts: arc (u,v) seen from u, arc
+            // (v,u) from v when u stays (a moving u updates v's count from its own row)
+            auto upd = [&](int v, int u, long long &dc, long long &in_c, long long &out_a, int &dv) {
                 const int a0 = a.label[v], c = a.newlab[v];
                 const int lo = a.label[u], nu = a.newlab[u];
                 const int ln = nu >= 0 ? nu : lo;
@@ -462,12 +445,17 @@ __device__ void run_instance(const Args &a, const int ii, Smem<NT> &sm) {
                 dc += w * ((int)(c != ln) - (int)(a0 != lo));
                 in_c += w * (int)(c == ln);
                 out_a += w * (int)(a0 == lo);
+                const int du = (int)(ln != c) - (int)(lo != a0);
+                if (du) atomicAdd(&a.ndiff[u], du);
+                if (nu < 0) dv += (int)(c != lo) - (int)(a0 != lo);
             };
             visit(a, nmov, [&](int i) { return mov[i]; }, [&](int, int64_t s, int64_t e) { return e - s > TD; },
                   [&](bool act, int v, int64_t s, int64_t e) {
                       if (!act) return;
                       long long in_c = 0, out_a = 0;
-                      for (int64_t j = s; j < e; ++j) upd(v, __ldg(a.col + j), dcut, in_c, out_a);
+                      int dv = 0;
+                      for (int64_t j = s; j < e; ++j) upd(v, __ldg(a.col + j), dcut, in_c, out_a, dv);
+                      if (dv) atomicAdd(&a.ndiff[v], dv);
                       arcs += (unsigned long long)(e - s);
                       ++visits;
                       const int a0 = a.label[v], c = a.newlab[v];
@@ -478,11 +466,14 @@ __device__ void run_instance(const Args &a, const int ii, Smem<NT> &sm) {
                   },
                   [&](int v, int64_t s, int64_t e) {
                       long long in_c = 0, out_a = 0, dc = 0;
-                      warp_row(a.col, s, e, lane, [&](int u) { upd(v, u, dc, in_c, out_a); }, [] { return false; });
+                      int dv = 0;
+                      warp_row(a.col, s, e, lane, [&](int u) { upd(v, u, dc, in_c, out_a, dv); }, [] { return false; });
                       for (int o = 16; o > 0; o >>= 1) {
                           in_c += __shfl_xor_sync(DMOLP_FULL_MASK, in_c, o);
                           out_a += __shfl_xor_sync(DMOLP_FULL_MASK, out_a, o);
+                          dv += __shfl_xor_sync(DMOLP_FULL_MASK, dv, o);
                       }
+                      if (lane == 0 && dv) atomicAdd(&a.ndiff[v], dv);
                       dcut += dc;
                       if (lane == 0) {
                           arcs += (unsigned long long)(e - s);
