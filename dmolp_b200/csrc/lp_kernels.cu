@@ -326,7 +326,7 @@ __device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
     b.mov[q] = v;
 }
 
-__global__ void __launch_bounds__(256, 6) k_decide(Buffers b, DecArgs a) {
+__global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
     if (b.ctrl->stopped) return;
     extern __shared__ int shist[];  // eff <= 32: 8 warps x 32x32 private counters + 8x32 totals; else 8 x eff
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
