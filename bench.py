@@ -37,6 +37,9 @@ WORKLOADS = {
                        iters=30),
     "rmat22-k64": dict(kind="rmat", scale=22, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=7, k=64, theta=10000,
                        iters=30),
+    # R-MAT scale 26, edge factor 24 (67.1 M vertices, ~3.2 B arcs), k = 64, 40 LP iterations
+    "rmat26": dict(kind="rmat", scale=26, edge_factor=24, a=0.57, b=0.19, c=0.19, seed=7, k=64, theta=10000,
+                   iters=40),
     # 3-D k-NN (k=12), 55,476 points, k = 8, 20 LP iterations
     "knn-c0": dict(kind="knn", n=55476, dim=3, knn=12, seed=1, k=8, theta=1000, iters=20),
     # 2048 graphs, V log-uniform in [1K, 200K], half k-NN 2-D/3-D (k_nn 8..14), half preferential attachment
