@@ -79,13 +79,15 @@ struct DecodeWork {
     const batch::Inst *inst;
     const int32_t *order;
     int ninst;
-    const float *Z;  // [nv * 16]
+    const float *Z;  // [nv * 16] proposal coordinates (first 8 columns used)
+    float *Y;        // [nv * 4] principal coordinates (work)
     int32_t *label;
     int32_t *l0, *l1;  // [nv] each
     int32_t *status;   // [ninst]
     int *next;
 };
 void decode(const DecodeWork &w, int grid, cudaStream_t s);
+void coords(const float *Xf, const float *Z, int nv, float *P, int num_sms, cudaStream_t s);
 
 }  // namespace mpnn
 }  // namespace dmolp

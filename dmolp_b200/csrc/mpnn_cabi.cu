@@ -59,7 +59,7 @@ struct dmolp_mpnn {
     bool cap_train = false;
     std::vector<void *> ws;
     __nv_bfloat16 *C1 = nullptr, *C2 = nullptr, *C3 = nullptr, *G = nullptr, *G3 = nullptr;
-    float *Z3 = nullptr, *dC = nullptr, *Xf = nullptr;
+    float *Z3 = nullptr, *dC = nullptr, *Xf = nullptr, *Pc = nullptr, *Y = nullptr;
     int32_t *vinst = nullptr, *dist = nullptr, *mind = nullptr, *f0 = nullptr, *f1 = nullptr, *cnt = nullptr;
     unsigned long long *akey = nullptr;
     int32_t *anchor = nullptr, *ecc = nullptr, *status = nullptr, *target = nullptr, *dl0 = nullptr, *dl1 = nullptr;
@@ -104,6 +104,8 @@ int ensure_ws(dmolp_mpnn *m, const batch::View &b, bool train) {
     MTRY(alloc_into(o, &m->C3, n * 128));
     MTRY(alloc_into(o, &m->Z3, n * 16));
     MTRY(alloc_into(o, &m->Xf, n * 16));
+    MTRY(alloc_into(o, &m->Pc, n * 16));
+    MTRY(alloc_into(o, &m->Y, n * 4));
     MTRY(alloc_into(o, &m->G3, n * 16));
     MTRY(alloc_into(o, &m->vinst, n));
     MTRY(alloc_into(o, &m->dist, n));
@@ -265,10 +267,11 @@ int dmolp_mpnn_create(int device, dmolp_mpnn **out) {
         dmolp_mpnn_destroy(m);
         return r;
     }
-    // Glorot-uniform weights from a fixed seed, zero biases
+    // Glorot-uniform weights from a fixed seed for the hidden layers, zero biases; the output layer starts at
+    // zero, so the untrained proposal is the random-walk features themselves (the network learns a residual)
     std::vector<float> p(kNumParams, 0.f);
     std::mt19937 rng(12345);
-    for (int l = 0; l < 3; ++l) {
+    for (int l = 0; l < 2; ++l) {
         const float a = std::sqrt(6.f / (float)(kK[l] + kN[l]));
         std::uniform_real_distribution<float> U(-a, a);
         for (int i = 0; i < kK[l] * kN[l]; ++i) p[kOffW[l] + i] = U(rng);
@@ -400,7 +403,8 @@ int dmolp_mpnn_train_step(dmolp_mpnn *m, dmolp_batch *b, const int32_t *target, 
     run_forward(m, v);
     MCUDA(cudaMemsetAsync(m->grads, 0, kNumParams * sizeof(float), s));
     MCUDA(cudaMemsetAsync(m->loss, 0, sizeof(double), s));
-    mpnn::loss(v.off, v.col, (int)v.nv, m->Z3, m->target, v.narcs > 0 ? 1.0 / (double)v.narcs : 0.0, m->G3,
+    coords(m->Xf, m->Z3, (int)v.nv, m->Pc, v.num_sms, s);
+    mpnn::loss(v.off, v.col, (int)v.nv, m->Pc, m->target, v.narcs > 0 ? 1.0 / (double)v.narcs : 0.0, m->G3,
                m->grads + kOffB[2], m->loss, v.num_sms, s);
     run_backward(m, v);
     adam(m->params, m->grads, m->m, m->v, kNumParams, lr, ++m->step, s);
@@ -421,11 +425,13 @@ int dmolp_mpnn_decode(dmolp_mpnn *m, dmolp_batch *b, const float *embedding, int
         MCUDA(cudaMemcpyAsync(m->Z3, embedding, (size_t)v.nv * 16 * sizeof(float), cudaMemcpyHostToDevice, v.stream));
     else if (!m->have_z)
         return fail(DMOLP_ERR_STATE, "run forward first or pass an embedding");
+    coords(m->Xf, m->Z3, (int)v.nv, m->Pc, v.num_sms, v.stream);
     DecodeWork w;
     w.inst = v.inst;
     w.order = v.order;
     w.ninst = v.ninst;
-    w.Z = m->Z3;
+    w.Z = m->Pc;
+    w.Y = m->Y;
     w.label = v.label;
     w.l0 = m->dl0;
     w.l1 = m->dl1;

@@ -535,13 +535,65 @@ __global__ void k_to_input(const float *Xf, int nv, __nv_bfloat16 *X, int ldx) {
         for (int j = 0; j < 16; ++j) X[(size_t)v * ldx + j] = __float2bfloat16_rn(Xf[(size_t)v * 16 + j]);
 }
 
+// Proposal coordinates: random-walk features + the network's first 8 outputs (its residual); 16 wide, the
+// upper 8 columns 0.
+__global__ void k_coords(const float *__restrict__ Xf, const float *__restrict__ Z, int nv, float *__restrict__ P) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)nv * 16;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = i >> 4;
+        const int j = (int)(i & 15);
+        P[i] = j < 8 ? __fadd_rn(Xf[v * 16 + 2 + j], Z[v * 16 + j]) : 0.f;
+    }
+}
+
 // ------------------------------------------------------------------------------------ decoder
-// Recursive coordinate bisection, one CTA per graph: every part with kp >= 2 labels splits (all parts of a
-// level at once) into kl = kp/2 and kp - kl labels; the left child takes the floor(n * kl / kp) vertices with
-// the smallest (coordinate, id) along the dimension of largest range.  The selection is an MSD radix select
-// over 64-bit keys (orderable float bits, id) with 6-bit digits, segmented by part.
+// One CTA per graph.  First the principal axes of the graph's proposal coordinates P (8 wide): mean and
+// covariance in double (thread partials in a fixed order, then a fixed reduction tree), cyclic Jacobi on the
+// 8x8 covariance by one thread, the top 3 axes by eigenvalue, each signed so that its largest-magnitude
+// component is positive; Y = (P - mean) @ axes.  Then recursive coordinate bisection of Y: every part with
+// kp >= 2 labels splits (all parts of a level at once) into kl = kp/2 and kp - kl labels; the left child takes
+// the floor(n * kl / kp) vertices with the smallest (coordinate, id) along the dimension of largest range.  The
+// selection is an MSD radix select over 64-bit keys (orderable float bits, id) with 6-bit digits, segmented
+// by part.
 constexpr int kDecThreads = 512;
 constexpr int kDecDigits = 64;
+constexpr int kDecDims = 3;
+constexpr int kPcaDims = 8;
+
+// Eigen-decomposition of a symmetric 8x8 matrix (cyclic Jacobi, double); eigenvalues on the diagonal of A,
+// eigenvectors in the columns of V.
+__device__ void jacobi8(double (&A)[kPcaDims][kPcaDims], double (&V)[kPcaDims][kPcaDims]) {
+    for (int i = 0; i < kPcaDims; ++i)
+        for (int j = 0; j < kPcaDims; ++j) V[i][j] = i == j ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 50; ++sweep) {
+        double off = 0.0;
+        for (int p = 0; p < kPcaDims; ++p)
+            for (int q = p + 1; q < kPcaDims; ++q) off += A[p][q] * A[p][q];
+        if (off < 1e-30) break;
+        for (int p = 0; p < kPcaDims; ++p)
+            for (int q = p + 1; q < kPcaDims; ++q) {
+                if (fabs(A[p][q]) < 1e-300) continue;
+                const double theta = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+                for (int r = 0; r < kPcaDims; ++r) {
+                    const double arp = A[r][p], arq = A[r][q];
+                    A[r][p] = c * arp - sn * arq;
+                    A[r][q] = sn * arp + c * arq;
+                }
+                for (int r = 0; r < kPcaDims; ++r) {
+                    const double apr = A[p][r], aqr = A[q][r];
+                    A[p][r] = c * apr - sn * aqr;
+                    A[q][r] = sn * apr + c * aqr;
+                }
+                for (int r = 0; r < kPcaDims; ++r) {
+                    const double vrp = V[r][p], vrq = V[r][q];
+                    V[r][p] = c * vrp - sn * vrq;
+                    V[r][q] = sn * vrp + c * vrq;
+                }
+            }
+    }
+}
 
 __device__ __forceinline__ unsigned orderable(float x) {
     const unsigned u = __float_as_uint(x);
@@ -553,7 +605,9 @@ __device__ __forceinline__ float from_orderable(unsigned o) {
 
 struct DecSmem {
     int kp[64], dim[64], cnt[64], need[64], below[64], keep[64];
-    unsigned mx[64][16], mn[64][16];
+    unsigned mx[64][kDecDims], mn[64][kDecDims];
+    double part[kDecThreads / 32][kPcaDims + kPcaDims * kPcaDims];
+    double mean[kPcaDims], axis[kPcaDims][kDecDims];
     int hist[64 * kDecDigits];
     int nact[2], open, inst, bad;
 };
@@ -586,7 +640,7 @@ __global__ void __launch_bounds__(kDecThreads) k_decode(DecodeWork w) {
         __syncthreads();
         for (int v = threadIdx.x; v < nv; v += blockDim.x) {
             w.label[vb + v] = 0;
-            for (int d = 0; d < 16; ++d)
+            for (int d = 0; d < kPcaDims; ++d)
                 if (!isfinite(w.Z[(size_t)(vb + v) * 16 + d])) sm.bad = 1;
         }
         __syncthreads();
@@ -595,11 +649,70 @@ __global__ void __launch_bounds__(kDecThreads) k_decode(DecodeWork w) {
             __syncthreads();
             continue;
         }
+        // ---- principal axes: mean, then the covariance of the centred coordinates ----
+        for (int pass = 0; pass < 2; ++pass) {
+            double acc[kPcaDims + kPcaDims * kPcaDims];
+            const int na = pass == 0 ? kPcaDims : kPcaDims * kPcaDims;
+            for (int i = 0; i < na; ++i) acc[i] = 0.0;
+            for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+                double x[kPcaDims];
+                for (int d = 0; d < kPcaDims; ++d) {
+                    x[d] = (double)w.Z[(size_t)(vb + v) * 16 + d];
+                    if (pass == 1) x[d] -= sm.mean[d];
+                }
+                if (pass == 0)
+                    for (int d = 0; d < kPcaDims; ++d) acc[d] += x[d];
+                else
+                    for (int p = 0; p < kPcaDims; ++p)
+                        for (int q = 0; q < kPcaDims; ++q) acc[p * kPcaDims + q] += x[p] * x[q];
+            }
+            for (int i = 0; i < na; ++i) {
+                double y = acc[i];
+                for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(DMOLP_FULL_MASK, y, o);
+                if (lane == 0) sm.part[wib][i] = y;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double tot[kPcaDims * kPcaDims];
+                for (int i = 0; i < na; ++i) {
+                    tot[i] = 0.0;
+                    for (int ww = 0; ww < kDecThreads / 32; ++ww) tot[i] += sm.part[ww][i];
+                }
+                if (pass == 0) {
+                    for (int d = 0; d < kPcaDims; ++d) sm.mean[d] = tot[d] / (double)nv;
+                } else {
+                    double A[kPcaDims][kPcaDims], V[kPcaDims][kPcaDims];
+                    for (int p = 0; p < kPcaDims; ++p)
+                        for (int q = 0; q < kPcaDims; ++q) A[p][q] = tot[p * kPcaDims + q];
+                    jacobi8(A, V);
+                    int used[kPcaDims] = {0, 0, 0, 0, 0, 0, 0, 0};
+                    for (int j = 0; j < kDecDims; ++j) {  // top eigenvalues, lowest index on ties
+                        int bi = -1;
+                        for (int i = 0; i < kPcaDims; ++i)
+                            if (!used[i] && (bi < 0 || A[i][i] > A[bi][bi])) bi = i;
+                        used[bi] = 1;
+                        int mi = 0;
+                        for (int r = 1; r < kPcaDims; ++r)
+                            if (fabs(V[r][bi]) > fabs(V[mi][bi])) mi = r;
+                        const double sg = V[mi][bi] < 0 ? -1.0 : 1.0;
+                        for (int r = 0; r < kPcaDims; ++r) sm.axis[r][j] = sg * V[r][bi];
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        for (int v = threadIdx.x; v < nv; v += blockDim.x)
+            for (int j = 0; j < kDecDims; ++j) {
+                double y = 0.0;
+                for (int d = 0; d < kPcaDims; ++d) y += ((double)w.Z[(size_t)(vb + v) * 16 + d] - sm.mean[d]) * sm.axis[d][j];
+                w.Y[(size_t)(vb + v) * 4 + j] = (float)y;
+            }
+        __syncthreads();
         for (int level = 0; level < 7; ++level) {
             // ---- per part: vertex count and coordinate ranges ----
-            for (int i = threadIdx.x; i < 64 * 16; i += blockDim.x) {
-                sm.mx[i / 16][i % 16] = 0u;
-                sm.mn[i / 16][i % 16] = 0xFFFFFFFFu;
+            for (int i = threadIdx.x; i < 64 * kDecDims; i += blockDim.x) {
+                sm.mx[i / kDecDims][i % kDecDims] = 0u;
+                sm.mn[i / kDecDims][i % kDecDims] = 0xFFFFFFFFu;
             }
             for (int p = threadIdx.x; p < 64; p += blockDim.x) sm.cnt[p] = 0;
             __syncthreads();
@@ -610,8 +723,8 @@ __global__ void __launch_bounds__(kDecThreads) k_decode(DecodeWork w) {
                 const unsigned m = __match_any_sync(DMOLP_FULL_MASK, lo);
                 const bool lead = lane == __ffs(m) - 1;
                 if (lo >= 0 && lead) atomicAdd(&sm.cnt[lo], __popc(m));
-                for (int d = 0; d < 16; ++d) {
-                    const unsigned o = lo >= 0 ? orderable(w.Z[(size_t)(vb + v) * 16 + d]) : 0u;
+                for (int d = 0; d < kDecDims; ++d) {
+                    const unsigned o = lo >= 0 ? orderable(w.Y[(size_t)(vb + v) * 4 + d]) : 0u;
                     const unsigned hi = __reduce_max_sync(m, o), lw = __reduce_min_sync(m, o);
                     if (lo >= 0 && lead) {
                         atomicMax(&sm.mx[lo][d], hi);
@@ -626,7 +739,7 @@ __global__ void __launch_bounds__(kDecThreads) k_decode(DecodeWork w) {
                 sm.dim[p] = 0;
                 if (sm.kp[p] >= 2 && sm.cnt[p] > 0) {
                     float best = -1.f;
-                    for (int d = 0; d < 16; ++d) {
+                    for (int d = 0; d < kDecDims; ++d) {
                         const float r = __fsub_rn(from_orderable(sm.mx[p][d]), from_orderable(sm.mn[p][d]));
                         if (r > best) {
                             best = r;
@@ -662,7 +775,7 @@ __global__ void __launch_bounds__(kDecThreads) k_decode(DecodeWork w) {
                         const int lo = w.label[vb + v];
                         if (lo >= 0 && sm.kp[lo] >= 2 && sm.need[lo] > 0) {
                             const unsigned long long key =
-                                ((unsigned long long)orderable(w.Z[(size_t)(vb + v) * 16 + sm.dim[lo]]) << 32) |
+                                ((unsigned long long)orderable(w.Y[(size_t)(vb + v) * 4 + sm.dim[lo]]) << 32) |
                                 (unsigned)v;
                             bin = lo * kDecDigits + (int)((key >> sh) & dmask);
                         }
@@ -737,7 +850,7 @@ __global__ void __launch_bounds__(kDecThreads) k_decode(DecodeWork w) {
                         const int lo = w.label[vb + v];
                         if (lo >= 0 && sm.kp[lo] >= 2) {
                             const unsigned long long key =
-                                ((unsigned long long)orderable(w.Z[(size_t)(vb + v) * 16 + sm.dim[lo]]) << 32) |
+                                ((unsigned long long)orderable(w.Y[(size_t)(vb + v) * 4 + sm.dim[lo]]) << 32) |
                                 (unsigned)v;
                             const int d = (int)((key >> sh) & dmask);
                             if (d < sm.below[lo]) w.label[vb + v] = -1 - lo;  // selected: stays in lo
@@ -896,6 +1009,10 @@ int features(const FeatWork &w, int num_sms, cudaStream_t s) {
 
 void features_to_input(const float *Xf, int nv, __nv_bfloat16 *X, int ldx, cudaStream_t s) {
     k_to_input<<<grid_for(nv, 148), 256, 0, s>>>(Xf, nv, X, ldx);
+}
+
+void coords(const float *Xf, const float *Z, int nv, float *P, int num_sms, cudaStream_t s) {
+    k_coords<<<grid_for((int64_t)nv * 16, num_sms), 256, 0, s>>>(Xf, Z, nv, P);
 }
 
 void decode(const DecodeWork &w, int grid, cudaStream_t s) {

@@ -275,7 +275,7 @@ int dmolp_batch_autotune(dmolp_batch *b, const dmolp_lp_config *cfg, dmolp_batch
 typedef struct dmolp_mpnn dmolp_mpnn;
 
 int64_t dmolp_mpnn_num_params(void);           /* length of the flat FP32 parameter vector */
-int dmolp_mpnn_create(int device, dmolp_mpnn **out);  /* Glorot-uniform weights from a fixed seed */
+int dmolp_mpnn_create(int device, dmolp_mpnn **out);  /* fixed-seed Glorot hidden layers, zero output layer */
 int dmolp_mpnn_destroy(dmolp_mpnn *m);
 /* Parameters, flat FP32: per layer W [K x N] row-major then b [N]; K = 32, 128, 128; N = 64, 64, 16.
  * Setting them resets the optimiser state. */
@@ -292,10 +292,12 @@ int dmolp_mpnn_prepare_training(dmolp_mpnn *m, dmolp_batch *b);
 /* Backward of the last forward pass for an upstream gradient d_embedding[nv*16]; grads[num_params] out. */
 int dmolp_mpnn_backward(dmolp_mpnn *m, dmolp_batch *b, const float *d_embedding, float *grads);
 /* One Adam step (lr; beta 0.9 / 0.999) on the edge-contrastive loss against target labels target[nv]:
- * mean over arcs (v,u) of |z_v - z_u|^2 when the targets agree, max(0, 1 - |z_v - z_u|^2) otherwise. */
+ * mean over arcs (v,u) of |p_v - p_u|^2 when the targets agree, max(0, 1 - |p_v - p_u|^2) otherwise, p the
+ * proposal coordinates. */
 int dmolp_mpnn_train_step(dmolp_mpnn *m, dmolp_batch *b, const int32_t *target, float lr, double *loss);
-/* Labels from an embedding (NULL = the last forward pass) into the batch's labels; status[ninst] (may be
- * NULL): 0 = proposal used, 1 = not usable (the graph keeps labels 0 and needs phase-1 seeding). */
+/* Labels from the current features and an embedding (NULL = the last forward pass) into the batch's
+ * labels; status[ninst] (may be NULL): 0 = proposal used, 1 = not usable (the graph keeps labels 0 and needs
+ * phase-1 seeding). */
 int dmolp_mpnn_decode(dmolp_mpnn *m, dmolp_batch *b, const float *embedding, int32_t *status);
 /* Features + forward + decode. */
 int dmolp_batch_propose(dmolp_batch *b, dmolp_mpnn *m, int32_t *status);

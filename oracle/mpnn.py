@@ -10,7 +10,9 @@ CPU restatement (numpy) of the learned initial-partition proposal, for checking 
   the hidden layers; BF16 weights and activations, FP32 accumulation -- the rounding points are the
   device's, so forward and backward can be compared closely;
 * its backward pass and the edge-contrastive training loss on a target partition;
-* the recursive coordinate bisection that turns the embedding into k balanced labels.
+* the decoder: proposal coordinates P = random-walk features + the network's first 8 outputs (a residual:
+  the output layer starts at zero), their per-graph principal axes, and recursive coordinate bisection of
+  the top 3 principal coordinates into k balanced labels.
 
 Only tests/ use this module.
 """
@@ -200,6 +202,13 @@ def backward(off, col, cache, dZ3, params, exact: bool = False):
     return np.concatenate([np.concatenate([dW.ravel(), db]) for dW, db in grads]).astype(ft)
 
 
+def coords(X, Z):
+    """Proposal coordinates [n,16]: random-walk features + the network's residual (first 8 outputs)."""
+    P = np.zeros((X.shape[0], 16), np.float32)
+    P[:, :8] = (X[:, 2:10].astype(np.float32) + Z[:, :8].astype(np.float32)).astype(np.float32)
+    return P
+
+
 def contrastive(off, col, Z, target):
     """Mean over arcs of y*d2 + (1-y)*max(0, MARGIN - d2), y = same target label; and dL/dZ."""
     n = off.shape[0] - 1
@@ -219,6 +228,25 @@ def contrastive(off, col, Z, target):
 def orderable(x: np.ndarray) -> np.ndarray:
     u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
     return np.where(u & 0x80000000, (~u) & 0xFFFFFFFF, u | 0x80000000)
+
+
+def principal(P: np.ndarray, d: int = 3) -> np.ndarray:
+    """Coordinates of the rows of P[:, :8] on their top-d principal axes (float64 covariance; each axis signed
+    so that its largest-magnitude component is positive), as float32 [n,16] with the rest 0."""
+    F = P[:, :8].astype(np.float64)
+    F = F - F.mean(axis=0)
+    w, V = np.linalg.eigh(F.T @ F)
+    V = V[:, ::-1][:, :d]
+    for j in range(d):
+        if V[np.argmax(np.abs(V[:, j])), j] < 0:
+            V[:, j] = -V[:, j]
+    Y = np.zeros((P.shape[0], 16), np.float32)
+    Y[:, :d] = (F @ V).astype(np.float32)
+    return Y
+
+
+def decode(X, Z, k: int) -> np.ndarray:
+    return rcb(principal(coords(X, Z)), k)
 
 
 def rcb(Z: np.ndarray, k: int) -> np.ndarray:

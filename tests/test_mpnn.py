@@ -140,7 +140,7 @@ def test_train_step_loss_matches_oracle_and_decreases(setup):
     tgt = np.concatenate([(np.arange(it.graph.num_vertices) * it.k // max(1, it.graph.num_vertices)).astype(np.int32)
                           for it in inst])
     Zr, _ = M.forward(off, col, X, P)
-    lr_, _ = M.contrastive(off, col, Zr, tgt)
+    lr_, _ = M.contrastive(off, col, M.coords(X, Zr), tgt)
     l0 = m.train_step(b, tgt, 1e-3)
     assert abs(l0 - lr_) <= 1e-2 * max(1.0, abs(lr_)), (l0, lr_)
     losses = [m.train_step(b, tgt, 1e-3) for _ in range(30)]
@@ -149,11 +149,14 @@ def test_train_step_loss_matches_oracle_and_decreases(setup):
 
 @pytest.mark.gpu
 def test_decoder_matches_oracle(setup):
+    """Principal axes + recursive bisection against the oracle's (float64 axes by another summation order:
+    a few vertices at a split may land on the other side)."""
     b, m, inst = setup
     rng = np.random.default_rng(5)
-    Z = rng.standard_normal((b.num_vertices, 16)).astype(np.float32)
-    Z[:, 3] *= 4.0  # a dominant dimension, and ties elsewhere
-    Z[b.vstart[2]:b.vstart[2] + 50, 5] = 0.25
+    X = rng.standard_normal((b.num_vertices, 16)).astype(np.float32)
+    X[:, 3] *= 4.0  # a dominant axis
+    m.set_features(b, X)
+    Z = (rng.standard_normal((b.num_vertices, 16)) * 0.1).astype(np.float32)
     st = m.decode(b, Z)
     lab = b.split(b.labels())
     for i, it in enumerate(inst):
@@ -161,8 +164,12 @@ def test_decoder_matches_oracle(setup):
             assert st[i] == 1
             continue
         assert st[i] == 0
-        ref = M.rcb(Z[b.vstart[i]:b.vstart[i + 1]], it.k)
-        assert np.array_equal(lab[i], ref), it.family
+        sl = slice(b.vstart[i], b.vstart[i + 1])
+        ref = M.decode(X[sl], Z[sl], it.k)
+        agree = np.mean(lab[i] == ref)
+        assert agree > 0.97, (it.family, agree)
+        c = np.bincount(lab[i], minlength=it.k)
+        assert c.max() - c.min() <= 6
 
 
 @pytest.mark.gpu
