@@ -394,13 +394,19 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     // movers alone
     c->symmetric = false;
     if (!unsorted && nv > 0) {
+        // the arc counts borrow the (zeroed) radix-select histogram and leave it zeroed
+        unsigned long long *counts = reinterpret_cast<unsigned long long *>(b.hist);
         DMOLP_CUDA(cudaMemsetAsync(b.flag, 0, sizeof(int), c->stream));
-        lp_check_symmetric(c);
+        DMOLP_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), c->stream));
+        lp_check_symmetric(c, counts);
         int missing = 1;
+        unsigned long long hc[2] = {0, 1};
         DMOLP_CUDA(cudaMemcpyAsync(&missing, b.flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DMOLP_CUDA(cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
+        DMOLP_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), c->stream));
         int s1 = sync(c);
         if (s1) return s1;
-        c->symmetric = missing == 0;
+        c->symmetric = missing == 0 && hc[0] == hc[1];
     }
     // log(t) and e^(-t/5) with the host's libm, as the reference computes them (phase2.cpp:199,
     // gpu_lp_boundary.cu:244)

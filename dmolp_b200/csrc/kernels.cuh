@@ -20,7 +20,7 @@ struct LpLaunch {
     int eff;       // labels scored: min(k,32) or k
     int mode;      // DMOLP_LP_MODE_*
 };
-void lp_check_symmetric(dmolp_ctx *c);  // sets *b.flag when an arc has no reverse
+void lp_check_symmetric(dmolp_ctx *c, unsigned long long *counts);  // *b.flag: a reverse is missing
 void lp_fill(dmolp_ctx *c, int32_t *p, int64_t n, int32_t v);
 void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped);
 void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip);

@@ -815,23 +815,62 @@ __global__ void k_collect_moves(Buffers b) {
     }
 }
 
-// Warp per vertex u: every arc (u,v) must have its reverse, found by binary search in v's (strictly
-// increasing) row; a missing one sets the flag.
-__global__ void k_symcheck(Buffers b, int nv) {
-    const int lane = threadIdx.x & 31;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    bool missing = false;
-    for (int u = gw; u < nv; u += nw) {
-        for (int64_t j = b.off[u] + lane; j < b.off[u + 1]; j += 32) {
-            const int v = b.col[j];
-            int64_t lo = b.off[v], hi = b.off[v + 1];
-            while (lo < hi) {
-                const int64_t mid = (lo + hi) >> 1;
-                if (b.col[mid] < u) lo = mid + 1;
-                else hi = mid;
-            }
-            if (lo >= b.off[v + 1] || b.col[lo] != u) missing = true;
+// Symmetry of the uploaded graph (rows strictly increasing).  Each arc (u,v), u != v, is looked up from its
+// larger endpoint only -- (degree, id) of u above v's: u must be in v's (shorter) row, by binary search.  The
+// other arcs are only counted.  With no duplicates the found reverses are distinct arcs, so the graph is
+// symmetric iff every lookup succeeds and both counts agree (flag[0] = missing, cnt[0..1] = the counts).
+__device__ __forceinline__ void sym_arc(const Buffers &b, int u, int64_t du, int v, bool &missing,
+                                        unsigned long long &big, unsigned long long &small) {
+    if (u == v) return;
+    const int64_t s = b.off[v], e = b.off[v + 1];
+    const int64_t dv = e - s;
+    if (du > dv || (du == dv && u > v)) {
+        ++big;
+        int64_t lo = s, hi = e;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (b.col[mid] < u) lo = mid + 1;
+            else hi = mid;
         }
+        if (lo >= e || b.col[lo] != u) missing = true;
+    } else {
+        ++small;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_symcheck(Buffers b, int g0, int g1, int nb0, int nb1, int nb2,
+                                                  unsigned long long *cnt) {
+    const int lane = threadIdx.x & 31;
+    bool missing = false;
+    unsigned long long big = 0, small = 0;
+    if ((int)blockIdx.x < g0) {  // thread per vertex
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb0; i += g0 * blockDim.x) {
+            const int u = b.bucket[0][i];
+            const int64_t s = b.off[u], e = b.off[u + 1];
+            for (int64_t j = s; j < e; ++j) sym_arc(b, u, e - s, __ldg(b.col + j), missing, big, small);
+        }
+    } else if ((int)blockIdx.x < g0 + g1) {  // warp per vertex
+        const int wpb = blockDim.x >> 5;
+        const int gw = ((int)blockIdx.x - g0) * wpb + (threadIdx.x >> 5), nw = g1 * wpb;
+        for (int i = gw; i < nb1; i += nw) {
+            const int u = b.bucket[1][i];
+            const int64_t s = b.off[u], e = b.off[u + 1];
+            for (int64_t j = s + lane; j < e; j += 32) sym_arc(b, u, e - s, __ldg(b.col + j), missing, big, small);
+        }
+    } else {  // block per vertex
+        const int gb = (int)blockIdx.x - g0 - g1, nbk = (int)gridDim.x - g0 - g1;
+        for (int i = gb; i < nb2; i += nbk) {
+            const int u = b.bucket[2][i];
+            const int64_t s = b.off[u], e = b.off[u + 1];
+            for (int64_t j = s + threadIdx.x; j < e; j += blockDim.x)
+                sym_arc(b, u, e - s, __ldg(b.col + j), missing, big, small);
+        }
+    }
+    big = warp_sum_u64(big);
+    small = warp_sum_u64(small);
+    if (lane == 0) {
+        if (big) atomicAdd(&cnt[0], big);
+        if (small) atomicAdd(&cnt[1], small);
     }
     if (__any_sync(DMOLP_FULL_MASK, missing) && lane == 0) *b.flag = 1;
 }
@@ -936,8 +975,11 @@ struct ProfScope {
 
 }  // namespace
 
-void lp_check_symmetric(dmolp_ctx *c) {
-    k_symcheck<<<grid_for(c), kBlock, 0, c->stream>>>(c->b, (int)c->nv);
+void lp_check_symmetric(dmolp_ctx *c, unsigned long long *counts) {
+    const int cap = c->num_sms * 8;
+    const int g0 = clampi((c->nb[0] + 255) / 256, 1, cap), g1 = clampi((c->nb[1] + 7) / 8, 1, cap);
+    const int g2 = clampi(c->nb[2], 1, c->num_sms * 2);
+    k_symcheck<<<g0 + g1 + g2, kBlock, 0, c->stream>>>(c->b, g0, g1, c->nb[0], c->nb[1], c->nb[2], counts);
     c->launches++;
 }
 

@@ -227,3 +227,31 @@ def test_reference_gpu_kernel_agrees(part):
             m = part.phase2(k, mode="fixed", iterations=10)
             assert np.array_equal(part.labels(), r["labels2"]), trial
             assert m.edge_cut == r["result"]["edge_cut"]
+
+
+def test_symmetry_detection_selects_the_statistics_path(part):
+    """An upload whose arcs all have reverses updates cut and balance from the movers; one missing reverse
+    switches the loop to the full statistics pass (one more launch per iteration)."""
+    from dmolp_b200 import graphs
+
+    g = graphs.knn(2000, 3, 10, seed=3)
+
+    def launches_for(gr):
+        part.upload(gr)
+        part.set_labels(np.zeros(gr.num_vertices, np.int32))
+        a = part.kernel_launches()
+        part.phase2(1, mode="fixed", iterations=3, records=False)
+        return part.kernel_launches() - a
+
+    sym = launches_for(g)
+    u = 7
+    v = int(g.indices[g.offsets[u]])
+    row = g.indices[g.offsets[v]:g.offsets[v + 1]]
+    keep = np.ones(g.num_arcs, bool)
+    keep[g.offsets[v] + int(np.nonzero(row == u)[0][0])] = False  # (v, u) goes, (u, v) stays
+    off = np.zeros(g.num_vertices + 1, np.int64)
+    off[1:] = np.cumsum(np.diff(g.offsets) - np.bincount(np.repeat(np.arange(g.num_vertices), np.diff(g.offsets))[~keep],
+                                                         minlength=g.num_vertices))
+    asym = launches_for(graphs.Graph(off, g.indices[keep]))
+    assert asym == sym + 3
+    assert launches_for(g) == sym
