@@ -32,7 +32,7 @@ EXPORTS = [
     "dmolp_mpnn_num_params", "dmolp_mpnn_create", "dmolp_mpnn_destroy", "dmolp_mpnn_set_params",
     "dmolp_mpnn_get_params", "dmolp_mpnn_features", "dmolp_mpnn_set_features", "dmolp_mpnn_forward",
     "dmolp_mpnn_prepare_training", "dmolp_mpnn_backward", "dmolp_mpnn_train_step", "dmolp_mpnn_decode",
-    "dmolp_batch_propose",
+    "dmolp_batch_propose", "dmolp_mpnn_gate", "dmolp_mpnn_train_gate",
 ]
 BATCH_MAX_K = 64
 
@@ -136,4 +136,6 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_mpnn_train_step.argtypes = [vp, vp, vp, ctypes.c_float, POINTER(c_double)]
     lib.dmolp_mpnn_decode.argtypes = [vp, vp, vp, vp]
     lib.dmolp_batch_propose.argtypes = [vp, vp, vp]
+    lib.dmolp_mpnn_gate.argtypes = [vp, vp, vp]
+    lib.dmolp_mpnn_train_gate.argtypes = [vp, vp, vp, ctypes.c_float, POINTER(c_double)]
     return lib

@@ -88,6 +88,8 @@ struct DecodeWork {
 };
 void decode(const DecodeWork &w, int grid, cudaStream_t s);
 void coords(const float *Xf, const float *Z, int nv, float *P, int num_sms, cudaStream_t s);
+void gate_scores(const float *Z, const int32_t *vinst, int nv, double *score, int num_sms, cudaStream_t s);
+void gate_grad(const float *g, const int32_t *vinst, int nv, float *dZ, int num_sms, cudaStream_t s);
 
 }  // namespace mpnn
 }  // namespace dmolp

@@ -1,6 +1,7 @@
 // C-ABI of the learned initial-partition proposal (include/dmolp_b200.h, dmolp_mpnn_* and
 // dmolp_batch_propose): the network's parameters and Adam state, its per-batch workspace, features,
 // forward, backward, one training step and the decoder into a batch's labels.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -65,7 +66,8 @@ struct dmolp_mpnn {
     int32_t *anchor = nullptr, *ecc = nullptr, *status = nullptr, *target = nullptr, *dl0 = nullptr, *dl1 = nullptr;
     int *next = nullptr;
     float *P0 = nullptr, *Q0 = nullptr, *P1 = nullptr, *Q1 = nullptr;
-    double *stats = nullptr;
+    double *stats = nullptr, *gscore = nullptr;
+    float *ggrad = nullptr;
     bool have_z = false;
 };
 
@@ -122,6 +124,8 @@ int ensure_ws(dmolp_mpnn *m, const batch::View &b, bool train) {
     MTRY(alloc_into(o, &m->ecc, b.ninst));
     MTRY(alloc_into(o, &m->status, b.ninst));
     MTRY(alloc_into(o, &m->stats, (size_t)16 * b.ninst));
+    MTRY(alloc_into(o, &m->gscore, b.ninst));
+    MTRY(alloc_into(o, &m->ggrad, b.ninst));
     MTRY(alloc_into(o, &m->P0, n * 8));
     MTRY(alloc_into(o, &m->Q0, n * 8));
     MTRY(alloc_into(o, &m->P1, n * 8));
@@ -442,10 +446,69 @@ int dmolp_mpnn_decode(dmolp_mpnn *m, dmolp_batch *b, const float *embedding, int
     return sync_check(m, v.stream, "decode");
 }
 
+int dmolp_mpnn_gate(dmolp_mpnn *m, dmolp_batch *b, double *scores) {
+    batch::View v;
+    MTRY(get_view(m, b, &v));
+    if (!scores) return fail(DMOLP_ERR_ARG, "null scores");
+    if (!m->have_z) return fail(DMOLP_ERR_STATE, "run forward first");
+    MCUDA(cudaMemsetAsync(m->gscore, 0, v.ninst * sizeof(double), v.stream));
+    gate_scores(m->Z3, m->vinst, (int)v.nv, m->gscore, v.num_sms, v.stream);
+    MCUDA(cudaMemcpyAsync(scores, m->gscore, v.ninst * sizeof(double), cudaMemcpyDeviceToHost, v.stream));
+    MTRY(sync_check(m, v.stream, "gate"));
+    std::vector<batch::Inst> hi(v.ninst);
+    MCUDA(cudaMemcpy(hi.data(), v.inst, v.ninst * sizeof(batch::Inst), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < v.ninst; ++i) scores[i] = hi[i].nv > 0 ? scores[i] / (double)hi[i].nv : 0.0;
+    return DMOLP_OK;
+}
+
+int dmolp_mpnn_train_gate(dmolp_mpnn *m, dmolp_batch *b, const float *target, float lr, double *loss) {
+    batch::View v;
+    MTRY(get_view(m, b, &v));
+    if (!target) return fail(DMOLP_ERR_ARG, "null target");
+    if (!m->cap_train || m->cap_nv < v.nv) return fail(DMOLP_ERR_STATE, "call dmolp_mpnn_prepare_training first");
+    cudaStream_t s = v.stream;
+    run_forward(m, v);
+    std::vector<double> sc(v.ninst);
+    MTRY(dmolp_mpnn_gate(m, b, sc.data()));
+    std::vector<batch::Inst> hi(v.ninst);
+    MCUDA(cudaMemcpy(hi.data(), v.inst, v.ninst * sizeof(batch::Inst), cudaMemcpyDeviceToHost));
+    // binary cross-entropy of sigmoid(score) against the target, mean over graphs
+    std::vector<float> g(v.ninst, 0.f);
+    double L = 0.0;
+    int ng = 0;
+    for (int i = 0; i < v.ninst; ++i) ng += hi[i].nv > 0;
+    for (int i = 0; i < v.ninst; ++i) {
+        if (hi[i].nv == 0) continue;
+        const double p = 1.0 / (1.0 + std::exp(-sc[i])), y = target[i];
+        L += -(y * std::log(std::max(p, 1e-12)) + (1.0 - y) * std::log(std::max(1.0 - p, 1e-12)));
+        g[i] = (float)((p - y) / (double)std::max(1, ng) / (double)hi[i].nv);
+    }
+    MCUDA(cudaMemcpyAsync(m->ggrad, g.data(), v.ninst * sizeof(float), cudaMemcpyHostToDevice, s));
+    MCUDA(cudaMemsetAsync(m->grads, 0, kNumParams * sizeof(float), s));
+    gate_grad(m->ggrad, m->vinst, (int)v.nv, m->dC, v.num_sms, s);
+    grad_out(m->dC, (int)v.nv, m->G3, m->grads + kOffB[2], v.num_sms, s);
+    run_backward(m, v);
+    adam(m->params, m->grads, m->m, m->v, kNumParams, lr, ++m->step, s);
+    cast_weights(m->params, m->W, m->Wt, s);
+    MTRY(sync_check(m, s, "train_gate"));
+    if (loss) *loss = ng > 0 ? L / ng : 0.0;
+    m->have_z = false;
+    return DMOLP_OK;
+}
+
 int dmolp_batch_propose(dmolp_batch *b, dmolp_mpnn *m, int32_t *status) {
     MTRY(dmolp_mpnn_features(m, b, nullptr));
     MTRY(dmolp_mpnn_forward(m, b, nullptr));
-    return dmolp_mpnn_decode(m, b, nullptr, status);
+    batch::View v;
+    MTRY(get_view(m, b, &v));
+    std::vector<double> sc(v.ninst);
+    MTRY(dmolp_mpnn_gate(m, b, sc.data()));
+    std::vector<int32_t> st(v.ninst);
+    MTRY(dmolp_mpnn_decode(m, b, nullptr, st.data()));
+    for (int i = 0; i < v.ninst; ++i)
+        if (st[i] == 0 && sc[i] < 0.0) st[i] = 2;  // the gate prefers phase-1 seeding for this graph
+    if (status) std::memcpy(status, st.data(), v.ninst * sizeof(int32_t));
+    return DMOLP_OK;
 }
 
 }  // extern "C"

@@ -535,6 +535,32 @@ __global__ void k_to_input(const float *Xf, int nv, __nv_bfloat16 *X, int ldx) {
         for (int j = 0; j < 16; ++j) X[(size_t)v * ldx + j] = __float2bfloat16_rn(Xf[(size_t)v * 16 + j]);
 }
 
+// Gate scores: per graph, the mean of the network's output column 8 over its vertices (double sums).
+__global__ void k_gate_scores(const float *Z, const int32_t *vinst, int nv, double *score) {
+    const int lane = threadIdx.x & 31;
+    for (int v0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); v0 < nv; v0 += gridDim.x * blockDim.x) {
+        const int v = v0 + lane;
+        const int i = v < nv ? vinst[v] : -1;
+        double x = v < nv ? (double)Z[(size_t)v * 16 + 8] : 0.0;
+        const int i0 = __shfl_sync(DMOLP_FULL_MASK, i, 0);
+        if (__all_sync(DMOLP_FULL_MASK, i == i0)) {
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(DMOLP_FULL_MASK, x, o);
+            if (lane == 0) atomicAdd(&score[i0], x);
+        } else if (i >= 0) {
+            atomicAdd(&score[i], x);
+        }
+    }
+}
+
+// Upstream gradient of the gate loss: column 8 of vertex v gets g[graph of v], the other columns 0.
+__global__ void k_gate_grad(const float *g, const int32_t *vinst, int nv, float *dZ) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)nv * 16;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t v = i >> 4;
+        dZ[i] = (i & 15) == 8 ? g[vinst[v]] : 0.f;
+    }
+}
+
 // Proposal coordinates: random-walk features + the network's first 8 outputs (its residual); 16 wide, the
 // upper 8 columns 0.
 __global__ void k_coords(const float *__restrict__ Xf, const float *__restrict__ Z, int nv, float *__restrict__ P) {
@@ -547,17 +573,15 @@ __global__ void k_coords(const float *__restrict__ Xf, const float *__restrict__
 }
 
 // ------------------------------------------------------------------------------------ decoder
-// One CTA per graph.  First the principal axes of the graph's proposal coordinates P (8 wide): mean and
-// covariance in double (thread partials in a fixed order, then a fixed reduction tree), cyclic Jacobi on the
-// 8x8 covariance by one thread, the top 3 axes by eigenvalue, each signed so that its largest-magnitude
-// component is positive; Y = (P - mean) @ axes.  Then recursive coordinate bisection of Y: every part with
+// Recursive inertial bisection of the proposal coordinates P (8 wide), one CTA per graph: every part with
 // kp >= 2 labels splits (all parts of a level at once) into kl = kp/2 and kp - kl labels; the left child takes
-// the floor(n * kl / kp) vertices with the smallest (coordinate, id) along the dimension of largest range.  The
-// selection is an MSD radix select over 64-bit keys (orderable float bits, id) with 6-bit digits, segmented
-// by part.
+// the floor(n * kl / kp) vertices with the smallest (projection, id) on the part's principal axis.  The axis:
+// mean and covariance of the part in double (thread partials in a fixed order, then a fixed reduction
+// tree), cyclic Jacobi on the 8x8 covariance by one thread, the eigenvector of the largest eigenvalue signed
+// so that its largest-magnitude component is positive.  The selection is an MSD radix select over 64-bit keys
+// (orderable float bits of the projection, id) with 6-bit digits, segmented by part.
 constexpr int kDecThreads = 512;
 constexpr int kDecDigits = 64;
-constexpr int kDecDims = 3;
 constexpr int kPcaDims = 8;
 
 // Eigen-decomposition of a symmetric 8x8 matrix (cyclic Jacobi, double); eigenvalues on the diagonal of A,
@@ -599,15 +623,11 @@ __device__ __forceinline__ unsigned orderable(float x) {
     const unsigned u = __float_as_uint(x);
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
-__device__ __forceinline__ float from_orderable(unsigned o) {
-    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
-}
 
 struct DecSmem {
     int kp[64], dim[64], cnt[64], need[64], below[64], keep[64];
-    unsigned mx[64][kDecDims], mn[64][kDecDims];
-    double part[kDecThreads / 32][kPcaDims + kPcaDims * kPcaDims];
-    double mean[kPcaDims], axis[kPcaDims][kDecDims];
+    double part[kDecThreads / 32][kPcaDims * kPcaDims];
+    double mean[kPcaDims], axis[kPcaDims][2];  // principal axis of the current part, its mean
     int hist[64 * kDecDigits];
     int nact[2], open, inst, bad;
 };
@@ -649,71 +669,9 @@ __global__ void __launch_bounds__(kDecThreads) k_decode(DecodeWork w) {
             __syncthreads();
             continue;
         }
-        // ---- principal axes: mean, then the covariance of the centred coordinates ----
-        for (int pass = 0; pass < 2; ++pass) {
-            double acc[kPcaDims + kPcaDims * kPcaDims];
-            const int na = pass == 0 ? kPcaDims : kPcaDims * kPcaDims;
-            for (int i = 0; i < na; ++i) acc[i] = 0.0;
-            for (int v = threadIdx.x; v < nv; v += blockDim.x) {
-                double x[kPcaDims];
-                for (int d = 0; d < kPcaDims; ++d) {
-                    x[d] = (double)w.Z[(size_t)(vb + v) * 16 + d];
-                    if (pass == 1) x[d] -= sm.mean[d];
-                }
-                if (pass == 0)
-                    for (int d = 0; d < kPcaDims; ++d) acc[d] += x[d];
-                else
-                    for (int p = 0; p < kPcaDims; ++p)
-                        for (int q = 0; q < kPcaDims; ++q) acc[p * kPcaDims + q] += x[p] * x[q];
-            }
-            for (int i = 0; i < na; ++i) {
-                double y = acc[i];
-                for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(DMOLP_FULL_MASK, y, o);
-                if (lane == 0) sm.part[wib][i] = y;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double tot[kPcaDims * kPcaDims];
-                for (int i = 0; i < na; ++i) {
-                    tot[i] = 0.0;
-                    for (int ww = 0; ww < kDecThreads / 32; ++ww) tot[i] += sm.part[ww][i];
-                }
-                if (pass == 0) {
-                    for (int d = 0; d < kPcaDims; ++d) sm.mean[d] = tot[d] / (double)nv;
-                } else {
-                    double A[kPcaDims][kPcaDims], V[kPcaDims][kPcaDims];
-                    for (int p = 0; p < kPcaDims; ++p)
-                        for (int q = 0; q < kPcaDims; ++q) A[p][q] = tot[p * kPcaDims + q];
-                    jacobi8(A, V);
-                    int used[kPcaDims] = {0, 0, 0, 0, 0, 0, 0, 0};
-                    for (int j = 0; j < kDecDims; ++j) {  // top eigenvalues, lowest index on ties
-                        int bi = -1;
-                        for (int i = 0; i < kPcaDims; ++i)
-                            if (!used[i] && (bi < 0 || A[i][i] > A[bi][bi])) bi = i;
-                        used[bi] = 1;
-                        int mi = 0;
-                        for (int r = 1; r < kPcaDims; ++r)
-                            if (fabs(V[r][bi]) > fabs(V[mi][bi])) mi = r;
-                        const double sg = V[mi][bi] < 0 ? -1.0 : 1.0;
-                        for (int r = 0; r < kPcaDims; ++r) sm.axis[r][j] = sg * V[r][bi];
-                    }
-                }
-            }
-            __syncthreads();
-        }
-        for (int v = threadIdx.x; v < nv; v += blockDim.x)
-            for (int j = 0; j < kDecDims; ++j) {
-                double y = 0.0;
-                for (int d = 0; d < kPcaDims; ++d) y += ((double)w.Z[(size_t)(vb + v) * 16 + d] - sm.mean[d]) * sm.axis[d][j];
-                w.Y[(size_t)(vb + v) * 4 + j] = (float)y;
-            }
-        __syncthreads();
         for (int level = 0; level < 7; ++level) {
-            // ---- per part: vertex count and coordinate ranges ----
-            for (int i = threadIdx.x; i < 64 * kDecDims; i += blockDim.x) {
-                sm.mx[i / kDecDims][i % kDecDims] = 0u;
-                sm.mn[i / kDecDims][i % kDecDims] = 0xFFFFFFFFu;
-            }
+            // ---- per splitting part: vertex count, mean, covariance, principal axis (fixed-order double
+            //      reductions, so the result does not depend on scheduling); Y = projection on the axis ----
             for (int p = threadIdx.x; p < 64; p += blockDim.x) sm.cnt[p] = 0;
             __syncthreads();
             for (int i0 = (int)(threadIdx.x & ~31u); i0 < nv; i0 += blockDim.x) {
@@ -721,34 +679,107 @@ __global__ void __launch_bounds__(kDecThreads) k_decode(DecodeWork w) {
                 int lo = v < nv ? w.label[vb + v] : -1;
                 if (lo >= 0 && sm.kp[lo] < 2) lo = -1;
                 const unsigned m = __match_any_sync(DMOLP_FULL_MASK, lo);
-                const bool lead = lane == __ffs(m) - 1;
-                if (lo >= 0 && lead) atomicAdd(&sm.cnt[lo], __popc(m));
-                for (int d = 0; d < kDecDims; ++d) {
-                    const unsigned o = lo >= 0 ? orderable(w.Y[(size_t)(vb + v) * 4 + d]) : 0u;
-                    const unsigned hi = __reduce_max_sync(m, o), lw = __reduce_min_sync(m, o);
-                    if (lo >= 0 && lead) {
-                        atomicMax(&sm.mx[lo][d], hi);
-                        atomicMin(&sm.mn[lo][d], lw);
-                    }
-                }
+                if (lo >= 0 && lane == __ffs(m) - 1) atomicAdd(&sm.cnt[lo], __popc(m));
             }
             __syncthreads();
+            for (int lo = 0; lo < 64; ++lo) {
+                if (sm.kp[lo] < 2 || sm.cnt[lo] == 0) continue;  // block-uniform
+                // mean of the part
+                {
+                    double acc[kPcaDims];
+#pragma unroll
+                    for (int d = 0; d < kPcaDims; ++d) acc[d] = 0.0;
+                    for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+                        if (w.label[vb + v] != lo) continue;
+                        const float4 *z = reinterpret_cast<const float4 *>(w.Z + (size_t)(vb + v) * 16);
+                        const float4 z0 = z[0], z1 = z[1];
+                        const float x[kPcaDims] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
+#pragma unroll
+                        for (int d = 0; d < kPcaDims; ++d) acc[d] += (double)x[d];
+                    }
+#pragma unroll
+                    for (int d = 0; d < kPcaDims; ++d) {
+                        double y = acc[d];
+                        for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(DMOLP_FULL_MASK, y, o);
+                        if (lane == 0) sm.part[wib][d] = y;
+                    }
+                    __syncthreads();
+                    if (threadIdx.x < kPcaDims) {
+                        double t = 0.0;
+                        for (int ww = 0; ww < kDecThreads / 32; ++ww) t += sm.part[ww][threadIdx.x];
+                        sm.mean[threadIdx.x] = t / (double)sm.cnt[lo];
+                    }
+                    __syncthreads();
+                }
+                // covariance (upper triangle, 36 entries), then the principal axis
+                {
+                    constexpr int kTri = kPcaDims * (kPcaDims + 1) / 2;
+                    double acc[kTri];
+#pragma unroll
+                    for (int i = 0; i < kTri; ++i) acc[i] = 0.0;
+                    double mu[kPcaDims];
+#pragma unroll
+                    for (int d = 0; d < kPcaDims; ++d) mu[d] = sm.mean[d];
+                    for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+                        if (w.label[vb + v] != lo) continue;
+                        const float4 *z = reinterpret_cast<const float4 *>(w.Z + (size_t)(vb + v) * 16);
+                        const float4 z0 = z[0], z1 = z[1];
+                        const float xf[kPcaDims] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
+                        double x[kPcaDims];
+#pragma unroll
+                        for (int d = 0; d < kPcaDims; ++d) x[d] = (double)xf[d] - mu[d];
+                        int i = 0;
+#pragma unroll
+                        for (int a2 = 0; a2 < kPcaDims; ++a2)
+#pragma unroll
+                            for (int b2 = a2; b2 < kPcaDims; ++b2) acc[i++] += x[a2] * x[b2];
+                    }
+#pragma unroll
+                    for (int i = 0; i < kTri; ++i) {
+                        double y = acc[i];
+                        for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(DMOLP_FULL_MASK, y, o);
+                        if (lane == 0) sm.part[wib][i] = y;
+                    }
+                    __syncthreads();
+                    if (threadIdx.x == 0) {
+                        double A[kPcaDims][kPcaDims], V[kPcaDims][kPcaDims];
+                        int i = 0;
+                        for (int a2 = 0; a2 < kPcaDims; ++a2)
+                            for (int b2 = a2; b2 < kPcaDims; ++b2, ++i) {
+                                double t = 0.0;
+                                for (int ww = 0; ww < kDecThreads / 32; ++ww) t += sm.part[ww][i];
+                                A[a2][b2] = t;
+                                A[b2][a2] = t;
+                            }
+                        jacobi8(A, V);
+                        int bi = 0;  // largest eigenvalue, lowest index on ties
+                        for (int r = 1; r < kPcaDims; ++r)
+                            if (A[r][r] > A[bi][bi]) bi = r;
+                        int mi = 0;
+                        for (int r = 1; r < kPcaDims; ++r)
+                            if (fabs(V[r][bi]) > fabs(V[mi][bi])) mi = r;
+                        const double sg = V[mi][bi] < 0 ? -1.0 : 1.0;
+                        for (int r = 0; r < kPcaDims; ++r) {
+                            sm.axis[r][0] = sg * V[r][bi];
+                            sm.axis[r][1] = sm.mean[r];
+                        }
+                    }
+                    __syncthreads();
+                }
+                for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+                    if (w.label[vb + v] != lo) continue;
+                    double y = 0.0;
+                    for (int d = 0; d < kPcaDims; ++d)
+                        y += ((double)w.Z[(size_t)(vb + v) * 16 + d] - sm.axis[d][1]) * sm.axis[d][0];
+                    w.Y[(size_t)(vb + v) * 4] = (float)y;
+                }
+                __syncthreads();
+            }
             if (threadIdx.x < 64) {
                 const int p = threadIdx.x;
                 sm.need[p] = 0;
                 sm.dim[p] = 0;
-                if (sm.kp[p] >= 2 && sm.cnt[p] > 0) {
-                    float best = -1.f;
-                    for (int d = 0; d < kDecDims; ++d) {
-                        const float r = __fsub_rn(from_orderable(sm.mx[p][d]), from_orderable(sm.mn[p][d]));
-                        if (r > best) {
-                            best = r;
-                            sm.dim[p] = d;
-                        }
-                    }
-                    const int kl = sm.kp[p] / 2;
-                    sm.need[p] = (int)(((long long)sm.cnt[p] * kl) / sm.kp[p]);
-                }
+                if (sm.kp[p] >= 2 && sm.cnt[p] > 0) sm.need[p] = (int)(((long long)sm.cnt[p] * (sm.kp[p] / 2)) / sm.kp[p]);
             }
             for (int i = threadIdx.x; i < 64 * kDecDigits; i += blockDim.x) sm.hist[i] = 0;
             if (threadIdx.x == 0) {
@@ -1009,6 +1040,14 @@ int features(const FeatWork &w, int num_sms, cudaStream_t s) {
 
 void features_to_input(const float *Xf, int nv, __nv_bfloat16 *X, int ldx, cudaStream_t s) {
     k_to_input<<<grid_for(nv, 148), 256, 0, s>>>(Xf, nv, X, ldx);
+}
+
+void gate_scores(const float *Z, const int32_t *vinst, int nv, double *score, int num_sms, cudaStream_t s) {
+    k_gate_scores<<<grid_for(nv, num_sms), 256, 0, s>>>(Z, vinst, nv, score);
+}
+
+void gate_grad(const float *g, const int32_t *vinst, int nv, float *dZ, int num_sms, cudaStream_t s) {
+    k_gate_grad<<<grid_for((int64_t)nv * 16, num_sms), 256, 0, s>>>(g, vinst, nv, dZ);
 }
 
 void coords(const float *Xf, const float *Z, int nv, float *P, int num_sms, cudaStream_t s) {

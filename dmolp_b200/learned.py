@@ -1,10 +1,12 @@
 """Learned initial partition over libdmolp_b200.so (include/dmolp_b200.h, dmolp_mpnn_* / dmolp_batch_propose).
 
 A 3-layer mean-aggregation message-passing network (BF16 weights, FP32 accumulation on the tensor cores,
-the project's own forward and backward kernels) embeds every vertex of a batch of graphs; recursive
-coordinate bisection of the embedding gives k balanced labels per graph.  It replaces phase 1 (BFS / hub
-seeding) as the start of phase 2; graphs it cannot serve fall back to phase 1.  The network is trained on
-final partitions that the plain method (phase 1 + phase 2) produces.
+the project's own forward and backward kernels) runs over every vertex of a batch of graphs.  Its first 8
+outputs are a residual on the 8 random-walk features (proposal coordinates, cut into k balanced labels per
+graph by recursive inertial bisection); its output 8, averaged over a graph, is a learned gate that says
+whether the proposal will end at an edge cut no higher than phase 1's.  The proposal replaces phase 1
+(BFS / hub seeding) as the start of phase 2 where the gate accepts it; elsewhere phase 1 is the fallback.
+The gate is trained on runs of the plain method (phase 1 + phase 2): which start ended lower.
 """
 from __future__ import annotations
 
@@ -100,6 +102,17 @@ class Proposal:
         self._check(self.lib.dmolp_mpnn_train_step(self.h, b.h, _p(t), c_float(lr), byref(loss)))
         return loss.value
 
+    def gate(self, b: Batch) -> np.ndarray:
+        out = np.empty(b.num_instances, np.float64)
+        self._check(self.lib.dmolp_mpnn_gate(self.h, b.h, _p(out)))
+        return out
+
+    def train_gate(self, b: Batch, y: np.ndarray, lr: float) -> float:
+        t = np.ascontiguousarray(y, np.float32)
+        loss = c_double()
+        self._check(self.lib.dmolp_mpnn_train_gate(self.h, b.h, _p(t), c_float(lr), byref(loss)))
+        return loss.value
+
     def decode(self, b: Batch, Z: np.ndarray | None = None) -> np.ndarray:
         st = np.empty(b.num_instances, np.int32)
         z = None if Z is None else np.ascontiguousarray(Z, np.float32)
@@ -108,7 +121,7 @@ class Proposal:
 
     def propose(self, b: Batch) -> np.ndarray:
         """Labels of every graph of the batch from the network (into the batch); returns per-graph status
-        (0 = proposal used, 1 = needs phase-1 seeding)."""
+        (0 = proposal used, 1 = proposal not usable, 2 = the gate prefers phase 1)."""
         st = np.empty(b.num_instances, np.int32)
         self._check(self.lib.dmolp_batch_propose(b.h, self.h, _p(st)))
         return st
@@ -159,6 +172,30 @@ def plain_targets(instances: list[Instance], theta: int = 1000, device: int = 0)
     out = b.split(b.labels())
     b.close()
     return [x.copy() for x in out]
+
+
+def train_gate(model: Proposal, sets: list[tuple[list[Instance], np.ndarray]], epochs: int, lr: float = 1e-3,
+               device: int = 0, log=None) -> list[float]:
+    """Adam on the gate's binary cross-entropy over training minibatches (graphs, 0/1 targets)."""
+    prepared = []
+    for inst, y in sets:
+        b = Batch(device)
+        b.upload(inst)
+        model.prepare_training(b)
+        X = model.features(b)
+        prepared.append((b, X, np.asarray(y, np.float32)))
+    losses = []
+    for ep in range(epochs):
+        tot = 0.0
+        for b, X, y in prepared:
+            model.set_features(b, X)
+            tot += model.train_gate(b, y, lr)
+        losses.append(tot / len(prepared))
+        if log:
+            log(ep, losses[-1])
+    for b, _, _ in prepared:
+        b.close()
+    return losses
 
 
 def train(model: Proposal, sets: list[tuple[list[Instance], list[np.ndarray]]], epochs: int, lr: float = 1e-3,

@@ -299,7 +299,14 @@ int dmolp_mpnn_train_step(dmolp_mpnn *m, dmolp_batch *b, const int32_t *target, 
  * labels; status[ninst] (may be NULL): 0 = proposal used, 1 = not usable (the graph keeps labels 0 and needs
  * phase-1 seeding). */
 int dmolp_mpnn_decode(dmolp_mpnn *m, dmolp_batch *b, const float *embedding, int32_t *status);
-/* Features + forward + decode. */
+/* The learned gate: per graph, the mean of output column 8 over its vertices after the last forward pass;
+ * >= 0 means the proposal is expected to end at an edge cut no higher than phase-1 seeding's. */
+int dmolp_mpnn_gate(dmolp_mpnn *m, dmolp_batch *b, double *scores);
+/* One Adam step on the gate alone: binary cross-entropy of sigmoid(score) against target[ninst] (1 = the
+ * proposal beat phase 1 on this graph, from runs of the plain method). */
+int dmolp_mpnn_train_gate(dmolp_mpnn *m, dmolp_batch *b, const float *target, float lr, double *loss);
+/* Features + forward + decode + gate.  status: 0 = proposal used, 1 = not usable, 2 = the gate prefers
+ * phase-1 seeding; for 1 and 2 the caller seeds the graph with phase 1. */
 int dmolp_batch_propose(dmolp_batch *b, dmolp_mpnn *m, int32_t *status);
 
 /* Per-part vertex counts and intra-part edge counts of instance i after the last run (k entries each). */

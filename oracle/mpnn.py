@@ -11,8 +11,8 @@ CPU restatement (numpy) of the learned initial-partition proposal, for checking 
   device's, so forward and backward can be compared closely;
 * its backward pass and the edge-contrastive training loss on a target partition;
 * the decoder: proposal coordinates P = random-walk features + the network's first 8 outputs (a residual:
-  the output layer starts at zero), their per-graph principal axes, and recursive coordinate bisection of
-  the top 3 principal coordinates into k balanced labels.
+  the output layer starts at zero), cut into k balanced labels by recursive inertial bisection (every part
+  split at the median of its projection on its own principal axis).
 
 Only tests/ use this module.
 """
@@ -245,8 +245,44 @@ def principal(P: np.ndarray, d: int = 3) -> np.ndarray:
     return Y
 
 
+def rib(P: np.ndarray, k: int) -> np.ndarray:
+    """Recursive inertial bisection of the rows of P[:, :8] into k labels: every part with kp >= 2 labels
+    splits at the same level into kl = kp // 2 and kp - kl labels; the left child takes the
+    floor(|S| * kl / kp) vertices with the smallest (projection, id) on the part's principal axis (float64
+    covariance; the axis signed so that its largest-magnitude component is positive; projection rounded to
+    float32)."""
+    n = P.shape[0]
+    lab = np.zeros(n, np.int64)
+    parts = {0: k}
+    while any(kp >= 2 for kp in parts.values()):
+        new = {}
+        for lo, kp in parts.items():
+            if kp < 2:
+                new[lo] = kp
+                continue
+            S = np.nonzero(lab == lo)[0]
+            kl = kp // 2
+            nl = (len(S) * kl) // kp
+            if len(S):
+                F = P[S, :8].astype(np.float64)
+                mu = F.mean(axis=0)
+                C = (F - mu).T @ (F - mu)
+                w, V = np.linalg.eigh(C)
+                a = V[:, -1]
+                if a[np.argmax(np.abs(a))] < 0:
+                    a = -a
+                y = ((F - mu) @ a).astype(np.float32)
+                key = (orderable(y) << np.uint64(32)) | S.astype(np.uint64)
+                order = S[np.argsort(key, kind="stable")]
+                lab[order[nl:]] = lo + kl
+            new[lo] = kl
+            new[lo + kl] = kp - kl
+        parts = new
+    return lab.astype(np.int32)
+
+
 def decode(X, Z, k: int) -> np.ndarray:
-    return rcb(principal(coords(X, Z)), k)
+    return rib(coords(X, Z), k)
 
 
 def rcb(Z: np.ndarray, k: int) -> np.ndarray:

@@ -181,3 +181,23 @@ def test_propose_then_lp(setup):
     for i, it in enumerate(inst[:3]):
         c = np.bincount(lab[i], minlength=it.k)
         assert c.min() > 0 and c.max() - c.min() <= 6
+
+
+@pytest.mark.gpu
+def test_gate_scores_and_training(setup):
+    """The gate is the per-graph mean of output 8; its cross-entropy training step lowers the loss."""
+    b, m, inst = setup
+    rng = np.random.default_rng(8)
+    P = (rng.standard_normal(M.num_params()) * 0.2).astype(np.float32)
+    m.set_params(P)
+    m.features(b, copy=False)
+    Z = m.forward(b)
+    sc = m.gate(b)
+    for i in range(len(inst)):
+        sl = slice(b.vstart[i], b.vstart[i + 1])
+        assert abs(sc[i] - float(Z[sl, 8].astype(np.float64).mean())) < 1e-5 * max(1.0, abs(sc[i]))
+    y = np.array([1, 0, 1, 0], np.float32)
+    l0 = m.train_gate(b, y, 1e-2)
+    for _ in range(40):
+        last = m.train_gate(b, y, 1e-2)
+    assert last < l0
