@@ -175,6 +175,7 @@ def test_decoder_matches_oracle(setup):
 @pytest.mark.gpu
 def test_propose_then_lp(setup):
     b, m, inst = setup
+    m.set_params(np.zeros(M.num_params(), np.float32))  # gate 0: every usable proposal is accepted
     st = m.propose(b)
     assert list(st) == [0, 0, 0, 1]
     lab = b.split(b.labels())
