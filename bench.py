@@ -312,13 +312,15 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
 
     # ---- phase 1 (single-graph path) for every instance: the starting partitions ----
     p = Partitioner(local_rank)
-    lab1, p1_ms = [], 0.0
+    lab1, p1_ms, p1_each = [], 0.0, []
     t0 = time.perf_counter()
     for it in inst:
+        t1 = time.perf_counter()
         p.upload(it.graph)
         m1 = p.phase1(it.k, w["theta"])
         p1_ms += m1.gpu_ms
         lab1.append(p.labels())
+        p1_each.append(time.perf_counter() - t1)
     p1_wall = time.perf_counter() - t0
 
     # ---- plain: phase 2 of the single-graph path, one instance after another ----
@@ -379,6 +381,41 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
     assert np.array_equal(out, np.concatenate(final)), "end-to-end labels differ"
     b.close()
 
+    # ---- batched + learned: the proposal for every graph (features, network, decoder, gate), phase 1 where
+    #      the gate declines (its per-graph wall time measured above is charged), then the batched phase 2 ----
+    learned = None
+    try:
+        from dmolp_b200.learned import WEIGHTS, Proposal
+
+        model = Proposal(local_rank, WEIGHTS)
+        b2 = Batch(local_rank)
+        b2.upload(arrays=arrays)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = model.propose(b2)
+        prop_s = time.perf_counter() - t0
+        lab = b2.labels()
+        fb = np.nonzero(st != 0)[0]
+        for i in fb:
+            lab[b2.vstart[i]:b2.vstart[i + 1]] = lab1[i]
+        b2.set_labels(lab)
+        fb_s = float(sum(p1_each[i] for i in fb))
+        res_l, lms = b2.run("ref")
+        b2.close()
+        model.close()
+        plain_cut = float(sum(r["edge_cut"] for r in res))
+        total_s = prop_s + fb_s + lms / 1e3
+        plain_total_s = p1_wall + plain_wall * n / max(1, ns)
+        learned = {"graphs_per_s": n / total_s, "proposal_wall_s": prop_s, "fallbacks": int(len(fb)),
+                   "fallback_phase1_wall_s": fb_s, "lp_ms": lms,
+                   "cut_ratio_vs_plain": float(sum(r["edge_cut"] for r in res_l)) / max(1.0, plain_cut),
+                   "vertex_balance_mean": float(np.mean([r["vertex_balance"] for r in res_l])),
+                   "plain_vertex_balance_mean": float(np.mean([r["vertex_balance"] for r in res])),
+                   "plain_pipeline_graphs_per_s": n / plain_total_s,
+                   "speedup_vs_plain_pipeline": plain_total_s / total_s}
+    except Exception as e:  # report, do not hide
+        learned = {"error": str(e)[:300]}
+
     t_max = elapsed
     if dist:
         t = torch.tensor([elapsed], device="cuda")
@@ -406,6 +443,7 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
                    "edge_cut_sum_plain": plain_cut,
                    "phase1_single_graph_ms_device": p1_ms, "phase1_single_graph_wall_s": p1_wall,
                    "iterations_mean": float(np.mean([r["iterations_run"] for r in res])),
+                   "learned": learned,
                    "l2": "batch CSR %.0f MB > L2" % (na_tot * 4 / 1e6), "parallelism": f"replicas x{world}"},
         "e2e": {"value": n * world / e2e_s, "unit": "graphs/s", "wall_s": e2e_s,
                 "h2d_bytes_per_step": int(sum(a.nbytes for a in arrays) + lab_h.nbytes),
