@@ -403,12 +403,12 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
         res_l, lms = b2.run("ref")
         b2.close()
         model.close()
-        plain_cut = float(sum(r["edge_cut"] for r in res))
+        all_plain_cut = float(sum(r["edge_cut"] for r in res))
         total_s = prop_s + fb_s + lms / 1e3
         plain_total_s = p1_wall + plain_wall * n / max(1, ns)
         learned = {"graphs_per_s": n / total_s, "proposal_wall_s": prop_s, "fallbacks": int(len(fb)),
                    "fallback_phase1_wall_s": fb_s, "lp_ms": lms,
-                   "cut_ratio_vs_plain": float(sum(r["edge_cut"] for r in res_l)) / max(1.0, plain_cut),
+                   "cut_ratio_vs_plain": float(sum(r["edge_cut"] for r in res_l)) / max(1.0, all_plain_cut),
                    "vertex_balance_mean": float(np.mean([r["vertex_balance"] for r in res_l])),
                    "plain_vertex_balance_mean": float(np.mean([r["vertex_balance"] for r in res])),
                    "plain_pipeline_graphs_per_s": n / plain_total_s,
