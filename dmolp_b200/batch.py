@@ -176,6 +176,16 @@ class Batch:
         out = [{f: getattr(r, f) for f, _ in cabi.BatchResult._fields_} for r in res]
         return out, ms.value
 
+    def phase1(self, theta: int, seeds: bool = False):
+        """Phase 1 (BFS / hub seeding) for every graph, labels into the batch.  Returns (per-graph dicts,
+        seeds [n, 64] or None, device ms)."""
+        res = (cabi.BatchP1Result * self.num_instances)()
+        sd = np.empty((self.num_instances, cabi.BATCH_MAX_K), np.int32) if seeds else None
+        ms = c_double()
+        self._check(self.lib.dmolp_batch_phase1(self.h, theta, _p(sd) if seeds else None, res, byref(ms)))
+        out = [{f: getattr(r, f) for f, _ in cabi.BatchP1Result._fields_} for r in res]
+        return out, sd, ms.value
+
     def counts(self, i: int) -> tuple[np.ndarray, np.ndarray]:
         k = int(self.parts[i])
         vc = np.zeros(k, np.int64)

@@ -32,7 +32,7 @@ EXPORTS = [
     "dmolp_mpnn_num_params", "dmolp_mpnn_create", "dmolp_mpnn_destroy", "dmolp_mpnn_set_params",
     "dmolp_mpnn_get_params", "dmolp_mpnn_features", "dmolp_mpnn_set_features", "dmolp_mpnn_forward",
     "dmolp_mpnn_prepare_training", "dmolp_mpnn_backward", "dmolp_mpnn_train_step", "dmolp_mpnn_decode",
-    "dmolp_batch_propose", "dmolp_mpnn_gate", "dmolp_mpnn_train_gate",
+    "dmolp_batch_propose", "dmolp_mpnn_gate", "dmolp_mpnn_train_gate", "dmolp_batch_phase1",
 ]
 BATCH_MAX_K = 64
 
@@ -68,6 +68,10 @@ class BatchResult(ctypes.Structure):
     _fields_ = [("edge_cut", c_int64), ("traversed_edges", c_uint64), ("arcs_read", c_uint64),
                 ("vertex_visits", c_uint64), ("vertex_balance", c_double), ("edge_balance", c_double), ("iterations_run", c_int32),
                 ("stop_reason", c_int32), ("status", c_int32), ("changes", c_int32)]
+
+
+class BatchP1Result(ctypes.Structure):
+    _fields_ = [("num_seeds_found", c_int32), ("rounds", c_int32), ("traversed_edges", c_uint64)]
 
 
 def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
@@ -137,5 +141,6 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_mpnn_decode.argtypes = [vp, vp, vp, vp]
     lib.dmolp_batch_propose.argtypes = [vp, vp, vp]
     lib.dmolp_mpnn_gate.argtypes = [vp, vp, vp]
+    lib.dmolp_batch_phase1.argtypes = [vp, c_int, vp, vp, POINTER(c_double)]
     lib.dmolp_mpnn_train_gate.argtypes = [vp, vp, vp, ctypes.c_float, POINTER(c_double)]
     return lib

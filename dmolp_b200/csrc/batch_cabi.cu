@@ -37,6 +37,12 @@ struct dmolp_batch {
     bool tuned = false;
     dmolp_batch_tuning tuning{512, 16, 0, 0};
     std::map<std::tuple<int, int, int, int, int, int>, cudaGraphExec_t> graphs;
+    // phase 1: per-vertex degrees on the host (for the hub lists), device work arrays, cached hub lists
+    std::vector<int32_t> h_deg;
+    std::vector<int64_t> h_vstart;
+    bool have_hubs = false;
+    P1Args p1{};
+    std::vector<P1Out> h_p1;
 };
 
 namespace {
@@ -260,6 +266,15 @@ int dmolp_batch_upload(dmolp_batch *b, int32_t ninst, const int64_t *vstart, con
     BTRY(balloc(b, &lt, kMaxIter + 1));
     BTRY(balloc(b, &rt, kMaxIter + 1));
     BTRY(balloc(b, &ctr, 4));
+    uint8_t *cov = nullptr, *seedm = nullptr, *selm = nullptr;
+    int32_t *claim = nullptr, *seeds_out = nullptr;
+    P1Out *p1out = nullptr;
+    BTRY(balloc(b, &cov, nv));
+    BTRY(balloc(b, &seedm, nv));
+    BTRY(balloc(b, &selm, nv));
+    BTRY(balloc(b, &claim, nv));
+    BTRY(balloc(b, &seeds_out, (size_t)ninst * kBatchMaxK));
+    BTRY(balloc(b, &p1out, ninst));
     std::vector<Inst> hi(ninst);
     for (int i = 0; i < ninst; ++i) {
         Inst &I = hi[i];
@@ -333,6 +348,33 @@ int dmolp_batch_upload(dmolp_batch *b, int32_t ninst, const int64_t *vstart, con
     b->ninst = ninst;
     b->nv = nv;
     b->narcs = narcs;
+    // phase 1: host degrees (hub lists are computed on the first dmolp_batch_phase1 call)
+    b->h_deg.resize(nv);
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < nv; ++v) b->h_deg[v] = (int32_t)(offsets[v + 1] - offsets[v]);
+    b->h_vstart.assign(vstart, vstart + ninst + 1);
+    b->have_hubs = false;
+    P1Args &q = b->p1;
+    q = P1Args();
+    q.off = off;
+    q.col = col;
+    q.label = label;
+    q.inst = inst;
+    q.order = order;
+    q.ninst = ninst;
+    q.next = ctr + 3;
+    q.cov = cov;
+    q.seedm = seedm;
+    q.sel = selm;
+    q.claim = claim;
+    q.l_front0 = w0;
+    q.l_front1 = w1;
+    q.l_claim = lb;
+    q.l_act0 = lc;
+    q.l_act1 = la;
+    q.seeds_out = seeds_out;
+    q.out = p1out;
+    b->h_p1.assign(ninst, P1Out());
     b->has_graph = true;
     return DMOLP_OK;
 }
@@ -450,6 +492,84 @@ int dmolp_batch_autotune(dmolp_batch *b, const dmolp_lp_config *cfg, dmolp_batch
     b->tuned = true;
     if (best) *best = bt;
     if (best_ms) *best_ms = bms;
+    return DMOLP_OK;
+}
+
+int dmolp_batch_phase1(dmolp_batch *b, int theta, int32_t *seeds, dmolp_batch_p1_result *results, double *gpu_ms) {
+    if (!b || !b->has_graph) return fail(DMOLP_ERR_STATE, "no batch uploaded");
+    if (theta < 1) return fail(DMOLP_ERR_ARG, "theta must be >= 1 (with theta = 0 the reference never ends)");
+    BCUDA(cudaSetDevice(b->device));
+    const int n = b->ninst;
+    P1Args &q = b->p1;
+    if (!b->have_hubs) {
+        // hub lists and first seeds per graph, in the reference's order (init.cpp:139-187)
+        std::vector<std::vector<int>> hubs(n);
+        std::vector<int32_t> first(n, 0), first_hub(n, -1);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int i = 0; i < n; ++i) {
+            const int64_t v0 = b->h_vstart[i], v1 = b->h_vstart[i + 1];
+            std::vector<int32_t> deg(b->h_deg.begin() + v0, b->h_deg.begin() + v1);
+            hubs[i] = hubs_of(deg);
+            std::pair<int, int> f(-1, -1);
+            for (int64_t v = v1 - v0 - 1; v >= 0; --v) {  // init.cpp:179-187, with its id-vs-degree tie test
+                const int d = deg[v];
+                if (d > f.second || (d == f.second && (int)v < f.second)) f = std::make_pair((int)v, d);
+            }
+            first[i] = f.first < 0 ? 0 : f.first;
+            auto it = std::find(hubs[i].begin(), hubs[i].end(), f.first);
+            first_hub[i] = it == hubs[i].end() ? -1 : (int32_t)(it - hubs[i].begin());
+        }
+        std::vector<int64_t> hstart(n + 1, 0);
+        for (int i = 0; i < n; ++i) hstart[i + 1] = hstart[i] + (int64_t)hubs[i].size();
+        std::vector<int32_t> flat(std::max<int64_t>(1, hstart[n]));
+        for (int i = 0; i < n; ++i) std::copy(hubs[i].begin(), hubs[i].end(), flat.begin() + hstart[i]);
+        int32_t *dh = nullptr, *df = nullptr, *dfh = nullptr;
+        int64_t *dhs = nullptr;
+        uint8_t *used = nullptr;
+        BTRY(balloc(b, &dh, flat.size()));
+        BTRY(balloc(b, &dhs, n + 1));
+        BTRY(balloc(b, &df, n));
+        BTRY(balloc(b, &dfh, n));
+        BTRY(balloc(b, &used, flat.size()));
+        BCUDA(cudaMemcpyAsync(dh, flat.data(), flat.size() * sizeof(int32_t), cudaMemcpyHostToDevice, b->stream));
+        BCUDA(cudaMemcpyAsync(dhs, hstart.data(), (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, b->stream));
+        BCUDA(cudaMemcpyAsync(df, first.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, b->stream));
+        BCUDA(cudaMemcpyAsync(dfh, first_hub.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, b->stream));
+        BTRY(bsync(b));
+        q.hubs = dh;
+        q.hstart = dhs;
+        q.first = df;
+        q.first_hub = dfh;
+        q.hub_used = used;
+        b->have_hubs = true;
+    }
+    q.theta = theta;
+    BCUDA(cudaEventRecord(b->ev0, b->stream));
+    launch_p1(q, std::max(1, std::min(n, b->num_sms * 2)), b->stream);
+    BCUDA(cudaGetLastError());
+    BCUDA(cudaEventRecord(b->ev1, b->stream));
+    BCUDA(cudaMemcpyAsync(b->h_p1.data(), q.out, n * sizeof(P1Out), cudaMemcpyDeviceToHost, b->stream));
+    if (seeds)
+        BCUDA(cudaMemcpyAsync(seeds, q.seeds_out, (size_t)n * kBatchMaxK * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                              b->stream));
+    BTRY(bsync(b));
+    if (gpu_ms) {
+        float ms = 0;
+        BCUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+        *gpu_ms = ms;
+    }
+    if (seeds)  // union ids -> ids inside each graph
+        for (int i = 0; i < n; ++i)
+            for (int p = 0; p < kBatchMaxK; ++p) {
+                int32_t &s = seeds[(size_t)i * kBatchMaxK + p];
+                if (s >= 0) s -= (int32_t)b->h_vstart[i];
+            }
+    if (results)
+        for (int i = 0; i < n; ++i) {
+            results[i].num_seeds_found = b->h_p1[i].nseeds_found;
+            results[i].rounds = b->h_p1[i].rounds;
+            results[i].traversed_edges = b->h_p1[i].te;
+        }
     return DMOLP_OK;
 }
 

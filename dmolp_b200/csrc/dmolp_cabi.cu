@@ -203,6 +203,7 @@ int run_block_graph(dmolp_ctx *c, const LpLaunch &L, int t0, int cnt) {
 
 namespace dmolp {
 void set_last_error(const std::string &msg) { g_err = msg; }
+std::vector<int> hubs_of(const std::vector<int32_t> &degree) { return find_hubs(degree); }
 }  // namespace dmolp
 
 extern "C" {

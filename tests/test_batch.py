@@ -192,3 +192,36 @@ def test_bad_labels_leave_instance_and_report():
     o = oracle.phase2(inst[0].graph.offsets, inst[0].graph.indices, lab[0], 4, "fixed", 5, "ref")
     assert np.array_equal(out[0], o.labels)
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("theta", [1, 7, 100])
+def test_batched_phase1_matches_single_graph_path(batch, theta):
+    """Phase 1 of every graph in one launch: seeds, labels, rounds and traversed edges as dmolp_phase1
+    gives them for each graph alone (which the oracle and the reference pin)."""
+    from dmolp_b200.partitioner import Partitioner
+
+    b, inst, _ = batch
+    res, seeds, ms = b.phase1(theta, seeds=True)
+    assert ms > 0
+    got = b.split(b.labels())
+    p = Partitioner(0)
+    for i, it in enumerate(inst):
+        g = it.graph
+        if g.num_vertices == 0:
+            continue
+        p.upload(g)
+        m = p.phase1(it.k, theta)
+        assert np.array_equal(got[i], p.labels()), (i, it.family, theta)
+        assert seeds[i, :it.k].tolist() == m.seeds, i
+        assert res[i]["num_seeds_found"] == m.num_seeds_found and res[i]["rounds"] == m.rounds, i
+        assert res[i]["traversed_edges"] == m.traversed_edges, i
+    p.close()
+    # phase 1 then phase 2, both batched: each graph as the oracle's whole path
+    b.run("ref")
+    fin = b.split(b.labels())
+    for i, it in enumerate(inst[:6]):
+        g = it.graph
+        o1 = oracle.phase1(g.offsets, g.indices, g.raw_deg(), it.k, theta)
+        o2 = oracle.phase2(g.offsets, g.indices, o1.labels, it.k, "ref", 0)
+        assert np.array_equal(fin[i], o2.labels), i
