@@ -381,40 +381,51 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
     assert np.array_equal(out, np.concatenate(final)), "end-to-end labels differ"
     b.close()
 
-    # ---- batched + learned: the proposal for every graph (features, network, decoder, gate), phase 1 where
-    #      the gate declines (its per-graph wall time measured above is charged), then the batched phase 2 ----
-    learned = None
+    # ---- whole pipelines, phase 1 + phase 2 for every graph, wall clock including host work:
+    #      plain one graph after another (the single-graph path), plain batched (batched phase 1 + batched
+    #      phase 2), batched + learned (the proposal for every graph -- features, network, decoder, gate --
+    #      batched phase 1 for the graphs the gate declines, batched phase 2) ----
+    pipelines = None
     try:
         from dmolp_b200.learned import WEIGHTS, Proposal
 
-        model = Proposal(local_rank, WEIGHTS)
+        plain_total_s = p1_wall + plain_wall * n / max(1, ns)
+        all_plain_cut = float(sum(r["edge_cut"] for r in res))
         b2 = Batch(local_rank)
         b2.upload(arrays=arrays)
+        b2.tuning = {k: tune[k] for k in ("block_threads", "thread_row_max", "blocks_per_sm", "reserved")}
+        b2.phase1(w["theta"])  # hub lists are computed once per upload on the host: not part of a run
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b2.phase1(w["theta"])
+        res_p, lms_p = b2.run("ref")
+        batched_plain_s = time.perf_counter() - t0
+        lab_p = b2.split(b2.labels())
+        same_as_plain = all(np.array_equal(lab_p[i], final[i]) for i in range(n))
+        model = Proposal(local_rank, WEIGHTS)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         st = model.propose(b2)
         prop_s = time.perf_counter() - t0
-        lab = b2.labels()
-        fb = np.nonzero(st != 0)[0]
-        for i in fb:
-            lab[b2.vstart[i]:b2.vstart[i + 1]] = lab1[i]
-        b2.set_labels(lab)
-        fb_s = float(sum(p1_each[i] for i in fb))
+        if st.any():
+            b2.phase1(w["theta"], only=st != 0)
         res_l, lms = b2.run("ref")
+        learned_s = time.perf_counter() - t0
         b2.close()
         model.close()
-        all_plain_cut = float(sum(r["edge_cut"] for r in res))
-        total_s = prop_s + fb_s + lms / 1e3
-        plain_total_s = p1_wall + plain_wall * n / max(1, ns)
-        learned = {"graphs_per_s": n / total_s, "proposal_wall_s": prop_s, "fallbacks": int(len(fb)),
-                   "fallback_phase1_wall_s": fb_s, "lp_ms": lms,
-                   "cut_ratio_vs_plain": float(sum(r["edge_cut"] for r in res_l)) / max(1.0, all_plain_cut),
-                   "vertex_balance_mean": float(np.mean([r["vertex_balance"] for r in res_l])),
-                   "plain_vertex_balance_mean": float(np.mean([r["vertex_balance"] for r in res])),
-                   "plain_pipeline_graphs_per_s": n / plain_total_s,
-                   "speedup_vs_plain_pipeline": plain_total_s / total_s}
+        pipelines = {
+            "plain_one_graph_after_another": {"graphs_per_s": n / plain_total_s, "wall_s": plain_total_s},
+            "plain_batched": {"graphs_per_s": n / batched_plain_s, "wall_s": batched_plain_s,
+                              "identical_labels_to_one_by_one": same_as_plain},
+            "batched_learned": {"graphs_per_s": n / learned_s, "wall_s": learned_s, "proposal_wall_s": prop_s,
+                                "fallbacks": int((st != 0).sum()),
+                                "cut_ratio_vs_plain": float(sum(r["edge_cut"] for r in res_l)) / max(1.0, all_plain_cut),
+                                "vertex_balance_mean": float(np.mean([r["vertex_balance"] for r in res_l]))},
+            "plain_vertex_balance_mean": float(np.mean([r["vertex_balance"] for r in res])),
+            "speedup_batched_learned_vs_plain": plain_total_s / learned_s,
+            "speedup_plain_batched_vs_plain": plain_total_s / batched_plain_s}
     except Exception as e:  # report, do not hide
-        learned = {"error": str(e)[:300]}
+        pipelines = {"error": str(e)[:300]}
 
     t_max = elapsed
     if dist:
@@ -443,7 +454,7 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
                    "edge_cut_sum_plain": plain_cut,
                    "phase1_single_graph_ms_device": p1_ms, "phase1_single_graph_wall_s": p1_wall,
                    "iterations_mean": float(np.mean([r["iterations_run"] for r in res])),
-                   "learned": learned,
+                   "pipelines": pipelines,
                    "l2": "batch CSR %.0f MB > L2" % (na_tot * 4 / 1e6), "parallelism": f"replicas x{world}"},
         "e2e": {"value": n * world / e2e_s, "unit": "graphs/s", "wall_s": e2e_s,
                 "h2d_bytes_per_step": int(sum(a.nbytes for a in arrays) + lab_h.nbytes),

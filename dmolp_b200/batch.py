@@ -176,13 +176,15 @@ class Batch:
         out = [{f: getattr(r, f) for f, _ in cabi.BatchResult._fields_} for r in res]
         return out, ms.value
 
-    def phase1(self, theta: int, seeds: bool = False):
-        """Phase 1 (BFS / hub seeding) for every graph, labels into the batch.  Returns (per-graph dicts,
-        seeds [n, 64] or None, device ms)."""
+    def phase1(self, theta: int, seeds: bool = False, only=None):
+        """Phase 1 (BFS / hub seeding) for every graph (or those with only[i] true), labels into the batch.
+        Returns (per-graph dicts, seeds [n, 64] or None, device ms)."""
         res = (cabi.BatchP1Result * self.num_instances)()
         sd = np.empty((self.num_instances, cabi.BATCH_MAX_K), np.int32) if seeds else None
+        mask = None if only is None else np.ascontiguousarray(np.asarray(only, bool), np.uint8)
         ms = c_double()
-        self._check(self.lib.dmolp_batch_phase1(self.h, theta, _p(sd) if seeds else None, res, byref(ms)))
+        self._check(self.lib.dmolp_batch_phase1(self.h, theta, None if mask is None else _p(mask),
+                                                _p(sd) if seeds else None, res, byref(ms)))
         out = [{f: getattr(r, f) for f, _ in cabi.BatchP1Result._fields_} for r in res]
         return out, sd, ms.value
 

@@ -141,6 +141,6 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_mpnn_decode.argtypes = [vp, vp, vp, vp]
     lib.dmolp_batch_propose.argtypes = [vp, vp, vp]
     lib.dmolp_mpnn_gate.argtypes = [vp, vp, vp]
-    lib.dmolp_batch_phase1.argtypes = [vp, c_int, vp, vp, POINTER(c_double)]
+    lib.dmolp_batch_phase1.argtypes = [vp, c_int, vp, vp, vp, POINTER(c_double)]
     lib.dmolp_mpnn_train_gate.argtypes = [vp, vp, vp, ctypes.c_float, POINTER(c_double)]
     return lib

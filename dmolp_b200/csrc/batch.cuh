@@ -85,6 +85,7 @@ struct P1Args {
     int32_t *l_front0, *l_front1, *l_claim, *l_act0, *l_act1;  // per-graph slices at vbase
     int32_t *seeds_out;                                        // [ninst][kBatchMaxK]
     P1Out *out;
+    const uint8_t *only;  // [ninst] or null: run only the graphs flagged 1
     int theta;
 };
 

@@ -42,6 +42,7 @@ struct dmolp_batch {
     std::vector<int64_t> h_vstart;
     bool have_hubs = false;
     P1Args p1{};
+    uint8_t *p1_only = nullptr;
     std::vector<P1Out> h_p1;
 };
 
@@ -354,6 +355,7 @@ int dmolp_batch_upload(dmolp_batch *b, int32_t ninst, const int64_t *vstart, con
     for (int64_t v = 0; v < nv; ++v) b->h_deg[v] = (int32_t)(offsets[v + 1] - offsets[v]);
     b->h_vstart.assign(vstart, vstart + ninst + 1);
     b->have_hubs = false;
+    b->p1_only = nullptr;
     P1Args &q = b->p1;
     q = P1Args();
     q.off = off;
@@ -495,7 +497,8 @@ int dmolp_batch_autotune(dmolp_batch *b, const dmolp_lp_config *cfg, dmolp_batch
     return DMOLP_OK;
 }
 
-int dmolp_batch_phase1(dmolp_batch *b, int theta, int32_t *seeds, dmolp_batch_p1_result *results, double *gpu_ms) {
+int dmolp_batch_phase1(dmolp_batch *b, int theta, const uint8_t *only, int32_t *seeds, dmolp_batch_p1_result *results,
+                       double *gpu_ms) {
     if (!b || !b->has_graph) return fail(DMOLP_ERR_STATE, "no batch uploaded");
     if (theta < 1) return fail(DMOLP_ERR_ARG, "theta must be >= 1 (with theta = 0 the reference never ends)");
     BCUDA(cudaSetDevice(b->device));
@@ -544,6 +547,13 @@ int dmolp_batch_phase1(dmolp_batch *b, int theta, int32_t *seeds, dmolp_batch_p1
         b->have_hubs = true;
     }
     q.theta = theta;
+    q.only = nullptr;
+    if (only) {
+        if (!b->p1_only) BTRY(balloc(b, &b->p1_only, n));
+        BCUDA(cudaMemcpyAsync(b->p1_only, only, n, cudaMemcpyHostToDevice, b->stream));
+        q.only = b->p1_only;
+    }
+    BCUDA(cudaMemsetAsync(q.out, 0, n * sizeof(P1Out), b->stream));
     BCUDA(cudaEventRecord(b->ev0, b->stream));
     launch_p1(q, std::max(1, std::min(n, b->num_sms * 2)), b->stream);
     BCUDA(cudaGetLastError());

@@ -408,6 +408,10 @@ __global__ void __launch_bounds__(kP1Threads) k_batch_p1(P1Args a) {
         __syncthreads();
         const int q = sm.inst;
         if (q >= a.ninst) break;
+        if (a.only && !a.only[a.order[q]]) {  // this graph keeps its labels
+            __syncthreads();                   // every thread has read sm.inst before it is rewritten
+            continue;
+        }
         run_p1(a, a.order[q], sm);
     }
 }

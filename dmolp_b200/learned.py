@@ -128,7 +128,8 @@ class Proposal:
 
 
 def phase1_labels(instances: list[Instance], theta: int, device: int = 0, which=None) -> list[np.ndarray]:
-    """The plain seeding (phase 1 of the single-graph path) for the given instances."""
+    """The plain seeding (phase 1 of the single-graph path, one graph after another) for the given
+    instances."""
     p = Partitioner(device)
     out = []
     for i, it in enumerate(instances):
@@ -142,20 +143,15 @@ def phase1_labels(instances: list[Instance], theta: int, device: int = 0, which=
     return out
 
 
-def propose_with_fallback(model: Proposal, b: Batch, instances: list[Instance], theta: int = 1000,
+def propose_with_fallback(model: Proposal, b: Batch, instances: list[Instance] | None = None, theta: int = 1000,
                           device: int = 0) -> tuple[np.ndarray, float]:
-    """Learned labels for every graph of the batch, phase-1 seeding for the graphs the proposal flags.
-    Returns (status per graph, seconds spent in the fallback)."""
+    """Learned labels for every graph of the batch, phase-1 seeding (batched, one launch) for the graphs the
+    proposal flags.  Returns (status per graph, seconds spent in the fallback)."""
     st = model.propose(b)
     t = 0.0
     if st.any():
         t0 = time.perf_counter()
-        lab = b.labels()
-        fb = phase1_labels(instances, theta, device, which=st != 0)
-        for i, l1 in enumerate(fb):
-            if l1 is not None:
-                lab[b.vstart[i]:b.vstart[i + 1]] = l1
-        b.set_labels(lab)
+        b.phase1(theta, only=st != 0)
         t = time.perf_counter() - t0
     return st, t
 

@@ -310,7 +310,7 @@ int dmolp_mpnn_train_gate(dmolp_mpnn *m, dmolp_batch *b, const float *target, fl
 int dmolp_batch_propose(dmolp_batch *b, dmolp_mpnn *m, int32_t *status);
 
 /* Phase 1 on every instance (as dmolp_phase1 with this theta, labels into the batch), one persistent
- * launch.  Degrees are the CSR row lengths (the graphs of a batch have sorted, duplicate-free rows).  The
+ * launch; only[ninst] (may be NULL) restricts it to the instances flagged 1, the others keep their labels.  Degrees are the CSR row lengths (the graphs of a batch have sorted, duplicate-free rows).  The
  * reference's order-dependent hub lists and first seeds are computed on the host once per upload.
  * seeds[ninst * DMOLP_BATCH_MAX_K] (may be NULL): each graph's seeds (ids inside the graph, -1 unused);
  * results[ninst] (may be NULL); gpu_ms (may be NULL) = device time of the launch. */
@@ -319,7 +319,8 @@ typedef struct {
     int32_t rounds;                /* expansion rounds */
     uint64_t traversed_edges;      /* arcs read by ball marking + expansion */
 } dmolp_batch_p1_result;
-int dmolp_batch_phase1(dmolp_batch *b, int theta, int32_t *seeds, dmolp_batch_p1_result *results, double *gpu_ms);
+int dmolp_batch_phase1(dmolp_batch *b, int theta, const uint8_t *only, int32_t *seeds, dmolp_batch_p1_result *results,
+                       double *gpu_ms);
 
 /* Per-part vertex counts and intra-part edge counts of instance i after the last run (k entries each). */
 int dmolp_batch_counts(dmolp_batch *b, int32_t inst, int64_t *vertex_counts, int64_t *edge_counts);

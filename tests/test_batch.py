@@ -217,6 +217,16 @@ def test_batched_phase1_matches_single_graph_path(batch, theta):
         assert res[i]["num_seeds_found"] == m.num_seeds_found and res[i]["rounds"] == m.rounds, i
         assert res[i]["traversed_edges"] == m.traversed_edges, i
     p.close()
+    # a masked run leaves the other graphs' labels alone
+    before = b.labels()
+    b.set_labels(np.zeros(b.num_vertices, np.int32))
+    only = np.arange(len(inst)) % 2 == 0
+    b.phase1(theta, only=only)
+    masked = b.split(b.labels())
+    for i in range(len(inst)):
+        ref = before[b.vstart[i]:b.vstart[i + 1]] if only[i] else np.zeros(inst[i].graph.num_vertices, np.int32)
+        assert np.array_equal(masked[i], ref), i
+    b.phase1(theta)
     # phase 1 then phase 2, both batched: each graph as the oracle's whole path
     b.run("ref")
     fin = b.split(b.labels())
