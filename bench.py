@@ -467,6 +467,57 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
     }
 
 
+def batched_summary(n: int, theta: int, device: int) -> dict:
+    """A compact view of the batched forms for the default bench line: n graphs of the batched mix, whole
+    pipeline (phase 1 + phase 2 with the reference's stopping rules) one graph after another on the
+    single-graph path, batched, and batched + learned (the proposal where its gate accepts it, batched
+    phase 1 elsewhere); wall clock, edge cut against the one-by-one run."""
+    import torch
+
+    from dmolp_b200.batch import Batch, random_instances
+    from dmolp_b200.learned import WEIGHTS, Proposal
+    from dmolp_b200.partitioner import Partitioner
+
+    inst = random_instances(n, seed=11, vmin=1000, vmax=200_000)
+    p = Partitioner(device)
+    cuts = []
+    t0 = time.perf_counter()
+    for it in inst:
+        p.upload(it.graph)
+        p.phase1(it.k, theta)
+        cuts.append(p.phase2(it.k, mode="ref", records=False).edge_cut)
+    one_s = time.perf_counter() - t0
+    p.close()
+    b = Batch(device)
+    b.upload(inst)
+    b.phase1(theta)  # the host-side hub lists are built once per upload
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.phase1(theta)
+    res, _ = b.run("ref")
+    bat_s = time.perf_counter() - t0
+    same = [r["edge_cut"] for r in res] == cuts
+    m = Proposal(device, WEIGHTS)
+    m.propose(b)  # workspace allocation, once per batch size
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = m.propose(b)
+    if st.any():
+        b.phase1(theta, only=st != 0)
+    res_l, _ = b.run("ref")
+    lrn_s = time.perf_counter() - t0
+    m.close()
+    b.close()
+    tot = float(sum(cuts))
+    return {"graphs": n, "workload": "batched mix (V log-uniform in [1000, 200000], half k-NN, half preferential "
+                                     "attachment, k in 2..64), phase 1 theta %d + phase 2 reference rules" % theta,
+            "plain_one_by_one_graphs_per_s": n / one_s, "plain_batched_graphs_per_s": n / bat_s,
+            "plain_batched_identical_cuts": same, "batched_learned_graphs_per_s": n / lrn_s,
+            "batched_learned_cut_ratio": float(sum(r["edge_cut"] for r in res_l)) / max(1.0, tot),
+            "batched_learned_fallbacks": int((st != 0).sum()),
+            "speedup_batched_learned_vs_plain": one_s / lrn_s}
+
+
 # ------------------------------------------------------------------------------------------- CPU baselines
 def reference_cpu_run(g, labels1, w, repeats: int, iters: int, threads: int, timeout: float = 900,
                       mode: str = "fixed", gpu: bool = False):
@@ -606,6 +657,11 @@ def main():
                 line["cpu_baseline"] = cpu_baseline(g, labels1, w, args)
             except Exception as e:  # report, do not hide
                 line["cpu_baseline"] = {"error": str(e)[:300]}
+        if world == 1 and not args.quick and w["kind"] != "batch":
+            try:
+                line["batched"] = batched_summary(256, 1000, local_rank)
+            except Exception as e:  # report, do not hide
+                line["batched"] = {"error": str(e)[:300]}
         print(json.dumps(line), flush=True)
 
 
