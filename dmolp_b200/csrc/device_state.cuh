@@ -75,7 +75,6 @@ struct Buffers {
     int32_t *stamp = nullptr;  // [nv] iteration stamp of candidate marking (push)
     int32_t *sstamp = nullptr; // [nv] iteration stamp of the selected window (pull)
     int32_t *ndiff = nullptr;  // [nv] neighbours with another label (the boundary test is ndiff > 0)
-    uint16_t *lab16 = nullptr; // [nv] 16-bit copy of label for the neighbour gathers of decisions and updates
     int32_t *cand = nullptr;   // [nv] phase-1 claimed list / stand-alone window list
     int32_t *win[2] = {nullptr, nullptr};  // [nv] each: selected window of the iteration (by parity)
     int32_t *bv = nullptr, *bnew = nullptr;  // [nv] mover pairs of dmolp_lp_apply; phase-1 records

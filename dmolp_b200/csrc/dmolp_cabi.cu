@@ -327,7 +327,6 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     ALLOC(b.stamp, n);
     ALLOC(b.sstamp, n);
     ALLOC(b.ndiff, n);
-    ALLOC(b.lab16, n);
     ALLOC(b.cand, n);
     ALLOC(b.win[0], n);
     ALLOC(b.win[1], n);

@@ -60,18 +60,17 @@ __device__ __forceinline__ int priv_total(const int *h, int eff, int lane) {
 
 // Count labels < eff of the arcs [s, e) into the calling warp's histogram: lane-private counters (eff <= 32,
 // h has 32*32 ints) or a shared histogram h[eff] with one atomic per group of equal labels (__match_any).
-template <typename L>
-__device__ __forceinline__ int64_t warp_count(const int32_t *__restrict__ col, const L *__restrict__ label,
+__device__ __forceinline__ int64_t warp_count(const int32_t *__restrict__ col, const int32_t *__restrict__ label,
                                               int64_t s, int64_t e, int lane, int eff, int *h) {
     if (eff <= 32) {
         return warp_row(col, s, e, lane, [&](int u) {
-            const int lu = (int)label[u];
+            const int lu = label[u];
             if ((unsigned)lu < (unsigned)eff) h[lu * 32 + ((lane + lu) & 31)] += 1;
         }, [] { return false; });
     }
     for (int64_t j0 = s; j0 < e; j0 += 32) {
         const int64_t j = j0 + lane;
-        const int lu = j < e ? (int)label[__ldcs(col + j)] : -1;
+        const int lu = j < e ? label[__ldcs(col + j)] : -1;
         const bool ok = (unsigned)lu < (unsigned)eff;
         const unsigned m = __match_any_sync(DMOLP_FULL_MASK, ok ? lu : -(lane + 1));
         if (ok && lane == __ffs(m) - 1) atomicAdd(&h[lu], __popc(m));

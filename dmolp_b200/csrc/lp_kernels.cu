@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
             for (int j = 0; j < deg; j += 4) {
                 int l[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) l[q] = j + q < deg ? (int)b.lab16[__ldg(b.col + s + j + q)] : -1;
+                for (int q = 0; q < 4; ++q) l[q] = j + q < deg ? b.label[__ldg(b.col + s + j + q)] : -1;
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
                     if ((unsigned)l[q] < (unsigned)eff) {
@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
             else
                 for (int c = lane; c < eff; c += 32) h[c] = 0;
             __syncwarp();
-            warp_count(b.col, b.lab16, s, e, lane, eff, h);
+            warp_count(b.col, b.label, s, e, lane, eff, h);
             __syncwarp();
             double best;
             int blab, own_cnt;
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
             else
                 for (int c = lane; c < eff; c += 32) h[c] = 0;
             __syncwarp();
-            warp_count(b.col, b.lab16, s, e, lane, eff, h);
+            warp_count(b.col, b.label, s, e, lane, eff, h);
             __syncwarp();
             int32_t *row = b.hh + (size_t)ch.x * DMOLP_MAX_K;
             if (priv) {
@@ -505,7 +505,7 @@ __global__ void k_update(Buffers b, int k, int t) {
         long long in_c = 0, out_a = 0, dc = 0;
         int dv = 0;
         warp_row(b.col, s, e, lane, [&](int u) {
-            const int lo = b.lab16[u];
+            const int lo = b.label[u];
             const int nu = b.newlab[u];
             const int ln = nu >= 0 ? nu : lo;
             const int w = nu >= 0 ? 1 : 2;
@@ -552,9 +552,7 @@ __global__ void k_apply(Buffers b) {
     const int n = b.cnt->nchanged;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int v = b.mov[i];
-        const int nl = b.newlab[v];
-        b.label[v] = nl;
-        b.lab16[v] = (uint16_t)nl;
+        b.label[v] = b.newlab[v];
         b.newlab[v] = -1;
     }
 }
@@ -580,7 +578,6 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
     if (bx < a.gv) {
         for (int v = bx * blockDim.x + threadIdx.x; v < a.nv; v += a.gv * blockDim.x) {
             const int lv = b.label[v];
-            b.lab16[v] = (uint16_t)lv;  // -1 and labels >= 65536 never pass an eff test
             if ((unsigned)lv < (unsigned)k) atomicAdd(&svc[lv], 1ull);
             else bad = true;
         }
@@ -798,11 +795,6 @@ __global__ void k_classify(Buffers b, int n, int eff) {
             if (cls == c) b.dec[c][s2] = v;
         }
     }
-}
-
-__global__ void k_lab16(Buffers b, int nv) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
-        b.lab16[v] = (uint16_t)b.label[v];
 }
 
 __global__ void k_zero_small(Buffers b) {
@@ -1083,12 +1075,11 @@ void lp_apply_list(dmolp_ctx *c, int k, int eff, int n) {
     Buffers &b = c->b;
     const int grid = grid_for(c);
     k_zero_small<<<1, 1, 0, c->stream>>>(b);
-    k_lab16<<<grid, kBlock, 0, c->stream>>>(b, (int)c->nv);
     k_classify<<<grid, kBlock, 0, c->stream>>>(b, n, eff);
     launch_decide(c, 1, eff);
     k_collect_moves<<<grid, kBlock, 0, c->stream>>>(b);
     k_apply<<<grid, kBlock, 0, c->stream>>>(b);
-    c->launches += 5;
+    c->launches += 4;
 }
 
 }  // namespace dmolp
