@@ -50,6 +50,25 @@ WORKLOADS = {
 }
 
 
+def rank_seed(seed: int, rank: int) -> int:
+    """Each rank of a multi-GPU run partitions its own batch of graphs (weak scaling, no collective on the
+    data path): the instance generator's seed per rank."""
+    return seed + 1000 * rank
+
+
+def max_over_ranks(dist, values: list[float]) -> list[float]:
+    """Element-wise maximum of per-rank timings (the job's time is its slowest rank's); identity without a
+    process group.  The tensor lives where the backend wants it (GPU for NCCL, host for gloo)."""
+    if not dist:
+        return list(values)
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(values, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def describe(w: dict) -> str:
     if w["kind"] == "batch":
         return (f"{w['n']} graphs, V log-uniform in [{w['vmin']}, {w['vmax']}], half 2-D/3-D k-NN (k_nn 8-14), "
@@ -243,12 +262,7 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
     h2d = g.offsets.nbytes + g.indices.nbytes + g.raw_deg().nbytes + labels1.nbytes
     d2h = labels1.nbytes
 
-    t_max = elapsed
-    e2e_max = e2e_elapsed
-    if dist:
-        t = torch.tensor([elapsed, e2e_elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max, e2e_max = float(t[0]), float(t[1])
+    t_max, e2e_max = max_over_ranks(dist, [elapsed, e2e_elapsed])
     p.close()
     if rank != 0:
         return None
@@ -305,7 +319,7 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
     torch.cuda.set_device(local_rank)
     n = w["n"]
     t0 = time.perf_counter()
-    inst = random_instances(n, seed=w["seed"] + 1000 * rank, vmin=w["vmin"], vmax=w["vmax"])
+    inst = random_instances(n, seed=rank_seed(w["seed"], rank), vmin=w["vmin"], vmax=w["vmax"])
     gen_s = time.perf_counter() - t0
     arrays = union(inst)
     nv_tot, na_tot = int(arrays[0][-1]), int(arrays[1][-1])
@@ -427,11 +441,7 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
     except Exception as e:  # report, do not hide
         pipelines = {"error": str(e)[:300]}
 
-    t_max = elapsed
-    if dist:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t[0])
+    (t_max,) = max_over_ranks(dist, [elapsed])
     if rank != 0:
         return None
     peak, peak_kind = measured_peaks()
