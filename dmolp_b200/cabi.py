@@ -33,6 +33,7 @@ EXPORTS = [
     "dmolp_mpnn_get_params", "dmolp_mpnn_features", "dmolp_mpnn_set_features", "dmolp_mpnn_forward",
     "dmolp_mpnn_prepare_training", "dmolp_mpnn_backward", "dmolp_mpnn_train_step", "dmolp_mpnn_decode",
     "dmolp_batch_propose", "dmolp_mpnn_gate", "dmolp_mpnn_train_gate", "dmolp_batch_phase1",
+    "dmolp_graph_upload_adjtext", "dmolp_graph_load_adjtext", "dmolp_graph_size", "dmolp_graph_get",
 ]
 BATCH_MAX_K = 64
 
@@ -70,6 +71,12 @@ class BatchResult(ctypes.Structure):
                 ("stop_reason", c_int32), ("status", c_int32), ("changes", c_int32)]
 
 
+class IngestInfo(ctypes.Structure):
+    _fields_ = [("num_vertices", c_int64), ("num_arcs", c_int64), ("num_tokens", c_int64),
+                ("rows_sorted_on_device", c_int64), ("read_ms", c_double), ("parse_ms", c_double),
+                ("total_ms", c_double), ("kernels", c_int64)]
+
+
 class BatchP1Result(ctypes.Structure):
     _fields_ = [("num_seeds_found", c_int32), ("rounds", c_int32), ("traversed_edges", c_uint64)]
 
@@ -82,6 +89,10 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_create.argtypes = [c_int, POINTER(vp)]
     lib.dmolp_destroy.argtypes = [vp]
     lib.dmolp_graph_upload.argtypes = [vp, c_int64, c_int64, vp, vp, vp]
+    lib.dmolp_graph_upload_adjtext.argtypes = [vp, c_char_p, c_int64, POINTER(IngestInfo)]
+    lib.dmolp_graph_load_adjtext.argtypes = [vp, c_char_p, POINTER(IngestInfo)]
+    lib.dmolp_graph_size.argtypes = [vp, POINTER(c_int64), POINTER(c_int64)]
+    lib.dmolp_graph_get.argtypes = [vp, vp, vp, vp]
     lib.dmolp_phase1.argtypes = [vp, c_int, c_int, vp, vp, vp, POINTER(Phase1Info)]
     lib.dmolp_lp_run.argtypes = [vp, c_int, POINTER(LpConfig), POINTER(LpResult), vp, c_int]
     lib.dmolp_metrics.argtypes = [vp, c_int, POINTER(c_int64), vp, vp]

@@ -158,4 +158,10 @@ struct dmolp_ctx {
     double prof_ms[5] = {0, 0, 0, 0, 0};
     long long prof_launches[5] = {0, 0, 0, 0, 0};
     double prof_bytes[5] = {0, 0, 0, 0, 0};
+    // pinned staging ring of dmolp_graph_load_adjtext (allocated on first use)
+    char *pin[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t pin_ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
+
+constexpr int kPinSlots = 4;
+constexpr int64_t kPinSlot = 32ll << 20;  // bytes per staging slot

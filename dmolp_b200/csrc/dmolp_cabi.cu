@@ -3,9 +3,13 @@
 // Host-side steps that decide ORDER-dependent results stay on the host, in the reference's exact form:
 // the hub sort (an unstable std::sort over vertices V-1..0, src/phase1/init.cpp:139-177) and the first-seed
 // scan (init.cpp:179-187).  Everything that touches the graph's arcs runs on the device.
+#include <fcntl.h>
 #include <omp.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -13,6 +17,7 @@
 #include <vector>
 
 #include "../../include/dmolp_b200.h"
+#include "ingest.cuh"
 #include "kernels.cuh"
 
 using namespace dmolp;
@@ -206,93 +211,10 @@ void set_last_error(const std::string &msg) { g_err = msg; }
 std::vector<int> hubs_of(const std::vector<int32_t> &degree) { return find_hubs(degree); }
 }  // namespace dmolp
 
-extern "C" {
+namespace {
 
-const char *dmolp_last_error(void) { return g_err.c_str(); }
-
-int dmolp_current_device(void) {
-    int d = 0;
-    if (cudaGetDevice(&d) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return d;
-}
-
-int dmolp_create(int device, dmolp_ctx **out) {
-    if (!out) return fail(DMOLP_ERR_ARG, "out is null");
-    int n = 0;
-    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
-        cudaGetLastError();
-        return fail(DMOLP_ERR_NO_GPU, "no CUDA device");
-    }
-    if (device < 0 || device >= n) return fail(DMOLP_ERR_ARG, "device index out of range");
-    DMOLP_CUDA(cudaSetDevice(device));
-    dmolp_ctx *c = new dmolp_ctx();
-    c->device = device;
-    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
-    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
-    if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
-    if (e != cudaSuccess) {
-        delete c;
-        return fail(DMOLP_ERR_CUDA, std::string("stream/event: ") + cudaGetErrorString(e));
-    }
-    *out = c;
-    return DMOLP_OK;
-}
-
-int dmolp_destroy(dmolp_ctx *c) {
-    if (!c) return DMOLP_OK;
-    cudaSetDevice(c->device);
-    cudaStreamSynchronize(c->stream);
-    free_all(c);
-    if (c->ev0) cudaEventDestroy(c->ev0);
-    if (c->ev1) cudaEventDestroy(c->ev1);
-    if (c->stream) cudaStreamDestroy(c->stream);
-    delete c;
-    return DMOLP_OK;
-}
-
-int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *off, const int32_t *col,
-                       const int32_t *raw) {
-    if (!c) return fail(DMOLP_ERR_ARG, "null context");
-    if (nv < 0 || nv > 0x7ffffffe || narcs < 0 || (!off && nv >= 0) || (!col && narcs > 0))
-        return fail(DMOLP_ERR_ARG, "bad graph sizes or null arrays");
-    if (off[0] != 0 || off[nv] != narcs) return fail(DMOLP_ERR_ARG, "offsets must start at 0 and end at narcs");
-    // Validate on the host: every device access below is then in bounds.
-    int bad = 0, unsorted = 0;
-    int64_t maxdeg = 0, maxraw = 0;
-#pragma omp parallel for reduction(| : bad, unsorted) reduction(max : maxdeg, maxraw) schedule(static)
-    for (int64_t v = 0; v < nv; ++v) {
-        const int64_t d = off[v + 1] - off[v];
-        if (d < 0 || d > 0x7fffffff) bad |= 1;
-        maxdeg = std::max(maxdeg, d);
-        if (raw) {
-            if (raw[v] < 0) bad |= 4;
-            maxraw = std::max(maxraw, (int64_t)raw[v]);
-        }
-    }
-    if (!raw) maxraw = maxdeg;
-    if (!bad) {
-#pragma omp parallel for reduction(| : bad) schedule(static)
-        for (int64_t j = 0; j < narcs; ++j)
-            if ((uint32_t)col[j] >= (uint64_t)nv) bad |= 2;
-    }
-    if (!bad) {  // rows strictly increasing: a precondition of the symmetry test
-#pragma omp parallel for reduction(| : unsorted) schedule(dynamic, 4096)
-        for (int64_t v = 0; v < nv; ++v)
-            for (int64_t j = off[v] + 1; j < off[v + 1]; ++j)
-                if (col[j] <= col[j - 1]) {
-                    unsorted = 1;
-                    break;
-                }
-    }
-    if (bad & 1) return fail(DMOLP_ERR_ARG, "offsets are not non-decreasing");
-    if (bad & 2) return fail(DMOLP_ERR_ARG, "a neighbour id is outside [0, nv)");
-    if (bad & 4) return fail(DMOLP_ERR_ARG, "negative raw degree");
-
-    DMOLP_CUDA(cudaSetDevice(c->device));
+// Frees the previous graph and allocates every resident buffer for a graph of the given sizes.
+int graph_alloc(dmolp_ctx *c, int64_t nv, int64_t narcs, int64_t maxdeg, int64_t maxraw, const int64_t nbc[3]) {
     DMOLP_CUDA(cudaStreamSynchronize(c->stream));
     free_all(c);
     c->nv = nv;
@@ -302,19 +224,10 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     c->ibits = bits_for(nv > 0 ? nv - 1 : 0);
     c->dbits = bits_for(maxdeg);
     c->rbits = bits_for(maxraw);
-    c->h_rawdeg.resize(nv);
-    for (int64_t v = 0; v < nv; ++v) c->h_rawdeg[v] = raw ? raw[v] : (int32_t)(off[v + 1] - off[v]);
-    // degree classes (isolated vertices belong to none: they are never on a boundary)
-    std::vector<int32_t> bl[3];
-    for (int64_t v = 0; v < nv; ++v) {
-        const int64_t d = off[v + 1] - off[v];
-        if (d == 0) continue;
-        bl[d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2)].push_back((int32_t)v);
-    }
-    for (int i = 0; i < 3; ++i) c->nb[i] = (int)bl[i].size();
+    for (int i = 0; i < 3; ++i) c->nb[i] = (int)nbc[i];
     c->chunk_cap = narcs / kChunk + 2;
-    c->hubq_cap = narcs / kHubChunk + (int64_t)bl[2].size() + 2;
-
+    c->hubq_cap = narcs / kHubChunk + nbc[2] + 2;
+    const size_t nball[3] = {(size_t)nbc[0], (size_t)nbc[1], (size_t)nbc[2]};
     Buffers &b = c->b;
     const size_t n = (size_t)nv + 1;
     int st = DMOLP_OK;
@@ -361,31 +274,31 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     ALLOC(b.p1cnt, 8);
     ALLOC(b.p1te, 1);
     ALLOC(b.flag, 1);
-    ALLOC(b.ball, bl[0].size() + bl[1].size() + bl[2].size());
+    ALLOC(b.ball, nball[0] + nball[1] + nball[2]);
     b.bucket[0] = b.ball;
-    b.bucket[1] = b.ball + bl[0].size();
-    b.bucket[2] = b.bucket[1] + bl[1].size();
+    b.bucket[1] = b.ball + nball[0];
+    b.bucket[2] = b.bucket[1] + nball[1];
     for (int i = 0; i < 3; ++i) ALLOC(b.dec[i], n);
     ALLOC(b.newlab, n);
     ALLOC(b.mov, n);
     ALLOC(b.chunkq, (size_t)c->chunk_cap);
     ALLOC(b.hubq, (size_t)c->hubq_cap);
-    ALLOC(b.hh, bl[2].size() * (size_t)DMOLP_MAX_K);
+    ALLOC(b.hh, nball[2] * (size_t)DMOLP_MAX_K);
 #undef ALLOC
     b.claim = b.stamp;  // phase 1 and the LP loop never run at the same time
-    DMOLP_CUDA(cudaMemcpyAsync(b.off, off, n * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
-    if (narcs)
-        DMOLP_CUDA(cudaMemcpyAsync(b.col, col, (size_t)narcs * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
-    DMOLP_CUDA(cudaMemcpyAsync(b.rawdeg, c->h_rawdeg.data(), (size_t)nv * sizeof(int32_t), cudaMemcpyHostToDevice,
-                               c->stream));
+    return DMOLP_OK;
+}
+
+// After off, col, rawdeg and the degree-class lists are on the device: clears the loop state, tests
+// whether every arc has its reverse (when rows are strictly increasing) and loads the log / exp tables.
+int graph_finish(dmolp_ctx *c, bool rows_sorted) {
+    Buffers &b = c->b;
+    const int64_t nv = c->nv;
+    const size_t n = (size_t)nv + 1;
     DMOLP_CUDA(cudaMemsetAsync(b.label, 0, n * sizeof(int32_t), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.hist, 0, (size_t)DMOLP_MAX_K * kRadix * sizeof(unsigned int), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.ctrl, 0, sizeof(LpControl), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.cnt, 0, sizeof(LpCounters), c->stream));
-    for (int i = 0; i < 3; ++i)
-        if (!bl[i].empty())
-            DMOLP_CUDA(cudaMemcpyAsync(b.bucket[i], bl[i].data(), bl[i].size() * sizeof(int32_t),
-                                       cudaMemcpyHostToDevice, c->stream));
     const int npos = c->nb[0] + c->nb[1] + c->nb[2];
     DMOLP_CUDA(cudaMemcpyAsync(&b.cnt->npos, &npos, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.bown, 0xff, n * sizeof(int32_t), c->stream));  // all record slots empty
@@ -394,7 +307,7 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     // every arc has its reverse (checked on the device): the LP loop may update its statistics from the
     // movers alone
     c->symmetric = false;
-    if (!unsorted && nv > 0) {
+    if (rows_sorted && nv > 0) {
         // the arc counts borrow the (zeroed) radix-select histogram and leave it zeroed
         unsigned long long *counts = reinterpret_cast<unsigned long long *>(b.hist);
         DMOLP_CUDA(cudaMemsetAsync(b.flag, 0, sizeof(int), c->stream));
@@ -422,6 +335,312 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     if (s2) return s2;
     c->has_graph = true;
     return DMOLP_OK;
+}
+
+// Device buffer for `len` bytes of text, padded to whole parse tiles (padding zeroed).
+int text_buffer(dmolp_ctx *c, int64_t len, uint8_t **out) {
+    const int64_t cap = ingest::padded_bytes(len);
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, (size_t)cap);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DMOLP_ERR_NOMEM, std::string("cudaMalloc (text): ") + cudaGetErrorString(e));
+    }
+    *out = (uint8_t *)q;
+    DMOLP_CUDA(cudaMemsetAsync(*out + len, 0, (size_t)(cap - len), c->stream));
+    return DMOLP_OK;
+}
+
+int pinned_ring(dmolp_ctx *c) {
+    for (int s = 0; s < kPinSlots; ++s) {
+        if (!c->pin[s]) DMOLP_CUDA(cudaHostAlloc((void **)&c->pin[s], kPinSlot, cudaHostAllocDefault));
+        if (!c->pin_ev[s]) DMOLP_CUDA(cudaEventCreateWithFlags(&c->pin_ev[s], cudaEventDisableTiming));
+    }
+    return DMOLP_OK;
+}
+
+// Parse the text on the device into the resident CSR.  A text the parse rejects leaves the previous graph
+// in place; a CUDA failure after that leaves no graph.
+int ingest_text(dmolp_ctx *c, uint8_t *d_txt, int64_t len, int64_t body0, int64_t body1, dmolp_ingest_info *info) {
+    ingest::Parsed p;
+    std::string err;
+    DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
+    if (ingest::parse(c->stream, d_txt, len, body0, body1, p, err)) {
+        ingest::release(p);
+        cudaGetLastError();
+        return fail(DMOLP_ERR_ARG, err);
+    }
+    int st = graph_alloc(c, p.nv, p.narcs, p.maxdeg, p.maxraw, p.nb);
+    if (!st) {
+        Buffers &b = c->b;
+        int32_t *const bucket[3] = {b.bucket[0], b.bucket[1], b.bucket[2]};
+        if (ingest::build(c->stream, p, b.off, b.col, b.rawdeg, bucket, err)) st = fail(DMOLP_ERR_CUDA, err);
+    }
+    if (!st) {
+        DMOLP_CUDA(cudaEventRecord(c->ev1, c->stream));
+        c->h_rawdeg.resize(p.nv);
+        if (p.nv)
+            DMOLP_CUDA(cudaMemcpyAsync(c->h_rawdeg.data(), c->b.rawdeg, (size_t)p.nv * sizeof(int32_t),
+                                       cudaMemcpyDeviceToHost, c->stream));
+        st = sync(c);
+    }
+    c->launches += p.launches;
+    if (info) {
+        info->num_vertices = p.nv;
+        info->num_arcs = p.narcs;
+        info->num_tokens = p.ntok;
+        info->rows_sorted_on_device = p.rows_sorted;
+        info->parse_ms = 0.0;
+        float ms = 0.f;
+        if (!st && cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) info->parse_ms = ms;
+        info->kernels = p.launches;
+    }
+    ingest::release(p);
+    if (st) {
+        free_all(c);
+        return st;
+    }
+    return graph_finish(c, true);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *dmolp_last_error(void) { return g_err.c_str(); }
+
+int dmolp_current_device(void) {
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return d;
+}
+
+int dmolp_create(int device, dmolp_ctx **out) {
+    if (!out) return fail(DMOLP_ERR_ARG, "out is null");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(DMOLP_ERR_NO_GPU, "no CUDA device");
+    }
+    if (device < 0 || device >= n) return fail(DMOLP_ERR_ARG, "device index out of range");
+    DMOLP_CUDA(cudaSetDevice(device));
+    dmolp_ctx *c = new dmolp_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(DMOLP_ERR_CUDA, std::string("stream/event: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return DMOLP_OK;
+}
+
+int dmolp_destroy(dmolp_ctx *c) {
+    if (!c) return DMOLP_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_all(c);
+    for (int i = 0; i < kPinSlots; ++i) {
+        if (c->pin[i]) cudaFreeHost(c->pin[i]);
+        if (c->pin_ev[i]) cudaEventDestroy(c->pin_ev[i]);
+    }
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return DMOLP_OK;
+}
+
+int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *off, const int32_t *col,
+                       const int32_t *raw) {
+    if (!c) return fail(DMOLP_ERR_ARG, "null context");
+    if (nv < 0 || nv > 0x7ffffffe || narcs < 0 || (!off && nv >= 0) || (!col && narcs > 0))
+        return fail(DMOLP_ERR_ARG, "bad graph sizes or null arrays");
+    if (off[0] != 0 || off[nv] != narcs) return fail(DMOLP_ERR_ARG, "offsets must start at 0 and end at narcs");
+    // Validate on the host: every device access below is then in bounds.
+    int bad = 0, unsorted = 0;
+    int64_t maxdeg = 0, maxraw = 0;
+#pragma omp parallel for reduction(| : bad, unsorted) reduction(max : maxdeg, maxraw) schedule(static)
+    for (int64_t v = 0; v < nv; ++v) {
+        const int64_t d = off[v + 1] - off[v];
+        if (d < 0 || d > 0x7fffffff) bad |= 1;
+        maxdeg = std::max(maxdeg, d);
+        if (raw) {
+            if (raw[v] < 0) bad |= 4;
+            maxraw = std::max(maxraw, (int64_t)raw[v]);
+        }
+    }
+    if (!raw) maxraw = maxdeg;
+    if (!bad) {
+#pragma omp parallel for reduction(| : bad) schedule(static)
+        for (int64_t j = 0; j < narcs; ++j)
+            if ((uint32_t)col[j] >= (uint64_t)nv) bad |= 2;
+    }
+    if (!bad) {  // rows strictly increasing: a precondition of the symmetry test
+#pragma omp parallel for reduction(| : unsorted) schedule(dynamic, 4096)
+        for (int64_t v = 0; v < nv; ++v)
+            for (int64_t j = off[v] + 1; j < off[v + 1]; ++j)
+                if (col[j] <= col[j - 1]) {
+                    unsorted = 1;
+                    break;
+                }
+    }
+    if (bad & 1) return fail(DMOLP_ERR_ARG, "offsets are not non-decreasing");
+    if (bad & 2) return fail(DMOLP_ERR_ARG, "a neighbour id is outside [0, nv)");
+    if (bad & 4) return fail(DMOLP_ERR_ARG, "negative raw degree");
+
+    // degree classes (isolated vertices belong to none: they are never on a boundary)
+    std::vector<int32_t> bl[3];
+    for (int64_t v = 0; v < nv; ++v) {
+        const int64_t d = off[v + 1] - off[v];
+        if (d == 0) continue;
+        bl[d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2)].push_back((int32_t)v);
+    }
+    const int64_t nb[3] = {(int64_t)bl[0].size(), (int64_t)bl[1].size(), (int64_t)bl[2].size()};
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    int st = graph_alloc(c, nv, narcs, maxdeg, maxraw, nb);
+    if (st) return st;
+    c->h_rawdeg.resize(nv);
+    for (int64_t v = 0; v < nv; ++v) c->h_rawdeg[v] = raw ? raw[v] : (int32_t)(off[v + 1] - off[v]);
+    Buffers &b = c->b;
+    DMOLP_CUDA(cudaMemcpyAsync(b.off, off, (size_t)(nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+    if (narcs)
+        DMOLP_CUDA(cudaMemcpyAsync(b.col, col, (size_t)narcs * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(b.rawdeg, c->h_rawdeg.data(), (size_t)nv * sizeof(int32_t), cudaMemcpyHostToDevice,
+                               c->stream));
+    for (int i = 0; i < 3; ++i)
+        if (!bl[i].empty())
+            DMOLP_CUDA(cudaMemcpyAsync(b.bucket[i], bl[i].data(), bl[i].size() * sizeof(int32_t),
+                                       cudaMemcpyHostToDevice, c->stream));
+    return graph_finish(c, !unsorted);
+}
+
+int dmolp_graph_upload_adjtext(dmolp_ctx *c, const char *text, int64_t len, dmolp_ingest_info *info) {
+    if (!c) return fail(DMOLP_ERR_ARG, "null context");
+    if (len < 0 || (!text && len > 0)) return fail(DMOLP_ERR_ARG, "bad text buffer");
+    const auto t0 = std::chrono::steady_clock::now();
+    const char *nl = len > 0 ? (const char *)memchr(text, '\n', (size_t)len) : nullptr;
+    if (!nl) return fail(DMOLP_ERR_ARG, "missing header line");
+    const int64_t body0 = (int64_t)(nl - text) + 1;
+    int64_t body1 = len;  // anything after the last newline is an unterminated line: dropped
+    while (body1 > body0 && text[body1 - 1] != '\n') --body1;
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    uint8_t *d_txt = nullptr;
+    int st = text_buffer(c, len, &d_txt);
+    if (st) return st;
+    DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(d_txt, text, (size_t)len, cudaMemcpyHostToDevice, c->stream));
+    DMOLP_CUDA(cudaEventRecord(c->ev1, c->stream));
+    DMOLP_CUDA(cudaEventSynchronize(c->ev1));
+    float copy_ms = 0.f;
+    cudaEventElapsedTime(&copy_ms, c->ev0, c->ev1);
+    st = ingest_text(c, d_txt, len, body0, body1, info);
+    cudaFree(d_txt);
+    if (info) {
+        info->read_ms = copy_ms;
+        info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return st;
+}
+
+int dmolp_graph_load_adjtext(dmolp_ctx *c, const char *path, dmolp_ingest_info *info) {
+    if (!c || !path) return fail(DMOLP_ERR_ARG, "null context or path");
+    const auto t0 = std::chrono::steady_clock::now();
+    const int fd = open(path, O_RDONLY);
+    if (fd < 0) return fail(DMOLP_ERR_ARG, std::string("cannot open ") + path);
+    struct stat sb;
+    if (fstat(fd, &sb) != 0) {
+        close(fd);
+        return fail(DMOLP_ERR_ARG, std::string("cannot stat ") + path);
+    }
+    const int64_t len = (int64_t)sb.st_size;
+    int st = DMOLP_OK;
+    uint8_t *d_txt = nullptr;
+    if (cudaSetDevice(c->device) != cudaSuccess) st = fail(DMOLP_ERR_CUDA, "cudaSetDevice failed");
+    if (!st) st = text_buffer(c, len, &d_txt);
+    if (!st) st = pinned_ring(c);
+    // Read slot-sized pieces with all host threads into pinned memory and copy each to the device while
+    // the next is read; note the first and the last newline on the way.
+    int64_t body0 = -1, body1 = -1;
+    for (int64_t pos = 0, i = 0; !st && pos < len; pos += kPinSlot, ++i) {
+        const int s = (int)(i % kPinSlots);
+        if (i >= kPinSlots && cudaEventSynchronize(c->pin_ev[s]) != cudaSuccess) {
+            st = fail(DMOLP_ERR_CUDA, "pinned copy failed");
+            break;
+        }
+        const int64_t n = std::min<int64_t>(kPinSlot, len - pos);
+        char *dst = c->pin[s];
+        int ok = 1;
+        const int T = std::max(1, std::min(omp_get_max_threads(), 16));
+#pragma omp parallel for num_threads(T) reduction(& : ok) schedule(static, 1)
+        for (int t = 0; t < T; ++t) {
+            int64_t a = n * t / T;
+            const int64_t z = n * (t + 1) / T;
+            while (a < z) {
+                const ssize_t r = pread(fd, dst + a, (size_t)(z - a), (off_t)(pos + a));
+                if (r <= 0) {
+                    ok = 0;
+                    break;
+                }
+                a += r;
+            }
+        }
+        if (!ok) {
+            st = fail(DMOLP_ERR_ARG, std::string("short read of ") + path);
+            break;
+        }
+        if (body0 < 0) {
+            const char *q = (const char *)memchr(dst, '\n', (size_t)n);
+            if (q) body0 = pos + (q - dst) + 1;
+        }
+        for (int64_t j = n; j > 0; --j)
+            if (dst[j - 1] == '\n') {
+                body1 = pos + j;
+                break;
+            }
+        if (cudaMemcpyAsync(d_txt + pos, dst, (size_t)n, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+            cudaEventRecord(c->pin_ev[s], c->stream) != cudaSuccess)
+            st = fail(DMOLP_ERR_CUDA, "text copy failed");
+    }
+    close(fd);
+    if (!st && cudaStreamSynchronize(c->stream) != cudaSuccess) st = fail(DMOLP_ERR_CUDA, "text copy failed");
+    const double read_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (!st && body0 < 0) st = fail(DMOLP_ERR_ARG, "missing header line");
+    if (!st) st = ingest_text(c, d_txt, len, body0, std::max(body0, body1), info);
+    if (d_txt) cudaFree(d_txt);
+    if (info) {
+        info->read_ms = read_ms;
+        info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return st;
+}
+
+int dmolp_graph_size(dmolp_ctx *c, int64_t *nv, int64_t *narcs) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    if (nv) *nv = c->nv;
+    if (narcs) *narcs = c->narcs;
+    return DMOLP_OK;
+}
+
+int dmolp_graph_get(dmolp_ctx *c, int64_t *offsets, int32_t *indices, int32_t *raw_degree) {
+    if (!c || !c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    if (offsets)
+        DMOLP_CUDA(cudaMemcpyAsync(offsets, c->b.off, (size_t)(c->nv + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    if (indices && c->narcs)
+        DMOLP_CUDA(cudaMemcpyAsync(indices, c->b.col, (size_t)c->narcs * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    if (raw_degree && c->nv)
+        DMOLP_CUDA(cudaMemcpyAsync(raw_degree, c->b.rawdeg, (size_t)c->nv * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                   c->stream));
+    return sync(c);
 }
 
 int dmolp_labels_get(dmolp_ctx *c, int32_t *labels) {

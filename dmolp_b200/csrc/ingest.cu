@@ -1,0 +1,711 @@
+// Device parse of the reference's adjacency text into the resident CSR (declarations in ingest.cuh).
+//
+// Semantics (the reference's load_graph, src/phase1/init.cpp:15-100, as the host loader adjtext.cpp
+// restates them): the body is every newline-terminated line after the header; line v lists the neighbours
+// of vertex v.  fast_atoi tokenisation: a token starts at the first byte of a non-empty line and at every
+// digit that follows a non-digit; its value is its run of digits (empty: 0).  A NUL byte ends the parse of
+// its line.  The raw degree is the token count; the CSR row is the sorted, de-duplicated token list
+// (src/phase1/partition.cpp:227-262, self-loops kept).  An id >= V is rejected.
+//
+// Text passes are tiled: a block reads 16 KiB as 4 steps of 256 coalesced 16-byte loads, classifies the
+// 16 bytes of a load with byte-SIMD compares into newline / digit / NUL bit masks, and emits tokens in
+// text order from a block scan of per-thread counts plus the tile's prefix (count pass -> scan -> emit
+// pass).  Rows that are not strictly increasing (only in hand-written input: the reference's converter
+// writes sorted rows) are sorted on the device, by length class, then de-duplicated by a token scan.
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "device_state.cuh"
+#include "ingest.cuh"
+
+namespace dmolp {
+namespace ingest {
+namespace {
+
+constexpr uint32_t kFirst = 0x80000000u;  // token flag: first token of its line
+constexpr uint32_t kVal = 0x7fffffffu;
+constexpr int kSmallRow = 32;             // unsorted rows up to this length: one thread sorts
+constexpr int kMidRow = 4096;             // ... up to this length: one block, in shared memory
+constexpr int kNW = kTxtThreads / 32;
+
+struct Scal {
+    unsigned long long nul;         // NUL bytes in the body
+    unsigned long long violations;  // tokens not above their predecessor in the same line
+    unsigned long long maxdeg, maxraw;
+    int bad_id;                     // some token >= V
+    int nlist[3];                   // unsorted rows per length class
+};
+
+// 0xff/0x00 per byte -> one bit per byte (byte 0 -> bit 0)
+__device__ __forceinline__ uint32_t byte_bits(uint32_t m) { return ((m & 0x80808080u) * 0x00204081u) >> 28; }
+
+struct Chunk {
+    uint32_t nl, zero, dig, body, ts;  // 16-bit masks over the chunk's bytes; ts = token starts
+    uint32_t prev_nl;                  // (nl << 1) | previous byte is a newline
+};
+
+// Classify the 16 bytes at `pos` (16-aligned).  All 32 lanes must call it (the previous byte comes from
+// the neighbouring lane).
+__device__ __forceinline__ Chunk chunk_at(const uint8_t *__restrict__ txt, int64_t pos, int64_t body0, int64_t body1) {
+    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(txt + pos));
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+    Chunk c;
+    c.nl = c.zero = c.dig = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        c.nl |= byte_bits(__vcmpeq4(w[i], 0x0a0a0a0au)) << (4 * i);
+        c.zero |= byte_bits(__vcmpeq4(w[i], 0u)) << (4 * i);
+        c.dig |= byte_bits(__vcmpgeu4(w[i], 0x30303030u) & __vcmpleu4(w[i], 0x39393939u)) << (4 * i);
+    }
+    const int lane = threadIdx.x & 31;
+    uint32_t pb = __shfl_up_sync(DMOLP_FULL_MASK, q.w >> 24, 1);
+    if (lane == 0) pb = pos > 0 ? txt[pos - 1] : 0u;
+    const uint32_t pnl = pb == '\n', pdig = pb - '0' <= 9u;
+    const int64_t lo = body0 - pos, hi = body1 - pos;
+    const uint32_t below = lo <= 0 ? 0u : (lo >= 16 ? 0xffffu : (1u << lo) - 1);
+    const uint32_t upto = hi <= 0 ? 0u : (hi >= 16 ? 0xffffu : (1u << hi) - 1);
+    c.body = upto & ~below;
+    c.prev_nl = ((c.nl << 1) | pnl) & 0xffffu;
+    const uint32_t prev_dig = ((c.dig << 1) | pdig) & 0xffffu;
+    c.ts = c.body & ~c.nl & ~c.zero & (c.prev_nl | (c.dig & ~prev_dig));
+    return c;
+}
+
+// Exclusive block scan of a 32-bit value (packed counters whose block totals cannot carry).
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *total, uint32_t *s_w) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(DMOLP_FULL_MASK, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_w[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t x = lane < kNW ? s_w[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(DMOLP_FULL_MASK, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane < kNW) s_w[lane] = x;
+    }
+    __syncthreads();
+    const uint32_t before = wid ? s_w[wid - 1] : 0u;
+    *total = s_w[kNW - 1];
+    __syncthreads();  // s_w is reused by the next call
+    return before + incl - v;
+}
+
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t *s_w) {
+    uint32_t t;
+    block_excl_scan(v, &t, s_w);
+    return t;
+}
+
+// ---- text passes ----
+
+__global__ void __launch_bounds__(kTxtThreads) k_txt_count(const uint8_t *__restrict__ txt, int64_t body0,
+                                                           int64_t body1, uint32_t *__restrict__ tcnt, Scal *sc) {
+    __shared__ uint32_t s_w[kNW];
+    const int64_t tile = blockIdx.x;
+    uint32_t nl = 0, tk = 0, nz = 0;
+#pragma unroll
+    for (int s = 0; s < kTxtSteps; ++s) {
+        const int64_t pos = tile * kTileBytes + (int64_t)(s * kTxtThreads + threadIdx.x) * kChunkBytes;
+        const Chunk c = chunk_at(txt, pos, body0, body1);
+        nl += __popc(c.nl & c.body);
+        tk += __popc(c.ts);
+        nz += __popc(c.zero & c.body);
+    }
+    // tile totals are at most 16 Ki each: pack two per word
+    const uint32_t nlt = block_sum(nl | (tk << 16), s_w);
+    const uint32_t nzt = block_sum(nz, s_w);
+    if (threadIdx.x == 0) {
+        tcnt[2 * tile] = nlt & 0xffffu;
+        tcnt[2 * tile + 1] = nlt >> 16;
+        if (nzt) atomicAdd(&sc->nul, (unsigned long long)nzt);
+    }
+}
+
+// A NUL ends the parse of its line: zero every byte from each NUL up to the next NUL or newline, so that
+// no token starts after the first NUL of a line.  Writers only ever store zeros below the line's newline,
+// so overlapping walks are harmless.
+__global__ void k_txt_nulfill(uint8_t *txt, int64_t body0, int64_t body1) {
+    const int64_t c0 = body0 / 16, c1 = (body1 + 15) / 16;
+    for (int64_t ci = c0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; ci < c1;
+         ci += (int64_t)gridDim.x * blockDim.x) {
+        for (int j = 0; j < 16; ++j) {
+            const int64_t p = ci * 16 + j;
+            if (p < body0 || p >= body1 || txt[p] != 0) continue;
+            for (int64_t q = p + 1; q < body1; ++q) {
+                const uint8_t b = ((volatile uint8_t *)txt)[q];
+                if (b == '\n' || b == 0) break;
+                ((volatile uint8_t *)txt)[q] = 0;
+            }
+        }
+    }
+}
+
+// Exclusive prefix over n records of NC 32-bit counters: out[i*NC+c] = sum_{j<i} cnt[j*NC+c],
+// out[n*NC+c] = total.  One block; each thread owns a contiguous range of records.
+template <int NC>
+__global__ void __launch_bounds__(1024) k_scan(const uint32_t *__restrict__ cnt, int64_t n, int64_t *__restrict__ out) {
+    __shared__ long long s_w[32][NC];
+    const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int64_t per = (n + T - 1) / T;
+    const int64_t a = std::min<int64_t>(n, tid * per), z = std::min<int64_t>(n, a + per);
+    long long s[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) s[c] = 0;
+    for (int64_t i = a; i < z; ++i)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) s[c] += cnt[i * NC + c];
+    long long incl[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        incl[c] = s[c];
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(DMOLP_FULL_MASK, incl[c], o);
+            if (lane >= o) incl[c] += y;
+        }
+        if (lane == 31) s_w[wid][c] = incl[c];
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = T / 32;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            long long x = lane < nw ? s_w[lane][c] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long y = __shfl_up_sync(DMOLP_FULL_MASK, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane < nw) s_w[lane][c] = x;
+        }
+    }
+    __syncthreads();
+    long long run[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) run[c] = (wid ? s_w[wid - 1][c] : 0) + incl[c] - s[c];
+    for (int64_t i = a; i < z; ++i)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            out[i * NC + c] = run[c];
+            run[c] += cnt[i * NC + c];
+        }
+    if (tid == T - 1)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) out[n * NC + c] = run[c];
+}
+
+// Tokens in text order: value (bit 31 = first token of its line); end_tok[l] = tokens before line l's
+// newline.  Values are parsed with saturation at 2^31, so any id >= V is caught.
+__global__ void __launch_bounds__(kTxtThreads) k_txt_emit(const uint8_t *__restrict__ txt, int64_t body0,
+                                                          int64_t body1, int64_t nv, const int64_t *__restrict__ toff,
+                                                          uint32_t *__restrict__ tok, int64_t *__restrict__ end_tok,
+                                                          Scal *sc) {
+    __shared__ uint32_t s_w[kNW];
+    const int64_t tile = blockIdx.x;
+    int64_t lbase = toff[2 * tile], tbase = toff[2 * tile + 1];
+    int bad = 0;
+#pragma unroll 1
+    for (int s = 0; s < kTxtSteps; ++s) {
+        const int64_t pos = tile * kTileBytes + (int64_t)(s * kTxtThreads + threadIdx.x) * kChunkBytes;
+        const Chunk c = chunk_at(txt, pos, body0, body1);
+        const uint32_t nlm = c.nl & c.body;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan((uint32_t)__popc(nlm) << 16 | (uint32_t)__popc(c.ts), &tot, s_w);
+        int64_t l = lbase + (ex >> 16), t = tbase + (ex & 0xffffu);
+        uint32_t ev = nlm | c.ts;
+        while (ev) {
+            const int j = __ffs(ev) - 1;
+            ev &= ev - 1;
+            if ((nlm >> j) & 1u) {
+                end_tok[l++] = t;
+            } else {
+                uint64_t x = 0;
+                if ((c.dig >> j) & 1u) {
+                    int64_t q = pos + j;
+                    uint32_t b = txt[q];
+                    while (b - '0' <= 9u) {
+                        x = x * 10 + (b - '0');
+                        if (x > kVal) x = (uint64_t)kVal + 1;
+                        b = txt[++q];
+                    }
+                }
+                if ((int64_t)x >= nv) bad = 1;
+                tok[t++] = ((uint32_t)x & kVal) | (((c.prev_nl >> j) & 1u) ? kFirst : 0u);
+            }
+        }
+        lbase += tot >> 16;
+        tbase += tot & 0xffffu;
+    }
+    if (bad) atomicOr(&sc->bad_id, 1);
+}
+
+// ---- row order ----
+
+__device__ __forceinline__ int64_t row_of(const int64_t *__restrict__ end_tok, int64_t nv, int64_t t) {
+    int64_t lo = 0, hi = nv;  // first line whose newline comes after token t
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (end_tok[mid] > t) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+__global__ void k_tok_check(const uint32_t *__restrict__ tok, int64_t ntok, const int64_t *__restrict__ end_tok,
+                            int64_t nv, uint8_t *__restrict__ badrow, Scal *sc) {
+    unsigned long long nbad = 0;
+    for (int64_t t = 1 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntok; t += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t cur = tok[t];
+        if (cur & kFirst) continue;
+        if ((cur & kVal) <= (tok[t - 1] & kVal)) {
+            ++nbad;
+            badrow[row_of(end_tok, nv, t)] = 1;
+        }
+    }
+    nbad = warp_sum_u64(nbad);
+    if ((threadIdx.x & 31) == 0 && nbad) atomicAdd(&sc->violations, nbad);
+}
+
+__global__ void k_rows_classify(const int64_t *__restrict__ end_tok, int64_t nv, const uint8_t *__restrict__ badrow,
+                                int32_t *__restrict__ lists, Scal *sc) {
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < nv; l += (int64_t)gridDim.x * blockDim.x) {
+        if (!badrow[l]) continue;
+        const int64_t len = end_tok[l] - (l ? end_tok[l - 1] : 0);
+        const int cls = len <= kSmallRow ? 0 : (len <= kMidRow ? 1 : 2);
+        lists[cls * nv + atomicAdd(&sc->nlist[cls], 1)] = (int32_t)l;
+    }
+}
+
+__device__ __forceinline__ void row_bounds(const int64_t *end_tok, int64_t l, int64_t *s, int64_t *e) {
+    *s = l ? end_tok[l - 1] : 0;
+    *e = end_tok[l];
+}
+
+__global__ void k_sort_small(uint32_t *__restrict__ tok, const int64_t *__restrict__ end_tok,
+                             const int32_t *__restrict__ list, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t s, e;
+    row_bounds(end_tok, list[i], &s, &e);
+    const int len = (int)(e - s);
+    uint32_t a[kSmallRow];
+    for (int j = 0; j < len; ++j) {
+        const uint32_t x = tok[s + j] & kVal;
+        int q = j;
+        while (q > 0 && a[q - 1] > x) {
+            a[q] = a[q - 1];
+            --q;
+        }
+        a[q] = x;
+    }
+    for (int j = 0; j < len; ++j) tok[s + j] = a[j] | (j == 0 ? kFirst : 0u);
+}
+
+// In-place bitonic sort of a[0..P) (P a power of two) by all threads of the block.
+__device__ __forceinline__ void bitonic(uint32_t *a, int P) {
+    for (int k = 2; k <= P; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                const int x = i ^ j;
+                if (x > i) {
+                    const uint32_t u = a[i], v = a[x];
+                    if ((u > v) == ((i & k) == 0)) {
+                        a[i] = v;
+                        a[x] = u;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+}
+
+__global__ void __launch_bounds__(512) k_sort_mid(uint32_t *__restrict__ tok, const int64_t *__restrict__ end_tok,
+                                                  const int32_t *__restrict__ list) {
+    __shared__ uint32_t a[kMidRow];
+    int64_t s, e;
+    row_bounds(end_tok, list[blockIdx.x], &s, &e);
+    const int len = (int)(e - s);
+    int P = 2;
+    while (P < len) P <<= 1;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) a[i] = i < len ? (tok[s + i] & kVal) : 0xffffffffu;
+    __syncthreads();
+    bitonic(a, P);
+    for (int i = threadIdx.x; i < len; i += blockDim.x) tok[s + i] = a[i] | (i == 0 ? kFirst : 0u);
+}
+
+// Rows above kMidRow tokens: sort kMidRow-token chunks in shared memory, then merge pairs of runs in
+// global memory (tok <-> tmp), the block's threads splitting each merge's output along the merge path.
+__global__ void __launch_bounds__(1024) k_sort_big(uint32_t *__restrict__ tok, uint32_t *__restrict__ tmp,
+                                                   const int64_t *__restrict__ end_tok, const int32_t *__restrict__ list) {
+    __shared__ uint32_t a[kMidRow];
+    int64_t s, e;
+    row_bounds(end_tok, list[blockIdx.x], &s, &e);
+    const int64_t len = e - s;
+    uint32_t *src = tok + s, *dst = tmp + s;
+    for (int64_t c0 = 0; c0 < len; c0 += kMidRow) {
+        const int n = (int)std::min<int64_t>(kMidRow, len - c0);
+        for (int i = threadIdx.x; i < kMidRow; i += blockDim.x) a[i] = i < n ? (src[c0 + i] & kVal) : 0xffffffffu;
+        __syncthreads();
+        bitonic(a, kMidRow);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) src[c0 + i] = a[i];
+        __syncthreads();
+    }
+    for (int64_t w = kMidRow; w < len; w <<= 1) {
+        for (int64_t a0 = 0; a0 < len; a0 += 2 * w) {
+            const int64_t na = std::min<int64_t>(w, len - a0), nb = std::min<int64_t>(w, len - a0 - na);
+            const uint32_t *X = src + a0, *Y = src + a0 + na;
+            uint32_t *O = dst + a0;
+            const int64_t n = na + nb, per = (n + blockDim.x - 1) / blockDim.x;
+            const int64_t d0 = std::min<int64_t>(n, threadIdx.x * per), d1 = std::min<int64_t>(n, d0 + per);
+            if (d0 >= d1) continue;
+            int64_t lo = std::max<int64_t>(0, d0 - nb), hi = std::min<int64_t>(d0, na);
+            while (lo < hi) {  // elements of X among the first d0 outputs (ties: X first)
+                const int64_t mid = (lo + hi) >> 1;
+                if (X[mid] <= Y[d0 - 1 - mid]) lo = mid + 1;
+                else hi = mid;
+            }
+            int64_t i = lo, j = d0 - lo;
+            for (int64_t d = d0; d < d1; ++d) {
+                if (j >= nb || (i < na && X[i] <= Y[j])) O[d] = X[i++];
+                else O[d] = Y[j++];
+            }
+        }
+        __syncthreads();
+        uint32_t *t = src;
+        src = dst;
+        dst = t;
+    }
+    uint32_t *row = tok + s;
+    for (int64_t i = threadIdx.x; i < len; i += blockDim.x) row[i] = src[i] | (i == 0 ? kFirst : 0u);
+}
+
+// ---- de-duplication: keep the first token of each line and every token unlike its predecessor ----
+
+__device__ __forceinline__ bool kept(const uint32_t *tok, int64_t t) {
+    const uint32_t x = tok[t];
+    return (x & kFirst) || (x & kVal) != (tok[t - 1] & kVal);
+}
+
+__global__ void __launch_bounds__(kTxtThreads) k_keep_count(const uint32_t *__restrict__ tok, int64_t ntok,
+                                                            uint32_t *__restrict__ tcnt) {
+    __shared__ uint32_t s_w[kNW];
+    uint32_t n = 0;
+    for (int i = threadIdx.x; i < kTokTile; i += kTxtThreads) {
+        const int64_t t = blockIdx.x * kTokTile + i;
+        if (t < ntok) n += kept(tok, t);
+    }
+    const uint32_t tot = block_sum(n, s_w);
+    if (threadIdx.x == 0) tcnt[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kTxtThreads) k_keep_pos(const uint32_t *__restrict__ tok, int64_t ntok,
+                                                          const int64_t *__restrict__ toff, int64_t *__restrict__ keptpos) {
+    __shared__ uint32_t s_w[kNW];
+    int64_t base = toff[blockIdx.x];
+    for (int i0 = 0; i0 < kTokTile; i0 += kTxtThreads) {
+        const int64_t t = blockIdx.x * kTokTile + i0 + threadIdx.x;
+        const uint32_t k = t < ntok ? kept(tok, t) : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan(k, &tot, s_w);
+        if (t < ntok) keptpos[t] = base + ex;
+        base += tot;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) keptpos[ntok] = base;
+}
+
+// ---- per line: raw degree, CSR degree, classes ----
+
+struct LineInfo {
+    int64_t e_arc;  // arcs up to the end of the row (CSR offset of the next row)
+    int64_t raw, deg;
+    int cls;        // 0..2, or 3 for degree 0
+};
+
+__device__ __forceinline__ LineInfo line_info(const int64_t *__restrict__ end_tok, const int64_t *__restrict__ keptpos,
+                                              int64_t l) {
+    const int64_t s = l ? end_tok[l - 1] : 0, e = end_tok[l];
+    LineInfo r;
+    r.raw = e - s;
+    if (keptpos) {
+        r.e_arc = keptpos[e];
+        r.deg = r.e_arc - keptpos[s];
+    } else {
+        r.e_arc = e;
+        r.deg = r.raw;
+    }
+    r.cls = r.deg == 0 ? 3 : (r.deg <= kSmallDeg ? 0 : (r.deg <= kLargeDeg ? 1 : 2));
+    return r;
+}
+
+__global__ void __launch_bounds__(kTxtThreads) k_lines_count(const int64_t *__restrict__ end_tok,
+                                                             const int64_t *__restrict__ keptpos, int64_t nv,
+                                                             uint32_t *__restrict__ lcnt, Scal *sc) {
+    __shared__ uint32_t s_w[kNW];
+    uint32_t cnt3 = 0;  // 10-bit fields
+    unsigned long long md = 0, mr = 0;
+    for (int s = 0; s < kLineSteps; ++s) {
+        const int64_t l = blockIdx.x * kLineTile + s * kTxtThreads + threadIdx.x;
+        if (l >= nv) break;
+        const LineInfo r = line_info(end_tok, keptpos, l);
+        if (r.cls < 3) cnt3 += 1u << (10 * r.cls);
+        md = max(md, (unsigned long long)r.deg);
+        mr = max(mr, (unsigned long long)r.raw);
+    }
+    // per-class totals of a tile reach 4096: sum the three fields separately
+    const uint32_t c0 = block_sum(cnt3 & 1023u, s_w), c1 = block_sum((cnt3 >> 10) & 1023u, s_w),
+                   c2 = block_sum(cnt3 >> 20, s_w);
+    for (int o = 16; o > 0; o >>= 1) {
+        md = max(md, __shfl_xor_sync(DMOLP_FULL_MASK, md, o));
+        mr = max(mr, __shfl_xor_sync(DMOLP_FULL_MASK, mr, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (md) atomicMax(&sc->maxdeg, md);
+        if (mr) atomicMax(&sc->maxraw, mr);
+    }
+    if (threadIdx.x == 0) {
+        lcnt[3 * blockIdx.x] = c0;
+        lcnt[3 * blockIdx.x + 1] = c1;
+        lcnt[3 * blockIdx.x + 2] = c2;
+    }
+}
+
+__global__ void __launch_bounds__(kTxtThreads) k_lines_emit(const int64_t *__restrict__ end_tok,
+                                                            const int64_t *__restrict__ keptpos, int64_t nv,
+                                                            const int64_t *__restrict__ loff, int64_t *__restrict__ off,
+                                                            int32_t *__restrict__ raw, int32_t *b0, int32_t *b1,
+                                                            int32_t *b2) {
+    __shared__ uint32_t s_w[kNW];
+    int64_t base[3] = {loff[3 * blockIdx.x], loff[3 * blockIdx.x + 1], loff[3 * blockIdx.x + 2]};
+    if (blockIdx.x == 0 && threadIdx.x == 0) off[0] = 0;
+    for (int s = 0; s < kLineSteps; ++s) {
+        const int64_t l = blockIdx.x * kLineTile + s * kTxtThreads + threadIdx.x;
+        if (blockIdx.x * kLineTile + s * kTxtThreads >= nv) break;  // uniform across the block
+        LineInfo r;
+        r.cls = 3;
+        if (l < nv) {
+            r = line_info(end_tok, keptpos, l);
+            off[l + 1] = r.e_arc;
+            raw[l] = (int32_t)r.raw;
+        }
+        // per-step class counts are at most 256: three 10-bit fields
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan(r.cls < 3 ? 1u << (10 * r.cls) : 0u, &tot, s_w);
+        if (r.cls < 3) {
+            int32_t *b = r.cls == 0 ? b0 : (r.cls == 1 ? b1 : b2);
+            b[base[r.cls] + ((ex >> (10 * r.cls)) & 1023u)] = (int32_t)l;
+        }
+        for (int c = 0; c < 3; ++c) base[c] += (tot >> (10 * c)) & 1023u;
+    }
+}
+
+// ---- columns ----
+
+__global__ void k_col_copy(const uint32_t *__restrict__ tok, int64_t ntok, int32_t *__restrict__ col) {
+    const int64_t n4 = ntok / 4;
+    const uint4 *src = reinterpret_cast<const uint4 *>(tok);
+    int4 *dst = reinterpret_cast<int4 *>(col);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint4 q = __ldcs(src + i);
+        __stcs(dst + i, make_int4((int)(q.x & kVal), (int)(q.y & kVal), (int)(q.z & kVal), (int)(q.w & kVal)));
+    }
+    for (int64_t t = n4 * 4 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntok; t += (int64_t)gridDim.x * blockDim.x)
+        col[t] = (int)(tok[t] & kVal);
+}
+
+__global__ void k_keep_compact(const uint32_t *__restrict__ tok, int64_t ntok, const int64_t *__restrict__ keptpos,
+                               int32_t *__restrict__ col) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ntok; t += (int64_t)gridDim.x * blockDim.x)
+        if (kept(tok, t)) col[keptpos[t]] = (int)(tok[t] & kVal);
+}
+
+// ---- host side ----
+
+template <typename T>
+bool dev_alloc(T **p, size_t n, std::string &err) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return false;
+    }
+    *p = (T *)q;
+    return true;
+}
+
+#define ING_CUDA(call)                                                              \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) {                                                    \
+            err = std::string(#call) + ": " + cudaGetErrorString(e_);               \
+            return 1;                                                               \
+        }                                                                           \
+    } while (0)
+#define ING_ALLOC(ptr, n) \
+    if (!dev_alloc(&(ptr), (n), err)) return 1
+
+int grid_for(int64_t n, int threads) {
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, (int64_t)sms * 16));
+}
+
+}  // namespace
+
+void release(Parsed &p) {
+    for (void *q : {(void *)p.tok, (void *)p.tmp, (void *)p.end_tok, (void *)p.keptpos, (void *)p.tcnt,
+                    (void *)p.toff, (void *)p.loff, (void *)p.badrow, (void *)p.lists, p.scal})
+        if (q) cudaFree(q);
+    p = Parsed();
+}
+
+int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t body1, Parsed &p, std::string &err) {
+    release(p);
+    (void)len;
+    Scal *sc = nullptr;
+    ING_ALLOC(sc, 1);
+    p.scal = sc;
+    ING_CUDA(cudaMemsetAsync(sc, 0, sizeof(Scal), st));
+    const int64_t nt = body1 > body0 ? (body1 + kTileBytes - 1) / kTileBytes : 0;
+    int64_t tot[2] = {0, 0};
+    if (nt > 0) {
+        ING_ALLOC(p.tcnt, (size_t)2 * nt);
+        ING_ALLOC(p.toff, (size_t)2 * (nt + 1));
+        k_txt_count<<<(unsigned)nt, kTxtThreads, 0, st>>>(d_txt, body0, body1, p.tcnt, sc);
+        ++p.launches;
+        unsigned long long nul = 0;
+        ING_CUDA(cudaMemcpyAsync(&nul, &sc->nul, sizeof(nul), cudaMemcpyDeviceToHost, st));
+        ING_CUDA(cudaStreamSynchronize(st));
+        if (nul) {
+            k_txt_nulfill<<<grid_for((body1 - body0) / 16 + 1, 256), 256, 0, st>>>(d_txt, body0, body1);
+            k_txt_count<<<(unsigned)nt, kTxtThreads, 0, st>>>(d_txt, body0, body1, p.tcnt, sc);
+            p.launches += 2;
+        }
+        k_scan<2><<<1, 1024, 0, st>>>(p.tcnt, nt, p.toff);
+        ++p.launches;
+        ING_CUDA(cudaMemcpyAsync(tot, p.toff + 2 * nt, sizeof(tot), cudaMemcpyDeviceToHost, st));
+        ING_CUDA(cudaStreamSynchronize(st));
+        ING_CUDA(cudaGetLastError());
+    }
+    p.nv = tot[0];
+    p.ntok = tot[1];
+    if (p.nv > 0x7ffffffe) {
+        err = "too many vertices for int32 ids";
+        return 1;
+    }
+    ING_ALLOC(p.tok, (size_t)p.ntok);
+    ING_ALLOC(p.end_tok, (size_t)p.nv);
+    ING_ALLOC(p.badrow, (size_t)p.nv);
+    Scal h{};
+    if (p.nv > 0) {
+        k_txt_emit<<<(unsigned)nt, kTxtThreads, 0, st>>>(d_txt, body0, body1, p.nv, p.toff, p.tok, p.end_tok, sc);
+        ING_CUDA(cudaMemsetAsync(p.badrow, 0, (size_t)p.nv, st));
+        ++p.launches;
+        if (p.ntok > 1) {
+            k_tok_check<<<grid_for(p.ntok, 256), 256, 0, st>>>(p.tok, p.ntok, p.end_tok, p.nv, p.badrow, sc);
+            ++p.launches;
+        }
+        ING_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, st));
+        ING_CUDA(cudaStreamSynchronize(st));
+        ING_CUDA(cudaGetLastError());
+    }
+    if (h.bad_id) {
+        err = "a neighbour id is outside [0, V)";
+        return 1;
+    }
+    p.sorted = h.violations == 0;
+    p.narcs = p.ntok;
+    if (!p.sorted) {
+        ING_ALLOC(p.lists, (size_t)3 * p.nv);
+        k_rows_classify<<<grid_for(p.nv, 256), 256, 0, st>>>(p.end_tok, p.nv, p.badrow, p.lists, sc);
+        ++p.launches;
+        ING_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, st));
+        ING_CUDA(cudaStreamSynchronize(st));
+        p.rows_sorted = (int64_t)h.nlist[0] + h.nlist[1] + h.nlist[2];
+        if (h.nlist[0]) {
+            k_sort_small<<<(h.nlist[0] + 127) / 128, 128, 0, st>>>(p.tok, p.end_tok, p.lists, h.nlist[0]);
+            ++p.launches;
+        }
+        if (h.nlist[1]) {
+            k_sort_mid<<<h.nlist[1], 512, 0, st>>>(p.tok, p.end_tok, p.lists + p.nv);
+            ++p.launches;
+        }
+        if (h.nlist[2]) {
+            ING_ALLOC(p.tmp, (size_t)p.ntok);
+            k_sort_big<<<h.nlist[2], 1024, 0, st>>>(p.tok, p.tmp, p.end_tok, p.lists + 2 * p.nv);
+            ++p.launches;
+        }
+        const int64_t ntt = (p.ntok + kTokTile - 1) / kTokTile;
+        uint32_t *kc = nullptr;
+        int64_t *ko = nullptr;
+        ING_ALLOC(kc, (size_t)ntt);
+        cudaFree(p.tcnt);
+        p.tcnt = kc;
+        ING_ALLOC(ko, (size_t)ntt + 1);
+        cudaFree(p.toff);
+        p.toff = ko;
+        ING_ALLOC(p.keptpos, (size_t)p.ntok + 1);
+        k_keep_count<<<(unsigned)ntt, kTxtThreads, 0, st>>>(p.tok, p.ntok, p.tcnt);
+        k_scan<1><<<1, 1024, 0, st>>>(p.tcnt, ntt, p.toff);
+        k_keep_pos<<<(unsigned)ntt, kTxtThreads, 0, st>>>(p.tok, p.ntok, p.toff, p.keptpos);
+        p.launches += 3;
+        ING_CUDA(cudaMemcpyAsync(&p.narcs, p.keptpos + p.ntok, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    }
+    const int64_t nlt = (p.nv + kLineTile - 1) / kLineTile;
+    uint32_t *lcnt = nullptr;
+    ING_ALLOC(lcnt, (size_t)3 * nlt);
+    ING_ALLOC(p.loff, (size_t)3 * (nlt + 1));
+    int64_t nb[3] = {0, 0, 0};
+    if (nlt > 0) {
+        k_lines_count<<<(unsigned)nlt, kTxtThreads, 0, st>>>(p.end_tok, p.keptpos, p.nv, lcnt, sc);
+        k_scan<3><<<1, 1024, 0, st>>>(lcnt, nlt, p.loff);
+        p.launches += 2;
+        ING_CUDA(cudaMemcpyAsync(nb, p.loff + 3 * nlt, sizeof(nb), cudaMemcpyDeviceToHost, st));
+        ING_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, st));
+    }
+    const cudaError_t e = cudaStreamSynchronize(st);
+    cudaFree(lcnt);
+    if (e != cudaSuccess) {
+        err = std::string("ingest: ") + cudaGetErrorString(e);
+        return 1;
+    }
+    ING_CUDA(cudaGetLastError());
+    for (int c = 0; c < 3; ++c) p.nb[c] = nb[c];
+    p.maxdeg = (int64_t)h.maxdeg;
+    p.maxraw = (int64_t)h.maxraw;
+    if (p.maxraw > 0x7fffffff) {
+        err = "a line has more than 2^31-1 tokens";
+        return 1;
+    }
+    return 0;
+}
+
+int build(cudaStream_t st, Parsed &p, int64_t *off, int32_t *col, int32_t *raw, int32_t *const bucket[3],
+          std::string &err) {
+    const int64_t nlt = (p.nv + kLineTile - 1) / kLineTile;
+    if (nlt > 0) {
+        k_lines_emit<<<(unsigned)nlt, kTxtThreads, 0, st>>>(p.end_tok, p.keptpos, p.nv, p.loff, off, raw, bucket[0],
+                                                            bucket[1], bucket[2]);
+        ++p.launches;
+    } else {
+        ING_CUDA(cudaMemsetAsync(off, 0, sizeof(int64_t), st));
+    }
+    if (p.ntok > 0) {
+        if (p.sorted) k_col_copy<<<grid_for(p.ntok / 4 + 1, 256), 256, 0, st>>>(p.tok, p.ntok, col);
+        else k_keep_compact<<<grid_for(p.ntok, 256), 256, 0, st>>>(p.tok, p.ntok, p.keptpos, col);
+        ++p.launches;
+    }
+    ING_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace ingest
+}  // namespace dmolp

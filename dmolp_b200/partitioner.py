@@ -97,6 +97,7 @@ class Partitioner:
         self._check(self.lib.dmolp_create(device, byref(self.ctx)))
         self.graph: Graph | None = None
         self.num_vertices = 0
+        self.raw_total: int | None = None  # sum of raw degrees of a device-parsed graph
 
     def _check(self, rc: int) -> None:
         if rc != cabi.DMOLP_OK:
@@ -128,6 +129,31 @@ class Partitioner:
                                                 None if raw is None else _p(raw)))
         self.graph = g
         self.num_vertices = g.num_vertices
+        self.raw_total = None
+
+    def upload_adjtext(self, source) -> dict:
+        """Parse the reference's adjacency text on the device into the resident graph.  `source` is a file
+        path (read through the pinned staging ring) or the text itself (bytes).  Returns sizes and times."""
+        info = cabi.IngestInfo()
+        if isinstance(source, (bytes, bytearray, memoryview)):
+            data = bytes(source)
+            self._check(self.lib.dmolp_graph_upload_adjtext(self.ctx, data, len(data), byref(info)))
+        else:
+            self._check(self.lib.dmolp_graph_load_adjtext(self.ctx, os.fsencode(source), byref(info)))
+        self.graph = None
+        self.num_vertices = int(info.num_vertices)
+        self.raw_total = int(info.num_tokens)
+        return {f: getattr(info, f) for f, _ in cabi.IngestInfo._fields_}
+
+    def graph_arrays(self) -> Graph:
+        """The resident graph copied back to the host (offsets, indices, raw degree)."""
+        nv, na = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.dmolp_graph_size(self.ctx, byref(nv), byref(na)))
+        off = np.empty(nv.value + 1, np.int64)
+        col = np.empty(na.value, np.int32)
+        raw = np.empty(nv.value, np.int32)
+        self._check(self.lib.dmolp_graph_get(self.ctx, _p(off), _p(col), _p(raw)))
+        return Graph(off, col, raw)
 
     def labels(self) -> np.ndarray:
         out = np.empty(self.num_vertices, np.int32)
@@ -154,7 +180,8 @@ class Partitioner:
         return Phase1Metrics(
             initial_edge_cut=info.initial_edge_cut, initial_vertex_balance=info.initial_vertex_balance,
             initial_edge_balance=info.initial_edge_balance, total_vertices=self.num_vertices,
-            total_edges=int(g.raw_deg().astype(np.int64).sum() // 2) if g is not None else 0,
+            total_edges=(int(g.raw_deg().astype(np.int64).sum() // 2) if g is not None
+                         else (self.raw_total or 0) // 2),
             partition_vertex_counts=vc.tolist(), partition_edge_counts=ec.tolist(), seeds=seeds.tolist(),
             num_seeds_found=info.num_seeds_found, rounds=info.rounds, num_hubs=info.num_hubs,
             traversed_edges=info.traversed_edges, gpu_ms=info.gpu_ms)

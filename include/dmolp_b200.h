@@ -102,6 +102,36 @@ int dmolp_destroy(dmolp_ctx *ctx);
 int dmolp_graph_upload(dmolp_ctx *ctx, int64_t nv, int64_t narcs, const int64_t *offsets, const int32_t *indices,
                        const int32_t *raw_degree);
 
+/* The reference's adjacency text parsed ON THE DEVICE into the resident graph: first line = header
+ * (ignored, as the reference's vertex count comes from the lines), line v+1 = neighbour ids of vertex v.
+ * Same result as dmolp_adjtext_load + dmolp_graph_upload: fast_atoi tokenisation (a token starts at the
+ * first byte of a non-empty line and at every digit after a non-digit; its value is its digit run, empty =
+ * 0), a NUL ends its line's parse, an unterminated last line is dropped, raw degree = tokens on the line,
+ * CSR row = sorted, de-duplicated tokens with self-loops kept; an id >= V is an error (DMOLP_ERR_ARG, and
+ * the previous graph stays).  Replaces load_graph (src/phase1/init.cpp:25-100) and the CSR construction of
+ * build_local_graph_and_ghosts (src/phase1/partition.cpp:227-262).
+ * dmolp_graph_upload_adjtext takes the text in host memory (len bytes); dmolp_graph_load_adjtext reads a
+ * file through a pinned staging ring, copying each piece to the device while the next is read.
+ * info (may be NULL) receives sizes and times. */
+typedef struct {
+    int64_t num_vertices;
+    int64_t num_arcs;               /* after de-duplication */
+    int64_t num_tokens;             /* sum of raw degrees */
+    int64_t rows_sorted_on_device;  /* rows that were not strictly increasing in the text */
+    double read_ms;                 /* file read + host-to-device copy (wall clock), or the copy alone */
+    double parse_ms;                /* parse + CSR build on the device (CUDA events, first to last kernel) */
+    double total_ms;                /* the whole call (wall clock), state set-up included */
+    int64_t kernels;                /* kernels launched by the parse */
+} dmolp_ingest_info;
+int dmolp_graph_upload_adjtext(dmolp_ctx *ctx, const char *text, int64_t len, dmolp_ingest_info *info);
+int dmolp_graph_load_adjtext(dmolp_ctx *ctx, const char *path, dmolp_ingest_info *info);
+
+/* Sizes of the resident graph, and a copy of it to host arrays offsets[nv+1], indices[narcs],
+ * raw_degree[nv] (any may be NULL).  The reference's run_phase1 hands its Graph back to the caller
+ * (src/phase1/phase1.cpp:22-160); this is how a device-parsed graph gets there. */
+int dmolp_graph_size(dmolp_ctx *ctx, int64_t *nv, int64_t *narcs);
+int dmolp_graph_get(dmolp_ctx *ctx, int64_t *offsets, int32_t *indices, int32_t *raw_degree);
+
 /* Phase 1: hubs, first seed, seeds, theta-limited multi-source BFS growth, initial metrics.  Leaves the
  * labels on the device.  seeds_out[k], vertex_counts[k], edge_counts[k] may be NULL.
  * Replaces find_hub_nodes / find_first_seed (src/phase1/init.cpp:139-187), find_seeds
