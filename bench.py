@@ -47,6 +47,9 @@ WORKLOADS = {
     "batch2048": dict(kind="batch", n=2048, seed=11, vmin=1000, vmax=200_000, theta=1000),
     # the same mix, 256 graphs (profiling and quick checks)
     "batch256": dict(kind="batch", n=256, seed=11, vmin=1000, vmax=200_000, theta=1000),
+    # the rmat22 graph as the reference's adjacency text, parsed into the resident CSR
+    "ingest-rmat22": dict(kind="ingest", graph=dict(kind="rmat", scale=22, edge_factor=16, a=0.57, b=0.19, c=0.19,
+                                                    seed=7)),
 }
 
 
@@ -83,6 +86,8 @@ def describe(w: dict) -> str:
 def make_graph(w: dict):
     from dmolp_b200 import graphs
 
+    if w["kind"] == "ingest":
+        return make_graph(w["graph"])
     if w["kind"] == "rmat":
         return graphs.rmat(w["scale"], w["edge_factor"], w["a"], w["b"], w["c"], seed=w["seed"])
     return graphs.knn(w["n"], w["dim"], w["knn"], w["seed"])
@@ -303,6 +308,156 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
                      "kernels": prof},
         "clocks": clocks,
     }
+    return line
+
+
+# ------------------------------------------------------------------------------------------- ingestion
+def reference_load(path: str, timeout: float = 600) -> dict:
+    """The reference's own load_graph (oracle/_ref, built from its sources) on the file: seconds."""
+    import oracle
+
+    with tempfile.TemporaryDirectory() as td:
+        pr = subprocess.run([oracle.REF_HARNESS, path, "1", "1", "--out", td, "--load-only", "--threads", "1"],
+                            capture_output=True, text=True, timeout=timeout)
+        if pr.returncode != 0:
+            raise RuntimeError(pr.stderr[-500:])
+        return json.loads(pr.stdout.strip().splitlines()[-1])
+
+
+def ingest_text_file(g, td: str) -> str:
+    from dmolp_b200 import graphs
+
+    path = os.path.join(td, "graph.txt")
+    graphs.write_adjtext(g, path)
+    return path
+
+
+def run_ingest(args, w, rank: int, world: int, local_rank: int, dist) -> dict | None:
+    """Adjacency text -> resident CSR: the reference's load_graph + CSR build (src/phase1/init.cpp:25-100,
+    src/phase1/partition.cpp:227-262) as the device parse.  A step parses the whole text once: `value` with the
+    text already in HBM (dmolp_graph_upload_adjtext_device), `e2e` from the file (page cache) through
+    dmolp_graph_load_adjtext, file read and host-to-device copy included."""
+    import torch
+
+    from dmolp_b200.partitioner import Partitioner, load_adjtext
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    g = make_graph(w)
+    td = tempfile.mkdtemp(prefix="dmolp_ingest_")
+    try:
+        path = ingest_text_file(g, td)
+        host = np.fromfile(path, np.uint8)
+        nbytes = int(host.size)
+        text = torch.from_numpy(host).to(dev)
+        p = Partitioner(local_rank)
+        stream = torch.cuda.ExternalStream(p.lib.dmolp_stream(p.ctx), device=dev)
+        p.upload_adjtext(text)
+        h = p.graph_arrays()  # parity at full size: the generator's CSR, raw degree = CSR degree
+        parity = bool(np.array_equal(h.offsets, g.offsets) and np.array_equal(h.indices, g.indices)
+                      and np.array_equal(h.raw_degree, g.degree()))
+        del h
+        sampler = ClockSampler(local_rank)
+        if not args.quick:
+            sampler.start()
+        for _ in range(max(1, args.warmup)):
+            p.upload_adjtext(text)
+        launches0 = p.kernel_launches()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        infos = [p.upload_adjtext(text) for _ in range(args.steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        elapsed = e0.elapsed_time(e1) / 1e3
+        launches = p.kernel_launches() - launches0
+        clocks = sampler.stop() if not args.quick else None
+        # end to end from the file: read through the pinned ring, copy, parse, resident state
+        e2e_n = 0 if args.quick else max(1, min(args.steps, 5))
+        t0 = time.perf_counter()
+        e2e_infos = [p.upload_adjtext(path) for _ in range(e2e_n)]
+        e2e_s = time.perf_counter() - t0
+        t_max, e2e_max = max_over_ranks(dist, [elapsed, e2e_s])
+        host_loader = None
+        ref = None
+        if rank == 0 and world == 1 and not args.quick and not args.no_cpu_baseline:
+            t0 = time.perf_counter()
+            hg = load_adjtext(path)
+            host_loader = {"seconds": time.perf_counter() - t0, "cores": os.cpu_count() or 1,
+                           "identical_csr": bool(np.array_equal(hg.offsets, g.offsets)
+                                                 and np.array_equal(hg.indices, g.indices)),
+                           "kind": "this package's host loader (OpenMP, adjtext.cpp)"}
+            del hg
+            import oracle
+
+            if oracle.reference_available():
+                try:
+                    ref = reference_load(path)
+                except Exception as e:  # report, do not hide
+                    ref = {"error": str(e)[:300]}
+        p.close()
+    finally:
+        for f in os.listdir(td):
+            os.remove(os.path.join(td, f))
+        os.rmdir(td)
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peaks()
+    i0 = infos[0]
+    ntok, nv = int(i0["num_tokens"]), int(i0["num_vertices"])
+    count_ms = statistics.mean(i["count_ms"] for i in infos)
+    emit_ms = statistics.mean(i["emit_ms"] for i in infos)
+    body = nbytes  # header and trailing newline are a few bytes
+    kern = {"k_txt_count": {"ms": count_ms, "bytes": body}, "k_txt_emit": {"ms": emit_ms, "bytes": body + 4 * ntok + 8 * nv}}
+    dom = max(kern, key=lambda k: kern[k]["ms"])
+    achieved = kern[dom]["bytes"] / (kern[dom]["ms"] / 1e3) / 1e9
+    line = {
+        "metric": "adjacency text parsed into the resident CSR, bytes/s",
+        "value": nbytes * args.steps * world / t_max / 1e9,
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic (seeded generator, written as the reference's adjacency text)",
+        "config": {"workload": "R-MAT scale 22, edge factor 16, seed 7, as adjacency text (%.2f GB)" % (nbytes / 1e9),
+                   "text_bytes": nbytes, "num_vertices": nv, "num_tokens": ntok, "num_arcs": int(i0["num_arcs"]),
+                   "arcs_per_s": int(i0["num_arcs"]) * args.steps * world / t_max,
+                   "parity_full_size": parity, "parse_ms_per_step": statistics.mean(i["parse_ms"] for i in infos),
+                   "l2": "inputs larger than L2 (text %.0f MB)" % (nbytes / 1e6), "parallelism": f"replicas x{world}"},
+        "e2e": ({"value": nbytes * e2e_n * world / e2e_max / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
+                 "d2h_bytes_per_step": 4 * nv, "steps": e2e_n,
+                 "read_ms_per_step": statistics.mean(i["read_ms"] for i in e2e_infos),
+                 "parse_ms_per_step": statistics.mean(i["parse_ms"] for i in e2e_infos),
+                 "seconds_per_step": e2e_max / e2e_n,
+                 "path": "dmolp_graph_load_adjtext: file (page cache) -> pinned ring -> HBM -> parse -> resident graph"}
+                if e2e_n else None),
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_source": peak_kind,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic_from_profiles(dom, args.workload),
+                     "algorithmic_bytes_per_launch": kern[dom]["bytes"], "avg_launch_ms": kern[dom]["ms"],
+                     "kernels": kern},
+        "clocks": clocks,
+    }
+    if ref is not None:
+        if "load_seconds" in ref:
+            line["cpu_baseline"] = {"value": nbytes / ref["load_seconds"] / 1e9, "unit": "GB/s", "cores": 1,
+                                    "kind": "reference", "seconds": ref["load_seconds"],
+                                    "sample": "the whole text through the reference's load_graph (file -> adjacency "
+                                              "map; its CSR build inside phase 1 not included)"}
+        else:
+            line["cpu_baseline"] = ref
+    if host_loader is not None:
+        host_loader["value"] = nbytes / host_loader["seconds"] / 1e9
+        host_loader["unit"] = "GB/s"
+        line["host_loader"] = host_loader
     return line
 
 
@@ -588,10 +743,57 @@ def cpu_baseline(g, labels1, w, args) -> dict:
             "sample": sample, "seconds": r["lp_seconds"]}
 
 
+def run_reference_ingest(args, w) -> dict:
+    """--impl reference for the ingestion workload: the reference's load_graph on the same text, one whole
+    load per step, single-threaded as the reference reads."""
+    import oracle
+
+    g = make_graph(w)
+    td = tempfile.mkdtemp(prefix="dmolp_ingest_ref_")
+    try:
+        path = ingest_text_file(g, td)
+        nbytes = os.path.getsize(path)
+        if oracle.reference_available():
+            runs = [reference_load(path)["load_seconds"] for _ in range(args.warmup + args.steps)]
+            kind = "reference"
+        else:
+            from dmolp_b200.partitioner import load_adjtext
+
+            runs = []
+            for _ in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                load_adjtext(path)
+                runs.append(time.perf_counter() - t0)
+            kind = "port"
+    finally:
+        for f in os.listdir(td):
+            os.remove(os.path.join(td, f))
+        os.rmdir(td)
+    secs = sum(runs[args.warmup:]) or sum(runs)
+    n = len(runs[args.warmup:]) or len(runs)
+    value = nbytes * n / secs / 1e9
+    return {
+        "impl": "reference", "metric": "adjacency text parsed into the resident CSR, bytes/s", "value": value,
+        "unit": "GB/s", "n_gpus": args.gpus, "steps": n, "warmup": args.warmup, "ms_per_step": secs / n * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator, written as the reference's adjacency text)",
+        "config": {"workload": "R-MAT scale 22, edge factor 16, seed 7, as adjacency text (%.2f GB)" % (nbytes / 1e9),
+                   "text_bytes": nbytes},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": 1, "kind": kind,
+                         "sample": "per step: the whole text through load_graph (file -> adjacency map)"},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def run_reference_arm(args, w) -> dict:
     """--impl reference: the reference's own implementation of the path on this box's host cores."""
     import oracle
 
+    if w["kind"] == "ingest":
+        return run_reference_ingest(args, w)
+    if w["kind"] == "batch":
+        return {"impl": "reference", "unavailable": "the reference has no batched path; its per-graph CPU phase 2 "
+                                                    "is the rmat22/knn-c0 reference arm"}
     g = make_graph(w)
     # phase-1 labels from the oracle (the reference's phase 1 is undefined on R-MAT: fewer seeds than parts)
     labels1 = oracle.phase1(g.offsets, g.indices, g.raw_deg(), w["k"], w["theta"]).labels
@@ -653,12 +855,13 @@ def main():
         torch.cuda.set_device(local_rank)
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
-    line = (run_batch if w["kind"] == "batch" else run_ours)(args, w, rank, world, local_rank, dist)
+    runner = {"batch": run_batch, "ingest": run_ingest}.get(w["kind"], run_ours)
+    line = runner(args, w, rank, world, local_rank, dist)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0 and line is not None:
-        if world == 1 and not args.no_cpu_baseline and not args.quick and w["kind"] != "batch":
+        if world == 1 and not args.no_cpu_baseline and not args.quick and w["kind"] not in ("batch", "ingest"):
             g = make_graph(w)
             import oracle
 
@@ -667,7 +870,7 @@ def main():
                 line["cpu_baseline"] = cpu_baseline(g, labels1, w, args)
             except Exception as e:  # report, do not hide
                 line["cpu_baseline"] = {"error": str(e)[:300]}
-        if world == 1 and not args.quick and w["kind"] != "batch":
+        if world == 1 and not args.quick and w["kind"] not in ("batch", "ingest"):
             try:
                 line["batched"] = batched_summary(256, 1000, local_rank)
             except Exception as e:  # report, do not hide

@@ -34,6 +34,7 @@ EXPORTS = [
     "dmolp_mpnn_prepare_training", "dmolp_mpnn_backward", "dmolp_mpnn_train_step", "dmolp_mpnn_decode",
     "dmolp_batch_propose", "dmolp_mpnn_gate", "dmolp_mpnn_train_gate", "dmolp_batch_phase1",
     "dmolp_graph_upload_adjtext", "dmolp_graph_load_adjtext", "dmolp_graph_size", "dmolp_graph_get",
+    "dmolp_graph_upload_adjtext_device",
 ]
 BATCH_MAX_K = 64
 
@@ -74,7 +75,7 @@ class BatchResult(ctypes.Structure):
 class IngestInfo(ctypes.Structure):
     _fields_ = [("num_vertices", c_int64), ("num_arcs", c_int64), ("num_tokens", c_int64),
                 ("rows_sorted_on_device", c_int64), ("read_ms", c_double), ("parse_ms", c_double),
-                ("total_ms", c_double), ("kernels", c_int64)]
+                ("total_ms", c_double), ("kernels", c_int64), ("count_ms", c_double), ("emit_ms", c_double)]
 
 
 class BatchP1Result(ctypes.Structure):
@@ -91,6 +92,7 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_graph_upload.argtypes = [vp, c_int64, c_int64, vp, vp, vp]
     lib.dmolp_graph_upload_adjtext.argtypes = [vp, c_char_p, c_int64, POINTER(IngestInfo)]
     lib.dmolp_graph_load_adjtext.argtypes = [vp, c_char_p, POINTER(IngestInfo)]
+    lib.dmolp_graph_upload_adjtext_device.argtypes = [vp, vp, c_int64, POINTER(IngestInfo)]
     lib.dmolp_graph_size.argtypes = [vp, POINTER(c_int64), POINTER(c_int64)]
     lib.dmolp_graph_get.argtypes = [vp, vp, vp, vp]
     lib.dmolp_phase1.argtypes = [vp, c_int, c_int, vp, vp, vp, POINTER(Phase1Info)]

@@ -394,6 +394,8 @@ int ingest_text(dmolp_ctx *c, uint8_t *d_txt, int64_t len, int64_t body0, int64_
         float ms = 0.f;
         if (!st && cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) info->parse_ms = ms;
         info->kernels = p.launches;
+        info->count_ms = p.count_ms;
+        info->emit_ms = p.emit_ms;
     }
     ingest::release(p);
     if (st) {
@@ -544,6 +546,46 @@ int dmolp_graph_upload_adjtext(dmolp_ctx *c, const char *text, int64_t len, dmol
     cudaFree(d_txt);
     if (info) {
         info->read_ms = copy_ms;
+        info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return st;
+}
+
+int dmolp_graph_upload_adjtext_device(dmolp_ctx *c, const char *d_text, int64_t len, dmolp_ingest_info *info) {
+    if (!c) return fail(DMOLP_ERR_ARG, "null context");
+    if (len < 0 || (!d_text && len > 0)) return fail(DMOLP_ERR_ARG, "bad text buffer");
+    const auto t0 = std::chrono::steady_clock::now();
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    // the header's newline and the last newline, from pieces of the two ends of the text
+    constexpr int64_t kPiece = 1 << 16;
+    std::vector<char> piece((size_t)kPiece);
+    int64_t body0 = -1, body1 = -1;
+    for (int64_t pos = 0; pos < len && body0 < 0; pos += kPiece) {
+        const int64_t n = std::min(kPiece, len - pos);
+        DMOLP_CUDA(cudaMemcpy(piece.data(), d_text + pos, (size_t)n, cudaMemcpyDeviceToHost));
+        const char *q = (const char *)memchr(piece.data(), '\n', (size_t)n);
+        if (q) body0 = pos + (q - piece.data()) + 1;
+    }
+    if (body0 < 0) return fail(DMOLP_ERR_ARG, "missing header line");
+    for (int64_t end = len; end > body0 && body1 < 0; end -= kPiece) {
+        const int64_t a = std::max(body0, end - kPiece);
+        DMOLP_CUDA(cudaMemcpy(piece.data(), d_text + a, (size_t)(end - a), cudaMemcpyDeviceToHost));
+        for (int64_t j = end - a; j > 0; --j)
+            if (piece[(size_t)j - 1] == '\n') {
+                body1 = a + j;
+                break;
+            }
+    }
+    if (body1 < 0) body1 = body0;
+    uint8_t *d_txt = nullptr;
+    int st = text_buffer(c, len, &d_txt);
+    if (st) return st;
+    DMOLP_CUDA(cudaMemcpyAsync(d_txt, d_text, (size_t)len, cudaMemcpyDeviceToDevice, c->stream));
+    const double read_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    st = ingest_text(c, d_txt, len, body0, body1, info);
+    cudaFree(d_txt);
+    if (info) {
+        info->read_ms = read_ms;
         info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     return st;

@@ -551,6 +551,14 @@ bool dev_alloc(T **p, size_t n, std::string &err) {
 #define ING_ALLOC(ptr, n) \
     if (!dev_alloc(&(ptr), (n), err)) return 1
 
+struct Events {  // timing of the two text passes, destroyed on every exit path
+    cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+    ~Events() {
+        for (cudaEvent_t x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
+
 int grid_for(int64_t n, int threads) {
     int sms = 148;
     int dev = 0;
@@ -570,6 +578,8 @@ void release(Parsed &p) {
 int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t body1, Parsed &p, std::string &err) {
     release(p);
     (void)len;
+    Events ev;
+    for (cudaEvent_t &e : ev.e) ING_CUDA(cudaEventCreate(&e));
     Scal *sc = nullptr;
     ING_ALLOC(sc, 1);
     p.scal = sc;
@@ -579,7 +589,9 @@ int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t b
     if (nt > 0) {
         ING_ALLOC(p.tcnt, (size_t)2 * nt);
         ING_ALLOC(p.toff, (size_t)2 * (nt + 1));
+        ING_CUDA(cudaEventRecord(ev.e[0], st));
         k_txt_count<<<(unsigned)nt, kTxtThreads, 0, st>>>(d_txt, body0, body1, p.tcnt, sc);
+        ING_CUDA(cudaEventRecord(ev.e[1], st));
         ++p.launches;
         unsigned long long nul = 0;
         ING_CUDA(cudaMemcpyAsync(&nul, &sc->nul, sizeof(nul), cudaMemcpyDeviceToHost, st));
@@ -606,7 +618,9 @@ int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t b
     ING_ALLOC(p.badrow, (size_t)p.nv);
     Scal h{};
     if (p.nv > 0) {
+        ING_CUDA(cudaEventRecord(ev.e[2], st));
         k_txt_emit<<<(unsigned)nt, kTxtThreads, 0, st>>>(d_txt, body0, body1, p.nv, p.toff, p.tok, p.end_tok, sc);
+        ING_CUDA(cudaEventRecord(ev.e[3], st));
         ING_CUDA(cudaMemsetAsync(p.badrow, 0, (size_t)p.nv, st));
         ++p.launches;
         if (p.ntok > 1) {
@@ -616,6 +630,8 @@ int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t b
         ING_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, st));
         ING_CUDA(cudaStreamSynchronize(st));
         ING_CUDA(cudaGetLastError());
+        cudaEventElapsedTime(&p.count_ms, ev.e[0], ev.e[1]);
+        cudaEventElapsedTime(&p.emit_ms, ev.e[2], ev.e[3]);
     }
     if (h.bad_id) {
         err = "a neighbour id is outside [0, V)";

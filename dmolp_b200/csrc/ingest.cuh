@@ -33,6 +33,7 @@ struct Parsed {
     int sorted = 1;          // every row was already strictly increasing: no device sort ran
     int64_t rows_sorted = 0; // rows the device sorted
     long long launches = 0;  // kernels launched
+    float count_ms = 0.f, emit_ms = 0.f;  // device time of the text count pass and of the token emit pass
     // device scratch
     uint32_t *tok = nullptr;      // [ntok] values; bit 31 marks the first token of a line
     uint32_t *tmp = nullptr;      // [ntok] merge buffer of the long-row sort (only when needed)

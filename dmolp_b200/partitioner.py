@@ -133,9 +133,13 @@ class Partitioner:
 
     def upload_adjtext(self, source) -> dict:
         """Parse the reference's adjacency text on the device into the resident graph.  `source` is a file
-        path (read through the pinned staging ring) or the text itself (bytes).  Returns sizes and times."""
+        path (read through the pinned staging ring), the text itself (bytes), or the text already on the
+        device (a uint8 CUDA tensor).  Returns sizes and times."""
         info = cabi.IngestInfo()
-        if isinstance(source, (bytes, bytearray, memoryview)):
+        if hasattr(source, "data_ptr"):  # a uint8 CUDA tensor on this context's device
+            self._check(self.lib.dmolp_graph_upload_adjtext_device(self.ctx, c_void_p(source.data_ptr()),
+                                                                   source.numel(), byref(info)))
+        elif isinstance(source, (bytes, bytearray, memoryview)):
             data = bytes(source)
             self._check(self.lib.dmolp_graph_upload_adjtext(self.ctx, data, len(data), byref(info)))
         else:

@@ -122,9 +122,14 @@ typedef struct {
     double parse_ms;                /* parse + CSR build on the device (CUDA events, first to last kernel) */
     double total_ms;                /* the whole call (wall clock), state set-up included */
     int64_t kernels;                /* kernels launched by the parse */
+    double count_ms;                /* device time of the text count pass (one kernel) */
+    double emit_ms;                 /* device time of the token emit pass (one kernel) */
 } dmolp_ingest_info;
 int dmolp_graph_upload_adjtext(dmolp_ctx *ctx, const char *text, int64_t len, dmolp_ingest_info *info);
 int dmolp_graph_load_adjtext(dmolp_ctx *ctx, const char *path, dmolp_ingest_info *info);
+/* The same parse of text already in device memory (d_text: len bytes on the context's device, e.g. read
+ * there by the caller's own I/O path); the text is copied into the parse buffer and left unchanged. */
+int dmolp_graph_upload_adjtext_device(dmolp_ctx *ctx, const char *d_text, int64_t len, dmolp_ingest_info *info);
 
 /* Sizes of the resident graph, and a copy of it to host arrays offsets[nv+1], indices[narcs],
  * raw_degree[nv] (any may be NULL).  The reference's run_phase1 hands its Graph back to the caller

@@ -222,14 +222,15 @@ namespace {
 struct Args {
     std::string graph, out, mode = "fixed", labels_in;
     int k = 0, theta = 0, iters = 20, threads = 1, repeat = 1;
-    bool phase1_only = false, dump_seeds = true;
+    bool phase1_only = false, dump_seeds = true, load_only = false;
 };
 
 void usage() {
     fprintf(stderr,
             "ref_harness <graph.txt> <k> <theta> --out DIR [--mode ref|fixed] [--iters N] [--gpu]\n"
             "            [--threads T] [--phase1-only] [--labels-in FILE] [--no-seed-dump] [--repeat R]\n"
-            "  --repeat R  (fixed mode) run phase 2 R times from the same start, one timing line each\n");
+            "  --repeat R  (fixed mode) run phase 2 R times from the same start, one timing line each\n"
+            "  --load-only time the reference's load_graph (src/phase1/init.cpp:25) on the file alone\n");
     exit(2);
 }
 
@@ -340,6 +341,7 @@ int main(int argc, char **argv) {
         else if (s == "--labels-in") a.labels_in = next();
         else if (s == "--no-seed-dump") a.dump_seeds = false;
         else if (s == "--repeat") a.repeat = atoi(next());
+        else if (s == "--load-only") a.load_only = true;
         else if (s.size() && s[0] == '-') usage();
         else pos.push_back(argv[i]);
     }
@@ -349,6 +351,26 @@ int main(int argc, char **argv) {
     a.theta = atoi(pos[2]);
     if (a.mode != "ref" && a.mode != "fixed") usage();
     mkdir(a.out.c_str(), 0755);
+    if (a.load_only) {
+        // The reference's text loader alone: file -> adjacency map and local degrees, as run_phase1 calls it.
+        omp_set_num_threads(a.threads > 0 ? a.threads : 1);
+        int real_out = dup(1);
+        if (!freopen((a.out + "/reference_stdout.log").c_str(), "w", stdout)) return 3;
+        std::unordered_map<int, std::vector<int>> adj;
+        std::unordered_map<int, int> ldeg;
+        int V = 0;
+        uint64_t E = 0;
+        auto t0 = std::chrono::high_resolution_clock::now();
+        load_graph(a.graph.c_str(), 0, 1, adj, ldeg, V, E);
+        const double secs = std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t0).count();
+        uint64_t tokens = 0;
+        for (auto &kv : adj) tokens += kv.second.size();
+        FILE *rs = fdopen(real_out, "w");
+        fprintf(rs, "{\"load_seconds\":%.6f,\"V\":%d,\"E\":%llu,\"lines\":%zu,\"tokens\":%llu}\n", secs, V,
+                (unsigned long long)E, adj.size(), (unsigned long long)tokens);
+        fclose(rs);
+        return 0;
+    }
     omp_set_num_threads(a.threads > 0 ? a.threads : 1);
 
     // The reference prints a lot from inside its functions; keep our own stdout for the summary.

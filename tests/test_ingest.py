@@ -34,9 +34,15 @@ def oracle_csr(text: bytes):
         return oracle.load_adjtext(p)
 
 
-def check_same(part, text, via_file=False):
+def check_same(part, text, via_file=False, via_device=False):
     off, col, raw = oracle_csr(text)
-    if via_file:
+    if via_device:
+        import torch
+
+        t = torch.frombuffer(bytearray(text), dtype=torch.uint8).cuda() if text else torch.zeros(0, dtype=torch.uint8,
+                                                                                                  device="cuda")
+        info = part.upload_adjtext(t)
+    elif via_file:
         with tempfile.TemporaryDirectory() as td:
             p = os.path.join(td, "g.txt")
             with open(p, "wb") as f:
@@ -117,6 +123,7 @@ def test_device_parse_matches_oracle(part, name):
     info = check_same(part, TEXTS[name])
     assert info["kernels"] > 0 or info["num_vertices"] == 0
     check_same(part, TEXTS[name], via_file=True)
+    check_same(part, TEXTS[name], via_device=True)
 
 
 @pytest.mark.gpu
@@ -125,6 +132,7 @@ def test_device_parse_sorts_and_dedupes_every_row_class(part):
     info = check_same(part, text)
     assert info["rows_sorted_on_device"] > 0
     check_same(part, text, via_file=True)
+    check_same(part, text, via_device=True)
 
 
 @pytest.mark.gpu
@@ -146,6 +154,7 @@ def test_device_parse_long_lines_across_tiles(part):
     assert len(text) > 33 << 20
     info = check_same(part, text, via_file=True)
     assert info["rows_sorted_on_device"] == 0
+    check_same(part, text, via_device=True)
 
 
 @pytest.mark.gpu
