@@ -75,7 +75,8 @@ class BatchResult(ctypes.Structure):
 class IngestInfo(ctypes.Structure):
     _fields_ = [("num_vertices", c_int64), ("num_arcs", c_int64), ("num_tokens", c_int64),
                 ("rows_sorted_on_device", c_int64), ("read_ms", c_double), ("parse_ms", c_double),
-                ("total_ms", c_double), ("kernels", c_int64), ("count_ms", c_double), ("emit_ms", c_double)]
+                ("total_ms", c_double), ("kernels", c_int64), ("count_ms", c_double), ("emit_ms", c_double),
+                ("setup_ms", c_double)]
 
 
 class BatchP1Result(ctypes.Structure):

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "ingest.cuh"
 
 namespace dmolp {
 
@@ -115,6 +116,7 @@ struct Buffers {
     int *p1cnt = nullptr;                // [8] phase-1 counters
     unsigned long long *p1te = nullptr;  // [1]
     int *flag = nullptr;                 // [1] scratch flag (symmetry check)
+    unsigned long long *symcnt = nullptr;  // [2] arc counts of the symmetry check
 };
 
 }  // namespace dmolp
@@ -129,8 +131,11 @@ struct dmolp_ctx {
     int nb[3] = {0, 0, 0};                // vertices per degree class
     int64_t chunk_cap = 0, hubq_cap = 0;
     bool symmetric = false;               // every arc (u,v) has its reverse: incremental statistics apply
+    bool symmetry_known = false;          // `symmetric` has been tested for the resident graph
+    bool rows_sorted = false;             // every row strictly increasing (precondition of the test)
     bool has_graph = false;
     std::vector<int32_t> h_rawdeg;        // host copy for the hub sort
+    bool h_rawdeg_valid = false;          // h_rawdeg mirrors the resident raw degrees
     dmolp::Buffers b;
     std::vector<void *> allocations;
     long long launches = 0;
@@ -158,6 +163,9 @@ struct dmolp_ctx {
     double prof_ms[5] = {0, 0, 0, 0, 0};
     long long prof_launches[5] = {0, 0, 0, 0, 0};
     double prof_bytes[5] = {0, 0, 0, 0, 0};
+    void *arena = nullptr;                 // every resident buffer of the graph (layout in graph_alloc)
+    size_t arena_cap = 0;
+    dmolp::ingest::Pool scratch;           // device scratch of the text parse, reused across loads
     // pinned staging ring of dmolp_graph_load_adjtext (allocated on first use)
     char *pin[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t pin_ev[4] = {nullptr, nullptr, nullptr, nullptr};

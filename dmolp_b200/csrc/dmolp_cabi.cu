@@ -213,26 +213,21 @@ std::vector<int> hubs_of(const std::vector<int32_t> &degree) { return find_hubs(
 
 namespace {
 
-// Frees the previous graph and allocates every resident buffer for a graph of the given sizes.
-int graph_alloc(dmolp_ctx *c, int64_t nv, int64_t narcs, int64_t maxdeg, int64_t maxraw, const int64_t nbc[3]) {
-    DMOLP_CUDA(cudaStreamSynchronize(c->stream));
-    free_all(c);
-    c->nv = nv;
-    c->narcs = narcs;
-    c->maxdeg = maxdeg;
-    c->maxraw = maxraw;
-    c->ibits = bits_for(nv > 0 ? nv - 1 : 0);
-    c->dbits = bits_for(maxdeg);
-    c->rbits = bits_for(maxraw);
-    for (int i = 0; i < 3; ++i) c->nb[i] = (int)nbc[i];
-    c->chunk_cap = narcs / kChunk + 2;
-    c->hubq_cap = narcs / kHubChunk + nbc[2] + 2;
-    const size_t nball[3] = {(size_t)nbc[0], (size_t)nbc[1], (size_t)nbc[2]};
+// Places buffer `p` of n elements at the next 256-byte boundary of the arena (only sizes it when base is null).
+template <typename T>
+void place(char *base, size_t &off, T **p, size_t n) {
+    off = (off + 255) & ~(size_t)255;
+    if (base) *p = reinterpret_cast<T *>(base + off);
+    off += std::max<size_t>(n, 1) * sizeof(T);
+}
+
+// Byte layout of every resident buffer of a graph inside one arena; returns the arena size.  With base null
+// only the size is computed.
+size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t nball[3]) {
     Buffers &b = c->b;
     const size_t n = (size_t)nv + 1;
-    int st = DMOLP_OK;
-#define ALLOC(ptr, count) \
-    if ((st = dalloc(c, &(ptr), (count))) != DMOLP_OK) { free_all(c); return st; }
+    size_t off = 0;
+#define ALLOC(ptr, count) place(base, off, &(ptr), (count))
     ALLOC(b.off, n);
     ALLOC(b.col, (size_t)narcs);
     ALLOC(b.rawdeg, n);
@@ -274,10 +269,13 @@ int graph_alloc(dmolp_ctx *c, int64_t nv, int64_t narcs, int64_t maxdeg, int64_t
     ALLOC(b.p1cnt, 8);
     ALLOC(b.p1te, 1);
     ALLOC(b.flag, 1);
+    ALLOC(b.symcnt, 2);
     ALLOC(b.ball, nball[0] + nball[1] + nball[2]);
-    b.bucket[0] = b.ball;
-    b.bucket[1] = b.ball + nball[0];
-    b.bucket[2] = b.bucket[1] + nball[1];
+    if (base) {
+        b.bucket[0] = b.ball;
+        b.bucket[1] = b.ball + nball[0];
+        b.bucket[2] = b.bucket[1] + nball[1];
+    }
     for (int i = 0; i < 3; ++i) ALLOC(b.dec[i], n);
     ALLOC(b.newlab, n);
     ALLOC(b.mov, n);
@@ -285,7 +283,41 @@ int graph_alloc(dmolp_ctx *c, int64_t nv, int64_t narcs, int64_t maxdeg, int64_t
     ALLOC(b.hubq, (size_t)c->hubq_cap);
     ALLOC(b.hh, nball[2] * (size_t)DMOLP_MAX_K);
 #undef ALLOC
-    b.claim = b.stamp;  // phase 1 and the LP loop never run at the same time
+    return off;
+}
+
+// Frees the previous graph's state and lays out every resident buffer for a graph of the given sizes in
+// the context's arena: one allocation, kept for later graphs that fit (it grows to the largest graph
+// uploaded on the context).  Repeated uploads then allocate nothing.
+int graph_alloc(dmolp_ctx *c, int64_t nv, int64_t narcs, int64_t maxdeg, int64_t maxraw, const int64_t nbc[3]) {
+    DMOLP_CUDA(cudaStreamSynchronize(c->stream));
+    free_all(c);
+    c->nv = nv;
+    c->narcs = narcs;
+    c->maxdeg = maxdeg;
+    c->maxraw = maxraw;
+    c->ibits = bits_for(nv > 0 ? nv - 1 : 0);
+    c->dbits = bits_for(maxdeg);
+    c->rbits = bits_for(maxraw);
+    for (int i = 0; i < 3; ++i) c->nb[i] = (int)nbc[i];
+    c->chunk_cap = narcs / kChunk + 2;
+    c->hubq_cap = narcs / kHubChunk + nbc[2] + 2;
+    const size_t nball[3] = {(size_t)nbc[0], (size_t)nbc[1], (size_t)nbc[2]};
+    const size_t need = layout(c, nullptr, nv, narcs, nball);
+    if (need > c->arena_cap) {
+        if (c->arena) cudaFree(c->arena);
+        c->arena = nullptr;
+        c->arena_cap = 0;
+        cudaError_t e = cudaMalloc(&c->arena, need);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            c->arena = nullptr;
+            return fail(DMOLP_ERR_NOMEM, std::string("cudaMalloc (graph arena): ") + cudaGetErrorString(e));
+        }
+        c->arena_cap = need;
+    }
+    layout(c, (char *)c->arena, nv, narcs, nball);
+    c->b.claim = c->b.stamp;  // phase 1 and the LP loop never run at the same time
     return DMOLP_OK;
 }
 
@@ -304,24 +336,10 @@ int graph_finish(dmolp_ctx *c, bool rows_sorted) {
     DMOLP_CUDA(cudaMemsetAsync(b.bown, 0xff, n * sizeof(int32_t), c->stream));  // all record slots empty
     lp_fill(c, b.newlab, (int64_t)n, -1);
     select_prepare();
-    // every arc has its reverse (checked on the device): the LP loop may update its statistics from the
-    // movers alone
+    // whether every arc has its reverse is tested when the LP loop first needs it (ensure_symmetry)
     c->symmetric = false;
-    if (rows_sorted && nv > 0) {
-        // the arc counts borrow the (zeroed) radix-select histogram and leave it zeroed
-        unsigned long long *counts = reinterpret_cast<unsigned long long *>(b.hist);
-        DMOLP_CUDA(cudaMemsetAsync(b.flag, 0, sizeof(int), c->stream));
-        DMOLP_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), c->stream));
-        lp_check_symmetric(c, counts);
-        int missing = 1;
-        unsigned long long hc[2] = {0, 1};
-        DMOLP_CUDA(cudaMemcpyAsync(&missing, b.flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        DMOLP_CUDA(cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
-        DMOLP_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), c->stream));
-        int s1 = sync(c);
-        if (s1) return s1;
-        c->symmetric = missing == 0 && hc[0] == hc[1];
-    }
+    c->symmetry_known = false;
+    c->rows_sorted = rows_sorted;
     // log(t) and e^(-t/5) with the host's libm, as the reference computes them (phase2.cpp:199,
     // gpu_lp_boundary.cu:244)
     std::vector<double> lt(kMaxIter + 1, 0.0), rt(kMaxIter + 1, 1.0);
@@ -337,16 +355,35 @@ int graph_finish(dmolp_ctx *c, bool rows_sorted) {
     return DMOLP_OK;
 }
 
-// Device buffer for `len` bytes of text, padded to whole parse tiles (padding zeroed).
+// Whether every arc has its reverse, tested on the device the first time the LP loop needs it (then the
+// loop may update cut and balance from the movers alone); graphs whose rows are not strictly increasing
+// always take the full statistics pass.
+int ensure_symmetry(dmolp_ctx *c) {
+    if (c->symmetry_known) return DMOLP_OK;
+    Buffers &b = c->b;
+    c->symmetric = false;
+    if (c->rows_sorted && c->nv > 0) {
+        DMOLP_CUDA(cudaMemsetAsync(b.flag, 0, sizeof(int), c->stream));
+        DMOLP_CUDA(cudaMemsetAsync(b.symcnt, 0, 2 * sizeof(unsigned long long), c->stream));
+        lp_check_symmetric(c, b.symcnt);
+        int missing = 1;
+        unsigned long long hc[2] = {0, 1};
+        DMOLP_CUDA(cudaMemcpyAsync(&missing, b.flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DMOLP_CUDA(cudaMemcpyAsync(hc, b.symcnt, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
+        int s1 = sync(c);
+        if (s1) return s1;
+        c->symmetric = missing == 0 && hc[0] == hc[1];
+    }
+    c->symmetry_known = true;
+    return DMOLP_OK;
+}
+
+// Device buffer (parse scratch) for `len` bytes of text, padded to whole parse tiles (padding zeroed).
 int text_buffer(dmolp_ctx *c, int64_t len, uint8_t **out) {
     const int64_t cap = ingest::padded_bytes(len);
-    void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, (size_t)cap);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return fail(DMOLP_ERR_NOMEM, std::string("cudaMalloc (text): ") + cudaGetErrorString(e));
-    }
-    *out = (uint8_t *)q;
+    std::string err;
+    *out = (uint8_t *)c->scratch.get(ingest::kText, (size_t)cap, err);
+    if (!*out) return fail(DMOLP_ERR_NOMEM, err);
     DMOLP_CUDA(cudaMemsetAsync(*out + len, 0, (size_t)(cap - len), c->stream));
     return DMOLP_OK;
 }
@@ -365,12 +402,14 @@ int ingest_text(dmolp_ctx *c, uint8_t *d_txt, int64_t len, int64_t body0, int64_
     ingest::Parsed p;
     std::string err;
     DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
-    if (ingest::parse(c->stream, d_txt, len, body0, body1, p, err)) {
+    if (ingest::parse(c->stream, d_txt, len, body0, body1, c->scratch, p, err)) {
         ingest::release(p);
         cudaGetLastError();
         return fail(DMOLP_ERR_ARG, err);
     }
+    const auto ta = std::chrono::steady_clock::now();
     int st = graph_alloc(c, p.nv, p.narcs, p.maxdeg, p.maxraw, p.nb);
+    double setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
     if (!st) {
         Buffers &b = c->b;
         int32_t *const bucket[3] = {b.bucket[0], b.bucket[1], b.bucket[2]};
@@ -378,10 +417,8 @@ int ingest_text(dmolp_ctx *c, uint8_t *d_txt, int64_t len, int64_t body0, int64_
     }
     if (!st) {
         DMOLP_CUDA(cudaEventRecord(c->ev1, c->stream));
-        c->h_rawdeg.resize(p.nv);
-        if (p.nv)
-            DMOLP_CUDA(cudaMemcpyAsync(c->h_rawdeg.data(), c->b.rawdeg, (size_t)p.nv * sizeof(int32_t),
-                                       cudaMemcpyDeviceToHost, c->stream));
+        c->h_rawdeg.clear();  // the host mirror of the raw degrees is fetched when phase 1 first needs it
+        c->h_rawdeg_valid = false;
         st = sync(c);
     }
     c->launches += p.launches;
@@ -402,7 +439,11 @@ int ingest_text(dmolp_ctx *c, uint8_t *d_txt, int64_t len, int64_t body0, int64_
         free_all(c);
         return st;
     }
-    return graph_finish(c, true);
+    const auto tf = std::chrono::steady_clock::now();
+    st = graph_finish(c, true);
+    setup_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tf).count();
+    if (info) info->setup_ms = setup_ms;
+    return st;
 }
 
 }  // namespace
@@ -448,6 +489,8 @@ int dmolp_destroy(dmolp_ctx *c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     free_all(c);
+    if (c->arena) cudaFree(c->arena);
+    c->scratch.release();
     for (int i = 0; i < kPinSlots; ++i) {
         if (c->pin[i]) cudaFreeHost(c->pin[i]);
         if (c->pin_ev[i]) cudaEventDestroy(c->pin_ev[i]);
@@ -510,6 +553,7 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     if (st) return st;
     c->h_rawdeg.resize(nv);
     for (int64_t v = 0; v < nv; ++v) c->h_rawdeg[v] = raw ? raw[v] : (int32_t)(off[v + 1] - off[v]);
+    c->h_rawdeg_valid = true;
     Buffers &b = c->b;
     DMOLP_CUDA(cudaMemcpyAsync(b.off, off, (size_t)(nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
     if (narcs)
@@ -543,7 +587,7 @@ int dmolp_graph_upload_adjtext(dmolp_ctx *c, const char *text, int64_t len, dmol
     float copy_ms = 0.f;
     cudaEventElapsedTime(&copy_ms, c->ev0, c->ev1);
     st = ingest_text(c, d_txt, len, body0, body1, info);
-    cudaFree(d_txt);
+    c->scratch.trim(ingest::kKeepScratch);
     if (info) {
         info->read_ms = copy_ms;
         info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -583,7 +627,7 @@ int dmolp_graph_upload_adjtext_device(dmolp_ctx *c, const char *d_text, int64_t 
     DMOLP_CUDA(cudaMemcpyAsync(d_txt, d_text, (size_t)len, cudaMemcpyDeviceToDevice, c->stream));
     const double read_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     st = ingest_text(c, d_txt, len, body0, body1, info);
-    cudaFree(d_txt);
+    c->scratch.trim(ingest::kKeepScratch);
     if (info) {
         info->read_ms = read_ms;
         info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -655,7 +699,7 @@ int dmolp_graph_load_adjtext(dmolp_ctx *c, const char *path, dmolp_ingest_info *
     const double read_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (!st && body0 < 0) st = fail(DMOLP_ERR_ARG, "missing header line");
     if (!st) st = ingest_text(c, d_txt, len, body0, std::max(body0, body1), info);
-    if (d_txt) cudaFree(d_txt);
+    c->scratch.trim(ingest::kKeepScratch);
     if (info) {
         info->read_ms = read_ms;
         info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -922,6 +966,15 @@ int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *ve
     DMOLP_CUDA(cudaSetDevice(c->device));
     Buffers &b = c->b;
     const int64_t nv = c->nv;
+    if (!c->h_rawdeg_valid) {  // a device-parsed graph: fetch the raw degrees once
+        c->h_rawdeg.resize(nv);
+        if (nv)
+            DMOLP_CUDA(cudaMemcpyAsync(c->h_rawdeg.data(), b.rawdeg, (size_t)nv * sizeof(int32_t),
+                                       cudaMemcpyDeviceToHost, c->stream));
+        int s0 = sync(c);
+        if (s0) return s0;
+        c->h_rawdeg_valid = true;
+    }
     dmolp_phase1_info inf;
     std::memset(&inf, 0, sizeof(inf));
     DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
@@ -997,6 +1050,8 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
         return fail(DMOLP_ERR_ARG, "iterations must be in [0, 500]");
     if (cfg->cap != DMOLP_LP_CAP_REF && cfg->cap != DMOLP_LP_CAP_FULL) return fail(DMOLP_ERR_ARG, "bad cap");
     DMOLP_CUDA(cudaSetDevice(c->device));
+    int sy = ensure_symmetry(c);
+    if (sy) return sy;
     Buffers &b = c->b;
     LpLaunch L;
     L.k = k;

@@ -37,8 +37,15 @@ struct Scal {
     int nlist[3];                   // unsorted rows per length class
 };
 
-// 0xff/0x00 per byte -> one bit per byte (byte 0 -> bit 0)
-__device__ __forceinline__ uint32_t byte_bits(uint32_t m) { return ((m & 0x80808080u) * 0x00204081u) >> 28; }
+// Byte tests on a 32-bit word, one flag per byte in bit 7 of that byte.  Exact for every byte value: the
+// additions work on 7-bit fields, so no carry crosses into the next byte.
+__device__ __forceinline__ uint32_t zero_bytes(uint32_t w) { return ~(((w & 0x7f7f7f7fu) + 0x7f7f7f7fu) | w) & 0x80808080u; }
+__device__ __forceinline__ uint32_t digit_bytes(uint32_t w) {  // '0'..'9'
+    const uint32_t lo = w & 0x7f7f7f7fu;
+    return (lo + 0x50505050u) & ~(lo + 0x46464646u) & ~w & 0x80808080u;
+}
+// bit-7 byte flags -> 4-bit mask (byte 0 -> bit 0)
+__device__ __forceinline__ uint32_t byte_bits(uint32_t m) { return (m * 0x00204081u) >> 28; }
 
 struct Chunk {
     uint32_t nl, zero, dig, body, ts;  // 16-bit masks over the chunk's bytes; ts = token starts
@@ -47,16 +54,25 @@ struct Chunk {
 
 // Classify the 16 bytes at `pos` (16-aligned).  All 32 lanes must call it (the previous byte comes from
 // the neighbouring lane).
-__device__ __forceinline__ Chunk chunk_at(const uint8_t *__restrict__ txt, int64_t pos, int64_t body0, int64_t body1) {
+__device__ __forceinline__ Chunk chunk_at(const uint8_t *__restrict__ txt, int64_t pos, int64_t body0, int64_t body1,
+                                         uint4 *raw = nullptr) {
     const uint4 q = __ldg(reinterpret_cast<const uint4 *>(txt + pos));
+    if (raw) *raw = q;
     const uint32_t w[4] = {q.x, q.y, q.z, q.w};
     Chunk c;
     c.nl = c.zero = c.dig = 0;
+    uint32_t anyz = 0;
+    uint32_t zw[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        c.nl |= byte_bits(__vcmpeq4(w[i], 0x0a0a0a0au)) << (4 * i);
-        c.zero |= byte_bits(__vcmpeq4(w[i], 0u)) << (4 * i);
-        c.dig |= byte_bits(__vcmpgeu4(w[i], 0x30303030u) & __vcmpleu4(w[i], 0x39393939u)) << (4 * i);
+        c.nl |= byte_bits(zero_bytes(w[i] ^ 0x0a0a0a0au)) << (4 * i);
+        c.dig |= byte_bits(digit_bytes(w[i])) << (4 * i);
+        zw[i] = zero_bytes(w[i]);
+        anyz |= zw[i];
+    }
+    if (anyz) {  // NUL bytes: the tile padding, or a NUL in the text
+#pragma unroll
+        for (int i = 0; i < 4; ++i) c.zero |= byte_bits(zw[i]) << (4 * i);
     }
     const int lane = threadIdx.x & 31;
     uint32_t pb = __shfl_up_sync(DMOLP_FULL_MASK, q.w >> 24, 1);
@@ -70,6 +86,16 @@ __device__ __forceinline__ Chunk chunk_at(const uint8_t *__restrict__ txt, int64
     const uint32_t prev_dig = ((c.dig << 1) | pdig) & 0xffffu;
     c.ts = c.body & ~c.nl & ~c.zero & (c.prev_nl | (c.dig & ~prev_dig));
     return c;
+}
+
+// Value of a run of 1..8 ASCII digits held little-endian in v (first digit in the lowest byte): left-pad to
+// eight digits with '0', then combine digit pairs, quads and halves with three multiplications (Lemire's
+// eight-digit SWAR parse, "Faster integer parsing", 2021).
+__device__ __forceinline__ uint32_t parse_digits8(uint64_t v, int n) {
+    if (n < 8) v = (v << (8 * (8 - n))) | (0x3030303030303030ull >> (8 * n));
+    v = ((v & 0x0f0f0f0f0f0f0f0full) * 2561) >> 8;
+    v = ((v & 0x00ff00ff00ff00ffull) * 6553601) >> 16;
+    return (uint32_t)(((v & 0x0000ffff0000ffffull) * 42949672960001ull) >> 32);
 }
 
 // Exclusive block scan of a 32-bit value (packed counters whose block totals cannot carry).
@@ -202,46 +228,82 @@ __global__ void __launch_bounds__(1024) k_scan(const uint32_t *__restrict__ cnt,
 }
 
 // Tokens in text order: value (bit 31 = first token of its line); end_tok[l] = tokens before line l's
-// newline.  Values are parsed with saturation at 2^31, so any id >= V is caught.
+// newline.  Per step a warp owns a 512-byte window: the lanes classify their 16 bytes, stage them in
+// shared memory with the window's token starts, then parse the window's tokens round-robin (lane i takes
+// tokens i, i+32, ...), so the digit loops are balanced across the warp and the stores are coalesced.
+// Values are parsed with saturation at 2^31, so any id >= V is caught.
+constexpr int kWin = 32 * kChunkBytes;  // bytes of a warp's window
+constexpr int kLook = 32;               // look-ahead staged past the window
+
 __global__ void __launch_bounds__(kTxtThreads) k_txt_emit(const uint8_t *__restrict__ txt, int64_t body0,
                                                           int64_t body1, int64_t nv, const int64_t *__restrict__ toff,
                                                           uint32_t *__restrict__ tok, int64_t *__restrict__ end_tok,
                                                           Scal *sc) {
     __shared__ uint32_t s_w[kNW];
+    __shared__ __align__(16) uint8_t s_txt[kNW][kWin + kLook];
+    __shared__ uint16_t s_pos[kNW][kWin];  // window offset of each token start; bit 15 = first of its line
     const int64_t tile = blockIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint8_t *wt = s_txt[wid];
+    uint16_t *wp = s_pos[wid];
     int64_t lbase = toff[2 * tile], tbase = toff[2 * tile + 1];
     int bad = 0;
 #pragma unroll 1
     for (int s = 0; s < kTxtSteps; ++s) {
         const int64_t pos = tile * kTileBytes + (int64_t)(s * kTxtThreads + threadIdx.x) * kChunkBytes;
-        const Chunk c = chunk_at(txt, pos, body0, body1);
+        uint4 q;
+        const Chunk c = chunk_at(txt, pos, body0, body1, &q);
+        reinterpret_cast<uint4 *>(wt)[lane] = q;
+        if (lane < kLook / 16)  // the bytes after the window, for digit runs that cross its end
+            reinterpret_cast<uint4 *>(wt + kWin)[lane] =
+                __ldg(reinterpret_cast<const uint4 *>(txt + pos - lane * kChunkBytes + kWin) + lane);
         const uint32_t nlm = c.nl & c.body;
+        const uint32_t ntk = (uint32_t)__popc(c.ts);
         uint32_t tot;
-        const uint32_t ex = block_excl_scan((uint32_t)__popc(nlm) << 16 | (uint32_t)__popc(c.ts), &tot, s_w);
-        int64_t l = lbase + (ex >> 16), t = tbase + (ex & 0xffffu);
-        uint32_t ev = nlm | c.ts;
-        while (ev) {
-            const int j = __ffs(ev) - 1;
-            ev &= ev - 1;
-            if ((nlm >> j) & 1u) {
-                end_tok[l++] = t;
-            } else {
-                uint64_t x = 0;
-                if ((c.dig >> j) & 1u) {
-                    int64_t q = pos + j;
-                    uint32_t b = txt[q];
-                    while (b - '0' <= 9u) {
-                        x = x * 10 + (b - '0');
-                        if (x > kVal) x = (uint64_t)kVal + 1;
-                        b = txt[++q];
-                    }
-                }
-                if ((int64_t)x >= nv) bad = 1;
-                tok[t++] = ((uint32_t)x & kVal) | (((c.prev_nl >> j) & 1u) ? kFirst : 0u);
+        const uint32_t ex = block_excl_scan((uint32_t)__popc(nlm) << 16 | ntk, &tot, s_w);
+        const int64_t t0 = tbase + (ex & 0xffffu);  // this lane's first token
+        int64_t l = lbase + (ex >> 16);
+        const uint32_t wex = __shfl_sync(DMOLP_FULL_MASK, ex & 0xffffu, 0);
+        const int o = (int)((ex & 0xffffu) - wex);  // offset of this lane's tokens in the window's list
+        const int wtot = __shfl_sync(DMOLP_FULL_MASK, o + (int)ntk, 31);
+        uint32_t m = c.ts;
+        for (int k = 0; m; ++k) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            wp[o + k] = (uint16_t)(lane * kChunkBytes + j) | (((c.prev_nl >> j) & 1u) ? 0x8000u : 0u);
+        }
+        for (uint32_t n = nlm; n; n &= n - 1) {
+            const int j = __ffs(n) - 1;
+            end_tok[l++] = t0 + __popc(c.ts & ((1u << j) - 1));
+        }
+        __syncwarp();
+        const int64_t tw = t0 - o;  // the window's first token
+        for (int i = lane; i < wtot; i += 32) {
+            const uint32_t e = wp[i];
+            const int x0 = (int)(e & 0x7fffu);
+            // the 8 bytes from the token start, out of three aligned words of the staged window
+            const uint32_t *w32 = reinterpret_cast<const uint32_t *>(wt) + (x0 >> 2);
+            const uint32_t a0 = w32[0], a1 = w32[1], a2 = w32[2], a3 = w32[3];
+            const uint32_t sh = 8u * (x0 & 3);
+            const uint32_t lo = __funnelshift_r(a0, a1, sh), hi = __funnelshift_r(a1, a2, sh);
+            const uint32_t nx = __funnelshift_r(a2, a3, sh);  // bytes 8..11 of the token
+            const uint32_t dm = byte_bits(digit_bytes(lo)) | byte_bits(digit_bytes(hi)) << 4 |
+                                byte_bits(digit_bytes(nx)) << 8;
+            const int n = __ffs(~dm) - 1;  // leading digits (0..12)
+            uint32_t x;
+            if (n <= 8) {
+                x = n ? parse_digits8((uint64_t)hi << 32 | lo, n) : 0u;
+            } else {  // nine digits or more (ids >= 10^8, or leading zeros): digit by digit
+                int64_t g = pos - lane * kChunkBytes + x0;
+                x = 0;
+                for (uint32_t b = txt[g]; b - '0' <= 9u; b = txt[++g]) x = x > 214748364u ? 0x80000000u : x * 10 + (b - '0');
             }
+            if ((int64_t)x >= nv) bad = 1;
+            tok[tw + i] = (x & kVal) | ((e & 0x8000u) ? kFirst : 0u);
         }
         lbase += tot >> 16;
         tbase += tot & 0xffffu;
+        __syncwarp();
     }
     if (bad) atomicOr(&sc->bad_id, 1);
 }
@@ -528,16 +590,9 @@ __global__ void k_keep_compact(const uint32_t *__restrict__ tok, int64_t ntok, c
 // ---- host side ----
 
 template <typename T>
-bool dev_alloc(T **p, size_t n, std::string &err) {
-    void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
-        return false;
-    }
-    *p = (T *)q;
-    return true;
+bool pool_get(Pool &pool, int slot, T **p, size_t n, std::string &err) {
+    *p = (T *)pool.get(slot, std::max<size_t>(n, 1) * sizeof(T), err);
+    return *p != nullptr;
 }
 
 #define ING_CUDA(call)                                                              \
@@ -548,8 +603,8 @@ bool dev_alloc(T **p, size_t n, std::string &err) {
             return 1;                                                               \
         }                                                                           \
     } while (0)
-#define ING_ALLOC(ptr, n) \
-    if (!dev_alloc(&(ptr), (n), err)) return 1
+#define ING_ALLOC(slot, ptr, n) \
+    if (!pool_get(*p.pool, (slot), &(ptr), (n), err)) return 1
 
 struct Events {  // timing of the two text passes, destroyed on every exit path
     cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -568,27 +623,56 @@ int grid_for(int64_t n, int threads) {
 
 }  // namespace
 
-void release(Parsed &p) {
-    for (void *q : {(void *)p.tok, (void *)p.tmp, (void *)p.end_tok, (void *)p.keptpos, (void *)p.tcnt,
-                    (void *)p.toff, (void *)p.loff, (void *)p.badrow, (void *)p.lists, p.scal})
-        if (q) cudaFree(q);
-    p = Parsed();
+void *Pool::get(int slot, size_t bytes, std::string &err) {
+    if (cap[slot] < bytes) {
+        if (ptr[slot]) cudaFree(ptr[slot]);
+        ptr[slot] = nullptr;
+        cap[slot] = 0;
+        const size_t want = (bytes + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
+        cudaError_t e = cudaMalloc(&ptr[slot], want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ptr[slot] = nullptr;
+            err = std::string("cudaMalloc (parse scratch): ") + cudaGetErrorString(e);
+            return nullptr;
+        }
+        cap[slot] = want;
+    }
+    return ptr[slot];
 }
 
-int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t body1, Parsed &p, std::string &err) {
+size_t Pool::held() const {
+    size_t t = 0;
+    for (size_t c : cap) t += c;
+    return t;
+}
+
+void Pool::release() {
+    for (int i = 0; i < kNumSlots; ++i) {
+        if (ptr[i]) cudaFree(ptr[i]);
+        ptr[i] = nullptr;
+        cap[i] = 0;
+    }
+}
+
+void release(Parsed &p) { p = Parsed(); }
+
+int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t body1, Pool &pool, Parsed &p,
+          std::string &err) {
     release(p);
+    p.pool = &pool;
     (void)len;
     Events ev;
     for (cudaEvent_t &e : ev.e) ING_CUDA(cudaEventCreate(&e));
     Scal *sc = nullptr;
-    ING_ALLOC(sc, 1);
+    ING_ALLOC(kScal, sc, 1);
     p.scal = sc;
     ING_CUDA(cudaMemsetAsync(sc, 0, sizeof(Scal), st));
     const int64_t nt = body1 > body0 ? (body1 + kTileBytes - 1) / kTileBytes : 0;
     int64_t tot[2] = {0, 0};
     if (nt > 0) {
-        ING_ALLOC(p.tcnt, (size_t)2 * nt);
-        ING_ALLOC(p.toff, (size_t)2 * (nt + 1));
+        ING_ALLOC(kTcnt, p.tcnt, (size_t)2 * nt);
+        ING_ALLOC(kToff, p.toff, (size_t)2 * (nt + 1));
         ING_CUDA(cudaEventRecord(ev.e[0], st));
         k_txt_count<<<(unsigned)nt, kTxtThreads, 0, st>>>(d_txt, body0, body1, p.tcnt, sc);
         ING_CUDA(cudaEventRecord(ev.e[1], st));
@@ -613,9 +697,9 @@ int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t b
         err = "too many vertices for int32 ids";
         return 1;
     }
-    ING_ALLOC(p.tok, (size_t)p.ntok);
-    ING_ALLOC(p.end_tok, (size_t)p.nv);
-    ING_ALLOC(p.badrow, (size_t)p.nv);
+    ING_ALLOC(kTok, p.tok, (size_t)p.ntok);
+    ING_ALLOC(kEndTok, p.end_tok, (size_t)p.nv);
+    ING_ALLOC(kBadrow, p.badrow, (size_t)p.nv);
     Scal h{};
     if (p.nv > 0) {
         ING_CUDA(cudaEventRecord(ev.e[2], st));
@@ -640,7 +724,7 @@ int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t b
     p.sorted = h.violations == 0;
     p.narcs = p.ntok;
     if (!p.sorted) {
-        ING_ALLOC(p.lists, (size_t)3 * p.nv);
+        ING_ALLOC(kLists, p.lists, (size_t)3 * p.nv);
         k_rows_classify<<<grid_for(p.nv, 256), 256, 0, st>>>(p.end_tok, p.nv, p.badrow, p.lists, sc);
         ++p.launches;
         ING_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, st));
@@ -655,20 +739,14 @@ int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t b
             ++p.launches;
         }
         if (h.nlist[2]) {
-            ING_ALLOC(p.tmp, (size_t)p.ntok);
+            ING_ALLOC(kTmp, p.tmp, (size_t)p.ntok);
             k_sort_big<<<h.nlist[2], 1024, 0, st>>>(p.tok, p.tmp, p.end_tok, p.lists + 2 * p.nv);
             ++p.launches;
         }
         const int64_t ntt = (p.ntok + kTokTile - 1) / kTokTile;
-        uint32_t *kc = nullptr;
-        int64_t *ko = nullptr;
-        ING_ALLOC(kc, (size_t)ntt);
-        cudaFree(p.tcnt);
-        p.tcnt = kc;
-        ING_ALLOC(ko, (size_t)ntt + 1);
-        cudaFree(p.toff);
-        p.toff = ko;
-        ING_ALLOC(p.keptpos, (size_t)p.ntok + 1);
+        ING_ALLOC(kTcnt, p.tcnt, (size_t)ntt);  // the text tiles' counters are no longer needed
+        ING_ALLOC(kToff, p.toff, (size_t)ntt + 1);
+        ING_ALLOC(kKeptpos, p.keptpos, (size_t)p.ntok + 1);
         k_keep_count<<<(unsigned)ntt, kTxtThreads, 0, st>>>(p.tok, p.ntok, p.tcnt);
         k_scan<1><<<1, 1024, 0, st>>>(p.tcnt, ntt, p.toff);
         k_keep_pos<<<(unsigned)ntt, kTxtThreads, 0, st>>>(p.tok, p.ntok, p.toff, p.keptpos);
@@ -677,8 +755,8 @@ int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t b
     }
     const int64_t nlt = (p.nv + kLineTile - 1) / kLineTile;
     uint32_t *lcnt = nullptr;
-    ING_ALLOC(lcnt, (size_t)3 * nlt);
-    ING_ALLOC(p.loff, (size_t)3 * (nlt + 1));
+    ING_ALLOC(kLcnt, lcnt, (size_t)3 * nlt);
+    ING_ALLOC(kLoff, p.loff, (size_t)3 * (nlt + 1));
     int64_t nb[3] = {0, 0, 0};
     if (nlt > 0) {
         k_lines_count<<<(unsigned)nlt, kTxtThreads, 0, st>>>(p.end_tok, p.keptpos, p.nv, lcnt, sc);
@@ -688,7 +766,6 @@ int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t b
         ING_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, st));
     }
     const cudaError_t e = cudaStreamSynchronize(st);
-    cudaFree(lcnt);
     if (e != cudaSuccess) {
         err = std::string("ingest: ") + cudaGetErrorString(e);
         return 1;

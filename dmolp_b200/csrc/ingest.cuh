@@ -20,10 +20,28 @@ constexpr int kLineSteps = 16;                // lines per thread in the per-lin
 constexpr int64_t kLineTile = (int64_t)kTxtThreads * kLineSteps;
 constexpr int64_t kTokTile = 4096;            // tokens per block in the de-duplication scan
 
-// Device text buffer size for `len` bytes: whole tiles, so every 16-byte load stays inside the allocation.
-inline int64_t padded_bytes(int64_t len) { return (len / kTileBytes + 1) * kTileBytes; }
+// Device text buffer size for `len` bytes: whole tiles plus one, so every 16-byte load of a tile and the
+// look-ahead past a warp's window stay inside the allocation.
+inline int64_t padded_bytes(int64_t len) { return (len / kTileBytes + 2) * kTileBytes; }
 
-// Parse state between the sizing pass and the CSR build (device scratch owned here).
+// Grow-only device scratch of the parse, kept by the context so that repeated loads allocate nothing
+// (trimmed after a load when it holds more than kKeepScratch bytes).
+enum Slot { kText, kScal, kTcnt, kToff, kTok, kTmp, kEndTok, kKeptpos, kBadrow, kLists, kLcnt, kLoff, kNumSlots };
+constexpr size_t kKeepScratch = size_t(6) << 30;
+
+struct Pool {
+    void *ptr[kNumSlots] = {};
+    size_t cap[kNumSlots] = {};
+    // At least `bytes` bytes in `slot` (contents not kept when it grows); null with `err` set on failure.
+    void *get(int slot, size_t bytes, std::string &err);
+    size_t held() const;
+    void release();
+    void trim(size_t keep) {
+        if (held() > keep) release();
+    }
+};
+
+// Parse state between the sizing pass and the CSR build (device scratch borrowed from a Pool).
 struct Parsed {
     int64_t nv = 0;          // newline-terminated lines after the header
     int64_t ntok = 0;        // tokens (sum of raw degrees)
@@ -45,20 +63,22 @@ struct Parsed {
     uint8_t *badrow = nullptr;    // [nv] row needs sorting
     int32_t *lists = nullptr;     // rows to sort, by length class
     void *scal = nullptr;         // device counters
+    Pool *pool = nullptr;
 };
 
 // Sizing pass: d_txt holds the text padded to padded_bytes(len) (padding zeroed), body = [body0, body1)
 // (after the header's newline, up to and including the last newline).  NUL bytes in the body are
 // overwritten in place (a NUL ends the parse of its line).  On success p holds the sizes and the scratch.
 // Returns 0, or 1 with `err` set (bad id, too many vertices, CUDA failure).
-int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t body1, Parsed &p, std::string &err);
+int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t body1, Pool &pool, Parsed &p,
+          std::string &err);
 
 // CSR build into the context's arrays: off[nv+1], col[narcs], raw[nv], and the degree-class lists
 // bucket[c][nb[c]] in ascending id order.
 int build(cudaStream_t st, Parsed &p, int64_t *off, int32_t *col, int32_t *raw, int32_t *const bucket[3],
           std::string &err);
 
-void release(Parsed &p);
+void release(Parsed &p);  // returns the scratch to the pool (nothing is freed)
 
 }  // namespace ingest
 }  // namespace dmolp

@@ -124,6 +124,7 @@ typedef struct {
     int64_t kernels;                /* kernels launched by the parse */
     double count_ms;                /* device time of the text count pass (one kernel) */
     double emit_ms;                 /* device time of the token emit pass (one kernel) */
+    double setup_ms;                /* resident-state allocation and initialisation (wall clock) */
 } dmolp_ingest_info;
 int dmolp_graph_upload_adjtext(dmolp_ctx *ctx, const char *text, int64_t len, dmolp_ingest_info *info);
 int dmolp_graph_load_adjtext(dmolp_ctx *ctx, const char *path, dmolp_ingest_info *info);

@@ -243,15 +243,27 @@ def test_symmetry_detection_selects_the_statistics_path(part):
         part.phase2(1, mode="fixed", iterations=3, records=False)
         return part.kernel_launches() - a
 
+    def drop_arc(gr, x, y):  # the graph without arc (x, y); (y, x) stays
+        row = gr.indices[gr.offsets[x]:gr.offsets[x + 1]]
+        keep = np.ones(gr.num_arcs, bool)
+        keep[gr.offsets[x] + int(np.nonzero(row == y)[0][0])] = False
+        off = np.zeros(gr.num_vertices + 1, np.int64)
+        src = np.repeat(np.arange(gr.num_vertices), np.diff(gr.offsets))
+        off[1:] = np.cumsum(np.diff(gr.offsets) - np.bincount(src[~keep], minlength=gr.num_vertices))
+        return graphs.Graph(off, gr.indices[keep])
+
     sym = launches_for(g)
     u = 7
     v = int(g.indices[g.offsets[u]])
-    row = g.indices[g.offsets[v]:g.offsets[v + 1]]
-    keep = np.ones(g.num_arcs, bool)
-    keep[g.offsets[v] + int(np.nonzero(row == u)[0][0])] = False  # (v, u) goes, (u, v) stays
-    off = np.zeros(g.num_vertices + 1, np.int64)
-    off[1:] = np.cumsum(np.diff(g.offsets) - np.bincount(np.repeat(np.arange(g.num_vertices), np.diff(g.offsets))[~keep],
-                                                         minlength=g.num_vertices))
-    asym = launches_for(graphs.Graph(off, g.indices[keep]))
-    assert asym == sym + 3
+    # the missing reverse on either side: the endpoint that searches and the one that is only counted
+    assert launches_for(drop_arc(g, v, u)) == sym + 3
+    assert launches_for(drop_arc(g, u, v)) == sym + 3
     assert launches_for(g) == sym
+    # a skewed graph: an arc between a hub and a leaf, dropped from the hub's row and from the leaf's
+    r = graphs.rmat(12, 8, seed=5)
+    deg = np.diff(r.offsets)
+    hub = int(np.argmax(deg))
+    leaf = int(r.indices[r.offsets[hub]:r.offsets[hub + 1]][np.argmin(deg[r.indices[r.offsets[hub]:r.offsets[hub + 1]]])])
+    rs = launches_for(r)
+    assert launches_for(drop_arc(r, hub, leaf)) == rs + 3
+    assert launches_for(drop_arc(r, leaf, hub)) == rs + 3

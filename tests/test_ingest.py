@@ -23,6 +23,7 @@ TEXTS = {
     "nul_mid_line": b"3\n1 2\x00 0\n2\x00\n\x00 1\n",
     "nul_runs": b"4\n3\x00\x00 1\x002\n0 1\n\x00\n1 2 3\x00\n",
     "trailing_separators": b"2\n1 ,; \n0\t\t\n",
+    "long_digit_runs": b"3\n000000001 0000000000002 00000002\n00000000\n000000000000000000000001 2\n",
 }
 
 
@@ -163,7 +164,8 @@ def test_device_parse_rejects_bad_ids_and_keeps_previous_graph(part):
 
     part.upload_adjtext(TEXTS["plain"])
     before = part.graph_arrays()
-    for bad in (b"2\n1\n5\n", b"2\n1\n99999999999999999999\n", b"no newline"):
+    for bad in (b"2\n1\n5\n", b"2\n1\n99999999999999999999\n", b"2\n1\n4294967296\n", b"2\n1\n2147483648\n",
+                b"no newline"):
         with pytest.raises(DmolpError):
             part.upload_adjtext(bad)
     after = part.graph_arrays()
