@@ -382,18 +382,22 @@ Phase1Metrics run_phase1(int mpi_rank, int mpi_size, const char *graph_file, int
     std::lock_guard<std::mutex> lk(g_mu);
     Phase1Metrics m{};
     const auto t0 = Clock::now();
-    dmolp_host_graph *hg = nullptr;
-    if (dmolp_adjtext_load(graph_file, &hg) != 0) {
-        fprintf(stderr, "Process %d: Error opening file: %s (%s)\n", mpi_rank, graph_file, dmolp_adjtext_error());
+    // The text is parsed on the device into the resident graph (load_graph + the CSR build of
+    // build_local_graph_and_ghosts); the caller's Graph gets a host copy of it.
+    g_main.ensure_ctx();
+    dmolp_ingest_info ii;
+    if (dmolp_graph_load_adjtext(g_main.ctx, graph_file, &ii) != 0) {
+        fprintf(stderr, "Process %d: Error opening file: %s (%s)\n", mpi_rank, graph_file, dmolp_last_error());
         std::exit(1);
     }
-    const int64_t nv = dmolp_host_graph_nv(hg), na = dmolp_host_graph_narcs(hg);
-    std::vector<int64_t> off(dmolp_host_graph_offsets(hg), dmolp_host_graph_offsets(hg) + nv + 1);
-    std::vector<int> col(dmolp_host_graph_indices(hg), dmolp_host_graph_indices(hg) + na);
-    std::vector<int> raw(dmolp_host_graph_raw_degree(hg), dmolp_host_graph_raw_degree(hg) + nv);
-    dmolp_host_graph_free(hg);
-    uint64_t e2 = 0;
-    for (int r : raw) e2 += (uint64_t)r;
+    const int64_t nv = ii.num_vertices, na = ii.num_arcs;
+    std::vector<int64_t> off(nv + 1);
+    std::vector<int> col(na);
+    std::vector<int> raw(nv);
+    check(dmolp_graph_get(g_main.ctx, off.data(), col.data(), raw.data()), "dmolp_graph_get");
+    g_main.nv = nv;
+    g_main.rp = g_main.ci = nullptr;
+    const uint64_t e2 = (uint64_t)ii.num_tokens;
     m.loading_time_ms = ms_since(t0);
     const auto t1 = Clock::now();
     std::vector<int> lab;
@@ -421,8 +425,7 @@ Phase1Metrics run_phase1(int mpi_rank, int mpi_size, const char *graph_file, int
             vc[p] = (int)v64[p];
             ec[p] = (int)e64[p];
         }
-    } else {
-        g_main.upload(off, col, &raw);
+    } else {  // the graph parsed above is already resident
         std::vector<int64_t> v64(num_parts), e64(num_parts);
         std::vector<int32_t> seeds(num_parts);
         dmolp_phase1_info info;

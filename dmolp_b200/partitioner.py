@@ -244,9 +244,8 @@ class Partitioner:
 def run_phase1(graph_file: str, num_parts: int, theta: int, device: int = 0):
     """The reference's run_phase1 (src/phase1/phase1.cpp:18) at one rank: returns (metrics, partitioner); the
     partitioner keeps the graph and the phase-1 labels resident for run_phase2."""
-    g = load_adjtext(graph_file)
     p = Partitioner(device)
-    p.upload(g)
+    p.upload_adjtext(graph_file)  # parsed on the device into the resident graph
     return p.phase1(num_parts, theta), p
 
 

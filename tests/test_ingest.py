@@ -197,3 +197,24 @@ def test_device_parsed_graph_partitions_like_host_loaded(part):
     assert m1.total_edges == m2.total_edges
     assert r1.edge_cut == r2.edge_cut and np.array_equal(lab1, q.labels())
     q.close()
+
+
+@pytest.mark.gpu
+def test_run_phase1_from_file_matches_oracle(tmp_path):
+    """The reference's run_phase1(graph_file, ...) form: the file parsed on the device, then phase 1 and
+    phase 2 on the resident graph, against the oracle on the same text."""
+    from dmolp_b200 import graphs
+    from dmolp_b200.partitioner import run_phase1, run_phase2
+
+    g = graphs.knn(3000, 3, 10, seed=2)
+    path = str(tmp_path / "g.txt")
+    graphs.write_adjtext(g, path)
+    off, col, raw = oracle.load_adjtext(path)
+    m, p = run_phase1(path, 8, 100)
+    o1 = oracle.phase1(off, col, raw, 8, 100)
+    assert np.array_equal(p.labels(), o1.labels) and m.seeds == o1.seeds.tolist()
+    assert m.total_edges == int(raw.astype(np.int64).sum()) // 2
+    r = run_phase2(p, 8, mode="fixed", iterations=10)
+    o2 = oracle.phase2(off, col, o1.labels, 8, "fixed", 10)
+    assert np.array_equal(p.labels(), o2.labels) and r.edge_cut == o2.res.edge_cut
+    p.close()
