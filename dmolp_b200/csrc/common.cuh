@@ -14,6 +14,7 @@ constexpr int kWarpsPerBlock = kBlock / kWarp;
 constexpr int kRadixBits = 8;               // digit width of the segmented radix select
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kMaxIter = 500;               // the reference's max_iter (src/phase2/phase2.cpp:263)
+constexpr int kSelHistBuffers = 3;          // the radix select's global histograms rotate over three buffers
 
 // 5-bit bit reversal: the position at which the reference's 32-lane shuffle-down tree prefers a lane
 // among equal scores (lane with the smaller reversed index wins).

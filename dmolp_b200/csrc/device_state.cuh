@@ -49,9 +49,9 @@ struct LpControl {
     int error;          // 1 = odd cut-arc count or invalid label (the reference aborts)
     int mode;           // DMOLP_LP_MODE_*
     int pull;           // next iteration finds candidates by pulling (rows scanned for a window member)
-    int sel_done;       // radix select: blocks finished the current histogram
-    int sel_open;       // radix select: segments still needing records
-    int sel_pass;       // radix select: the pass whose digit decisions are current
+    int sel_open[2];    // radix select: segments still needing records after a pass (by pass parity)
+    unsigned int bar_count, bar_gen;  // grid barrier of the cooperative selection kernel
+    int wait_timeout;   // a grid barrier gave up waiting (never expected: the launch is cooperative)
 };
 
 // One LP iteration record as kept on the device.
@@ -163,6 +163,7 @@ struct dmolp_ctx {
     double prof_ms[5] = {0, 0, 0, 0, 0};
     long long prof_launches[5] = {0, 0, 0, 0, 0};
     double prof_bytes[5] = {0, 0, 0, 0, 0};
+    cudaError_t launch_error = cudaSuccess;  // first failed launch that returns no status to its caller
     void *arena = nullptr;                 // every resident buffer of the graph (layout in graph_alloc)
     size_t arena_cap = 0;
     dmolp::ingest::Pool scratch;           // device scratch of the text parse, reused across loads

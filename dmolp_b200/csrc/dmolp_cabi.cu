@@ -88,6 +88,26 @@ int sync(dmolp_ctx *c) {
     return check_launch(c);
 }
 
+// A grid barrier of the cooperative window selection that gave up waiting (never expected: its launch is
+// cooperative): report it, and clear the barrier state for the next launch.
+int check_waits(dmolp_ctx *c) {
+    if (c->launch_error != cudaSuccess) {
+        const cudaError_t e = c->launch_error;
+        c->launch_error = cudaSuccess;
+        cudaGetLastError();
+        return fail(DMOLP_ERR_CUDA, std::string("window selection launch: ") + cudaGetErrorString(e));
+    }
+    int to = 0;
+    DMOLP_CUDA(cudaMemcpyAsync(&to, &c->b.ctrl->wait_timeout, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    int st = sync(c);
+    if (st) return st;
+    if (!to) return DMOLP_OK;
+    // bar_count, bar_gen, wait_timeout are adjacent
+    DMOLP_CUDA(cudaMemsetAsync(&c->b.ctrl->bar_count, 0, 3 * sizeof(int), c->stream));
+    sync(c);
+    return fail(DMOLP_ERR_CUDA, "a grid barrier of the window selection timed out");
+}
+
 // The reference's balance = max over parts of count / expected (src/phase2/phase2.cpp:426-432).
 void balances(const std::vector<long long> &vc, const std::vector<long long> &ec, int k, double *vb, double *eb,
               int64_t *tv_out, int64_t *te_out) {
@@ -245,7 +265,7 @@ size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t 
     ALLOC(b.bsel, n);
     ALLOC(b.active[0], n);
     ALLOC(b.active[1], n);
-    ALLOC(b.hist, (size_t)DMOLP_MAX_K * kRadix);
+    ALLOC(b.hist, (size_t)kSelHistBuffers * DMOLP_MAX_K * kRadix);
     ALLOC(b.need, DMOLP_MAX_K);
     ALLOC(b.sel_below, DMOLP_MAX_K);
     ALLOC(b.keep_digit, DMOLP_MAX_K);
@@ -328,7 +348,8 @@ int graph_finish(dmolp_ctx *c, bool rows_sorted) {
     const int64_t nv = c->nv;
     const size_t n = (size_t)nv + 1;
     DMOLP_CUDA(cudaMemsetAsync(b.label, 0, n * sizeof(int32_t), c->stream));
-    DMOLP_CUDA(cudaMemsetAsync(b.hist, 0, (size_t)DMOLP_MAX_K * kRadix * sizeof(unsigned int), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.hist, 0, (size_t)kSelHistBuffers * DMOLP_MAX_K * kRadix * sizeof(unsigned int),
+                               c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.ctrl, 0, sizeof(LpControl), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.cnt, 0, sizeof(LpCounters), c->stream));
     const int npos = c->nb[0] + c->nb[1] + c->nb[2];
@@ -954,7 +975,7 @@ int dmolp_expand_partitions(dmolp_ctx *c, int k, int theta, const int32_t *seeds
     int r = 0;
     st = expand_impl(c, k, theta, seedk, &r);
     if (rounds) *rounds = r;
-    return st;
+    return st ? st : check_waits(c);
 }
 
 int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *vertex_counts, int64_t *edge_counts,
@@ -1037,7 +1058,7 @@ int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *ve
     }
     if (info) *info = inf;
     if (bad) return fail(DMOLP_ERR_BAD_LABELS, "phase 1 left a label outside [0,k)");
-    return DMOLP_OK;
+    return check_waits(c);
 }
 
 int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_result *res, dmolp_lp_record *records,
@@ -1097,6 +1118,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     DMOLP_CUDA(cudaMemcpyAsync(recs.data(), b.rec, kMaxIter * sizeof(LpRecordDev), cudaMemcpyDeviceToHost, c->stream));
     st = sync(c);
     if (st) return st;
+    if (ctl.wait_timeout || c->launch_error != cudaSuccess) return check_waits(c);
     if (ctl.error) return fail(DMOLP_ERR_BAD_LABELS, "label outside [0,k) or odd cut-arc count");
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -1240,7 +1262,7 @@ int dmolp_window_select(dmolp_ctx *c, int k, int iteration, const double *RE, co
     if (st) return st;
     std::sort(out, out + n);
     *nout = n;
-    return DMOLP_OK;
+    return check_waits(c);
 }
 
 int dmolp_lp_apply(dmolp_ctx *c, int k, int cap, const double *penalty, const int32_t *window, int64_t nwindow,
