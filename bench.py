@@ -236,7 +236,8 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
     if args.quick:
         p.close()
         return {"metric": "LP traversed edges/s", "value": te / elapsed, "unit": "TE/s", "ms_per_step":
-                elapsed / args.steps * 1e3, "quick": True, "kernels": prof, "gpu_launches": int(launches)}
+                elapsed / args.steps * 1e3, "quick": True, "kernels": prof, "gpu_launches": int(launches),
+                "phase1": {"gpu_ms": m1.gpu_ms, "stage_ms": m1.stage_ms, "rounds": m1.rounds}}
     # ---- end to end through the public API, host buffers in pinned memory ----
     off_h = torch.from_numpy(g.offsets).pin_memory()
     col_h = torch.from_numpy(g.indices).pin_memory()
@@ -295,7 +296,8 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
                    "label_cap": "reference (min(k,32))", "num_vertices": g.num_vertices, "num_arcs": g.num_arcs,
                    "te_per_step": te // args.steps, "edge_cut": last.edge_cut,
                    "vertex_balance": last.vertex_balance, "edge_balance": last.edge_balance,
-                   "phase1_gpu_ms": m1.gpu_ms, "phase1_initial_edge_cut": m1.initial_edge_cut,
+                   "phase1_gpu_ms": m1.gpu_ms, "phase1_stage_ms": m1.stage_ms, "phase1_rounds": m1.rounds,
+                   "phase1_initial_edge_cut": m1.initial_edge_cut,
                    "l2": "inputs larger than L2 (CSR arcs %.0f MB)" % (g.indices.nbytes / 1e6),
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_te * world / e2e_max, "unit": "TE/s", "h2d_bytes_per_step": int(h2d),

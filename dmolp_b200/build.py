@@ -32,7 +32,7 @@ NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", *GENCODE, "-Xcompiler", "-fPIC,-
               "--expt-relaxed-constexpr", "-Xptxas", "-v"]
 
 CUDA_SOURCES = ["dmolp_cabi.cu", "lp_kernels.cu", "seed_kernels.cu", "select_kernels.cu", "adjtext.cpp",
-                "noalloc.cu", "ingest.cu", "batch_kernels.cu", "batch_cabi.cu", "batch_p1.cu", "mpnn_kernels.cu", "mpnn_cabi.cu"]
+                "noalloc.cu", "ingest.cu", "hubsort.cpp", "batch_kernels.cu", "batch_cabi.cu", "batch_p1.cu", "mpnn_kernels.cu", "mpnn_cabi.cu"]
 CUDA_HEADERS = ["common.cuh", "device_state.cuh", "kernels.cuh", "lp_device.cuh", "batch.cuh", "mpnn.cuh", "umma.cuh", "ingest.cuh"]
 DROPIN_SOURCES = ["dropin.cpp"]
 

@@ -34,7 +34,7 @@ EXPORTS = [
     "dmolp_mpnn_prepare_training", "dmolp_mpnn_backward", "dmolp_mpnn_train_step", "dmolp_mpnn_decode",
     "dmolp_batch_propose", "dmolp_mpnn_gate", "dmolp_mpnn_train_gate", "dmolp_batch_phase1",
     "dmolp_graph_upload_adjtext", "dmolp_graph_load_adjtext", "dmolp_graph_size", "dmolp_graph_get",
-    "dmolp_graph_upload_adjtext_device",
+    "dmolp_graph_upload_adjtext_device", "dmolp_find_hubs_pairs", "dmolp_degree_order",
 ]
 BATCH_MAX_K = 64
 
@@ -42,7 +42,8 @@ BATCH_MAX_K = 64
 class Phase1Info(ctypes.Structure):
     _fields_ = [("initial_edge_cut", c_int64), ("initial_vertex_balance", c_double),
                 ("initial_edge_balance", c_double), ("num_seeds_found", c_int32), ("rounds", c_int32),
-                ("num_hubs", c_int64), ("traversed_edges", c_uint64), ("gpu_ms", c_double)]
+                ("num_hubs", c_int64), ("traversed_edges", c_uint64), ("gpu_ms", c_double),
+                ("hubs_ms", c_double), ("seeds_ms", c_double), ("expand_ms", c_double)]
 
 
 class LpConfig(ctypes.Structure):
@@ -95,6 +96,8 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_graph_load_adjtext.argtypes = [vp, c_char_p, POINTER(IngestInfo)]
     lib.dmolp_graph_upload_adjtext_device.argtypes = [vp, vp, c_int64, POINTER(IngestInfo)]
     lib.dmolp_graph_size.argtypes = [vp, POINTER(c_int64), POINTER(c_int64)]
+    lib.dmolp_find_hubs_pairs.argtypes = [c_int64, vp, vp, vp, POINTER(c_int64)]
+    lib.dmolp_degree_order.argtypes = [c_int64, vp, vp]
     lib.dmolp_graph_get.argtypes = [vp, vp, vp, vp]
     lib.dmolp_phase1.argtypes = [vp, c_int, c_int, vp, vp, vp, POINTER(Phase1Info)]
     lib.dmolp_lp_run.argtypes = [vp, c_int, POINTER(LpConfig), POINTER(LpResult), vp, c_int]

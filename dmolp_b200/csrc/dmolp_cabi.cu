@@ -157,35 +157,13 @@ int run_stats(dmolp_ctx *c, int k, unsigned long long *cut_arcs, std::vector<lon
     return DMOLP_OK;
 }
 
-// src/phase1/init.cpp:139-177 (see the comment at the top of this file).
+// src/phase1/init.cpp:139-177 (see the comment at the top of this file): pairs in the order the reference's
+// degree map iterates at one rank (V-1..0), sorted with std::sort's exact permutation on all host threads.
 std::vector<int> find_hubs(const std::vector<int32_t> &raw) {
     const int64_t nv = (int64_t)raw.size();
-    std::vector<std::pair<int, int>> sd;
-    sd.reserve(nv);
-    for (int64_t v = nv - 1; v >= 0; --v) sd.emplace_back((int)v, raw[v]);
-    std::sort(sd.begin(), sd.end(),
-              [](const std::pair<int, int> &a, const std::pair<int, int> &b) { return a.second < b.second; });
-    const int N = (int)sd.size();
-    std::vector<int> hubs;
-    if (N < 2) return hubs;
-    std::vector<double> cum(N);
-    double total = 0.0, run = 0.0;
-    for (int i = 0; i < N; ++i) {
-        total += sd[i].second;
-        run += sd[i].second;
-        cum[i] = run;
-    }
-    for (int i = 0; i < N; ++i) cum[i] /= total;
-    const double inv_n = 1.0 / N;
-    const double x1 = N * inv_n, y1 = cum[N - 1];
-    const double x0 = (N - 1) * inv_n, y0 = cum[N - 2];
-    const double slope = (y1 - y0) / (x1 - x0);
-    const double x_int = x1 - y1 / slope;
-    for (int i = N - 1; i >= 0; --i) {
-        if ((i + 1) * inv_n > x_int) hubs.push_back(sd[i].first);
-        else break;
-    }
-    return hubs;
+    std::vector<std::pair<int, int>> sd(nv);
+    for (int64_t i = 0; i < nv; ++i) sd[i] = std::make_pair((int)(nv - 1 - i), raw[nv - 1 - i]);
+    return dmolp::hubs_from_pairs(std::move(sd));
 }
 
 // Capture (once) and launch the iterations [t0, t0+cnt) of an LP run as one CUDA graph.
@@ -1001,6 +979,7 @@ int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *ve
     DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
 
     // ---- hubs and first seed on the host (order-dependent; see the top of this file) ----
+    const auto th0 = std::chrono::steady_clock::now();
     std::vector<int> hubs = find_hubs(c->h_rawdeg);
     std::pair<int, int> first(-1, -1);
     for (int64_t v = nv - 1; v >= 0; --v) {  // init.cpp:179-187, including its id-vs-degree tie test
@@ -1009,11 +988,15 @@ int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *ve
     }
     inf.num_hubs = (int64_t)hubs.size();
     DMOLP_CUDA(cudaMemsetAsync(b.p1te, 0, sizeof(unsigned long long), c->stream));
+    const auto th1 = std::chrono::steady_clock::now();
+    inf.hubs_ms = std::chrono::duration<double, std::milli>(th1 - th0).count();
     std::vector<int> seeds;
     st = find_seeds_impl(c, k, first.first, hubs, seeds);
     if (st) return st;
     inf.num_seeds_found = (int32_t)seeds.size();
     complete_seeds(c, k, hubs, seeds);
+    const auto th2 = std::chrono::steady_clock::now();
+    inf.seeds_ms = std::chrono::duration<double, std::milli>(th2 - th1).count();
     std::vector<int32_t> seedk(k, -1);
     for (int p = 0; p < k && p < (int)seeds.size(); ++p) seedk[p] = seeds[p];
     if (seeds_out) std::copy(seedk.begin(), seedk.end(), seeds_out);
@@ -1036,6 +1019,7 @@ int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *ve
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     inf.gpu_ms = ms;
+    inf.expand_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - th2).count();
     inf.traversed_edges = te;
     inf.initial_edge_cut = (int64_t)(arcs / 2);
     const double ev = (double)nv / k;

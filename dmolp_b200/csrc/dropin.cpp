@@ -151,31 +151,18 @@ void parse_line(const char *p, const char *end, std::vector<int> &out) {
     }
 }
 
-// find_hub_nodes' input is the degree map in its iteration order (src/phase1/init.cpp:139-177).
-std::vector<int> hubs_from_pairs(std::vector<std::pair<int, int>> sd) {
-    std::sort(sd.begin(), sd.end(),
-              [](const std::pair<int, int> &a, const std::pair<int, int> &b) { return a.second < b.second; });
-    const int N = (int)sd.size();
-    std::vector<int> hubs;
-    if (N < 2) return hubs;
-    std::vector<double> cum(N);
-    double total = 0.0, run = 0.0;
-    for (int i = 0; i < N; ++i) {
-        total += sd[i].second;
-        run += sd[i].second;
-        cum[i] = run;
+// find_hub_nodes' input is the degree map in its iteration order (src/phase1/init.cpp:139-177); the sort
+// (std::sort's exact permutation) and the tangent rule run in the C-ABI library on all host threads.
+std::vector<int> hubs_from_pairs(const std::vector<std::pair<int, int>> &sd) {
+    const int64_t n = (int64_t)sd.size();
+    std::vector<int32_t> ids(n), deg(n), hubs(n);
+    for (int64_t i = 0; i < n; ++i) {
+        ids[i] = sd[i].first;
+        deg[i] = sd[i].second;
     }
-    for (int i = 0; i < N; ++i) cum[i] /= total;
-    const double inv_n = 1.0 / N;
-    const double x1 = N * inv_n, y1 = cum[N - 1];
-    const double x0 = (N - 1) * inv_n, y0 = cum[N - 2];
-    const double slope = (y1 - y0) / (x1 - x0);
-    const double x_int = x1 - y1 / slope;
-    for (int i = N - 1; i >= 0; --i) {
-        if ((i + 1) * inv_n > x_int) hubs.push_back(sd[i].first);
-        else break;
-    }
-    return hubs;
+    int64_t nh = 0;
+    check(dmolp_find_hubs_pairs(n, ids.data(), deg.data(), hubs.data(), &nh), "dmolp_find_hubs_pairs");
+    return std::vector<int>(hubs.begin(), hubs.begin() + nh);
 }
 
 void phase1_balance(const std::vector<int> &vc, const std::vector<int> &ec, int nv, int k, Phase1Metrics &m) {

@@ -1,0 +1,264 @@
+// Hub list of phase 1 (src/phase1/init.cpp:139-177) with the reference's exact sort order, computed on all
+// host threads.
+//
+// find_hub_nodes sorts (vertex, degree) pairs by degree with std::sort, which is not stable: among equal
+// degrees the order it leaves depends on every step of libstdc++'s introsort, and that order decides which of
+// two equal-degree hubs seeding picks first.  This file restates that published algorithm step for step
+// (median-of-three pivot moved to the front, unguarded Hoare partition, a depth limit of 2*floor(log2 n) with
+// heapsort below it, ranges of at most 16 left to a final insertion pass) so that the permutation is the same,
+// and runs it in parallel where the algorithm itself is independent:
+//   * after a partition, the two sides are sorted without looking at each other: large right sides become
+//     OpenMP tasks;
+//   * the final insertion pass never moves an element left of a position p with max(a[0..p)) <= min(a[p..n)),
+//     so the array is cut at such positions and the pieces are finished in parallel.
+// tests/test_hubsort.py checks the permutation against std::sort itself on tie-heavy and adversarial inputs.
+#include <omp.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <utility>
+#include <vector>
+
+#include "../../include/dmolp_b200.h"
+
+namespace {
+
+using Pair = std::pair<int32_t, int32_t>;  // (vertex, degree), ordered by degree only
+constexpr int64_t kSmall = 16;             // ranges this short are left to the final insertion pass
+constexpr int64_t kTaskMin = 1 << 15;      // right sides at least this long become tasks
+constexpr int64_t kParallelMin = 1 << 18;  // shorter inputs are sorted on the calling thread
+
+inline bool less(const Pair &a, const Pair &b) { return a.second < b.second; }
+
+// ---- heapsort, used below the depth limit ----
+void sift_up(Pair *a, int64_t hole, int64_t top, Pair v) {
+    int64_t parent = (hole - 1) / 2;
+    while (hole > top && less(a[parent], v)) {
+        a[hole] = a[parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    a[hole] = v;
+}
+
+void sift_down(Pair *a, int64_t hole, int64_t len, Pair v) {
+    const int64_t top = hole;
+    int64_t child = hole;
+    while (child < (len - 1) / 2) {
+        child = 2 * (child + 1);
+        if (less(a[child], a[child - 1])) --child;
+        a[hole] = a[child];
+        hole = child;
+    }
+    if ((len & 1) == 0 && child == (len - 2) / 2) {
+        child = 2 * (child + 1);
+        a[hole] = a[child - 1];
+        hole = child - 1;
+    }
+    sift_up(a, hole, top, v);
+}
+
+void heapsort(Pair *a, int64_t len) {
+    if (len >= 2) {  // build the heap
+        for (int64_t parent = (len - 2) / 2;; --parent) {
+            sift_down(a, parent, len, a[parent]);
+            if (parent == 0) break;
+        }
+    }
+    for (int64_t last = len; last > 1;) {  // pop the maximum to the back
+        --last;
+        const Pair v = a[last];
+        a[last] = a[0];
+        sift_down(a, 0, last, v);
+    }
+}
+
+// ---- quicksort steps ----
+void median_to_front(Pair *res, Pair *x, Pair *y, Pair *z) {
+    if (less(*x, *y)) {
+        if (less(*y, *z)) std::swap(*res, *y);
+        else if (less(*x, *z)) std::swap(*res, *z);
+        else std::swap(*res, *x);
+    } else if (less(*x, *z)) {
+        std::swap(*res, *x);
+    } else if (less(*y, *z)) {
+        std::swap(*res, *z);
+    } else {
+        std::swap(*res, *y);
+    }
+}
+
+Pair *partition_around_front(Pair *first, Pair *last) {
+    Pair *mid = first + (last - first) / 2;
+    median_to_front(first, first + 1, mid, last - 1);
+    const Pair *pivot = first;
+    Pair *lo = first + 1, *hi = last;
+    for (;;) {
+        while (less(*lo, *pivot)) ++lo;
+        --hi;
+        while (less(*pivot, *hi)) --hi;
+        if (!(lo < hi)) return lo;
+        std::swap(*lo, *hi);
+        ++lo;
+    }
+}
+
+void introsort_loop(Pair *first, Pair *last, int64_t depth) {
+    while (last - first > kSmall) {
+        if (depth == 0) {
+            heapsort(first, last - first);
+            return;
+        }
+        --depth;
+        Pair *cut = partition_around_front(first, last);
+        if (last - cut >= kTaskMin) {
+#pragma omp task firstprivate(cut, last, depth)
+            introsort_loop(cut, last, depth);
+        } else {
+            introsort_loop(cut, last, depth);
+        }
+        last = cut;
+    }
+}
+
+// ---- final insertion pass ----
+void linear_insert(Pair *pos) {  // unguarded: some element to the left is not greater
+    const Pair v = *pos;
+    Pair *prev = pos - 1;
+    while (less(v, *prev)) {
+        *pos = *prev;
+        pos = prev;
+        --prev;
+    }
+    *pos = v;
+}
+
+void guarded_insertion(Pair *first, Pair *last) {
+    if (first == last) return;
+    for (Pair *i = first + 1; i != last; ++i) {
+        if (less(*i, *first)) {
+            const Pair v = *i;
+            std::move_backward(first, i, i + 1);
+            *first = v;
+        } else {
+            linear_insert(i);
+        }
+    }
+}
+
+int lg(int64_t n) {
+    int b = 0;
+    while (n > 1) {
+        n >>= 1;
+        ++b;
+    }
+    return b;
+}
+
+}  // namespace
+
+namespace dmolp {
+
+// The permutation std::sort(a, a + n, by degree) leaves, computed in parallel for large n.
+void sort_by_degree(Pair *a, int64_t n) {
+    if (n <= 1) return;
+    const int T = n >= kParallelMin ? std::max(1, omp_get_max_threads()) : 1;
+    if (T > 1) {
+#pragma omp parallel num_threads(T)
+#pragma omp single
+        introsort_loop(a, a + n, 2 * (int64_t)lg(n));
+    } else {
+        introsort_loop(a, a + n, 2 * (int64_t)lg(n));
+    }
+    if (n <= kSmall) {
+        guarded_insertion(a, a + n);
+        return;
+    }
+    guarded_insertion(a, a + kSmall);
+    if (T == 1) {
+        for (Pair *i = a + kSmall; i != a + n; ++i) linear_insert(i);
+        return;
+    }
+    // Cut points p with max(a[0..p)) <= min(a[p..n)): no element moves left across them, and a piece that
+    // starts at one sorts the same way on its own (its insertions stop at p either way).  After the loop every
+    // range is either sorted (heapsort) or at most kSmall long with all of it between its neighbours, so it
+    // suffices that the kSmall elements before p are not above the kSmall elements from p on.
+    auto safe = [&](int64_t p) {
+        int32_t left = INT32_MIN, right = INT32_MAX;
+        for (int64_t i = std::max<int64_t>(0, p - kSmall); i < p; ++i) left = std::max(left, a[i].second);
+        for (int64_t i = p; i < std::min(n, p + kSmall); ++i) right = std::min(right, a[i].second);
+        return left <= right;
+    };
+    const int64_t step = std::max<int64_t>(n / (8 * (int64_t)T), 4096);
+    std::vector<int64_t> cuts{kSmall};
+    for (int64_t p = kSmall + step; p < n; p += step) {
+        int64_t q = p;
+        while (q < n && !safe(q)) ++q;
+        if (q < n && q > cuts.back()) cuts.push_back(q);
+        p = std::max(p, q);
+    }
+    cuts.push_back(n);
+    const int64_t pieces = (int64_t)cuts.size() - 1;
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1)
+    for (int64_t s = 0; s < pieces; ++s) {
+        if (s == 0) {  // continues the sorted first kSmall elements
+            for (Pair *i = a + cuts[0]; i != a + cuts[1]; ++i) linear_insert(i);
+        } else {       // never reads left of its start
+            guarded_insertion(a + cuts[s], a + cuts[s + 1]);
+        }
+    }
+}
+
+// find_hub_nodes on pairs in the reference's map order.
+std::vector<int> hubs_from_pairs(std::vector<Pair> sd) {
+    sort_by_degree(sd.data(), (int64_t)sd.size());
+    const int N = (int)sd.size();
+    std::vector<int> hubs;
+    if (N < 2) return hubs;
+    // The reference accumulates the sorted degrees in a double, left to right (init.cpp:145-160).  Every
+    // partial sum of non-negative integers below 2^53 is exact in a double, so the integer sums give the same
+    // bits: only the total and the sum without the last element are needed.
+    int64_t total_i = 0;
+#pragma omp parallel for reduction(+ : total_i) schedule(static) if (N >= kParallelMin)
+    for (int i = 0; i < N; ++i) total_i += sd[i].second;
+    const double total = (double)total_i;
+    const double y1 = (double)total_i / total, y0 = (double)(total_i - sd[N - 1].second) / total;
+    const double inv_n = 1.0 / N;
+    const double x1 = N * inv_n;
+    const double x0 = (N - 1) * inv_n;
+    const double slope = (y1 - y0) / (x1 - x0);
+    const double x_int = x1 - y1 / slope;
+    for (int i = N - 1; i >= 0; --i) {
+        if ((i + 1) * inv_n > x_int) hubs.push_back(sd[i].first);
+        else break;
+    }
+    return hubs;
+}
+
+}  // namespace dmolp
+
+extern "C" {
+
+int dmolp_degree_order(int64_t n, int32_t *ids, int32_t *degrees) {
+    if (n < 0 || (n > 0 && (!ids || !degrees))) return DMOLP_ERR_ARG;
+    std::vector<Pair> a(n);
+    for (int64_t i = 0; i < n; ++i) a[i] = Pair(ids[i], degrees[i]);
+    dmolp::sort_by_degree(a.data(), n);
+    for (int64_t i = 0; i < n; ++i) {
+        ids[i] = a[i].first;
+        degrees[i] = a[i].second;
+    }
+    return DMOLP_OK;
+}
+
+int dmolp_find_hubs_pairs(int64_t n, const int32_t *ids, const int32_t *degrees, int32_t *hubs, int64_t *nhubs) {
+    if (n < 0 || n > 0x7fffffff || (n > 0 && (!ids || !degrees || !hubs)) || !nhubs) return DMOLP_ERR_ARG;
+    std::vector<Pair> a(n);
+    for (int64_t i = 0; i < n; ++i) a[i] = Pair(ids[i], degrees[i]);
+    const std::vector<int> h = dmolp::hubs_from_pairs(std::move(a));
+    std::copy(h.begin(), h.end(), hubs);
+    *nhubs = (int64_t)h.size();
+    return DMOLP_OK;
+}
+
+}  // extern "C"

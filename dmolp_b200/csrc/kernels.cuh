@@ -1,9 +1,16 @@
 // Host-side launchers of the DMOLP kernels (one translation unit per kernel family).
 #pragma once
 
+#include <utility>
+#include <vector>
+
 #include "device_state.cuh"
 
 namespace dmolp {
+
+// ---- host (hubsort.cpp) ----
+// find_hub_nodes on (vertex, degree) pairs in the reference's map order, std::sort's tie order kept.
+std::vector<int> hubs_from_pairs(std::vector<std::pair<int, int>> sd);
 
 // ---- segmented radix select (select_kernels.cu) ----
 // Records i < *n_dev carry a segment seg[i] in [0,nseg) (or -1: an empty slot, ignored) and a 64-bit key

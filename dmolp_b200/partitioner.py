@@ -48,6 +48,7 @@ class Phase1Metrics:  # include/graph_types.h:276-309
     num_hubs: int
     traversed_edges: int
     gpu_ms: float
+    stage_ms: dict = field(default_factory=dict)  # hubs / seeds / expand (wall clock)
 
 
 @dataclass
@@ -188,7 +189,8 @@ class Partitioner:
                          else (self.raw_total or 0) // 2),
             partition_vertex_counts=vc.tolist(), partition_edge_counts=ec.tolist(), seeds=seeds.tolist(),
             num_seeds_found=info.num_seeds_found, rounds=info.rounds, num_hubs=info.num_hubs,
-            traversed_edges=info.traversed_edges, gpu_ms=info.gpu_ms)
+            traversed_edges=info.traversed_edges, gpu_ms=info.gpu_ms,
+            stage_ms={"hubs": info.hubs_ms, "seeds": info.seeds_ms, "expand": info.expand_ms})
 
     # ---- phase 2 ----
     def phase2(self, k: int, mode: str = "ref", iterations: int = 20, cap: str = "ref",

@@ -51,6 +51,9 @@ typedef struct {
     int64_t num_hubs;
     uint64_t traversed_edges;      /* arcs read by ball marking + expansion */
     double gpu_ms;                 /* device time of the phase (CUDA events) */
+    double hubs_ms;                /* host: hub sort and first seed (wall clock) */
+    double seeds_ms;               /* seed search and completion (wall clock) */
+    double expand_ms;              /* expansion rounds and initial metrics (wall clock) */
 } dmolp_phase1_info;
 
 typedef struct {
@@ -209,6 +212,15 @@ int dmolp_labels_restore(dmolp_ctx *ctx);
  * No reference counterpart. */
 int dmolp_set_profiling(dmolp_ctx *ctx, int enable);
 int dmolp_kernel_profile(dmolp_ctx *ctx, int kernel, double *total_ms, int64_t *launches, double *bytes);
+
+/* ---- phase-1 hubs on the host (no device work) ----
+ * dmolp_find_hubs_pairs: find_hub_nodes (src/phase1/init.cpp:139-177) on n (id, degree) pairs given in the
+ * reference's degree-map order: the pairs sorted by degree in exactly the order std::sort leaves them (ties
+ * included), the Lorenz-curve tangent's x-intercept, and the hubs past it in descending sort order; hubs
+ * needs room for n entries.  dmolp_degree_order returns that sorted order itself (ids[], degrees[] rewritten
+ * in place).  Both run on all host threads and give std::sort's permutation (checked against it). */
+int dmolp_find_hubs_pairs(int64_t n, const int32_t *ids, const int32_t *degrees, int32_t *hubs, int64_t *nhubs);
+int dmolp_degree_order(int64_t n, int32_t *ids, int32_t *degrees);
 
 /* ---- host-side graph loading (no device work) ----
  * Parse the reference's adjacency text: first line V, line i+1 = neighbour ids of vertex i.  Produces the

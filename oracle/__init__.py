@@ -50,6 +50,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_last_error.restype = c_char_p
         L.oracle_load_adjtext.argtypes = [c_char_p, POINTER(c_int64), POINTER(c_int64), c_void_p, c_void_p, c_void_p]
         L.oracle_find_hubs.argtypes = [c_int64, c_void_p, c_void_p, POINTER(c_int64)]
+        L.oracle_degree_order.argtypes = [c_int64, c_void_p, c_void_p]
         L.oracle_phase1.argtypes = [c_int64, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p,
                                     c_void_p, POINTER(Phase1Result)]
         L.oracle_phase2.argtypes = [c_int64, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_void_p,
@@ -78,6 +79,14 @@ def load_adjtext(path: str):
     raw = np.empty(nv.value, np.int32)
     _check(lib().oracle_load_adjtext(os.fsencode(path), ctypes.byref(nv), ctypes.byref(na), _p(off), _p(col), _p(raw)))
     return off, col, raw
+
+
+def degree_order(ids: np.ndarray, degrees: np.ndarray):
+    """(ids, degrees) in the order std::sort by degree leaves them (find_hub_nodes' sort, init.cpp:142)."""
+    i = np.ascontiguousarray(ids, np.int32).copy()
+    d = np.ascontiguousarray(degrees, np.int32).copy()
+    _check(lib().oracle_degree_order(i.shape[0], _p(i), _p(d)))
+    return i, d
 
 
 def find_hubs(raw_degree: np.ndarray) -> np.ndarray:

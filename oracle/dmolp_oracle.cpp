@@ -490,6 +490,21 @@ int oracle_load_adjtext(const char *path, int64_t *nv_out, int64_t *narcs_out, i
     return 0;
 }
 
+// The permutation std::sort leaves on (id, degree) pairs ordered by degree: the sort of find_hub_nodes
+// (src/phase1/init.cpp:142), run by this toolchain's libstdc++ itself.
+int oracle_degree_order(int64_t n, int32_t *ids, int32_t *degrees) {
+    std::vector<std::pair<int, int>> a(n);
+    for (int64_t i = 0; i < n; ++i) a[i] = std::make_pair(ids[i], degrees[i]);
+    std::sort(a.begin(), a.end(), [](const std::pair<int, int> &x, const std::pair<int, int> &y) {
+        return x.second < y.second;
+    });
+    for (int64_t i = 0; i < n; ++i) {
+        ids[i] = a[i].first;
+        degrees[i] = a[i].second;
+    }
+    return 0;
+}
+
 int oracle_find_hubs(int64_t nv, const int32_t *rawdeg, int32_t *hubs_out, int64_t *nhubs) {
     std::vector<int> h = find_hubs(nv, rawdeg);
     *nhubs = (int64_t)h.size();

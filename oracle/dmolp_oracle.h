@@ -49,6 +49,7 @@ typedef struct {
  * token count used as the vertex degree in phase 1.  Two calls: sizes first (off/col/rawdeg NULL). */
 int oracle_load_adjtext(const char *path, int64_t *nv, int64_t *narcs, int64_t *off, int32_t *col, int32_t *rawdeg);
 
+int oracle_degree_order(int64_t n, int32_t *ids, int32_t *degrees);
 int oracle_find_hubs(int64_t nv, const int32_t *rawdeg, int32_t *hubs_out, int64_t *nhubs);
 
 int oracle_phase1(int64_t nv, const int64_t *off, const int32_t *col, const int32_t *rawdeg, int k, int theta,
