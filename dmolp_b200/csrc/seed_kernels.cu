@@ -127,8 +127,26 @@ __global__ void k_p1_need(Buffers b, int k, int theta) {
     }
 }
 
-// Warp per selected frontier vertex: claim unlabelled neighbours with atomicMin(part).  The one thread that
-// turns a claim from INT_MAX appends the vertex to the claimed list.
+// Claims of the arcs [s, e) of a selected frontier vertex of part p, one warp: unlabelled neighbours take
+// atomicMin(part); the one thread that turns a claim from INT_MAX appends the vertex to the claimed list.
+__device__ __forceinline__ void claim_arcs(const Buffers &b, int p, int64_t s, int64_t e) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t j0 = s; j0 < e; j0 += 32) {
+        const int64_t j = j0 + lane;
+        bool first = false;
+        int v = 0;
+        if (j < e) {
+            v = ld_stream(b.col + j);
+            if (b.label[v] < 0) first = atomicMin(&b.claim[v], p) == INT_MAX;
+        }
+        const int slot = warp_append(&b.p1cnt[2], first);
+        if (first) b.cand[slot] = v;
+    }
+}
+
+// Warp per selected frontier vertex: its first kChunk arcs; the rest of a longer row (the seeds are hubs) is
+// queued in kChunk pieces for k_p1_claim_chunks, so that no warp walks a whole hub row alone.  Claims are
+// atomicMin, so the order in which pieces run does not matter.
 __global__ void k_p1_claim(Buffers b, int cur) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
@@ -140,21 +158,31 @@ __global__ void k_p1_claim(Buffers b, int cur) {
         const int u = front[i];
         const int p = b.bown[i];
         const int64_t s = b.off[u], e = b.off[u + 1];
-        if (lane == 0) te += (unsigned long long)(e - s);
-        for (int64_t j0 = s; j0 < e; j0 += 32) {
-            const int64_t j = j0 + lane;
-            bool first = false;
-            int v = 0;
-            if (j < e) {
-                v = ld_stream(b.col + j);
-                if (b.label[v] < 0) first = atomicMin(&b.claim[v], p) == INT_MAX;
+        if (lane == 0) {
+            te += (unsigned long long)(e - s);
+            for (int64_t c = s + kChunk; c < e; c += kChunk) {
+                const int q = atomicAdd(&b.p1cnt[5], 1);
+                b.chunkq[q] = make_int2(i, (int)(c - s));
             }
-            const int slot = warp_append(&b.p1cnt[2], first);
-            if (first) b.cand[slot] = v;
         }
+        claim_arcs(b, p, s, e - s > kChunk ? s + kChunk : e);
     }
     te = warp_sum_u64(te);
     if (lane == 0 && te) atomicAdd(b.p1te, te);
+}
+
+// Warp per queued piece of a long frontier row.
+__global__ void k_p1_claim_chunks(Buffers b, int cur) {
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int n = b.p1cnt[5];
+    const int32_t *front = b.win[cur];
+    for (int q = gw; q < n; q += nw) {
+        const int2 c = b.chunkq[q];
+        const int u = front[c.x];
+        const int64_t rs = b.off[u], re = b.off[u + 1];
+        const int64_t s = rs + c.y;
+        claim_arcs(b, b.bown[c.x], s, re - s > kChunk ? s + kChunk : re);
+    }
 }
 
 // Claimed vertices take their part and join the next frontier; unselected frontier vertices carry over.
@@ -191,6 +219,7 @@ __global__ void k_p1_advance(Buffers b) {
     b.p1cnt[0] = b.p1cnt[1];
     b.p1cnt[1] = 0;
     b.p1cnt[2] = 0;
+    b.p1cnt[5] = 0;
 }
 
 int grid_for(dmolp_ctx *c) { return c->num_sms * 4; }
@@ -233,9 +262,10 @@ void p1_round(dmolp_ctx *c, int k, int theta, int cur) {
     c->launches += 2;
     select_smallest(c, c->b.bown, c->b.bkey, &c->b.p1cnt[4], k, c->rbits + c->ibits, c->b.bsel, nullptr);
     k_p1_claim<<<grid, kBlock, 0, c->stream>>>(c->b, cur);
+    k_p1_claim_chunks<<<grid, kBlock, 0, c->stream>>>(c->b, cur);
     k_p1_commit<<<grid, kBlock, 0, c->stream>>>(c->b, cur);
     k_p1_advance<<<1, 1, 0, c->stream>>>(c->b);
-    c->launches += 3;
+    c->launches += 4;
 }
 
 }  // namespace dmolp
