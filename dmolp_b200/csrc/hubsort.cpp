@@ -88,11 +88,49 @@ void median_to_front(Pair *res, Pair *x, Pair *y, Pair *z) {
     }
 }
 
+// Hoare's partition pairs the k-th element from the left that is not below the pivot with the k-th element
+// from the right that is not above it, swapping pairs until the two scans meet.  While the scanned regions
+// are a block apart, that pairing is computed here from 64-element bitmasks (no data-dependent branches);
+// the scalar loop then resumes right after the last swapped pair, exactly where it would have been.
+constexpr int64_t kBlockLen = 64;
+
+Pair *block_pairs(Pair *lo0, Pair *hi0, int32_t pv, Pair **hi_out) {
+    Pair *lf = lo0, *rf = hi0;      // next unscanned position from the left; scanned region from the right
+    Pair *last_l = nullptr, *last_r = nullptr;
+    uint64_t lm = 0, rm = 0;        // pending offenders: bit i = lbase + i;  bit j = rtop - 1 - j
+    Pair *lbase = lf, *rtop = rf;
+    for (;;) {
+        if (!lm) {
+            if (rf - lf < 2 * kBlockLen) break;
+            lbase = lf;
+            for (int i = 0; i < kBlockLen; ++i) lm |= (uint64_t)(lf[i].second >= pv) << i;
+            lf += kBlockLen;
+        }
+        if (!rm) {
+            if (rf - lf < kBlockLen) break;
+            rtop = rf;
+            for (int j = 0; j < kBlockLen; ++j) rm |= (uint64_t)(rf[-1 - j].second <= pv) << j;
+            rf -= kBlockLen;
+        }
+        while (lm && rm) {
+            Pair *x = lbase + __builtin_ctzll(lm), *y = rtop - 1 - __builtin_ctzll(rm);
+            std::swap(*x, *y);
+            last_l = x;
+            last_r = y;
+            lm &= lm - 1;
+            rm &= rm - 1;
+        }
+    }
+    *hi_out = last_r ? last_r : hi0;
+    return last_l ? last_l + 1 : lo0;
+}
+
 Pair *partition_around_front(Pair *first, Pair *last) {
     Pair *mid = first + (last - first) / 2;
     median_to_front(first, first + 1, mid, last - 1);
     const Pair *pivot = first;
     Pair *lo = first + 1, *hi = last;
+    if (last - first > 4 * kBlockLen) lo = block_pairs(first + 1, last, first->second, &hi);
     for (;;) {
         while (less(*lo, *pivot)) ++lo;
         --hi;
