@@ -141,7 +141,9 @@ Pair *partition_around_front(Pair *first, Pair *last) {
     }
 }
 
-void introsort_loop(Pair *first, Pair *last, int64_t depth) {
+// `spawn`: inside sort_by_degree's own parallel region, whose closing barrier waits for the tasks.  Anywhere
+// else (in particular inside a caller's parallel loop, where a task would outlive the call) it stays false.
+void introsort_loop(Pair *first, Pair *last, int64_t depth, bool spawn) {
     while (last - first > kSmall) {
         if (depth == 0) {
             heapsort(first, last - first);
@@ -149,11 +151,11 @@ void introsort_loop(Pair *first, Pair *last, int64_t depth) {
         }
         --depth;
         Pair *cut = partition_around_front(first, last);
-        if (last - cut >= kTaskMin) {
+        if (spawn && last - cut >= kTaskMin) {
 #pragma omp task firstprivate(cut, last, depth)
-            introsort_loop(cut, last, depth);
+            introsort_loop(cut, last, depth, true);
         } else {
-            introsort_loop(cut, last, depth);
+            introsort_loop(cut, last, depth, spawn);
         }
         last = cut;
     }
@@ -200,13 +202,13 @@ namespace dmolp {
 // The permutation std::sort(a, a + n, by degree) leaves, computed in parallel for large n.
 void sort_by_degree(Pair *a, int64_t n) {
     if (n <= 1) return;
-    const int T = n >= kParallelMin ? std::max(1, omp_get_max_threads()) : 1;
+    const int T = n >= kParallelMin && !omp_in_parallel() ? std::max(1, omp_get_max_threads()) : 1;
     if (T > 1) {
 #pragma omp parallel num_threads(T)
 #pragma omp single
-        introsort_loop(a, a + n, 2 * (int64_t)lg(n));
+        introsort_loop(a, a + n, 2 * (int64_t)lg(n), true);
     } else {
-        introsort_loop(a, a + n, 2 * (int64_t)lg(n));
+        introsort_loop(a, a + n, 2 * (int64_t)lg(n), false);
     }
     if (n <= kSmall) {
         guarded_insertion(a, a + n);

@@ -57,3 +57,50 @@ def test_hub_lists_match_the_oracle():
         assert core().dmolp_find_hubs_pairs(n, ids.ctypes.data, pair_deg.ctypes.data, h.ctypes.data,
                                             ctypes.byref(nh)) == cabi.DMOLP_OK
         assert np.array_equal(h[:nh.value], oracle.find_hubs(deg))
+
+
+NESTED = r"""
+#include <omp.h>
+#include <cstdio>
+#include <vector>
+#include <random>
+#include <algorithm>
+#include <cstdint>
+extern "C" int dmolp_degree_order(int64_t n, int32_t *ids, int32_t *degrees);
+int main() {
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : bad)
+    for (int g = 0; g < 48; ++g) {
+        std::mt19937_64 rng(g);
+        const int64_t n = 1000 + (int64_t)(rng() % 250000);
+        std::vector<int32_t> ids(n), deg(n);
+        for (int64_t i = 0; i < n; ++i) { ids[i] = (int32_t)(n - 1 - i); deg[i] = (int32_t)(rng() % 40); }
+        std::vector<std::pair<int, int>> p(n);
+        for (int64_t i = 0; i < n; ++i) p[i] = {ids[i], deg[i]};
+        std::sort(p.begin(), p.end(), [](const std::pair<int, int> &x, const std::pair<int, int> &y) {
+            return x.second < y.second; });
+        dmolp_degree_order(n, ids.data(), deg.data());
+        for (int64_t i = 0; i < n; ++i) bad += p[i].first != ids[i];
+    }
+    printf("%d\n", bad);
+    return 0;
+}
+"""
+
+
+def test_degree_order_inside_a_callers_parallel_loop(tmp_path):
+    """The batched phase 1 computes many graphs' hubs from inside its own OpenMP loop: the sort must neither
+    leave work behind (tasks outliving the call) nor differ from std::sort there."""
+    import os
+    import subprocess
+
+    from dmolp_b200 import build
+
+    src = tmp_path / "nested.cpp"
+    src.write_text(NESTED)
+    exe = tmp_path / "nested"
+    lib = os.path.join(build.LIB)
+    subprocess.run([build.CXX, "-O2", "-fopenmp", str(src), "-o", str(exe), "-L" + lib, "-ldmolp_b200",
+                    "-Wl,-rpath," + lib], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, timeout=300)
+    assert out.stdout.strip() == "0"
