@@ -70,6 +70,24 @@ __device__ __forceinline__ void zero_share(unsigned int *buf, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) buf[i] = 0;
 }
 
+// Adds a record's bin (or nothing: bin < 0, unique per lane) to the block's histogram, merging lanes of the
+// same bin with __match_any_sync.  All 32 lanes call it.
+__device__ __forceinline__ void hist_add(int bin, bool use_smem, unsigned int *shist, unsigned int *gh) {
+    const int lane = threadIdx.x & 31;
+    const unsigned m = __match_any_sync(DMOLP_FULL_MASK, bin);
+    if (bin >= 0 && lane == __ffs(m) - 1) {
+        if (use_smem) atomicAdd(&shist[bin], (unsigned)__popc(m));
+        else atomicAdd(&gh[bin], (unsigned)__popc(m));
+    }
+}
+
+__device__ __forceinline__ void hist_flush(bool use_smem, const unsigned int *shist, unsigned int *gh, int nbins) {
+    if (!use_smem) return;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x)
+        if (shist[i]) atomicAdd(&gh[i], shist[i]);
+}
+
 __global__ void __launch_bounds__(kSelThreads) k_select(SelArgs a) {
     if (a.stopped && *a.stopped) return;  // the same for every block: all return, no barrier is left open
     extern __shared__ unsigned int smem[];
@@ -81,49 +99,45 @@ __global__ void __launch_bounds__(kSelThreads) k_select(SelArgs a) {
     __shared__ int s_open, s_cnt;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int p = threadIdx.x; p < nseg; p += blockDim.x) s_need[p] = a.need[p];
+    if (use_smem)
+        for (int i = threadIdx.x; i < nbins; i += blockDim.x) shist[i] = 0;
     const int n0 = *a.n_dev;
     const int cap = (n0 + gridDim.x - 1) / gridDim.x;
     const int lo = blockIdx.x * cap;
     int my_n = max(0, min(n0, lo + cap) - lo);  // pass 0: record slots [lo, lo + my_n)
+    __syncthreads();
+    // ---- histogram of the first digit over this block's record slots ----
+    {
+        const int shift = a.top - kRadixBits;
+        for (int i0 = 0; i0 < my_n; i0 += blockDim.x) {
+            const int i = i0 + threadIdx.x;
+            int bin = -(lane + 1);  // unique non-bin value for idle lanes and empty slots
+            if (i < my_n) {
+                const int r = lo + i;
+                const int p = a.seg[r];
+                if (p >= 0 && s_need[p] > 0) bin = p * kRadix + (int)((a.key[r] >> shift) & (kRadix - 1));
+            }
+            hist_add(bin, use_smem, shist, a.ghist);
+        }
+        hist_flush(use_smem, shist, a.ghist, nbins);
+    }
     int pass = 0;
     for (; pass < a.npass; ++pass) {
         const int shift = a.top - kRadixBits * (pass + 1);
         const int32_t *src = pass ? (((pass - 1) & 1) ? a.act1 : a.act0) + lo : nullptr;
         int32_t *dst = ((pass & 1) ? a.act1 : a.act0) + lo;
         unsigned int *gh = a.ghist + (size_t)(pass % kSelHistBuffers) * nbins;
-        // ---- histogram of this block's records ----
-        if (use_smem) {
-            for (int i = threadIdx.x; i < nbins; i += blockDim.x) shist[i] = 0;
-        }
+        unsigned int *gh_next = a.ghist + (size_t)((pass + 1) % kSelHistBuffers) * nbins;
+        grid_sync(a.ctl);  // this pass's histogram is complete
+        if (pass > 0)      // read by every block in the previous pass, before the barrier just passed
+            zero_share(a.ghist + (size_t)((pass - 1) % kSelHistBuffers) * nbins, nbins);
         if (threadIdx.x == 0) {
             s_open = 0;
             s_cnt = 0;
         }
+        if (use_smem)  // the block's histogram of the next digit
+            for (int i = threadIdx.x; i < nbins; i += blockDim.x) shist[i] = 0;
         __syncthreads();
-        // Keys crowd into few bins (a digit of small degrees is mostly 0): lanes with the same bin are
-        // merged with __match_any_sync and add once.
-        for (int i0 = 0; i0 < my_n; i0 += blockDim.x) {
-            const int i = i0 + threadIdx.x;
-            int bin = -(lane + 1);  // unique non-bin value for idle lanes and empty slots
-            if (i < my_n) {
-                const int r = src ? src[i] : lo + i;
-                const int p = a.seg[r];
-                if (p >= 0 && s_need[p] > 0) bin = p * kRadix + (int)((a.key[r] >> shift) & (kRadix - 1));
-            }
-            const unsigned m = __match_any_sync(DMOLP_FULL_MASK, bin);
-            if (bin >= 0 && lane == __ffs(m) - 1) {
-                if (use_smem) atomicAdd(&shist[bin], (unsigned)__popc(m));
-                else atomicAdd(&gh[bin], (unsigned)__popc(m));
-            }
-        }
-        if (use_smem) {
-            __syncthreads();
-            for (int i = threadIdx.x; i < nbins; i += blockDim.x)
-                if (shist[i]) atomicAdd(&gh[i], shist[i]);
-        }
-        grid_sync(a.ctl);
-        if (pass > 0)  // read by every block in the previous pass, before the barrier just passed
-            zero_share(a.ghist + (size_t)((pass - 1) % kSelHistBuffers) * nbins, nbins);
         // ---- digit decisions, the same in every block ----
         for (int p = wid; p < nseg; p += nw) {
             const int nd = s_need[p];
@@ -177,19 +191,25 @@ __global__ void __launch_bounds__(kSelThreads) k_select(SelArgs a) {
             }
         }
         __syncthreads();
-        const bool more = s_open > 0;
-        // ---- partition of this block's records ----
+        const bool more = s_open > 0 && pass + 1 < a.npass;
+        const int shift_next = shift - kRadixBits;
+        // ---- partition of this block's records, and the next digit's histogram of the records kept ----
         for (int i0 = 0; i0 < my_n; i0 += blockDim.x) {
             const int i = i0 + threadIdx.x;
             bool keep = false;
-            int r = 0;
+            int r = 0, bin = -(lane + 1);
             if (i < my_n) {
                 r = src ? src[i] : lo + i;
                 const int p = a.seg[r];
                 if (p >= 0) {  // skip empty record slots
-                    const int d = (int)((a.key[r] >> shift) & (kRadix - 1));
-                    if (d < s_below[p]) a.sel[r] = 1;
-                    else keep = more && d == s_keep[p];
+                    const uint64_t key = a.key[r];
+                    const int d = (int)((key >> shift) & (kRadix - 1));
+                    if (d < s_below[p]) {
+                        a.sel[r] = 1;
+                    } else if (more && d == s_keep[p]) {
+                        keep = true;
+                        bin = p * kRadix + (int)((key >> shift_next) & (kRadix - 1));
+                    }
                 }
             }
             const unsigned m = __ballot_sync(DMOLP_FULL_MASK, keep);
@@ -198,7 +218,9 @@ __global__ void __launch_bounds__(kSelThreads) k_select(SelArgs a) {
             if (m && lane == leader) base = atomicAdd(&s_cnt, __popc(m));
             base = __shfl_sync(DMOLP_FULL_MASK, base, leader);
             if (keep) dst[base + __popc(m & ((1u << lane) - 1))] = r;
+            if (more) hist_add(bin, use_smem, shist, gh_next);
         }
+        if (more) hist_flush(use_smem, shist, gh_next, nbins);
         __syncthreads();
         my_n = s_cnt;
         __syncthreads();  // every thread has read s_cnt before the next pass resets it
