@@ -85,6 +85,7 @@ struct DecodeWork {
     int32_t *l0, *l1;  // [nv] each
     int32_t *status;   // [ninst]
     int *next;
+    const uint8_t *skip;  // [ninst] or null: graphs left alone (status 2, labels untouched)
 };
 void decode(const DecodeWork &w, int grid, cudaStream_t s);
 void coords(const float *Xf, const float *Z, int nv, float *P, int num_sms, cudaStream_t s);

@@ -64,6 +64,7 @@ struct dmolp_mpnn {
     int32_t *vinst = nullptr, *dist = nullptr, *mind = nullptr, *f0 = nullptr, *f1 = nullptr, *cnt = nullptr;
     unsigned long long *akey = nullptr;
     int32_t *anchor = nullptr, *ecc = nullptr, *status = nullptr, *target = nullptr, *dl0 = nullptr, *dl1 = nullptr;
+    uint8_t *skip = nullptr;  // [ninst] graphs the decoder leaves to phase 1
     int *next = nullptr;
     float *P0 = nullptr, *Q0 = nullptr, *P1 = nullptr, *Q1 = nullptr;
     double *stats = nullptr, *gscore = nullptr;
@@ -123,6 +124,7 @@ int ensure_ws(dmolp_mpnn *m, const batch::View &b, bool train) {
     MTRY(alloc_into(o, &m->anchor, (size_t)kAnchors * b.ninst));
     MTRY(alloc_into(o, &m->ecc, b.ninst));
     MTRY(alloc_into(o, &m->status, b.ninst));
+    MTRY(alloc_into(o, &m->skip, b.ninst));
     MTRY(alloc_into(o, &m->stats, (size_t)16 * b.ninst));
     MTRY(alloc_into(o, &m->gscore, b.ninst));
     MTRY(alloc_into(o, &m->ggrad, b.ninst));
@@ -421,7 +423,9 @@ int dmolp_mpnn_train_step(dmolp_mpnn *m, dmolp_batch *b, const int32_t *target, 
     return DMOLP_OK;
 }
 
-int dmolp_mpnn_decode(dmolp_mpnn *m, dmolp_batch *b, const float *embedding, int32_t *status) {
+// Decoder over the batch; graphs marked in skip_host (may be null) keep their labels and get status 2.
+static int decode_impl(dmolp_mpnn *m, dmolp_batch *b, const float *embedding, const uint8_t *skip_host,
+                       int32_t *status) {
     batch::View v;
     MTRY(get_view(m, b, &v));
     if (m->cap_nv < v.nv) return fail(DMOLP_ERR_STATE, "no workspace for this batch");
@@ -441,9 +445,18 @@ int dmolp_mpnn_decode(dmolp_mpnn *m, dmolp_batch *b, const float *embedding, int
     w.l1 = m->dl1;
     w.status = m->status;
     w.next = m->next;
+    w.skip = nullptr;
+    if (skip_host) {
+        MCUDA(cudaMemcpyAsync(m->skip, skip_host, v.ninst, cudaMemcpyHostToDevice, v.stream));
+        w.skip = m->skip;
+    }
     decode(w, std::max(1, std::min(v.ninst, v.num_sms * 2)), v.stream);
     if (status) MCUDA(cudaMemcpyAsync(status, m->status, v.ninst * sizeof(int32_t), cudaMemcpyDeviceToHost, v.stream));
     return sync_check(m, v.stream, "decode");
+}
+
+int dmolp_mpnn_decode(dmolp_mpnn *m, dmolp_batch *b, const float *embedding, int32_t *status) {
+    return decode_impl(m, b, embedding, nullptr, status);
 }
 
 int dmolp_mpnn_gate(dmolp_mpnn *m, dmolp_batch *b, double *scores) {
@@ -503,10 +516,11 @@ int dmolp_batch_propose(dmolp_batch *b, dmolp_mpnn *m, int32_t *status) {
     MTRY(get_view(m, b, &v));
     std::vector<double> sc(v.ninst);
     MTRY(dmolp_mpnn_gate(m, b, sc.data()));
+    // only the graphs the gate accepts are decoded; the others keep their labels for phase 1 (status 2)
+    std::vector<uint8_t> skip(v.ninst);
+    for (int i = 0; i < v.ninst; ++i) skip[i] = sc[i] < 0.0;
     std::vector<int32_t> st(v.ninst);
-    MTRY(dmolp_mpnn_decode(m, b, nullptr, st.data()));
-    for (int i = 0; i < v.ninst; ++i)
-        if (st[i] == 0 && sc[i] < 0.0) st[i] = 2;  // the gate prefers phase-1 seeding for this graph
+    MTRY(decode_impl(m, b, nullptr, skip.data(), st.data()));
     if (status) std::memcpy(status, st.data(), v.ninst * sizeof(int32_t));
     return DMOLP_OK;
 }

@@ -376,17 +376,30 @@ __global__ void k_fill_i32(int32_t *p, int n, int32_t x) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = x;
 }
 
-// One BFS level: unvisited neighbours of the frontier get level + 1.
+// One BFS level: unvisited neighbours of the frontier get level + 1.  The frontier counts rotate over three
+// counters: level L reads cnt[L%3], appends to cnt[(L+1)%3] and clears cnt[(L+2)%3], the count the next
+// level appends to (nothing reads it now), so levels run back to back with no host work in between; a level
+// after the frontier has emptied does nothing.
 __global__ void k_bfs_level(const int64_t *__restrict__ off, const int32_t *__restrict__ col, int32_t *dist,
-                            const int32_t *fin, const int *nin, int32_t *fout, int *nout, int level) {
-    const int n = *nin;
+                            const int32_t *fin, int32_t *fout, int *cnt, int level) {
+    const int n = cnt[level % 3];
+    int *nout = cnt + (level + 1) % 3;
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt[(level + 2) % 3] = 0;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     for (int i = gw; i < n; i += nw) {
         const int v = fin[i];
-        for (int64_t j = off[v] + lane; j < off[v + 1]; j += 32) {
-            const int u = __ldg(col + j);
-            if (dist[u] < 0 && atomicCAS(&dist[u], -1, level + 1) == -1) fout[atomicAdd(nout, 1)] = u;
+        const int64_t s = off[v], e = off[v + 1];
+        for (int64_t j0 = s; j0 < e; j0 += 32) {  // warp-uniform trip count: one append per warp and step
+            const int64_t j = j0 + lane;
+            int u = 0;
+            bool found = false;
+            if (j < e) {
+                u = __ldg(col + j);
+                found = dist[u] < 0 && atomicCAS(&dist[u], -1, level + 1) == -1;
+            }
+            const int slot = warp_append(nout, found);
+            if (found) fout[slot] = u;
         }
     }
 }
@@ -436,15 +449,8 @@ __global__ void k_rw_step(const FeatWork w, const float *Pin, const float *Qin, 
         const int i = w.vinst[v];
         const int T = min(max(w.ecc[i], 1), kTMax);
         const float4 *pi = reinterpret_cast<const float4 *>(Pin + (size_t)v * 8);
-        const float4 *qi = reinterpret_cast<const float4 *>(Qin + (size_t)v * 8);
         float4 *po = reinterpret_cast<float4 *>(Pout + (size_t)v * 8), *qo = reinterpret_cast<float4 *>(Qout + (size_t)v * 8);
-        if (step >= T) {
-            po[0] = pi[0];
-            po[1] = pi[1];
-            qo[0] = qi[0];
-            qo[1] = qi[1];
-            continue;
-        }
+        if (step >= T) continue;  // the graph has walked its T steps: its result stays in the buffer of step T-1
         float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         const int64_t b = w.off[v], e = w.off[v + 1];
         for (int64_t j = b; j < e; ++j) {
@@ -476,8 +482,9 @@ __global__ void k_rw_step(const FeatWork w, const float *Pin, const float *Qin, 
     }
 }
 
-// log landing probabilities, their per-graph sums and sums of squares (double).
-__global__ void k_rw_log(const FeatWork w, const float *P) {
+// log landing probabilities, their per-graph sums and sums of squares (double).  A graph that walked T steps
+// left its probabilities in P0 (T even) or P1 (T odd): steps alternate the two buffers.
+__global__ void k_rw_log(const FeatWork w) {
     const int lane = threadIdx.x & 31;
     for (int v0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); v0 < w.nv; v0 += gridDim.x * blockDim.x) {
         const int v = v0 + lane;
@@ -487,6 +494,7 @@ __global__ void k_rw_log(const FeatWork w, const float *P) {
         for (int j = 0; j < 8; ++j) {
             double a = 0.0, b = 0.0;
             if (v < w.nv) {
+                const float *P = (min(max(w.ecc[i], 1), kTMax) & 1) ? w.P1 : w.P0;
                 const float L = logf(fmaxf(P[(size_t)v * 8 + j], kPFloor));
                 w.Xf[(size_t)v * 16 + 2 + j] = L;
                 a = (double)L;
@@ -650,6 +658,11 @@ __global__ void __launch_bounds__(kDecThreads) k_decode(DecodeWork w) {
         const int q = sm.inst;
         if (q >= w.ninst) break;
         const int ii = w.order[q];
+        if (w.skip && w.skip[ii]) {  // the gate prefers phase-1 seeding: nothing to decode
+            if (threadIdx.x == 0) w.status[ii] = 2;
+            __syncthreads();
+            continue;
+        }
         const batch::Inst I = w.inst[ii];
         const int k = I.k, nv = I.nv, vb = (int)I.vbase;
         for (int p = threadIdx.x; p < 64; p += blockDim.x) sm.kp[p] = 0;
@@ -989,6 +1002,8 @@ void cast_weights(const float *params, __nv_bfloat16 *const W[3], __nv_bfloat16 
     k_cast<<<32, 256, 0, s>>>(params, W[0], W[1], W[2], Wt[0], Wt[1], Wt[2]);
 }
 
+constexpr int kBfsChunk = 64;  // BFS levels launched between two looks at the frontier size
+
 int features(const FeatWork &w, int num_sms, cudaStream_t s) {
     const int g = grid_for(w.nv, num_sms);
     k_vinst<<<g, 256, 0, s>>>(w.inst, w.ninst, w.nv, w.vinst);
@@ -1001,19 +1016,17 @@ int features(const FeatWork &w, int num_sms, cudaStream_t s) {
         k_fill_i32<<<g, 256, 0, s>>>(w.dist, w.nv, -1);
         cudaMemsetAsync(w.cnt, 0, 4 * sizeof(int), s);
         k_anchor_pick<<<(w.ninst + 255) / 256, 256, 0, s>>>(w, j);
-        int32_t *fin = w.front0, *fout = w.front1;
-        int *nin = w.cnt, *nout = w.cnt + 1;
-        for (int level = 0;; ++level) {
+        // levels in chunks of kBfsChunk launches; the host looks at the frontier once per chunk
+        const int gb = num_sms * 16;
+        for (int level = 0;; level += kBfsChunk) {
+            for (int l = level; l < level + kBfsChunk; ++l)
+                k_bfs_level<<<gb, 256, 0, s>>>(w.off, w.col, w.dist, (l & 1) ? w.front1 : w.front0,
+                                               (l & 1) ? w.front0 : w.front1, w.cnt, l);
             int h = 0;
-            cudaMemcpyAsync(&h, nin, sizeof(int), cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(&h, w.cnt + (level + kBfsChunk) % 3, sizeof(int), cudaMemcpyDeviceToHost, s);
             cudaError_t e = cudaStreamSynchronize(s);
             if (e != cudaSuccess) return (int)e;
             if (h == 0) break;
-            cudaMemsetAsync(nout, 0, sizeof(int), s);
-            k_bfs_level<<<grid_for((int64_t)h * 32, num_sms), 256, 0, s>>>(w.off, w.col, w.dist, fin, nin, fout, nout,
-                                                                           level);
-            std::swap(fin, fout);
-            std::swap(nin, nout);
         }
         k_mind<<<g, 256, 0, s>>>(w, j);
     }
@@ -1032,7 +1045,7 @@ int features(const FeatWork &w, int num_sms, cudaStream_t s) {
         std::swap(P, P2);
         std::swap(Q, Q2);
     }
-    k_rw_log<<<g, 256, 0, s>>>(w, P);
+    k_rw_log<<<g, 256, 0, s>>>(w);
     k_feat_final<<<g, 256, 0, s>>>(w);
     if (w.X) k_to_input<<<g, 256, 0, s>>>(w.Xf, w.nv, w.X, w.ldx);
     return (int)cudaGetLastError();
