@@ -17,8 +17,22 @@ std::vector<int> hubs_from_pairs(std::vector<std::pair<int, int>> sd);
 // whose top bit is below `keybits`; keys are unique.  For every segment p, marks sel[i] = 1 on the need[p] records with the
 // smallest keys (need[] is consumed).  sel[] must be zero on entry.  `stopped` (may be null) turns the
 // launches into no-ops once it is non-zero.
+// The LP window straight out of the selection: each selected record slot i (vertex vertex[i], segment = its
+// label) is stamped sstamp[v] = t, appended to win / nwin and to its decision-class list dec[c] / ndec[c],
+// and its degree added to *te.
+struct SplitArgs {
+    const int32_t *vertex;
+    const int64_t *off;
+    int32_t *sstamp;
+    int32_t *win;
+    int *nwin;
+    int32_t *dec[3];
+    int *ndec;
+    unsigned long long *te;
+    int t, eff;
+};
 void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, const int *n_dev, int nseg, int keybits,
-                     uint8_t *sel, const int *stopped);
+                     uint8_t *sel, const int *stopped, const SplitArgs *split = nullptr);
 void select_prepare();  // kernel attributes; call once before any capture
 
 // ---- LP loop (lp_kernels.cu) ----

@@ -7,6 +7,14 @@
 
 namespace dmolp {
 
+// Decision class of a selected vertex: 0 thread (short row, own label scored, at most kDecSmallK labels),
+// 1 warp, 2 hub (row split into chunks).  A vertex whose own label is not scored goes to the warp class,
+// whose histogram also sees absent labels.
+__device__ __forceinline__ int dec_class(int deg, int own, int eff) {
+    if (deg > kLargeDeg) return 2;
+    return (deg > kDecSmall || (unsigned)own >= (unsigned)eff || eff > kDecSmallK) ? 1 : 0;
+}
+
 __device__ __forceinline__ int tiekey(int c) { return (c & ~31) | (int)brev5((unsigned)c & 31u); }
 
 __device__ __forceinline__ long long sll(unsigned long long x) { return (long long)x; }

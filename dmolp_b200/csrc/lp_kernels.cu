@@ -276,44 +276,6 @@ __device__ __forceinline__ int block_append(int *gctr, bool pred, int *s_tmp) {
     return pred ? s_tmp[1] + wb + __popc(m & ((1u << lane) - 1)) : -1;
 }
 
-// Decision class of a selected vertex: 0 thread (short row, own label scored, at most kDecSmallK labels),
-// 1 warp, 2 hub (row split into chunks).  A vertex whose own label is not scored goes to the warp class,
-// whose histogram also sees absent labels.
-__device__ __forceinline__ int dec_class(int deg, int own, int eff) {
-    if (deg > kLargeDeg) return 2;
-    return (deg > kDecSmall || (unsigned)own >= (unsigned)eff || eff > kDecSmallK) ? 1 : 0;
-}
-
-// Selected record slots: next window (for marking) and decision class.  A vertex whose own label is not
-// scored (>= eff) goes to the warp class, whose histogram also sees absent labels.
-__global__ void __launch_bounds__(256) k_split(Buffers b, int t, int eff) {
-    if (b.ctrl->stopped) return;
-    __shared__ int s_tmp[2];
-    const int n = b.cnt->npos;
-    int32_t *win = b.win[t & 1];
-    unsigned long long te = 0;
-    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
-        const int i = i0 + threadIdx.x;
-        const bool take = i < n && b.bsel[i];
-        int v = 0, cls = -1;
-        if (take) {
-            v = b.ball[i];
-            b.sstamp[v] = t;
-            const int deg = (int)(b.off[v + 1] - b.off[v]);
-            te += (unsigned long long)deg;
-            cls = dec_class(deg, b.bown[i], eff);
-        }
-        const int slot = block_append(&b.cnt->nwin[t & 1], take, s_tmp);
-        if (take) win[slot] = v;
-        for (int c = 0; c < 3; ++c) {
-            const int s2 = block_append(&b.cnt->ndec[c], cls == c, s_tmp);
-            if (cls == c) b.dec[c][s2] = v;
-        }
-    }
-    te = warp_sum_u64(te);
-    if ((threadIdx.x & 31) == 0 && te) atomicAdd(&b.rec[t - 1].te_sel, te);
-}
-
 // ------------------------------------------------------------------------------------ decide
 struct DecArgs {
     int t, eff;
@@ -1004,6 +966,22 @@ void lp_init_end(dmolp_ctx *c, int mode) {
     c->launches++;
 }
 
+// The window of iteration t as the selection emits it (see SplitArgs).
+SplitArgs split_args(const Buffers &b, int t, int eff) {
+    SplitArgs sp;
+    sp.vertex = b.ball;
+    sp.off = b.off;
+    sp.sstamp = b.sstamp;
+    sp.win = b.win[t & 1];
+    sp.nwin = &b.cnt->nwin[t & 1];
+    for (int c = 0; c < 3; ++c) sp.dec[c] = b.dec[c];
+    sp.ndec = b.cnt->ndec;
+    sp.te = &b.rec[t - 1].te_sel;
+    sp.t = t;
+    sp.eff = eff;
+    return sp;
+}
+
 void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     Buffers &b = c->b;
     const int grid = grid_for(c);
@@ -1025,9 +1003,9 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     c->launches += 2;
     {
         ProfScope ps(c, 4, t);
-        select_smallest(c, b.bown, b.bkey, &b.cnt->npos, L.k, c->dbits + c->ibits, b.bsel, stopped);
+        const SplitArgs sp = split_args(b, t, L.eff);
+        select_smallest(c, b.bown, b.bkey, &b.cnt->npos, L.k, c->dbits + c->ibits, b.bsel, stopped, &sp);
     }
-    k_split<<<grid, kBlock, 0, c->stream>>>(b, t, L.eff);
     {
         ProfScope ps(c, 1, t);
         launch_decide(c, t, L.eff);
@@ -1064,9 +1042,8 @@ void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int n
     k_bnd<<<bnd_grid(c, a), kBlock, k * sizeof(int), c->stream>>>(b, a, k);
     k_lp_need<<<1, 256, 0, c->stream>>>(b, k, t);
     c->launches += 5;
-    select_smallest(c, b.bown, b.bkey, &b.cnt->npos, k, c->dbits + c->ibits, b.bsel, nullptr);
-    k_split<<<grid, kBlock, 0, c->stream>>>(b, t, DMOLP_MAX_K);
-    c->launches += 1;
+    const SplitArgs sp = split_args(b, t, DMOLP_MAX_K);
+    select_smallest(c, b.bown, b.bkey, &b.cnt->npos, k, c->dbits + c->ibits, b.bsel, nullptr, &sp);
 }
 
 // dmolp_lp_apply: window in b.cand (n entries), penalties in b.tpen; movers reported in bv/bnew.

@@ -19,6 +19,7 @@
 // degree, then id).
 #include "../../include/dmolp_b200.h"
 #include "kernels.cuh"
+#include "lp_device.cuh"
 
 namespace dmolp {
 namespace {
@@ -38,6 +39,8 @@ struct SelArgs {
     uint8_t *sel;
     LpControl *ctl;
     const int *stopped;
+    SplitArgs sp;  // used when has_split: selected slots go straight to the LP window
+    int has_split;
 };
 
 // Sense-counting grid barrier (all blocks are resident: cooperative launch).  A wait that runs past
@@ -88,7 +91,7 @@ __device__ __forceinline__ void hist_flush(bool use_smem, const unsigned int *sh
         if (shist[i]) atomicAdd(&gh[i], shist[i]);
 }
 
-__global__ void __launch_bounds__(kSelThreads) k_select(SelArgs a) {
+__global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
     if (a.stopped && *a.stopped) return;  // the same for every block: all return, no barrier is left open
     extern __shared__ unsigned int smem[];
     const int nseg = a.nseg, nbins = nseg * kRadix;
@@ -121,6 +124,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select(SelArgs a) {
         }
         hist_flush(use_smem, shist, a.ghist, nbins);
     }
+    unsigned long long te = 0;  // degrees of the selected vertices (has_split)
     int pass = 0;
     for (; pass < a.npass; ++pass) {
         const int shift = a.top - kRadixBits * (pass + 1);
@@ -196,16 +200,17 @@ __global__ void __launch_bounds__(kSelThreads) k_select(SelArgs a) {
         // ---- partition of this block's records, and the next digit's histogram of the records kept ----
         for (int i0 = 0; i0 < my_n; i0 += blockDim.x) {
             const int i = i0 + threadIdx.x;
-            bool keep = false;
-            int r = 0, bin = -(lane + 1);
+            bool keep = false, take = false;
+            int r = 0, bin = -(lane + 1), p = -1;
             if (i < my_n) {
                 r = src ? src[i] : lo + i;
-                const int p = a.seg[r];
+                p = a.seg[r];
                 if (p >= 0) {  // skip empty record slots
                     const uint64_t key = a.key[r];
                     const int d = (int)((key >> shift) & (kRadix - 1));
                     if (d < s_below[p]) {
                         a.sel[r] = 1;
+                        take = true;
                     } else if (more && d == s_keep[p]) {
                         keep = true;
                         bin = p * kRadix + (int)((key >> shift_next) & (kRadix - 1));
@@ -219,12 +224,33 @@ __global__ void __launch_bounds__(kSelThreads) k_select(SelArgs a) {
             base = __shfl_sync(DMOLP_FULL_MASK, base, leader);
             if (keep) dst[base + __popc(m & ((1u << lane) - 1))] = r;
             if (more) hist_add(bin, use_smem, shist, gh_next);
+            if (a.has_split) {  // the LP window: stamp, append, decision class (all lanes take part)
+                int v = 0, cls = -1;
+                if (take) {
+                    v = a.sp.vertex[r];
+                    a.sp.sstamp[v] = a.sp.t;
+                    const int deg = (int)(a.sp.off[v + 1] - a.sp.off[v]);
+                    te += (unsigned long long)deg;
+                    cls = dec_class(deg, p, a.sp.eff);
+                }
+                const int slot = warp_append(a.sp.nwin, take);
+                if (take) a.sp.win[slot] = v;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int s2 = warp_append(&a.sp.ndec[c], cls == c);
+                    if (cls == c) a.sp.dec[c][s2] = v;
+                }
+            }
         }
         if (more) hist_flush(use_smem, shist, gh_next, nbins);
         __syncthreads();
         my_n = s_cnt;
         __syncthreads();  // every thread has read s_cnt before the next pass resets it
         if (!more) break;
+    }
+    if (a.has_split) {
+        te = warp_sum_u64(te);
+        if (lane == 0 && te) atomicAdd(a.sp.te, te);
     }
     // the last pass's histogram is still set: clear it once every block has read it
     grid_sync(a.ctl);
@@ -234,7 +260,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select(SelArgs a) {
 }  // namespace
 
 void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, const int *n_dev, int nseg, int keybits,
-                     uint8_t *sel, const int *stopped) {
+                     uint8_t *sel, const int *stopped, const SplitArgs *split) {
     const int npass = (keybits + kRadixBits - 1) / kRadixBits;
     const bool smem_hist = nseg <= kSmemSegMax;
     const size_t smem = (smem_hist ? (size_t)nseg * kRadix * sizeof(unsigned int) : 0) + 3 * (size_t)nseg * sizeof(int);
@@ -252,6 +278,8 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
     a.sel = sel;
     a.ctl = c->b.ctrl;
     a.stopped = stopped;
+    a.has_split = split != nullptr;
+    if (split) a.sp = *split;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)c->num_sms);  // one block per SM, all resident (cooperative launch)
     cfg.blockDim = dim3(kSelThreads);
