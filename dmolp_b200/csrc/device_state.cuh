@@ -35,6 +35,7 @@ struct LpCounters {
     int nhubq;        // queued row chunks of the hub decisions
     int npos;         // selection record slots: one per vertex with arcs (fixed per graph)
     unsigned long long cut_arcs;   // arcs whose endpoint labels differ (kept current incrementally)
+    int dgrab[3];     // decisions: work items taken so far per class (thread groups, warp groups, hub chunks)
 };
 
 // Loop control shared by the iteration kernels.
@@ -87,7 +88,10 @@ struct Buffers {
     int32_t *mov = nullptr;    // [nv] movers of the current iteration
     int2 *chunkq = nullptr;    // [chunk_cap] (vertex, first arc) of queued row chunks
     int2 *hubq = nullptr;      // [hubq_cap] (hub index, first arc) of queued hub-decision chunks
-    int32_t *hh = nullptr;     // [nb[2] * MAX_K] per-hub label counts of the current decisions
+    int32_t *hh = nullptr;     // [nb[2] * MAX_K] per-hub label counts, row = hub index: recounted for the
+                               // selected hubs each iteration, or (symmetric graphs) counted once per LP run
+                               // and kept current from the movers' arcs
+    int32_t *hidx = nullptr;   // [nv] hub index (position in bucket[2]) of a vertex with deg > kLargeDeg, else -1
     int32_t *active[2] = {nullptr, nullptr};  // [nv] radix-select active lists
     // per-part arrays (DMOLP_MAX_K); vc / intra hold signed values in two's complement
     unsigned int *hist = nullptr;        // [MAX_K * 256]

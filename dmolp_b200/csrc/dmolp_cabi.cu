@@ -280,6 +280,7 @@ size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t 
     ALLOC(b.chunkq, (size_t)c->chunk_cap);
     ALLOC(b.hubq, (size_t)c->hubq_cap);
     ALLOC(b.hh, nball[2] * (size_t)DMOLP_MAX_K);
+    ALLOC(b.hidx, n);
 #undef ALLOC
     return off;
 }
@@ -334,6 +335,7 @@ int graph_finish(dmolp_ctx *c, bool rows_sorted) {
     DMOLP_CUDA(cudaMemcpyAsync(&b.cnt->npos, &npos, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.bown, 0xff, n * sizeof(int32_t), c->stream));  // all record slots empty
     lp_fill(c, b.newlab, (int64_t)n, -1);
+    lp_hub_index(c);
     select_prepare();
     // whether every arc has its reverse is tested when the LP loop first needs it (ensure_symmetry)
     c->symmetric = false;
@@ -1070,6 +1072,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     DMOLP_CUDA(cudaMemsetAsync(b.ndiff, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
     lp_reset_stats(c, k, nullptr);
     lp_stats(c, k, nullptr, nullptr);
+    if (c->symmetric) lp_hub_counts(c, L.eff);
     lp_init_end(c, cfg->mode);
     int st = check_launch(c);
     if (st) return st;

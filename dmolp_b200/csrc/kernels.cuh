@@ -46,6 +46,10 @@ void lp_fill(dmolp_ctx *c, int32_t *p, int64_t n, int32_t v);
 void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped);
 void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip);
 void lp_init_end(dmolp_ctx *c, int mode);
+void lp_hub_index(dmolp_ctx *c);            // b.hidx from bucket[2] (once per graph)
+void lp_hub_counts(dmolp_ctx *c, int eff);  // label counts of every hub's row into b.hh (run start, symmetric)
+// One LP iteration.  On symmetric graphs the hub decisions read b.hh as lp_hub_counts left it and k_update
+// keeps it current; otherwise the selected hubs' rows are recounted.
 void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t);
 // one-off pieces used by dmolp_window_select / dmolp_lp_apply
 void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int nprev);

@@ -48,6 +48,7 @@ __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
         cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
         cn->nchunk = 0;
         cn->nhubq = 0;
+        cn->dgrab[0] = cn->dgrab[1] = cn->dgrab[2] = 0;
         ctl->stop_now = 0;
         ctl->skip_stats = 0;
         LpRecordDev &r = b.rec[t - 1];
@@ -258,28 +259,10 @@ __global__ void k_lp_need(Buffers b, int k, int t) {
     }
 }
 
-// ------------------------------------------------------------------------------------ split
-// Append under a predicate with one global atomic per block: every thread of the block must call it with
-// the same trip count.  s_tmp: two shared ints.
-__device__ __forceinline__ int block_append(int *gctr, bool pred, int *s_tmp) {
-    __syncthreads();
-    if (threadIdx.x == 0) s_tmp[0] = 0;
-    __syncthreads();
-    const unsigned m = __ballot_sync(DMOLP_FULL_MASK, pred);
-    const int lane = threadIdx.x & 31;
-    int wb = 0;
-    if (lane == 0 && m) wb = atomicAdd(&s_tmp[0], __popc(m));
-    wb = __shfl_sync(DMOLP_FULL_MASK, wb, 0);
-    __syncthreads();
-    if (threadIdx.x == 0) s_tmp[1] = s_tmp[0] ? atomicAdd(gctr, s_tmp[0]) : 0;
-    __syncthreads();
-    return pred ? s_tmp[1] + wb + __popc(m & ((1u << lane) - 1)) : -1;
-}
-
 // ------------------------------------------------------------------------------------ decide
 struct DecArgs {
     int t, eff;
-    int g0, g1;  // block split as in BndArgs
+    int wstride;  // shared ints per warp: lane-private counters (eff <= 32), histogram, or byte counters
 };
 
 __device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
@@ -288,46 +271,190 @@ __device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
     b.mov[q] = v;
 }
 
-__global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
+// Work distribution of k_decide: lane 0 takes the next item of a class with one atomic; the result is
+// broadcast only when the warp needs it, so the atomic's latency overlaps the current item.
+__device__ __forceinline__ int grab_issue(int *ctr, int lane) { return lane == 0 ? atomicAdd(ctr, 1) : 0; }
+__device__ __forceinline__ int grab_take(int pending) { return __shfl_sync(DMOLP_FULL_MASK, pending, 0); }
+
+// Lane-private label counts (eff <= 32) of the arcs [s, e): a step loads, per lane, the row's scalar head
+// and tail (first step only) and two 16-byte words of its body, then gathers all their labels, then counts,
+// so a row of up to 262 arcs costs one dependent load pair.
+__device__ __forceinline__ void count_priv(const int32_t *__restrict__ col, const int32_t *__restrict__ label,
+                                           int64_t s, int64_t e, int lane, int eff, int *h) {
+    int64_t a = (s + 3) & ~int64_t(3);
+    if (a > e) a = e;
+    const int64_t qe = e >> 2;  // body: int4 words [a/4, e/4)
+    const int64_t t0 = a > (qe << 2) ? a : (qe << 2);
+    const int4 *c4 = reinterpret_cast<const int4 *>(col);
+    bool first = true;
+    for (int64_t q0 = a >> 2; first || q0 < qe; q0 += 64) {
+        int u[10];
+        u[8] = first && s + lane < a ? __ldg(col + s + lane) : -1;
+        u[9] = first && t0 + lane < e ? __ldg(col + t0 + lane) : -1;
+        const int64_t q = q0 + lane;
+        int4 x = make_int4(-1, -1, -1, -1), y = make_int4(-1, -1, -1, -1);
+        if (q < qe) x = __ldcs(c4 + q);
+        if (q + 32 < qe) y = __ldcs(c4 + q + 32);
+        u[0] = x.x; u[1] = x.y; u[2] = x.z; u[3] = x.w;
+        u[4] = y.x; u[5] = y.y; u[6] = y.z; u[7] = y.w;
+        int l[10];
+#pragma unroll
+        for (int r = 0; r < 10; ++r) l[r] = u[r] >= 0 ? label[u[r]] : -1;
+#pragma unroll
+        for (int r = 0; r < 10; ++r)
+            if ((unsigned)l[r] < (unsigned)eff) h[l[r] * 32 + ((lane + l[r]) & 31)] += 1;
+        first = false;
+    }
+}
+
+// Label counts of the arcs [s, e) into the warp's region: lane-private counters (eff <= 32) or a shared
+// histogram of eff ints (warp_count's match-aggregated atomics).
+__device__ __forceinline__ void count_row(const Buffers &b, int64_t s, int64_t e, int lane, int eff, int *h) {
+    if (eff <= 32) {
+        priv_zero(h, eff, lane);
+        __syncwarp();
+        count_priv(b.col, b.label, s, e, lane, eff, h);
+    } else {
+        for (int c = lane; c < eff; c += 32) h[c] = 0;
+        __syncwarp();
+        warp_count(b.col, b.label, s, e, lane, eff, h);
+    }
+    __syncwarp();
+}
+
+// Hub rows (deg > kLargeDeg) in queued chunks of kHubChunk arcs, (list position, first arc) in b.hubq:
+// warp per chunk, its label counts added to the hub's row of b.hh.
+__device__ __forceinline__ void hub_chunks(const Buffers &b, const int32_t *list, int eff, int lane, int *h,
+                                           unsigned long long &rd) {
+    LpCounters *cn = b.cnt;
+    const int n = cn->nhubq;
+    int pend = grab_issue(&cn->dgrab[2], lane);
+    for (;;) {
+        const int q = grab_take(pend);
+        if (q >= n) break;
+        pend = grab_issue(&cn->dgrab[2], lane);
+        const int2 ch = b.hubq[q];
+        const int v = list[ch.x];
+        const int64_t s = b.off[v] + ch.y, rowe = b.off[v + 1];
+        const int64_t e = rowe - s > kHubChunk ? s + kHubChunk : rowe;
+        count_row(b, s, e, lane, eff, h);
+        int32_t *row = b.hh + (size_t)b.hidx[v] * DMOLP_MAX_K;
+        if (eff <= 32) {
+            const int cnt = priv_total(h, eff, lane);
+            if (cnt) atomicAdd(&row[lane], cnt);
+        } else {
+            for (int c = lane; c < eff; c += 32)
+                if (h[c]) atomicAdd(&row[c], h[c]);
+        }
+        if (lane == 0) rd += (unsigned long long)(e - s);
+        __syncwarp();
+    }
+}
+
+// Persistent warps take the selected window's work largest items first: hub row chunks (none queued when
+// the hub counts are kept current), then groups of warp-class vertices (metadata of the group loaded by
+// its lanes in one step), then groups of 32 thread-class vertices (lane per vertex).
+__global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
     if (b.ctrl->stopped) return;
-    extern __shared__ int shist[];  // eff <= 32: 8 warps x 32x32 private counters + 8x32 totals; else 8 x eff
+    extern __shared__ int shist[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int eff = a.eff;
     const bool priv = eff <= 32;
-    int *h = shist + wib * (priv ? 1024 : eff);
+    int *h = shist + wib * a.wstride;
+    LpCounters *cn = b.cnt;
     unsigned long long rd = 0;
-    if ((int)blockIdx.x < a.g0) {
-        // ---- thread per vertex: deg <= kDecSmall, own label scored, eff <= kDecSmallK.  Label counts are
-        //      bytes in this thread's column of shared memory (word w of thread t at shist[w * 256 + t]: four
-        //      labels per word, conflict-free); a 64-bit mask lists the labels seen, and only those are scored
-        //      -- an absent label scores 0 <= count[own] and cannot win ----
-        uint32_t *cw = reinterpret_cast<uint32_t *>(shist) + threadIdx.x;
-        for (int w = 0; w < kDecSmallK / 4; ++w) cw[w * kBlock] = 0u;
-        const int n = b.cnt->ndec[0];
-        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += a.g0 * blockDim.x) {
+
+    hub_chunks(b, b.dec[2], eff, lane, h, rd);
+
+    // ---- warp per vertex, groups of G consecutive list entries per item ----
+    {
+        const int n = cn->ndec[1];
+        const int nwarps = (int)gridDim.x * (int)(blockDim.x >> 5);
+        int G = n / (nwarps * 4);
+        G = G < 1 ? 1 : (G > 8 ? 8 : G);
+        const int ng = (n + G - 1) / G;
+        int pend = grab_issue(&cn->dgrab[1], lane);
+        for (;;) {
+            const int g = grab_take(pend);
+            if (g >= ng) break;
+            pend = grab_issue(&cn->dgrab[1], lane);
+            const int i0 = g * G, m = n - i0 < G ? n - i0 : G;
+            int gv = 0, gown = 0;
+            int64_t gs = 0, ge = 0;
+            if (lane < m) {
+                gv = b.dec[1][i0 + lane];
+                gown = b.label[gv];
+                gs = b.off[gv];
+                ge = b.off[gv + 1];
+            }
+            for (int j = 0; j < m; ++j) {
+                const int v = __shfl_sync(DMOLP_FULL_MASK, gv, j);
+                const int own = __shfl_sync(DMOLP_FULL_MASK, gown, j);
+                const int64_t s = __shfl_sync(DMOLP_FULL_MASK, gs, j), e = __shfl_sync(DMOLP_FULL_MASK, ge, j);
+                count_row(b, s, e, lane, eff, h);
+                double best;
+                int blab, own_cnt;
+                if (priv) {
+                    const int cnt = priv_total(h, eff, lane);
+                    warp_argmax(eff, b.tpen, lane, [&](int) { return cnt; }, best, blab);
+                    own_cnt = __shfl_sync(DMOLP_FULL_MASK, cnt, own & 31);
+                } else {
+                    warp_argmax(eff, b.tpen, lane, [&](int c) { return h[c]; }, best, blab);
+                    own_cnt = (unsigned)own < (unsigned)eff ? h[own] : 0;
+                }
+                if (lane == 0) {
+                    rd += (unsigned long long)(e - s);
+                    const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
+                    const int nl = best > own_raw ? blab : own;
+                    if (nl != own) park_move(b, v, nl);
+                }
+                __syncwarp();
+            }
+        }
+    }
+
+    // ---- thread per vertex: deg <= kDecSmall, own label scored, eff <= kDecSmallK.  Label counts are
+    //      bytes in this lane's column of the warp's region (word w of lane L at [w * 32 + L]: four labels
+    //      per word, conflict-free); a 64-bit mask lists the labels seen, and only those are scored -- an
+    //      absent label scores 0 <= count[own] and cannot win ----
+    {
+        const int n = cn->ndec[0];
+        const int ng = (n + 31) >> 5;
+        uint32_t *cw = reinterpret_cast<uint32_t *>(h) + lane;
+        if (ng > 0)
+            for (int w = 0; w < kDecSmallK / 4; ++w) cw[w * 32] = 0u;
+        int pend = grab_issue(&cn->dgrab[0], lane);
+        for (;;) {
+            const int g = grab_take(pend);
+            if (g >= ng) break;
+            pend = grab_issue(&cn->dgrab[0], lane);
+            const int i = g * 32 + lane;
+            if (i >= n) continue;
             const int v = b.dec[0][i];
             const int own = b.label[v];
             const int64_t s = b.off[v];
             const int deg = (int)(b.off[v + 1] - s);
             rd += deg;
             unsigned long long seen = 0ull;
-            for (int j = 0; j < deg; j += 4) {
-                int l[4];
+            for (int j = 0; j < deg; j += 8) {
+                int u[8], l[8];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) l[q] = j + q < deg ? b.label[__ldg(b.col + s + j + q)] : -1;
+                for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(b.col + s + j + q) : -1;
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
+                for (int q = 0; q < 8; ++q) l[q] = u[q] >= 0 ? b.label[u[q]] : -1;
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
                     if ((unsigned)l[q] < (unsigned)eff) {
-                        cw[(l[q] >> 2) * kBlock] += 1u << ((l[q] & 3) * 8);
+                        cw[(l[q] >> 2) * 32] += 1u << ((l[q] & 3) * 8);
                         seen |= 1ull << l[q];
                     }
             }
-            const int own_cnt = (int)((cw[(own >> 2) * kBlock] >> ((own & 3) * 8)) & 0xFFu);
+            const int own_cnt = (int)((cw[(own >> 2) * 32] >> ((own & 3) * 8)) & 0xFFu);
             double best = -DBL_MAX;
             int bkey = 0x7fffffff, blab = -1;
             for (unsigned long long m = seen; m; m &= m - 1) {
                 const int c = __ffsll((long long)m) - 1;
-                const int cnt = (int)((cw[(c >> 2) * kBlock] >> ((c & 3) * 8)) & 0xFFu);
+                const int cnt = (int)((cw[(c >> 2) * 32] >> ((c & 3) * 8)) & 0xFFu);
                 const double sc = __dmul_rn((double)cnt, b.tpen[c]);
                 const int key = tiekey(c);
                 if (better(sc, key, best, bkey)) {
@@ -336,83 +463,22 @@ __global__ void __launch_bounds__(256) k_decide(Buffers b, DecArgs a) {
                     blab = c;
                 }
             }
-            for (unsigned long long m = seen; m; m &= m - 1) cw[((__ffsll((long long)m) - 1) >> 2) * kBlock] = 0u;
+            for (unsigned long long m = seen; m; m &= m - 1) cw[((__ffsll((long long)m) - 1) >> 2) * 32] = 0u;
             if (blab >= 0 && best > (double)own_cnt && blab != own) park_move(b, v, blab);
-        }
-    } else if ((int)blockIdx.x < a.g0 + a.g1) {
-        // ---- warp per vertex ----
-        const int wpb = blockDim.x >> 5;
-        const int gw = ((int)blockIdx.x - a.g0) * wpb + wib, nw = a.g1 * wpb;
-        const int n = b.cnt->ndec[1];
-        for (int i = gw; i < n; i += nw) {
-            const int v = b.dec[1][i];
-            const int own = b.label[v];
-            const int64_t s = b.off[v], e = b.off[v + 1];
-            if (priv) priv_zero(h, eff, lane);
-            else
-                for (int c = lane; c < eff; c += 32) h[c] = 0;
-            __syncwarp();
-            warp_count(b.col, b.label, s, e, lane, eff, h);
-            __syncwarp();
-            double best;
-            int blab, own_cnt;
-            if (priv) {
-                const int cnt = priv_total(h, eff, lane);
-                warp_argmax(eff, b.tpen, lane, [&](int) { return cnt; }, best, blab);
-                own_cnt = __shfl_sync(DMOLP_FULL_MASK, cnt, own & 31);
-            } else {
-                warp_argmax(eff, b.tpen, lane, [&](int c) { return h[c]; }, best, blab);
-                own_cnt = (unsigned)own < (unsigned)eff ? h[own] : 0;
-            }
-            if (lane == 0) {
-                rd += (unsigned long long)(e - s);
-                const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
-                const int nl = best > own_raw ? blab : own;
-                if (nl != own) park_move(b, v, nl);
-            }
-            __syncwarp();
-        }
-    } else {
-        // ---- hubs (deg > kLargeDeg): warp per queued row chunk; counts go to the hub's row of hh ----
-        const int wpb = blockDim.x >> 5;
-        const int gw = ((int)blockIdx.x - a.g0 - a.g1) * wpb + wib, nw = ((int)gridDim.x - a.g0 - a.g1) * wpb;
-        const int n = b.cnt->nhubq;
-        for (int q = gw; q < n; q += nw) {
-            const int2 ch = b.hubq[q];
-            const int v = b.dec[2][ch.x];
-            const int64_t s = b.off[v] + ch.y, rowe = b.off[v + 1];
-            const int64_t e = rowe - s > kHubChunk ? s + kHubChunk : rowe;
-            if (priv) priv_zero(h, eff, lane);
-            else
-                for (int c = lane; c < eff; c += 32) h[c] = 0;
-            __syncwarp();
-            warp_count(b.col, b.label, s, e, lane, eff, h);
-            __syncwarp();
-            int32_t *row = b.hh + (size_t)ch.x * DMOLP_MAX_K;
-            if (priv) {
-                const int cnt = priv_total(h, eff, lane);
-                if (cnt) atomicAdd(&row[lane], cnt);
-            } else {
-                for (int c = lane; c < eff; c += 32)
-                    if (h[c]) atomicAdd(&row[c], h[c]);
-            }
-            if (lane == 0) rd += (unsigned long long)(e - s);
-            __syncwarp();
         }
     }
     rd = warp_sum_u64(rd);
     if (lane == 0 && rd) atomicAdd(&b.rec[a.t - 1].arcs_dec, rd);
 }
 
-// Hub decisions, before k_decide: clear each hub's count row and queue its row in kHubChunk pieces.
-__global__ void k_hub_prep(Buffers b, int eff) {
-    if (b.ctrl->stopped) return;
+// Hub rows queued in kHubChunk pieces for hub_chunks, with each hub's count row cleared: the selected hubs
+// (list = dec[2], n = ndec[2]) before k_decide, or every hub (list = bucket[2]) at the start of a run.
+__device__ __forceinline__ void hub_queue(const Buffers &b, const int32_t *list, int n, int eff) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    const int n = b.cnt->ndec[2];
     for (int i = gw; i < n; i += nw) {
-        const int v = b.dec[2][i];
-        int32_t *row = b.hh + (size_t)i * DMOLP_MAX_K;
+        const int v = list[i];
+        int32_t *row = b.hh + (size_t)b.hidx[v] * DMOLP_MAX_K;
         for (int c = lane; c < eff; c += 32) row[c] = 0;
         const int64_t deg = b.off[v + 1] - b.off[v];
         const int nch = (int)((deg + kHubChunk - 1) / kHubChunk);
@@ -421,6 +487,26 @@ __global__ void k_hub_prep(Buffers b, int eff) {
         base = __shfl_sync(DMOLP_FULL_MASK, base, 0);
         for (int c = lane; c < nch; c += 32) b.hubq[base + c] = make_int2(i, c * kHubChunk);
     }
+}
+
+__global__ void k_hub_prep(Buffers b, int eff) {
+    if (b.ctrl->stopped) return;
+    hub_queue(b, b.dec[2], b.cnt->ndec[2], eff);
+}
+
+// Run start on symmetric graphs: every hub's row counted once (k_hub_all_queue, then k_hub_all_count).
+__global__ void k_hub_all_queue(Buffers b, int nhub, int eff) { hub_queue(b, b.bucket[2], nhub, eff); }
+
+__global__ void __launch_bounds__(256, 4) k_hub_all_count(Buffers b, int eff, int wstride) {
+    extern __shared__ int shist[];
+    int *h = shist + (threadIdx.x >> 5) * wstride;
+    unsigned long long rd = 0;
+    hub_chunks(b, b.bucket[2], eff, threadIdx.x & 31, h, rd);
+}
+
+__global__ void k_hub_index(Buffers b, int nhub) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nhub; i += gridDim.x * blockDim.x)
+        b.hidx[b.bucket[2][i]] = i;
 }
 
 // Hub decisions, after k_decide: warp per hub, argmax over its summed counts.
@@ -432,7 +518,7 @@ __global__ void k_hub_final(Buffers b, int eff) {
     for (int i = gw; i < n; i += nw) {
         const int v = b.dec[2][i];
         const int own = b.label[v];
-        const int32_t *row = b.hh + (size_t)i * DMOLP_MAX_K;
+        const int32_t *row = b.hh + (size_t)b.hidx[v] * DMOLP_MAX_K;
         double best;
         int blab;
         warp_argmax(eff, b.tpen, lane, [&](int c) { return row[c]; }, best, blab);
@@ -449,8 +535,9 @@ __global__ void k_hub_final(Buffers b, int eff) {
 // label lo = label[u] and new label ln (newlab[u] if u moves, else lo), the arc leaves the cut count
 // [a != lo] and the intra count of a if a == lo, and enters them with (c, ln).  Weight 2 when u stays:
 // the reverse arc (u,v) changes the same way but is never visited; weight 1 when u moves (or u == v):
-// (u,v) is visited from u's side.  Vertex counts move by one.
-__global__ void k_update(Buffers b, int k, int t) {
+// (u,v) is visited from u's side.  Vertex counts move by one.  A hub neighbour u sees v's label go from
+// a to c: its row of label counts (labels < eff) moves by one.
+__global__ void k_update(Buffers b, int k, int eff, int t) {
     if (b.ctrl->stopped) return;
     extern __shared__ unsigned long long sacc[];  // [2k]: vertex-count deltas, intra-arc deltas
     for (int p = threadIdx.x; p < 2 * k; p += blockDim.x) sacc[p] = 0;
@@ -479,6 +566,12 @@ __global__ void k_update(Buffers b, int k, int t) {
             const int du = (int)(ln != c) - (int)(lo != a);
             if (du) atomicAdd(&b.ndiff[u], du);
             if (nu < 0) dv += (int)(c != lo) - (int)(a != lo);
+            const int hu = b.hidx[u];
+            if (hu >= 0) {
+                int32_t *row = b.hh + (size_t)hu * DMOLP_MAX_K;
+                if ((unsigned)a < (unsigned)eff) atomicAdd(&row[a], -1);
+                if ((unsigned)c < (unsigned)eff) atomicAdd(&row[c], 1);
+            }
         }, [] { return false; });
         for (int o = 16; o > 0; o >>= 1) {
             in_c += __shfl_xor_sync(DMOLP_FULL_MASK, in_c, o);
@@ -763,6 +856,7 @@ __global__ void k_zero_small(Buffers b) {
     LpCounters *cn = b.cnt;
     cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
     cn->nhubq = 0;
+    cn->dgrab[0] = cn->dgrab[1] = cn->dgrab[2] = 0;
     cn->nchanged = 0;
     b.ctrl->stopped = 0;
 }
@@ -863,22 +957,31 @@ BndArgs bnd_args(dmolp_ctx *c, int t, int all) {
 
 int bnd_grid(dmolp_ctx *c, const BndArgs &a) { return a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
 
-DecArgs dec_args(dmolp_ctx *c, int t, int eff) {
+int dec_wstride(int eff) { return eff <= 32 ? 1024 : (eff > (kDecSmallK / 4) * 32 ? eff : (kDecSmallK / 4) * 32); }
+
+size_t dec_smem(int eff) { return (size_t)kWarpsPerBlock * dec_wstride(eff) * sizeof(int); }
+
+DecArgs dec_args(int t, int eff) {
     DecArgs a;
     a.t = t;
     a.eff = eff;
-    a.g0 = c->num_sms * 2;
-    a.g1 = c->num_sms * 4;
+    a.wstride = dec_wstride(eff);
     return a;
 }
 
-int dec_grid(dmolp_ctx *c, const DecArgs &a) { return a.g0 + a.g1 + c->num_sms * 2; }
-
-size_t dec_smem(int eff) {
-    const size_t warp = eff <= 32 ? (size_t)(kWarpsPerBlock * 1024 + kWarpsPerBlock * 32) * sizeof(int)
-                                  : (size_t)kWarpsPerBlock * eff * sizeof(int);
-    const size_t thread = (size_t)(kDecSmallK / 4) * kBlock * sizeof(uint32_t);  // byte counters
-    return warp > thread ? warp : thread;
+// Persistent grid of k_decide: as many blocks as stay resident (the warps take their work from counters).
+int dec_grid(dmolp_ctx *c, int eff) {
+    static int per_sm[2] = {0, 0};
+    int &n = per_sm[eff <= 32 ? 0 : 1];
+    if (n == 0) {
+        int r = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_decide, kBlock, dec_smem(eff <= 32 ? 32 : DMOLP_MAX_K)) !=
+                cudaSuccess ||
+            r < 1)
+            r = kGridPerSm;
+        n = r;
+    }
+    return c->num_sms * n;
 }
 
 StatsArgs stats_args(dmolp_ctx *c, int k) {
@@ -897,15 +1000,21 @@ StatsArgs stats_args(dmolp_ctx *c, int k) {
 
 int stats_grid(dmolp_ctx *c, const StatsArgs &a) { return a.gv + a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
 
-// The LP decisions of the selected window: hub row chunks queued, the three classes counted / decided,
-// hub argmaxes last.
-void launch_decide(dmolp_ctx *c, int t, int eff) {
+// The LP decisions of the selected window: hub row chunks queued (unless the hub counts are kept current),
+// the classes counted / decided, hub argmaxes last.  Graphs without hubs launch k_decide alone.
+void launch_decide(dmolp_ctx *c, int t, int eff, bool recount_hubs) {
     Buffers &b = c->b;
-    k_hub_prep<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff);
-    const DecArgs d = dec_args(c, t, eff);
-    k_decide<<<dec_grid(c, d), kBlock, dec_smem(eff), c->stream>>>(b, d);
-    k_hub_final<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff);
-    c->launches += 3;
+    const bool hubs = c->nb[2] > 0;
+    if (hubs && recount_hubs) {
+        k_hub_prep<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff);
+        c->launches++;
+    }
+    k_decide<<<dec_grid(c, eff), kBlock, dec_smem(eff), c->stream>>>(b, dec_args(t, eff));
+    c->launches++;
+    if (hubs) {
+        k_hub_final<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff);
+        c->launches++;
+    }
 }
 
 // Optional timing of one kernel launch (dmolp_set_profiling): an event pair around it on the same stream.
@@ -961,6 +1070,24 @@ void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip) {
     c->launches++;
 }
 
+void lp_hub_index(dmolp_ctx *c) {
+    lp_fill(c, c->b.hidx, c->nv + 1, -1);
+    if (c->nb[2] > 0) {
+        k_hub_index<<<clampi((c->nb[2] + 255) / 256, 1, grid_for(c)), kBlock, 0, c->stream>>>(c->b, c->nb[2]);
+        c->launches++;
+    }
+}
+
+void lp_hub_counts(dmolp_ctx *c, int eff) {
+    if (c->nb[2] == 0) return;
+    Buffers &b = c->b;
+    cudaMemsetAsync(&b.cnt->nhubq, 0, sizeof(int), c->stream);
+    cudaMemsetAsync(&b.cnt->dgrab[2], 0, sizeof(int), c->stream);
+    k_hub_all_queue<<<clampi((c->nb[2] + 7) / 8, 1, grid_for(c)), kBlock, 0, c->stream>>>(b, c->nb[2], eff);
+    k_hub_all_count<<<c->num_sms * 4, kBlock, dec_smem(eff), c->stream>>>(b, eff, dec_wstride(eff));
+    c->launches += 2;
+}
+
 void lp_init_end(dmolp_ctx *c, int mode) {
     k_lp_init_end<<<1, 1, 0, c->stream>>>(c->b, mode);
     c->launches++;
@@ -1008,13 +1135,12 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     }
     {
         ProfScope ps(c, 1, t);
-        launch_decide(c, t, L.eff);
+        launch_decide(c, t, L.eff, !c->symmetric);
     }
-    c->launches += 1;
     if (c->symmetric) {
         {
             ProfScope ps(c, 3, t);
-            k_update<<<grid, kBlock, 2 * L.k * sizeof(unsigned long long), c->stream>>>(b, L.k, t);
+            k_update<<<grid, kBlock, 2 * L.k * sizeof(unsigned long long), c->stream>>>(b, L.k, L.eff, t);
         }
         k_apply<<<grid, kBlock, 0, c->stream>>>(b);
         c->launches += 2;
@@ -1053,7 +1179,7 @@ void lp_apply_list(dmolp_ctx *c, int k, int eff, int n) {
     const int grid = grid_for(c);
     k_zero_small<<<1, 1, 0, c->stream>>>(b);
     k_classify<<<grid, kBlock, 0, c->stream>>>(b, n, eff);
-    launch_decide(c, 1, eff);
+    launch_decide(c, 1, eff, true);
     k_collect_moves<<<grid, kBlock, 0, c->stream>>>(b);
     k_apply<<<grid, kBlock, 0, c->stream>>>(b);
     c->launches += 4;
