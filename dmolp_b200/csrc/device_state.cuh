@@ -36,6 +36,7 @@ struct LpCounters {
     int npos;         // selection record slots: one per vertex with arcs (fixed per graph)
     unsigned long long cut_arcs;   // arcs whose endpoint labels differ (kept current incrementally)
     int dgrab[3];     // decisions: work items taken so far per class (thread groups, warp groups, hub chunks)
+    int nhubw;        // queued row chunks of hubs that entered or left the window
 };
 
 // Loop control shared by the iteration kernels.
@@ -63,6 +64,8 @@ struct LpRecordDev {
     unsigned long long te_prev, te_cand, te_sel, te_stats;
     // arcs the kernels actually read: boundary test (early exit), decisions, incremental update
     unsigned long long arcs_bnd, arcs_dec, arcs_upd;
+    unsigned long long arcs_mark;  // arcs read by the window marking (window rows, rows of hubs that changed)
+    unsigned long long te_hubsel;  // arcs of the selected hubs (part of te_sel)
 };
 
 struct Buffers {
@@ -92,6 +95,9 @@ struct Buffers {
                                // selected hubs each iteration, or (symmetric graphs) counted once per LP run
                                // and kept current from the movers' arcs
     int32_t *hidx = nullptr;   // [nv] hub index (position in bucket[2]) of a vertex with deg > kLargeDeg, else -1
+    int32_t *hubwin = nullptr; // [nv] hubs of the previous window whose rows hold the vertex
+    int32_t *hub_in = nullptr; // [nb[2]] hub is counted in hubwin (was in the window hubwin describes)
+    int2 *hubwq = nullptr;     // [hubq_cap] (hub index, first arc) of rows entering or leaving hubwin
     int32_t *active[2] = {nullptr, nullptr};  // [nv] radix-select active lists
     // per-part arrays (DMOLP_MAX_K); vc / intra hold signed values in two's complement
     unsigned int *hist = nullptr;        // [MAX_K * 256]

@@ -281,6 +281,9 @@ size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t 
     ALLOC(b.hubq, (size_t)c->hubq_cap);
     ALLOC(b.hh, nball[2] * (size_t)DMOLP_MAX_K);
     ALLOC(b.hidx, n);
+    ALLOC(b.hubwin, n);
+    ALLOC(b.hub_in, nball[2]);
+    ALLOC(b.hubwq, (size_t)c->hubq_cap);
 #undef ALLOC
     return off;
 }
@@ -1070,6 +1073,10 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     DMOLP_CUDA(cudaMemsetAsync(b.stamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.sstamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.ndiff, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
+    if (c->nb[2] > 0) {
+        DMOLP_CUDA(cudaMemsetAsync(b.hubwin, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
+        DMOLP_CUDA(cudaMemsetAsync(b.hub_in, 0, (size_t)c->nb[2] * sizeof(int32_t), c->stream));
+    }
     lp_reset_stats(c, k, nullptr);
     lp_stats(c, k, nullptr, nullptr);
     if (c->symmetric) lp_hub_counts(c, L.eff);
@@ -1120,8 +1127,9 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
         //           boundary count of each candidate, id + window stamp per arc of a pull-mode walk, own
         //           label per boundary record
         //  decide : list id + offsets + own label per selected vertex, id + label per arc, 8 B per mover
-        //  mark   : list id + offsets per window vertex, id read + stamp write per arc
-        //  update : offsets + labels per mover, id + label + pending label per arc
+        //  mark   : list id + offsets per window vertex, id read + stamp write per arc of a walked row
+        //           (window rows up to 4096 arcs; hub rows only when the hub enters or leaves the window)
+        //  update : offsets + labels per mover, id + label + pending label + hub index per arc
         //  select : label + key of every record slot, read by the first histogram and partition pass
         const double nbk = (double)c->nb[0] + c->nb[1] + c->nb[2];
         dmolp_ctx::ProfEvents &pe = c->prof_pending;
@@ -1135,8 +1143,8 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
                 if (kind == 0)
                 bytes = (t > 1 ? 8.0 : 4.0) * nbk + 5.0 * nbk + 20.0 * ncand + 8.0 * (double)d.arcs_bnd + 8.0 * d.boundary;
                 else if (kind == 1) bytes = 24.0 * d.window + 8.0 * (double)d.arcs_dec + 8.0 * d.changes;
-                else if (kind == 2) bytes = (t > 1 ? 20.0 * recs[t - 2].window : 0.0) + 8.0 * (double)d.te_prev;
-                else if (kind == 3) bytes = 28.0 * d.changes + 12.0 * (double)d.arcs_upd;
+                else if (kind == 2) bytes = (t > 1 ? 20.0 * recs[t - 2].window : 0.0) + 8.0 * (double)d.arcs_mark;
+                else if (kind == 3) bytes = 28.0 * d.changes + 16.0 * (double)d.arcs_upd;
             else bytes = 24.0 * nbk + (double)d.window;  // select: first digit pass over every record slot
                 c->prof_ms[kind] += ems;
                 c->prof_launches[kind] += 1;
@@ -1169,7 +1177,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
             o.changes = d.changes;
             o.boundary = d.boundary;
             o.reserved = 0;
-            o.arcs_read = d.arcs_bnd + d.arcs_dec + d.arcs_upd + (i > 0 ? d.te_prev : 0);
+            o.arcs_read = d.arcs_bnd + d.arcs_dec + d.arcs_upd + d.arcs_mark;
             o.edge_cut = d.edge_cut;
             o.te_prev = d.te_prev;
             o.te_cand = d.te_cand;

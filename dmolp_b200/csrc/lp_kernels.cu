@@ -48,6 +48,7 @@ __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
         cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
         cn->nchunk = 0;
         cn->nhubq = 0;
+        cn->nhubw = 0;
         cn->dgrab[0] = cn->dgrab[1] = cn->dgrab[2] = 0;
         ctl->stop_now = 0;
         ctl->skip_stats = 0;
@@ -58,7 +59,7 @@ __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
         // sum of degrees over the previous window = the previous iteration's selected window
         r.te_prev = t == 1 ? (unsigned long long)narcs : b.rec[t - 2].te_sel;
         r.te_cand = r.te_sel = r.te_stats = 0;
-        r.arcs_bnd = r.arcs_dec = r.arcs_upd = 0;
+        r.arcs_bnd = r.arcs_dec = r.arcs_upd = r.arcs_mark = r.te_hubsel = 0;
     }
     // ---- statistics -> expected values and calculatePenalties (phase2.cpp:110-115, 158-209) ----
     if (threadIdx.x < 32)
@@ -73,16 +74,19 @@ __device__ __forceinline__ void stamp_once(const Buffers &b, int u, int t) {
 }
 
 // Warp per vertex of the previous window: stamp it and its first kChunk neighbours; the rest of a long row
-// is queued in kChunk pieces for k_mark_chunks.
-__global__ void k_mark(Buffers b, int t) {
+// is queued in kChunk pieces for k_mark_chunks.  Without walk_hubs a hub (deg > kLargeDeg) stamps only
+// itself: its neighbours are candidates through hubwin (k_hubwin_*).
+__global__ void k_mark(Buffers b, int t, int walk_hubs) {
     if (b.ctrl->stopped || b.ctrl->pull) return;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     const int32_t *prev = b.win[(t - 1) & 1];
     const int n = b.cnt->nwin[(t - 1) & 1];
+    unsigned long long rd = 0;
     for (int i = gw; i < n; i += nw) {
         const int v = prev[i];
-        const int64_t s = b.off[v], e = b.off[v + 1];
+        int64_t s = b.off[v], e = b.off[v + 1];
+        if (!walk_hubs && e - s > kLargeDeg) e = s;
         if (lane == 0) {
             b.stamp[v] = t;
             for (int64_t c = s + kChunk; c < e; c += kChunk) {
@@ -92,7 +96,10 @@ __global__ void k_mark(Buffers b, int t) {
         }
         const int64_t e1 = e - s > kChunk ? s + kChunk : e;
         warp_row(b.col, s, e1, lane, [&](int u) { stamp_once(b, u, t); }, [] { return false; });
+        if (lane == 0) rd += (unsigned long long)(e1 - s);
     }
+    rd = warp_sum_u64(rd);
+    if (lane == 0 && rd) atomicAdd(&b.rec[t - 1].arcs_mark, rd);
 }
 
 __global__ void k_mark_chunks(Buffers b, int t) {
@@ -100,17 +107,59 @@ __global__ void k_mark_chunks(Buffers b, int t) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     const int n = b.cnt->nchunk;
+    unsigned long long rd = 0;
     for (int i = gw; i < n; i += nw) {
         const int2 q = b.chunkq[i];
         const int64_t s = b.off[q.x] + q.y, rowe = b.off[q.x + 1];
         const int64_t e = rowe - s > kChunk ? s + kChunk : rowe;
         warp_row(b.col, s, e, lane, [&](int u) { stamp_once(b, u, t); }, [] { return false; });
+        if (lane == 0) rd += (unsigned long long)(e - s);
     }
+    rd = warp_sum_u64(rd);
+    if (lane == 0 && rd) atomicAdd(&b.rec[t - 1].arcs_mark, rd);
+}
+
+// hubwin[u] = hubs of the previous window whose rows hold u, kept across iterations: a hub that entered
+// the window (sstamp == t-1) adds one to every vertex of its row, a hub that left subtracts one.  Thread
+// per hub: flip hub_in and queue the row in kHubChunk pieces.
+__global__ void k_hubwin_queue(Buffers b, int t, int nhub) {
+    if (b.ctrl->stopped) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nhub; i += gridDim.x * blockDim.x) {
+        const int h = b.bucket[2][i];
+        const int now = b.sstamp[h] == t - 1;
+        if (now == b.hub_in[i]) continue;
+        b.hub_in[i] = now;
+        const int64_t deg = b.off[h + 1] - b.off[h];
+        const int nch = (int)((deg + kHubChunk - 1) / kHubChunk);
+        const int base = atomicAdd(&b.cnt->nhubw, nch);
+        for (int c = 0; c < nch; ++c) b.hubwq[base + c] = make_int2(i, c * kHubChunk);
+    }
+}
+
+// Warp per queued chunk: +1 (hub entered) or -1 (hub left) on every vertex of the chunk.
+__global__ void k_hubwin_apply(Buffers b, int t) {
+    if (b.ctrl->stopped) return;
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int n = b.cnt->nhubw;
+    unsigned long long rd = 0;
+    for (int i = gw; i < n; i += nw) {
+        const int2 q = b.hubwq[i];
+        const int h = b.bucket[2][q.x];
+        const int d = b.hub_in[q.x] ? 1 : -1;
+        const int64_t s = b.off[h] + q.y, rowe = b.off[h + 1];
+        const int64_t e = rowe - s > kHubChunk ? s + kHubChunk : rowe;
+        warp_row(b.col, s, e, lane, [&](int u) { atomicAdd(&b.hubwin[u], d); }, [] { return false; });
+        if (lane == 0) rd += (unsigned long long)(e - s);
+    }
+    rd = warp_sum_u64(rd);
+    if (lane == 0 && rd) atomicAdd(&b.rec[t - 1].arcs_mark, rd);
 }
 
 // ------------------------------------------------------------------------------------ bnd
 struct BndArgs {
     int t, all, ibits, maxdeg;
+    int hubwin;  // hubwin is current: hubs of the previous window make their neighbours candidates
     int nb0, nb1, nb2;
     int g0, g1;  // block split: [0,g0) thread class, [g0,g0+g1) warp class, rest block class
 };
@@ -129,7 +178,8 @@ __device__ __forceinline__ void put_slot(const Buffers &b, int pos, bool isb, in
 }
 
 // Candidacy: t = 1 every vertex; push mode stamp[v] == t (set by k_mark); pull mode v is in the previous
-// window (sstamp == t-1) or has a neighbour that is.  A candidate is on the boundary when it has a
+// window (sstamp == t-1) or has a neighbour that is; in both modes hubwin[v] > 0 (a hub of the previous
+// window lists v) when the hub rows are not walked.  A candidate is on the boundary when it has a
 // differently-labelled neighbour: ndiff[v] > 0, a count kept exact by the statistics pass and by k_update
 // (symmetric graphs) or by the full pass after every move (other graphs).  So only pull-mode candidacy
 // walks rows; at t = 1 and in push mode every record slot costs a handful of per-vertex reads.
@@ -161,14 +211,14 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
         const int n = a.nb0 + a.nb1 + a.nb2;
         for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += gridDim.x * blockDim.x) {
             const int v = b.ball[pos];
-            const bool cand = a.all || b.stamp[v] == a.t;
+            const bool cand = a.all || b.stamp[v] == a.t || (a.hubwin && b.hubwin[v] > 0);
             finish(pos, v, cand, cand ? (int)(b.off[v + 1] - b.off[v]) : 0);
         }
     } else if ((int)blockIdx.x < a.g0) {
         // ---- pull, thread per vertex (deg <= kSmallDeg): window stamps of the row, 4 at a time ----
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
             const int v = b.bucket[0][i];
-            bool cand = b.sstamp[v] == tp;
+            bool cand = b.sstamp[v] == tp || (a.hubwin && b.hubwin[v] > 0);
             const int64_t s = b.off[v];
             const int deg = (int)(b.off[v + 1] - s);
             if (!cand) {
@@ -189,7 +239,7 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
         for (int i = gw; i < a.nb1; i += nw) {
             const int pos = a.nb0 + i;
             const int v = b.bucket[1][i];
-            const bool cand0 = b.sstamp[v] == tp;
+            const bool cand0 = b.sstamp[v] == tp || (a.hubwin && b.hubwin[v] > 0);
             const int64_t s = b.off[v], e = b.off[v + 1];
             bool cand = cand0;
             if (!cand0) {  // warp-uniform
@@ -207,7 +257,7 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
         for (int i = gb; i < a.nb2; i += nbk) {
             const int pos = a.nb0 + a.nb1 + i;
             const int v = b.bucket[2][i];
-            const bool cand0 = b.sstamp[v] == tp;
+            const bool cand0 = b.sstamp[v] == tp || (a.hubwin && b.hubwin[v] > 0);
             const int64_t s = b.off[v], e = b.off[v + 1];
             bool cand = cand0;
             int64_t j0 = s;
@@ -509,8 +559,9 @@ __global__ void k_hub_index(Buffers b, int nhub) {
         b.hidx[b.bucket[2][i]] = i;
 }
 
-// Hub decisions, after k_decide: warp per hub, argmax over its summed counts.
-__global__ void k_hub_final(Buffers b, int eff) {
+// Hub decisions, after k_decide: warp per hub, argmax over its summed counts; the hubs' arcs are summed
+// for the next iteration's push / pull choice.
+__global__ void k_hub_final(Buffers b, int eff, int t) {
     if (b.ctrl->stopped) return;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
@@ -526,6 +577,7 @@ __global__ void k_hub_final(Buffers b, int eff) {
             const double own_raw = (unsigned)own < (unsigned)eff ? (double)row[own] : -1e300;
             const int nl = best > own_raw ? blab : own;
             if (nl != own) park_move(b, v, nl);
+            atomicAdd(&b.rec[t - 1].te_hubsel, (unsigned long long)(b.off[v + 1] - b.off[v]));
         }
     }
 }
@@ -757,8 +809,8 @@ __global__ void k_lp_end(Buffers b, int k, int t, long long narcs, int mode, int
     }
     ctl->iters_run = t;
     // the next iteration pulls when pushing would walk more than a quarter of all arcs (pulling finds the
-    // same candidates only when every arc has its reverse)
-    ctl->pull = symmetric && r.te_sel * 4ull > (unsigned long long)narcs;
+    // same candidates only when every arc has its reverse); hub rows are not walked by the push
+    ctl->pull = symmetric && (r.te_sel - r.te_hubsel) * 4ull > (unsigned long long)narcs;
     if (ctl->stop_now) {
         ctl->stopped = 1;
         ctl->stop_reason = ctl->stop_now;
@@ -940,10 +992,11 @@ int grid_for(dmolp_ctx *c) { return c->num_sms * kGridPerSm; }
 
 int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 
-BndArgs bnd_args(dmolp_ctx *c, int t, int all) {
+BndArgs bnd_args(dmolp_ctx *c, int t, int all, int hubwin) {
     BndArgs a;
     a.t = t;
     a.all = all;
+    a.hubwin = hubwin;
     a.ibits = c->ibits;
     a.maxdeg = (int)c->maxdeg;
     a.nb0 = c->nb[0];
@@ -1012,7 +1065,7 @@ void launch_decide(dmolp_ctx *c, int t, int eff, bool recount_hubs) {
     k_decide<<<dec_grid(c, eff), kBlock, dec_smem(eff), c->stream>>>(b, dec_args(t, eff));
     c->launches++;
     if (hubs) {
-        k_hub_final<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff);
+        k_hub_final<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff, t);
         c->launches++;
     }
 }
@@ -1109,6 +1162,8 @@ SplitArgs split_args(const Buffers &b, int t, int eff) {
     return sp;
 }
 
+static_assert(kChunk >= kLargeDeg, "the loop's marking queues no row chunks: its longest walked row is kLargeDeg");
+
 void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     Buffers &b = c->b;
     const int grid = grid_for(c);
@@ -1116,14 +1171,19 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     k_lp_begin<<<1, 256, 0, c->stream>>>(b, L.k, t, (long long)c->narcs);
     c->launches += 1;
     if (t > 1) {
+        // window rows up to kChunk = kLargeDeg arcs (no chunks to queue); hubs through hubwin
         ProfScope ps(c, 2, t);
-        k_mark<<<grid, kBlock, 0, c->stream>>>(b, t);
-        k_mark_chunks<<<grid, kBlock, 0, c->stream>>>(b, t);
-        c->launches += 2;
+        k_mark<<<grid, kBlock, 0, c->stream>>>(b, t, 0);
+        c->launches += 1;
+        if (c->nb[2] > 0) {
+            k_hubwin_queue<<<clampi((c->nb[2] + 255) / 256, 1, grid), kBlock, 0, c->stream>>>(b, t, c->nb[2]);
+            k_hubwin_apply<<<grid, kBlock, 0, c->stream>>>(b, t);
+            c->launches += 2;
+        }
     }
     {
         ProfScope ps(c, 0, t);
-        const BndArgs a = bnd_args(c, t, t == 1);
+        const BndArgs a = bnd_args(c, t, t == 1, c->nb[2] > 0);  // hubwin is cleared only for graphs with hubs
         k_bnd<<<bnd_grid(c, a), kBlock, L.k * sizeof(int), c->stream>>>(b, a, L.k);
     }
     k_lp_need<<<1, 256, 0, c->stream>>>(b, L.k, t);
@@ -1162,9 +1222,9 @@ void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int n
     Buffers &b = c->b;
     const int grid = grid_for(c);
     k_ws_begin<<<1, 256, 0, c->stream>>>(b, k, t, nprev);
-    k_mark<<<grid, kBlock, 0, c->stream>>>(b, t);
+    k_mark<<<grid, kBlock, 0, c->stream>>>(b, t, 1);
     k_mark_chunks<<<grid, kBlock, 0, c->stream>>>(b, t);
-    const BndArgs a = bnd_args(c, t, 0);
+    const BndArgs a = bnd_args(c, t, 0, 0);
     k_bnd<<<bnd_grid(c, a), kBlock, k * sizeof(int), c->stream>>>(b, a, k);
     k_lp_need<<<1, 256, 0, c->stream>>>(b, k, t);
     c->launches += 5;

@@ -92,3 +92,22 @@ def test_hub_decisions_reference_stopping_rules(part):
     o = oracle.phase2(g.offsets, g.indices, lab0, 16, "ref")
     assert np.array_equal(part.labels(), o.labels)
     assert m.edge_cut == o.res.edge_cut and m.iterations_run == o.res.iterations_run
+
+
+def test_graph_without_hubs_after_one_with_hubs(part):
+    """The per-graph arena is reused: a hub-free graph uploaded after a graph with hubs must not see the
+    earlier graph's hub-window counts."""
+    from dmolp_b200 import graphs
+
+    g = hub_graph(seed=4)
+    part.upload(g)
+    part.set_labels(np.random.default_rng(1).integers(0, 8, g.num_vertices).astype(np.int32))
+    part.phase2(8, mode="fixed", iterations=12)
+    h = graphs.knn(30000, 3, 10, seed=9)
+    assert np.diff(h.offsets).max() <= 4096
+    part.upload(h)
+    lab0 = np.random.default_rng(2).integers(0, 8, h.num_vertices).astype(np.int32)
+    part.set_labels(lab0)
+    m = part.phase2(8, mode="fixed", iterations=12)
+    o = oracle.phase2(h.offsets, h.indices, lab0, 8, "fixed", 12)
+    assert np.array_equal(part.labels(), o.labels) and m.edge_cut == o.res.edge_cut
