@@ -31,6 +31,7 @@ struct LpCounters {
     int nactive[2];   // radix-select active lists
     int nchanged;     // selected vertices whose label changed (movers)
     int ndec[3];      // selected vertices per decision class
+    int ndec_prev[3]; // the previous iteration's ndec (its window by class, for the marking)
     int nchunk;       // queued row chunks of the marking kernel
     int nhubq;        // queued row chunks of the hub decisions
     int npos;         // selection record slots: one per vertex with arcs (fixed per graph)

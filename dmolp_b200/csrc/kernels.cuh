@@ -17,22 +17,25 @@ std::vector<int> hubs_from_pairs(std::vector<std::pair<int, int>> sd);
 // whose top bit is below `keybits`; keys are unique.  For every segment p, marks sel[i] = 1 on the need[p] records with the
 // smallest keys (need[] is consumed).  sel[] must be zero on entry.  `stopped` (may be null) turns the
 // launches into no-ops once it is non-zero.
-// The LP window straight out of the selection: each selected record slot i (vertex vertex[i], segment = its
-// label) is stamped sstamp[v] = t, appended to win / nwin and to its decision-class list dec[c] / ndec[c],
-// and its degree added to *te.
+// The LP window straight out of the selection: the key of a selected record slot holds its vertex and
+// degree (key = (dk << ibits) | v, dk = maxdeg - deg when RE[label] > 1, else deg; label = its segment);
+// v is stamped sstamp[v] = t, appended to win / nwin and to its decision-class list dec[c] / ndec[c], and
+// its degree added to *te.
 struct SplitArgs {
-    const int32_t *vertex;
-    const int64_t *off;
+    const double *RE;
     int32_t *sstamp;
     int32_t *win;
     int *nwin;
     int32_t *dec[3];
     int *ndec;
     unsigned long long *te;
-    int t, eff;
+    int t, eff, ibits, maxdeg;
 };
+// first_hist_ready: the writer of the records has already added every record's first digit (bits
+// [select_first_shift(keybits), +8) of its key) into histogram buffer 0 of c->b.hist, bin seg * 256 + digit.
 void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, const int *n_dev, int nseg, int keybits,
-                     uint8_t *sel, const int *stopped, const SplitArgs *split = nullptr);
+                     uint8_t *sel, const int *stopped, const SplitArgs *split = nullptr, bool first_hist_ready = false);
+inline int select_first_shift(int keybits) { return ((keybits + kRadixBits - 1) / kRadixBits - 1) * kRadixBits; }
 void select_prepare();  // kernel attributes; call once before any capture
 
 // ---- LP loop (lp_kernels.cu) ----

@@ -53,6 +53,45 @@ __device__ __forceinline__ int64_t warp_row(const int32_t *__restrict__ col, int
     return read + (e - t0);
 }
 
+// The arcs [s, e) of a row visited by the lanes of a warp with many loads in flight: each step loads, per
+// lane, the row's scalar head and tail (first step only) and two 16-byte words of its body, then gathers
+// g(u) for all of them, then calls f(u, g(u)) for each, so a row of up to 262 arcs costs one dependent
+// load pair.  After each step stop() (evaluated warp-uniformly) may end the walk.  Returns the number of
+// arcs the warp read.
+template <typename G, typename F, typename S>
+__device__ __forceinline__ int64_t warp_row_wide(const int32_t *__restrict__ col, int64_t s, int64_t e, int lane,
+                                                 G g, F f, S stop) {
+    int64_t a = (s + 3) & ~int64_t(3);
+    if (a > e) a = e;
+    const int64_t qe = e >> 2;  // body: int4 words [a/4, e/4)
+    const int64_t t0 = a > (qe << 2) ? a : (qe << 2);
+    const int4 *c4 = reinterpret_cast<const int4 *>(col);
+    int64_t read = (a - s) + (e - t0);
+    bool first = true;
+    for (int64_t q0 = a >> 2; first || q0 < qe; q0 += 64) {
+        int u[10];
+        u[8] = first && s + lane < a ? __ldg(col + s + lane) : -1;
+        u[9] = first && t0 + lane < e ? __ldg(col + t0 + lane) : -1;
+        const int64_t q = q0 + lane;
+        int4 x = make_int4(-1, -1, -1, -1), y = make_int4(-1, -1, -1, -1);
+        if (q < qe) x = __ldcs(c4 + q);
+        if (q + 32 < qe) y = __ldcs(c4 + q + 32);
+        u[0] = x.x; u[1] = x.y; u[2] = x.z; u[3] = x.w;
+        u[4] = y.x; u[5] = y.y; u[6] = y.z; u[7] = y.w;
+        decltype(g(0)) v[10];
+#pragma unroll
+        for (int r = 0; r < 10; ++r)
+            if (u[r] >= 0) v[r] = g(u[r]);
+#pragma unroll
+        for (int r = 0; r < 10; ++r)
+            if (u[r] >= 0) f(u[r], v[r]);
+        if (q0 < qe) read += 4 * (qe - q0 < 64 ? qe - q0 : (int64_t)64);
+        first = false;
+        if (stop()) break;
+    }
+    return read;
+}
+
 // Lane-private label counters of one warp for labels < 32: lane L counts label c in
 // h[c*32 + ((L + c) & 31)].  Increments need no atomics and hit distinct banks for lanes sharing a label;
 // the sum over row c (lane c, rotated start) is bank-conflict free as well.

@@ -4,15 +4,19 @@
 //   begin    penalties from the current statistics (calculatePenalties, src/phase2/phase2.cpp:158-209);
 //            counter reset
 //   mark     stamp the previous window and its neighbours with t (expandBoundaryNodes' candidate set,
-//            src/phase2/gpu_lp_boundary.cu:195-240); rows longer than kChunk are split into queued chunks
-//   bnd      degree-bucketed boundary test of every stamped vertex (thread / warp / block per vertex),
-//            stopping at the first differently-labelled neighbour (gpu_lp_boundary.cu:251-270); a
-//            boundary vertex becomes a selection record keyed (degree asc|desc by RE[label], id)
-//   need/select  per label the ceil(e^(-t/5) n) smallest keys (gpu_lp_boundary.cu:244, 277-301)
-//   split    selected vertices form the next window and are routed to a decision class
+//            src/phase2/gpu_lp_boundary.cu:195-240): thread per short row, warp per longer row; a hub's
+//            row is walked only when the hub enters or leaves the window, keeping hubwin[u] (window hubs
+//            whose rows hold u) current
+//   bnd      degree-bucketed candidacy (stamp / hubwin, or a pull walk that stops at the first window
+//            neighbour) and the boundary test from the maintained count of differently-labelled neighbours
+//            (gpu_lp_boundary.cu:251-270); a boundary vertex becomes a selection record keyed (degree
+//            asc|desc by RE[label], id), and the first radix digit of the keys is histogrammed per label
+//   need/select  per label the ceil(e^(-t/5) n) smallest keys (gpu_lp_boundary.cu:244, 277-301); the
+//            selection's partition emits the next window and routes it to the decision classes
 //   decide   boundaryLPKernel_unified's rule (gpu_lp_boundary.cu:354-426) for the selected vertices only:
-//            thread per vertex (deg <= 16, pairwise counts), warp per vertex (shared histogram), block per
-//            vertex (deg > 4096); a changed label is parked in newlab[] (Jacobi: nothing moves yet)
+//            persistent warps over hub row chunks, warp-class groups and thread-class groups; on symmetric
+//            graphs the hubs' label counts are kept current instead of recounted; a changed label is
+//            parked in newlab[] (Jacobi: nothing moves yet)
 //   update   (symmetric graphs) edge cut, per-part intra arcs and vertex counts change only through the
 //            movers' arcs: each arc is re-scored with both endpoints' old and new labels, weighted 2 when
 //            the neighbour stays (its reverse arc is not visited) and 1 when it moves too.  Asymmetric
@@ -45,7 +49,10 @@ __global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
         cn->nbnd = 0;
         cn->nwin[t & 1] = 0;
         cn->nchanged = 0;
-        cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
+        for (int c = 0; c < 3; ++c) {
+            cn->ndec_prev[c] = t > 1 ? cn->ndec[c] : 0;
+            cn->ndec[c] = 0;
+        }
         cn->nchunk = 0;
         cn->nhubq = 0;
         cn->nhubw = 0;
@@ -73,10 +80,9 @@ __device__ __forceinline__ void stamp_once(const Buffers &b, int u, int t) {
     if (b.stamp[u] != t) b.stamp[u] = t;
 }
 
-// Warp per vertex of the previous window: stamp it and its first kChunk neighbours; the rest of a long row
-// is queued in kChunk pieces for k_mark_chunks.  Without walk_hubs a hub (deg > kLargeDeg) stamps only
-// itself: its neighbours are candidates through hubwin (k_hubwin_*).
-__global__ void k_mark(Buffers b, int t, int walk_hubs) {
+// dmolp_window_select's marking: warp per vertex of the previous window (win list): stamp it and its
+// first kChunk neighbours; the rest of a long row is queued in kChunk pieces for k_mark_chunks.
+__global__ void k_mark(Buffers b, int t) {
     if (b.ctrl->stopped || b.ctrl->pull) return;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
@@ -85,8 +91,7 @@ __global__ void k_mark(Buffers b, int t, int walk_hubs) {
     unsigned long long rd = 0;
     for (int i = gw; i < n; i += nw) {
         const int v = prev[i];
-        int64_t s = b.off[v], e = b.off[v + 1];
-        if (!walk_hubs && e - s > kLargeDeg) e = s;
+        const int64_t s = b.off[v], e = b.off[v + 1];
         if (lane == 0) {
             b.stamp[v] = t;
             for (int64_t c = s + kChunk; c < e; c += kChunk) {
@@ -114,6 +119,54 @@ __global__ void k_mark_chunks(Buffers b, int t) {
         const int64_t e = rowe - s > kChunk ? s + kChunk : rowe;
         warp_row(b.col, s, e, lane, [&](int u) { stamp_once(b, u, t); }, [] { return false; });
         if (lane == 0) rd += (unsigned long long)(e - s);
+    }
+    rd = warp_sum_u64(rd);
+    if (lane == 0 && rd) atomicAdd(&b.rec[t - 1].arcs_mark, rd);
+}
+
+// The loop's marking: the previous window by decision class (dec[c], ndec_prev[c]; the lists are rewritten
+// only by this iteration's selection, after the marking).  Blocks [0, g0): thread per vertex of class 0
+// (rows of at most kDecSmall arcs), then the hubs (class 2), which stamp only themselves -- their
+// neighbours are candidates through hubwin; blocks [g0, grid): warp per vertex of class 1.
+__global__ void __launch_bounds__(256, 5) k_mark_win(Buffers b, int t, int g0) {
+    if (b.ctrl->stopped || b.ctrl->pull) return;
+    const LpCounters *cn = b.cnt;
+    const int lane = threadIdx.x & 31;
+    unsigned long long rd = 0;
+    if ((int)blockIdx.x < g0) {
+        const int stride = g0 * blockDim.x;
+        const int n0 = cn->ndec_prev[0];
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n0; i += stride) {
+            const int v = b.dec[0][i];
+            const int64_t s = b.off[v];
+            const int deg = (int)(b.off[v + 1] - s);
+            b.stamp[v] = t;
+            rd += (unsigned long long)deg;
+            for (int j = 0; j < deg; j += 8) {  // eight ids in flight, then their stamps stored
+                int u[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(b.col + s + j + q) : -1;
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (u[q] >= 0) b.stamp[u[q]] = t;
+            }
+        }
+        const int n2 = cn->ndec_prev[2];
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) b.stamp[b.dec[2][i]] = t;
+    } else {
+        const int gw = (((int)blockIdx.x - g0) * (int)blockDim.x + (int)threadIdx.x) >> 5;
+        const int nw = (((int)gridDim.x - g0) * (int)blockDim.x) >> 5;
+        const int n1 = cn->ndec_prev[1];
+        for (int i = gw; i < n1; i += nw) {
+            const int v = b.dec[1][i];
+            const int64_t s = b.off[v], e = b.off[v + 1];
+            if (lane == 0) {
+                b.stamp[v] = t;
+                rd += (unsigned long long)(e - s);
+            }
+            warp_row_wide(b.col, s, e, lane, [](int) { return 0; }, [&](int u, int) { b.stamp[u] = t; },
+                          [] { return false; });
+        }
     }
     rd = warp_sum_u64(rd);
     if (lane == 0 && rd) atomicAdd(&b.rec[t - 1].arcs_mark, rd);
@@ -160,6 +213,8 @@ __global__ void k_hubwin_apply(Buffers b, int t) {
 struct BndArgs {
     int t, all, ibits, maxdeg;
     int hubwin;  // hubwin is current: hubs of the previous window make their neighbours candidates
+    unsigned int *hist;  // when set: first-digit histogram of the boundary records for the selection (k <= 32)
+    int hshift;          // its digit: bits [hshift, hshift + 8) of the key
     int nb0, nb1, nb2;
     int g0, g1;  // block split: [0,g0) thread class, [g0,g0+g1) warp class, rest block class
 };
@@ -183,10 +238,13 @@ __device__ __forceinline__ void put_slot(const Buffers &b, int pos, bool isb, in
 // differently-labelled neighbour: ndiff[v] > 0, a count kept exact by the statistics pass and by k_update
 // (symmetric graphs) or by the full pass after every move (other graphs).  So only pull-mode candidacy
 // walks rows; at t = 1 and in push mode every record slot costs a handful of per-vertex reads.
-__global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
+__global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
     if (b.ctrl->stopped) return;
-    extern __shared__ int s_npart[];  // [k] boundary records per label in this block
+    extern __shared__ int s_npart[];  // [k] boundary records per label in this block, then [k * 256] histogram
+    unsigned int *s_hist = reinterpret_cast<unsigned int *>(s_npart + k);
     for (int p = threadIdx.x; p < k; p += blockDim.x) s_npart[p] = 0;
+    if (a.hist)
+        for (int i = threadIdx.x; i < k * kRadix; i += blockDim.x) s_hist[i] = 0u;
     __syncthreads();
     const bool pull = !a.all && b.ctrl->pull;
     const int tp = a.t - 1;
@@ -199,12 +257,15 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
             ++nc;
             te += (unsigned long long)deg;
         }
+        uint64_t key = 0;
         if (isb) {
             own = b.label[v];
             ++nbd;
             atomicAdd(&s_npart[own], 1);
+            key = sel_key(b, own, deg, v, a.ibits, a.maxdeg);
+            if (a.hist) atomicAdd(&s_hist[own * kRadix + (int)((key >> a.hshift) & (kRadix - 1))], 1u);
         }
-        put_slot(b, pos, isb, own, isb ? sel_key(b, own, deg, v, a.ibits, a.maxdeg) : 0);
+        put_slot(b, pos, isb, own, key);
     };
     if (!pull) {
         // ---- every record slot, thread per slot ----
@@ -223,10 +284,14 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
             const int deg = (int)(b.off[v + 1] - s);
             if (!cand) {
                 int j = 0;
-                for (; j < deg && !cand; j += 4) {
+                for (; j < deg && !cand; j += 8) {  // eight ids, then their window stamps, in flight
+                    int u[8], st[8];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        if (j + q < deg) cand |= b.sstamp[__ldg(b.col + s + j + q)] == tp;
+                    for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(b.col + s + j + q) : -1;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) st[q] = u[q] >= 0 ? b.sstamp[u[q]] : tp - 1;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) cand |= st[q] == tp;
                 }
                 rd += (unsigned long long)(j < deg ? j : deg);
             }
@@ -244,8 +309,9 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
             bool cand = cand0;
             if (!cand0) {  // warp-uniform
                 bool fs = false;
-                const int64_t r = warp_row(b.col, s, e, lane, [&](int u) { fs |= (b.sstamp[u] == tp); },
-                                           [&] { return __any_sync(DMOLP_FULL_MASK, fs); });
+                const int64_t r = warp_row_wide(b.col, s, e, lane, [&](int u) { return b.sstamp[u]; },
+                                                [&](int, int st) { fs |= st == tp; },
+                                                [&] { return __any_sync(DMOLP_FULL_MASK, fs); });
                 cand = __any_sync(DMOLP_FULL_MASK, fs);
                 if (lane == 0) rd += (unsigned long long)r;
             }
@@ -264,10 +330,14 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
             if (!cand0) {  // block-uniform
                 for (j0 = s; j0 < e; j0 += blockDim.x * 4) {
                     bool fs = false;
+                    int u[4];
+#pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int64_t j = j0 + q * blockDim.x + threadIdx.x;
-                        if (j < e) fs |= (b.sstamp[__ldcs(b.col + j)] == tp);
+                        u[q] = j < e ? __ldcs(b.col + j) : -1;
                     }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) fs |= u[q] >= 0 && b.sstamp[u[q]] == tp;
                     if (__syncthreads_or(fs)) {
                         cand = true;
                         j0 += blockDim.x * 4;
@@ -295,6 +365,9 @@ __global__ void __launch_bounds__(256) k_bnd(Buffers b, BndArgs a, int k) {
     __syncthreads();
     for (int p = threadIdx.x; p < k; p += blockDim.x)
         if (s_npart[p]) atomicAdd(&b.npart[p], s_npart[p]);
+    if (a.hist)
+        for (int i = threadIdx.x; i < k * kRadix; i += blockDim.x)
+            if (s_hist[i]) atomicAdd(&a.hist[i], s_hist[i]);
 }
 
 // ------------------------------------------------------------------------------------ need
@@ -326,35 +399,12 @@ __device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
 __device__ __forceinline__ int grab_issue(int *ctr, int lane) { return lane == 0 ? atomicAdd(ctr, 1) : 0; }
 __device__ __forceinline__ int grab_take(int pending) { return __shfl_sync(DMOLP_FULL_MASK, pending, 0); }
 
-// Lane-private label counts (eff <= 32) of the arcs [s, e): a step loads, per lane, the row's scalar head
-// and tail (first step only) and two 16-byte words of its body, then gathers all their labels, then counts,
-// so a row of up to 262 arcs costs one dependent load pair.
+// Lane-private label counts (eff <= 32) of the arcs [s, e).
 __device__ __forceinline__ void count_priv(const int32_t *__restrict__ col, const int32_t *__restrict__ label,
                                            int64_t s, int64_t e, int lane, int eff, int *h) {
-    int64_t a = (s + 3) & ~int64_t(3);
-    if (a > e) a = e;
-    const int64_t qe = e >> 2;  // body: int4 words [a/4, e/4)
-    const int64_t t0 = a > (qe << 2) ? a : (qe << 2);
-    const int4 *c4 = reinterpret_cast<const int4 *>(col);
-    bool first = true;
-    for (int64_t q0 = a >> 2; first || q0 < qe; q0 += 64) {
-        int u[10];
-        u[8] = first && s + lane < a ? __ldg(col + s + lane) : -1;
-        u[9] = first && t0 + lane < e ? __ldg(col + t0 + lane) : -1;
-        const int64_t q = q0 + lane;
-        int4 x = make_int4(-1, -1, -1, -1), y = make_int4(-1, -1, -1, -1);
-        if (q < qe) x = __ldcs(c4 + q);
-        if (q + 32 < qe) y = __ldcs(c4 + q + 32);
-        u[0] = x.x; u[1] = x.y; u[2] = x.z; u[3] = x.w;
-        u[4] = y.x; u[5] = y.y; u[6] = y.z; u[7] = y.w;
-        int l[10];
-#pragma unroll
-        for (int r = 0; r < 10; ++r) l[r] = u[r] >= 0 ? label[u[r]] : -1;
-#pragma unroll
-        for (int r = 0; r < 10; ++r)
-            if ((unsigned)l[r] < (unsigned)eff) h[l[r] * 32 + ((lane + l[r]) & 31)] += 1;
-        first = false;
-    }
+    warp_row_wide(col, s, e, lane, [&](int u) { return label[u]; }, [&](int, int l) {
+        if ((unsigned)l < (unsigned)eff) h[l * 32 + ((lane + l) & 31)] += 1;
+    }, [] { return false; });
 }
 
 // Label counts of the arcs [s, e) into the warp's region: lane-private counters (eff <= 32) or a shared
@@ -589,7 +639,7 @@ __global__ void k_hub_final(Buffers b, int eff, int t) {
 // the reverse arc (u,v) changes the same way but is never visited; weight 1 when u moves (or u == v):
 // (u,v) is visited from u's side.  Vertex counts move by one.  A hub neighbour u sees v's label go from
 // a to c: its row of label counts (labels < eff) moves by one.
-__global__ void k_update(Buffers b, int k, int eff, int t) {
+__global__ void __launch_bounds__(256, 3) k_update(Buffers b, int k, int eff, int t) {
     if (b.ctrl->stopped) return;
     extern __shared__ unsigned long long sacc[];  // [2k]: vertex-count deltas, intra-arc deltas
     for (int p = threadIdx.x; p < 2 * k; p += blockDim.x) sacc[p] = 0;
@@ -605,9 +655,10 @@ __global__ void k_update(Buffers b, int k, int eff, int t) {
         const int64_t s = b.off[v], e = b.off[v + 1];
         long long in_c = 0, out_a = 0, dc = 0;
         int dv = 0;
-        warp_row(b.col, s, e, lane, [&](int u) {
-            const int lo = b.label[u];
-            const int nu = b.newlab[u];
+        warp_row_wide(b.col, s, e, lane, [&](int u) { return make_int3(b.label[u], b.newlab[u], b.hidx[u]); },
+                      [&](int u, int3 g) {
+            const int lo = g.x;
+            const int nu = g.y;
             const int ln = nu >= 0 ? nu : lo;
             const int w = nu >= 0 ? 1 : 2;
             dc += w * ((int)(c != ln) - (int)(a != lo));
@@ -618,7 +669,7 @@ __global__ void k_update(Buffers b, int k, int eff, int t) {
             const int du = (int)(ln != c) - (int)(lo != a);
             if (du) atomicAdd(&b.ndiff[u], du);
             if (nu < 0) dv += (int)(c != lo) - (int)(a != lo);
-            const int hu = b.hidx[u];
+            const int hu = g.z;
             if (hu >= 0) {
                 int32_t *row = b.hh + (size_t)hu * DMOLP_MAX_K;
                 if ((unsigned)a < (unsigned)eff) atomicAdd(&row[a], -1);
@@ -692,13 +743,22 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
         for (int i = (bx - a.gv) * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
             const int v = b.bucket[0][i];
             const int lv = b.label[v];
-            const int64_t s = b.off[v], e = b.off[v + 1];
+            const int64_t s = b.off[v];
+            const int deg = (int)(b.off[v + 1] - s);
             unsigned int same = 0, diff = 0;
-            for (int64_t j = s; j < e; ++j) {
-                const int lu = b.label[__ldg(b.col + j)];
-                bad |= (unsigned)lu >= (unsigned)k;
-                same += (lu == lv);
-                diff += (lu != lv);
+            for (int j = 0; j < deg; j += 8) {  // eight ids, then their eight labels, in flight
+                int u[8], l[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(b.col + s + j + q) : -1;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) l[q] = u[q] >= 0 ? b.label[u[q]] : lv;
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (u[q] >= 0) {
+                        bad |= (unsigned)l[q] >= (unsigned)k;
+                        same += (l[q] == lv);
+                        diff += (l[q] != lv);
+                    }
             }
             cut += diff;
             b.ndiff[v] = (int)diff;
@@ -711,8 +771,7 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
             const int v = b.bucket[1][i];
             const int lv = b.label[v];
             unsigned int same = 0, diff = 0;
-            warp_row(b.col, b.off[v], b.off[v + 1], lane, [&](int u) {
-                const int lu = b.label[u];
+            warp_row_wide(b.col, b.off[v], b.off[v + 1], lane, [&](int u) { return b.label[u]; }, [&](int, int lu) {
                 bad |= (unsigned)lu >= (unsigned)k;
                 same += (lu == lv);
                 diff += (lu != lv);
@@ -735,11 +794,22 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
             const int lv = b.label[v];
             const int64_t s = b.off[v], e = b.off[v + 1];
             unsigned int same = 0, diff = 0;
-            for (int64_t j = s + threadIdx.x; j < e; j += blockDim.x) {
-                const int lu = b.label[__ldcs(b.col + j)];
-                bad |= (unsigned)lu >= (unsigned)k;
-                same += (lu == lv);
-                diff += (lu != lv);
+            for (int64_t j0 = s; j0 < e; j0 += 4 * blockDim.x) {  // four ids per thread, then their labels
+                int u[4], l[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int64_t j = j0 + q * blockDim.x + threadIdx.x;
+                    u[q] = j < e ? __ldcs(b.col + j) : -1;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) l[q] = u[q] >= 0 ? b.label[u[q]] : lv;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (u[q] >= 0) {
+                        bad |= (unsigned)l[q] >= (unsigned)k;
+                        same += (l[q] == lv);
+                        diff += (l[q] != lv);
+                    }
             }
             cut += diff;
             for (int o = 16; o > 0; o >>= 1) {
@@ -992,11 +1062,17 @@ int grid_for(dmolp_ctx *c) { return c->num_sms * kGridPerSm; }
 
 int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 
-BndArgs bnd_args(dmolp_ctx *c, int t, int all, int hubwin) {
+constexpr int kBndHistMaxK = 32;  // k_bnd builds the selection's first histogram up to this many labels
+
+// hist_for_select: k_bnd adds the first-digit histogram of its records to histogram buffer 0 of the
+// selection that follows (k <= kBndHistMaxK).
+BndArgs bnd_args(dmolp_ctx *c, int t, int all, int hubwin, int k, bool hist_for_select) {
     BndArgs a;
     a.t = t;
     a.all = all;
     a.hubwin = hubwin;
+    a.hist = hist_for_select && k <= kBndHistMaxK ? c->b.hist : nullptr;
+    a.hshift = select_first_shift(c->dbits + c->ibits);
     a.ibits = c->ibits;
     a.maxdeg = (int)c->maxdeg;
     a.nb0 = c->nb[0];
@@ -1007,6 +1083,8 @@ BndArgs bnd_args(dmolp_ctx *c, int t, int all, int hubwin) {
     a.g1 = clampi((c->nb[1] + 7) / 8, 1, cap);
     return a;
 }
+
+size_t bnd_smem(int k, const BndArgs &a) { return (size_t)k * sizeof(int) + (a.hist ? (size_t)k * kRadix * sizeof(int) : 0); }
 
 int bnd_grid(dmolp_ctx *c, const BndArgs &a) { return a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
 
@@ -1147,10 +1225,11 @@ void lp_init_end(dmolp_ctx *c, int mode) {
 }
 
 // The window of iteration t as the selection emits it (see SplitArgs).
-SplitArgs split_args(const Buffers &b, int t, int eff) {
+SplitArgs split_args(const dmolp_ctx *c, const Buffers &b, int t, int eff) {
     SplitArgs sp;
-    sp.vertex = b.ball;
-    sp.off = b.off;
+    sp.RE = b.RE;
+    sp.ibits = c->ibits;
+    sp.maxdeg = (int)c->maxdeg;
     sp.sstamp = b.sstamp;
     sp.win = b.win[t & 1];
     sp.nwin = &b.cnt->nwin[t & 1];
@@ -1162,18 +1241,17 @@ SplitArgs split_args(const Buffers &b, int t, int eff) {
     return sp;
 }
 
-static_assert(kChunk >= kLargeDeg, "the loop's marking queues no row chunks: its longest walked row is kLargeDeg");
-
 void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     Buffers &b = c->b;
     const int grid = grid_for(c);
     const int *stopped = &b.ctrl->stopped;
+    bool hist_ready = false;
     k_lp_begin<<<1, 256, 0, c->stream>>>(b, L.k, t, (long long)c->narcs);
     c->launches += 1;
     if (t > 1) {
-        // window rows up to kChunk = kLargeDeg arcs (no chunks to queue); hubs through hubwin
+        // the previous window by decision class; hubs through hubwin
         ProfScope ps(c, 2, t);
-        k_mark<<<grid, kBlock, 0, c->stream>>>(b, t, 0);
+        k_mark_win<<<grid, kBlock, 0, c->stream>>>(b, t, grid / 2);
         c->launches += 1;
         if (c->nb[2] > 0) {
             k_hubwin_queue<<<clampi((c->nb[2] + 255) / 256, 1, grid), kBlock, 0, c->stream>>>(b, t, c->nb[2]);
@@ -1183,15 +1261,17 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
     }
     {
         ProfScope ps(c, 0, t);
-        const BndArgs a = bnd_args(c, t, t == 1, c->nb[2] > 0);  // hubwin is cleared only for graphs with hubs
-        k_bnd<<<bnd_grid(c, a), kBlock, L.k * sizeof(int), c->stream>>>(b, a, L.k);
+        // hubwin is cleared only for graphs with hubs
+        const BndArgs a = bnd_args(c, t, t == 1, c->nb[2] > 0, L.k, true);
+        k_bnd<<<bnd_grid(c, a), kBlock, bnd_smem(L.k, a), c->stream>>>(b, a, L.k);
+        hist_ready = a.hist != nullptr;
     }
     k_lp_need<<<1, 256, 0, c->stream>>>(b, L.k, t);
     c->launches += 2;
     {
         ProfScope ps(c, 4, t);
-        const SplitArgs sp = split_args(b, t, L.eff);
-        select_smallest(c, b.bown, b.bkey, &b.cnt->npos, L.k, c->dbits + c->ibits, b.bsel, stopped, &sp);
+        const SplitArgs sp = split_args(c, b, t, L.eff);
+        select_smallest(c, b.bown, b.bkey, &b.cnt->npos, L.k, c->dbits + c->ibits, b.bsel, stopped, &sp, hist_ready);
     }
     {
         ProfScope ps(c, 1, t);
@@ -1222,14 +1302,14 @@ void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int n
     Buffers &b = c->b;
     const int grid = grid_for(c);
     k_ws_begin<<<1, 256, 0, c->stream>>>(b, k, t, nprev);
-    k_mark<<<grid, kBlock, 0, c->stream>>>(b, t, 1);
+    k_mark<<<grid, kBlock, 0, c->stream>>>(b, t);
     k_mark_chunks<<<grid, kBlock, 0, c->stream>>>(b, t);
-    const BndArgs a = bnd_args(c, t, 0, 0);
-    k_bnd<<<bnd_grid(c, a), kBlock, k * sizeof(int), c->stream>>>(b, a, k);
+    const BndArgs a = bnd_args(c, t, 0, 0, k, true);
+    k_bnd<<<bnd_grid(c, a), kBlock, bnd_smem(k, a), c->stream>>>(b, a, k);
     k_lp_need<<<1, 256, 0, c->stream>>>(b, k, t);
     c->launches += 5;
-    const SplitArgs sp = split_args(b, t, DMOLP_MAX_K);
-    select_smallest(c, b.bown, b.bkey, &b.cnt->npos, k, c->dbits + c->ibits, b.bsel, nullptr, &sp);
+    const SplitArgs sp = split_args(c, b, t, DMOLP_MAX_K);
+    select_smallest(c, b.bown, b.bkey, &b.cnt->npos, k, c->dbits + c->ibits, b.bsel, nullptr, &sp, a.hist != nullptr);
 }
 
 // dmolp_lp_apply: window in b.cand (n entries), penalties in b.tpen; movers reported in bv/bnew.

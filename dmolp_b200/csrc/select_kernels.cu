@@ -41,6 +41,7 @@ struct SelArgs {
     const int *stopped;
     SplitArgs sp;  // used when has_split: selected slots go straight to the LP window
     int has_split;
+    int hist_ready;  // the first digit's histogram is already in buffer 0
 };
 
 // Sense-counting grid barrier (all blocks are resident: cooperative launch).  A wait that runs past
@@ -109,8 +110,8 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
     const int lo = blockIdx.x * cap;
     int my_n = max(0, min(n0, lo + cap) - lo);  // pass 0: record slots [lo, lo + my_n)
     __syncthreads();
-    // ---- histogram of the first digit over this block's record slots ----
-    {
+    // ---- histogram of the first digit over this block's record slots (unless the records' writer built it) ----
+    if (!a.hist_ready) {
         const int shift = a.top - kRadixBits;
         for (int i0 = 0; i0 < my_n; i0 += blockDim.x) {
             const int i = i0 + threadIdx.x;
@@ -118,13 +119,15 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
             if (i < my_n) {
                 const int r = lo + i;
                 const int p = a.seg[r];
-                if (p >= 0 && s_need[p] > 0) bin = p * kRadix + (int)((a.key[r] >> shift) & (kRadix - 1));
+                const uint64_t key = a.key[r];  // loaded with seg (an empty slot's stale key is not used)
+                if (p >= 0 && s_need[p] > 0) bin = p * kRadix + (int)((key >> shift) & (kRadix - 1));
             }
             hist_add(bin, use_smem, shist, a.ghist);
         }
         hist_flush(use_smem, shist, a.ghist, nbins);
     }
     unsigned long long te = 0;  // degrees of the selected vertices (has_split)
+    const uint64_t vmask = a.has_split ? (1ull << a.sp.ibits) - 1 : 0;
     int pass = 0;
     for (; pass < a.npass; ++pass) {
         const int shift = a.top - kRadixBits * (pass + 1);
@@ -202,11 +205,12 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
             const int i = i0 + threadIdx.x;
             bool keep = false, take = false;
             int r = 0, bin = -(lane + 1), p = -1;
+            uint64_t key = 0;
             if (i < my_n) {
                 r = src ? src[i] : lo + i;
                 p = a.seg[r];
+                key = a.key[r];
                 if (p >= 0) {  // skip empty record slots
-                    const uint64_t key = a.key[r];
                     const int d = (int)((key >> shift) & (kRadix - 1));
                     if (d < s_below[p]) {
                         a.sel[r] = 1;
@@ -227,18 +231,36 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
             if (a.has_split) {  // the LP window: stamp, append, decision class (all lanes take part)
                 int v = 0, cls = -1;
                 if (take) {
-                    v = a.sp.vertex[r];
+                    v = (int)(key & vmask);
+                    const int dk = (int)(key >> a.sp.ibits);
+                    const int deg = __ldg(a.sp.RE + p) > 1.0 ? a.sp.maxdeg - dk : dk;
                     a.sp.sstamp[v] = a.sp.t;
-                    const int deg = (int)(a.sp.off[v + 1] - a.sp.off[v]);
                     te += (unsigned long long)deg;
                     cls = dec_class(deg, p, a.sp.eff);
                 }
-                const int slot = warp_append(a.sp.nwin, take);
-                if (take) a.sp.win[slot] = v;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const int s2 = warp_append(&a.sp.ndec[c], cls == c);
-                    if (cls == c) a.sp.dec[c][s2] = v;
+                // the four appends (window, classes 0-2) with their atomics in flight together: lane j
+                // reserves list j's slots
+                const unsigned mw = __ballot_sync(DMOLP_FULL_MASK, take);
+                if (mw) {
+                    const unsigned m0 = __ballot_sync(DMOLP_FULL_MASK, cls == 0);
+                    const unsigned m1 = __ballot_sync(DMOLP_FULL_MASK, cls == 1);
+                    const unsigned m2 = __ballot_sync(DMOLP_FULL_MASK, cls == 2);
+                    int base = 0;
+                    if (lane < 4) {
+                        const unsigned mm = lane == 0 ? mw : (lane == 1 ? m0 : (lane == 2 ? m1 : m2));
+                        if (mm) base = atomicAdd(lane == 0 ? a.sp.nwin : &a.sp.ndec[lane - 1], __popc(mm));
+                    }
+                    const int bw = __shfl_sync(DMOLP_FULL_MASK, base, 0);
+                    const int b0 = __shfl_sync(DMOLP_FULL_MASK, base, 1);
+                    const int b1 = __shfl_sync(DMOLP_FULL_MASK, base, 2);
+                    const int b2 = __shfl_sync(DMOLP_FULL_MASK, base, 3);
+                    if (take) {
+                        const unsigned below = (1u << lane) - 1;
+                        a.sp.win[bw + __popc(mw & below)] = v;
+                        const unsigned mc = cls == 0 ? m0 : (cls == 1 ? m1 : m2);
+                        const int bc = cls == 0 ? b0 : (cls == 1 ? b1 : b2);
+                        a.sp.dec[cls][bc + __popc(mc & below)] = v;
+                    }
                 }
             }
         }
@@ -260,7 +282,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
 }  // namespace
 
 void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, const int *n_dev, int nseg, int keybits,
-                     uint8_t *sel, const int *stopped, const SplitArgs *split) {
+                     uint8_t *sel, const int *stopped, const SplitArgs *split, bool first_hist_ready) {
     const int npass = (keybits + kRadixBits - 1) / kRadixBits;
     const bool smem_hist = nseg <= kSmemSegMax;
     const size_t smem = (smem_hist ? (size_t)nseg * kRadix * sizeof(unsigned int) : 0) + 3 * (size_t)nseg * sizeof(int);
@@ -279,6 +301,7 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
     a.ctl = c->b.ctrl;
     a.stopped = stopped;
     a.has_split = split != nullptr;
+    a.hist_ready = first_hist_ready ? 1 : 0;
     if (split) a.sp = *split;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)c->num_sms);  // one block per SM, all resident (cooperative launch)
