@@ -250,8 +250,9 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
     const int tp = a.t - 1;
     const int lane = threadIdx.x & 31;
     unsigned long long te = 0, rd = 0, nc = 0, nbd = 0;
-    auto finish = [&](int pos, int v, bool cand, int deg) {
-        const bool isb = cand && b.ndiff[v] > 0;
+    // nd = ndiff[v] and lv = label[v], loaded by the caller ahead of the candidacy test
+    auto finish = [&](int pos, int v, bool cand, int deg, int nd, int lv) {
+        const bool isb = cand && nd > 0;
         int own = 0;
         if (cand) {
             ++nc;
@@ -259,7 +260,7 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
         }
         uint64_t key = 0;
         if (isb) {
-            own = b.label[v];
+            own = lv;
             ++nbd;
             atomicAdd(&s_npart[own], 1);
             key = sel_key(b, own, deg, v, a.ibits, a.maxdeg);
@@ -272,50 +273,77 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
         const int n = a.nb0 + a.nb1 + a.nb2;
         for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += gridDim.x * blockDim.x) {
             const int v = b.ball[pos];
-            const bool cand = a.all || b.stamp[v] == a.t || (a.hubwin && b.hubwin[v] > 0);
-            finish(pos, v, cand, cand ? (int)(b.off[v + 1] - b.off[v]) : 0);
+            const int st = b.stamp[v], hw = a.hubwin ? b.hubwin[v] : 0, nd = b.ndiff[v], lv = b.label[v];
+            const bool cand = a.all || st == a.t || hw > 0;
+            finish(pos, v, cand, cand ? (int)(b.off[v + 1] - b.off[v]) : 0, nd, lv);
         }
     } else if ((int)blockIdx.x < a.g0) {
-        // ---- pull, thread per vertex (deg <= kSmallDeg): window stamps of the row, 4 at a time ----
+        // ---- pull, thread per vertex (deg <= kSmallDeg): window stamps of the row, 8 at a time ----
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
             const int v = b.bucket[0][i];
-            bool cand = b.sstamp[v] == tp || (a.hubwin && b.hubwin[v] > 0);
+            const int st = b.sstamp[v], hw = a.hubwin ? b.hubwin[v] : 0, nd = b.ndiff[v], lv = b.label[v];
+            bool cand = st == tp || hw > 0;
             const int64_t s = b.off[v];
             const int deg = (int)(b.off[v + 1] - s);
             if (!cand) {
                 int j = 0;
                 for (; j < deg && !cand; j += 8) {  // eight ids, then their window stamps, in flight
-                    int u[8], st[8];
+                    int u[8], sv[8];
 #pragma unroll
                     for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(b.col + s + j + q) : -1;
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) st[q] = u[q] >= 0 ? b.sstamp[u[q]] : tp - 1;
+                    for (int q = 0; q < 8; ++q) sv[q] = u[q] >= 0 ? b.sstamp[u[q]] : tp - 1;
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) cand |= st[q] == tp;
+                    for (int q = 0; q < 8; ++q) cand |= sv[q] == tp;
                 }
                 rd += (unsigned long long)(j < deg ? j : deg);
             }
-            finish(i, v, cand, deg);
+            finish(i, v, cand, deg, nd, lv);
         }
     } else if ((int)blockIdx.x < a.g0 + a.g1) {
-        // ---- pull, warp per vertex ----
+        // ---- pull, 32 vertices (deg in (kSmallDeg, kLargeDeg]) per warp: each lane checks the first 8 arcs
+        //      of its row; the rows still undecided are walked by the whole warp, one after another ----
         const int wpb = blockDim.x >> 5;
         const int gw = ((int)blockIdx.x - a.g0) * wpb + (threadIdx.x >> 5), nw = a.g1 * wpb;
-        for (int i = gw; i < a.nb1; i += nw) {
-            const int pos = a.nb0 + i;
-            const int v = b.bucket[1][i];
-            const bool cand0 = b.sstamp[v] == tp || (a.hubwin && b.hubwin[v] > 0);
-            const int64_t s = b.off[v], e = b.off[v + 1];
-            bool cand = cand0;
-            if (!cand0) {  // warp-uniform
-                bool fs = false;
-                const int64_t r = warp_row_wide(b.col, s, e, lane, [&](int u) { return b.sstamp[u]; },
-                                                [&](int, int st) { fs |= st == tp; },
-                                                [&] { return __any_sync(DMOLP_FULL_MASK, fs); });
-                cand = __any_sync(DMOLP_FULL_MASK, fs);
-                if (lane == 0) rd += (unsigned long long)r;
+        for (int i0 = gw * 32; i0 < a.nb1; i0 += nw * 32) {
+            const int i = i0 + lane;
+            const bool valid = i < a.nb1;
+            int v = 0, nd = 0, lv = 0;
+            int64_t s = 0, e = 0;
+            bool cand = false;
+            if (valid) {
+                v = b.bucket[1][i];
+                const int st = b.sstamp[v], hw = a.hubwin ? b.hubwin[v] : 0;
+                nd = b.ndiff[v];
+                lv = b.label[v];
+                s = b.off[v];
+                e = b.off[v + 1];
+                cand = st == tp || hw > 0;
+                if (!cand) {  // deg > kSmallDeg >= 8: the first eight ids exist
+                    int u[8], sv[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) u[q] = __ldg(b.col + s + q);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) sv[q] = b.sstamp[u[q]];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) cand |= sv[q] == tp;
+                    rd += 8;
+                }
             }
-            if (lane == 0) finish(pos, v, cand, (int)(e - s));
+            for (unsigned m = __ballot_sync(DMOLP_FULL_MASK, valid && !cand); m; m &= m - 1) {
+                const int j = __ffs(m) - 1;
+                const int64_t sj = __shfl_sync(DMOLP_FULL_MASK, s, j) + 8, ej = __shfl_sync(DMOLP_FULL_MASK, e, j);
+                bool fs = false;
+                const int64_t r = warp_row_wide(b.col, sj, ej, lane, [&](int u) { return b.sstamp[u]; },
+                                                [&](int, int sv) { fs |= sv == tp; },
+                                                [&] { return __any_sync(DMOLP_FULL_MASK, fs); });
+                const bool cj = __any_sync(DMOLP_FULL_MASK, fs);
+                if (lane == j) {
+                    cand = cj;
+                    rd += (unsigned long long)r;
+                }
+            }
+            if (valid) finish(a.nb0 + i, v, cand, (int)(e - s), nd, lv);
         }
     } else {
         // ---- pull, block per vertex (deg > kLargeDeg) ----
@@ -336,8 +364,11 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
                         const int64_t j = j0 + q * blockDim.x + threadIdx.x;
                         u[q] = j < e ? __ldcs(b.col + j) : -1;
                     }
+                    int sv[4];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) fs |= u[q] >= 0 && b.sstamp[u[q]] == tp;
+                    for (int q = 0; q < 4; ++q) sv[q] = u[q] >= 0 ? b.sstamp[u[q]] : tp - 1;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) fs |= sv[q] == tp;
                     if (__syncthreads_or(fs)) {
                         cand = true;
                         j0 += blockDim.x * 4;
@@ -347,7 +378,7 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
             }
             if (threadIdx.x == 0) {
                 if (!cand0) rd += (unsigned long long)((j0 < e ? j0 : e) - s);
-                finish(pos, v, cand, (int)(e - s));
+                finish(pos, v, cand, (int)(e - s), b.ndiff[v], b.label[v]);
             }
             __syncthreads();
         }
@@ -878,9 +909,10 @@ __global__ void k_lp_end(Buffers b, int k, int t, long long narcs, int mode, int
         ch[DMOLP_MAX_K + p] = sll(b.intra[p]) / 2;
     }
     ctl->iters_run = t;
-    // the next iteration pulls when pushing would walk more than a quarter of all arcs (pulling finds the
-    // same candidates only when every arc has its reverse); hub rows are not walked by the push
-    ctl->pull = symmetric && (r.te_sel - r.te_hubsel) * 4ull > (unsigned long long)narcs;
+    // the next iteration pulls unless pushing would walk fewer than 1/16 of all arcs (pulling finds the
+    // same candidates only when every arc has its reverse); hub rows are not walked by the push.  Pulling
+    // mostly stops at a row's first arcs, so it wins until the window is small (measured on R-MAT 22).
+    ctl->pull = symmetric && (r.te_sel - r.te_hubsel) * 16ull > (unsigned long long)narcs;
     if (ctl->stop_now) {
         ctl->stopped = 1;
         ctl->stop_reason = ctl->stop_now;
