@@ -177,7 +177,7 @@ int run_block_graph(dmolp_ctx *c, const LpLaunch &L, int t0, int cnt) {
         DMOLP_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         c->capturing = true;
         c->capture_prof = dmolp_ctx::ProfEvents();
-        for (int t = t0; t < t0 + cnt; ++t) lp_iteration(c, L, t);
+        for (int t = t0; t < t0 + cnt; ++t) lp_iteration(c, L, t, t == t0, t == t0 + cnt - 1);
         c->capturing = false;
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         ge.kernels = c->launches - before;
@@ -1093,7 +1093,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
             st = run_block_graph(c, L, t0, cnt);
             if (st) return st;
         } else {
-            for (int t = t0; t < t0 + cnt; ++t) lp_iteration(c, L, t);
+            for (int t = t0; t < t0 + cnt; ++t) lp_iteration(c, L, t, t == t0, t == t0 + cnt - 1);
         }
         if (cfg->mode == DMOLP_LP_MODE_REF && t0 + cnt <= max_iter) {
             DMOLP_CUDA(cudaMemcpyAsync(&stopped, &b.ctrl->stopped, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

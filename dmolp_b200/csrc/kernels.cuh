@@ -20,9 +20,12 @@ std::vector<int> hubs_from_pairs(std::vector<std::pair<int, int>> sd);
 // The LP window straight out of the selection: the key of a selected record slot holds its vertex and
 // degree (key = (dk << ibits) | v, dk = maxdeg - deg when RE[label] > 1, else deg; label = its segment);
 // v is stamped sstamp[v] = t, appended to win / nwin and to its decision-class list dec[c] / ndec[c], and
-// its degree added to *te.
+// its degree added to *te.  The segments' needs are min(n, ceil(*ratio * n)) for n = npart[seg] (the
+// reference's ceil(e^(-t/5) n), gpu_lp_boundary.cu:244) instead of the need[] argument.
 struct SplitArgs {
     const double *RE;
+    const int32_t *npart;
+    const double *ratio;
     int32_t *sstamp;
     int32_t *win;
     int *nwin;
@@ -53,7 +56,7 @@ void lp_hub_index(dmolp_ctx *c);            // b.hidx from bucket[2] (once per g
 void lp_hub_counts(dmolp_ctx *c, int eff);  // label counts of every hub's row into b.hh (run start, symmetric)
 // One LP iteration.  On symmetric graphs the hub decisions read b.hh as lp_hub_counts left it and k_update
 // keeps it current; otherwise the selected hubs' rows are recounted.
-void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t);
+void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t, bool first, bool last);
 // one-off pieces used by dmolp_window_select / dmolp_lp_apply
 void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int nprev);
 void lp_apply_list(dmolp_ctx *c, int k, int eff, int n);

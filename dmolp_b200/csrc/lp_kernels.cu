@@ -2,7 +2,7 @@
 // launches with device-side counts, so a whole run is captured once into a CUDA graph and replayed:
 //
 //   begin    penalties from the current statistics (calculatePenalties, src/phase2/phase2.cpp:158-209);
-//            counter reset
+//            counter reset (with the previous iteration's end: one k_lp_turn between iterations)
 //   mark     stamp the previous window and its neighbours with t (expandBoundaryNodes' candidate set,
 //            src/phase2/gpu_lp_boundary.cu:195-240): thread per short row, warp per longer row; a hub's
 //            row is walked only when the hub enters or leaves the window, keeping hubwin[u] (window hubs
@@ -11,7 +11,7 @@
 //            neighbour) and the boundary test from the maintained count of differently-labelled neighbours
 //            (gpu_lp_boundary.cu:251-270); a boundary vertex becomes a selection record keyed (degree
 //            asc|desc by RE[label], id), and the first radix digit of the keys is histogrammed per label
-//   need/select  per label the ceil(e^(-t/5) n) smallest keys (gpu_lp_boundary.cu:244, 277-301); the
+//   select   per label the ceil(e^(-t/5) n) smallest keys (gpu_lp_boundary.cu:244, 277-301); the
 //            selection's partition emits the next window and routes it to the decision classes
 //   decide   boundaryLPKernel_unified's rule (gpu_lp_boundary.cu:354-426) for the selected vertices only:
 //            persistent warps over hub row chunks, warp-class groups and thread-class groups; on symmetric
@@ -39,9 +39,9 @@ namespace {
 constexpr int kGridPerSm = 4;
 
 // ------------------------------------------------------------------------------------ begin
-__global__ void k_lp_begin(Buffers b, int k, int t, long long narcs) {
+// Start of iteration t (one block): counters, the iteration record, penalties.
+__device__ void lp_begin(const Buffers &b, int k, int t, long long narcs) {
     LpControl *ctl = b.ctrl;
-    if (ctl->stopped) return;
     LpCounters *cn = b.cnt;
     for (int p = threadIdx.x; p < k; p += blockDim.x) b.npart[p] = 0;
     if (threadIdx.x == 0) {
@@ -401,22 +401,11 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
             if (s_hist[i]) atomicAdd(&a.hist[i], s_hist[i]);
 }
 
-// ------------------------------------------------------------------------------------ need
-// need[p] = min(n_p, ceil(e^(-t/5) * n_p))   (gpu_lp_boundary.cu:244, 296-297)
-__global__ void k_lp_need(Buffers b, int k, int t) {
-    if (b.ctrl->stopped) return;
-    const double ratio = b.ratiotab[t];
-    for (int p = threadIdx.x; p < k; p += blockDim.x) {
-        const int n = b.npart[p];
-        int m = (int)ceil(__dmul_rn(ratio, (double)n));
-        b.need[p] = m > n ? n : m;
-    }
-}
-
 // ------------------------------------------------------------------------------------ decide
 struct DecArgs {
     int t, eff;
-    int wstride;  // shared ints per warp: lane-private counters (eff <= 32), histogram, or byte counters
+    int wstride;    // shared ints per warp: lane-private counters (eff <= 32), histogram, or byte counters
+    int hub_ready;  // the hubs' label counts are current (kept from the movers): decide them first
 };
 
 __device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
@@ -482,6 +471,23 @@ __device__ __forceinline__ void hub_chunks(const Buffers &b, const int32_t *list
     }
 }
 
+// Decision of selected hub dec[2][i] from its row of label counts (warp; argmax over labels < eff); the
+// hubs' arcs are summed for the next iteration's push / pull choice.
+__device__ __forceinline__ void hub_decide(const Buffers &b, int i, int eff, int t, int lane) {
+    const int v = b.dec[2][i];
+    const int own = b.label[v];
+    const int32_t *row = b.hh + (size_t)b.hidx[v] * DMOLP_MAX_K;
+    double best;
+    int blab;
+    warp_argmax(eff, b.tpen, lane, [&](int c) { return row[c]; }, best, blab);
+    if (lane == 0) {
+        const double own_raw = (unsigned)own < (unsigned)eff ? (double)row[own] : -1e300;
+        const int nl = best > own_raw ? blab : own;
+        if (nl != own) park_move(b, v, nl);
+        atomicAdd(&b.rec[t - 1].te_hubsel, (unsigned long long)(b.off[v + 1] - b.off[v]));
+    }
+}
+
 // Persistent warps take the selected window's work largest items first: hub row chunks (none queued when
 // the hub counts are kept current), then groups of warp-class vertices (metadata of the group loaded by
 // its lanes in one step), then groups of 32 thread-class vertices (lane per vertex).
@@ -495,7 +501,19 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
     LpCounters *cn = b.cnt;
     unsigned long long rd = 0;
 
-    hub_chunks(b, b.dec[2], eff, lane, h, rd);
+    if (a.hub_ready) {
+        // ---- hub decisions from their kept label counts: warp per selected hub ----
+        const int n = cn->ndec[2];
+        int pend = grab_issue(&cn->dgrab[2], lane);
+        for (;;) {
+            const int q = grab_take(pend);
+            if (q >= n) break;
+            pend = grab_issue(&cn->dgrab[2], lane);
+            hub_decide(b, q, eff, a.t, lane);
+        }
+    } else {
+        hub_chunks(b, b.dec[2], eff, lane, h, rd);
+    }
 
     // ---- warp per vertex, groups of G consecutive list entries per item ----
     {
@@ -640,27 +658,13 @@ __global__ void k_hub_index(Buffers b, int nhub) {
         b.hidx[b.bucket[2][i]] = i;
 }
 
-// Hub decisions, after k_decide: warp per hub, argmax over its summed counts; the hubs' arcs are summed
-// for the next iteration's push / pull choice.
+// Hub decisions after k_decide summed the chunks of their rows: warp per hub.
 __global__ void k_hub_final(Buffers b, int eff, int t) {
     if (b.ctrl->stopped) return;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     const int n = b.cnt->ndec[2];
-    for (int i = gw; i < n; i += nw) {
-        const int v = b.dec[2][i];
-        const int own = b.label[v];
-        const int32_t *row = b.hh + (size_t)b.hidx[v] * DMOLP_MAX_K;
-        double best;
-        int blab;
-        warp_argmax(eff, b.tpen, lane, [&](int c) { return row[c]; }, best, blab);
-        if (lane == 0) {
-            const double own_raw = (unsigned)own < (unsigned)eff ? (double)row[own] : -1e300;
-            const int nl = best > own_raw ? blab : own;
-            if (nl != own) park_move(b, v, nl);
-            atomicAdd(&b.rec[t - 1].te_hubsel, (unsigned long long)(b.off[v + 1] - b.off[v]));
-        }
-    }
+    for (int i = gw; i < n; i += nw) hub_decide(b, i, eff, t, lane);
 }
 
 // ------------------------------------------------------------------------------------ update
@@ -869,10 +873,17 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
 }
 
 // ------------------------------------------------------------------------------------ end
-__global__ void k_lp_end(Buffers b, int k, int t, long long narcs, int mode, int symmetric) {
+// End of iteration t (one block; the scalar part on thread 0): the iteration record, the stopping rules of
+// run_phase2 (phase2.cpp:309-415), the next iteration's candidate mode.
+__device__ void lp_end(const Buffers &b, int k, int t, long long narcs, int mode, int symmetric) {
     LpControl *ctl = b.ctrl;
-    if (ctl->stopped) return;
     LpCounters *cn = b.cnt;
+    long long *ch = b.cnthist + (size_t)(t - 1) * 2 * DMOLP_MAX_K;
+    for (int p = threadIdx.x; p < k; p += blockDim.x) {
+        ch[p] = sll(b.vc[p]);
+        ch[DMOLP_MAX_K + p] = sll(b.intra[p]) / 2;
+    }
+    if (threadIdx.x != 0) return;
     LpRecordDev &r = b.rec[t - 1];
     r.window = cn->nwin[t & 1];
     r.candidates = t == 1 ? -1 : cn->ncand;
@@ -903,11 +914,6 @@ __global__ void k_lp_end(Buffers b, int k, int t, long long narcs, int mode, int
         }
     }
     r.edge_cut = ctl->prev_cut;
-    long long *ch = b.cnthist + (size_t)(t - 1) * 2 * DMOLP_MAX_K;
-    for (int p = 0; p < k; ++p) {
-        ch[p] = sll(b.vc[p]);
-        ch[DMOLP_MAX_K + p] = sll(b.intra[p]) / 2;
-    }
     ctl->iters_run = t;
     // the next iteration pulls unless pushing would walk fewer than 1/16 of all arcs (pulling finds the
     // same candidates only when every arc has its reverse); hub rows are not walked by the push.  Pulling
@@ -917,6 +923,23 @@ __global__ void k_lp_end(Buffers b, int k, int t, long long narcs, int mode, int
         ctl->stopped = 1;
         ctl->stop_reason = ctl->stop_now;
     }
+}
+
+// Between iterations, one block: the end of iteration t_end (when > 0), then, unless that stopped the
+// loop, the start of iteration t_begin (when > 0).
+__global__ void k_lp_turn(Buffers b, int k, int t_end, int t_begin, long long narcs, int mode, int symmetric) {
+    __shared__ int s_stopped;
+    if (threadIdx.x == 0) s_stopped = b.ctrl->stopped;
+    __syncthreads();
+    if (s_stopped) return;
+    if (t_end > 0) {
+        lp_end(b, k, t_end, narcs, mode, symmetric);
+        __syncthreads();
+        if (threadIdx.x == 0) s_stopped = b.ctrl->stopped;
+        __syncthreads();
+        if (s_stopped) return;
+    }
+    if (t_begin > 0) lp_begin(b, k, t_begin, narcs);
 }
 
 // Asymmetric graphs: decide whether the full statistics pass runs (the reference skips it on an empty
@@ -1124,11 +1147,12 @@ int dec_wstride(int eff) { return eff <= 32 ? 1024 : (eff > (kDecSmallK / 4) * 3
 
 size_t dec_smem(int eff) { return (size_t)kWarpsPerBlock * dec_wstride(eff) * sizeof(int); }
 
-DecArgs dec_args(int t, int eff) {
+DecArgs dec_args(int t, int eff, bool hub_ready) {
     DecArgs a;
     a.t = t;
     a.eff = eff;
     a.wstride = dec_wstride(eff);
+    a.hub_ready = hub_ready ? 1 : 0;
     return a;
 }
 
@@ -1163,8 +1187,8 @@ StatsArgs stats_args(dmolp_ctx *c, int k) {
 
 int stats_grid(dmolp_ctx *c, const StatsArgs &a) { return a.gv + a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
 
-// The LP decisions of the selected window: hub row chunks queued (unless the hub counts are kept current),
-// the classes counted / decided, hub argmaxes last.  Graphs without hubs launch k_decide alone.
+// The LP decisions of the selected window: hub row chunks queued, the classes counted / decided, hub
+// argmaxes last; when the hub counts are kept current, k_decide alone (hub argmaxes first).
 void launch_decide(dmolp_ctx *c, int t, int eff, bool recount_hubs) {
     Buffers &b = c->b;
     const bool hubs = c->nb[2] > 0;
@@ -1172,9 +1196,9 @@ void launch_decide(dmolp_ctx *c, int t, int eff, bool recount_hubs) {
         k_hub_prep<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff);
         c->launches++;
     }
-    k_decide<<<dec_grid(c, eff), kBlock, dec_smem(eff), c->stream>>>(b, dec_args(t, eff));
+    k_decide<<<dec_grid(c, eff), kBlock, dec_smem(eff), c->stream>>>(b, dec_args(t, eff, !recount_hubs));
     c->launches++;
-    if (hubs) {
+    if (hubs && recount_hubs) {
         k_hub_final<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff, t);
         c->launches++;
     }
@@ -1270,16 +1294,21 @@ SplitArgs split_args(const dmolp_ctx *c, const Buffers &b, int t, int eff) {
     sp.te = &b.rec[t - 1].te_sel;
     sp.t = t;
     sp.eff = eff;
+    sp.npart = b.npart;
+    sp.ratio = b.ratiotab + t;
     return sp;
 }
 
-void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
+void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t, bool first, bool last) {
     Buffers &b = c->b;
     const int grid = grid_for(c);
     const int *stopped = &b.ctrl->stopped;
     bool hist_ready = false;
-    k_lp_begin<<<1, 256, 0, c->stream>>>(b, L.k, t, (long long)c->narcs);
-    c->launches += 1;
+    const int sym = c->symmetric ? 1 : 0;
+    if (first) {  // otherwise the previous iteration's closing k_lp_turn began this one
+        k_lp_turn<<<1, 256, 0, c->stream>>>(b, L.k, 0, t, (long long)c->narcs, L.mode, sym);
+        c->launches += 1;
+    }
     if (t > 1) {
         // the previous window by decision class; hubs through hubwin
         ProfScope ps(c, 2, t);
@@ -1298,8 +1327,7 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
         k_bnd<<<bnd_grid(c, a), kBlock, bnd_smem(L.k, a), c->stream>>>(b, a, L.k);
         hist_ready = a.hist != nullptr;
     }
-    k_lp_need<<<1, 256, 0, c->stream>>>(b, L.k, t);
-    c->launches += 2;
+    c->launches += 1;
     {
         ProfScope ps(c, 4, t);
         const SplitArgs sp = split_args(c, b, t, L.eff);
@@ -1324,7 +1352,7 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t) {
                                                                                                 &b.ctrl->skip_stats);
         c->launches += 3;
     }
-    k_lp_end<<<1, 1, 0, c->stream>>>(b, L.k, t, (long long)c->narcs, L.mode, c->symmetric ? 1 : 0);
+    k_lp_turn<<<1, 256, 0, c->stream>>>(b, L.k, t, last ? 0 : t + 1, (long long)c->narcs, L.mode, sym);
     c->launches += 1;
 }
 
@@ -1338,8 +1366,7 @@ void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int n
     k_mark_chunks<<<grid, kBlock, 0, c->stream>>>(b, t);
     const BndArgs a = bnd_args(c, t, 0, 0, k, true);
     k_bnd<<<bnd_grid(c, a), kBlock, bnd_smem(k, a), c->stream>>>(b, a, k);
-    k_lp_need<<<1, 256, 0, c->stream>>>(b, k, t);
-    c->launches += 5;
+    c->launches += 4;
     const SplitArgs sp = split_args(c, b, t, DMOLP_MAX_K);
     select_smallest(c, b.bown, b.bkey, &b.cnt->npos, k, c->dbits + c->ibits, b.bsel, nullptr, &sp, a.hist != nullptr);
 }

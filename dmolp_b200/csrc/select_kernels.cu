@@ -102,7 +102,15 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
     int *s_below = s_need + nseg, *s_keep = s_below + nseg;
     __shared__ int s_open, s_cnt;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int p = threadIdx.x; p < nseg; p += blockDim.x) s_need[p] = a.need[p];
+    for (int p = threadIdx.x; p < nseg; p += blockDim.x) {
+        if (a.has_split) {  // need[p] = min(n_p, ceil(e^(-t/5) * n_p))   (gpu_lp_boundary.cu:244, 296-297)
+            const int n = a.sp.npart[p];
+            const int m = (int)ceil(__dmul_rn(*a.sp.ratio, (double)n));
+            s_need[p] = m > n ? n : m;
+        } else {
+            s_need[p] = a.need[p];
+        }
+    }
     if (use_smem)
         for (int i = threadIdx.x; i < nbins; i += blockDim.x) shist[i] = 0;
     const int n0 = *a.n_dev;
