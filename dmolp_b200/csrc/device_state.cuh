@@ -21,6 +21,7 @@ constexpr int kDecSmall = 32;    // LP decisions: rows of at most 32 arcs are co
 constexpr int kDecSmallK = 64;   // ... when at most 64 labels are scored (byte counters in shared memory)
 constexpr int kLargeDeg = 4096;  // deg > 4096: one block walks the row
 constexpr int kChunk = 4096;     // row chunk of the window-marking kernel
+constexpr int kHotMax = 16384;   // LP gathers: labels of up to this many highest-degree vertices per block
 constexpr int kHubChunk = 2048;  // row chunk of the decisions of deg > kLargeDeg vertices
 
 // Per-iteration counters of the LP loop (reset by the first kernel of each iteration).
@@ -99,6 +100,13 @@ struct Buffers {
     int32_t *hubwin = nullptr; // [nv] hubs of the previous window whose rows hold the vertex
     int32_t *hub_in = nullptr; // [nb[2]] hub is counted in hubwin (was in the window hubwin describes)
     int2 *hubwq = nullptr;     // [hubq_cap] (hub index, first arc) of rows entering or leaving hubwin
+    // hot set: the (at most kHotMax) vertices of highest degree, whose labels the label-gathering kernels
+    // read from a per-block shared copy
+    int32_t *colh = nullptr;   // [narcs] col with a hot neighbour u written as -(hrank[u] + 2)
+    int32_t *hrank = nullptr;  // [nv] rank of a hot vertex, else -1
+    int32_t *hotid = nullptr;  // [kHotMax] vertex of each rank
+    uint8_t *hotlab = nullptr; // [kHotMax] label of each hot vertex, clamped to 255 (kept current by k_apply)
+    unsigned int *degh = nullptr;  // [65536] degree histogram (hot-set threshold)
     int32_t *active[2] = {nullptr, nullptr};  // [nv] radix-select active lists
     // per-part arrays (DMOLP_MAX_K); vc / intra hold signed values in two's complement
     unsigned int *hist = nullptr;        // [MAX_K * 256]
@@ -145,6 +153,8 @@ struct dmolp_ctx {
     bool symmetry_known = false;          // `symmetric` has been tested for the resident graph
     bool rows_sorted = false;             // every row strictly increasing (precondition of the test)
     bool has_graph = false;
+    bool hot_ready = false;               // colh / hrank / hotid built for the resident graph
+    int nhot = 0;                         // hot vertices
     std::vector<int32_t> h_rawdeg;        // host copy for the hub sort
     bool h_rawdeg_valid = false;          // h_rawdeg mirrors the resident raw degrees
     dmolp::Buffers b;

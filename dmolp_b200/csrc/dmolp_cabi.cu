@@ -284,6 +284,11 @@ size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t 
     ALLOC(b.hubwin, n);
     ALLOC(b.hub_in, nball[2]);
     ALLOC(b.hubwq, (size_t)c->hubq_cap);
+    ALLOC(b.colh, (size_t)narcs);
+    ALLOC(b.hrank, n);
+    ALLOC(b.hotid, kHotMax);
+    ALLOC(b.hotlab, kHotMax);
+    ALLOC(b.degh, 65536);
 #undef ALLOC
     return off;
 }
@@ -338,6 +343,9 @@ int graph_finish(dmolp_ctx *c, bool rows_sorted) {
     DMOLP_CUDA(cudaMemcpyAsync(&b.cnt->npos, &npos, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.bown, 0xff, n * sizeof(int32_t), c->stream));  // all record slots empty
     lp_fill(c, b.newlab, (int64_t)n, -1);
+    lp_fill(c, b.hrank, (int64_t)n, -1);  // no hot set until the first LP run builds it
+    c->hot_ready = false;
+    c->nhot = 0;
     lp_hub_index(c);
     select_prepare();
     // whether every arc has its reverse is tested when the LP loop first needs it (ensure_symmetry)
@@ -357,6 +365,33 @@ int graph_finish(dmolp_ctx *c, bool rows_sorted) {
     if (s2) return s2;
     c->has_graph = true;
     return DMOLP_OK;
+}
+
+// The hot set of the resident graph, built the first time the LP loop runs on it: the vertices of the
+// highest degrees, at most kHotMax (all of degree >= d*, d* the smallest degree for which they fit).
+int lp_hot_prepare(dmolp_ctx *c) {
+    if (c->hot_ready) return DMOLP_OK;
+    Buffers &b = c->b;
+    std::vector<unsigned int> h(65536);
+    lp_hot_hist(c);
+    DMOLP_CUDA(cudaMemcpyAsync(h.data(), b.degh, h.size() * sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream));
+    int s = sync(c);
+    if (s) return s;
+    long long acc = 0;
+    int dstar = 0;
+    for (int d = 65535; d >= 1; --d) {
+        if (acc + h[d] > kHotMax) break;
+        acc += h[d];
+        dstar = d;
+    }
+    c->nhot = 0;
+    if (acc > 0) {
+        DMOLP_CUDA(cudaMemsetAsync(b.flag, 0, sizeof(int), c->stream));
+        lp_hot_build(c, dstar);
+        c->nhot = (int)acc;
+    }
+    c->hot_ready = true;
+    return check_launch(c);
 }
 
 // Whether every arc has its reverse, tested on the device the first time the LP loop needs it (then the
@@ -1060,8 +1095,8 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
         return fail(DMOLP_ERR_ARG, "iterations must be in [0, 500]");
     if (cfg->cap != DMOLP_LP_CAP_REF && cfg->cap != DMOLP_LP_CAP_FULL) return fail(DMOLP_ERR_ARG, "bad cap");
     DMOLP_CUDA(cudaSetDevice(c->device));
-    int sy = ensure_symmetry(c);
-    if (sy) return sy;
+    int st = ensure_symmetry(c);
+    if (st) return st;
     Buffers &b = c->b;
     LpLaunch L;
     L.k = k;
@@ -1077,11 +1112,14 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
         DMOLP_CUDA(cudaMemsetAsync(b.hubwin, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
         DMOLP_CUDA(cudaMemsetAsync(b.hub_in, 0, (size_t)c->nb[2] * sizeof(int32_t), c->stream));
     }
+    st = lp_hot_prepare(c);
+    if (st) return st;
+    lp_hot_refresh(c);
     lp_reset_stats(c, k, nullptr);
-    lp_stats(c, k, nullptr, nullptr);
+    lp_stats(c, k, nullptr, nullptr, true);
     if (c->symmetric) lp_hub_counts(c, L.eff);
     lp_init_end(c, cfg->mode);
-    int st = check_launch(c);
+    st = check_launch(c);
     if (st) return st;
     int stopped = 0;
     // Iterations in blocks: FIXED mode one block of all iterations, REF mode blocks of 8 with a check of

@@ -50,7 +50,11 @@ struct LpLaunch {
 void lp_check_symmetric(dmolp_ctx *c, unsigned long long *counts);  // *b.flag: a reverse is missing
 void lp_fill(dmolp_ctx *c, int32_t *p, int64_t n, int32_t v);
 void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped);
-void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip);
+// use_hot: the hot labels are current (lp_hot_refresh since the labels were last set outside the loop)
+void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot = false);
+void lp_hot_hist(dmolp_ctx *c);              // b.degh = histogram of min(degree, 65535), degree > 0
+void lp_hot_build(dmolp_ctx *c, int dstar);  // vertices of degree >= dstar ranked; colh; b.flag = their number
+void lp_hot_refresh(dmolp_ctx *c);           // hot labels from the resident labels
 void lp_init_end(dmolp_ctx *c, int mode);
 void lp_hub_index(dmolp_ctx *c);            // b.hidx from bucket[2] (once per graph)
 void lp_hub_counts(dmolp_ctx *c, int eff);  // label counts of every hub's row into b.hh (run start, symmetric)

@@ -57,7 +57,9 @@ __device__ __forceinline__ int64_t warp_row(const int32_t *__restrict__ col, int
 // lane, the row's scalar head and tail (first step only) and two 16-byte words of its body, then gathers
 // g(u) for all of them, then calls f(u, g(u)) for each, so a row of up to 262 arcs costs one dependent
 // load pair.  After each step stop() (evaluated warp-uniformly) may end the walk.  Returns the number of
-// arcs the warp read.
+// arcs the warp read.  Entries are ids (>= 0) or, in the hot-encoded rows, -(rank + 2); kNoArc marks an
+// empty slot.
+constexpr int kNoArc = -1;
 template <typename G, typename F, typename S>
 __device__ __forceinline__ int64_t warp_row_wide(const int32_t *__restrict__ col, int64_t s, int64_t e, int lane,
                                                  G g, F f, S stop) {
@@ -70,10 +72,10 @@ __device__ __forceinline__ int64_t warp_row_wide(const int32_t *__restrict__ col
     bool first = true;
     for (int64_t q0 = a >> 2; first || q0 < qe; q0 += 64) {
         int u[10];
-        u[8] = first && s + lane < a ? __ldg(col + s + lane) : -1;
-        u[9] = first && t0 + lane < e ? __ldg(col + t0 + lane) : -1;
+        u[8] = first && s + lane < a ? __ldg(col + s + lane) : kNoArc;
+        u[9] = first && t0 + lane < e ? __ldg(col + t0 + lane) : kNoArc;
         const int64_t q = q0 + lane;
-        int4 x = make_int4(-1, -1, -1, -1), y = make_int4(-1, -1, -1, -1);
+        int4 x = make_int4(kNoArc, kNoArc, kNoArc, kNoArc), y = x;
         if (q < qe) x = __ldcs(c4 + q);
         if (q + 32 < qe) y = __ldcs(c4 + q + 32);
         u[0] = x.x; u[1] = x.y; u[2] = x.z; u[3] = x.w;
@@ -81,10 +83,10 @@ __device__ __forceinline__ int64_t warp_row_wide(const int32_t *__restrict__ col
         decltype(g(0)) v[10];
 #pragma unroll
         for (int r = 0; r < 10; ++r)
-            if (u[r] >= 0) v[r] = g(u[r]);
+            if (u[r] != kNoArc) v[r] = g(u[r]);
 #pragma unroll
         for (int r = 0; r < 10; ++r)
-            if (u[r] >= 0) f(u[r], v[r]);
+            if (u[r] != kNoArc) f(u[r], v[r]);
         if (q0 < qe) read += 4 * (qe - q0 < 64 ? qe - q0 : (int64_t)64);
         first = false;
         if (stop()) break;

@@ -406,7 +406,22 @@ struct DecArgs {
     int t, eff;
     int wstride;    // shared ints per warp: lane-private counters (eff <= 32), histogram, or byte counters
     int hub_ready;  // the hubs' label counts are current (kept from the movers): decide them first
+    int use_hot;    // count through colh and the block's copy of the hot labels (eff <= 32)
 };
+
+// Label of a row entry u: a vertex id (u >= 0) or, in colh, the hot vertex of rank -(u + 2), whose label
+// (clamped to 255) is in the block's shared copy s_hot.
+__device__ __forceinline__ int nbr_label(const int32_t *__restrict__ label, const uint8_t *s_hot, int u) {
+    return u >= 0 ? label[u] : (int)s_hot[-u - 2];
+}
+
+// The block's copy of the hot labels (all threads; ends with a barrier).
+__device__ __forceinline__ void load_hot(const Buffers &b, uint8_t *s_hot) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(b.hotlab);
+    uint4 *dst = reinterpret_cast<uint4 *>(s_hot);
+    for (int i = threadIdx.x; i < kHotMax / 16; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+}
 
 __device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
     b.newlab[v] = nl;
@@ -419,21 +434,23 @@ __device__ __forceinline__ void park_move(const Buffers &b, int v, int nl) {
 __device__ __forceinline__ int grab_issue(int *ctr, int lane) { return lane == 0 ? atomicAdd(ctr, 1) : 0; }
 __device__ __forceinline__ int grab_take(int pending) { return __shfl_sync(DMOLP_FULL_MASK, pending, 0); }
 
-// Lane-private label counts (eff <= 32) of the arcs [s, e).
+// Lane-private label counts (eff <= 32) of the arcs [s, e) of col (b.col, or colh with s_hot).
 __device__ __forceinline__ void count_priv(const int32_t *__restrict__ col, const int32_t *__restrict__ label,
-                                           int64_t s, int64_t e, int lane, int eff, int *h) {
-    warp_row_wide(col, s, e, lane, [&](int u) { return label[u]; }, [&](int, int l) {
+                                           const uint8_t *s_hot, int64_t s, int64_t e, int lane, int eff, int *h) {
+    warp_row_wide(col, s, e, lane, [&](int u) { return nbr_label(label, s_hot, u); }, [&](int, int l) {
         if ((unsigned)l < (unsigned)eff) h[l * 32 + ((lane + l) & 31)] += 1;
     }, [] { return false; });
 }
 
 // Label counts of the arcs [s, e) into the warp's region: lane-private counters (eff <= 32) or a shared
 // histogram of eff ints (warp_count's match-aggregated atomics).
-__device__ __forceinline__ void count_row(const Buffers &b, int64_t s, int64_t e, int lane, int eff, int *h) {
+// col / s_hot: as for count_priv (the eff > 32 histogram reads b.col).
+__device__ __forceinline__ void count_row(const Buffers &b, const int32_t *col, const uint8_t *s_hot, int64_t s,
+                                          int64_t e, int lane, int eff, int *h) {
     if (eff <= 32) {
         priv_zero(h, eff, lane);
         __syncwarp();
-        count_priv(b.col, b.label, s, e, lane, eff, h);
+        count_priv(col, b.label, s_hot, s, e, lane, eff, h);
     } else {
         for (int c = lane; c < eff; c += 32) h[c] = 0;
         __syncwarp();
@@ -444,8 +461,8 @@ __device__ __forceinline__ void count_row(const Buffers &b, int64_t s, int64_t e
 
 // Hub rows (deg > kLargeDeg) in queued chunks of kHubChunk arcs, (list position, first arc) in b.hubq:
 // warp per chunk, its label counts added to the hub's row of b.hh.
-__device__ __forceinline__ void hub_chunks(const Buffers &b, const int32_t *list, int eff, int lane, int *h,
-                                           unsigned long long &rd) {
+__device__ __forceinline__ void hub_chunks(const Buffers &b, const int32_t *col, const uint8_t *s_hot,
+                                           const int32_t *list, int eff, int lane, int *h, unsigned long long &rd) {
     LpCounters *cn = b.cnt;
     const int n = cn->nhubq;
     int pend = grab_issue(&cn->dgrab[2], lane);
@@ -457,7 +474,7 @@ __device__ __forceinline__ void hub_chunks(const Buffers &b, const int32_t *list
         const int v = list[ch.x];
         const int64_t s = b.off[v] + ch.y, rowe = b.off[v + 1];
         const int64_t e = rowe - s > kHubChunk ? s + kHubChunk : rowe;
-        count_row(b, s, e, lane, eff, h);
+        count_row(b, col, s_hot, s, e, lane, eff, h);
         int32_t *row = b.hh + (size_t)b.hidx[v] * DMOLP_MAX_K;
         if (eff <= 32) {
             const int cnt = priv_total(h, eff, lane);
@@ -498,6 +515,13 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
     const int eff = a.eff;
     const bool priv = eff <= 32;
     int *h = shist + wib * a.wstride;
+    uint8_t *s_hot = nullptr;
+    const int32_t *col = b.col;
+    if (a.use_hot) {  // block-uniform
+        s_hot = reinterpret_cast<uint8_t *>(shist + kWarpsPerBlock * a.wstride);
+        load_hot(b, s_hot);
+        col = b.colh;
+    }
     LpCounters *cn = b.cnt;
     unsigned long long rd = 0;
 
@@ -512,7 +536,7 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
             hub_decide(b, q, eff, a.t, lane);
         }
     } else {
-        hub_chunks(b, b.dec[2], eff, lane, h, rd);
+        hub_chunks(b, col, s_hot, b.dec[2], eff, lane, h, rd);
     }
 
     // ---- warp per vertex, groups of G consecutive list entries per item ----
@@ -540,7 +564,7 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
                 const int v = __shfl_sync(DMOLP_FULL_MASK, gv, j);
                 const int own = __shfl_sync(DMOLP_FULL_MASK, gown, j);
                 const int64_t s = __shfl_sync(DMOLP_FULL_MASK, gs, j), e = __shfl_sync(DMOLP_FULL_MASK, ge, j);
-                count_row(b, s, e, lane, eff, h);
+                count_row(b, col, s_hot, s, e, lane, eff, h);
                 double best;
                 int blab, own_cnt;
                 if (priv) {
@@ -588,9 +612,9 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
             for (int j = 0; j < deg; j += 8) {
                 int u[8], l[8];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(b.col + s + j + q) : -1;
+                for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(col + s + j + q) : kNoArc;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) l[q] = u[q] >= 0 ? b.label[u[q]] : -1;
+                for (int q = 0; q < 8; ++q) l[q] = u[q] != kNoArc ? nbr_label(b.label, s_hot, u[q]) : -1;
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
                     if ((unsigned)l[q] < (unsigned)eff) {
@@ -650,7 +674,7 @@ __global__ void __launch_bounds__(256, 4) k_hub_all_count(Buffers b, int eff, in
     extern __shared__ int shist[];
     int *h = shist + (threadIdx.x >> 5) * wstride;
     unsigned long long rd = 0;
-    hub_chunks(b, b.bucket[2], eff, threadIdx.x & 31, h, rd);
+    hub_chunks(b, b.col, nullptr, b.bucket[2], eff, threadIdx.x & 31, h, rd);
 }
 
 __global__ void k_hub_index(Buffers b, int nhub) {
@@ -745,8 +769,11 @@ __global__ void k_apply(Buffers b) {
     const int n = b.cnt->nchanged;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int v = b.mov[i];
-        b.label[v] = b.newlab[v];
+        const int nl = b.newlab[v];
+        b.label[v] = nl;
         b.newlab[v] = -1;
+        const int r = b.hrank[v];
+        if (r >= 0) b.hotlab[r] = (unsigned)nl < 255u ? (uint8_t)nl : (uint8_t)255;
     }
 }
 
@@ -755,14 +782,23 @@ __global__ void k_apply(Buffers b) {
 // degree class the same-label and cut arcs.  Block ranges: [0,gv) vertex counts, then the three classes.
 struct StatsArgs {
     int k, nv, gv, g0, g1, nb0, nb1, nb2;
+    int use_hot;  // rows through colh and the block's copy of the hot labels (k <= 255)
 };
 
 __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int *stopped, const int *skip) {
     if ((stopped && *stopped) || (skip && *skip)) return;
-    extern __shared__ unsigned long long sacc[];  // [2k]: vertex counts, intra arcs
+    extern __shared__ unsigned long long sacc[];  // [2k]: vertex counts, intra arcs; then the hot labels
     const int k = a.k;
     unsigned long long *svc = sacc, *sin = sacc + k;
     for (int p = threadIdx.x; p < 2 * k; p += blockDim.x) sacc[p] = 0;
+    const uint8_t *s_hot = nullptr;
+    const int32_t *col = b.col;
+    if (a.use_hot) {  // block-uniform
+        uint8_t *sh = reinterpret_cast<uint8_t *>(sacc + 2 * k);
+        load_hot(b, sh);
+        s_hot = sh;
+        col = b.colh;
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     unsigned long long cut = 0;
@@ -784,12 +820,12 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
             for (int j = 0; j < deg; j += 8) {  // eight ids, then their eight labels, in flight
                 int u[8], l[8];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(b.col + s + j + q) : -1;
+                for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(col + s + j + q) : kNoArc;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) l[q] = u[q] >= 0 ? b.label[u[q]] : lv;
+                for (int q = 0; q < 8; ++q) l[q] = u[q] != kNoArc ? nbr_label(b.label, s_hot, u[q]) : lv;
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
-                    if (u[q] >= 0) {
+                    if (u[q] != kNoArc) {
                         bad |= (unsigned)l[q] >= (unsigned)k;
                         same += (l[q] == lv);
                         diff += (l[q] != lv);
@@ -806,7 +842,8 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
             const int v = b.bucket[1][i];
             const int lv = b.label[v];
             unsigned int same = 0, diff = 0;
-            warp_row_wide(b.col, b.off[v], b.off[v + 1], lane, [&](int u) { return b.label[u]; }, [&](int, int lu) {
+            warp_row_wide(col, b.off[v], b.off[v + 1], lane, [&](int u) { return nbr_label(b.label, s_hot, u); },
+                          [&](int, int lu) {
                 bad |= (unsigned)lu >= (unsigned)k;
                 same += (lu == lv);
                 diff += (lu != lv);
@@ -834,13 +871,13 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int64_t j = j0 + q * blockDim.x + threadIdx.x;
-                    u[q] = j < e ? __ldcs(b.col + j) : -1;
+                    u[q] = j < e ? __ldcs(col + j) : kNoArc;
                 }
 #pragma unroll
-                for (int q = 0; q < 4; ++q) l[q] = u[q] >= 0 ? b.label[u[q]] : lv;
+                for (int q = 0; q < 4; ++q) l[q] = u[q] != kNoArc ? nbr_label(b.label, s_hot, u[q]) : lv;
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    if (u[q] >= 0) {
+                    if (u[q] != kNoArc) {
                         bad |= (unsigned)l[q] >= (unsigned)k;
                         same += (l[q] == lv);
                         diff += (l[q] != lv);
@@ -869,6 +906,63 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
         if (svc[p]) atomicAdd(&b.vc[p], svc[p]);
         if (sin[p]) atomicAdd(&b.intra[p], sin[p]);
+    }
+}
+
+// ------------------------------------------------------------------------------------ hot set
+// degh[min(deg, 65535)] for every vertex with arcs; degrees below kHotHistLow in a block histogram first.
+constexpr int kHotHistLow = 4096;
+__global__ void k_hot_hist(Buffers b, int nv) {
+    __shared__ unsigned int sh[kHotHistLow];
+    for (int i = threadIdx.x; i < kHotHistLow; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        const int64_t d = b.off[v + 1] - b.off[v];
+        if (d <= 0) continue;
+        if (d < kHotHistLow) atomicAdd(&sh[d], 1u);
+        else atomicAdd(&b.degh[d < 65535 ? d : 65535], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kHotHistLow; i += blockDim.x)
+        if (sh[i]) atomicAdd(&b.degh[i], sh[i]);
+}
+
+// Vertices of degree >= dstar get ranks (b.flag counts them; the order of ranks is immaterial).
+__global__ void k_hot_assign(Buffers b, int nv, int dstar) {
+    for (int v0 = blockIdx.x * blockDim.x; v0 < nv; v0 += gridDim.x * blockDim.x) {
+        const int v = v0 + threadIdx.x;
+        const bool hot = v < nv && b.off[v + 1] - b.off[v] >= dstar;
+        const int r = warp_append(b.flag, hot);
+        if (hot) {
+            b.hrank[v] = r;
+            b.hotid[r] = v;
+        }
+    }
+}
+
+// colh = col with hot neighbours written as -(rank + 2).
+__global__ void k_hot_encode(Buffers b, long long narcs) {
+    const long long n4 = narcs >> 2;
+    const int4 *c4 = reinterpret_cast<const int4 *>(b.col);
+    int4 *h4 = reinterpret_cast<int4 *>(b.colh);
+    auto enc = [&](int u) {
+        const int r = b.hrank[u];
+        return r >= 0 ? -(r + 2) : u;
+    };
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+        const int4 x = __ldcs(c4 + i);
+        h4[i] = make_int4(enc(x.x), enc(x.y), enc(x.z), enc(x.w));
+    }
+    for (long long j = (n4 << 2) + blockIdx.x * (long long)blockDim.x + threadIdx.x; j < narcs;
+         j += (long long)gridDim.x * blockDim.x)
+        b.colh[j] = enc(b.col[j]);
+}
+
+// Hot labels from the resident labels, clamped to 255.
+__global__ void k_hot_refresh(Buffers b, int nhot) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nhot; r += gridDim.x * blockDim.x) {
+        const int l = b.label[b.hotid[r]];
+        b.hotlab[r] = (unsigned)l < 255u ? (uint8_t)l : (uint8_t)255;
     }
 }
 
@@ -1145,14 +1239,17 @@ int bnd_grid(dmolp_ctx *c, const BndArgs &a) { return a.g0 + a.g1 + clampi(c->nb
 
 int dec_wstride(int eff) { return eff <= 32 ? 1024 : (eff > (kDecSmallK / 4) * 32 ? eff : (kDecSmallK / 4) * 32); }
 
-size_t dec_smem(int eff) { return (size_t)kWarpsPerBlock * dec_wstride(eff) * sizeof(int); }
+size_t dec_smem(int eff, bool use_hot) {
+    return (size_t)kWarpsPerBlock * dec_wstride(eff) * sizeof(int) + (use_hot ? (size_t)kHotMax : 0);
+}
 
-DecArgs dec_args(int t, int eff, bool hub_ready) {
+DecArgs dec_args(int t, int eff, bool hub_ready, bool use_hot) {
     DecArgs a;
     a.t = t;
     a.eff = eff;
     a.wstride = dec_wstride(eff);
     a.hub_ready = hub_ready ? 1 : 0;
+    a.use_hot = use_hot ? 1 : 0;
     return a;
 }
 
@@ -1162,8 +1259,8 @@ int dec_grid(dmolp_ctx *c, int eff) {
     int &n = per_sm[eff <= 32 ? 0 : 1];
     if (n == 0) {
         int r = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_decide, kBlock, dec_smem(eff <= 32 ? 32 : DMOLP_MAX_K)) !=
-                cudaSuccess ||
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_decide, kBlock,
+                                                          dec_smem(eff <= 32 ? 32 : DMOLP_MAX_K, true)) != cudaSuccess ||
             r < 1)
             r = kGridPerSm;
         n = r;
@@ -1171,9 +1268,11 @@ int dec_grid(dmolp_ctx *c, int eff) {
     return c->num_sms * n;
 }
 
-StatsArgs stats_args(dmolp_ctx *c, int k) {
+// use_hot: the hot labels are current; applies when the graph has a hot set and k <= 255 (exact bytes).
+StatsArgs stats_args(dmolp_ctx *c, int k, bool use_hot) {
     StatsArgs a;
     a.k = k;
+    a.use_hot = use_hot && c->nhot > 0 && k <= 255;
     a.nv = (int)c->nv;
     const int cap = c->num_sms * 8;
     a.gv = clampi((int)((c->nv + 255) / 256), 1, c->num_sms * 2);
@@ -1187,16 +1286,22 @@ StatsArgs stats_args(dmolp_ctx *c, int k) {
 
 int stats_grid(dmolp_ctx *c, const StatsArgs &a) { return a.gv + a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
 
+size_t stats_smem(const StatsArgs &a) {
+    return 2 * (size_t)a.k * sizeof(unsigned long long) + (a.use_hot ? (size_t)kHotMax : 0);
+}
+
 // The LP decisions of the selected window: hub row chunks queued, the classes counted / decided, hub
-// argmaxes last; when the hub counts are kept current, k_decide alone (hub argmaxes first).
-void launch_decide(dmolp_ctx *c, int t, int eff, bool recount_hubs) {
+// argmaxes last; when the hub counts are kept current, k_decide alone (hub argmaxes first).  use_hot: the
+// hot labels are current (used when the graph has a hot set and eff <= 32).
+void launch_decide(dmolp_ctx *c, int t, int eff, bool recount_hubs, bool use_hot) {
     Buffers &b = c->b;
     const bool hubs = c->nb[2] > 0;
     if (hubs && recount_hubs) {
         k_hub_prep<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff);
         c->launches++;
     }
-    k_decide<<<dec_grid(c, eff), kBlock, dec_smem(eff), c->stream>>>(b, dec_args(t, eff, !recount_hubs));
+    const bool hot = use_hot && c->nhot > 0 && eff <= 32;
+    k_decide<<<dec_grid(c, eff), kBlock, dec_smem(eff, hot), c->stream>>>(b, dec_args(t, eff, !recount_hubs, hot));
     c->launches++;
     if (hubs && recount_hubs) {
         k_hub_final<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff, t);
@@ -1251,9 +1356,27 @@ void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped) {
     c->launches++;
 }
 
-void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip) {
-    const StatsArgs a = stats_args(c, k);
-    k_stats<<<stats_grid(c, a), kBlock, 2 * k * sizeof(unsigned long long), c->stream>>>(c->b, a, stopped, skip);
+void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot) {
+    const StatsArgs a = stats_args(c, k, use_hot);
+    k_stats<<<stats_grid(c, a), kBlock, stats_smem(a), c->stream>>>(c->b, a, stopped, skip);
+    c->launches++;
+}
+
+void lp_hot_hist(dmolp_ctx *c) {
+    cudaMemsetAsync(c->b.degh, 0, 65536 * sizeof(unsigned int), c->stream);
+    k_hot_hist<<<grid_for(c), kBlock, 0, c->stream>>>(c->b, (int)c->nv);
+    c->launches++;
+}
+
+void lp_hot_build(dmolp_ctx *c, int dstar) {
+    k_hot_assign<<<grid_for(c), kBlock, 0, c->stream>>>(c->b, (int)c->nv, dstar);
+    k_hot_encode<<<grid_for(c), kBlock, 0, c->stream>>>(c->b, c->narcs);
+    c->launches += 2;
+}
+
+void lp_hot_refresh(dmolp_ctx *c) {
+    if (c->nhot == 0) return;
+    k_hot_refresh<<<clampi((c->nhot + 255) / 256, 1, grid_for(c)), kBlock, 0, c->stream>>>(c->b, c->nhot);
     c->launches++;
 }
 
@@ -1271,7 +1394,7 @@ void lp_hub_counts(dmolp_ctx *c, int eff) {
     cudaMemsetAsync(&b.cnt->nhubq, 0, sizeof(int), c->stream);
     cudaMemsetAsync(&b.cnt->dgrab[2], 0, sizeof(int), c->stream);
     k_hub_all_queue<<<clampi((c->nb[2] + 7) / 8, 1, grid_for(c)), kBlock, 0, c->stream>>>(b, c->nb[2], eff);
-    k_hub_all_count<<<c->num_sms * 4, kBlock, dec_smem(eff), c->stream>>>(b, eff, dec_wstride(eff));
+    k_hub_all_count<<<c->num_sms * 4, kBlock, dec_smem(eff, false), c->stream>>>(b, eff, dec_wstride(eff));
     c->launches += 2;
 }
 
@@ -1335,7 +1458,7 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t, bool first, bool last)
     }
     {
         ProfScope ps(c, 1, t);
-        launch_decide(c, t, L.eff, !c->symmetric);
+        launch_decide(c, t, L.eff, !c->symmetric, true);
     }
     if (c->symmetric) {
         {
@@ -1347,9 +1470,8 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t, bool first, bool last)
     } else {
         k_apply<<<grid, kBlock, 0, c->stream>>>(b);
         k_lp_mid<<<1, 256, 0, c->stream>>>(b, L.k, t, L.mode);
-        const StatsArgs a = stats_args(c, L.k);
-        k_stats<<<stats_grid(c, a), kBlock, 2 * L.k * sizeof(unsigned long long), c->stream>>>(b, a, stopped,
-                                                                                                &b.ctrl->skip_stats);
+        const StatsArgs a = stats_args(c, L.k, true);
+        k_stats<<<stats_grid(c, a), kBlock, stats_smem(a), c->stream>>>(b, a, stopped, &b.ctrl->skip_stats);
         c->launches += 3;
     }
     k_lp_turn<<<1, 256, 0, c->stream>>>(b, L.k, t, last ? 0 : t + 1, (long long)c->narcs, L.mode, sym);
@@ -1378,7 +1500,7 @@ void lp_apply_list(dmolp_ctx *c, int k, int eff, int n) {
     const int grid = grid_for(c);
     k_zero_small<<<1, 1, 0, c->stream>>>(b);
     k_classify<<<grid, kBlock, 0, c->stream>>>(b, n, eff);
-    launch_decide(c, 1, eff, true);
+    launch_decide(c, 1, eff, true, false);
     k_collect_moves<<<grid, kBlock, 0, c->stream>>>(b);
     k_apply<<<grid, kBlock, 0, c->stream>>>(b);
     c->launches += 4;
