@@ -26,6 +26,7 @@ namespace {
 
 constexpr int kSmemSegMax = 64;  // 64 segments * 256 digits * 4 B = 64 KiB of shared histogram
 constexpr int kSelThreads = 1024;
+constexpr int kPartU = 2;  // records per thread and step of the partition
 constexpr unsigned int kBarrierSpins = 1u << 22;  // a generous bound; then give up and flag
 
 struct SelArgs {
@@ -208,67 +209,102 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
         __syncthreads();
         const bool more = s_open > 0 && pass + 1 < a.npass;
         const int shift_next = shift - kRadixBits;
-        // ---- partition of this block's records, and the next digit's histogram of the records kept ----
-        for (int i0 = 0; i0 < my_n; i0 += blockDim.x) {
-            const int i = i0 + threadIdx.x;
-            bool keep = false, take = false;
-            int r = 0, bin = -(lane + 1), p = -1;
-            uint64_t key = 0;
-            if (i < my_n) {
-                r = src ? src[i] : lo + i;
-                p = a.seg[r];
-                key = a.key[r];
-                if (p >= 0) {  // skip empty record slots
-                    const int d = (int)((key >> shift) & (kRadix - 1));
-                    if (d < s_below[p]) {
-                        a.sel[r] = 1;
-                        take = true;
-                    } else if (more && d == s_keep[p]) {
-                        keep = true;
-                        bin = p * kRadix + (int)((key >> shift_next) & (kRadix - 1));
+        // ---- partition of this block's records, and the next digit's histogram of the records kept;
+        //      kPartU records per thread and step, their loads and their appends' atomics issued together ----
+        for (int i0 = 0; i0 < my_n; i0 += kPartU * blockDim.x) {
+            bool keep[kPartU], take[kPartU];
+            int r[kPartU], bin[kPartU], p[kPartU];
+            uint64_t key[kPartU];
+#pragma unroll
+            for (int u = 0; u < kPartU; ++u) {
+                const int i = i0 + u * (int)blockDim.x + (int)threadIdx.x;
+                r[u] = i < my_n ? (src ? src[i] : lo + i) : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < kPartU; ++u) {
+                p[u] = r[u] >= 0 ? a.seg[r[u]] : -1;
+                key[u] = r[u] >= 0 ? a.key[r[u]] : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < kPartU; ++u) {
+                keep[u] = take[u] = false;
+                bin[u] = -(lane + 1) - 32 * u;  // unique non-bin value per lane and record
+                if (p[u] >= 0) {  // skip empty record slots
+                    const int d = (int)((key[u] >> shift) & (kRadix - 1));
+                    if (d < s_below[p[u]]) {
+                        a.sel[r[u]] = 1;
+                        take[u] = true;
+                    } else if (more && d == s_keep[p[u]]) {
+                        keep[u] = true;
+                        bin[u] = p[u] * kRadix + (int)((key[u] >> shift_next) & (kRadix - 1));
                     }
                 }
             }
-            const unsigned m = __ballot_sync(DMOLP_FULL_MASK, keep);
-            const int leader = m ? __ffs(m) - 1 : 0;
-            int base = 0;
-            if (m && lane == leader) base = atomicAdd(&s_cnt, __popc(m));
-            base = __shfl_sync(DMOLP_FULL_MASK, base, leader);
-            if (keep) dst[base + __popc(m & ((1u << lane) - 1))] = r;
-            if (more) hist_add(bin, use_smem, shist, gh_next);
-            if (a.has_split) {  // the LP window: stamp, append, decision class (all lanes take part)
-                int v = 0, cls = -1;
-                if (take) {
-                    v = (int)(key & vmask);
-                    const int dk = (int)(key >> a.sp.ibits);
-                    const int deg = __ldg(a.sp.RE + p) > 1.0 ? a.sp.maxdeg - dk : dk;
-                    a.sp.sstamp[v] = a.sp.t;
-                    te += (unsigned long long)deg;
-                    cls = dec_class(deg, p, a.sp.eff);
+            const unsigned below = (1u << lane) - 1;
+            {  // kept records to this block's slice: one shared atomic for the step
+                unsigned m[kPartU];
+                int tot = 0;
+#pragma unroll
+                for (int u = 0; u < kPartU; ++u) {
+                    m[u] = __ballot_sync(DMOLP_FULL_MASK, keep[u]);
+                    tot += __popc(m[u]);
                 }
-                // the four appends (window, classes 0-2) with their atomics in flight together: lane j
-                // reserves list j's slots
-                const unsigned mw = __ballot_sync(DMOLP_FULL_MASK, take);
-                if (mw) {
-                    const unsigned m0 = __ballot_sync(DMOLP_FULL_MASK, cls == 0);
-                    const unsigned m1 = __ballot_sync(DMOLP_FULL_MASK, cls == 1);
-                    const unsigned m2 = __ballot_sync(DMOLP_FULL_MASK, cls == 2);
-                    int base = 0;
-                    if (lane < 4) {
-                        const unsigned mm = lane == 0 ? mw : (lane == 1 ? m0 : (lane == 2 ? m1 : m2));
-                        if (mm) base = atomicAdd(lane == 0 ? a.sp.nwin : &a.sp.ndec[lane - 1], __popc(mm));
+                int base = 0;
+                if (tot && lane == 0) base = atomicAdd(&s_cnt, tot);
+                base = __shfl_sync(DMOLP_FULL_MASK, base, 0);
+#pragma unroll
+                for (int u = 0; u < kPartU; ++u) {
+                    if (keep[u]) dst[base + __popc(m[u] & below)] = r[u];
+                    base += __popc(m[u]);
+                }
+            }
+            if (more)
+#pragma unroll
+                for (int u = 0; u < kPartU; ++u) hist_add(bin[u], use_smem, shist, gh_next);
+            if (a.has_split) {  // the LP window: stamp, append, decision class (all lanes take part)
+                int v[kPartU], cls[kPartU];
+#pragma unroll
+                for (int u = 0; u < kPartU; ++u) {
+                    v[u] = 0;
+                    cls[u] = -1;
+                    if (take[u]) {
+                        v[u] = (int)(key[u] & vmask);
+                        const int dk = (int)(key[u] >> a.sp.ibits);
+                        const int deg = __ldg(a.sp.RE + p[u]) > 1.0 ? a.sp.maxdeg - dk : dk;
+                        a.sp.sstamp[v[u]] = a.sp.t;
+                        te += (unsigned long long)deg;
+                        cls[u] = dec_class(deg, p[u], a.sp.eff);
                     }
-                    const int bw = __shfl_sync(DMOLP_FULL_MASK, base, 0);
-                    const int b0 = __shfl_sync(DMOLP_FULL_MASK, base, 1);
-                    const int b1 = __shfl_sync(DMOLP_FULL_MASK, base, 2);
-                    const int b2 = __shfl_sync(DMOLP_FULL_MASK, base, 3);
-                    if (take) {
-                        const unsigned below = (1u << lane) - 1;
-                        a.sp.win[bw + __popc(mw & below)] = v;
-                        const unsigned mc = cls == 0 ? m0 : (cls == 1 ? m1 : m2);
-                        const int bc = cls == 0 ? b0 : (cls == 1 ? b1 : b2);
-                        a.sp.dec[cls][bc + __popc(mc & below)] = v;
+                }
+                // list j (0 window, 1-3 classes 0-2): the step's appends reserved by lane j's one atomic
+                unsigned ml[4][kPartU];
+                int cnt = 0;  // lane j: list j's appends of the step
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    int tj = 0;
+#pragma unroll
+                    for (int u = 0; u < kPartU; ++u) {
+                        ml[j][u] = __ballot_sync(DMOLP_FULL_MASK, j == 0 ? take[u] : cls[u] == j - 1);
+                        tj += __popc(ml[j][u]);
                     }
+                    if (lane == j) cnt = tj;
+                }
+                int base = 0;
+                if (lane < 4 && cnt) base = atomicAdd(lane == 0 ? a.sp.nwin : &a.sp.ndec[lane - 1], cnt);
+                int bl[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) bl[j] = __shfl_sync(DMOLP_FULL_MASK, base, j);
+#pragma unroll
+                for (int u = 0; u < kPartU; ++u) {
+                    if (take[u]) {
+                        a.sp.win[bl[0] + __popc(ml[0][u] & below)] = v[u];
+                        const int c = cls[u];
+                        const unsigned mc = c == 0 ? ml[1][u] : (c == 1 ? ml[2][u] : ml[3][u]);
+                        const int bc = c == 0 ? bl[1] : (c == 1 ? bl[2] : bl[3]);
+                        a.sp.dec[c][bc + __popc(mc & below)] = v[u];
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) bl[j] += __popc(ml[j][u]);
                 }
             }
         }
