@@ -107,6 +107,10 @@ struct Buffers {
     int32_t *hotid = nullptr;  // [kHotMax] vertex of each rank
     uint8_t *hotlab = nullptr; // [kHotMax] label of each hot vertex, clamped to 255 (kept current by k_apply)
     unsigned int *degh = nullptr;  // [65536] degree histogram (hot-set threshold)
+    // kept label counts (symmetric graphs, eff <= 32): vcnt[v * 32 + c] = neighbours of v with label c, for
+    // every vertex with at most kLargeDeg arcs (hubs: hh); built by the run's first statistics pass and
+    // kept current by k_update
+    uint16_t *vcnt = nullptr;      // [nv * 32]
     int32_t *active[2] = {nullptr, nullptr};  // [nv] radix-select active lists
     // per-part arrays (DMOLP_MAX_K); vc / intra hold signed values in two's complement
     unsigned int *hist = nullptr;        // [MAX_K * 256]
@@ -154,6 +158,7 @@ struct dmolp_ctx {
     bool rows_sorted = false;             // every row strictly increasing (precondition of the test)
     bool has_graph = false;
     bool hot_ready = false;               // colh / hrank / hotid built for the resident graph
+    bool counts_kept = false;             // the current LP run decides from vcnt / hh (no label gathers)
     int nhot = 0;                         // hot vertices
     std::vector<int32_t> h_rawdeg;        // host copy for the hub sort
     bool h_rawdeg_valid = false;          // h_rawdeg mirrors the resident raw degrees

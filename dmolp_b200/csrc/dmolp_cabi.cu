@@ -289,6 +289,7 @@ size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t 
     ALLOC(b.hotid, kHotMax);
     ALLOC(b.hotlab, kHotMax);
     ALLOC(b.degh, 65536);
+    ALLOC(b.vcnt, n * 32);
 #undef ALLOC
     return off;
 }
@@ -1116,7 +1117,9 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     if (st) return st;
     lp_hot_refresh(c);
     lp_reset_stats(c, k, nullptr);
-    lp_stats(c, k, nullptr, nullptr, true);
+    // symmetric graphs with at most 32 scored labels decide from kept label counts (no label gathers)
+    c->counts_kept = c->symmetric && L.eff <= 32;
+    lp_stats(c, k, nullptr, nullptr, true, c->counts_kept ? L.eff : 0);
     if (c->symmetric) lp_hub_counts(c, L.eff);
     lp_init_end(c, cfg->mode);
     st = check_launch(c);
@@ -1164,10 +1167,12 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
         //  bnd    : record slot (ball id, stamp, selection flag) of every vertex with arcs, offsets +
         //           boundary count of each candidate, id + window stamp per arc of a pull-mode walk, own
         //           label per boundary record
-        //  decide : list id + offsets + own label per selected vertex, id + label per arc, 8 B per mover
+        //  decide : list id + offsets + own label per selected vertex, id + label per arc, 8 B per mover;
+        //           with kept counts 64 B of counts per selected vertex and no arcs
         //  mark   : list id + offsets per window vertex, id read + stamp write per arc of a walked row
         //           (window rows up to 4096 arcs; hub rows only when the hub enters or leaves the window)
-        //  update : offsets + labels per mover, id + label + pending label + hub index per arc
+        //  update : offsets + labels per mover, id + label + pending label + hub index per arc (+ 8 B of
+        //           count updates per arc with kept counts)
         //  select : label + key of every record slot, read by the first histogram and partition pass
         const double nbk = (double)c->nb[0] + c->nb[1] + c->nb[2];
         dmolp_ctx::ProfEvents &pe = c->prof_pending;
@@ -1180,9 +1185,10 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
                 double bytes = 0;
                 if (kind == 0)
                 bytes = (t > 1 ? 8.0 : 4.0) * nbk + 5.0 * nbk + 20.0 * ncand + 8.0 * (double)d.arcs_bnd + 8.0 * d.boundary;
-                else if (kind == 1) bytes = 24.0 * d.window + 8.0 * (double)d.arcs_dec + 8.0 * d.changes;
+                else if (kind == 1)
+                    bytes = (c->counts_kept ? 88.0 : 24.0) * d.window + 8.0 * (double)d.arcs_dec + 8.0 * d.changes;
                 else if (kind == 2) bytes = (t > 1 ? 20.0 * recs[t - 2].window : 0.0) + 8.0 * (double)d.arcs_mark;
-                else if (kind == 3) bytes = 28.0 * d.changes + 16.0 * (double)d.arcs_upd;
+                else if (kind == 3) bytes = 28.0 * d.changes + (c->counts_kept ? 24.0 : 16.0) * (double)d.arcs_upd;
             else bytes = 24.0 * nbk + (double)d.window;  // select: first digit pass over every record slot
                 c->prof_ms[kind] += ems;
                 c->prof_launches[kind] += 1;

@@ -51,7 +51,8 @@ void lp_check_symmetric(dmolp_ctx *c, unsigned long long *counts);  // *b.flag: 
 void lp_fill(dmolp_ctx *c, int32_t *p, int64_t n, int32_t v);
 void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped);
 // use_hot: the hot labels are current (lp_hot_refresh since the labels were last set outside the loop)
-void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot = false);
+// keep_eff > 0: also write the kept label counts vcnt (labels < keep_eff <= 32) of every non-hub vertex
+void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot = false, int keep_eff = 0);
 void lp_hot_hist(dmolp_ctx *c);              // b.degh = histogram of min(degree, 65535), degree > 0
 void lp_hot_build(dmolp_ctx *c, int dstar);  // vertices of degree >= dstar ranked; colh; b.flag = their number
 void lp_hot_refresh(dmolp_ctx *c);           // hot labels from the resident labels

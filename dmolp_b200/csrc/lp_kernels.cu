@@ -407,6 +407,7 @@ struct DecArgs {
     int wstride;    // shared ints per warp: lane-private counters (eff <= 32), histogram, or byte counters
     int hub_ready;  // the hubs' label counts are current (kept from the movers): decide them first
     int use_hot;    // count through colh and the block's copy of the hot labels (eff <= 32)
+    int kept;       // non-hub vertices decide from their kept label counts (vcnt; eff <= 32)
 };
 
 // Label of a row entry u: a vertex id (u >= 0) or, in colh, the hot vertex of rank -(u + 2), whose label
@@ -539,63 +540,11 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
         hub_chunks(b, col, s_hot, b.dec[2], eff, lane, h, rd);
     }
 
-    // ---- warp per vertex, groups of G consecutive list entries per item ----
-    {
-        const int n = cn->ndec[1];
-        const int nwarps = (int)gridDim.x * (int)(blockDim.x >> 5);
-        int G = n / (nwarps * 4);
-        G = G < 1 ? 1 : (G > 8 ? 8 : G);
-        const int ng = (n + G - 1) / G;
-        int pend = grab_issue(&cn->dgrab[1], lane);
-        for (;;) {
-            const int g = grab_take(pend);
-            if (g >= ng) break;
-            pend = grab_issue(&cn->dgrab[1], lane);
-            const int i0 = g * G, m = n - i0 < G ? n - i0 : G;
-            int gv = 0, gown = 0;
-            int64_t gs = 0, ge = 0;
-            if (lane < m) {
-                gv = b.dec[1][i0 + lane];
-                gown = b.label[gv];
-                gs = b.off[gv];
-                ge = b.off[gv + 1];
-            }
-            for (int j = 0; j < m; ++j) {
-                const int v = __shfl_sync(DMOLP_FULL_MASK, gv, j);
-                const int own = __shfl_sync(DMOLP_FULL_MASK, gown, j);
-                const int64_t s = __shfl_sync(DMOLP_FULL_MASK, gs, j), e = __shfl_sync(DMOLP_FULL_MASK, ge, j);
-                count_row(b, col, s_hot, s, e, lane, eff, h);
-                double best;
-                int blab, own_cnt;
-                if (priv) {
-                    const int cnt = priv_total(h, eff, lane);
-                    warp_argmax(eff, b.tpen, lane, [&](int) { return cnt; }, best, blab);
-                    own_cnt = __shfl_sync(DMOLP_FULL_MASK, cnt, own & 31);
-                } else {
-                    warp_argmax(eff, b.tpen, lane, [&](int c) { return h[c]; }, best, blab);
-                    own_cnt = (unsigned)own < (unsigned)eff ? h[own] : 0;
-                }
-                if (lane == 0) {
-                    rd += (unsigned long long)(e - s);
-                    const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
-                    const int nl = best > own_raw ? blab : own;
-                    if (nl != own) park_move(b, v, nl);
-                }
-                __syncwarp();
-            }
-        }
-    }
-
-    // ---- thread per vertex: deg <= kDecSmall, own label scored, eff <= kDecSmallK.  Label counts are
-    //      bytes in this lane's column of the warp's region (word w of lane L at [w * 32 + L]: four labels
-    //      per word, conflict-free); a 64-bit mask lists the labels seen, and only those are scored -- an
-    //      absent label scores 0 <= count[own] and cannot win ----
-    {
-        const int n = cn->ndec[0];
+    if (a.kept) {
+        // ---- every other selected vertex from its kept label counts (vcnt): thread per vertex, 32 per
+        //      item, the rule of warp_argmax over labels < eff in one thread ----
+        const int n0 = cn->ndec[0], n = n0 + cn->ndec[1];
         const int ng = (n + 31) >> 5;
-        uint32_t *cw = reinterpret_cast<uint32_t *>(h) + lane;
-        if (ng > 0)
-            for (int w = 0; w < kDecSmallK / 4; ++w) cw[w * 32] = 0u;
         int pend = grab_issue(&cn->dgrab[0], lane);
         for (;;) {
             const int g = grab_take(pend);
@@ -603,41 +552,139 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
             pend = grab_issue(&cn->dgrab[0], lane);
             const int i = g * 32 + lane;
             if (i >= n) continue;
-            const int v = b.dec[0][i];
+            const int v = i < n0 ? b.dec[0][i] : b.dec[1][i - n0];
             const int own = b.label[v];
-            const int64_t s = b.off[v];
-            const int deg = (int)(b.off[v + 1] - s);
-            rd += deg;
-            unsigned long long seen = 0ull;
-            for (int j = 0; j < deg; j += 8) {
-                int u[8], l[8];
+            const uint4 *src = reinterpret_cast<const uint4 *>(b.vcnt + (size_t)v * 32);
+            uint32_t w[16];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(col + s + j + q) : kNoArc;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) l[q] = u[q] != kNoArc ? nbr_label(b.label, s_hot, u[q]) : -1;
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    if ((unsigned)l[q] < (unsigned)eff) {
-                        cw[(l[q] >> 2) * 32] += 1u << ((l[q] & 3) * 8);
-                        seen |= 1ull << l[q];
-                    }
+            for (int q = 0; q < 4; ++q) {
+                const uint4 x = src[q];
+                w[4 * q] = x.x;
+                w[4 * q + 1] = x.y;
+                w[4 * q + 2] = x.z;
+                w[4 * q + 3] = x.w;
             }
-            const int own_cnt = (int)((cw[(own >> 2) * 32] >> ((own & 3) * 8)) & 0xFFu);
             double best = -DBL_MAX;
-            int bkey = 0x7fffffff, blab = -1;
-            for (unsigned long long m = seen; m; m &= m - 1) {
-                const int c = __ffsll((long long)m) - 1;
-                const int cnt = (int)((cw[(c >> 2) * 32] >> ((c & 3) * 8)) & 0xFFu);
-                const double sc = __dmul_rn((double)cnt, b.tpen[c]);
-                const int key = tiekey(c);
-                if (better(sc, key, best, bkey)) {
-                    best = sc;
-                    bkey = key;
-                    blab = c;
+            int bkey = 0x7fffffff, blab = -1, own_cnt = 0;
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                if (c < eff) {
+                    const int cnt = (int)((w[c >> 1] >> ((c & 1) * 16)) & 0xFFFFu);
+                    const double sc = cnt > 0 ? __dmul_rn((double)cnt, __ldg(b.tpen + c)) : 0.0;
+                    const int key = tiekey(c);
+                    if (better(sc, key, best, bkey)) {
+                        best = sc;
+                        bkey = key;
+                        blab = c;
+                    }
+                    if (c == own) own_cnt = cnt;
                 }
             }
-            for (unsigned long long m = seen; m; m &= m - 1) cw[((__ffsll((long long)m) - 1) >> 2) * 32] = 0u;
-            if (blab >= 0 && best > (double)own_cnt && blab != own) park_move(b, v, blab);
+            const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
+            const int nl = best > own_raw ? blab : own;
+            if (nl != own) park_move(b, v, nl);
+        }
+    } else {
+        // ---- warp per vertex, groups of G consecutive list entries per item ----
+        {
+            const int n = cn->ndec[1];
+            const int nwarps = (int)gridDim.x * (int)(blockDim.x >> 5);
+            int G = n / (nwarps * 4);
+            G = G < 1 ? 1 : (G > 8 ? 8 : G);
+            const int ng = (n + G - 1) / G;
+            int pend = grab_issue(&cn->dgrab[1], lane);
+            for (;;) {
+                const int g = grab_take(pend);
+                if (g >= ng) break;
+                pend = grab_issue(&cn->dgrab[1], lane);
+                const int i0 = g * G, m = n - i0 < G ? n - i0 : G;
+                int gv = 0, gown = 0;
+                int64_t gs = 0, ge = 0;
+                if (lane < m) {
+                    gv = b.dec[1][i0 + lane];
+                    gown = b.label[gv];
+                    gs = b.off[gv];
+                    ge = b.off[gv + 1];
+                }
+                for (int j = 0; j < m; ++j) {
+                    const int v = __shfl_sync(DMOLP_FULL_MASK, gv, j);
+                    const int own = __shfl_sync(DMOLP_FULL_MASK, gown, j);
+                    const int64_t s = __shfl_sync(DMOLP_FULL_MASK, gs, j), e = __shfl_sync(DMOLP_FULL_MASK, ge, j);
+                    count_row(b, col, s_hot, s, e, lane, eff, h);
+                    double best;
+                    int blab, own_cnt;
+                    if (priv) {
+                        const int cnt = priv_total(h, eff, lane);
+                        warp_argmax(eff, b.tpen, lane, [&](int) { return cnt; }, best, blab);
+                        own_cnt = __shfl_sync(DMOLP_FULL_MASK, cnt, own & 31);
+                    } else {
+                        warp_argmax(eff, b.tpen, lane, [&](int c) { return h[c]; }, best, blab);
+                        own_cnt = (unsigned)own < (unsigned)eff ? h[own] : 0;
+                    }
+                    if (lane == 0) {
+                        rd += (unsigned long long)(e - s);
+                        const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
+                        const int nl = best > own_raw ? blab : own;
+                        if (nl != own) park_move(b, v, nl);
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+
+        // ---- thread per vertex: deg <= kDecSmall, own label scored, eff <= kDecSmallK.  Label counts are
+        //      bytes in this lane's column of the warp's region (word w of lane L at [w * 32 + L]: four labels
+        //      per word, conflict-free); a 64-bit mask lists the labels seen, and only those are scored -- an
+        //      absent label scores 0 <= count[own] and cannot win ----
+        {
+            const int n = cn->ndec[0];
+            const int ng = (n + 31) >> 5;
+            uint32_t *cw = reinterpret_cast<uint32_t *>(h) + lane;
+            if (ng > 0)
+                for (int w = 0; w < kDecSmallK / 4; ++w) cw[w * 32] = 0u;
+            int pend = grab_issue(&cn->dgrab[0], lane);
+            for (;;) {
+                const int g = grab_take(pend);
+                if (g >= ng) break;
+                pend = grab_issue(&cn->dgrab[0], lane);
+                const int i = g * 32 + lane;
+                if (i >= n) continue;
+                const int v = b.dec[0][i];
+                const int own = b.label[v];
+                const int64_t s = b.off[v];
+                const int deg = (int)(b.off[v + 1] - s);
+                rd += deg;
+                unsigned long long seen = 0ull;
+                for (int j = 0; j < deg; j += 8) {
+                    int u[8], l[8];
+    #pragma unroll
+                    for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(col + s + j + q) : kNoArc;
+    #pragma unroll
+                    for (int q = 0; q < 8; ++q) l[q] = u[q] != kNoArc ? nbr_label(b.label, s_hot, u[q]) : -1;
+    #pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        if ((unsigned)l[q] < (unsigned)eff) {
+                            cw[(l[q] >> 2) * 32] += 1u << ((l[q] & 3) * 8);
+                            seen |= 1ull << l[q];
+                        }
+                }
+                const int own_cnt = (int)((cw[(own >> 2) * 32] >> ((own & 3) * 8)) & 0xFFu);
+                double best = -DBL_MAX;
+                int bkey = 0x7fffffff, blab = -1;
+                for (unsigned long long m = seen; m; m &= m - 1) {
+                    const int c = __ffsll((long long)m) - 1;
+                    const int cnt = (int)((cw[(c >> 2) * 32] >> ((c & 3) * 8)) & 0xFFu);
+                    const double sc = __dmul_rn((double)cnt, b.tpen[c]);
+                    const int key = tiekey(c);
+                    if (better(sc, key, best, bkey)) {
+                        best = sc;
+                        bkey = key;
+                        blab = c;
+                    }
+                }
+                for (unsigned long long m = seen; m; m &= m - 1) cw[((__ffsll((long long)m) - 1) >> 2) * 32] = 0u;
+                if (blab >= 0 && best > (double)own_cnt && blab != own) park_move(b, v, blab);
+            }
         }
     }
     rd = warp_sum_u64(rd);
@@ -698,7 +745,7 @@ __global__ void k_hub_final(Buffers b, int eff, int t) {
 // the reverse arc (u,v) changes the same way but is never visited; weight 1 when u moves (or u == v):
 // (u,v) is visited from u's side.  Vertex counts move by one.  A hub neighbour u sees v's label go from
 // a to c: its row of label counts (labels < eff) moves by one.
-__global__ void __launch_bounds__(256, 3) k_update(Buffers b, int k, int eff, int t) {
+__global__ void __launch_bounds__(256, 3) k_update(Buffers b, int k, int eff, int t, int keep) {
     if (b.ctrl->stopped) return;
     extern __shared__ unsigned long long sacc[];  // [2k]: vertex-count deltas, intra-arc deltas
     for (int p = threadIdx.x; p < 2 * k; p += blockDim.x) sacc[p] = 0;
@@ -733,6 +780,18 @@ __global__ void __launch_bounds__(256, 3) k_update(Buffers b, int k, int eff, in
                 int32_t *row = b.hh + (size_t)hu * DMOLP_MAX_K;
                 if ((unsigned)a < (unsigned)eff) atomicAdd(&row[a], -1);
                 if ((unsigned)c < (unsigned)eff) atomicAdd(&row[c], 1);
+            } else if (keep) {
+                // u's 16-bit counts, two per word: a count leaves label a (it is >= 1: it counts v) and
+                // enters label c (it stays <= deg(u) <= kLargeDeg), so no carry or borrow crosses a half
+                uint32_t *w = reinterpret_cast<uint32_t *>(b.vcnt + (size_t)u * 32);
+                const bool ia = (unsigned)a < (unsigned)eff, ic = (unsigned)c < (unsigned)eff;
+                const uint32_t da = 1u << ((a & 1) * 16), dc = 1u << ((c & 1) * 16);
+                if (ia && ic && (a >> 1) == (c >> 1)) {
+                    atomicAdd(&w[a >> 1], dc - da);
+                } else {
+                    if (ia) atomicSub(&w[a >> 1], da);
+                    if (ic) atomicAdd(&w[c >> 1], dc);
+                }
             }
         }, [] { return false; });
         for (int o = 16; o > 0; o >>= 1) {
@@ -782,7 +841,8 @@ __global__ void k_apply(Buffers b) {
 // degree class the same-label and cut arcs.  Block ranges: [0,gv) vertex counts, then the three classes.
 struct StatsArgs {
     int k, nv, gv, g0, g1, nb0, nb1, nb2;
-    int use_hot;  // rows through colh and the block's copy of the hot labels (k <= 255)
+    int use_hot;   // rows through colh and the block's copy of the hot labels (k <= 255)
+    int keep_eff;  // > 0: write vcnt, the counts of labels < keep_eff (<= 32), of every non-hub vertex
 };
 
 __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int *stopped, const int *skip) {
@@ -798,6 +858,14 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
         load_hot(b, sh);
         s_hot = sh;
         col = b.colh;
+    }
+    // kept counts: byte counters of the thread class (word w of thread t at s_kc[w * 256 + t]) and one
+    // 32-int histogram per warp of the warp class
+    uint32_t *s_kc = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(sacc + 2 * k) + (a.use_hot ? kHotMax : 0));
+    int *s_kw = reinterpret_cast<int *>(s_kc + 8 * kBlock);
+    if (a.keep_eff) {
+        for (int i = threadIdx.x; i < 8 * kBlock; i += blockDim.x) s_kc[i] = 0u;
+        for (int i = threadIdx.x; i < kWarpsPerBlock * 32; i += blockDim.x) s_kw[i] = 0;
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -829,11 +897,26 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
                         bad |= (unsigned)l[q] >= (unsigned)k;
                         same += (l[q] == lv);
                         diff += (l[q] != lv);
+                        if ((unsigned)l[q] < (unsigned)a.keep_eff)
+                            s_kc[(l[q] >> 2) * kBlock + threadIdx.x] += 1u << ((l[q] & 3) * 8);
                     }
             }
             cut += diff;
             b.ndiff[v] = (int)diff;
             if (same && (unsigned)lv < (unsigned)k) atomicAdd(&sin[lv], (unsigned long long)same);
+            if (a.keep_eff) {  // the byte counters (deg <= 16) widened to 32 u16, cleared for the next vertex
+                uint32_t w[16];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const uint32_t x = s_kc[q * kBlock + threadIdx.x];
+                    s_kc[q * kBlock + threadIdx.x] = 0u;
+                    w[2 * q] = (x & 0xFFu) | ((x & 0xFF00u) << 8);
+                    w[2 * q + 1] = ((x >> 16) & 0xFFu) | ((x >> 8) & 0xFF0000u);
+                }
+                uint4 *dst = reinterpret_cast<uint4 *>(b.vcnt + (size_t)v * 32);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+            }
         }
     } else if (bx < a.gv + a.g0 + a.g1) {
         const int wpb = blockDim.x >> 5;
@@ -842,12 +925,20 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
             const int v = b.bucket[1][i];
             const int lv = b.label[v];
             unsigned int same = 0, diff = 0;
+            int *kw = s_kw + wib * 32;
             warp_row_wide(col, b.off[v], b.off[v + 1], lane, [&](int u) { return nbr_label(b.label, s_hot, u); },
                           [&](int, int lu) {
                 bad |= (unsigned)lu >= (unsigned)k;
                 same += (lu == lv);
                 diff += (lu != lv);
+                if ((unsigned)lu < (unsigned)a.keep_eff) atomicAdd(&kw[lu], 1);
             }, [] { return false; });
+            if (a.keep_eff) {  // lane c writes the count of label c (deg <= kLargeDeg fits 16 bits)
+                __syncwarp();
+                b.vcnt[(size_t)v * 32 + lane] = (uint16_t)kw[lane];
+                kw[lane] = 0;
+                __syncwarp();
+            }
             for (int o = 16; o > 0; o >>= 1) {
                 same += __shfl_xor_sync(DMOLP_FULL_MASK, same, o);
                 diff += __shfl_xor_sync(DMOLP_FULL_MASK, diff, o);
@@ -1243,8 +1334,9 @@ size_t dec_smem(int eff, bool use_hot) {
     return (size_t)kWarpsPerBlock * dec_wstride(eff) * sizeof(int) + (use_hot ? (size_t)kHotMax : 0);
 }
 
-DecArgs dec_args(int t, int eff, bool hub_ready, bool use_hot) {
+DecArgs dec_args(int t, int eff, bool hub_ready, bool use_hot, bool kept) {
     DecArgs a;
+    a.kept = kept ? 1 : 0;
     a.t = t;
     a.eff = eff;
     a.wstride = dec_wstride(eff);
@@ -1269,9 +1361,10 @@ int dec_grid(dmolp_ctx *c, int eff) {
 }
 
 // use_hot: the hot labels are current; applies when the graph has a hot set and k <= 255 (exact bytes).
-StatsArgs stats_args(dmolp_ctx *c, int k, bool use_hot) {
+StatsArgs stats_args(dmolp_ctx *c, int k, bool use_hot, int keep_eff = 0) {
     StatsArgs a;
     a.k = k;
+    a.keep_eff = keep_eff;
     a.use_hot = use_hot && c->nhot > 0 && k <= 255;
     a.nv = (int)c->nv;
     const int cap = c->num_sms * 8;
@@ -1287,13 +1380,14 @@ StatsArgs stats_args(dmolp_ctx *c, int k, bool use_hot) {
 int stats_grid(dmolp_ctx *c, const StatsArgs &a) { return a.gv + a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
 
 size_t stats_smem(const StatsArgs &a) {
-    return 2 * (size_t)a.k * sizeof(unsigned long long) + (a.use_hot ? (size_t)kHotMax : 0);
+    return 2 * (size_t)a.k * sizeof(unsigned long long) + (a.use_hot ? (size_t)kHotMax : 0) +
+           (a.keep_eff ? (8 * kBlock + kWarpsPerBlock * 32) * sizeof(int) : 0);
 }
 
 // The LP decisions of the selected window: hub row chunks queued, the classes counted / decided, hub
 // argmaxes last; when the hub counts are kept current, k_decide alone (hub argmaxes first).  use_hot: the
 // hot labels are current (used when the graph has a hot set and eff <= 32).
-void launch_decide(dmolp_ctx *c, int t, int eff, bool recount_hubs, bool use_hot) {
+void launch_decide(dmolp_ctx *c, int t, int eff, bool recount_hubs, bool use_hot, bool kept) {
     Buffers &b = c->b;
     const bool hubs = c->nb[2] > 0;
     if (hubs && recount_hubs) {
@@ -1301,7 +1395,8 @@ void launch_decide(dmolp_ctx *c, int t, int eff, bool recount_hubs, bool use_hot
         c->launches++;
     }
     const bool hot = use_hot && c->nhot > 0 && eff <= 32;
-    k_decide<<<dec_grid(c, eff), kBlock, dec_smem(eff, hot), c->stream>>>(b, dec_args(t, eff, !recount_hubs, hot));
+    k_decide<<<dec_grid(c, eff), kBlock, dec_smem(eff, hot && !kept), c->stream>>>(
+        b, dec_args(t, eff, !recount_hubs, hot && !kept, kept));
     c->launches++;
     if (hubs && recount_hubs) {
         k_hub_final<<<c->num_sms * 2, kBlock, 0, c->stream>>>(b, eff, t);
@@ -1356,8 +1451,8 @@ void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped) {
     c->launches++;
 }
 
-void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot) {
-    const StatsArgs a = stats_args(c, k, use_hot);
+void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot, int keep_eff) {
+    const StatsArgs a = stats_args(c, k, use_hot, keep_eff);
     k_stats<<<stats_grid(c, a), kBlock, stats_smem(a), c->stream>>>(c->b, a, stopped, skip);
     c->launches++;
 }
@@ -1458,12 +1553,13 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t, bool first, bool last)
     }
     {
         ProfScope ps(c, 1, t);
-        launch_decide(c, t, L.eff, !c->symmetric, true);
+        launch_decide(c, t, L.eff, !c->symmetric, true, c->counts_kept);
     }
     if (c->symmetric) {
         {
             ProfScope ps(c, 3, t);
-            k_update<<<grid, kBlock, 2 * L.k * sizeof(unsigned long long), c->stream>>>(b, L.k, L.eff, t);
+            k_update<<<grid, kBlock, 2 * L.k * sizeof(unsigned long long), c->stream>>>(b, L.k, L.eff, t,
+                                                                                         c->counts_kept ? 1 : 0);
         }
         k_apply<<<grid, kBlock, 0, c->stream>>>(b);
         c->launches += 2;
@@ -1500,7 +1596,7 @@ void lp_apply_list(dmolp_ctx *c, int k, int eff, int n) {
     const int grid = grid_for(c);
     k_zero_small<<<1, 1, 0, c->stream>>>(b);
     k_classify<<<grid, kBlock, 0, c->stream>>>(b, n, eff);
-    launch_decide(c, 1, eff, true, false);
+    launch_decide(c, 1, eff, true, false, false);
     k_collect_moves<<<grid, kBlock, 0, c->stream>>>(b);
     k_apply<<<grid, kBlock, 0, c->stream>>>(b);
     c->launches += 4;
