@@ -56,6 +56,7 @@ struct LpControl {
     int sel_open[2];    // radix select: segments still needing records after a pass (by pass parity)
     unsigned int bar_count, bar_gen;  // grid barrier of the cooperative selection kernel
     int wait_timeout;   // a grid barrier gave up waiting (never expected: the launch is cooperative)
+    int sel_tail;       // radix select: records appended to the list that block 0 finishes alone
 };
 
 // One LP iteration record as kept on the device.

@@ -27,6 +27,8 @@ namespace {
 constexpr int kSmemSegMax = 64;  // 64 segments * 256 digits * 4 B = 64 KiB of shared histogram
 constexpr int kSelThreads = 1024;
 constexpr int kPartU = 2;  // records per thread and step of the partition
+constexpr int kSelTail = 4096;  // at most this many records left: block 0 finishes the digits alone
+constexpr size_t kTailBytes = (size_t)kSelTail * (sizeof(uint64_t) + 4 * sizeof(int));
 constexpr unsigned int kBarrierSpins = 1u << 22;  // a generous bound; then give up and flag
 
 struct SelArgs {
@@ -43,6 +45,7 @@ struct SelArgs {
     SplitArgs sp;  // used when has_split: selected slots go straight to the LP window
     int has_split;
     int hist_ready;  // the first digit's histogram is already in buffer 0
+    int tail_ok;     // shared histograms and the tail region (kTailBytes) are in the dynamic shared memory
 };
 
 // Sense-counting grid barrier (all blocks are resident: cooperative launch).  A wait that runs past
@@ -93,6 +96,189 @@ __device__ __forceinline__ void hist_flush(bool use_smem, const unsigned int *sh
         if (shist[i]) atomicAdd(&gh[i], shist[i]);
 }
 
+// Digit decisions of one pass, the same in every block that runs them: per segment with records still
+// needed, the digit d* where the running count of cnt_at(seg * 256 + digit) crosses the need.  Records
+// below d* are selected; at d* either all of them (the need is met) or the segment stays open with the
+// rest of its need, *s_open counting open segments and *s_tied the records they keep.  Warps per segment.
+template <typename C>
+__device__ __forceinline__ void decide_digits(int nseg, int *s_need, int *s_below, int *s_keep, int *s_open,
+                                              int *s_tied, C cnt_at) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int p = wid; p < nseg; p += nw) {
+        const int nd = s_need[p];
+        if (nd <= 0) {
+            if (lane == 0) {
+                s_below[p] = 0;
+                s_keep[p] = -1;
+            }
+            continue;
+        }
+        unsigned int c[8];
+        unsigned int sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            c[j] = cnt_at(p * kRadix + lane * 8 + j);
+            sum += c[j];
+        }
+        unsigned int incl = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int y = __shfl_up_sync(DMOLP_FULL_MASK, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const unsigned int total = __shfl_sync(DMOLP_FULL_MASK, incl, 31);
+        if ((unsigned int)nd >= total) {  // every active record of the segment is selected
+            if (lane == 0) {
+                s_below[p] = kRadix;
+                s_keep[p] = -1;
+                s_need[p] = 0;
+            }
+            continue;
+        }
+        unsigned int run = incl - sum;  // exclusive prefix of this lane's 8 bins
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const unsigned int excl = run, inc = run + c[j];
+            if (excl < (unsigned int)nd && (unsigned int)nd <= inc) {
+                const int d = lane * 8 + j;
+                const unsigned int r = (unsigned int)nd - excl;
+                if (r == c[j]) {
+                    s_below[p] = d + 1;
+                    s_keep[p] = -1;
+                    s_need[p] = 0;
+                } else {
+                    s_below[p] = d;
+                    s_keep[p] = d;
+                    s_need[p] = (int)r;
+                    atomicAdd(s_open, 1);
+                    atomicAdd(s_tied, (int)c[j]);
+                }
+            }
+            run = inc;
+        }
+    }
+}
+
+// The LP window out of the selection (all 32 lanes call it): U records per lane, take[u] marking the
+// selected ones, whose key holds vertex and degree (SplitArgs).  Stamps them, adds their degrees to te and
+// appends them to the window and their decision-class lists, each list's appends of the call reserved by
+// one atomic (lane j for list j).
+template <int U>
+__device__ __forceinline__ void emit_window(const SelArgs &a, const bool *take, const uint64_t *key, const int *p,
+                                            uint64_t vmask, unsigned long long &te) {
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1;
+    int v[U], cls[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        v[u] = 0;
+        cls[u] = -1;
+        if (take[u]) {
+            v[u] = (int)(key[u] & vmask);
+            const int dk = (int)(key[u] >> a.sp.ibits);
+            const int deg = __ldg(a.sp.RE + p[u]) > 1.0 ? a.sp.maxdeg - dk : dk;
+            a.sp.sstamp[v[u]] = a.sp.t;
+            te += (unsigned long long)deg;
+            cls[u] = dec_class(deg, p[u], a.sp.eff);
+        }
+    }
+    // list j (0 window, 1-3 classes 0-2)
+    unsigned ml[4][U];
+    int cnt = 0;  // lane j: list j's appends of the call
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        int tj = 0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            ml[j][u] = __ballot_sync(DMOLP_FULL_MASK, j == 0 ? take[u] : cls[u] == j - 1);
+            tj += __popc(ml[j][u]);
+        }
+        if (lane == j) cnt = tj;
+    }
+    int base = 0;
+    if (lane < 4 && cnt) base = atomicAdd(lane == 0 ? a.sp.nwin : &a.sp.ndec[lane - 1], cnt);
+    int bl[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bl[j] = __shfl_sync(DMOLP_FULL_MASK, base, j);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        if (take[u]) {
+            a.sp.win[bl[0] + __popc(ml[0][u] & below)] = v[u];
+            const int c = cls[u];
+            const unsigned mc = c == 0 ? ml[1][u] : (c == 1 ? ml[2][u] : ml[3][u]);
+            const int bc = c == 0 ? bl[1] : (c == 1 ? bl[2] : bl[3]);
+            a.sp.dec[c][bc + __popc(mc & below)] = v[u];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bl[j] += __popc(ml[j][u]);
+    }
+}
+
+// Block 0 alone: the remaining digits [q0, npass) of the n <= kSelTail records of `list` (their id, segment
+// and key copied to shared memory), with shared histograms, the same decisions and a compaction per pass.
+__device__ void select_tail(const SelArgs &a, int q0, const int32_t *list, unsigned int *shist, int *s_need,
+                            int *s_below, int *s_keep, uint8_t *region, uint64_t vmask, unsigned long long &te) {
+    __shared__ int t_open, t_cnt, t_tied;
+    uint64_t *t_key = reinterpret_cast<uint64_t *>(region);
+    int *t_r = reinterpret_cast<int *>(t_key + kSelTail);
+    int *t_seg = t_r + kSelTail, *t_i0 = t_seg + kSelTail, *t_i1 = t_i0 + kSelTail;
+    const int nseg = a.nseg, nbins = nseg * kRadix;
+    int n = __ldcg(&a.ctl->sel_tail);  // the pass's tied count, <= kSelTail
+    n = n < kSelTail ? n : kSelTail;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int r = __ldcg(list + i);
+        t_r[i] = r;
+        t_seg[i] = a.seg[r];
+        t_key[i] = a.key[r];
+        t_i0[i] = i;
+    }
+    int m = n;
+    int *cur = t_i0, *nxt = t_i1;
+    for (int q = q0; q < a.npass; ++q) {
+        const int shift = a.top - kRadixBits * (q + 1);
+        for (int i = threadIdx.x; i < nbins; i += blockDim.x) shist[i] = 0u;
+        if (threadIdx.x == 0) {
+            t_open = 0;
+            t_cnt = 0;
+            t_tied = 0;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const int j = cur[i];
+            atomicAdd(&shist[t_seg[j] * kRadix + (int)((t_key[j] >> shift) & (kRadix - 1))], 1u);
+        }
+        __syncthreads();
+        decide_digits(nseg, s_need, s_below, s_keep, &t_open, &t_tied, [&](int i) { return shist[i]; });
+        __syncthreads();
+        const bool more = t_open > 0 && q + 1 < a.npass;
+        for (int i0 = 0; i0 < m; i0 += blockDim.x) {
+            const int i = i0 + threadIdx.x;
+            bool take = false;
+            uint64_t key = 0;
+            int p = 0;
+            if (i < m) {
+                const int j = cur[i];
+                p = t_seg[j];
+                key = t_key[j];
+                const int d = (int)((key >> shift) & (kRadix - 1));
+                if (d < s_below[p]) {
+                    a.sel[t_r[j]] = 1;
+                    take = true;
+                } else if (more && d == s_keep[p]) {
+                    nxt[atomicAdd(&t_cnt, 1)] = j;
+                }
+            }
+            if (a.has_split) emit_window<1>(a, &take, &key, &p, vmask, te);  // all lanes take part
+        }
+        __syncthreads();
+        m = t_cnt;
+        int *x = cur;
+        cur = nxt;
+        nxt = x;
+        __syncthreads();
+        if (!more) break;
+    }
+}
+
 __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
     if (a.stopped && *a.stopped) return;  // the same for every block: all return, no barrier is left open
     extern __shared__ unsigned int smem[];
@@ -101,8 +287,10 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
     unsigned int *shist = smem;
     int *s_need = reinterpret_cast<int *>(smem + (use_smem ? nbins : 0));
     int *s_below = s_need + nseg, *s_keep = s_below + nseg;
-    __shared__ int s_open, s_cnt;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint8_t *s_tail = reinterpret_cast<uint8_t *>(((uintptr_t)(s_keep + nseg) + 15) & ~(uintptr_t)15);
+    __shared__ int s_open, s_cnt, s_tied;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->sel_tail = 0;  // read only after a grid barrier
+    const int lane = threadIdx.x & 31;
     for (int p = threadIdx.x; p < nseg; p += blockDim.x) {
         if (a.has_split) {  // need[p] = min(n_p, ceil(e^(-t/5) * n_p))   (gpu_lp_boundary.cu:244, 296-297)
             const int n = a.sp.npart[p];
@@ -150,64 +338,18 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
         if (threadIdx.x == 0) {
             s_open = 0;
             s_cnt = 0;
+            s_tied = 0;
         }
         if (use_smem)  // the block's histogram of the next digit
             for (int i = threadIdx.x; i < nbins; i += blockDim.x) shist[i] = 0;
         __syncthreads();
         // ---- digit decisions, the same in every block ----
-        for (int p = wid; p < nseg; p += nw) {
-            const int nd = s_need[p];
-            if (nd <= 0) {
-                if (lane == 0) {
-                    s_below[p] = 0;
-                    s_keep[p] = -1;
-                }
-                continue;
-            }
-            unsigned int c[8];
-            unsigned int sum = 0;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                c[j] = __ldcg(gh + p * kRadix + lane * 8 + j);
-                sum += c[j];
-            }
-            unsigned int incl = sum;
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned int y = __shfl_up_sync(DMOLP_FULL_MASK, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const unsigned int total = __shfl_sync(DMOLP_FULL_MASK, incl, 31);
-            if ((unsigned int)nd >= total) {  // every active record of the segment is selected
-                if (lane == 0) {
-                    s_below[p] = kRadix;
-                    s_keep[p] = -1;
-                    s_need[p] = 0;
-                }
-                continue;
-            }
-            unsigned int run = incl - sum;  // exclusive prefix of this lane's 8 bins
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const unsigned int excl = run, inc = run + c[j];
-                if (excl < (unsigned int)nd && (unsigned int)nd <= inc) {
-                    const int d = lane * 8 + j;
-                    const unsigned int r = (unsigned int)nd - excl;
-                    if (r == c[j]) {
-                        s_below[p] = d + 1;
-                        s_keep[p] = -1;
-                        s_need[p] = 0;
-                    } else {
-                        s_below[p] = d;
-                        s_keep[p] = d;
-                        s_need[p] = (int)r;
-                        atomicAdd(&s_open, 1);
-                    }
-                }
-                run = inc;
-            }
-        }
+        decide_digits(nseg, s_need, s_below, s_keep, &s_open, &s_tied, [&](int i) { return __ldcg(gh + i); });
         __syncthreads();
         const bool more = s_open > 0 && pass + 1 < a.npass;
+        // few records left: this pass's kept records go to one list and block 0 finishes alone
+        const bool tail = more && a.tail_ok && s_tied <= kSelTail;
+        int32_t *tail_list = (pass & 1) ? a.act1 : a.act0;
         const int shift_next = shift - kRadixBits;
         // ---- partition of this block's records, and the next digit's histogram of the records kept;
         //      kPartU records per thread and step, their loads and their appends' atomics issued together ----
@@ -236,12 +378,12 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
                         take[u] = true;
                     } else if (more && d == s_keep[p[u]]) {
                         keep[u] = true;
-                        bin[u] = p[u] * kRadix + (int)((key[u] >> shift_next) & (kRadix - 1));
+                        if (!tail) bin[u] = p[u] * kRadix + (int)((key[u] >> shift_next) & (kRadix - 1));
                     }
                 }
             }
             const unsigned below = (1u << lane) - 1;
-            {  // kept records to this block's slice: one shared atomic for the step
+            {  // kept records to this block's slice (one shared atomic for the step) or to the tail list
                 unsigned m[kPartU];
                 int tot = 0;
 #pragma unroll
@@ -250,77 +392,43 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
                     tot += __popc(m[u]);
                 }
                 int base = 0;
-                if (tot && lane == 0) base = atomicAdd(&s_cnt, tot);
+                if (tot && lane == 0) base = tail ? atomicAdd(&a.ctl->sel_tail, tot) : atomicAdd(&s_cnt, tot);
                 base = __shfl_sync(DMOLP_FULL_MASK, base, 0);
+                int32_t *out = tail ? tail_list : dst;
 #pragma unroll
                 for (int u = 0; u < kPartU; ++u) {
-                    if (keep[u]) dst[base + __popc(m[u] & below)] = r[u];
+                    if (keep[u]) out[base + __popc(m[u] & below)] = r[u];
                     base += __popc(m[u]);
                 }
             }
-            if (more)
+            if (more && !tail)
 #pragma unroll
                 for (int u = 0; u < kPartU; ++u) hist_add(bin[u], use_smem, shist, gh_next);
-            if (a.has_split) {  // the LP window: stamp, append, decision class (all lanes take part)
-                int v[kPartU], cls[kPartU];
-#pragma unroll
-                for (int u = 0; u < kPartU; ++u) {
-                    v[u] = 0;
-                    cls[u] = -1;
-                    if (take[u]) {
-                        v[u] = (int)(key[u] & vmask);
-                        const int dk = (int)(key[u] >> a.sp.ibits);
-                        const int deg = __ldg(a.sp.RE + p[u]) > 1.0 ? a.sp.maxdeg - dk : dk;
-                        a.sp.sstamp[v[u]] = a.sp.t;
-                        te += (unsigned long long)deg;
-                        cls[u] = dec_class(deg, p[u], a.sp.eff);
-                    }
-                }
-                // list j (0 window, 1-3 classes 0-2): the step's appends reserved by lane j's one atomic
-                unsigned ml[4][kPartU];
-                int cnt = 0;  // lane j: list j's appends of the step
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    int tj = 0;
-#pragma unroll
-                    for (int u = 0; u < kPartU; ++u) {
-                        ml[j][u] = __ballot_sync(DMOLP_FULL_MASK, j == 0 ? take[u] : cls[u] == j - 1);
-                        tj += __popc(ml[j][u]);
-                    }
-                    if (lane == j) cnt = tj;
-                }
-                int base = 0;
-                if (lane < 4 && cnt) base = atomicAdd(lane == 0 ? a.sp.nwin : &a.sp.ndec[lane - 1], cnt);
-                int bl[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) bl[j] = __shfl_sync(DMOLP_FULL_MASK, base, j);
-#pragma unroll
-                for (int u = 0; u < kPartU; ++u) {
-                    if (take[u]) {
-                        a.sp.win[bl[0] + __popc(ml[0][u] & below)] = v[u];
-                        const int c = cls[u];
-                        const unsigned mc = c == 0 ? ml[1][u] : (c == 1 ? ml[2][u] : ml[3][u]);
-                        const int bc = c == 0 ? bl[1] : (c == 1 ? bl[2] : bl[3]);
-                        a.sp.dec[c][bc + __popc(mc & below)] = v[u];
-                    }
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) bl[j] += __popc(ml[j][u]);
-                }
-            }
+            if (a.has_split) emit_window<kPartU>(a, take, key, p, vmask, te);  // all lanes take part
+        }
+        if (tail) {
+            // the tail list is complete and this pass's histogram read by every block: clear it; block 0
+            // runs the remaining digits over the list in shared memory, the others are done
+            grid_sync(a.ctl);
+            zero_share(gh, nbins);
+            if (blockIdx.x == 0) select_tail(a, pass + 1, tail_list, shist, s_need, s_below, s_keep, s_tail, vmask, te);
+            break;
         }
         if (more) hist_flush(use_smem, shist, gh_next, nbins);
         __syncthreads();
         my_n = s_cnt;
         __syncthreads();  // every thread has read s_cnt before the next pass resets it
-        if (!more) break;
+        if (!more) {
+            // the last pass's histogram is still set: clear it once every block has read it
+            grid_sync(a.ctl);
+            zero_share(gh, nbins);
+            break;
+        }
     }
     if (a.has_split) {
         te = warp_sum_u64(te);
         if (lane == 0 && te) atomicAdd(a.sp.te, te);
     }
-    // the last pass's histogram is still set: clear it once every block has read it
-    grid_sync(a.ctl);
-    zero_share(a.ghist + (size_t)((pass < a.npass ? pass : a.npass - 1) % kSelHistBuffers) * nbins, nbins);
 }
 
 }  // namespace
@@ -329,7 +437,9 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
                      uint8_t *sel, const int *stopped, const SplitArgs *split, bool first_hist_ready) {
     const int npass = (keybits + kRadixBits - 1) / kRadixBits;
     const bool smem_hist = nseg <= kSmemSegMax;
-    const size_t smem = (smem_hist ? (size_t)nseg * kRadix * sizeof(unsigned int) : 0) + 3 * (size_t)nseg * sizeof(int);
+    // shared histograms, needs / decisions, and (with shared histograms) the tail region, 16-byte aligned
+    const size_t smem = (smem_hist ? (size_t)nseg * kRadix * sizeof(unsigned int) : 0) + 3 * (size_t)nseg * sizeof(int) +
+                        (smem_hist ? 16 + kTailBytes : 0);
     SelArgs a;
     a.seg = seg;
     a.key = key;
@@ -346,6 +456,7 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
     a.stopped = stopped;
     a.has_split = split != nullptr;
     a.hist_ready = first_hist_ready ? 1 : 0;
+    a.tail_ok = smem_hist ? 1 : 0;
     if (split) a.sp = *split;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)c->num_sms);  // one block per SM, all resident (cooperative launch)
@@ -364,7 +475,8 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
 
 void select_prepare() {
     cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(kSmemSegMax * kRadix * sizeof(unsigned int) + 3 * DMOLP_MAX_K * sizeof(int)));
+                         (int)(kSmemSegMax * kRadix * sizeof(unsigned int) + 3 * DMOLP_MAX_K * sizeof(int) + 16 +
+                               kTailBytes));
 }
 
 }  // namespace dmolp
