@@ -745,7 +745,7 @@ __global__ void k_hub_final(Buffers b, int eff, int t) {
 // the reverse arc (u,v) changes the same way but is never visited; weight 1 when u moves (or u == v):
 // (u,v) is visited from u's side.  Vertex counts move by one.  A hub neighbour u sees v's label go from
 // a to c: its row of label counts (labels < eff) moves by one.
-__global__ void __launch_bounds__(256, 3) k_update(Buffers b, int k, int eff, int t, int keep) {
+__global__ void __launch_bounds__(256, 2) k_update(Buffers b, int k, int eff, int t, int keep) {
     if (b.ctrl->stopped) return;
     extern __shared__ unsigned long long sacc[];  // [2k]: vertex-count deltas, intra-arc deltas
     for (int p = threadIdx.x; p < 2 * k; p += blockDim.x) sacc[p] = 0;
