@@ -160,11 +160,37 @@ __device__ __forceinline__ void decide_digits(int nseg, int *s_need, int *s_belo
 
 // The LP window out of the selection (all 32 lanes call it): U records per lane, take[u] marking the
 // selected ones, whose key holds vertex and degree (SplitArgs).  Stamps them, adds their degrees to te and
-// appends them to the window and their decision-class lists, each list's appends of the call reserved by
-// one atomic (lane j for list j).
+// appends them to the window and their decision-class lists.  With a staging area (stage: 4 lists x
+// kStage ids of this warp in shared memory, scnt: their fill), the appends collect there and a list is
+// written out with one atomic when it would overflow (stage_flush does the rest at the end); without it,
+// each list's appends of the call are reserved by one atomic (lane j for list j).
+constexpr int kStage = 128;
+static_assert((size_t)(kSelThreads / 32) * 4 * kStage * sizeof(int) <= kTailBytes, "the staging lives in the tail region");
+__device__ __forceinline__ int *list_ptr(const SelArgs &a, int j) { return j == 0 ? a.sp.win : a.sp.dec[j - 1]; }
+__device__ __forceinline__ int *list_ctr(const SelArgs &a, int j) { return j == 0 ? a.sp.nwin : &a.sp.ndec[j - 1]; }
+
+__device__ __forceinline__ void stage_flush_list(const SelArgs &a, int j, int *stage, int n) {
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0 && n) base = atomicAdd(list_ctr(a, j), n);
+    base = __shfl_sync(DMOLP_FULL_MASK, base, 0);
+    int *dst = list_ptr(a, j) + base;
+    for (int i = lane; i < n; i += 32) dst[i] = stage[i];
+}
+
+// The warp's staged ids of all four lists written out (all lanes).
+__device__ __forceinline__ void stage_flush(const SelArgs &a, int *stage, int *scnt) {
+    __syncwarp();
+    for (int j = 0; j < 4; ++j) stage_flush_list(a, j, stage + j * kStage, scnt[j]);
+    __syncwarp();
+    if ((threadIdx.x & 31) < 4) scnt[threadIdx.x & 31] = 0;
+    __syncwarp();
+}
+
 template <int U>
 __device__ __forceinline__ void emit_window(const SelArgs &a, const bool *take, const uint64_t *key, const int *p,
-                                            uint64_t vmask, unsigned long long &te) {
+                                            uint64_t vmask, unsigned long long &te, int *stage = nullptr,
+                                            int *scnt = nullptr) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1;
     int v[U], cls[U];
@@ -183,19 +209,46 @@ __device__ __forceinline__ void emit_window(const SelArgs &a, const bool *take, 
     }
     // list j (0 window, 1-3 classes 0-2)
     unsigned ml[4][U];
-    int cnt = 0;  // lane j: list j's appends of the call
+    int tl[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        int tj = 0;
+        tl[j] = 0;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             ml[j][u] = __ballot_sync(DMOLP_FULL_MASK, j == 0 ? take[u] : cls[u] == j - 1);
-            tj += __popc(ml[j][u]);
+            tl[j] += __popc(ml[j][u]);
         }
-        if (lane == j) cnt = tj;
     }
+    if (stage) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!tl[j]) continue;  // warp-uniform
+            int *sj = stage + j * kStage;
+            int c0 = scnt[j];
+            if (c0 + tl[j] > kStage) {
+                __syncwarp();
+                stage_flush_list(a, j, sj, c0);
+                c0 = 0;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const bool mine = j == 0 ? take[u] : cls[u] == j - 1;
+                if (mine) sj[c0 + __popc(ml[j][u] & below)] = v[u];
+                c0 += __popc(ml[j][u]);
+            }
+            __syncwarp();
+            if (lane == 0) scnt[j] = c0;
+            __syncwarp();
+        }
+        return;
+    }
+    int cnt = 0;  // lane j: list j's appends of the call
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (lane == j) cnt = tl[j];
     int base = 0;
-    if (lane < 4 && cnt) base = atomicAdd(lane == 0 ? a.sp.nwin : &a.sp.ndec[lane - 1], cnt);
+    if (lane < 4 && cnt) base = atomicAdd(list_ctr(a, lane), cnt);
     int bl[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) bl[j] = __shfl_sync(DMOLP_FULL_MASK, base, j);
@@ -289,6 +342,15 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
     int *s_below = s_need + nseg, *s_keep = s_below + nseg;
     uint8_t *s_tail = reinterpret_cast<uint8_t *>(((uintptr_t)(s_keep + nseg) + 15) & ~(uintptr_t)15);
     __shared__ int s_open, s_cnt, s_tied;
+    // window appends staged per warp (4 lists x kStage ids) in the tail region, which the tail uses only
+    // after every warp has flushed; without that region the appends go straight out
+    __shared__ int s_scnt[kSelThreads / 32][4];
+    int *w_stage = nullptr, *w_scnt = nullptr;
+    if (a.tail_ok && a.has_split) {
+        w_stage = reinterpret_cast<int *>(s_tail) + (threadIdx.x >> 5) * 4 * kStage;
+        w_scnt = s_scnt[threadIdx.x >> 5];
+        if ((threadIdx.x & 31) < 4) w_scnt[threadIdx.x & 31] = 0;
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl->sel_tail = 0;  // read only after a grid barrier
     const int lane = threadIdx.x & 31;
     for (int p = threadIdx.x; p < nseg; p += blockDim.x) {
@@ -404,11 +466,13 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
             if (more && !tail)
 #pragma unroll
                 for (int u = 0; u < kPartU; ++u) hist_add(bin[u], use_smem, shist, gh_next);
-            if (a.has_split) emit_window<kPartU>(a, take, key, p, vmask, te);  // all lanes take part
+            if (a.has_split) emit_window<kPartU>(a, take, key, p, vmask, te, w_stage, w_scnt);  // all lanes
         }
         if (tail) {
             // the tail list is complete and this pass's histogram read by every block: clear it; block 0
             // runs the remaining digits over the list in shared memory, the others are done
+            if (w_stage) stage_flush(a, w_stage, w_scnt);
+            __syncthreads();  // the tail region is free
             grid_sync(a.ctl);
             zero_share(gh, nbins);
             if (blockIdx.x == 0) select_tail(a, pass + 1, tail_list, shist, s_need, s_below, s_keep, s_tail, vmask, te);
@@ -419,6 +483,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
         my_n = s_cnt;
         __syncthreads();  // every thread has read s_cnt before the next pass resets it
         if (!more) {
+            if (w_stage) stage_flush(a, w_stage, w_scnt);
             // the last pass's histogram is still set: clear it once every block has read it
             grid_sync(a.ctl);
             zero_share(gh, nbins);
