@@ -548,56 +548,84 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     if (nv < 0 || nv > 0x7ffffffe || narcs < 0 || (!off && nv >= 0) || (!col && narcs > 0))
         return fail(DMOLP_ERR_ARG, "bad graph sizes or null arrays");
     if (off[0] != 0 || off[nv] != narcs) return fail(DMOLP_ERR_ARG, "offsets must start at 0 and end at narcs");
-    // Validate on the host: every device access below is then in bounds.
+    // Validate on the host: every device access below is then in bounds.  One parallel pass over the rows
+    // checks the degrees, the ids and whether every row is strictly increasing (the symmetry test's
+    // precondition), and counts each thread's vertices per degree class.
     int bad = 0, unsorted = 0;
     int64_t maxdeg = 0, maxraw = 0;
-#pragma omp parallel for reduction(| : bad, unsorted) reduction(max : maxdeg, maxraw) schedule(static)
-    for (int64_t v = 0; v < nv; ++v) {
-        const int64_t d = off[v + 1] - off[v];
-        if (d < 0 || d > 0x7fffffff) bad |= 1;
-        maxdeg = std::max(maxdeg, d);
-        if (raw) {
-            if (raw[v] < 0) bad |= 4;
-            maxraw = std::max(maxraw, (int64_t)raw[v]);
+    const int nth = std::max(1, omp_get_max_threads());
+    std::vector<int64_t> ccnt((size_t)nth * 3, 0);
+#pragma omp parallel num_threads(nth) reduction(| : bad, unsorted) reduction(max : maxdeg, maxraw)
+    {
+        const int th = omp_get_thread_num();
+        const int64_t v0 = nv * th / nth, v1 = nv * (th + 1) / nth;  // contiguous ranges: classes stay in id order
+        int64_t cc[3] = {0, 0, 0};
+        for (int64_t v = v0; v < v1; ++v) {
+            const int64_t s0 = off[v], d = off[v + 1] - s0;
+            if (d < 0 || d > 0x7fffffff || s0 < 0 || off[v + 1] > narcs) {  // the row is read only when in bounds
+                bad |= 1;
+                continue;
+            }
+            maxdeg = std::max(maxdeg, d);
+            if (raw) {
+                if (raw[v] < 0) bad |= 4;
+                maxraw = std::max(maxraw, (int64_t)raw[v]);
+            }
+            if (d == 0) continue;
+            cc[d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2)]++;
+            const int32_t *r = col + s0;
+            uint32_t prev = (uint32_t)r[0];
+            if (prev >= (uint64_t)nv) bad |= 2;
+            for (int64_t j = 1; j < d; ++j) {
+                const uint32_t x = (uint32_t)r[j];
+                if (x >= (uint64_t)nv) bad |= 2;
+                if ((int32_t)x <= (int32_t)prev) unsorted = 1;
+                prev = x;
+            }
         }
+        for (int i = 0; i < 3; ++i) ccnt[(size_t)th * 3 + i] = cc[i];
     }
     if (!raw) maxraw = maxdeg;
-    if (!bad) {
-#pragma omp parallel for reduction(| : bad) schedule(static)
-        for (int64_t j = 0; j < narcs; ++j)
-            if ((uint32_t)col[j] >= (uint64_t)nv) bad |= 2;
-    }
-    if (!bad) {  // rows strictly increasing: a precondition of the symmetry test
-#pragma omp parallel for reduction(| : unsorted) schedule(dynamic, 4096)
-        for (int64_t v = 0; v < nv; ++v)
-            for (int64_t j = off[v] + 1; j < off[v + 1]; ++j)
-                if (col[j] <= col[j - 1]) {
-                    unsorted = 1;
-                    break;
-                }
-    }
     if (bad & 1) return fail(DMOLP_ERR_ARG, "offsets are not non-decreasing");
     if (bad & 2) return fail(DMOLP_ERR_ARG, "a neighbour id is outside [0, nv)");
     if (bad & 4) return fail(DMOLP_ERR_ARG, "negative raw degree");
 
-    // degree classes (isolated vertices belong to none: they are never on a boundary)
+    // degree classes (isolated vertices belong to none: they are never on a boundary), ascending ids inside
+    // a class: each thread fills its range's share at the prefix of the counts before it
     std::vector<int32_t> bl[3];
-    for (int64_t v = 0; v < nv; ++v) {
-        const int64_t d = off[v + 1] - off[v];
-        if (d == 0) continue;
-        bl[d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2)].push_back((int32_t)v);
+    std::vector<int64_t> cpos((size_t)nth * 3);
+    for (int i = 0; i < 3; ++i) {
+        int64_t acc = 0;
+        for (int th = 0; th < nth; ++th) {
+            cpos[(size_t)th * 3 + i] = acc;
+            acc += ccnt[(size_t)th * 3 + i];
+        }
+        bl[i].resize((size_t)acc);
+    }
+#pragma omp parallel num_threads(nth)
+    {
+        const int th = omp_get_thread_num();
+        const int64_t v0 = nv * th / nth, v1 = nv * (th + 1) / nth;
+        int64_t pos[3] = {cpos[(size_t)th * 3], cpos[(size_t)th * 3 + 1], cpos[(size_t)th * 3 + 2]};
+        for (int64_t v = v0; v < v1; ++v) {
+            const int64_t d = off[v + 1] - off[v];
+            if (d == 0) continue;
+            const int c = d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2);
+            bl[c][(size_t)pos[c]++] = (int32_t)v;
+        }
     }
     const int64_t nb[3] = {(int64_t)bl[0].size(), (int64_t)bl[1].size(), (int64_t)bl[2].size()};
     DMOLP_CUDA(cudaSetDevice(c->device));
     int st = graph_alloc(c, nv, narcs, maxdeg, maxraw, nb);
     if (st) return st;
-    c->h_rawdeg.resize(nv);
-    for (int64_t v = 0; v < nv; ++v) c->h_rawdeg[v] = raw ? raw[v] : (int32_t)(off[v + 1] - off[v]);
-    c->h_rawdeg_valid = true;
     Buffers &b = c->b;
     DMOLP_CUDA(cudaMemcpyAsync(b.off, off, (size_t)(nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
-    if (narcs)
+    if (narcs)  // the largest copy first, overlapping the host work below
         DMOLP_CUDA(cudaMemcpyAsync(b.col, col, (size_t)narcs * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    c->h_rawdeg.resize(nv);
+#pragma omp parallel for num_threads(nth) schedule(static)
+    for (int64_t v = 0; v < nv; ++v) c->h_rawdeg[v] = raw ? raw[v] : (int32_t)(off[v + 1] - off[v]);
+    c->h_rawdeg_valid = true;
     DMOLP_CUDA(cudaMemcpyAsync(b.rawdeg, c->h_rawdeg.data(), (size_t)nv * sizeof(int32_t), cudaMemcpyHostToDevice,
                                c->stream));
     for (int i = 0; i < 3; ++i)
