@@ -548,6 +548,16 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
     if (nv < 0 || nv > 0x7ffffffe || narcs < 0 || (!off && nv >= 0) || (!col && narcs > 0))
         return fail(DMOLP_ERR_ARG, "bad graph sizes or null arrays");
     if (off[0] != 0 || off[nv] != narcs) return fail(DMOLP_ERR_ARG, "offsets must start at 0 and end at narcs");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    // The arcs go to a device staging buffer first (from pinned memory the copy overlaps the validation
+    // below) and reach the graph only once the validation passed.
+    int32_t *stage = nullptr;
+    if (narcs) {
+        std::string err;
+        stage = (int32_t *)c->scratch.get(ingest::kTok, (size_t)narcs * sizeof(int32_t), err);
+        if (!stage) return fail(DMOLP_ERR_NOMEM, err);
+        DMOLP_CUDA(cudaMemcpyAsync(stage, col, (size_t)narcs * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    }
     // Validate on the host: every device access below is then in bounds.  One parallel pass over the rows
     // checks the degrees, the ids and whether every row is strictly increasing (the symmetry test's
     // precondition), and counts each thread's vertices per degree class.
@@ -586,6 +596,7 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
         for (int i = 0; i < 3; ++i) ccnt[(size_t)th * 3 + i] = cc[i];
     }
     if (!raw) maxraw = maxdeg;
+    if (bad) cudaStreamSynchronize(c->stream);  // the staging copy still reads the caller's arcs
     if (bad & 1) return fail(DMOLP_ERR_ARG, "offsets are not non-decreasing");
     if (bad & 2) return fail(DMOLP_ERR_ARG, "a neighbour id is outside [0, nv)");
     if (bad & 4) return fail(DMOLP_ERR_ARG, "negative raw degree");
@@ -615,13 +626,12 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
         }
     }
     const int64_t nb[3] = {(int64_t)bl[0].size(), (int64_t)bl[1].size(), (int64_t)bl[2].size()};
-    DMOLP_CUDA(cudaSetDevice(c->device));
     int st = graph_alloc(c, nv, narcs, maxdeg, maxraw, nb);
     if (st) return st;
     Buffers &b = c->b;
     DMOLP_CUDA(cudaMemcpyAsync(b.off, off, (size_t)(nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
-    if (narcs)  // the largest copy first, overlapping the host work below
-        DMOLP_CUDA(cudaMemcpyAsync(b.col, col, (size_t)narcs * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    if (narcs)
+        DMOLP_CUDA(cudaMemcpyAsync(b.col, stage, (size_t)narcs * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
     c->h_rawdeg.resize(nv);
 #pragma omp parallel for num_threads(nth) schedule(static)
     for (int64_t v = 0; v < nv; ++v) c->h_rawdeg[v] = raw ? raw[v] : (int32_t)(off[v + 1] - off[v]);
