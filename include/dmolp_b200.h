@@ -98,7 +98,9 @@ int dmolp_create(int device, dmolp_ctx **out);
 int dmolp_destroy(dmolp_ctx *ctx);
 
 /* Copy a CSR graph to the device and keep it resident.  offsets[nv+1] (int64), indices[narcs] (int32,
- * 0 <= id < nv), raw_degree[nv] (the per-line token count phase 1 sorts by; NULL = CSR degree).
+ * 0 <= id < nv), raw_degree[nv] (the per-line token count phase 1 sorts by; NULL = CSR degree).  The
+ * arrays are validated first (a rejected upload keeps the previous graph); indices in pinned host memory
+ * are copied while the validation runs.
  * Replaces the per-iteration subgraph allocation and copies of runBoundaryLPOnGPU_SubgraphUnified
  * (src/phase2/gpu_lp_boundary.cu:456-471) and the Graph built by build_local_graph_and_ghosts
  * (src/phase1/partition.cpp:182). */
