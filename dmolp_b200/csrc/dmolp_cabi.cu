@@ -642,7 +642,9 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
         if (!bl[i].empty())
             DMOLP_CUDA(cudaMemcpyAsync(b.bucket[i], bl[i].data(), bl[i].size() * sizeof(int32_t),
                                        cudaMemcpyHostToDevice, c->stream));
-    return graph_finish(c, !unsorted);
+    st = graph_finish(c, !unsorted);  // ends with a stream sync: the staging copy is done
+    c->scratch.trim(ingest::kKeepScratch);
+    return st;
 }
 
 int dmolp_graph_upload_adjtext(dmolp_ctx *c, const char *text, int64_t len, dmolp_ingest_info *info) {
