@@ -5,9 +5,10 @@ Mirrors the reference's partitioning interface at one rank:
     run_phase1(graph_file, num_parts, theta)  ->  Phase1Metrics   (src/phase1/phase1.cpp:18)
     run_phase2(num_partitions)                ->  PartitioningMetrics (src/phase2/phase2.cpp:256)
 
-with the same metric definitions.  Differences, all documented in DESIGN.md: a fixed-iteration mode, an
-uncapped label mode, seed completion when the reference's seed rule finds fewer than k seeds, and errors
-returned as exceptions where the reference calls MPI_Abort.  There is no CPU fallback: every call runs the
+with the same metric definitions.  Differences: a fixed-iteration mode (exactly `iterations` iterations,
+no stopping rule), an uncapped label mode (all k labels scored instead of the first 32), seed completion
+when the reference's seed rule finds fewer than k seeds, and errors returned as exceptions where the
+reference calls MPI_Abort.  There is no CPU fallback: every call runs the
 CUDA library, and a missing library or GPU raises.
 """
 from __future__ import annotations
