@@ -28,7 +28,8 @@ class Phase1Result(ctypes.Structure):
 class IterRecord(ctypes.Structure):
     _fields_ = [("iteration", c_int32), ("window", c_int32), ("candidates", c_int32), ("changes", c_int32),
                 ("edge_cut", c_int64), ("window_hash", c_uint64), ("labels_hash", c_uint64),
-                ("te_prev", c_uint64), ("te_cand", c_uint64), ("te_sel", c_uint64), ("te_stats", c_uint64)]
+                ("te_prev", c_uint64), ("te_cand", c_uint64), ("te_sel", c_uint64), ("te_stats", c_uint64),
+                ("window_sum", c_uint64)]
 
 
 class Phase2Result(ctypes.Structure):
@@ -57,6 +58,10 @@ def lib() -> ctypes.CDLL:
                                     c_void_p, c_void_p, POINTER(Phase2Result)]
         L.oracle_lp_decide.argtypes = [c_int32, c_void_p, c_int64, c_void_p, c_int, c_int]
         L.oracle_lp_decide.restype = c_int32
+        L.oracle_fnv1a.argtypes = [c_void_p, ctypes.c_size_t]
+        L.oracle_fnv1a.restype = c_uint64
+        L.oracle_set_sum.argtypes = [c_void_p, c_int64]
+        L.oracle_set_sum.restype = c_uint64
         _lib = L
     return _lib
 
@@ -201,8 +206,19 @@ def f64_bits(x: float) -> str:
 
 
 def fnv1a(a: np.ndarray) -> int:
+    """64-bit FNV-1a over the array's bytes (the hash the reference harness writes)."""
+    a = np.ascontiguousarray(a)
+    if a.nbytes >= 4096 and os.path.exists(os.path.join(HERE, "libdmolp_oracle.so")):
+        return int(lib().oracle_fnv1a(_p(a), a.nbytes))
     h = 1469598103934665603
-    for b in np.ascontiguousarray(a).view(np.uint8).tobytes():
+    for b in a.view(np.uint8).tobytes():
         h ^= b
         h = (h * 1099511628211) & 0xFFFFFFFFFFFFFFFF
     return h
+
+
+def set_sum(ids: np.ndarray) -> int:
+    """Order-independent checksum of a vertex set: sum mod 2^64 of SplitMix64(id) (the reference harness's
+    window_sum and the CUDA path's per-iteration window checksum)."""
+    v = np.ascontiguousarray(ids, np.int32)
+    return int(lib().oracle_set_sum(_p(v), v.shape[0]))

@@ -35,6 +35,18 @@ uint64_t fnv1a(const void *data, size_t n) {
     return h;
 }
 
+// Order-independent checksum of a vertex set: sum (mod 2^64) of the SplitMix64 finaliser of each id.
+uint64_t set_sum(const int *v, size_t n) {
+    uint64_t s = 0;
+    for (size_t i = 0; i < n; ++i) {
+        uint64_t z = (uint64_t)(uint32_t)v[i] + 0x9e3779b97f4a7c15ULL;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+        s += z ^ (z >> 31);
+    }
+    return s;
+}
+
 struct Csr {
     int64_t nv;
     const int64_t *off;
@@ -643,6 +655,7 @@ int oracle_phase2(int64_t nv, const int64_t *off, const int32_t *col, int k, int
             r.changes = changes;
             r.edge_cut = prev_cut;
             r.window_hash = fnv1a(window.data(), window.size() * sizeof(int));
+            r.window_sum = set_sum(window.data(), window.size());
             r.labels_hash = fnv1a(label, (size_t)nv * sizeof(int32_t));
             r.te_prev = te_prev;
             r.te_cand = te_cand;
@@ -669,6 +682,10 @@ int oracle_phase2(int64_t nv, const int64_t *off, const int32_t *col, int k, int
     res->total_edges = fs.total_edges;
     return 0;
 }
+
+uint64_t oracle_fnv1a(const void *data, size_t n) { return fnv1a(data, n); }
+
+uint64_t oracle_set_sum(const int32_t *v, int64_t n) { return set_sum(v, (size_t)n); }
 
 int32_t oracle_lp_decide(int32_t own, const int32_t *nbr_labels, int64_t deg, const double *penalty, int k, int cap) {
     return lp_decide(own, nbr_labels, deg, penalty, k, cap);

@@ -4,6 +4,7 @@
  */
 #ifndef DMOLP_ORACLE_H
 #define DMOLP_ORACLE_H
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -31,6 +32,7 @@ typedef struct {
     uint64_t window_hash;
     uint64_t labels_hash;
     uint64_t te_prev, te_cand, te_sel, te_stats;
+    uint64_t window_sum; /* sum of SplitMix64(id) over the window, mod 2^64 */
 } oracle_iter_record;
 
 typedef struct {
@@ -69,6 +71,8 @@ int oracle_phase2(int64_t nv, const int64_t *off, const int32_t *col, int k, int
 int32_t oracle_lp_decide(int32_t own, const int32_t *nbr_labels, int64_t deg, const double *penalty, int k, int cap);
 
 const char *oracle_last_error(void);
+uint64_t oracle_fnv1a(const void *data, size_t n);
+uint64_t oracle_set_sum(const int32_t *v, int64_t n);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,20 @@ uint64_t set_hash(std::vector<int> v) {
     return fnv1a(v.data(), v.size() * sizeof(int));
 }
 
+// Order-independent checksum of a vertex set: the sum (mod 2^64) of the SplitMix64 finaliser of each id.
+// The CUDA path accumulates the same sum while it emits a window, so whole runs can be compared per
+// iteration without copying windows back.
+uint64_t set_sum(const std::vector<int> &v) {
+    uint64_t s = 0;
+    for (int x : v) {
+        uint64_t z = (uint64_t)(uint32_t)x + 0x9e3779b97f4a7c15ULL;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+        s += z ^ (z >> 31);
+    }
+    return s;
+}
+
 /*
  * CPU restatement of boundaryLPKernel_unified (gpu_lp_boundary.cu:327-427): one simulated warp per
  * boundary index; shared double histogram of neighbour labels < min(k,32) (:358-384); best starts at the
@@ -280,10 +294,11 @@ PartitioningMetrics run_phase2_fixed(int k, int iters, Graph &g, GhostNodes &gh,
         te_total += te_prev + te_cand + te_sel + te_stats;
         if (trace) {
             fprintf(trace,
-                    "{\"iter\":%d,\"window\":%zu,\"window_hash\":\"%016llx\",\"candidates\":%zu,\"changes\":%d,"
+                    "{\"iter\":%d,\"window\":%zu,\"window_hash\":\"%016llx\",\"window_sum\":\"%016llx\",\"candidates\":%zu,\"changes\":%d,"
                     "\"edge_cut\":%d,\"labels_hash\":\"%016llx\",\"vertex_counts\":%s,\"edge_counts\":%s,"
                     "\"penalty\":%s,\"RE\":%s,\"te\":[%llu,%llu,%llu,%llu]}\n",
-                    iter + 1, window.size(), (unsigned long long)set_hash(window), cand.size(), changes,
+                    iter + 1, window.size(), (unsigned long long)set_hash(window), (unsigned long long)set_sum(window),
+                    cand.size(), changes,
                     prev_edge_cut,
                     (unsigned long long)fnv1a(g.vertex_labels.data(), g.vertex_labels.size() * sizeof(int)),
                     json_ivec(stats.global_vertex_counts).c_str(), json_ivec(stats.global_edge_counts).c_str(),
