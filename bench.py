@@ -155,6 +155,28 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
 
 
+def golden_parity(w: dict, labels1: np.ndarray, labels: np.ndarray, result) -> dict | None:
+    """The timed run against the reference's own outputs for this workload (tests/golden/rmat22_full.json,
+    written by tests/golden/make_golden_full.py from the reference's phase-2 steps): phase-1 labels, final
+    labels, edge cut and traversed edges.  None when no fixture covers the workload."""
+    from dmolp_b200 import graphs
+
+    if not (w["kind"] == "rmat" and w["scale"] == 22 and w["edge_factor"] == 16 and w["seed"] == 7):
+        return None
+    try:
+        gold = json.load(open(os.path.join(ROOT, "tests", "golden", "rmat22_full.json")))[f"k{w['k']}"]
+    except (OSError, KeyError):
+        return None
+    if gold["iters"] != w["iters"] or gold["theta"] != w["theta"]:
+        return None
+    checks = {"phase1_labels": "%016x" % graphs.fnv1a(labels1) == gold["labels1_hash"],
+              "labels": "%016x" % graphs.fnv1a(labels) == gold["labels2_hash"],
+              "edge_cut": int(result.edge_cut) == int(gold["result"]["edge_cut"]),
+              "traversed_edges": int(result.traversed_edges) == int(gold["result"]["te_total"])}
+    return {"ok": all(checks.values()), "checks": checks,
+            "against": f"reference phase-2 run, tests/golden/rmat22_full.json k{w['k']}"}
+
+
 def traffic_from_profiles(kernel: str, workload: str):
     """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/ncu_traffic.json)."""
     try:
@@ -223,6 +245,7 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
         prof[name] = dict(ms=ms.value, launches=n.value, bytes=by.value)
     p.lib.dmolp_set_profiling(p.ctx, 0)
     final_labels = p.labels()
+    parity = golden_parity(w, labels1, final_labels, last)
 
     rec_step = None
     if args.records:
@@ -237,6 +260,7 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
         p.close()
         return {"metric": "LP traversed edges/s", "value": te / elapsed, "unit": "TE/s", "ms_per_step":
                 elapsed / args.steps * 1e3, "quick": True, "kernels": prof, "gpu_launches": int(launches),
+                "parity": parity,
                 "phase1": {"gpu_ms": m1.gpu_ms, "stage_ms": m1.stage_ms, "rounds": m1.rounds}}
     # ---- end to end through the public API, host buffers in pinned memory ----
     off_h = torch.from_numpy(g.offsets).pin_memory()
@@ -299,7 +323,8 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
                    "phase1_gpu_ms": m1.gpu_ms, "phase1_stage_ms": m1.stage_ms, "phase1_rounds": m1.rounds,
                    "phase1_initial_edge_cut": m1.initial_edge_cut,
                    "l2": "inputs larger than L2 (CSR arcs %.0f MB)" % (g.indices.nbytes / 1e6),
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "parity": None if parity is None else parity["ok"], "parity_detail": parity},
         "e2e": {"value": e2e_te * world / e2e_max, "unit": "TE/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "wall_s": e2e_wall, "steps": e2e_steps},
         "gpu_launches": int(launches),

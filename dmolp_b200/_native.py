@@ -40,6 +40,8 @@ def gen() -> ctypes.CDLL:
         lib.dmolp_csr_write_adjtext.argtypes = [c_void_p, c_char_p]
         lib.dmolp_csr_free.argtypes = [c_void_p]
         lib.dmolp_csr_free.restype = None
+        lib.dmolp_fnv1a.argtypes = [c_void_p, c_int64]
+        lib.dmolp_fnv1a.restype = c_uint64
         _gen = lib
     return _gen
 

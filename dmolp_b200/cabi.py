@@ -25,11 +25,12 @@ EXPORTS = [
     "dmolp_adjtext_error", "dmolp_host_graph_nv", "dmolp_host_graph_narcs", "dmolp_host_graph_offsets",
     "dmolp_host_graph_indices", "dmolp_host_graph_raw_degree", "dmolp_host_graph_free", "dmolp_stream",
     "dmolp_labels_save", "dmolp_labels_restore", "dmolp_set_profiling", "dmolp_kernel_profile",
-    "dmolp_find_seeds", "dmolp_expand_partitions", "dmolp_current_device", "dmolp_metrics_noalloc",
+    "dmolp_set_wait_limit",
+    "dmolp_find_seeds", "dmolp_expand_partitions", "dmolp_current_device", "dmolp_device_code_version", "dmolp_metrics_noalloc",
     "dmolp_batch_create", "dmolp_batch_destroy", "dmolp_batch_upload", "dmolp_batch_labels_set",
     "dmolp_batch_labels_get", "dmolp_batch_device_labels", "dmolp_batch_stream", "dmolp_batch_lp_run",
     "dmolp_batch_autotune", "dmolp_batch_counts", "dmolp_batch_labels_save", "dmolp_batch_labels_restore",
-    "dmolp_mpnn_num_params", "dmolp_mpnn_create", "dmolp_mpnn_destroy", "dmolp_mpnn_set_params",
+    "dmolp_mpnn_num_params", "dmolp_mpnn_create", "dmolp_mpnn_destroy", "dmolp_mpnn_set_wait_limit", "dmolp_mpnn_set_params",
     "dmolp_mpnn_get_params", "dmolp_mpnn_features", "dmolp_mpnn_set_features", "dmolp_mpnn_forward",
     "dmolp_mpnn_prepare_training", "dmolp_mpnn_backward", "dmolp_mpnn_train_step", "dmolp_mpnn_decode",
     "dmolp_batch_propose", "dmolp_mpnn_gate", "dmolp_mpnn_train_gate", "dmolp_batch_phase1",
@@ -59,7 +60,8 @@ class LpResult(ctypes.Structure):
 class LpRecord(ctypes.Structure):
     _fields_ = [("iteration", c_int32), ("window", c_int32), ("candidates", c_int32), ("changes", c_int32),
                 ("boundary", c_int32), ("reserved", c_int32), ("edge_cut", c_int64), ("te_prev", c_uint64),
-                ("te_cand", c_uint64), ("te_sel", c_uint64), ("te_stats", c_uint64), ("arcs_read", c_uint64)]
+                ("te_cand", c_uint64), ("te_sel", c_uint64), ("te_stats", c_uint64), ("arcs_read", c_uint64),
+                ("window_sum", c_uint64)]
 
 
 class BatchTuning(ctypes.Structure):
@@ -89,6 +91,7 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_last_error.restype = c_char_p
     lib.dmolp_last_error.argtypes = []
     lib.dmolp_current_device.argtypes = []
+    lib.dmolp_device_code_version.argtypes = [c_int, POINTER(c_int)]
     lib.dmolp_create.argtypes = [c_int, POINTER(vp)]
     lib.dmolp_destroy.argtypes = [vp]
     lib.dmolp_graph_upload.argtypes = [vp, c_int64, c_int64, vp, vp, vp]
@@ -126,6 +129,7 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_labels_save.argtypes = [vp]
     lib.dmolp_labels_restore.argtypes = [vp]
     lib.dmolp_set_profiling.argtypes = [vp, c_int]
+    lib.dmolp_set_wait_limit.argtypes = [vp, ctypes.c_uint32]
     lib.dmolp_find_seeds.argtypes = [vp, c_int, c_int32, vp, c_int64, vp, POINTER(c_int32)]
     lib.dmolp_expand_partitions.argtypes = [vp, c_int, c_int, vp, c_int32, POINTER(c_int32)]
     lib.dmolp_metrics_noalloc.argtypes = [c_int, c_int64, vp, vp, vp, c_int, vp, POINTER(c_int64), vp, vp]
@@ -147,6 +151,7 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_mpnn_num_params.restype = c_int64
     lib.dmolp_mpnn_create.argtypes = [c_int, POINTER(vp)]
     lib.dmolp_mpnn_destroy.argtypes = [vp]
+    lib.dmolp_mpnn_set_wait_limit.argtypes = [vp, ctypes.c_uint32]
     lib.dmolp_mpnn_set_params.argtypes = [vp, vp]
     lib.dmolp_mpnn_get_params.argtypes = [vp, vp]
     lib.dmolp_mpnn_features.argtypes = [vp, vp, vp]

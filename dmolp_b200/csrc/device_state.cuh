@@ -24,6 +24,9 @@ constexpr int kChunk = 4096;     // row chunk of the window-marking kernel
 constexpr int kHotMax = 16384;   // LP gathers: labels of up to this many highest-degree vertices per block
 constexpr int kHubChunk = 2048;  // row chunk of the decisions of deg > kLargeDeg vertices
 
+// Polls of a grid-barrier generation word before the barrier gives up (about a second on B200).
+constexpr unsigned int kDefaultWaitPolls = 1u << 22;
+
 // Per-iteration counters of the LP loop (reset by the first kernel of each iteration).
 struct LpCounters {
     int ncand;        // candidates this iteration (t >= 2)
@@ -39,6 +42,7 @@ struct LpCounters {
     unsigned long long cut_arcs;   // arcs whose endpoint labels differ (kept current incrementally)
     int dgrab[3];     // decisions: work items taken so far per class (thread groups, warp groups, hub chunks)
     int nhubw;        // queued row chunks of hubs that entered or left the window
+    int ntail;        // degree-bin selection: records of partial superbins of degree >= 2048 (coarse ties)
 };
 
 // Loop control shared by the iteration kernels.
@@ -55,7 +59,7 @@ struct LpControl {
     int pull;           // next iteration finds candidates by pulling (rows scanned for a window member)
     int sel_open[2];    // radix select: segments still needing records after a pass (by pass parity)
     unsigned int bar_count, bar_gen;  // grid barrier of the cooperative selection kernel
-    int wait_timeout;   // a grid barrier gave up waiting (never expected: the launch is cooperative)
+    int wait_timeout;   // a grid barrier gave up waiting (1 + the barrier's index in the kernel)
     int sel_tail;       // radix select: records appended to the list that block 0 finishes alone
 };
 
@@ -69,6 +73,7 @@ struct LpRecordDev {
     unsigned long long arcs_bnd, arcs_dec, arcs_upd;
     unsigned long long arcs_mark;  // arcs read by the window marking (window rows, rows of hubs that changed)
     unsigned long long te_hubsel;  // arcs of the selected hubs (part of te_sel)
+    unsigned long long win_sum;    // sum of window_mix(v) over the selected window (order-independent checksum)
 };
 
 struct Buffers {
@@ -114,7 +119,13 @@ struct Buffers {
     uint16_t *vcnt = nullptr;      // [nv * 32]
     int32_t *active[2] = {nullptr, nullptr};  // [nv] radix-select active lists
     // per-part arrays (DMOLP_MAX_K); vc / intra hold signed values in two's complement
-    unsigned int *hist = nullptr;        // [MAX_K * 256]
+    unsigned int *hist = nullptr;        // [kSelHistBuffers * MAX_K * 256] radix-select histograms
+    // degree-bin window selection (k <= kDegSelMaxK): superbin counts of the boundary records per label
+    // (written by the boundary test), fine-bin counts of the partial superbins (by iteration parity), and
+    // each selection block's fine-bin counts
+    unsigned int *dsup = nullptr;        // [kDegSelMaxK * kDsBins]
+    unsigned int *dfine[2] = {nullptr, nullptr};  // [kDegSelMaxK * kDsFine] each
+    unsigned int *dcntb = nullptr;       // [num_sms * kDegSelMaxK * kDsFine]
     int32_t *need = nullptr;             // [MAX_K]
     int32_t *sel_below = nullptr;        // [MAX_K]
     int32_t *keep_digit = nullptr;       // [MAX_K]
@@ -160,6 +171,7 @@ struct dmolp_ctx {
     bool has_graph = false;
     bool hot_ready = false;               // colh / hrank / hotid built for the resident graph
     bool counts_kept = false;             // the current LP run decides from vcnt / hh (no label gathers)
+    unsigned int wait_polls = dmolp::kDefaultWaitPolls;  // polls of a grid barrier before it gives up
     int nhot = 0;                         // hot vertices
     std::vector<int32_t> h_rawdeg;        // host copy for the hub sort
     bool h_rawdeg_valid = false;          // h_rawdeg mirrors the resident raw degrees

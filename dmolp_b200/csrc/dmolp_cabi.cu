@@ -88,8 +88,18 @@ int sync(dmolp_ctx *c) {
     return check_launch(c);
 }
 
-// A grid barrier of the cooperative window selection that gave up waiting (never expected: its launch is
-// cooperative): report it, and clear the barrier state for the next launch.
+// Clears the degree-bin selection's counts (superbin and fine-bin counts of both parities).
+int clear_select_bins(dmolp_ctx *c) {
+    Buffers &b = c->b;
+    DMOLP_CUDA(cudaMemsetAsync(b.dsup, 0, (size_t)kDegSelMaxK * kDsBins * sizeof(unsigned int), c->stream));
+    for (int i = 0; i < 2; ++i)
+        DMOLP_CUDA(cudaMemsetAsync(b.dfine[i], 0, (size_t)kDegSelMaxK * kDsFine * sizeof(unsigned int), c->stream));
+    return DMOLP_OK;
+}
+
+// A grid barrier of a cooperative selection that gave up waiting (its blocks are co-resident, so only a
+// wait limit far below the default makes this happen): report it, and clear the barrier state and the
+// selections' counts for the next launch.
 int check_waits(dmolp_ctx *c) {
     if (c->launch_error != cudaSuccess) {
         const cudaError_t e = c->launch_error;
@@ -104,8 +114,14 @@ int check_waits(dmolp_ctx *c) {
     if (!to) return DMOLP_OK;
     // bar_count, bar_gen, wait_timeout are adjacent
     DMOLP_CUDA(cudaMemsetAsync(&c->b.ctrl->bar_count, 0, 3 * sizeof(int), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(c->b.hist, 0, (size_t)kSelHistBuffers * DMOLP_MAX_K * kRadix * sizeof(unsigned int),
+                               c->stream));
+    int st2 = clear_select_bins(c);
+    if (st2) return st2;
     sync(c);
-    return fail(DMOLP_ERR_CUDA, "a grid barrier of the window selection timed out");
+    return fail(DMOLP_ERR_CUDA, "grid barrier " + std::to_string(to - 1) +
+                                    " of a window selection gave up waiting (wait limit " +
+                                    std::to_string(c->wait_polls) + " polls)");
 }
 
 // The reference's balance = max over parts of count / expected (src/phase2/phase2.cpp:426-432).
@@ -244,6 +260,10 @@ size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t 
     ALLOC(b.active[0], n);
     ALLOC(b.active[1], n);
     ALLOC(b.hist, (size_t)kSelHistBuffers * DMOLP_MAX_K * kRadix);
+    ALLOC(b.dsup, (size_t)kDegSelMaxK * kDsBins);
+    ALLOC(b.dfine[0], (size_t)kDegSelMaxK * kDsFine);
+    ALLOC(b.dfine[1], (size_t)kDegSelMaxK * kDsFine);
+    ALLOC(b.dcntb, (size_t)c->num_sms * kDegSelMaxK * kDsFine);
     ALLOC(b.need, DMOLP_MAX_K);
     ALLOC(b.sel_below, DMOLP_MAX_K);
     ALLOC(b.keep_digit, DMOLP_MAX_K);
@@ -340,6 +360,10 @@ int graph_finish(dmolp_ctx *c, bool rows_sorted) {
                                c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.ctrl, 0, sizeof(LpControl), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.cnt, 0, sizeof(LpCounters), c->stream));
+    {
+        const int st0 = clear_select_bins(c);
+        if (st0) return st0;
+    }
     const int npos = c->nb[0] + c->nb[1] + c->nb[2];
     DMOLP_CUDA(cudaMemcpyAsync(&b.cnt->npos, &npos, sizeof(int), cudaMemcpyHostToDevice, c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.bown, 0xff, n * sizeof(int32_t), c->stream));  // all record slots empty
@@ -491,6 +515,23 @@ int ingest_text(dmolp_ctx *c, uint8_t *d_txt, int64_t len, int64_t body0, int64_
 extern "C" {
 
 const char *dmolp_last_error(void) { return g_err.c_str(); }
+
+int dmolp_device_code_version(int device, int *version) {
+    if (!version) return fail(DMOLP_ERR_ARG, "null pointer");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(DMOLP_ERR_NO_GPU, "no CUDA device");
+    }
+    if (device < 0 || device >= n) return fail(DMOLP_ERR_ARG, "device index out of range");
+    int cur = 0;
+    cudaGetDevice(&cur);
+    DMOLP_CUDA(cudaSetDevice(device));
+    *version = dmolp::select_binary_version();
+    cudaSetDevice(cur);
+    if (*version < 0) return fail(DMOLP_ERR_CUDA, "cudaFuncGetAttributes failed");
+    return DMOLP_OK;
+}
 
 int dmolp_current_device(void) {
     int d = 0;
@@ -855,6 +896,16 @@ int dmolp_labels_restore(dmolp_ctx *c) {
     return DMOLP_OK;
 }
 
+int dmolp_set_wait_limit(dmolp_ctx *c, uint32_t polls) {
+    if (!c) return fail(DMOLP_ERR_ARG, "null context");
+    const unsigned int v = polls ? polls : kDefaultWaitPolls;
+    if (v != c->wait_polls) {
+        drop_graphs(c);  // captured launches carry the limit as an argument
+        c->wait_polls = v;
+    }
+    return DMOLP_OK;
+}
+
 int dmolp_set_profiling(dmolp_ctx *c, int enable) {
     if (!c) return fail(DMOLP_ERR_ARG, "null context");
     c->profiling = enable != 0;
@@ -1148,6 +1199,8 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     DMOLP_CUDA(cudaEventRecord(c->ev0, c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.stamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.sstamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
+    st = clear_select_bins(c);
+    if (st) return st;
     DMOLP_CUDA(cudaMemsetAsync(b.ndiff, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
     if (c->nb[2] > 0) {
         DMOLP_CUDA(cudaMemsetAsync(b.hubwin, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
@@ -1213,7 +1266,8 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
         //           (window rows up to 4096 arcs; hub rows only when the hub enters or leaves the window)
         //  update : offsets + labels per mover, id + label + pending label + hub index per arc (+ 8 B of
         //           count updates per arc with kept counts)
-        //  select : label + key of every record slot, read by the first histogram and partition pass
+        //  select : label + key of every record slot (one pass), and per selected vertex its stamp, window
+        //           entry and decision-class entry
         const double nbk = (double)c->nb[0] + c->nb[1] + c->nb[2];
         dmolp_ctx::ProfEvents &pe = c->prof_pending;
         for (size_t i = 0; i < pe.kind.size(); ++i) {
@@ -1229,7 +1283,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
                     bytes = (c->counts_kept ? 88.0 : 24.0) * d.window + 8.0 * (double)d.arcs_dec + 8.0 * d.changes;
                 else if (kind == 2) bytes = (t > 1 ? 20.0 * recs[t - 2].window : 0.0) + 8.0 * (double)d.arcs_mark;
                 else if (kind == 3) bytes = 28.0 * d.changes + (c->counts_kept ? 24.0 : 16.0) * (double)d.arcs_upd;
-            else bytes = 24.0 * nbk + (double)d.window;  // select: first digit pass over every record slot
+            else bytes = 12.0 * nbk + 12.0 * (double)d.window;  // select
                 c->prof_ms[kind] += ems;
                 c->prof_launches[kind] += 1;
                 c->prof_bytes[kind] += bytes;
@@ -1267,6 +1321,7 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
             o.te_cand = d.te_cand;
             o.te_sel = d.te_sel;
             o.te_stats = d.te_stats;
+            o.window_sum = d.win_sum;
         }
     }
     if (res) *res = r;
@@ -1325,6 +1380,10 @@ int dmolp_window_select(dmolp_ctx *c, int k, int iteration, const double *RE, co
     const int t = iteration;
     Buffers &b = c->b;
     DMOLP_CUDA(cudaMemsetAsync(b.stamp, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
+    {
+        const int st0 = clear_select_bins(c);
+        if (st0) return st0;
+    }
     if (!pv.empty())
         DMOLP_CUDA(cudaMemcpyAsync(b.win[(t - 1) & 1], pv.data(), pv.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                                    c->stream));

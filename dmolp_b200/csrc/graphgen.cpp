@@ -132,6 +132,16 @@ extern "C" {
 
 const char *dmolp_gen_last_error(void) { return g_err.c_str(); }
 
+uint64_t dmolp_fnv1a(const void *data, int64_t n) {
+    uint64_t h = 1469598103934665603ULL;
+    const unsigned char *p = (const unsigned char *)data;
+    for (int64_t i = 0; i < n; ++i) {
+        h ^= p[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
 int dmolp_gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed, int permute,
                    dmolp_csr **out) {
     try {

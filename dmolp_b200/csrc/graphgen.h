@@ -21,6 +21,8 @@ int64_t dmolp_csr_narcs(const dmolp_csr *g);
 int dmolp_csr_copy(const dmolp_csr *g, int64_t *off, int32_t *col);
 int dmolp_csr_write_adjtext(const dmolp_csr *g, const char *path);
 void dmolp_csr_free(dmolp_csr *g);
+/* 64-bit FNV-1a over n bytes: the fingerprint the parity fixtures record for label arrays. */
+uint64_t dmolp_fnv1a(const void *data, int64_t n);
 
 #ifdef __cplusplus
 }

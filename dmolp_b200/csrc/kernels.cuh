@@ -32,6 +32,7 @@ struct SplitArgs {
     int32_t *dec[3];
     int *ndec;
     unsigned long long *te;
+    unsigned long long *wsum;  // += window_mix(v) for every selected v
     int t, eff, ibits, maxdeg;
 };
 // first_hist_ready: the writer of the records has already added every record's first digit (bits
@@ -40,6 +41,11 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
                      uint8_t *sel, const int *stopped, const SplitArgs *split = nullptr, bool first_hist_ready = false);
 inline int select_first_shift(int keybits) { return ((keybits + kRadixBits - 1) / kRadixBits - 1) * kRadixBits; }
 void select_prepare();  // kernel attributes; call once before any capture
+// The LP window by degree bins (k_select_deg): the same window as select_smallest with `split`, for at most
+// kDegSelMaxK labels, with the boundary test's superbin counts in b.dsup (BndArgs::dsup).  Returns false
+// (nothing launched) for more labels.
+bool select_window_deg(dmolp_ctx *c, int nseg, const SplitArgs &split, const int *stopped);
+int select_binary_version();  // sm version of the loaded device code (major * 10 + minor), -1 on failure
 
 // ---- LP loop (lp_kernels.cu) ----
 struct LpLaunch {

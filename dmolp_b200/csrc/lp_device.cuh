@@ -15,6 +15,15 @@ __device__ __forceinline__ int dec_class(int deg, int own, int eff) {
     return (deg > kDecSmall || (unsigned)own >= (unsigned)eff || eff > kDecSmallK) ? 1 : 0;
 }
 
+// SplitMix64 finaliser of a vertex id: summed over a window it gives an order-independent checksum of the
+// set (the oracle and the reference harness report the same sum).
+__device__ __forceinline__ unsigned long long window_mix(int v) {
+    unsigned long long z = (unsigned long long)(unsigned)v + 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
 __device__ __forceinline__ int tiekey(int c) { return (c & ~31) | (int)brev5((unsigned)c & 31u); }
 
 __device__ __forceinline__ long long sll(unsigned long long x) { return (long long)x; }

@@ -56,6 +56,7 @@ __device__ void lp_begin(const Buffers &b, int k, int t, long long narcs) {
         cn->nchunk = 0;
         cn->nhubq = 0;
         cn->nhubw = 0;
+        cn->ntail = 0;
         cn->dgrab[0] = cn->dgrab[1] = cn->dgrab[2] = 0;
         ctl->stop_now = 0;
         ctl->skip_stats = 0;
@@ -67,6 +68,7 @@ __device__ void lp_begin(const Buffers &b, int k, int t, long long narcs) {
         r.te_prev = t == 1 ? (unsigned long long)narcs : b.rec[t - 2].te_sel;
         r.te_cand = r.te_sel = r.te_stats = 0;
         r.arcs_bnd = r.arcs_dec = r.arcs_upd = r.arcs_mark = r.te_hubsel = 0;
+        r.win_sum = 0;
     }
     // ---- statistics -> expected values and calculatePenalties (phase2.cpp:110-115, 158-209) ----
     if (threadIdx.x < 32)
@@ -215,6 +217,7 @@ struct BndArgs {
     int hubwin;  // hubwin is current: hubs of the previous window make their neighbours candidates
     unsigned int *hist;  // when set: first-digit histogram of the boundary records for the selection (k <= 32)
     int hshift;          // its digit: bits [hshift, hshift + 8) of the key
+    unsigned int *dsup;  // when set: degree-superbin counts of the boundary records per label (k <= 64)
     int nb0, nb1, nb2;
     int g0, g1;  // block split: [0,g0) thread class, [g0,g0+g1) warp class, rest block class
 };
@@ -240,11 +243,12 @@ __device__ __forceinline__ void put_slot(const Buffers &b, int pos, bool isb, in
 // walks rows; at t = 1 and in push mode every record slot costs a handful of per-vertex reads.
 __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
     if (b.ctrl->stopped) return;
-    extern __shared__ int s_npart[];  // [k] boundary records per label in this block, then [k * 256] histogram
+    // [k] boundary records per label in this block, then [k * 256] first-digit or [k * kDsBins] superbin counts
+    extern __shared__ int s_npart[];
     unsigned int *s_hist = reinterpret_cast<unsigned int *>(s_npart + k);
     for (int p = threadIdx.x; p < k; p += blockDim.x) s_npart[p] = 0;
-    if (a.hist)
-        for (int i = threadIdx.x; i < k * kRadix; i += blockDim.x) s_hist[i] = 0u;
+    const int nhist = a.dsup ? k * kDsBins : (a.hist ? k * kRadix : 0);
+    for (int i = threadIdx.x; i < nhist; i += blockDim.x) s_hist[i] = 0u;
     __syncthreads();
     const bool pull = !a.all && b.ctrl->pull;
     const int tp = a.t - 1;
@@ -264,7 +268,8 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
             ++nbd;
             atomicAdd(&s_npart[own], 1);
             key = sel_key(b, own, deg, v, a.ibits, a.maxdeg);
-            if (a.hist) atomicAdd(&s_hist[own * kRadix + (int)((key >> a.hshift) & (kRadix - 1))], 1u);
+            if (a.dsup) atomicAdd(&s_hist[own * kDsBins + dsel_bin(deg).x], 1u);
+            else if (a.hist) atomicAdd(&s_hist[own * kRadix + (int)((key >> a.hshift) & (kRadix - 1))], 1u);
         }
         put_slot(b, pos, isb, own, key);
     };
@@ -396,9 +401,9 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
     __syncthreads();
     for (int p = threadIdx.x; p < k; p += blockDim.x)
         if (s_npart[p]) atomicAdd(&b.npart[p], s_npart[p]);
-    if (a.hist)
-        for (int i = threadIdx.x; i < k * kRadix; i += blockDim.x)
-            if (s_hist[i]) atomicAdd(&a.hist[i], s_hist[i]);
+    unsigned int *gh = a.dsup ? a.dsup : a.hist;
+    for (int i = threadIdx.x; i < nhist; i += blockDim.x)
+        if (s_hist[i]) atomicAdd(&gh[i], s_hist[i]);
 }
 
 // ------------------------------------------------------------------------------------ decide
@@ -1188,11 +1193,13 @@ __global__ void k_ws_begin(Buffers b, int k, int t, int nprev) {
         cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
         cn->nwin[(t - 1) & 1] = nprev;
         cn->nwin[t & 1] = 0;
+        cn->ntail = 0;
         b.ctrl->stopped = 0;
         b.ctrl->pull = 0;
         LpRecordDev &r = b.rec[t - 1];
         r.te_prev = r.te_cand = r.te_sel = r.te_stats = 0;
         r.arcs_bnd = r.arcs_dec = r.arcs_upd = 0;
+        r.win_sum = 0;
     }
 }
 
@@ -1237,22 +1244,68 @@ __global__ void k_collect_moves(Buffers b) {
 // larger endpoint only -- (degree, id) of u above v's: u must be in v's (shorter) row, by binary search.  The
 // other arcs are only counted.  With no duplicates the found reverses are distinct arcs, so the graph is
 // symmetric iff every lookup succeeds and both counts agree (flag[0] = missing, cnt[0..1] = the counts).
-__device__ __forceinline__ void sym_arc(const Buffers &b, int u, int64_t du, int v, bool &missing,
-                                        unsigned long long &big, unsigned long long &small) {
-    if (u == v) return;
-    const int64_t s = b.off[v], e = b.off[v + 1];
-    const int64_t dv = e - s;
-    if (du > dv || (du == dv && u > v)) {
-        ++big;
-        int64_t lo = s, hi = e;
-        while (lo < hi) {
-            const int64_t mid = (lo + hi) >> 1;
-            if (b.col[mid] < u) lo = mid + 1;
-            else hi = mid;
+template <int U>
+__device__ __forceinline__ void sym_arcs(const Buffers &b, int u, int64_t du, const int *v, bool &missing,
+                                         unsigned long long &big, unsigned long long &small) {
+    // U arcs (u, v[q]) at once (v[q] < 0: no arc): their rows' bounds loaded together, then lower-bound
+    // searches for u advanced in lockstep, so U independent loads are in flight per step
+    int64_t lo[U], hi[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+        lo[q] = v[q] >= 0 ? b.off[v[q]] : 0;
+        hi[q] = v[q] >= 0 ? b.off[v[q] + 1] : 0;
+    }
+    bool srch[U];
+    int64_t e[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+        const int64_t dv = hi[q] - lo[q];
+        srch[q] = false;
+        e[q] = hi[q];
+        if (v[q] >= 0 && v[q] != u) {
+            if (du > dv || (du == dv && u > v[q])) {
+                ++big;
+                srch[q] = true;
+            } else {
+                ++small;
+            }
         }
-        if (lo >= e || b.col[lo] != u) missing = true;
-    } else {
-        ++small;
+        if (!srch[q]) lo[q] = hi[q];
+    }
+    for (;;) {
+        bool any = false;
+        int x[U];
+#pragma unroll
+        for (int q = 0; q < U; ++q) x[q] = lo[q] < hi[q] ? __ldg(b.col + ((lo[q] + hi[q]) >> 1)) : 0;
+#pragma unroll
+        for (int q = 0; q < U; ++q) {
+            if (lo[q] < hi[q]) {
+                const int64_t mid = (lo[q] + hi[q]) >> 1;
+                if (x[q] < u) lo[q] = mid + 1;
+                else hi[q] = mid;
+                any |= lo[q] < hi[q];
+            }
+        }
+        if (!any) break;
+    }
+#pragma unroll
+    for (int q = 0; q < U; ++q)
+        if (srch[q] && (lo[q] >= e[q] || __ldg(b.col + lo[q]) != u)) missing = true;
+}
+
+// Every arc of u's row [s, e) in groups of U; lanes of a group (thread, warp or block) take the arcs
+// j = s + first, s + first + step, ...
+template <int U>
+__device__ __forceinline__ void sym_row(const Buffers &b, int u, int64_t s, int64_t e, int64_t first, int64_t step,
+                                        bool &missing, unsigned long long &big, unsigned long long &small) {
+    for (int64_t j0 = s + first; j0 < e; j0 += U * step) {
+        int v[U];
+#pragma unroll
+        for (int q = 0; q < U; ++q) {
+            const int64_t j = j0 + q * step;
+            v[q] = j < e ? __ldg(b.col + j) : -1;
+        }
+        sym_arcs<U>(b, u, e - s, v, missing, big, small);
     }
 }
 
@@ -1264,24 +1317,20 @@ __global__ void __launch_bounds__(256) k_symcheck(Buffers b, int g0, int g1, int
     if ((int)blockIdx.x < g0) {  // thread per vertex
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nb0; i += g0 * blockDim.x) {
             const int u = b.bucket[0][i];
-            const int64_t s = b.off[u], e = b.off[u + 1];
-            for (int64_t j = s; j < e; ++j) sym_arc(b, u, e - s, __ldg(b.col + j), missing, big, small);
+            sym_row<4>(b, u, b.off[u], b.off[u + 1], 0, 1, missing, big, small);
         }
     } else if ((int)blockIdx.x < g0 + g1) {  // warp per vertex
         const int wpb = blockDim.x >> 5;
         const int gw = ((int)blockIdx.x - g0) * wpb + (threadIdx.x >> 5), nw = g1 * wpb;
         for (int i = gw; i < nb1; i += nw) {
             const int u = b.bucket[1][i];
-            const int64_t s = b.off[u], e = b.off[u + 1];
-            for (int64_t j = s + lane; j < e; j += 32) sym_arc(b, u, e - s, __ldg(b.col + j), missing, big, small);
+            sym_row<2>(b, u, b.off[u], b.off[u + 1], lane, 32, missing, big, small);
         }
     } else {  // block per vertex
         const int gb = (int)blockIdx.x - g0 - g1, nbk = (int)gridDim.x - g0 - g1;
         for (int i = gb; i < nb2; i += nbk) {
             const int u = b.bucket[2][i];
-            const int64_t s = b.off[u], e = b.off[u + 1];
-            for (int64_t j = s + threadIdx.x; j < e; j += blockDim.x)
-                sym_arc(b, u, e - s, __ldg(b.col + j), missing, big, small);
+            sym_row<4>(b, u, b.off[u], b.off[u + 1], threadIdx.x, blockDim.x, missing, big, small);
         }
     }
     big = warp_sum_u64(big);
@@ -1305,13 +1354,15 @@ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 constexpr int kBndHistMaxK = 32;  // k_bnd builds the selection's first histogram up to this many labels
 
 // hist_for_select: k_bnd adds the first-digit histogram of its records to histogram buffer 0 of the
-// selection that follows (k <= kBndHistMaxK).
-BndArgs bnd_args(dmolp_ctx *c, int t, int all, int hubwin, int k, bool hist_for_select) {
+// radix selection that follows (k <= kBndHistMaxK); deg_sel: k_bnd counts its records per degree superbin
+// for the degree-bin selection instead.
+BndArgs bnd_args(dmolp_ctx *c, int t, int all, int hubwin, int k, bool hist_for_select, bool deg_sel = false) {
     BndArgs a;
     a.t = t;
     a.all = all;
     a.hubwin = hubwin;
-    a.hist = hist_for_select && k <= kBndHistMaxK ? c->b.hist : nullptr;
+    a.dsup = deg_sel ? c->b.dsup : nullptr;
+    a.hist = !deg_sel && hist_for_select && k <= kBndHistMaxK ? c->b.hist : nullptr;
     a.hshift = select_first_shift(c->dbits + c->ibits);
     a.ibits = c->ibits;
     a.maxdeg = (int)c->maxdeg;
@@ -1324,7 +1375,10 @@ BndArgs bnd_args(dmolp_ctx *c, int t, int all, int hubwin, int k, bool hist_for_
     return a;
 }
 
-size_t bnd_smem(int k, const BndArgs &a) { return (size_t)k * sizeof(int) + (a.hist ? (size_t)k * kRadix * sizeof(int) : 0); }
+size_t bnd_smem(int k, const BndArgs &a) {
+    return (size_t)k * sizeof(int) +
+           (a.dsup ? (size_t)k * kDsBins * sizeof(int) : (a.hist ? (size_t)k * kRadix * sizeof(int) : 0));
+}
 
 int bnd_grid(dmolp_ctx *c, const BndArgs &a) { return a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
 
@@ -1510,6 +1564,7 @@ SplitArgs split_args(const dmolp_ctx *c, const Buffers &b, int t, int eff) {
     for (int c = 0; c < 3; ++c) sp.dec[c] = b.dec[c];
     sp.ndec = b.cnt->ndec;
     sp.te = &b.rec[t - 1].te_sel;
+    sp.wsum = &b.rec[t - 1].win_sum;
     sp.t = t;
     sp.eff = eff;
     sp.npart = b.npart;
@@ -1538,10 +1593,11 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t, bool first, bool last)
             c->launches += 2;
         }
     }
+    const bool deg_sel = L.k <= kDegSelMaxK;  // the degree-bin selection (else the radix selection)
     {
         ProfScope ps(c, 0, t);
         // hubwin is cleared only for graphs with hubs
-        const BndArgs a = bnd_args(c, t, t == 1, c->nb[2] > 0, L.k, true);
+        const BndArgs a = bnd_args(c, t, t == 1, c->nb[2] > 0, L.k, true, deg_sel);
         k_bnd<<<bnd_grid(c, a), kBlock, bnd_smem(L.k, a), c->stream>>>(b, a, L.k);
         hist_ready = a.hist != nullptr;
     }
@@ -1549,7 +1605,8 @@ void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t, bool first, bool last)
     {
         ProfScope ps(c, 4, t);
         const SplitArgs sp = split_args(c, b, t, L.eff);
-        select_smallest(c, b.bown, b.bkey, &b.cnt->npos, L.k, c->dbits + c->ibits, b.bsel, stopped, &sp, hist_ready);
+        if (!(deg_sel && select_window_deg(c, L.k, sp, stopped)))
+            select_smallest(c, b.bown, b.bkey, &b.cnt->npos, L.k, c->dbits + c->ibits, b.bsel, stopped, &sp, hist_ready);
     }
     {
         ProfScope ps(c, 1, t);
@@ -1582,11 +1639,13 @@ void lp_window_from_list(dmolp_ctx *c, int k, int t, const double *RE_dev, int n
     k_ws_begin<<<1, 256, 0, c->stream>>>(b, k, t, nprev);
     k_mark<<<grid, kBlock, 0, c->stream>>>(b, t);
     k_mark_chunks<<<grid, kBlock, 0, c->stream>>>(b, t);
-    const BndArgs a = bnd_args(c, t, 0, 0, k, true);
+    const bool deg_sel = k <= kDegSelMaxK;
+    const BndArgs a = bnd_args(c, t, 0, 0, k, true, deg_sel);
     k_bnd<<<bnd_grid(c, a), kBlock, bnd_smem(k, a), c->stream>>>(b, a, k);
     c->launches += 4;
     const SplitArgs sp = split_args(c, b, t, DMOLP_MAX_K);
-    select_smallest(c, b.bown, b.bkey, &b.cnt->npos, k, c->dbits + c->ibits, b.bsel, nullptr, &sp, a.hist != nullptr);
+    if (!(deg_sel && select_window_deg(c, k, sp, nullptr)))
+        select_smallest(c, b.bown, b.bkey, &b.cnt->npos, k, c->dbits + c->ibits, b.bsel, nullptr, &sp, a.hist != nullptr);
 }
 
 // dmolp_lp_apply: window in b.cand (n entries), penalties in b.tpen; movers reported in bv/bnew.

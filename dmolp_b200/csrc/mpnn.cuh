@@ -42,6 +42,7 @@ struct GemmArgs {
     int ldo32;
     float *out_w;
     int *err;
+    uint32_t polls;  // polls of the MMA completion barrier before the GEMM gives up (then: err, TMEM freed)
 };
 
 // One launch of the tensor-core GEMM: N = output tile width, KT = K tile.

@@ -51,6 +51,7 @@ struct dmolp_mpnn {
     float *params = nullptr, *grads = nullptr, *m = nullptr, *v = nullptr;
     __nv_bfloat16 *W[3] = {}, *Wt[3] = {};
     int *err = nullptr;
+    uint32_t wait_polls = 1u << 24;  // GEMM completion-barrier polls before it gives up (dmolp_mpnn_set_wait_limit)
     double *loss = nullptr;
     int step = 0;
     std::vector<void *> fixed;
@@ -167,6 +168,7 @@ GemmArgs base_args(dmolp_mpnn *m, int rows) {
     std::memset(&g, 0, sizeof(g));
     g.rows = rows;
     g.err = m->err;
+    g.polls = m->wait_polls;
     return g;
 }
 
@@ -289,6 +291,12 @@ int dmolp_mpnn_create(int device, dmolp_mpnn **out) {
     }
     cudaMemset(m->err, 0, sizeof(int));
     *out = m;
+    return DMOLP_OK;
+}
+
+int dmolp_mpnn_set_wait_limit(dmolp_mpnn *m, uint32_t polls) {
+    if (!m) return fail(DMOLP_ERR_ARG, "null network");
+    m->wait_polls = polls ? polls : (1u << 24);
     return DMOLP_OK;
 }
 

@@ -24,7 +24,9 @@ namespace dmolp {
 namespace mpnn {
 namespace {
 
-constexpr uint32_t kWaitLimit = 1u << 20;  // polls of an mbarrier before a GEMM gives up (>> any real MMA)
+// Polls of the MMA completion barrier after a GEMM gave up (GemmArgs::polls): the MMA in flight still
+// completes before its TMEM is freed; far above any real MMA's time.
+constexpr uint32_t kWaitLimit = 1u << 24;
 
 __device__ __forceinline__ uint4 zero4() { return make_uint4(0, 0, 0, 0); }
 
@@ -104,7 +106,7 @@ __global__ void __launch_bounds__(128) k_gemm(GemmArgs g) {
                                    umma::smem_desc(b0 + 256 * s, 128, KT * 16), idesc, kc > 0 || s > 0);
                 umma::mma_commit(&mbar);
             }
-            const bool done = umma::mbar_wait(&mbar, phase, kWaitLimit);
+            const bool done = umma::mbar_wait(&mbar, phase, g.polls);
             ok = __syncthreads_and(done);
             if (!ok) break;
             phase ^= 1;

@@ -29,7 +29,6 @@ constexpr int kSelThreads = 1024;
 constexpr int kPartU = 2;  // records per thread and step of the partition
 constexpr int kSelTail = 4096;  // at most this many records left: block 0 finishes the digits alone
 constexpr size_t kTailBytes = (size_t)kSelTail * (sizeof(uint64_t) + 4 * sizeof(int));
-constexpr unsigned int kBarrierSpins = 1u << 22;  // a generous bound; then give up and flag
 
 struct SelArgs {
     const int32_t *seg;
@@ -46,15 +45,22 @@ struct SelArgs {
     int has_split;
     int hist_ready;  // the first digit's histogram is already in buffer 0
     int tail_ok;     // shared histograms and the tail region (kTailBytes) are in the dynamic shared memory
+    unsigned int polls;  // grid barrier wait limit
 };
 
-// Sense-counting grid barrier (all blocks are resident: cooperative launch).  A wait that runs past
-// kBarrierSpins sets ctl->wait_timeout and returns, so the kernel always ends.
-__device__ __forceinline__ void grid_sync(LpControl *ctl) {
+// Sense-counting grid barrier (all blocks are resident: cooperative launch).  Returns false when the wait
+// ran past `polls` polls of the generation word, or another block's barrier already gave up: then
+// ctl->wait_timeout holds 1 + the id of the first barrier that gave up, the loop is stopped, and the caller's
+// block leaves the kernel at once (every block that waits at a later barrier leaves too), so the kernel
+// always ends; the host reports the timeout and clears the barrier state.
+__device__ __forceinline__ bool grid_sync(LpControl *ctl, unsigned int polls, int id) {
+    __shared__ int s_pass;
     __threadfence();  // each thread's own global writes and reductions are visible before the arrival
     __syncthreads();
     if (threadIdx.x == 0) {
+        int pass = 1;
         volatile unsigned int *gen = &ctl->bar_gen;
+        volatile int *gave_up = &ctl->wait_timeout;
         const unsigned int g = *gen;
         __threadfence();
         if (atomicAdd(&ctl->bar_count, 1u) == gridDim.x - 1) {
@@ -63,15 +69,19 @@ __device__ __forceinline__ void grid_sync(LpControl *ctl) {
             atomicAdd(&ctl->bar_gen, 1u);
         } else {
             for (unsigned int i = 0; *gen == g; ++i) {
-                if (i >= kBarrierSpins) {
-                    atomicExch(&ctl->wait_timeout, 1);
+                if (i >= polls || *gave_up) {
+                    atomicCAS(&ctl->wait_timeout, 0, 1 + id);
+                    atomicExch(&ctl->stopped, 1);  // the iteration's later kernels return at once
+                    pass = 0;
                     break;
                 }
             }
         }
         __threadfence();
+        s_pass = pass;
     }
     __syncthreads();
+    return s_pass != 0;
 }
 
 __device__ __forceinline__ void zero_share(unsigned int *buf, int n) {
@@ -166,30 +176,31 @@ __device__ __forceinline__ void decide_digits(int nseg, int *s_need, int *s_belo
 // each list's appends of the call are reserved by one atomic (lane j for list j).
 constexpr int kStage = 128;
 static_assert((size_t)(kSelThreads / 32) * 4 * kStage * sizeof(int) <= kTailBytes, "the staging lives in the tail region");
-__device__ __forceinline__ int *list_ptr(const SelArgs &a, int j) { return j == 0 ? a.sp.win : a.sp.dec[j - 1]; }
-__device__ __forceinline__ int *list_ctr(const SelArgs &a, int j) { return j == 0 ? a.sp.nwin : &a.sp.ndec[j - 1]; }
+__device__ __forceinline__ int *list_ptr(const SplitArgs &sp, int j) { return j == 0 ? sp.win : sp.dec[j - 1]; }
+__device__ __forceinline__ int *list_ctr(const SplitArgs &sp, int j) { return j == 0 ? sp.nwin : &sp.ndec[j - 1]; }
 
-__device__ __forceinline__ void stage_flush_list(const SelArgs &a, int j, int *stage, int n) {
+__device__ __forceinline__ void stage_flush_list(const SplitArgs &sp, int j, int *stage, int n) {
     const int lane = threadIdx.x & 31;
     int base = 0;
-    if (lane == 0 && n) base = atomicAdd(list_ctr(a, j), n);
+    if (lane == 0 && n) base = atomicAdd(list_ctr(sp, j), n);
     base = __shfl_sync(DMOLP_FULL_MASK, base, 0);
-    int *dst = list_ptr(a, j) + base;
+    int *dst = list_ptr(sp, j) + base;
     for (int i = lane; i < n; i += 32) dst[i] = stage[i];
 }
 
 // The warp's staged ids of all four lists written out (all lanes).
-__device__ __forceinline__ void stage_flush(const SelArgs &a, int *stage, int *scnt) {
+__device__ __forceinline__ void stage_flush(const SplitArgs &sp, int *stage, int *scnt) {
     __syncwarp();
-    for (int j = 0; j < 4; ++j) stage_flush_list(a, j, stage + j * kStage, scnt[j]);
+    for (int j = 0; j < 4; ++j) stage_flush_list(sp, j, stage + j * kStage, scnt[j]);
     __syncwarp();
     if ((threadIdx.x & 31) < 4) scnt[threadIdx.x & 31] = 0;
     __syncwarp();
 }
 
 template <int U>
-__device__ __forceinline__ void emit_window(const SelArgs &a, const bool *take, const uint64_t *key, const int *p,
-                                            uint64_t vmask, unsigned long long &te, int *stage = nullptr,
+__device__ __forceinline__ void emit_window(const SplitArgs &sp, const bool *take, const uint64_t *key, const int *p,
+                                            uint64_t vmask, unsigned long long &te, unsigned long long &ws,
+                                            int *stage = nullptr,
                                             int *scnt = nullptr) {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1;
@@ -200,11 +211,12 @@ __device__ __forceinline__ void emit_window(const SelArgs &a, const bool *take, 
         cls[u] = -1;
         if (take[u]) {
             v[u] = (int)(key[u] & vmask);
-            const int dk = (int)(key[u] >> a.sp.ibits);
-            const int deg = __ldg(a.sp.RE + p[u]) > 1.0 ? a.sp.maxdeg - dk : dk;
-            a.sp.sstamp[v[u]] = a.sp.t;
+            const int dk = (int)(key[u] >> sp.ibits);
+            const int deg = __ldg(sp.RE + p[u]) > 1.0 ? sp.maxdeg - dk : dk;
+            sp.sstamp[v[u]] = sp.t;
             te += (unsigned long long)deg;
-            cls[u] = dec_class(deg, p[u], a.sp.eff);
+            ws += window_mix(v[u]);
+            cls[u] = dec_class(deg, p[u], sp.eff);
         }
     }
     // list j (0 window, 1-3 classes 0-2)
@@ -227,7 +239,7 @@ __device__ __forceinline__ void emit_window(const SelArgs &a, const bool *take, 
             int c0 = scnt[j];
             if (c0 + tl[j] > kStage) {
                 __syncwarp();
-                stage_flush_list(a, j, sj, c0);
+                stage_flush_list(sp, j, sj, c0);
                 c0 = 0;
             }
             __syncwarp();
@@ -248,18 +260,18 @@ __device__ __forceinline__ void emit_window(const SelArgs &a, const bool *take, 
     for (int j = 0; j < 4; ++j)
         if (lane == j) cnt = tl[j];
     int base = 0;
-    if (lane < 4 && cnt) base = atomicAdd(list_ctr(a, lane), cnt);
+    if (lane < 4 && cnt) base = atomicAdd(list_ctr(sp, lane), cnt);
     int bl[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) bl[j] = __shfl_sync(DMOLP_FULL_MASK, base, j);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         if (take[u]) {
-            a.sp.win[bl[0] + __popc(ml[0][u] & below)] = v[u];
+            sp.win[bl[0] + __popc(ml[0][u] & below)] = v[u];
             const int c = cls[u];
             const unsigned mc = c == 0 ? ml[1][u] : (c == 1 ? ml[2][u] : ml[3][u]);
             const int bc = c == 0 ? bl[1] : (c == 1 ? bl[2] : bl[3]);
-            a.sp.dec[c][bc + __popc(mc & below)] = v[u];
+            sp.dec[c][bc + __popc(mc & below)] = v[u];
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) bl[j] += __popc(ml[j][u]);
@@ -269,7 +281,8 @@ __device__ __forceinline__ void emit_window(const SelArgs &a, const bool *take, 
 // Block 0 alone: the remaining digits [q0, npass) of the n <= kSelTail records of `list` (their id, segment
 // and key copied to shared memory), with shared histograms, the same decisions and a compaction per pass.
 __device__ void select_tail(const SelArgs &a, int q0, const int32_t *list, unsigned int *shist, int *s_need,
-                            int *s_below, int *s_keep, uint8_t *region, uint64_t vmask, unsigned long long &te) {
+                            int *s_below, int *s_keep, uint8_t *region, uint64_t vmask, unsigned long long &te,
+                            unsigned long long &ws) {
     __shared__ int t_open, t_cnt, t_tied;
     uint64_t *t_key = reinterpret_cast<uint64_t *>(region);
     int *t_r = reinterpret_cast<int *>(t_key + kSelTail);
@@ -320,7 +333,7 @@ __device__ void select_tail(const SelArgs &a, int q0, const int32_t *list, unsig
                     nxt[atomicAdd(&t_cnt, 1)] = j;
                 }
             }
-            if (a.has_split) emit_window<1>(a, &take, &key, &p, vmask, te);  // all lanes take part
+            if (a.has_split) emit_window<1>(a.sp, &take, &key, &p, vmask, te, ws);  // all lanes take part
         }
         __syncthreads();
         m = t_cnt;
@@ -385,7 +398,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
         }
         hist_flush(use_smem, shist, a.ghist, nbins);
     }
-    unsigned long long te = 0;  // degrees of the selected vertices (has_split)
+    unsigned long long te = 0, ws = 0;  // degrees and window_mix sum of the selected vertices (has_split)
     const uint64_t vmask = a.has_split ? (1ull << a.sp.ibits) - 1 : 0;
     int pass = 0;
     for (; pass < a.npass; ++pass) {
@@ -394,7 +407,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
         int32_t *dst = ((pass & 1) ? a.act1 : a.act0) + lo;
         unsigned int *gh = a.ghist + (size_t)(pass % kSelHistBuffers) * nbins;
         unsigned int *gh_next = a.ghist + (size_t)((pass + 1) % kSelHistBuffers) * nbins;
-        grid_sync(a.ctl);  // this pass's histogram is complete
+        if (!grid_sync(a.ctl, a.polls, 1 + pass)) return;  // this pass's histogram is complete
         if (pass > 0)      // read by every block in the previous pass, before the barrier just passed
             zero_share(a.ghist + (size_t)((pass - 1) % kSelHistBuffers) * nbins, nbins);
         if (threadIdx.x == 0) {
@@ -466,16 +479,16 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
             if (more && !tail)
 #pragma unroll
                 for (int u = 0; u < kPartU; ++u) hist_add(bin[u], use_smem, shist, gh_next);
-            if (a.has_split) emit_window<kPartU>(a, take, key, p, vmask, te, w_stage, w_scnt);  // all lanes
+            if (a.has_split) emit_window<kPartU>(a.sp, take, key, p, vmask, te, ws, w_stage, w_scnt);  // all lanes
         }
         if (tail) {
             // the tail list is complete and this pass's histogram read by every block: clear it; block 0
             // runs the remaining digits over the list in shared memory, the others are done
-            if (w_stage) stage_flush(a, w_stage, w_scnt);
+            if (w_stage) stage_flush(a.sp, w_stage, w_scnt);
             __syncthreads();  // the tail region is free
-            grid_sync(a.ctl);
+            if (!grid_sync(a.ctl, a.polls, 9)) return;
             zero_share(gh, nbins);
-            if (blockIdx.x == 0) select_tail(a, pass + 1, tail_list, shist, s_need, s_below, s_keep, s_tail, vmask, te);
+            if (blockIdx.x == 0) select_tail(a, pass + 1, tail_list, shist, s_need, s_below, s_keep, s_tail, vmask, te, ws);
             break;
         }
         if (more) hist_flush(use_smem, shist, gh_next, nbins);
@@ -483,17 +496,381 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
         my_n = s_cnt;
         __syncthreads();  // every thread has read s_cnt before the next pass resets it
         if (!more) {
-            if (w_stage) stage_flush(a, w_stage, w_scnt);
+            if (w_stage) stage_flush(a.sp, w_stage, w_scnt);
             // the last pass's histogram is still set: clear it once every block has read it
-            grid_sync(a.ctl);
+            if (!grid_sync(a.ctl, a.polls, 10)) return;
             zero_share(gh, nbins);
             break;
         }
     }
     if (a.has_split) {
         te = warp_sum_u64(te);
+        ws = warp_sum_u64(ws);
         if (lane == 0 && te) atomicAdd(a.sp.te, te);
+        if (lane == 0 && ws) atomicAdd(a.sp.wsum, ws);
     }
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Degree-bin window selection (LP, at most kDegSelMaxK labels).
+//
+// Per label p the window takes need_p = min(n_p, ceil(e^(-t/5) n_p)) of the label's n_p boundary records:
+// the smallest degrees first, or the largest first when RE[p] > 1, ids ascending among equal degrees
+// (gpu_lp_boundary.cu:244, 282-300).  The boundary test has counted every label's records per degree
+// superbin (dsel_bin, Buffers::dsup).  One cooperative launch, one block per SM, ONE grid barrier:
+//   0. every block finds, per label, the superbin where the running count in the label's order reaches
+//      need_p; records of the superbins before it are taken, the rest of that superbin is partial;
+//   1. each warp walks its own contiguous range of record slots in order: taken records go to the window;
+//      records of a partial superbin go to the warp's list (in slot order) and into the block's fine-bin
+//      counts (stored per block in dcntb, summed into dfine); those of degree >= 2048 also to a tail list;
+//   -- grid barrier --
+//   2. every block finds, per label, the fine bin of the partial superbin where the count reaches the rest
+//      of the need.  Below degree 2048 a fine bin is a single degree, and record slots hold the vertices of
+//      one degree in ascending id order (slots follow the degree classes, ids ascending inside a class), so
+//      a record of the partial fine bin is taken when fewer than the rest of the need precede it: in the
+//      blocks before this one (dcntb), in the warps before this one, in its warp's list before it.  Block 0
+//      ranks the tail's records of a partial coarse fine bin by their keys (degree, then id).
+// ------------------------------------------------------------------------------------------------------
+constexpr int kDsThreads = 1024;
+constexpr int kDsWarps = kDsThreads / 32;
+constexpr int kDsU = 2;          // record slots per lane and step of the first walk
+constexpr int kDsTieCap = 4096;  // coarse tied records ranked in shared memory (more: ranked from global)
+
+struct DegSelArgs {
+    const int32_t *seg;        // bown: label of a boundary record, -1 for an empty slot
+    const uint64_t *key;       // bkey: (dk << ibits) | v
+    const int *n_dev;          // record slots
+    int32_t *lists;            // the warps' lists of partial-superbin records (active[0])
+    int32_t *tail;             // partial-superbin records of degree >= 2048 (active[1])
+    int *ntail;
+    unsigned int *dsup;        // [nseg * kDsBins] from the boundary test; cleared here after the barrier
+    unsigned int *dfine;       // [nseg * kDsFine] fine counts of this iteration's partial superbins
+    unsigned int *dfine_next;  // the other parity's buffer, cleared here for the next iteration
+    unsigned int *dcntb;       // [gridDim.x * nseg * kDsFine]
+    int nseg;
+    unsigned int polls;
+    LpControl *ctl;
+    const int *stopped;
+    SplitArgs sp;
+};
+
+// Dynamic shared memory of k_select_deg for nseg labels (16-byte aligned pieces).
+__host__ __device__ constexpr size_t ds_smem_bytes(int nseg) {
+    return (size_t)kDsTieCap * 8 + (size_t)kDsTieCap * 8 + (size_t)8 * nseg * 4 + (size_t)nseg * kDsFine * 4 +
+           (size_t)2 * kDsWarps * nseg * 4 + (size_t)kDsWarps * 4 * kStage * 4;
+}
+
+// Order position of superbin / fine bin x in a label's order (descending degree when dir).
+__device__ __forceinline__ int ds_ord(int x, int n, int dir) { return dir ? n - 1 - x : x; }
+
+// Running-count crossing over `per` consecutive order positions per lane (all lanes): the position where
+// the count reaches need (0 < need < total), the records before it and its count.
+template <int PER, typename C>
+__device__ __forceinline__ void ds_cross(int need, C cnt_at, int lane, int &pos, int &before, int &count) {
+    unsigned int c[PER], sum = 0;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        c[j] = cnt_at(lane * PER + j);
+        sum += c[j];
+    }
+    unsigned int incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(DMOLP_FULL_MASK, incl, o);
+        if (lane >= o) incl += y;
+    }
+    unsigned int run = incl - sum;
+    int fpos = -1, fbefore = 0, fcount = 0;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        if (run < (unsigned)need && (unsigned)need <= run + c[j]) {
+            fpos = lane * PER + j;
+            fbefore = (int)run;
+            fcount = (int)c[j];
+        }
+        run += c[j];
+    }
+    const unsigned m = __ballot_sync(DMOLP_FULL_MASK, fpos >= 0);
+    const int src = m ? __ffs(m) - 1 : 0;
+    pos = __shfl_sync(DMOLP_FULL_MASK, fpos, src);
+    before = __shfl_sync(DMOLP_FULL_MASK, fbefore, src);
+    count = __shfl_sync(DMOLP_FULL_MASK, fcount, src);
+}
+
+__global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
+    if (a.stopped && *a.stopped) return;  // the same for every block: all return, no barrier is left open
+    extern __shared__ __align__(16) unsigned char ds_smem[];
+    const int nseg = a.nseg, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1;
+    uint64_t *s_tkey = reinterpret_cast<uint64_t *>(ds_smem);       // [kDsTieCap] coarse ties (block 0)
+    int *s_tslot = reinterpret_cast<int *>(s_tkey + kDsTieCap);     // [kDsTieCap]
+    int *s_tseg = s_tslot + kDsTieCap;                              // [kDsTieCap]
+    int *s_otake = s_tseg + kDsTieCap;  // [nseg] superbin order positions below this are taken
+    int *s_opart = s_otake + nseg;      // [nseg] order position of the partial superbin, -1 none
+    int *s_rem = s_opart + nseg;        // [nseg] records still needed from the partial superbin
+    int *s_dir = s_rem + nseg;          // [nseg] 1: largest degree first (RE > 1)
+    int *s_ftake = s_dir + nseg;        // [nseg] fine order positions below this are taken
+    int *s_fpart = s_ftake + nseg;      // [nseg] fine order position of the partial fine bin, -1 none
+    int *s_frem = s_fpart + nseg;       // [nseg] records still needed from the partial fine bin
+    int *s_pre = s_frem + nseg;         // [nseg] the partial fine bin's records in the blocks before this one
+    unsigned int *s_f = reinterpret_cast<unsigned int *>(s_pre + nseg);  // [nseg * kDsFine] this block's
+    int *s_wc = reinterpret_cast<int *>(s_f + nseg * kDsFine);  // [kDsWarps * nseg] partial fine bin per warp
+    int *s_wrun = s_wc + kDsWarps * nseg;                       // [kDsWarps * nseg] running rank per warp
+    int *s_stage = s_wrun + kDsWarps * nseg;                    // [kDsWarps * 4 * kStage] window appends
+    __shared__ int s_scnt[kDsWarps][4];
+    __shared__ int s_ntie;
+    int *w_stage = s_stage + wid * 4 * kStage, *w_scnt = s_scnt[wid];
+    if (lane < 4) w_scnt[lane] = 0;
+    for (int i = threadIdx.x; i < nseg * kDsFine; i += blockDim.x) s_f[i] = 0u;
+    for (int i = threadIdx.x; i < kDsWarps * nseg; i += blockDim.x) s_wc[i] = 0;
+    if (threadIdx.x == 0) s_ntie = 0;
+    // the other parity's fine counts were read by the previous iteration's selection: clear them
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nseg * kDsFine; i += gridDim.x * blockDim.x)
+        a.dfine_next[i] = 0u;
+    // ---- 0. per label: the superbin where the need is reached ----
+    const double ratio = *a.sp.ratio;
+    for (int p = wid; p < nseg; p += kDsWarps) {
+        const int n = a.sp.npart[p];
+        const int m = (int)ceil(__dmul_rn(ratio, (double)n));  // ceil(e^(-t/5) n), gpu_lp_boundary.cu:296-297
+        const int need = m > n ? n : m;
+        const int dir = __ldg(a.sp.RE + p) > 1.0 ? 1 : 0;
+        int take = need >= n ? kDsBins : 0, part = -1, rem = 0;
+        if (need > 0 && need < n) {
+            int pos, before, count;
+            ds_cross<(kDsBins + 31) / 32>(need, [&](int o) {
+                return o < kDsBins ? __ldcg(a.dsup + p * kDsBins + ds_ord(o, kDsBins, dir)) : 0u;
+            }, lane, pos, before, count);
+            if (pos < 0) {  // inconsistent counts (never expected): take nothing more
+                take = 0;
+            } else if (need - before == count) {
+                take = pos + 1;
+            } else {
+                take = pos;
+                part = pos;
+                rem = need - before;
+            }
+        }
+        if (lane == 0) {
+            s_otake[p] = take;
+            s_opart[p] = part;
+            s_rem[p] = rem;
+            s_dir[p] = dir;
+        }
+    }
+    __syncthreads();
+    // ---- 1. each warp walks its own contiguous range of record slots ----
+    const int n0 = *a.n_dev;
+    const int cap = (n0 + gridDim.x - 1) / gridDim.x;
+    const int lo = blockIdx.x * cap;
+    const int my_n = max(0, min(n0, lo + cap) - lo);
+    const int wcap = (my_n + kDsWarps - 1) / kDsWarps;
+    const int wlo = lo + min(my_n, wid * wcap), whi = lo + min(my_n, (wid + 1) * wcap);
+    int32_t *wlist = a.lists + wlo;  // at most whi - wlo entries
+    int wl = 0;                      // the warp's list length (warp-uniform)
+    const int ibits = a.sp.ibits, maxdeg = a.sp.maxdeg;
+    const uint64_t vmask = (1ull << ibits) - 1;
+    unsigned long long te = 0, ws = 0;
+    auto bins_of = [&](uint64_t key, int p, int &o, int &fo, bool &coarse) {
+        const int dir = s_dir[p];
+        const int dk = (int)(key >> ibits);
+        const int2 bf = dsel_bin(dir ? maxdeg - dk : dk);
+        o = ds_ord(bf.x, kDsBins, dir);
+        fo = ds_ord(bf.y, kDsFine, dir);
+        coarse = bf.x >= kDsCoarse0;
+        return bf;
+    };
+    for (int r0 = wlo; r0 < whi; r0 += 32 * kDsU) {
+        int r[kDsU], p[kDsU];
+        uint64_t key[kDsU];
+        bool take[kDsU], part[kDsU], tl[kDsU];
+#pragma unroll
+        for (int u = 0; u < kDsU; ++u) {
+            r[u] = r0 + u * 32 + lane;
+            p[u] = r[u] < whi ? a.seg[r[u]] : -1;
+            key[u] = r[u] < whi ? a.key[r[u]] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kDsU; ++u) {
+            take[u] = part[u] = tl[u] = false;
+            if (p[u] >= 0) {
+                int o, fo;
+                bool coarse;
+                const int2 bf = bins_of(key[u], p[u], o, fo, coarse);
+                if (o < s_otake[p[u]]) {
+                    take[u] = true;
+                } else if (o == s_opart[p[u]]) {
+                    part[u] = true;
+                    tl[u] = coarse;
+                    atomicAdd(&s_f[p[u] * kDsFine + bf.y], 1u);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kDsU; ++u) {  // partial-superbin records to the warp's list, in slot order
+            const unsigned mp = __ballot_sync(DMOLP_FULL_MASK, part[u]);
+            if (part[u]) wlist[wl + __popc(mp & below)] = r[u];
+            wl += __popc(mp);
+            const int q = warp_append(a.ntail, tl[u]);
+            if (tl[u]) a.tail[q] = r[u];
+        }
+        emit_window<kDsU>(a.sp, take, key, p, vmask, te, ws, w_stage, w_scnt);  // all lanes
+    }
+    __syncthreads();
+    // this block's fine counts: kept per block for the prefixes, summed for the fine decisions
+    for (int i = threadIdx.x; i < nseg * kDsFine; i += blockDim.x) {
+        const unsigned int v = s_f[i];
+        a.dcntb[(size_t)blockIdx.x * nseg * kDsFine + i] = v;
+        if (v) atomicAdd(&a.dfine[i], v);
+    }
+    if (!grid_sync(a.ctl, a.polls, 0)) return;
+    // every block has read the superbin counts: clear them for the next boundary test
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nseg * kDsBins; i += gridDim.x * blockDim.x) a.dsup[i] = 0u;
+    // ---- 2. per label with a partial superbin: the fine bin where the rest of the need is reached ----
+    for (int p = wid; p < nseg; p += kDsWarps) {
+        int take = 0, part = -1, rem = 0, pre = 0;
+        const int opart = s_opart[p];
+        if (opart >= 0) {
+            const int dir = s_dir[p];
+            const int need = s_rem[p];
+            int pos, before, count;
+            ds_cross<kDsFine / 32>(need, [&](int fo) {
+                return __ldcg(a.dfine + p * kDsFine + ds_ord(fo, kDsFine, dir));
+            }, lane, pos, before, count);
+            if (pos < 0) {
+                take = 0;
+            } else if (need - before == count) {
+                take = pos + 1;
+            } else {
+                take = pos;
+                part = pos;
+                rem = need - before;
+                if (ds_ord(opart, kDsBins, dir) < kDsCoarse0) {  // one degree: the blocks before this one
+                    const int f = ds_ord(pos, kDsFine, dir);
+                    for (int b = lane; b < (int)blockIdx.x; b += 32)
+                        pre += (int)__ldcg(a.dcntb + (size_t)b * nseg * kDsFine + p * kDsFine + f);
+                    for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(DMOLP_FULL_MASK, pre, o);
+                }
+            }
+        }
+        if (lane == 0) {
+            s_ftake[p] = take;
+            s_fpart[p] = part;
+            s_frem[p] = rem;
+            s_pre[p] = pre;
+        }
+    }
+    __syncthreads();
+    // a record of the warp's list: its label, key, fine order position, and whether it is an exact tie
+    auto list_rec = [&](int i, int &p, uint64_t &key, int &fo, bool &tie) {
+        p = -1;
+        key = 0;
+        fo = -1;
+        tie = false;
+        if (i < wl) {
+            const int r = wlist[i];
+            p = a.seg[r];
+            key = a.key[r];
+            int o;
+            bool coarse;
+            bins_of(key, p, o, fo, coarse);
+            tie = !coarse && fo == s_fpart[p];
+        }
+    };
+    // exact ties: this warp's count per label, then every warp's base rank
+    for (int i0 = 0; i0 < wl; i0 += 32) {
+        int p, fo;
+        uint64_t key;
+        bool tie;
+        list_rec(i0 + lane, p, key, fo, tie);
+        const unsigned m = __match_any_sync(DMOLP_FULL_MASK, tie ? p : -1 - lane);
+        if (tie && lane == __ffs(m) - 1) s_wc[wid * nseg + p] += __popc(m);
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kDsWarps * nseg; i += blockDim.x) {
+        const int w = i / nseg, p = i - w * nseg;
+        int base = s_pre[p];
+        for (int x = 0; x < w; ++x) base += s_wc[x * nseg + p];
+        s_wrun[i] = base;
+    }
+    __syncthreads();
+    for (int i0 = 0; i0 < wl; i0 += 32) {
+        int p, fo;
+        uint64_t key;
+        bool tie;
+        list_rec(i0 + lane, p, key, fo, tie);
+        bool take = p >= 0 && fo < s_ftake[p];
+        const unsigned m = __match_any_sync(DMOLP_FULL_MASK, tie ? p : -1 - lane);
+        if (tie) take = s_wrun[wid * nseg + p] + __popc(m & below) < s_frem[p];
+        __syncwarp();
+        if (tie && lane == __ffs(m) - 1) s_wrun[wid * nseg + p] += __popc(m);
+        __syncwarp();
+        emit_window<1>(a.sp, &take, &key, &p, vmask, te, ws, w_stage, w_scnt);  // all lanes
+    }
+    // ---- block 0: ties in a partial fine bin of degree >= 2048, ranked by key ----
+    if (blockIdx.x == 0) {
+        const int nt = __ldcg(a.ntail);
+        auto tail_rec = [&](int i, int &p, uint64_t &key) {  // a tail record of a partial coarse fine bin?
+            const int r = __ldcg(a.tail + i);
+            p = a.seg[r];
+            key = a.key[r];
+            int o, fo;
+            bool coarse;
+            bins_of(key, p, o, fo, coarse);
+            return coarse && fo == s_fpart[p];
+        };
+        for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+            int p;
+            uint64_t key;
+            if (tail_rec(i, p, key)) {
+                const int q = atomicAdd(&s_ntie, 1);
+                if (q < kDsTieCap) {
+                    s_tkey[q] = key;
+                    s_tslot[q] = __ldcg(a.tail + i);
+                    s_tseg[q] = p;
+                }
+            }
+        }
+        __syncthreads();
+        const int m = s_ntie;
+        if (m <= kDsTieCap) {
+            for (int i0 = 0; i0 < m; i0 += blockDim.x) {
+                const int i = i0 + (int)threadIdx.x;
+                bool take = false;
+                int p = -1;
+                uint64_t key = 0;
+                if (i < m) {
+                    p = s_tseg[i];
+                    key = s_tkey[i];
+                    int rank = 0;
+                    for (int j = 0; j < m; ++j) rank += (s_tseg[j] == p && s_tkey[j] < key);
+                    take = rank < s_frem[p];
+                }
+                emit_window<1>(a.sp, &take, &key, &p, vmask, te, ws, w_stage, w_scnt);  // all lanes
+            }
+        } else {  // more ties than the shared arrays hold: rank against the tail in global memory
+            for (int i0 = 0; i0 < nt; i0 += blockDim.x) {
+                const int i = i0 + (int)threadIdx.x;
+                bool take = false;
+                int p = -1;
+                uint64_t key = 0;
+                if (i < nt && tail_rec(i, p, key)) {
+                    int rank = 0;
+                    for (int j = 0; j < nt; ++j) {
+                        int pj;
+                        uint64_t kj;
+                        rank += (tail_rec(j, pj, kj) && pj == p && kj < key);
+                    }
+                    take = rank < s_frem[p];
+                }
+                emit_window<1>(a.sp, &take, &key, &p, vmask, te, ws, w_stage, w_scnt);  // all lanes
+            }
+        }
+    }
+    stage_flush(a.sp, w_stage, w_scnt);
+    te = warp_sum_u64(te);
+    ws = warp_sum_u64(ws);
+    if (lane == 0 && te) atomicAdd(a.sp.te, te);
+    if (lane == 0 && ws) atomicAdd(a.sp.wsum, ws);
 }
 
 }  // namespace
@@ -522,6 +899,7 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
     a.has_split = split != nullptr;
     a.hist_ready = first_hist_ready ? 1 : 0;
     a.tail_ok = smem_hist ? 1 : 0;
+    a.polls = c->wait_polls;
     if (split) a.sp = *split;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)c->num_sms);  // one block per SM, all resident (cooperative launch)
@@ -538,7 +916,51 @@ void select_smallest(dmolp_ctx *c, const int32_t *seg, const uint64_t *key, cons
     c->launches += 1;
 }
 
+bool select_window_deg(dmolp_ctx *c, int nseg, const SplitArgs &split, const int *stopped) {
+    if (nseg > kDegSelMaxK) return false;
+    DegSelArgs a;
+    a.seg = c->b.bown;
+    a.key = c->b.bkey;
+    a.n_dev = &c->b.cnt->npos;
+    a.lists = c->b.active[0];
+    a.tail = c->b.active[1];
+    a.ntail = &c->b.cnt->ntail;
+    a.dsup = c->b.dsup;
+    a.dfine = c->b.dfine[split.t & 1];
+    a.dfine_next = c->b.dfine[(split.t + 1) & 1];
+    a.dcntb = c->b.dcntb;
+    a.nseg = nseg;
+    a.polls = c->wait_polls;
+    a.ctl = c->b.ctrl;
+    a.stopped = stopped;
+    a.sp = split;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)c->num_sms);  // one block per SM, all resident (cooperative launch)
+    cfg.blockDim = dim3(kDsThreads);
+    cfg.dynamicSmemBytes = ds_smem_bytes(nseg);
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_select_deg, a);
+    if (e != cudaSuccess && c->launch_error == cudaSuccess) c->launch_error = e;  // reported by the entry point
+    c->launches += 1;
+    return true;
+}
+
+int select_binary_version() {
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k_select) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    return fa.binaryVersion;
+}
+
 void select_prepare() {
+    cudaFuncSetAttribute(k_select_deg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ds_smem_bytes(kDegSelMaxK));
     cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(kSmemSegMax * kRadix * sizeof(unsigned int) + 3 * DMOLP_MAX_K * sizeof(int) + 16 +
                                kTailBytes));

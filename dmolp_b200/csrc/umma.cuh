@@ -74,14 +74,15 @@ __device__ __forceinline__ void mma_commit(uint64_t *mbar) {
 __device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mbar)), "r"(count));
 }
-// Wait for the phase with parity `phase` to complete; gives up after `limit` polls and returns false.
+// Wait for the phase with parity `phase` to complete; gives up after `limit` polls and returns false.  Each
+// poll is the non-blocking test_wait, so a limit is a fixed number of checks.
 __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t phase, uint32_t limit) {
     const uint32_t a = smem_addr(mbar);
     for (uint32_t i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
             "selp.b32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done)
             : "r"(a), "r"(phase));

@@ -96,6 +96,12 @@ def from_edges(n: int, edges) -> Graph:
     return Graph(off, both[:, 1].astype(np.int32) if len(both) else np.zeros(0, np.int32))
 
 
+def fnv1a(a: np.ndarray) -> int:
+    """64-bit FNV-1a over the array's bytes (the label fingerprint the parity fixtures record)."""
+    a = np.ascontiguousarray(a)
+    return int(_native.gen().dmolp_fnv1a(a.ctypes.data_as(ctypes.c_void_p), a.nbytes))
+
+
 def write_adjtext(g: Graph, path: str) -> None:
     """Write the reference's adjacency text format (first line V; line i+1 = neighbours of i)."""
     lib = _native.gen()

@@ -7,8 +7,9 @@
  * unless the name says _device.  Calls on one context must come from one host thread at a time.
  *
  * The reference (DMOLP, C++/MPI/CUDA) has no C-ABI; each entry point below names the reference interface
- * it replaces (paths relative to the reference tree).  The reference's C++ signatures themselves are
- * provided on top of this ABI by libdmolp_dropin.so.
+ * it replaces (paths relative to the reference tree).  The reference's C++ signatures themselves
+ * (run_phase1, run_phase2 and the lower-level functions of include/phase1 and include/phase2) are provided on
+ * top of this ABI by libdmolp_dropin.so.
  */
 #ifndef DMOLP_B200_H
 #define DMOLP_B200_H
@@ -85,12 +86,19 @@ typedef struct {                   /* one per LP iteration */
     int64_t edge_cut;
     uint64_t te_prev, te_cand, te_sel, te_stats;  /* traversed-edge terms of the reference's loop */
     uint64_t arcs_read;            /* arcs this implementation actually read in the iteration */
+    uint64_t window_sum;           /* order-independent checksum of the selected window: the sum, mod 2^64,
+                                      of the SplitMix64 finaliser of each vertex id */
 } dmolp_lp_record;
 
 const char *dmolp_last_error(void);
 
 /* The calling thread's current CUDA device (0 when none is set). */
 int dmolp_current_device(void);
+
+/* The architecture of this library's device code as the CUDA runtime loaded it on `device`
+ * (cudaFuncAttributes::binaryVersion of one of its kernels: 100 for sm_100a).  No counterpart in the
+ * reference. */
+int dmolp_device_code_version(int device, int *version);
 
 /* Create a context on CUDA device `device`.  Replaces the device set-up of allocateGPU
  * (src/main.cpp:25-121), which picks local_rank % device_count. */
@@ -215,6 +223,13 @@ int dmolp_labels_restore(dmolp_ctx *ctx);
 int dmolp_set_profiling(dmolp_ctx *ctx, int enable);
 int dmolp_kernel_profile(dmolp_ctx *ctx, int kernel, double *total_ms, int64_t *launches, double *bytes);
 
+/* How long a grid barrier of the cooperative window selections waits before it gives up: `polls` reads of
+ * its generation word (0 = the default, 2^22, about a second).  Its blocks are co-resident (cooperative
+ * launch), so the default is never reached; a barrier that gives up stops the loop and every block leaves the
+ * kernel, and the call returns DMOLP_ERR_CUDA naming the barrier, with the context ready for the next call.
+ * No reference counterpart (the reference's kernel has no barrier).  Mainly for testing that path. */
+int dmolp_set_wait_limit(dmolp_ctx *ctx, uint32_t polls);
+
 /* ---- phase-1 hubs on the host (no device work) ----
  * dmolp_find_hubs_pairs: find_hub_nodes (src/phase1/init.cpp:139-177) on n (id, degree) pairs given in the
  * reference's degree-map order: the pairs sorted by degree in exactly the order std::sort leaves them (ties
@@ -248,7 +263,12 @@ void dmolp_host_graph_free(dmolp_host_graph *g);
  * of 2*DMOLP_NOALLOC_MAX_K+2 64-bit counters (16 KiB), held by every GPU that loads the library until exit;
  * k above DMOLP_NOALLOC_MAX_K is rejected with DMOLP_ERR_ARG.  Every call shares that array and clears the
  * part it uses first; calls that overlap on the GPU race.  The first call on a device looks up the array's
- * address with that device current; make it before any stream capture.  Errors: dmolp_last_error(). */
+ * address with that device current; make it before any stream capture.  That address is kept for the life of
+ * the process, so a cudaDeviceReset after the first call on a device is not supported.  The calling thread's
+ * current device is the same after the call as before.  A neighbour id outside [0,nv) or a decreasing pair of
+ * offsets is skipped by the kernel and reported as DMOLP_ERR_ARG (offsets[nv] cannot be range-checked: the
+ * call takes no arc count); a label outside [0,k) or an odd cut-arc count is DMOLP_ERR_BAD_LABELS.
+ * Errors: dmolp_last_error(). */
 #define DMOLP_NOALLOC_MAX_K 1024
 int dmolp_metrics_noalloc(int device, int64_t nv, const int64_t *offsets_device, const int32_t *indices_device,
                           const int32_t *labels_device, int k, void *stream, int64_t *edge_cut, int64_t *vertex_counts,
@@ -327,6 +347,10 @@ typedef struct dmolp_mpnn dmolp_mpnn;
 int64_t dmolp_mpnn_num_params(void);           /* length of the flat FP32 parameter vector */
 int dmolp_mpnn_create(int device, dmolp_mpnn **out);  /* fixed-seed Glorot hidden layers, zero output layer */
 int dmolp_mpnn_destroy(dmolp_mpnn *m);
+/* Polls of a GEMM's MMA completion barrier before the GEMM gives up (0 = the default, 2^24 non-blocking
+ * checks, a fraction of a second; far above any real MMA).  A GEMM that gives up waits (bounded) for the MMA in flight, frees its tensor memory and sets an
+ * error flag: the call returns DMOLP_ERR_CUDA and the network stays usable.  Mainly for testing that path. */
+int dmolp_mpnn_set_wait_limit(dmolp_mpnn *m, uint32_t polls);
 /* Parameters, flat FP32: per layer W [K x N] row-major then b [N]; K = 32, 128, 128; N = 64, 64, 16.
  * Setting them resets the optimiser state. */
 int dmolp_mpnn_set_params(dmolp_mpnn *m, const float *params);

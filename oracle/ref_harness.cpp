@@ -250,37 +250,54 @@ void usage() {
 
 // Fixed-iteration phase 2: the steps of phase2.cpp:295-416 for exactly `iters` iterations.
 // Also counts traversed edges per iteration: deg over prev window, over candidates, over the selected
-// window, plus one pass over all arcs for the statistics.
+// window, plus one pass over all arcs for the statistics.  lp_seconds (and each trace record's "seconds",
+// cumulative) times the reference's own steps only: penalties, window expansion, the LP step and applying
+// its changes, the statistics and the edge cut; the traversed-edge count and the trace are not timed.
 PartitioningMetrics run_phase2_fixed(int k, int iters, Graph &g, GhostNodes &gh, FILE *trace, double &lp_seconds,
                                      uint64_t &te_total) {
-    auto t0 = std::chrono::high_resolution_clock::now();
+    using clk = std::chrono::high_resolution_clock;
+    double busy = 0.0;
+    auto since = [](clk::time_point a) { return std::chrono::duration<double>(clk::now() - a).count(); };
+    auto t0 = clk::now();
     int prev_edge_cut = computeEdgeCut(g, g.vertex_labels, gh, 0);
     PartitionStats stats = computePartitionStats(g, g.vertex_labels, gh, k);
     std::vector<int> window;
     for (int i = 0; i < g.num_vertices; ++i) window.push_back(i);
+    busy += since(t0);
     const int nv = g.num_vertices + (int)gh.ghost_labels.size();
     auto deg = [&](int v) -> uint64_t { return (uint64_t)(g.row_ptr[v + 1] - g.row_ptr[v]); };
+    std::vector<char> mark(nv > 0 ? nv : 1, 0);
+    std::vector<int> touched;
     te_total = 0;
     for (int iter = 0; iter < iters; ++iter) {
+        auto ta = clk::now();
         auto pens = calculatePenalties(stats, k, iter + 1, 0);
+        busy += since(ta);
         uint64_t te_prev = 0, te_cand = 0, te_sel = 0, te_stats = 0;
         // candidates = prev window plus its neighbours (gpu_lp_boundary.cu:207-240), for the TE count only
-        std::vector<int> cand;
+        touched.clear();
+        auto touch = [&](int v) {
+            if (v >= 0 && v < nv && !mark[v]) {
+                mark[v] = 1;
+                touched.push_back(v);
+            }
+        };
         for (int v : window) {
             if (v < 0 || v >= nv) continue;
-            cand.push_back(v);
+            touch(v);
             if (v < g.num_vertices) {
                 te_prev += deg(v);
-                for (int e = g.row_ptr[v]; e < g.row_ptr[v + 1]; ++e) cand.push_back(g.col_indices[e]);
+                for (int e = g.row_ptr[v]; e < g.row_ptr[v + 1]; ++e) touch(g.col_indices[e]);
             }
         }
-        std::sort(cand.begin(), cand.end());
-        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-        for (int c : cand)
+        for (int c : touched) {
             if (c < g.num_vertices) te_cand += deg(c);
+            mark[c] = 0;
+        }
+        const size_t ncand = touched.size();
+        ta = clk::now();
         window = expandBoundaryNodes(g.row_ptr, g.col_indices, window, g.vertex_labels, pens[0], pens[1], nv, iter + 1);
         int changes = 0;
-        for (int v : window) te_sel += deg(v);
         if (!window.empty()) {
             GPULabelUpdateResult r = oracle_ref_streaming(g.row_ptr, g.col_indices, window, g.vertex_labels,
                                                           gh.ghost_labels, g.global_ids, pens[0], g.num_vertices, k,
@@ -291,24 +308,24 @@ PartitioningMetrics run_phase2_fixed(int k, int iters, Graph &g, GhostNodes &gh,
             prev_edge_cut = computeEdgeCut(g, g.vertex_labels, gh, 0);
             te_stats = (uint64_t)g.row_ptr[g.num_vertices];
         }
+        busy += since(ta);
+        for (int v : window) te_sel += deg(v);
         te_total += te_prev + te_cand + te_sel + te_stats;
         if (trace) {
             fprintf(trace,
-                    "{\"iter\":%d,\"window\":%zu,\"window_hash\":\"%016llx\",\"window_sum\":\"%016llx\",\"candidates\":%zu,\"changes\":%d,"
-                    "\"edge_cut\":%d,\"labels_hash\":\"%016llx\",\"vertex_counts\":%s,\"edge_counts\":%s,"
-                    "\"penalty\":%s,\"RE\":%s,\"te\":[%llu,%llu,%llu,%llu]}\n",
+                    "{\"iter\":%d,\"window\":%zu,\"window_hash\":\"%016llx\",\"window_sum\":\"%016llx\",\"candidates\":%zu,"
+                    "\"changes\":%d,\"edge_cut\":%d,\"labels_hash\":\"%016llx\",\"vertex_counts\":%s,\"edge_counts\":%s,"
+                    "\"penalty\":%s,\"RE\":%s,\"te\":[%llu,%llu,%llu,%llu],\"seconds\":%.6f}\n",
                     iter + 1, window.size(), (unsigned long long)set_hash(window), (unsigned long long)set_sum(window),
-                    cand.size(), changes,
-                    prev_edge_cut,
+                    ncand, changes, prev_edge_cut,
                     (unsigned long long)fnv1a(g.vertex_labels.data(), g.vertex_labels.size() * sizeof(int)),
                     json_ivec(stats.global_vertex_counts).c_str(), json_ivec(stats.global_edge_counts).c_str(),
                     json_dvec_bits(pens[0]).c_str(), json_dvec_bits(pens[1]).c_str(), (unsigned long long)te_prev,
-                    (unsigned long long)te_cand, (unsigned long long)te_sel, (unsigned long long)te_stats);
+                    (unsigned long long)te_cand, (unsigned long long)te_sel, (unsigned long long)te_stats, busy);
             fflush(trace);
         }
     }
-    auto t1 = std::chrono::high_resolution_clock::now();
-    lp_seconds = std::chrono::duration<double>(t1 - t0).count();
+    lp_seconds = busy;
     // final metrics exactly as phase2.cpp:424-441
     PartitionStats fs = computePartitionStats(g, g.vertex_labels, gh, k);
     double max_v = 0.0, max_e = 0.0;

@@ -1,5 +1,9 @@
 // Test driver for libdmolp_dropin.so: calls the reference's C++ entry points as the reference's callers
-// do and prints what they return as JSON lines for tests/test_dropin.py.
+// do and prints what they return as JSON lines for tests/test_dropin.py.  The same source, linked against
+// the reference's own objects instead (oracle/Makefile target dropin_driver_ref), prints what the reference
+// returns for the same calls (built with DMOLP_DRIVER_REFERENCE: the three functions the reference declares
+// but never defines -- freeChunkSubgraph, runBoundaryLPOnGPU_Safe, cleanupGPUResources,
+// include/phase2/gpu_lp_boundary.h:67,85,105 -- are not called there).
 //
 //   dropin_driver <graph.txt> <k> <theta> <iters> [--host-only]
 //
@@ -108,10 +112,14 @@ int main(int argc, char **argv) {
                                                         rg.global_ids, rg.num_vertices);
     BoundarySubgraph ch = createChunkSubgraph(sg, 0, sg.num_nodes / 2);
     printf("{\"what\":\"subgraph\",\"nodes\":%d,\"edges\":%d,\"boundary\":%zu,\"mapping_hash\":\"%016llx\","
-           "\"chunk_nodes\":%d,\"chunk_edges\":%d,\"random_labels_hash\":\"%016llx\",\"random_edges\":%d}\n",
+           "\"chunk_nodes\":%d,\"chunk_edges\":%d,\"random_labels_hash\":\"%016llx\",\"random_edges\":%d,"
+           "\"random_row_ptr_hash\":\"%016llx\",\"random_col_hash\":\"%016llx\",\"random_vertices\":%d}\n",
            sg.num_nodes, sg.num_edges, sg.boundary_indices.size(), (unsigned long long)fnv(sg.node_mapping),
-           ch.num_nodes, ch.num_edges, (unsigned long long)fnv(rg.vertex_labels), rg.num_edges);
+           ch.num_nodes, ch.num_edges, (unsigned long long)fnv(rg.vertex_labels), rg.num_edges,
+           (unsigned long long)fnv(rg.row_ptr), (unsigned long long)fnv(rg.col_indices), rg.num_vertices);
+#ifndef DMOLP_DRIVER_REFERENCE
     freeChunkSubgraph(ch);
+#endif
     if (host_only) return 0;
 
     // lower-level phase 1 on the GPU
@@ -146,15 +154,47 @@ int main(int argc, char **argv) {
     BoundarySubgraph sub = createBoundarySubgraphUnified(g.row_ptr, g.col_indices, w, labels1, {}, g.global_ids, V);
     GPULabelUpdateResult r2 = runBoundaryLPOnGPU_SubgraphUnified(sub, pen, k);
     GPULabelUpdateResult r3 = runBoundaryLPOnGPU_Chunked(sub, pen, k, (size_t)1 << 40);
+    int same4 = 1;
+#ifndef DMOLP_DRIVER_REFERENCE
     std::vector<int> l4;
     runBoundaryLPOnGPU_Safe(g.row_ptr, g.col_indices, labels1, l4, pen, w, k);
-    int same4 = 1;
     for (int i = 0; i < r1.change_count; ++i)
         if (l4[r1.updated_nodes[i]] != r1.updated_labels[i]) same4 = 0;
+#endif
     printf("{\"what\":\"single_step\",\"window\":%zu,\"window_hash\":\"%016llx\",\"changes\":[%d,%d,%d],"
            "\"same_nodes\":%d,\"safe_consistent\":%d}\n",
            w.size(), (unsigned long long)fnv(w), r1.change_count, r2.change_count, r3.change_count,
            (int)(r1.updated_nodes == r2.updated_nodes && r1.updated_labels == r2.updated_labels), same4);
+
+    // the same step with penalties, through the chunked paths: the chunked entry point with room for one
+    // chunk of the minimum size (1024 subgraph nodes) and the streaming entry point with no room at all
+    std::vector<double> pen2(k);
+    for (int p = 0; p < k; ++p) pen2[p] = 0.05 * (double)((p * 7) % 5 - 2);
+    auto step_line = [&](const char *what, const GPULabelUpdateResult &r) {
+        printf("{\"what\":\"%s\",\"changes\":%d,\"nodes_hash\":\"%016llx\",\"labels_hash\":\"%016llx\"}\n", what,
+               r.change_count, (unsigned long long)fnv(r.updated_nodes), (unsigned long long)fnv(r.updated_labels));
+    };
+    step_line("step_unified", runBoundaryLPOnGPU_SubgraphUnified(sub, pen2, k));
+    step_line("step_chunked", runBoundaryLPOnGPU_Chunked(sub, pen2, k, 1));
+    step_line("step_streaming_chunked",
+              runBoundaryLPOnGPU_Streaming(g.row_ptr, g.col_indices, w, labels1, {}, g.global_ids, pen2, V, k, 0));
+    step_line("step_streaming",
+              runBoundaryLPOnGPU_Streaming(g.row_ptr, g.col_indices, w, labels1, {}, g.global_ids, pen2, V, k, 512));
+    printf("{\"what\":\"chunks\",\"subgraph_nodes\":%d,\"subgraph_edges\":%d}\n", sub.num_nodes, sub.num_edges);
+
+    // -m random: random_partition's graph and labels, then phase 2 from them
+    Graph gr;
+    GhostNodes ghr;
+    Phase1Metrics mr = run_phase1(0, 1, path, k, theta, true, false, gr, ghr);
+    printf("{\"what\":\"random_phase1\",\"cut\":%d,\"E\":%d,\"row_ptr_hash\":\"%016llx\",\"col_hash\":\"%016llx\","
+           "\"labels_hash\":\"%016llx\",\"vc\":%s}\n",
+           mr.initial_edge_cut, gr.num_edges, (unsigned long long)fnv(gr.row_ptr), (unsigned long long)fnv(gr.col_indices),
+           (unsigned long long)fnv(gr.vertex_labels), ivec(mr.partition_vertex_counts).c_str());
+    PartitioningMetrics mr2 = run_phase2(0, 1, k, gr, ghr, 0);
+    printf("{\"what\":\"random_phase2\",\"cut\":%d,\"vbal\":%.17g,\"ebal\":%.17g,\"labels_hash\":\"%016llx\"}\n",
+           mr2.edge_cut, mr2.vertex_balance, mr2.edge_balance, (unsigned long long)fnv(gr.vertex_labels));
+#ifndef DMOLP_DRIVER_REFERENCE
     cleanupGPUResources();
+#endif
     return 0;
 }

@@ -36,11 +36,15 @@ def test_library_exports_every_declared_symbol():
     assert set(declared) <= exported
 
 
+@pytest.mark.gpu
 def test_library_is_built_for_sm100a():
-    from dmolp_b200 import _native
+    """The runtime reports the loaded device code as sm_100 (the library carries sm_100a code only)."""
+    from dmolp_b200 import _native, cabi
 
-    out = subprocess.run(["cuobjdump", "--list-elf", _native.core_path()], capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+    v = ctypes.c_int(0)
+    lib = _native.core()
+    assert lib.dmolp_device_code_version(0, ctypes.byref(v)) == cabi.DMOLP_OK, lib.dmolp_last_error()
+    assert v.value == 100
 
 
 @pytest.mark.skipif(os.path.exists("/dev/nvidia0"), reason="a GPU is present")

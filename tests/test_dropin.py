@@ -15,6 +15,7 @@ from conftest import ROOT, f64_hex, golden_graph
 LIB = os.path.join(ROOT, "dmolp_b200", "lib")
 DROPIN = os.path.join(LIB, "libdmolp_dropin.so")
 MAIN = os.path.join(ROOT, "oracle", "_ref", "dmolp_main_dropin")
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "dropin_driver_ref")  # the same driver on the reference's objects
 
 REFERENCE_SIGNATURES = [
     "run_phase1(int, int, char const*, int, int, bool, bool, Graph&, GhostNodes&)",
@@ -37,9 +38,12 @@ def build_driver() -> str:
     return out
 
 
-def run_driver(txt, k, theta, iters, host_only=False, env=None):
-    cmd = [build_driver(), txt, str(k), str(theta), str(iters)] + (["--host-only"] if host_only else [])
-    p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=600)
+def run_driver(txt, k, theta, iters, host_only=False, env=None, reference=False):
+    exe = REF_DRIVER if reference else build_driver()
+    cmd = [exe, txt, str(k), str(theta), str(iters)] + (["--host-only"] if host_only else [])
+    # one OpenMP thread: the reference's subgraph construction races on a vector<bool> with more
+    env = dict(env or os.environ, OMP_NUM_THREADS="1")
+    p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=900)
     assert p.returncode == 0, p.stderr[-2000:]
     return {d["what"]: d for d in (json.loads(l) for l in p.stdout.splitlines() if l.startswith("{\"what\""))}
 
@@ -131,3 +135,58 @@ def test_reference_main_runs_on_the_dropin():
     assert m and int(m.group(1)) == case["phase1"]["initial_edge_cut"]
     cuts = re.findall(r"Phase 2 \S+:\s+(\d+)", p.stdout)
     assert cuts and int(cuts[0]) == case["runs"]["ref"]["result"]["edge_cut"], p.stdout[-3000:]
+
+
+# Texts for the host entry points: duplicates, self-loops, an empty line and rows without their reverse arcs;
+# random_partition drops self-loops and duplicates (src/phase1/random.cpp:89-90).
+HOST_TEXTS = {
+    "dups_selfloops": "7\n1 1 2 0 3\n0 0 2\n1 0 0 6\n\n5 5 3\n4\n2 2 2\n",
+    "path": "6\n1\n0 2\n1 3\n2 4\n3 5\n4\n",
+}
+
+
+@pytest.mark.skipif(not os.path.exists(REF_DRIVER), reason="built only where the reference sources exist")
+@pytest.mark.parametrize("name", sorted(HOST_TEXTS) + ["knn5000"])
+def test_host_entry_points_equal_the_reference_functions(name):
+    """load_graph, gather_degrees, find_hub_nodes, find_first_seed, random_partition (its CSR and labels),
+    createBoundarySubgraphUnified and createChunkSubgraph: the drop-in's answers equal the reference's own
+    functions' on the same text (the same driver linked against either)."""
+    from dmolp_b200 import graphs
+
+    with tempfile.TemporaryDirectory() as td:
+        txt = os.path.join(td, "g.txt")
+        if name in HOST_TEXTS:
+            open(txt, "w").write(HOST_TEXTS[name])
+        else:
+            graphs.write_adjtext(graphs.knn(5000, 3, 10, seed=12), txt)
+        ours = run_driver(txt, 3, 2, 5, host_only=True)
+        ref = run_driver(txt, 3, 2, 5, host_only=True, reference=True)
+    assert ours == ref
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(REF_DRIVER), reason="built only where the reference sources exist")
+def test_device_entry_points_equal_the_reference_functions():
+    """Every entry point of the driver against the reference's own functions (its phase 1, its run_phase2
+    loop, its single-step GPU functions with its kernel built for sm_100a), on a 5,000-vertex 3-D k-NN graph:
+    lower-level and whole phase 1, run_phase2 with the reference's stopping rules, one LP step through
+    runBoundaryLPOnGPU_SubgraphUnified, _Chunked with room for one 1024-node chunk (the subgraph needs five:
+    arcs across chunks are dropped, gpu_lp_boundary.cu:571-675) and _Streaming with and without room, and the
+    -m random path (random_partition, then run_phase2)."""
+    from dmolp_b200 import graphs
+
+    g = graphs.knn(5000, 3, 10, seed=12)
+    k, theta = 6, 100
+    with tempfile.TemporaryDirectory() as td:
+        txt = os.path.join(td, "g.txt")
+        graphs.write_adjtext(g, txt)
+        ours = run_driver(txt, k, theta, 0)
+        ref = run_driver(txt, k, theta, 0, reference=True)
+    assert ours["chunks"]["subgraph_nodes"] > 4 * 1024  # five chunks of the minimum size
+    for what in ("host", "subgraph", "lower_phase1", "phase1", "phase2", "step_unified", "step_chunked",
+                 "step_streaming_chunked", "step_streaming", "chunks", "random_phase1", "random_phase2"):
+        assert ours[what] == ref[what], what
+    for key in ("window", "window_hash", "changes"):
+        assert ours["single_step"][key] == ref["single_step"][key], key
+    # the chunked paths drop arcs that cross chunks: they differ from the whole subgraph's step here
+    assert ours["step_chunked"] != ours["step_unified"]

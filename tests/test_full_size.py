@@ -1,16 +1,25 @@
 """The plain path at its benchmark size: R-MAT scale 22, edge factor 16, seed 7 (4.19 M vertices, 128 M arcs).
 
-The oracle is affordable here for phase 1 and the first LP iterations, which must agree bit for bit.  For the
-full 30-iteration run the test relies on properties that hold at any size: the edge cut and part sizes the
-run reports equal a recount from its final labels, the statistics kept incrementally equal the full pass,
-a rerun from the same start repeats itself exactly, and under the reference's 32-label cap (k = 64) no vertex
-moves to a label of 32 or more."""
+Every LP iteration of the benchmarked runs (k = 32, and k = 16 and 64, 30 iterations each) is held to the
+reference's own outputs on this graph (tests/golden/rmat22_full.json, written by make_golden_full.py from the
+reference's phase-2 steps started from the oracle's phase-1 labels): per iteration the window's size and
+order-independent checksum, the candidates, the changes, the edge cut, the part counts, the penalty bits and
+the traversed-edge terms, then the final labels' hash, cut and balances.  The oracle also pins phase 1 and the
+first iterations directly, and properties that hold at any size check the 30-iteration run once more: the
+reported cut and part sizes equal a recount from the final labels and the full statistics pass, a rerun
+repeats itself exactly, and under the reference's 32-label cap (k = 64) no vertex moves to a label >= 32."""
+import json
+import os
+
 import numpy as np
 import pytest
 
 import oracle
+from conftest import GOLDEN, f64_hex
 
 pytestmark = pytest.mark.gpu
+
+FULL = os.path.join(GOLDEN, "rmat22_full.json")
 
 
 @pytest.fixture(scope="module")
@@ -80,3 +89,27 @@ def test_label_cap_at_k64(setup):
     assert moved.any()
     assert after[moved].max() < 32  # only the first min(k, 32) labels are scored (gpu_lp_boundary.cu:360)
     assert r.edge_cut == recount(g, src, after, 64)[0]
+
+
+@pytest.mark.parametrize("k", [32, 16, 64])
+def test_every_iteration_matches_reference(setup, k):
+    g, p, _ = setup
+    gold = json.load(open(FULL))[f"k{k}"]
+    assert (gold["num_vertices"], gold["num_arcs"]) == (g.num_vertices, g.num_arcs)
+    m1 = p.phase1(k, gold["theta"])
+    assert "%016x" % oracle.fnv1a(p.labels()) == gold["labels1_hash"]
+    assert m1.initial_edge_cut == gold["phase1_initial_edge_cut"] and m1.seeds == gold["phase1_seeds"]
+    m = p.phase2(k, mode="fixed", iterations=gold["iters"])
+    pen, cnt = p.history(k, gold["iters"])
+    assert len(m.records) == len(gold["trace"]) == gold["iters"]
+    for i, t in enumerate(gold["trace"]):
+        r = m.records[i]
+        assert (r.window, "%016x" % r.window_sum) == (t["window"], t["window_sum"]), (k, i + 1)
+        assert (r.candidates, r.changes, r.edge_cut) == (t["candidates"], t["changes"], t["edge_cut"]), (k, i + 1)
+        assert [r.te_prev, r.te_cand, r.te_sel, r.te_stats] == t["te"], (k, i + 1)
+        assert [f64_hex(x) for x in pen[i]] == t["penalty"], (k, i + 1)
+        assert cnt[i][:k].tolist() == t["vertex_counts"] and cnt[i][k:].tolist() == t["edge_counts"], (k, i + 1)
+    assert "%016x" % oracle.fnv1a(p.labels()) == gold["labels2_hash"] == gold["trace"][-1]["labels_hash"]
+    res = gold["result"]
+    assert m.edge_cut == res["edge_cut"] and m.traversed_edges == res["te_total"]
+    assert f64_hex(m.vertex_balance) == res["vertex_balance"] and f64_hex(m.edge_balance) == res["edge_balance"]

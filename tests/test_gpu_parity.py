@@ -103,6 +103,9 @@ def test_random_cases_against_oracle(part, seed):
         m2 = part.phase2(k, mode="fixed", iterations=iters, cap=cap)
         o2 = oracle.phase2(g.offsets, g.indices, lab0, k, "fixed", iters, cap=cap)
         assert np.array_equal(part.labels(), o2.labels), (seed, trial, k, cap)
+        # per iteration: the window's order-independent checksum, its size and the changes
+        assert [(r.window, r.window_sum, r.changes) for r in m2.records] == \
+               [(r.window, r.window_sum, r.changes) for r in o2.records], (seed, trial)
         assert m2.edge_cut == o2.res.edge_cut
         assert m2.traversed_edges == o2.res.te_total
         assert f64_hex(m2.vertex_balance) == f64_hex(o2.res.vertex_balance)
