@@ -716,10 +716,13 @@ def batched_summary(n: int, theta: int, device: int) -> dict:
 
 
 # ------------------------------------------------------------------------------------------- CPU baselines
-def reference_cpu_run(g, labels1, w, repeats: int, iters: int, threads: int, timeout: float = 900,
-                      mode: str = "fixed", gpu: bool = False):
-    """The reference's own phase-2 code (oracle/_ref, built from its sources) on the host cores; with gpu=True
-    its own CUDA path (boundaryLPKernel_unified, built unmodified for sm_100a) instead of the CPU kernel."""
+def reference_iterations(g, labels1, w, iters: int, threads: int, gpu: bool = False, timeout: float = 3600) -> list:
+    """The reference's own phase-2 code (oracle/_ref/ref_harness, built from its sources) on the host cores:
+    one fixed-mode run of `iters` LP iterations from the phase-1 labels, continuing from iteration to
+    iteration as the workload does.  Returns per iteration (seconds, traversed edges): the harness times the
+    reference's steps only (penalties, window expansion, the LP step and its changes, statistics, cut), not
+    its own traversed-edge count.  gpu=True: the reference's own CUDA path (boundaryLPKernel_unified, built
+    unmodified for sm_100a) instead of the CPU restatement of its kernel."""
     import oracle
 
     with tempfile.TemporaryDirectory() as td:
@@ -729,18 +732,28 @@ def reference_cpu_run(g, labels1, w, repeats: int, iters: int, threads: int, tim
         graphs.write_adjtext(g, txt)
         lab = os.path.join(td, "labels1.bin")
         labels1.astype(np.int32).tofile(lab)
-        cmd = [oracle.REF_HARNESS, txt, str(w["k"]), str(w["theta"]), "--out", os.path.join(td, "o"), "--mode",
-               mode, "--iters", str(iters), "--threads", str(threads), "--labels-in", lab, "--no-seed-dump",
-               "--repeat", str(repeats)] + (["--gpu"] if gpu else [])
+        out = os.path.join(td, "o")
+        cmd = [oracle.REF_HARNESS, txt, str(w["k"]), str(w["theta"]), "--out", out, "--mode", "fixed", "--iters",
+               str(iters), "--threads", str(threads), "--labels-in", lab, "--no-seed-dump"] + (["--gpu"] if gpu else [])
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         pr = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout)
         if pr.returncode != 0:
             raise RuntimeError(pr.stderr[-1000:])
-        reps = [json.loads(l) for l in pr.stdout.splitlines() if l.startswith("{\"repeat\"")]
-        if not reps:
-            reps = [json.loads(pr.stdout.splitlines()[-1])]
-            reps[0]["repeat"] = 0
-        return reps
+        trace = [json.loads(l) for l in open(os.path.join(out, "trace.jsonl")) if l.strip()]
+    its, prev = [], 0.0
+    for t in trace:
+        its.append((t["seconds"] - prev, sum(t["te"])))
+        prev = t["seconds"]
+    return its
+
+
+def iteration_steps(g, labels1, w, n: int, threads: int, gpu: bool = False) -> list:
+    """n consecutive LP iterations of the workload (a new run from the phase-1 labels after every
+    w["iters"] iterations), as (seconds, traversed edges) per iteration."""
+    its = []
+    while len(its) < n:
+        its += reference_iterations(g, labels1, w, min(w["iters"], n - len(its)), threads, gpu)
+    return its
 
 
 def port_cpu_run(g, labels1, w, iters: int):
@@ -756,17 +769,18 @@ def cpu_baseline(g, labels1, w, args) -> dict:
 
     threads = os.cpu_count() or 1
     iters = args.cpu_sample_iters
-    sample = f"LP iteration{'s' if iters > 1 else ''} 1..{iters} of {w['iters']} on the full graph"
+    sample = f"LP iterations 1..{iters} of {w['iters']} on the full graph (one run from the phase-1 labels)"
     if oracle.reference_available():
-        reps = reference_cpu_run(g, labels1, w, 1, iters, threads)
-        r = reps[-1]
-        out = {"value": r["te_total"] / r["lp_seconds"], "unit": "TE/s", "cores": threads, "kind": "reference",
-               "sample": sample, "seconds": r["lp_seconds"]}
+        its = iteration_steps(g, labels1, w, iters, threads)
+        secs, te = sum(x for x, _ in its), sum(y for _, y in its)
+        out = {"value": te / secs, "unit": "TE/s", "cores": threads, "kind": "reference", "sample": sample,
+               "seconds": secs, "note": "the reference's early iterations are its slowest per traversed edge; "
+                                        "--impl reference times iterations later in the run as well"}
         try:  # the reference's own GPU path on the same B200, same sample
-            rg = reference_cpu_run(g, labels1, w, 1, iters, threads, gpu=True)[-1]
-            out["reference_gpu"] = {"value": rg["te_total"] / rg["lp_seconds"], "unit": "TE/s", "sample": sample,
-                                    "seconds": rg["lp_seconds"],
-                                    "kind": "reference run_phase2 loop with its boundaryLPKernel_unified (sm_100a)"}
+            gi = iteration_steps(g, labels1, w, iters, threads, gpu=True)
+            gs, gt = sum(x for x, _ in gi), sum(y for _, y in gi)
+            out["reference_gpu"] = {"value": gt / gs, "unit": "TE/s", "sample": sample, "seconds": gs,
+                                    "kind": "reference run_phase2 steps with its boundaryLPKernel_unified (sm_100a)"}
         except Exception as e:  # report, do not hide
             out["reference_gpu"] = {"error": str(e)[:300]}
         return out
@@ -861,7 +875,11 @@ def run_reference_ingest(args, w) -> dict:
 
 
 def run_reference_arm(args, w) -> dict:
-    """--impl reference: the reference's own implementation of the path on this box's host cores."""
+    """--impl reference: the reference's own implementation of the path on this box's host cores.  A step is
+    one LP iteration of the workload's run, taken in order from one continuous run (from the phase-1
+    labels; a new run after every w["iters"] iterations): the first W iterations are the warm-up, the next K
+    are timed.  Per traversed edge the reference's first iterations are its slowest, so this sample sits at
+    or above the rate of a whole run (the line reports that rate too when the steps cover one)."""
     import oracle
 
     if w["kind"] == "ingest":
@@ -873,28 +891,40 @@ def run_reference_arm(args, w) -> dict:
     # phase-1 labels from the oracle (the reference's phase 1 is undefined on R-MAT: fewer seeds than parts)
     labels1 = oracle.phase1(g.offsets, g.indices, g.raw_deg(), w["k"], w["theta"]).labels
     threads = os.cpu_count() or 1
-    iters = args.cpu_sample_iters
-    sample = f"per step: LP iteration{'s' if iters > 1 else ''} 1..{iters} of {w['iters']} on the full graph"
+    n = args.warmup + args.steps
     if oracle.reference_available():
-        reps = reference_cpu_run(g, labels1, w, args.warmup + args.steps, iters, threads, timeout=3600)
+        its = iteration_steps(g, labels1, w, n, threads)
         kind, cores = "reference", threads
     else:
-        reps = [dict(port_cpu_run(g, labels1, w, iters), repeat=i) for i in range(args.warmup + args.steps)]
+        its = []
+        for _ in range(n):
+            r = port_cpu_run(g, labels1, w, 1)
+            its.append((r["lp_seconds"], r["te_total"]))
         kind, cores = "port", 1
-    timed = [r for r in reps if r["repeat"] >= args.warmup] or reps
-    secs = sum(r["lp_seconds"] for r in timed)
-    te = sum(r["te_total"] for r in timed)
+    timed = its[args.warmup:] or its
+    secs = sum(x for x, _ in timed)
+    te = sum(y for _, y in timed)
     value = te / secs
-    return {
+    first = args.warmup + 1
+    sample = (f"per step: one LP iteration of the {w['iters']}-iteration run, in order; warm-up iterations 1..{args.warmup}, "
+              f"timed iterations {first}..{args.warmup + len(timed)} (counted modulo a new run every {w['iters']})")
+    line = {
         "impl": "reference", "metric": "LP traversed edges/s", "value": value, "unit": "TE/s", "n_gpus": args.gpus,
         "steps": len(timed), "warmup": args.warmup, "ms_per_step": secs / len(timed) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator)",
         "config": {"workload": describe(w), "k": w["k"], "iterations": w["iters"], "mode": "fixed",
-                   "num_vertices": g.num_vertices, "num_arcs": g.num_arcs},
+                   "label_cap": "reference (min(k,32))", "num_vertices": g.num_vertices, "num_arcs": g.num_arcs,
+                   "l2": "host run", "parallelism": "host threads x%d" % cores},
         "cpu_baseline": {"value": value, "unit": "TE/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": "TE/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "iterations": [{"seconds": x, "traversed_edges": y} for x, y in its],
     }
+    if len(its) >= w["iters"]:
+        run = its[:w["iters"]]
+        line["whole_run"] = {"value": sum(y for _, y in run) / sum(x for x, _ in run), "unit": "TE/s",
+                             "seconds": sum(x for x, _ in run), "iterations": w["iters"]}
+    return line
 
 
 def main():
@@ -904,7 +934,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="rmat22", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-sample-iters", type=int, default=1)
+    ap.add_argument("--cpu-sample-iters", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="timed steps only: no clock soak, e2e or CPU baseline")
     ap.add_argument("--records", action="store_true", help="print one step's per-iteration records to stderr")
@@ -947,7 +977,7 @@ def main():
                 line["cpu_baseline"] = {"error": str(e)[:300]}
         if world == 1 and not args.quick and w["kind"] not in ("batch", "ingest"):
             try:
-                line["batched"] = batched_summary(256, 1000, local_rank)
+                line["batched"] = batched_summary(2048, 1000, local_rank)  # the batched config: 2048 graphs
             except Exception as e:  # report, do not hide
                 line["batched"] = {"error": str(e)[:300]}
             try:

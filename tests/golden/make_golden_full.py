@@ -82,7 +82,9 @@ def main() -> None:
             for k, f in futs.items():
                 case = f.result()
                 out[f"k{k}"] = case
-                json.dump(out, open(OUT, "w"), indent=1, sort_keys=True)
+                with open(OUT + ".tmp", "w") as fh:  # replaced whole, never seen half-written
+                    json.dump(out, fh, indent=1, sort_keys=True)
+                os.replace(OUT + ".tmp", OUT)
                 print(f"k={k}: edge cut {case['result']['edge_cut']}, {case['seconds']:.0f} s", flush=True)
 
 
