@@ -50,6 +50,8 @@ WORKLOADS = {
     # the rmat22 graph as the reference's adjacency text, parsed into the resident CSR
     "ingest-rmat22": dict(kind="ingest", graph=dict(kind="rmat", scale=22, edge_factor=16, a=0.57, b=0.19, c=0.19,
                                                     seed=7)),
+    # the learned proposal against the plain method on R-MAT scale 24 and a 3-D geometric 2 M-vertex graph, k = 32
+    "learned-eval": dict(kind="learned"),
 }
 
 
@@ -664,6 +666,42 @@ def run_batch(args, w, rank: int, world: int, local_rank: int, dist) -> dict | N
     }
 
 
+LEARNED_EVAL = [  # held-out graphs of the learned proposal's evaluation: R-MAT scale 24, 3-D geometric 2 M, k = 32
+    dict(name="rmat24", kind="rmat", scale=24, edge_factor=16, seed=9, k=32, theta=10000),
+    dict(name="knn3d-2M", kind="knn", n=2_000_000, dim=3, knn=12, seed=41, k=32, theta=10000),
+]
+
+
+def learned_eval_summary(device: int) -> dict:
+    """The learned proposal on large held-out graphs against the plain method: edge cut, vertex / edge balance
+    and iterations to converge of phase 2 (reference stopping rules) from each start, the gate's decision, and
+    the proposal with the gate ignored."""
+    from dmolp_b200 import graphs
+    from dmolp_b200.learned import WEIGHTS, Proposal, evaluate_large
+
+    model = Proposal(device, WEIGHTS)
+    out = {}
+    try:
+        for spec in LEARNED_EVAL:
+            t0 = time.perf_counter()
+            if spec["kind"] == "rmat":
+                g = graphs.rmat(spec["scale"], spec["edge_factor"], seed=spec["seed"])
+            else:
+                g = graphs.knn(spec["n"], spec["dim"], spec["knn"], seed=spec["seed"])
+            gen_s = time.perf_counter() - t0
+            r = evaluate_large(model, g, spec["k"], spec["theta"], device)
+            r["generate_s"] = gen_s
+            pl = r["plain"]
+            for key in ("learned", "proposal_gate_ignored"):
+                if key in r:
+                    r[key]["cut_ratio_vs_plain"] = r[key]["edge_cut"] / max(1, pl["edge_cut"])
+            out[spec["name"]] = r
+            del g
+    finally:
+        model.close()
+    return out
+
+
 def batched_summary(n: int, theta: int, device: int) -> dict:
     """A compact view of the batched forms for the default bench line: n graphs of the batched mix, whole
     pipeline (phase 1 + phase 2 with the reference's stopping rules) one graph after another on the
@@ -887,6 +925,8 @@ def run_reference_arm(args, w) -> dict:
     if w["kind"] == "batch":
         return {"impl": "reference", "unavailable": "the reference has no batched path; its per-graph CPU phase 2 "
                                                     "is the rmat22/knn-c0 reference arm"}
+    if w["kind"] == "learned":
+        return {"impl": "reference", "unavailable": "the reference has no learned proposal"}
     g = make_graph(w)
     # phase-1 labels from the oracle (the reference's phase 1 is undefined on R-MAT: fewer seeds than parts)
     labels1 = oracle.phase1(g.offsets, g.indices, g.raw_deg(), w["k"], w["theta"]).labels
@@ -960,6 +1000,11 @@ def main():
         torch.cuda.set_device(local_rank)
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
+    if w["kind"] == "learned":
+        if rank == 0:
+            print(json.dumps({"metric": "learned proposal vs plain (edge cut, balance, iterations)",
+                              "learned_eval": learned_eval_summary(local_rank)}), flush=True)
+        return
     runner = {"batch": run_batch, "ingest": run_ingest}.get(w["kind"], run_ours)
     line = runner(args, w, rank, world, local_rank, dist)
     if dist:
@@ -980,6 +1025,10 @@ def main():
                 line["batched"] = batched_summary(2048, 1000, local_rank)  # the batched config: 2048 graphs
             except Exception as e:  # report, do not hide
                 line["batched"] = {"error": str(e)[:300]}
+            try:
+                line["learned_eval"] = learned_eval_summary(local_rank)
+            except Exception as e:  # report, do not hide
+                line["learned_eval"] = {"error": str(e)[:300]}
             try:
                 line["ingest"] = ingest_summary(make_graph(w), local_rank)
             except Exception as e:  # report, do not hide

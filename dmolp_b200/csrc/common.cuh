@@ -18,13 +18,13 @@ constexpr int kSelHistBuffers = 3;          // the radix select's global histogr
 
 // Degree bins of the LP window selection (k <= kDegSelMaxK).  A record's degree d falls in a superbin s
 // and a fine bin f inside it: s = d for d < 64 (one degree each); 64 + (d - 64) / 64 for d < 2048 (64
-// degrees, f = the offset); for d >= 2048 a 1/32-octave bin c = 32 * (floor(log2 d) - 11) + the next five
-// bits of d, s = 95 + c / 64, f = c % 64.  Ascending (s, f) is ascending degree; records that share a fine
-// bin below 2048 share their degree.
+// degrees, f = the offset); for d >= 2048 one superbin per octave, s = 95 + floor(log2 d) - 11, and f = the
+// six bits of d below its leading one (1/64 octave).  Ascending (s, f) is ascending degree; records that share
+// a fine bin below 2048 share their degree.
 constexpr int kDegSelMaxK = 64;
 constexpr int kDsSingle = 64;                         // superbins of one degree
 constexpr int kDsCoarse0 = kDsSingle + 31;            // first superbin of degrees >= 2048
-constexpr int kDsBins = kDsCoarse0 + 10;              // superbins per label (degrees < 2^31)
+constexpr int kDsBins = kDsCoarse0 + 20;              // superbins per label (degrees < 2^31)
 constexpr int kDsFine = 64;                           // fine bins per superbin
 constexpr int kDsExactMax = 2048;                     // degrees below this have a fine bin of their own
 
@@ -32,8 +32,7 @@ __device__ __forceinline__ int2 dsel_bin(int d) {
     if (d < kDsSingle) return make_int2(d, 0);
     if (d < kDsExactMax) return make_int2(kDsSingle + ((d - kDsSingle) >> 6), (d - kDsSingle) & 63);
     const int j = 31 - __clz(d);
-    const int c = 32 * (j - 11) + ((d >> (j - 5)) & 31);
-    return make_int2(kDsCoarse0 + (c >> 6), c & 63);
+    return make_int2(kDsCoarse0 + (j - 11), (d >> (j - 6)) & 63);
 }
 
 // 5-bit bit reversal: the position at which the reference's 32-lane shuffle-down tree prefers a lane

@@ -42,7 +42,6 @@ struct LpCounters {
     unsigned long long cut_arcs;   // arcs whose endpoint labels differ (kept current incrementally)
     int dgrab[3];     // decisions: work items taken so far per class (thread groups, warp groups, hub chunks)
     int nhubw;        // queued row chunks of hubs that entered or left the window
-    int ntail;        // degree-bin selection: records of partial superbins of degree >= 2048 (coarse ties)
 };
 
 // Loop control shared by the iteration kernels.
@@ -126,6 +125,7 @@ struct Buffers {
     unsigned int *dsup = nullptr;        // [kDegSelMaxK * kDsBins]
     unsigned int *dfine[2] = {nullptr, nullptr};  // [kDegSelMaxK * kDsFine] each
     unsigned int *dcntb = nullptr;       // [num_sms * kDegSelMaxK * kDsFine]
+    int *dtcnt = nullptr;                // [2 * kDegSelMaxK] tail records per label (by iteration parity)
     int32_t *need = nullptr;             // [MAX_K]
     int32_t *sel_below = nullptr;        // [MAX_K]
     int32_t *keep_digit = nullptr;       // [MAX_K]

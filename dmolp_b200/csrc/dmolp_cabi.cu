@@ -88,12 +88,13 @@ int sync(dmolp_ctx *c) {
     return check_launch(c);
 }
 
-// Clears the degree-bin selection's counts (superbin and fine-bin counts of both parities).
+// Clears the degree-bin selection's counts (superbin counts; fine-bin and tail counts of both parities).
 int clear_select_bins(dmolp_ctx *c) {
     Buffers &b = c->b;
     DMOLP_CUDA(cudaMemsetAsync(b.dsup, 0, (size_t)kDegSelMaxK * kDsBins * sizeof(unsigned int), c->stream));
     for (int i = 0; i < 2; ++i)
         DMOLP_CUDA(cudaMemsetAsync(b.dfine[i], 0, (size_t)kDegSelMaxK * kDsFine * sizeof(unsigned int), c->stream));
+    DMOLP_CUDA(cudaMemsetAsync(b.dtcnt, 0, 2 * kDegSelMaxK * sizeof(int), c->stream));
     return DMOLP_OK;
 }
 
@@ -264,6 +265,7 @@ size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t 
     ALLOC(b.dfine[0], (size_t)kDegSelMaxK * kDsFine);
     ALLOC(b.dfine[1], (size_t)kDegSelMaxK * kDsFine);
     ALLOC(b.dcntb, (size_t)c->num_sms * kDegSelMaxK * kDsFine);
+    ALLOC(b.dtcnt, 2 * kDegSelMaxK);
     ALLOC(b.need, DMOLP_MAX_K);
     ALLOC(b.sel_below, DMOLP_MAX_K);
     ALLOC(b.keep_digit, DMOLP_MAX_K);

@@ -56,7 +56,6 @@ __device__ void lp_begin(const Buffers &b, int k, int t, long long narcs) {
         cn->nchunk = 0;
         cn->nhubq = 0;
         cn->nhubw = 0;
-        cn->ntail = 0;
         cn->dgrab[0] = cn->dgrab[1] = cn->dgrab[2] = 0;
         ctl->stop_now = 0;
         ctl->skip_stats = 0;
@@ -228,11 +227,11 @@ __device__ __forceinline__ uint64_t sel_key(const Buffers &b, int own, int deg, 
 }
 
 // Record slot pos (the vertex's position in ball): own label and key of a boundary vertex, -1 otherwise.
-// No global append: every slot is rewritten each iteration.
+// No global append: every slot is rewritten each iteration.  (The LP selections emit the window directly;
+// the selection flags bsel are read only by phase 1, which clears its own.)
 __device__ __forceinline__ void put_slot(const Buffers &b, int pos, bool isb, int own, uint64_t key) {
     b.bown[pos] = isb ? own : -1;
     if (isb) b.bkey[pos] = key;
-    b.bsel[pos] = 0;
 }
 
 // Candidacy: t = 1 every vertex; push mode stamp[v] == t (set by k_mark); pull mode v is in the previous
@@ -1193,7 +1192,6 @@ __global__ void k_ws_begin(Buffers b, int k, int t, int nprev) {
         cn->ndec[0] = cn->ndec[1] = cn->ndec[2] = 0;
         cn->nwin[(t - 1) & 1] = nprev;
         cn->nwin[t & 1] = 0;
-        cn->ntail = 0;
         b.ctrl->stopped = 0;
         b.ctrl->pull = 0;
         LpRecordDev &r = b.rec[t - 1];

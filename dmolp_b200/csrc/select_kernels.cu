@@ -521,28 +521,29 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
 //   0. every block finds, per label, the superbin where the running count in the label's order reaches
 //      need_p; records of the superbins before it are taken, the rest of that superbin is partial;
 //   1. each warp walks its own contiguous range of record slots in order: taken records go to the window;
-//      records of a partial superbin go to the warp's list (in slot order) and into the block's fine-bin
-//      counts (stored per block in dcntb, summed into dfine); those of degree >= 2048 also to a tail list;
+//      records of a partial superbin of degree < 2048 go to the warp's list (in slot order) and into the
+//      block's fine-bin counts (stored per block in dcntb, summed into dfine); those of degree >= 2048 to
+//      their label's segment of a tail list (segments sized by the superbin counts) and into dfine;
 //   -- grid barrier --
 //   2. every block finds, per label, the fine bin of the partial superbin where the count reaches the rest
 //      of the need.  Below degree 2048 a fine bin is a single degree, and record slots hold the vertices of
 //      one degree in ascending id order (slots follow the degree classes, ids ascending inside a class), so
 //      a record of the partial fine bin is taken when fewer than the rest of the need precede it: in the
-//      blocks before this one (dcntb), in the warps before this one, in its warp's list before it.  Block 0
-//      ranks the tail's records of a partial coarse fine bin by their keys (degree, then id).
+//      blocks before this one (dcntb), in the warps before this one, in its warp's list before it.  Above,
+//      block p ranks label p's tail records of the partial fine bin by their keys (degree, then id).
 // ------------------------------------------------------------------------------------------------------
 constexpr int kDsThreads = 1024;
 constexpr int kDsWarps = kDsThreads / 32;
 constexpr int kDsU = 2;          // record slots per lane and step of the first walk
-constexpr int kDsTieCap = 4096;  // coarse tied records ranked in shared memory (more: ranked from global)
+constexpr int kDsTieCap = 4096;  // a label's coarse tied records ranked in shared memory (more: from global)
 
 struct DegSelArgs {
     const int32_t *seg;        // bown: label of a boundary record, -1 for an empty slot
     const uint64_t *key;       // bkey: (dk << ibits) | v
     const int *n_dev;          // record slots
-    int32_t *lists;            // the warps' lists of partial-superbin records (active[0])
-    int32_t *tail;             // partial-superbin records of degree >= 2048 (active[1])
-    int *ntail;
+    int32_t *lists;            // the warps' lists of partial-superbin records below degree 2048 (active[0])
+    int32_t *tail;             // partial-superbin records of degree >= 2048, one segment per label (active[1])
+    int *tcnt, *tcnt_next;     // [nseg] tail records per label (this iteration / the next one's, cleared here)
     unsigned int *dsup;        // [nseg * kDsBins] from the boundary test; cleared here after the barrier
     unsigned int *dfine;       // [nseg * kDsFine] fine counts of this iteration's partial superbins
     unsigned int *dfine_next;  // the other parity's buffer, cleared here for the next iteration
@@ -554,9 +555,9 @@ struct DegSelArgs {
     SplitArgs sp;
 };
 
-// Dynamic shared memory of k_select_deg for nseg labels (16-byte aligned pieces).
+// Dynamic shared memory of k_select_deg for nseg labels.
 __host__ __device__ constexpr size_t ds_smem_bytes(int nseg) {
-    return (size_t)kDsTieCap * 8 + (size_t)kDsTieCap * 8 + (size_t)8 * nseg * 4 + (size_t)nseg * kDsFine * 4 +
+    return (size_t)kDsTieCap * 8 + (size_t)10 * nseg * 4 + (size_t)nseg * kDsFine * 4 +
            (size_t)2 * kDsWarps * nseg * 4 + (size_t)kDsWarps * 4 * kStage * 4;
 }
 
@@ -601,31 +602,36 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
     extern __shared__ __align__(16) unsigned char ds_smem[];
     const int nseg = a.nseg, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned below = (1u << lane) - 1;
-    uint64_t *s_tkey = reinterpret_cast<uint64_t *>(ds_smem);       // [kDsTieCap] coarse ties (block 0)
-    int *s_tslot = reinterpret_cast<int *>(s_tkey + kDsTieCap);     // [kDsTieCap]
-    int *s_tseg = s_tslot + kDsTieCap;                              // [kDsTieCap]
-    int *s_otake = s_tseg + kDsTieCap;  // [nseg] superbin order positions below this are taken
-    int *s_opart = s_otake + nseg;      // [nseg] order position of the partial superbin, -1 none
-    int *s_rem = s_opart + nseg;        // [nseg] records still needed from the partial superbin
-    int *s_dir = s_rem + nseg;          // [nseg] 1: largest degree first (RE > 1)
-    int *s_ftake = s_dir + nseg;        // [nseg] fine order positions below this are taken
-    int *s_fpart = s_ftake + nseg;      // [nseg] fine order position of the partial fine bin, -1 none
-    int *s_frem = s_fpart + nseg;       // [nseg] records still needed from the partial fine bin
-    int *s_pre = s_frem + nseg;         // [nseg] the partial fine bin's records in the blocks before this one
+    uint64_t *s_tkey = reinterpret_cast<uint64_t *>(ds_smem);       // [kDsTieCap] keys of this block's coarse ties
+    int *s_otake = reinterpret_cast<int *>(s_tkey + kDsTieCap);     // [nseg] superbin order positions below this are taken
+    int *s_opart = s_otake + nseg;       // [nseg] order position of the partial superbin, -1 none
+    int *s_rem = s_opart + nseg;         // [nseg] records still needed from the partial superbin
+    int *s_dir = s_rem + nseg;           // [nseg] 1: largest degree first (RE > 1)
+    int *s_kind = s_dir + nseg;          // [nseg] partial superbin: 0 none, 1 one degree, 2 < 2048, 3 coarse
+    int *s_toff = s_kind + nseg;         // [nseg] the label's segment of the tail list
+    int *s_ftake = s_toff + nseg;        // [nseg] fine order positions below this are taken
+    int *s_fpart = s_ftake + nseg;       // [nseg] fine order position of the partial fine bin, -1 none
+    int *s_frem = s_fpart + nseg;        // [nseg] records still needed from the partial fine bin
+    int *s_pre = s_frem + nseg;          // [nseg] the partial fine bin's records in the blocks before this one
     unsigned int *s_f = reinterpret_cast<unsigned int *>(s_pre + nseg);  // [nseg * kDsFine] this block's
     int *s_wc = reinterpret_cast<int *>(s_f + nseg * kDsFine);  // [kDsWarps * nseg] partial fine bin per warp
     int *s_wrun = s_wc + kDsWarps * nseg;                       // [kDsWarps * nseg] running rank per warp
     int *s_stage = s_wrun + kDsWarps * nseg;                    // [kDsWarps * 4 * kStage] window appends
     __shared__ int s_scnt[kDsWarps][4];
-    __shared__ int s_ntie;
+    __shared__ int s_ntie, s_walk1;
     int *w_stage = s_stage + wid * 4 * kStage, *w_scnt = s_scnt[wid];
     if (lane < 4) w_scnt[lane] = 0;
     for (int i = threadIdx.x; i < nseg * kDsFine; i += blockDim.x) s_f[i] = 0u;
     for (int i = threadIdx.x; i < kDsWarps * nseg; i += blockDim.x) s_wc[i] = 0;
-    if (threadIdx.x == 0) s_ntie = 0;
-    // the other parity's fine counts were read by the previous iteration's selection: clear them
+    if (threadIdx.x == 0) {
+        s_ntie = 0;
+        s_walk1 = 0;
+    }
+    // the other parity's fine and tail counts were used by the previous iteration's selection: clear them
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nseg * kDsFine; i += gridDim.x * blockDim.x)
         a.dfine_next[i] = 0u;
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < nseg; i += blockDim.x) a.tcnt_next[i] = 0;
     // ---- 0. per label: the superbin where the need is reached ----
     const double ratio = *a.sp.ratio;
     for (int p = wid; p < nseg; p += kDsWarps) {
@@ -633,7 +639,7 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         const int m = (int)ceil(__dmul_rn(ratio, (double)n));  // ceil(e^(-t/5) n), gpu_lp_boundary.cu:296-297
         const int need = m > n ? n : m;
         const int dir = __ldg(a.sp.RE + p) > 1.0 ? 1 : 0;
-        int take = need >= n ? kDsBins : 0, part = -1, rem = 0;
+        int take = need >= n ? kDsBins : 0, part = -1, rem = 0, kind = 0, tsize = 0;
         if (need > 0 && need < n) {
             int pos, before, count;
             ds_cross<(kDsBins + 31) / 32>(need, [&](int o) {
@@ -647,6 +653,9 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
                 take = pos;
                 part = pos;
                 rem = need - before;
+                const int sb = ds_ord(pos, kDsBins, dir);
+                kind = sb < kDsSingle ? 1 : (sb < kDsCoarse0 ? 2 : 3);
+                if (kind == 3) tsize = count;
             }
         }
         if (lane == 0) {
@@ -654,7 +663,22 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
             s_opart[p] = part;
             s_rem[p] = rem;
             s_dir[p] = dir;
+            s_kind[p] = kind;
+            s_toff[p] = tsize;  // the segment sizes, turned into offsets below
         }
+    }
+    __syncthreads();
+    if (wid == 0) {  // exclusive prefix of the tail segment sizes (nseg <= 64: two per lane)
+        const int x0 = lane < nseg ? s_toff[lane] : 0, x1 = lane + 32 < nseg ? s_toff[lane + 32] : 0;
+        int incl = x0 + x1;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(DMOLP_FULL_MASK, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - x0 - x1;
+        __syncwarp();
+        if (lane < nseg) s_toff[lane] = excl;
+        if (lane + 32 < nseg) s_toff[lane + 32] = excl + x0;
     }
     __syncthreads();
     // ---- 1. each warp walks its own contiguous range of record slots ----
@@ -669,19 +693,18 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
     const int ibits = a.sp.ibits, maxdeg = a.sp.maxdeg;
     const uint64_t vmask = (1ull << ibits) - 1;
     unsigned long long te = 0, ws = 0;
-    auto bins_of = [&](uint64_t key, int p, int &o, int &fo, bool &coarse) {
+    auto bins_of = [&](uint64_t key, int p, int &o, int &fo) {
         const int dir = s_dir[p];
         const int dk = (int)(key >> ibits);
         const int2 bf = dsel_bin(dir ? maxdeg - dk : dk);
         o = ds_ord(bf.x, kDsBins, dir);
         fo = ds_ord(bf.y, kDsFine, dir);
-        coarse = bf.x >= kDsCoarse0;
         return bf;
     };
     for (int r0 = wlo; r0 < whi; r0 += 32 * kDsU) {
-        int r[kDsU], p[kDsU];
+        int r[kDsU], p[kDsU], fb[kDsU];
         uint64_t key[kDsU];
-        bool take[kDsU], part[kDsU], tl[kDsU];
+        bool take[kDsU], part[kDsU];
 #pragma unroll
         for (int u = 0; u < kDsU; ++u) {
             r[u] = r0 + u * 32 + lane;
@@ -690,27 +713,39 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         }
 #pragma unroll
         for (int u = 0; u < kDsU; ++u) {
-            take[u] = part[u] = tl[u] = false;
+            take[u] = part[u] = false;
+            fb[u] = -1;
             if (p[u] >= 0) {
                 int o, fo;
-                bool coarse;
-                const int2 bf = bins_of(key[u], p[u], o, fo, coarse);
+                const int2 bf = bins_of(key[u], p[u], o, fo);
                 if (o < s_otake[p[u]]) {
                     take[u] = true;
                 } else if (o == s_opart[p[u]]) {
                     part[u] = true;
-                    tl[u] = coarse;
-                    atomicAdd(&s_f[p[u] * kDsFine + bf.y], 1u);
+                    fb[u] = p[u] * kDsFine + bf.y;
                 }
             }
         }
 #pragma unroll
-        for (int u = 0; u < kDsU; ++u) {  // partial-superbin records to the warp's list, in slot order
-            const unsigned mp = __ballot_sync(DMOLP_FULL_MASK, part[u]);
-            if (part[u]) wlist[wl + __popc(mp & below)] = r[u];
+        for (int u = 0; u < kDsU; ++u) {
+            // fine counts, one shared atomic per (label, fine bin) group of the warp; a partial superbin of
+            // one degree has a single fine bin, so its group is also the warp's count of the label's ties
+            const unsigned mg = __match_any_sync(DMOLP_FULL_MASK, fb[u] >= 0 ? fb[u] : -1 - lane);
+            const bool coarse = part[u] && s_kind[p[u]] == 3;
+            if (part[u] && lane == __ffs(mg) - 1) {
+                atomicAdd(&s_f[fb[u]], (unsigned)__popc(mg));
+                if (s_kind[p[u]] == 1) s_wc[wid * nseg + p[u]] += __popc(mg);
+            }
+            // records below degree 2048 to the warp's list, in slot order; coarse ones to their label's
+            // tail segment (one global atomic per label group of the warp)
+            const unsigned mp = __ballot_sync(DMOLP_FULL_MASK, part[u] && !coarse);
+            if (part[u] && !coarse) wlist[wl + __popc(mp & below)] = r[u];
             wl += __popc(mp);
-            const int q = warp_append(a.ntail, tl[u]);
-            if (tl[u]) a.tail[q] = r[u];
+            const unsigned mc = __match_any_sync(DMOLP_FULL_MASK, coarse ? p[u] : -1 - lane);
+            int q = 0;
+            if (coarse && lane == __ffs(mc) - 1) q = atomicAdd(&a.tcnt[p[u]], __popc(mc));
+            q = __shfl_sync(DMOLP_FULL_MASK, q, coarse ? __ffs(mc) - 1 : lane);
+            if (coarse) a.tail[s_toff[p[u]] + q + __popc(mc & below)] = r[u];
         }
         emit_window<kDsU>(a.sp, take, key, p, vmask, te, ws, w_stage, w_scnt);  // all lanes
     }
@@ -727,8 +762,8 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
     // ---- 2. per label with a partial superbin: the fine bin where the rest of the need is reached ----
     for (int p = wid; p < nseg; p += kDsWarps) {
         int take = 0, part = -1, rem = 0, pre = 0;
-        const int opart = s_opart[p];
-        if (opart >= 0) {
+        const int kind = s_kind[p];
+        if (kind != 0) {
             const int dir = s_dir[p];
             const int need = s_rem[p];
             int pos, before, count;
@@ -743,11 +778,12 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
                 take = pos;
                 part = pos;
                 rem = need - before;
-                if (ds_ord(opart, kDsBins, dir) < kDsCoarse0) {  // one degree: the blocks before this one
+                if (kind != 3) {  // one degree: its records in the blocks before this one
                     const int f = ds_ord(pos, kDsFine, dir);
                     for (int b = lane; b < (int)blockIdx.x; b += 32)
                         pre += (int)__ldcg(a.dcntb + (size_t)b * nseg * kDsFine + p * kDsFine + f);
                     for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(DMOLP_FULL_MASK, pre, o);
+                    if (lane == 0 && kind == 2) s_walk1 = 1;  // the warps' counts need a walk of the lists
                 }
             }
         }
@@ -770,22 +806,23 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
             p = a.seg[r];
             key = a.key[r];
             int o;
-            bool coarse;
-            bins_of(key, p, o, fo, coarse);
-            tie = !coarse && fo == s_fpart[p];
+            bins_of(key, p, o, fo);
+            tie = fo == s_fpart[p];
         }
     };
-    // exact ties: this warp's count per label, then every warp's base rank
-    for (int i0 = 0; i0 < wl; i0 += 32) {
-        int p, fo;
-        uint64_t key;
-        bool tie;
-        list_rec(i0 + lane, p, key, fo, tie);
-        const unsigned m = __match_any_sync(DMOLP_FULL_MASK, tie ? p : -1 - lane);
-        if (tie && lane == __ffs(m) - 1) s_wc[wid * nseg + p] += __popc(m);
-        __syncwarp();
+    if (s_walk1) {  // exact ties of multi-degree superbins: this warp's count per label
+        for (int i0 = 0; i0 < wl; i0 += 32) {
+            int p, fo;
+            uint64_t key;
+            bool tie;
+            list_rec(i0 + lane, p, key, fo, tie);
+            tie = tie && s_kind[p] == 2;
+            const unsigned m = __match_any_sync(DMOLP_FULL_MASK, tie ? p : -1 - lane);
+            if (tie && lane == __ffs(m) - 1) s_wc[wid * nseg + p] += __popc(m);
+            __syncwarp();
+        }
+        __syncthreads();
     }
-    __syncthreads();
     for (int i = threadIdx.x; i < kDsWarps * nseg; i += blockDim.x) {
         const int w = i / nseg, p = i - w * nseg;
         int base = s_pre[p];
@@ -806,64 +843,66 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         __syncwarp();
         emit_window<1>(a.sp, &take, &key, &p, vmask, te, ws, w_stage, w_scnt);  // all lanes
     }
-    // ---- block 0: ties in a partial fine bin of degree >= 2048, ranked by key ----
-    if (blockIdx.x == 0) {
-        const int nt = __ldcg(a.ntail);
-        auto tail_rec = [&](int i, int &p, uint64_t &key) {  // a tail record of a partial coarse fine bin?
-            const int r = __ldcg(a.tail + i);
-            p = a.seg[r];
-            key = a.key[r];
-            int o, fo;
-            bool coarse;
-            bins_of(key, p, o, fo, coarse);
-            return coarse && fo == s_fpart[p];
-        };
-        for (int i = threadIdx.x; i < nt; i += blockDim.x) {
-            int p;
-            uint64_t key;
-            if (tail_rec(i, p, key)) {
-                const int q = atomicAdd(&s_ntie, 1);
-                if (q < kDsTieCap) {
-                    s_tkey[q] = key;
-                    s_tslot[q] = __ldcg(a.tail + i);
-                    s_tseg[q] = p;
+    // ---- block p (p, p + gridDim.x, ...): label p's records of a partial superbin of degree >= 2048 ----
+    for (int p = blockIdx.x; p < nseg; p += gridDim.x) {
+        if (s_kind[p] != 3) continue;  // block-uniform
+        const int nt = __ldcg(a.tcnt + p);
+        const int32_t *seg_tail = a.tail + s_toff[p];
+        const int ftake = s_ftake[p], fpart = s_fpart[p], frem = s_frem[p];
+        __syncthreads();  // s_ntie and the shared tie arrays are free
+        if (threadIdx.x == 0) s_ntie = 0;
+        __syncthreads();
+        // the segment in chunks: records of fine bins before the partial one are taken, those of the partial
+        // fine bin are collected for ranking
+        for (int i0 = 0; i0 < nt; i0 += blockDim.x) {
+            const int i = i0 + (int)threadIdx.x;
+            bool take = false;
+            uint64_t key = 0;
+            int pp = p;
+            if (i < nt) {
+                const int r = __ldcg(seg_tail + i);
+                key = a.key[r];
+                int o, fo;
+                bins_of(key, p, o, fo);
+                if (fo < ftake) {
+                    take = true;
+                } else if (fo == fpart) {
+                    const int q = atomicAdd(&s_ntie, 1);
+                    if (q < kDsTieCap) s_tkey[q] = key;
                 }
             }
+            emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
         }
         __syncthreads();
         const int m = s_ntie;
-        if (m <= kDsTieCap) {
-            for (int i0 = 0; i0 < m; i0 += blockDim.x) {
-                const int i = i0 + (int)threadIdx.x;
-                bool take = false;
-                int p = -1;
-                uint64_t key = 0;
-                if (i < m) {
-                    p = s_tseg[i];
+        const int rounds = m <= kDsTieCap ? m : nt;  // ranked in shared memory, or from the segment
+        for (int i0 = 0; i0 < rounds; i0 += blockDim.x) {
+            const int i = i0 + (int)threadIdx.x;
+            bool take = false;
+            uint64_t key = 0;
+            int pp = p;
+            if (i < rounds) {
+                int rank = 0;
+                if (m <= kDsTieCap) {
                     key = s_tkey[i];
-                    int rank = 0;
-                    for (int j = 0; j < m; ++j) rank += (s_tseg[j] == p && s_tkey[j] < key);
-                    take = rank < s_frem[p];
-                }
-                emit_window<1>(a.sp, &take, &key, &p, vmask, te, ws, w_stage, w_scnt);  // all lanes
-            }
-        } else {  // more ties than the shared arrays hold: rank against the tail in global memory
-            for (int i0 = 0; i0 < nt; i0 += blockDim.x) {
-                const int i = i0 + (int)threadIdx.x;
-                bool take = false;
-                int p = -1;
-                uint64_t key = 0;
-                if (i < nt && tail_rec(i, p, key)) {
-                    int rank = 0;
-                    for (int j = 0; j < nt; ++j) {
-                        int pj;
-                        uint64_t kj;
-                        rank += (tail_rec(j, pj, kj) && pj == p && kj < key);
+                    for (int j = 0; j < m; ++j) rank += s_tkey[j] < key;
+                    take = rank < frem;
+                } else {
+                    key = a.key[__ldcg(seg_tail + i)];
+                    int o, fo;
+                    bins_of(key, p, o, fo);
+                    if (fo == fpart) {
+                        for (int j = 0; j < nt; ++j) {
+                            const uint64_t kj = a.key[__ldcg(seg_tail + j)];
+                            int oj, foj;
+                            bins_of(kj, p, oj, foj);
+                            rank += foj == fpart && kj < key;
+                        }
+                        take = rank < frem;
                     }
-                    take = rank < s_frem[p];
                 }
-                emit_window<1>(a.sp, &take, &key, &p, vmask, te, ws, w_stage, w_scnt);  // all lanes
             }
+            emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
         }
     }
     stage_flush(a.sp, w_stage, w_scnt);
@@ -924,7 +963,8 @@ bool select_window_deg(dmolp_ctx *c, int nseg, const SplitArgs &split, const int
     a.n_dev = &c->b.cnt->npos;
     a.lists = c->b.active[0];
     a.tail = c->b.active[1];
-    a.ntail = &c->b.cnt->ntail;
+    a.tcnt = c->b.dtcnt + (split.t & 1) * kDegSelMaxK;
+    a.tcnt_next = c->b.dtcnt + ((split.t + 1) & 1) * kDegSelMaxK;
     a.dsup = c->b.dsup;
     a.dfine = c->b.dfine[split.t & 1];
     a.dfine_next = c->b.dfine[(split.t + 1) & 1];

@@ -217,3 +217,50 @@ def train(model: Proposal, sets: list[tuple[list[Instance], list[np.ndarray]]], 
     for b, _, _ in prepared:
         b.close()
     return losses
+
+
+def evaluate_large(model: Proposal, g, k: int, theta: int, device: int = 0) -> dict:
+    """One large graph, k parts: the plain method (phase 1, then phase 2 with the reference's stopping rules,
+    on the single-graph path) against the learned start -- the proposal where the gate accepts it, phase 1
+    where it declines -- and against the proposal itself with the gate ignored.  Per start: edge cut, vertex
+    and edge balance, iterations to converge, wall time of the start and of phase 2."""
+    import torch
+
+    def run_from(p: Partitioner, labels: np.ndarray | None) -> dict:
+        if labels is not None:
+            p.set_labels(labels)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m = p.phase2(k, mode="ref", records=False)
+        return {"edge_cut": int(m.edge_cut), "vertex_balance": m.vertex_balance, "edge_balance": m.edge_balance,
+                "iterations": int(m.iterations_run), "phase2_s": time.perf_counter() - t0}
+
+    p = Partitioner(device)
+    p.upload(g)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    p.phase1(k, theta)
+    plain_start_s = time.perf_counter() - t0
+    lab1 = p.labels()
+    plain = run_from(p, None)
+    plain["start_s"] = plain_start_s
+    b = Batch(device)
+    b.upload([Instance(g, k, "eval")])
+    model.propose(b)  # workspace set-up for this size (not timed)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = model.propose(b)
+    gate = float(model.gate(b)[0])
+    prop_s = time.perf_counter() - t0
+    out = {"num_vertices": g.num_vertices, "num_arcs": g.num_arcs, "k": k, "theta": theta, "plain": plain,
+           "gate_score": gate, "gate_accepts": bool(st[0] == 0)}
+    forced_st = st if st[0] == 0 else model.decode(b)  # the proposal with the gate ignored
+    if forced_st[0] == 0:
+        forced = run_from(p, b.labels())
+        forced["start_s"] = prop_s
+        out["proposal_gate_ignored"] = forced
+    out["learned"] = out.get("proposal_gate_ignored") if st[0] == 0 else dict(plain, start_s=plain_start_s + prop_s)
+    b.close()
+    p.set_labels(lab1)
+    p.close()
+    return out

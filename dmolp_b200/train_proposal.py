@@ -43,6 +43,35 @@ def evaluate(model: Proposal, inst, plain, theta: int, device: int = 0) -> dict:
     return out
 
 
+def chunked_targets(inst, theta: int, chunk: int = 1024, device: int = 0) -> tuple[np.ndarray, dict]:
+    """The gate's targets for many graphs, chunk by chunk (a batch per chunk): per graph the plain method
+    (batched phase 1, identical per graph to the single-graph phase 1, then phase 2 with the reference's
+    stopping rules) and the untrained proposal (accepted for every graph) followed by the same phase 2;
+    target 1 where the proposal ended at an edge cut no higher than the plain method's."""
+    y = np.zeros(len(inst), np.float32)
+    model = Proposal(device)
+    stats = {"plain_cut": 0, "proposal_cut": 0, "chunks": 0}
+    for c0 in range(0, len(inst), chunk):
+        part = inst[c0:c0 + chunk]
+        b = Batch(device)
+        b.upload(part)
+        b.phase1(theta)
+        plain, _ = b.run("ref")
+        st = model.propose(b)
+        if st.any():
+            b.phase1(theta, only=st != 0)
+        prop, _ = b.run("ref")
+        b.close()
+        pc = np.array([r["edge_cut"] for r in plain])
+        qc = np.array([r["edge_cut"] for r in prop])
+        y[c0:c0 + len(part)] = (qc <= pc).astype(np.float32)
+        stats["plain_cut"] += int(pc.sum())
+        stats["proposal_cut"] += int(qc.sum())
+        stats["chunks"] += 1
+    model.close()
+    return y, stats
+
+
 def cut_of(g, lab) -> int:
     src = np.repeat(np.arange(g.num_vertices), np.diff(g.offsets))
     return int((lab[src] != lab[g.indices]).sum() // 2)
@@ -86,13 +115,14 @@ def main():
     ap.add_argument("--seed", type=int, default=101)
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--chunk", type=int, default=1024, help="graphs per batch when computing the targets")
     a = ap.parse_args()
     rep = {"args": vars(a)}
     t0 = time.time()
     tr = random_instances(a.train, seed=a.seed, vmin=a.vmin, vmax=a.vmax)
-    plain = plain_eval(tr, a.theta)
-    always = evaluate(Proposal(0), tr, plain, a.theta)  # the untrained gate accepts every proposal
-    y = (np.array(always["cut"]) <= np.array(plain["cut"])).astype(np.float32)
+    rep["generate_s"] = time.time() - t0
+    t0 = time.time()
+    y, rep["target_stats"] = chunked_targets(tr, a.theta, a.chunk)
     rep["targets_s"] = time.time() - t0
     rep["train_targets_positive"] = float(y.mean())
     sets = [(tr[i:i + a.minibatch], y[i:i + a.minibatch]) for i in range(0, len(tr), a.minibatch)]

@@ -170,7 +170,7 @@ def test_device_entry_points_equal_the_reference_functions():
     """Every entry point of the driver against the reference's own functions (its phase 1, its run_phase2
     loop, its single-step GPU functions with its kernel built for sm_100a), on a 5,000-vertex 3-D k-NN graph:
     lower-level and whole phase 1, run_phase2 with the reference's stopping rules, one LP step through
-    runBoundaryLPOnGPU_SubgraphUnified, _Chunked with room for one 1024-node chunk (the subgraph needs five:
+    runBoundaryLPOnGPU_SubgraphUnified, _Chunked with room for one 1024-node chunk (the subgraph needs four:
     arcs across chunks are dropped, gpu_lp_boundary.cu:571-675) and _Streaming with and without room, and the
     -m random path (random_partition, then run_phase2)."""
     from dmolp_b200 import graphs
@@ -182,7 +182,7 @@ def test_device_entry_points_equal_the_reference_functions():
         graphs.write_adjtext(g, txt)
         ours = run_driver(txt, k, theta, 0)
         ref = run_driver(txt, k, theta, 0, reference=True)
-    assert ours["chunks"]["subgraph_nodes"] > 4 * 1024  # five chunks of the minimum size
+    assert ours["chunks"]["subgraph_nodes"] > 3 * 1024  # four chunks of the minimum size
     for what in ("host", "subgraph", "lower_phase1", "phase1", "phase2", "step_unified", "step_chunked",
                  "step_streaming_chunked", "step_streaming", "chunks", "random_phase1", "random_phase2"):
         assert ours[what] == ref[what], what
