@@ -31,6 +31,7 @@ def gen() -> ctypes.CDLL:
         lib.dmolp_gen_rmat.argtypes = [c_int, c_int, c_double, c_double, c_double, c_uint64, c_int, POINTER(c_void_p)]
         lib.dmolp_gen_knn.argtypes = [c_int64, c_int, c_int, c_uint64, POINTER(c_void_p)]
         lib.dmolp_gen_ba.argtypes = [c_int64, c_int, c_uint64, POINTER(c_void_p)]
+        lib.dmolp_gen_band.argtypes = [c_int64, c_int, c_int, c_uint64, POINTER(c_void_p)]
         lib.dmolp_csr_from_arrays.argtypes = [c_int64, c_int64, c_void_p, c_void_p, POINTER(c_void_p)]
         lib.dmolp_csr_nv.argtypes = [c_void_p]
         lib.dmolp_csr_nv.restype = c_int64

@@ -126,6 +126,8 @@ struct Buffers {
     unsigned int *dfine[2] = {nullptr, nullptr};  // [kDegSelMaxK * kDsFine] each
     unsigned int *dcntb = nullptr;       // [num_sms * kDegSelMaxK * kDsFine]
     int *dtcnt = nullptr;                // [2 * kDegSelMaxK] tail records per label (by iteration parity)
+    uint64_t *dlkey = nullptr;           // [nv] keys of the selection warps' lists (labels in active[0])
+    uint64_t *dtkey = nullptr;           // [nv] keys of the selection's tail segments
     int32_t *need = nullptr;             // [MAX_K]
     int32_t *sel_below = nullptr;        // [MAX_K]
     int32_t *keep_digit = nullptr;       // [MAX_K]

@@ -266,6 +266,8 @@ size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t 
     ALLOC(b.dfine[1], (size_t)kDegSelMaxK * kDsFine);
     ALLOC(b.dcntb, (size_t)c->num_sms * kDegSelMaxK * kDsFine);
     ALLOC(b.dtcnt, 2 * kDegSelMaxK);
+    ALLOC(b.dlkey, n);
+    ALLOC(b.dtkey, n);
     ALLOC(b.need, DMOLP_MAX_K);
     ALLOC(b.sel_below, DMOLP_MAX_K);
     ALLOC(b.keep_digit, DMOLP_MAX_K);

@@ -653,7 +653,23 @@ GPULabelUpdateResult runBoundaryLPOnGPU_Streaming(const std::vector<int> &row_pt
                                                   const std::vector<int> &global_ids,
                                                   const std::vector<double> &penalty, int num_local_nodes,
                                                   int num_partitions, size_t max_memory_mb) {
-    (void)max_memory_mb;
+    // The reference sizes the subgraph against max_memory_mb and takes the chunked path when it does not fit
+    // (gpu_lp_boundary.cu:541-563).  The subgraph's footprint is bounded by the whole graph's: when that bound
+    // fits, so does the subgraph, and the resident path gives the same result; otherwise the subgraph is
+    // built and measured exactly as the reference does.
+    const size_t avail = max_memory_mb * 1024 * 1024;
+    const size_t nodes_max = (size_t)num_local_nodes + ghost_labels.size();
+    const size_t bound = (nodes_max + 1) * sizeof(int) + col_idx.size() * sizeof(int) + 2 * nodes_max * sizeof(int) +
+                         nodes_max * sizeof(int) + boundary_nodes.size() * sizeof(int) + penalty.size() * sizeof(double);
+    if (bound > avail) {
+        BoundarySubgraph sg = createBoundarySubgraphUnified(row_ptr, col_idx, boundary_nodes, local_labels,
+                                                            ghost_labels, global_ids, num_local_nodes);
+        const size_t need = sg.row_ptr.size() * sizeof(int) + sg.col_idx.size() * sizeof(int) +
+                            2 * sg.labels.size() * sizeof(int) + sg.local_node_flags.size() * sizeof(int) +
+                            sg.boundary_indices.size() * sizeof(int) + penalty.size() * sizeof(double);
+        if (need > avail) return runBoundaryLPOnGPU_Chunked(sg, penalty, num_partitions, avail);
+        return runBoundaryLPOnGPU_SubgraphUnified(sg, penalty, num_partitions);
+    }
     if (!ghost_labels.empty()) {
         BoundarySubgraph sg = createBoundarySubgraphUnified(row_ptr, col_idx, boundary_nodes, local_labels,
                                                             ghost_labels, global_ids, num_local_nodes);

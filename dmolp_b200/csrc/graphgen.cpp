@@ -355,6 +355,62 @@ int dmolp_gen_ba(int64_t n, int m, uint64_t seed, dmolp_csr **out) {
     }
 }
 
+int dmolp_gen_band(int64_t n, int wmin, int wmax, uint64_t seed, dmolp_csr **out) {
+    try {
+        if (n < 3 || n > (int64_t(1) << 31) - 1 || wmin < 1 || wmax < wmin || 2 * (int64_t)wmax >= n) {
+            g_err = "band: bad parameters";
+            return 1;
+        }
+        // vertex i on a cycle of n, with a reach w_i uniform in [wmin, wmax]; i ~ j when their distance on
+        // the cycle is at most max(w_i, w_j) (symmetric); rows come out sorted
+        std::vector<int32_t> w((size_t)n);
+        Rng r(seed, 0);
+        for (int64_t i = 0; i < n; ++i) w[(size_t)i] = wmin + (int32_t)r.below((uint64_t)(wmax - wmin + 1));
+        dmolp_csr *g = new dmolp_csr();
+        g->nv = n;
+        g->off.assign((size_t)n + 1, 0);
+        // the candidates of i, ascending: distances up to wmax on both sides, as one or two id ranges
+        auto visit = [&](int64_t i, auto f) {
+            const int64_t lo = i - wmax, hi = i + wmax;
+            auto range = [&](int64_t a, int64_t b) {  // ids a..b (inclusive), all in [0, n)
+                for (int64_t j = a; j <= b; ++j) {
+                    if (j == i) continue;
+                    int64_t d = j > i ? j - i : i - j;
+                    if (n - d < d) d = n - d;
+                    if (d <= std::max(w[(size_t)i], w[(size_t)j])) f((int32_t)j);
+                }
+            };
+            if (lo < 0) {
+                range(0, hi);
+                range(lo + n, n - 1);
+            } else if (hi >= n) {
+                range(0, hi - n);
+                range(lo, n - 1);
+            } else {
+                range(lo, hi);
+            }
+        };
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t i = 0; i < n; ++i) {
+            int64_t c = 0;
+            visit(i, [&](int32_t) { ++c; });
+            g->off[(size_t)i + 1] = c;
+        }
+        for (int64_t i = 0; i < n; ++i) g->off[(size_t)i + 1] += g->off[(size_t)i];
+        g->col.resize((size_t)g->off[(size_t)n]);
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t i = 0; i < n; ++i) {
+            int32_t *dst = g->col.data() + g->off[(size_t)i];
+            visit(i, [&](int32_t j) { *dst++ = j; });
+        }
+        *out = g;
+        return 0;
+    } catch (const std::bad_alloc &) {
+        g_err = "band: out of host memory";
+        return 2;
+    }
+}
+
 int dmolp_csr_from_arrays(int64_t nv, int64_t narcs, const int64_t *off, const int32_t *col, dmolp_csr **out) {
     try {
         dmolp_csr *g = new dmolp_csr();

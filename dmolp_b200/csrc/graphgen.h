@@ -15,6 +15,10 @@ int dmolp_gen_rmat(int scale, int edge_factor, double a, double b, double c, uin
                    dmolp_csr **out);
 int dmolp_gen_knn(int64_t n, int dim, int knn, uint64_t seed, dmolp_csr **out);
 int dmolp_gen_ba(int64_t n, int m, uint64_t seed, dmolp_csr **out);
+/* Band graph: vertex i on a cycle of n with a reach w_i uniform in [wmin, wmax]; i ~ j when their distance on
+ * the cycle is at most max(w_i, w_j).  Dense rows: with n = 65536, wmin = 12000, wmax = 24000 it has about
+ * 2.6e9 arcs (beyond 32-bit arc offsets). */
+int dmolp_gen_band(int64_t n, int wmin, int wmax, uint64_t seed, dmolp_csr **out);
 int dmolp_csr_from_arrays(int64_t nv, int64_t narcs, const int64_t *off, const int32_t *col, dmolp_csr **out);
 int64_t dmolp_csr_nv(const dmolp_csr *g);
 int64_t dmolp_csr_narcs(const dmolp_csr *g);

@@ -104,8 +104,12 @@ __global__ void k_p1_fallback(Buffers b, int nv, int best, int cur) {
     }
 }
 
-// Selection records of the current frontier: segment = part, key = (raw degree, id).
-__global__ void k_p1_records(Buffers b, int cur, int ibits) {
+// Selection records of the current frontier: segment = part, key = (raw degree, id).  The records per part
+// are counted in shared memory first (k parts), then added with one global atomic per part and block.
+__global__ void k_p1_records(Buffers b, int cur, int ibits, int k) {
+    extern __shared__ int s_np[];  // [k]
+    for (int p = threadIdx.x; p < k; p += blockDim.x) s_np[p] = 0;
+    __syncthreads();
     const int n = b.p1cnt[0];
     const int32_t *front = b.win[cur];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -114,8 +118,11 @@ __global__ void k_p1_records(Buffers b, int cur, int ibits) {
         b.bown[i] = p;
         b.bkey[i] = ((uint64_t)(unsigned)b.rawdeg[v] << ibits) | (uint64_t)v;
         b.bsel[i] = 0;
-        atomicAdd(&b.npart[p], 1);
+        atomicAdd(&s_np[p], 1);
     }
+    __syncthreads();
+    for (int p = threadIdx.x; p < k; p += blockDim.x)
+        if (s_np[p]) atomicAdd(&b.npart[p], s_np[p]);
     if (blockIdx.x == 0 && threadIdx.x == 0) b.p1cnt[4] = n;
 }
 
@@ -257,7 +264,7 @@ void p1_fallback(dmolp_ctx *c, int best_part, int cur) {
 // One expansion round on frontier buffer `cur` (the frontier lives in win[cur], its size in p1cnt[0]).
 void p1_round(dmolp_ctx *c, int k, int theta, int cur) {
     const int grid = grid_for(c);
-    k_p1_records<<<grid, kBlock, 0, c->stream>>>(c->b, cur, c->ibits);
+    k_p1_records<<<grid, kBlock, (size_t)k * sizeof(int), c->stream>>>(c->b, cur, c->ibits, k);
     k_p1_need<<<1, 256, 0, c->stream>>>(c->b, k, theta);
     c->launches += 2;
     select_smallest(c, c->b.bown, c->b.bkey, &c->b.p1cnt[4], k, c->rbits + c->ibits, c->b.bsel, nullptr);

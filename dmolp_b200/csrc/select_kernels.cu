@@ -521,16 +521,17 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(SelArgs a) {
 //   0. every block finds, per label, the superbin where the running count in the label's order reaches
 //      need_p; records of the superbins before it are taken, the rest of that superbin is partial;
 //   1. each warp walks its own contiguous range of record slots in order: taken records go to the window;
-//      records of a partial superbin of degree < 2048 go to the warp's list (in slot order) and into the
-//      block's fine-bin counts (stored per block in dcntb, summed into dfine); those of degree >= 2048 to
-//      their label's segment of a tail list (segments sized by the superbin counts) and into dfine;
+//      records of a partial superbin of degree < 2048 go to the warp's list (label and key, in slot order)
+//      and into the block's fine-bin counts (stored per block in dcntb, summed into dfine); the keys of those
+//      of degree >= 2048 to their label's segment of a tail list (segments sized by the superbin counts) and
+//      into dfine;
 //   -- grid barrier --
 //   2. every block finds, per label, the fine bin of the partial superbin where the count reaches the rest
 //      of the need.  Below degree 2048 a fine bin is a single degree, and record slots hold the vertices of
 //      one degree in ascending id order (slots follow the degree classes, ids ascending inside a class), so
 //      a record of the partial fine bin is taken when fewer than the rest of the need precede it: in the
 //      blocks before this one (dcntb), in the warps before this one, in its warp's list before it.  Above,
-//      block p ranks label p's tail records of the partial fine bin by their keys (degree, then id).
+//      block p sorts label p's tail keys of the partial fine bin (degree, then id) and takes the first ones.
 // ------------------------------------------------------------------------------------------------------
 constexpr int kDsThreads = 1024;
 constexpr int kDsWarps = kDsThreads / 32;
@@ -541,8 +542,9 @@ struct DegSelArgs {
     const int32_t *seg;        // bown: label of a boundary record, -1 for an empty slot
     const uint64_t *key;       // bkey: (dk << ibits) | v
     const int *n_dev;          // record slots
-    int32_t *lists;            // the warps' lists of partial-superbin records below degree 2048 (active[0])
-    int32_t *tail;             // partial-superbin records of degree >= 2048, one segment per label (active[1])
+    int32_t *lists;            // the warps' lists of partial-superbin records below degree 2048: labels ...
+    uint64_t *lkeys;           // ... and keys (the same positions)
+    uint64_t *tail;            // keys of partial-superbin records of degree >= 2048, one segment per label
     int *tcnt, *tcnt_next;     // [nseg] tail records per label (this iteration / the next one's, cleared here)
     unsigned int *dsup;        // [nseg * kDsBins] from the boundary test; cleared here after the barrier
     unsigned int *dfine;       // [nseg * kDsFine] fine counts of this iteration's partial superbins
@@ -688,7 +690,8 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
     const int my_n = max(0, min(n0, lo + cap) - lo);
     const int wcap = (my_n + kDsWarps - 1) / kDsWarps;
     const int wlo = lo + min(my_n, wid * wcap), whi = lo + min(my_n, (wid + 1) * wcap);
-    int32_t *wlist = a.lists + wlo;  // at most whi - wlo entries
+    int32_t *wlist = a.lists + wlo;  // at most whi - wlo entries: label, and the key in lkeys
+    uint64_t *wkey = a.lkeys + wlo;
     int wl = 0;                      // the warp's list length (warp-uniform)
     const int ibits = a.sp.ibits, maxdeg = a.sp.maxdeg;
     const uint64_t vmask = (1ull << ibits) - 1;
@@ -728,24 +731,28 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         }
 #pragma unroll
         for (int u = 0; u < kDsU; ++u) {
-            // fine counts, one shared atomic per (label, fine bin) group of the warp; a partial superbin of
-            // one degree has a single fine bin, so its group is also the warp's count of the label's ties
-            const unsigned mg = __match_any_sync(DMOLP_FULL_MASK, fb[u] >= 0 ? fb[u] : -1 - lane);
+            // fine counts; a partial superbin of one degree has a single fine bin, so its records are also
+            // counted per warp (the ties' ranks need no second walk of the list)
             const bool coarse = part[u] && s_kind[p[u]] == 3;
-            if (part[u] && lane == __ffs(mg) - 1) {
-                atomicAdd(&s_f[fb[u]], (unsigned)__popc(mg));
-                if (s_kind[p[u]] == 1) s_wc[wid * nseg + p[u]] += __popc(mg);
+            if (part[u]) {
+                atomicAdd(&s_f[fb[u]], 1u);
+                if (s_kind[p[u]] == 1) atomicAdd(&s_wc[wid * nseg + p[u]], 1);
             }
             // records below degree 2048 to the warp's list, in slot order; coarse ones to their label's
             // tail segment (one global atomic per label group of the warp)
             const unsigned mp = __ballot_sync(DMOLP_FULL_MASK, part[u] && !coarse);
-            if (part[u] && !coarse) wlist[wl + __popc(mp & below)] = r[u];
+            if (part[u] && !coarse) {
+                wlist[wl + __popc(mp & below)] = p[u];
+                wkey[wl + __popc(mp & below)] = key[u];
+            }
             wl += __popc(mp);
-            const unsigned mc = __match_any_sync(DMOLP_FULL_MASK, coarse ? p[u] : -1 - lane);
-            int q = 0;
-            if (coarse && lane == __ffs(mc) - 1) q = atomicAdd(&a.tcnt[p[u]], __popc(mc));
-            q = __shfl_sync(DMOLP_FULL_MASK, q, coarse ? __ffs(mc) - 1 : lane);
-            if (coarse) a.tail[s_toff[p[u]] + q + __popc(mc & below)] = r[u];
+            if (__any_sync(DMOLP_FULL_MASK, coarse)) {
+                const unsigned mc = __match_any_sync(DMOLP_FULL_MASK, coarse ? p[u] : -1 - lane);
+                int q = 0;
+                if (coarse && lane == __ffs(mc) - 1) q = atomicAdd(&a.tcnt[p[u]], __popc(mc));
+                q = __shfl_sync(DMOLP_FULL_MASK, q, coarse ? __ffs(mc) - 1 : lane);
+                if (coarse) a.tail[s_toff[p[u]] + q + __popc(mc & below)] = key[u];
+            }
         }
         emit_window<kDsU>(a.sp, take, key, p, vmask, te, ws, w_stage, w_scnt);  // all lanes
     }
@@ -802,9 +809,8 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         fo = -1;
         tie = false;
         if (i < wl) {
-            const int r = wlist[i];
-            p = a.seg[r];
-            key = a.key[r];
+            p = wlist[i];
+            key = wkey[i];
             int o;
             bins_of(key, p, o, fo);
             tie = fo == s_fpart[p];
@@ -847,21 +853,20 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
     for (int p = blockIdx.x; p < nseg; p += gridDim.x) {
         if (s_kind[p] != 3) continue;  // block-uniform
         const int nt = __ldcg(a.tcnt + p);
-        const int32_t *seg_tail = a.tail + s_toff[p];
+        const uint64_t *seg_tail = a.tail + s_toff[p];
         const int ftake = s_ftake[p], fpart = s_fpart[p], frem = s_frem[p];
-        __syncthreads();  // s_ntie and the shared tie arrays are free
+        __syncthreads();  // s_ntie and the shared tie keys are free
         if (threadIdx.x == 0) s_ntie = 0;
         __syncthreads();
         // the segment in chunks: records of fine bins before the partial one are taken, those of the partial
-        // fine bin are collected for ranking
+        // fine bin are collected
         for (int i0 = 0; i0 < nt; i0 += blockDim.x) {
             const int i = i0 + (int)threadIdx.x;
             bool take = false;
             uint64_t key = 0;
             int pp = p;
             if (i < nt) {
-                const int r = __ldcg(seg_tail + i);
-                key = a.key[r];
+                key = __ldcg(seg_tail + i);
                 int o, fo;
                 bins_of(key, p, o, fo);
                 if (fo < ftake) {
@@ -875,25 +880,47 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         }
         __syncthreads();
         const int m = s_ntie;
-        const int rounds = m <= kDsTieCap ? m : nt;  // ranked in shared memory, or from the segment
-        for (int i0 = 0; i0 < rounds; i0 += blockDim.x) {
-            const int i = i0 + (int)threadIdx.x;
-            bool take = false;
-            uint64_t key = 0;
-            int pp = p;
-            if (i < rounds) {
-                int rank = 0;
-                if (m <= kDsTieCap) {
-                    key = s_tkey[i];
-                    for (int j = 0; j < m; ++j) rank += s_tkey[j] < key;
-                    take = rank < frem;
-                } else {
-                    key = a.key[__ldcg(seg_tail + i)];
+        if (m <= kDsTieCap) {
+            // the ties sorted by key (bitonic, padded to a power of two): the first frem are taken
+            int n2 = 1;
+            while (n2 < m) n2 <<= 1;
+            for (int i = m + (int)threadIdx.x; i < n2; i += blockDim.x) s_tkey[i] = ~0ull;
+            for (int size = 2; size <= n2; size <<= 1) {
+                for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                    __syncthreads();
+                    for (int i = threadIdx.x; i < (n2 >> 1); i += blockDim.x) {
+                        const int lo = 2 * stride * (i / stride) + (i % stride), hi = lo + stride;
+                        const uint64_t x = s_tkey[lo], y = s_tkey[hi];
+                        if ((x > y) == ((lo & size) == 0)) {
+                            s_tkey[lo] = y;
+                            s_tkey[hi] = x;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            const int nt2 = frem < m ? frem : m;
+            for (int i0 = 0; i0 < nt2; i0 += blockDim.x) {
+                const int i = i0 + (int)threadIdx.x;
+                bool take = i < nt2;
+                uint64_t key = take ? s_tkey[i] : 0;
+                int pp = p;
+                emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
+            }
+        } else {  // more ties than the shared keys hold: each ranked against the segment in global memory
+            for (int i0 = 0; i0 < nt; i0 += blockDim.x) {
+                const int i = i0 + (int)threadIdx.x;
+                bool take = false;
+                uint64_t key = 0;
+                int pp = p;
+                if (i < nt) {
+                    key = __ldcg(seg_tail + i);
                     int o, fo;
                     bins_of(key, p, o, fo);
                     if (fo == fpart) {
+                        int rank = 0;
                         for (int j = 0; j < nt; ++j) {
-                            const uint64_t kj = a.key[__ldcg(seg_tail + j)];
+                            const uint64_t kj = __ldcg(seg_tail + j);
                             int oj, foj;
                             bins_of(kj, p, oj, foj);
                             rank += foj == fpart && kj < key;
@@ -901,8 +928,8 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
                         take = rank < frem;
                     }
                 }
+                emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
             }
-            emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
         }
     }
     stage_flush(a.sp, w_stage, w_scnt);
@@ -962,7 +989,8 @@ bool select_window_deg(dmolp_ctx *c, int nseg, const SplitArgs &split, const int
     a.key = c->b.bkey;
     a.n_dev = &c->b.cnt->npos;
     a.lists = c->b.active[0];
-    a.tail = c->b.active[1];
+    a.lkeys = c->b.dlkey;
+    a.tail = c->b.dtkey;
     a.tcnt = c->b.dtcnt + (split.t & 1) * kDegSelMaxK;
     a.tcnt_next = c->b.dtcnt + ((split.t + 1) & 1) * kDegSelMaxK;
     a.dsup = c->b.dsup;

@@ -83,6 +83,15 @@ def barabasi_albert(n: int, m: int, seed: int = 1) -> Graph:
     return g
 
 
+def band(n: int, wmin: int, wmax: int, seed: int = 1) -> Graph:
+    """Band graph on a cycle: i ~ j when their cycle distance is at most max(w_i, w_j), w uniform in
+    [wmin, wmax] (dense rows; large parameters give more than 2^31 arcs)."""
+    g = _call(_native.gen().dmolp_gen_band, n, wmin, wmax, seed)
+    g.name = f"band-n{n}-w{wmin}-{wmax}-seed{seed}"
+    g.meta = dict(kind="band", n=n, wmin=wmin, wmax=wmax, seed=seed)
+    return g
+
+
 def from_edges(n: int, edges) -> Graph:
     """Undirected graph from an edge list (pairs); symmetrised, de-duplicated, self-loops dropped."""
     e = np.asarray(list(edges), dtype=np.int64).reshape(-1, 2)

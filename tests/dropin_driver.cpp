@@ -11,6 +11,7 @@
 // subgraph and chunk construction).
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <unordered_map>
@@ -161,9 +162,13 @@ int main(int argc, char **argv) {
     for (int i = 0; i < r1.change_count; ++i)
         if (l4[r1.updated_nodes[i]] != r1.updated_labels[i]) same4 = 0;
 #endif
-    printf("{\"what\":\"single_step\",\"window\":%zu,\"window_hash\":\"%016llx\",\"changes\":[%d,%d,%d],"
+    // the window as a set (the reference returns it grouped by an unordered_map over labels, this library in
+    // ascending ids; every consumer treats it as a set)
+    std::vector<int> ws = w;
+    std::sort(ws.begin(), ws.end());
+    printf("{\"what\":\"single_step\",\"window\":%zu,\"window_set_hash\":\"%016llx\",\"changes\":[%d,%d,%d],"
            "\"same_nodes\":%d,\"safe_consistent\":%d}\n",
-           w.size(), (unsigned long long)fnv(w), r1.change_count, r2.change_count, r3.change_count,
+           ws.size(), (unsigned long long)fnv(ws), r1.change_count, r2.change_count, r3.change_count,
            (int)(r1.updated_nodes == r2.updated_nodes && r1.updated_labels == r2.updated_labels), same4);
 
     // the same step with penalties, through the chunked paths: the chunked entry point with room for one

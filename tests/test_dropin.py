@@ -186,7 +186,7 @@ def test_device_entry_points_equal_the_reference_functions():
     for what in ("host", "subgraph", "lower_phase1", "phase1", "phase2", "step_unified", "step_chunked",
                  "step_streaming_chunked", "step_streaming", "chunks", "random_phase1", "random_phase2"):
         assert ours[what] == ref[what], what
-    for key in ("window", "window_hash", "changes"):
+    for key in ("window", "window_set_hash", "changes"):
         assert ours["single_step"][key] == ref["single_step"][key], key
     # the chunked paths drop arcs that cross chunks: they differ from the whole subgraph's step here
     assert ours["step_chunked"] != ours["step_unified"]
