@@ -207,8 +207,6 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
         p._check(p.lib.dmolp_labels_restore(p.ctx))
         return p.phase2(w["k"], mode="fixed", iterations=w["iters"], records=False)
 
-    # profiling events live inside the captured graphs: capture them during warm-up, not in the timed region
-    p.lib.dmolp_set_profiling(p.ctx, 1)
     sampler = ClockSampler(local_rank)
     if not args.quick:
         sampler.start()
@@ -217,7 +215,6 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
             step()
     for _ in range(max(1, args.warmup)):
         step()
-    p.lib.dmolp_set_profiling(p.ctx, 1)  # reset the accumulated kernel times
     launches0 = p.kernel_launches()
     if dist:
         dist.barrier()
@@ -234,9 +231,24 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    clocks = sampler.stop() if not args.quick else None
     launches = p.kernel_launches() - launches0
     elapsed = e0.elapsed_time(e1) / 1e3
+    final_labels = p.labels()
+    # Per-kernel device times for the roofline: the same K steps again, with CUDA events recorded around the
+    # profiled kernels inside the captured graphs (a graph of their own, captured in one untimed step).  The
+    # events lengthen a run by ~1 ms, so the headline steps above run without them.
+    p.lib.dmolp_set_profiling(p.ctx, 1)
+    step()
+    p.lib.dmolp_set_profiling(p.ctx, 1)  # reset the accumulated kernel times
+    pe0 = torch.cuda.Event(enable_timing=True)
+    pe1 = torch.cuda.Event(enable_timing=True)
+    pe0.record(stream)
+    for _ in range(args.steps):
+        step()
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if not args.quick else None
+    prof_elapsed = pe0.elapsed_time(pe1) / 1e3
     prof = {}
     for kid, name in ((0, "boundary_test"), (1, "lp_decide"), (2, "window_mark"), (3, "cut_update"),
                       (4, "window_select")):
@@ -246,7 +258,6 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
         p.lib.dmolp_kernel_profile(p.ctx, kid, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(by))
         prof[name] = dict(ms=ms.value, launches=n.value, bytes=by.value)
     p.lib.dmolp_set_profiling(p.ctx, 0)
-    final_labels = p.labels()
     parity = golden_parity(w, labels1, final_labels, last)
 
     rec_step = None
@@ -293,6 +304,25 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
     assert np.array_equal(out_h.numpy(), final_labels), "end-to-end labels differ from the resident run"
     h2d = g.offsets.nbytes + g.indices.nbytes + g.raw_deg().nbytes + labels1.nbytes
     d2h = labels1.nbytes
+    # where an end-to-end step's time goes (one more step, untimed above; each call returns synchronised)
+    parts = {}
+    t = time.perf_counter()
+    p._check(p.lib.dmolp_graph_upload(p.ctx, g.num_vertices, g.num_arcs, ctypes.c_void_p(off_h.data_ptr()),
+                                      ctypes.c_void_p(col_h.data_ptr()), ctypes.c_void_p(raw_h.data_ptr())))
+    parts["upload_ms"] = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    p._check(p.lib.dmolp_labels_set(p.ctx, ctypes.c_void_p(lab_h.data_ptr())))
+    torch.cuda.synchronize()
+    parts["labels_set_ms"] = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    p.symmetric()
+    parts["symmetry_test_ms"] = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    p.phase2(w["k"], mode="fixed", iterations=w["iters"], records=False)
+    parts["phase2_first_run_ms"] = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    p._check(p.lib.dmolp_labels_get(p.ctx, ctypes.c_void_p(out_h.data_ptr())))
+    parts["labels_get_ms"] = (time.perf_counter() - t) * 1e3
 
     t_max, e2e_max = max_over_ranks(dist, [elapsed, e2e_elapsed])
     p.close()
@@ -328,12 +358,14 @@ def run_ours(args, w, rank: int, world: int, local_rank: int, dist) -> dict | No
                    "parallelism": f"replicas x{world}",
                    "parity": None if parity is None else parity["ok"], "parity_detail": parity},
         "e2e": {"value": e2e_te * world / e2e_max, "unit": "TE/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "wall_s": e2e_wall, "steps": e2e_steps},
+                "d2h_bytes_per_step": int(d2h), "wall_s": e2e_wall, "steps": e2e_steps, "parts": parts},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                      "traffic": traffic_from_profiles(dom, args.workload),
                      "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": per_launch_s * 1e3,
+                     "timing": "CUDA events around each launch, in K further steps of the same workload "
+                               "(%.3f ms per step with the events)" % (prof_elapsed / args.steps * 1e3),
                      "kernels": prof},
         "clocks": clocks,
     }

@@ -26,6 +26,8 @@ EXPORTS = [
     "dmolp_host_graph_indices", "dmolp_host_graph_raw_degree", "dmolp_host_graph_free", "dmolp_stream",
     "dmolp_labels_save", "dmolp_labels_restore", "dmolp_set_profiling", "dmolp_kernel_profile",
     "dmolp_set_wait_limit",
+    "dmolp_set_symmetry_test",
+    "dmolp_graph_symmetric",
     "dmolp_find_seeds", "dmolp_expand_partitions", "dmolp_current_device", "dmolp_device_code_version", "dmolp_metrics_noalloc",
     "dmolp_batch_create", "dmolp_batch_destroy", "dmolp_batch_upload", "dmolp_batch_labels_set",
     "dmolp_batch_labels_get", "dmolp_batch_device_labels", "dmolp_batch_stream", "dmolp_batch_lp_run",
@@ -130,6 +132,8 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_labels_restore.argtypes = [vp]
     lib.dmolp_set_profiling.argtypes = [vp, c_int]
     lib.dmolp_set_wait_limit.argtypes = [vp, ctypes.c_uint32]
+    lib.dmolp_set_symmetry_test.argtypes = [vp, ctypes.c_int]
+    lib.dmolp_graph_symmetric.argtypes = [vp, POINTER(c_int)]
     lib.dmolp_find_seeds.argtypes = [vp, c_int, c_int32, vp, c_int64, vp, POINTER(c_int32)]
     lib.dmolp_expand_partitions.argtypes = [vp, c_int, c_int, vp, c_int32, POINTER(c_int32)]
     lib.dmolp_metrics_noalloc.argtypes = [c_int, c_int64, vp, vp, vp, c_int, vp, POINTER(c_int64), vp, vp]

@@ -153,7 +153,7 @@ struct Buffers {
     int *p1cnt = nullptr;                // [8] phase-1 counters
     unsigned long long *p1te = nullptr;  // [1]
     int *flag = nullptr;                 // [1] scratch flag (symmetry check)
-    unsigned long long *symcnt = nullptr;  // [2] arc counts of the symmetry check
+    unsigned long long *symcnt = nullptr;  // [2] arc counts / multiset sums of the symmetry test
 };
 
 }  // namespace dmolp
@@ -170,6 +170,8 @@ struct dmolp_ctx {
     bool symmetric = false;               // every arc (u,v) has its reverse: incremental statistics apply
     bool symmetry_known = false;          // `symmetric` has been tested for the resident graph
     bool rows_sorted = false;             // every row strictly increasing (precondition of the test)
+    bool symmetry_exact = false;          // test by reverse-arc searches instead of the multiset sums
+    unsigned long long sym_key = 0;       // key of the multiset symmetry sum, drawn per context
     bool has_graph = false;
     bool hot_ready = false;               // colh / hrank / hotid built for the resident graph
     bool counts_kept = false;             // the current LP run decides from vcnt / hh (no label gathers)

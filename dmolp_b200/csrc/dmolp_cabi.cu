@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -425,7 +426,9 @@ int lp_hot_prepare(dmolp_ctx *c) {
 
 // Whether every arc has its reverse, tested on the device the first time the LP loop needs it (then the
 // loop may update cut and balance from the movers alone); graphs whose rows are not strictly increasing
-// always take the full statistics pass.
+// always take the full statistics pass.  By default one streaming pass forms the keyed multiset sum (zero
+// for every symmetric graph; zero for an asymmetric one with probability about 2^-64); with
+// dmolp_set_symmetry_test(ctx, 1) every reverse arc is looked up instead.
 int ensure_symmetry(dmolp_ctx *c) {
     if (c->symmetry_known) return DMOLP_OK;
     Buffers &b = c->b;
@@ -433,14 +436,15 @@ int ensure_symmetry(dmolp_ctx *c) {
     if (c->rows_sorted && c->nv > 0) {
         DMOLP_CUDA(cudaMemsetAsync(b.flag, 0, sizeof(int), c->stream));
         DMOLP_CUDA(cudaMemsetAsync(b.symcnt, 0, 2 * sizeof(unsigned long long), c->stream));
-        lp_check_symmetric(c, b.symcnt);
+        if (c->symmetry_exact) lp_check_symmetric(c, b.symcnt);
+        else lp_symmetry_hash(c, b.symcnt, c->sym_key);
         int missing = 1;
         unsigned long long hc[2] = {0, 1};
         DMOLP_CUDA(cudaMemcpyAsync(&missing, b.flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         DMOLP_CUDA(cudaMemcpyAsync(hc, b.symcnt, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
         int s1 = sync(c);
         if (s1) return s1;
-        c->symmetric = missing == 0 && hc[0] == hc[1];
+        c->symmetric = c->symmetry_exact ? (missing == 0 && hc[0] == hc[1]) : hc[0] == 0;
     }
     c->symmetry_known = true;
     return DMOLP_OK;
@@ -557,6 +561,10 @@ int dmolp_create(int device, dmolp_ctx **out) {
     DMOLP_CUDA(cudaSetDevice(device));
     dmolp_ctx *c = new dmolp_ctx();
     c->device = device;
+    {  // key of the multiset symmetry sum: unknown outside the process, so no input is built to defeat it
+        std::random_device rd;
+        c->sym_key = ((unsigned long long)rd() << 32) ^ rd();
+    }
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
@@ -594,100 +602,44 @@ int dmolp_graph_upload(dmolp_ctx *c, int64_t nv, int64_t narcs, const int64_t *o
         return fail(DMOLP_ERR_ARG, "bad graph sizes or null arrays");
     if (off[0] != 0 || off[nv] != narcs) return fail(DMOLP_ERR_ARG, "offsets must start at 0 and end at narcs");
     DMOLP_CUDA(cudaSetDevice(c->device));
-    // The arcs go to a device staging buffer first (from pinned memory the copy overlaps the validation
-    // below) and reach the graph only once the validation passed.
-    int32_t *stage = nullptr;
-    if (narcs) {
-        std::string err;
-        stage = (int32_t *)c->scratch.get(ingest::kTok, (size_t)narcs * sizeof(int32_t), err);
-        if (!stage) return fail(DMOLP_ERR_NOMEM, err);
-        DMOLP_CUDA(cudaMemcpyAsync(stage, col, (size_t)narcs * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    // The arrays go as they are to device staging buffers (from pinned memory at the link's rate) and are
+    // checked there: every row bound, every id, whether rows are strictly increasing, the degree classes.
+    // They reach the graph only once the check passed, so a rejected upload leaves the previous graph.
+    std::string err;
+    int64_t *s_off = (int64_t *)c->scratch.get(ingest::kEndTok, (size_t)(nv + 1) * sizeof(int64_t), err);
+    int32_t *s_col = narcs ? (int32_t *)c->scratch.get(ingest::kTok, (size_t)narcs * sizeof(int32_t), err) : nullptr;
+    int32_t *s_raw = raw && nv ? (int32_t *)c->scratch.get(ingest::kBadrow, (size_t)nv * sizeof(int32_t), err) : nullptr;
+    if (!s_off || (narcs && !s_col) || (raw && nv && !s_raw)) return fail(DMOLP_ERR_NOMEM, err);
+    DMOLP_CUDA(cudaMemcpyAsync(s_off, off, (size_t)(nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+    if (s_raw) DMOLP_CUDA(cudaMemcpyAsync(s_raw, raw, (size_t)nv * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    if (narcs)
+        DMOLP_CUDA(cudaMemcpyAsync(s_col, col, (size_t)narcs * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    ingest::CsrInfo ci;
+    if (ingest::check_csr(c->stream, s_off, s_col, s_raw, nv, narcs, c->scratch, ci, err)) {
+        cudaGetLastError();
+        return fail(DMOLP_ERR_CUDA, err);
     }
-    // Validate on the host: every device access below is then in bounds.  One parallel pass over the rows
-    // checks the degrees, the ids and whether every row is strictly increasing (the symmetry test's
-    // precondition), and counts each thread's vertices per degree class.
-    int bad = 0, unsorted = 0;
-    int64_t maxdeg = 0, maxraw = 0;
-    const int nth = std::max(1, omp_get_max_threads());
-    std::vector<int64_t> ccnt((size_t)nth * 3, 0);
-#pragma omp parallel num_threads(nth) reduction(| : bad, unsorted) reduction(max : maxdeg, maxraw)
-    {
-        const int th = omp_get_thread_num();
-        const int64_t v0 = nv * th / nth, v1 = nv * (th + 1) / nth;  // contiguous ranges: classes stay in id order
-        int64_t cc[3] = {0, 0, 0};
-        for (int64_t v = v0; v < v1; ++v) {
-            const int64_t s0 = off[v], d = off[v + 1] - s0;
-            if (d < 0 || d > 0x7fffffff || s0 < 0 || off[v + 1] > narcs) {  // the row is read only when in bounds
-                bad |= 1;
-                continue;
-            }
-            maxdeg = std::max(maxdeg, d);
-            if (raw) {
-                if (raw[v] < 0) bad |= 4;
-                maxraw = std::max(maxraw, (int64_t)raw[v]);
-            }
-            if (d == 0) continue;
-            cc[d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2)]++;
-            const int32_t *r = col + s0;
-            uint32_t prev = (uint32_t)r[0];
-            if (prev >= (uint64_t)nv) bad |= 2;
-            for (int64_t j = 1; j < d; ++j) {
-                const uint32_t x = (uint32_t)r[j];
-                if (x >= (uint64_t)nv) bad |= 2;
-                if ((int32_t)x <= (int32_t)prev) unsorted = 1;
-                prev = x;
-            }
-        }
-        for (int i = 0; i < 3; ++i) ccnt[(size_t)th * 3 + i] = cc[i];
-    }
-    if (!raw) maxraw = maxdeg;
-    if (bad) cudaStreamSynchronize(c->stream);  // the staging copy still reads the caller's arcs
-    if (bad & 1) return fail(DMOLP_ERR_ARG, "offsets are not non-decreasing");
-    if (bad & 2) return fail(DMOLP_ERR_ARG, "a neighbour id is outside [0, nv)");
-    if (bad & 4) return fail(DMOLP_ERR_ARG, "negative raw degree");
-
-    // degree classes (isolated vertices belong to none: they are never on a boundary), ascending ids inside
-    // a class: each thread fills its range's share at the prefix of the counts before it
-    std::vector<int32_t> bl[3];
-    std::vector<int64_t> cpos((size_t)nth * 3);
-    for (int i = 0; i < 3; ++i) {
-        int64_t acc = 0;
-        for (int th = 0; th < nth; ++th) {
-            cpos[(size_t)th * 3 + i] = acc;
-            acc += ccnt[(size_t)th * 3 + i];
-        }
-        bl[i].resize((size_t)acc);
-    }
-#pragma omp parallel num_threads(nth)
-    {
-        const int th = omp_get_thread_num();
-        const int64_t v0 = nv * th / nth, v1 = nv * (th + 1) / nth;
-        int64_t pos[3] = {cpos[(size_t)th * 3], cpos[(size_t)th * 3 + 1], cpos[(size_t)th * 3 + 2]};
-        for (int64_t v = v0; v < v1; ++v) {
-            const int64_t d = off[v + 1] - off[v];
-            if (d == 0) continue;
-            const int c = d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2);
-            bl[c][(size_t)pos[c]++] = (int32_t)v;
-        }
-    }
-    const int64_t nb[3] = {(int64_t)bl[0].size(), (int64_t)bl[1].size(), (int64_t)bl[2].size()};
-    int st = graph_alloc(c, nv, narcs, maxdeg, maxraw, nb);
+    c->launches += ci.launches;
+    if (ci.bad & 1) return fail(DMOLP_ERR_ARG, "offsets are not non-decreasing");
+    if (ci.bad & 2) return fail(DMOLP_ERR_ARG, "a neighbour id is outside [0, nv)");
+    if (ci.bad & 4) return fail(DMOLP_ERR_ARG, "negative raw degree");
+    const int64_t maxraw = raw ? ci.maxraw : ci.maxdeg;
+    int st = graph_alloc(c, nv, narcs, ci.maxdeg, maxraw, ci.nb);
     if (st) return st;
     Buffers &b = c->b;
-    DMOLP_CUDA(cudaMemcpyAsync(b.off, off, (size_t)(nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+    DMOLP_CUDA(cudaMemcpyAsync(b.off, s_off, (size_t)(nv + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, c->stream));
     if (narcs)
-        DMOLP_CUDA(cudaMemcpyAsync(b.col, stage, (size_t)narcs * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
-    c->h_rawdeg.resize(nv);
-#pragma omp parallel for num_threads(nth) schedule(static)
-    for (int64_t v = 0; v < nv; ++v) c->h_rawdeg[v] = raw ? raw[v] : (int32_t)(off[v + 1] - off[v]);
-    c->h_rawdeg_valid = true;
-    DMOLP_CUDA(cudaMemcpyAsync(b.rawdeg, c->h_rawdeg.data(), (size_t)nv * sizeof(int32_t), cudaMemcpyHostToDevice,
-                               c->stream));
-    for (int i = 0; i < 3; ++i)
-        if (!bl[i].empty())
-            DMOLP_CUDA(cudaMemcpyAsync(b.bucket[i], bl[i].data(), bl[i].size() * sizeof(int32_t),
-                                       cudaMemcpyHostToDevice, c->stream));
-    st = graph_finish(c, !unsorted);  // ends with a stream sync: the staging copy is done
+        DMOLP_CUDA(cudaMemcpyAsync(b.col, s_col, (size_t)narcs * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+    // raw degrees from the caller's array, or the CSR degrees; the host mirror the phase-1 hub sort reads is
+    // fetched when phase 1 first needs it
+    if (s_raw) DMOLP_CUDA(cudaMemcpyAsync(b.rawdeg, s_raw, (size_t)nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+    else lp_degrees(c, b.off, nv, b.rawdeg);
+    c->h_rawdeg.clear();
+    c->h_rawdeg_valid = false;
+    int32_t *const bucket[3] = {b.bucket[0], b.bucket[1], b.bucket[2]};
+    if (ingest::csr_classes(c->stream, b.off, nv, ci, bucket, err)) return fail(DMOLP_ERR_CUDA, err);
+    if (nv > 0) c->launches++;
+    st = graph_finish(c, ci.sorted != 0);  // ends with a stream sync: the staging copies are done
     c->scratch.trim(ingest::kKeepScratch);
     return st;
 }
@@ -906,6 +858,26 @@ int dmolp_set_wait_limit(dmolp_ctx *c, uint32_t polls) {
     if (v != c->wait_polls) {
         drop_graphs(c);  // captured launches carry the limit as an argument
         c->wait_polls = v;
+    }
+    return DMOLP_OK;
+}
+
+int dmolp_graph_symmetric(dmolp_ctx *c, int *symmetric) {
+    if (!c || !symmetric) return fail(DMOLP_ERR_ARG, "null argument");
+    if (!c->has_graph) return fail(DMOLP_ERR_STATE, "no graph uploaded");
+    DMOLP_CUDA(cudaSetDevice(c->device));
+    const int st = ensure_symmetry(c);
+    if (st) return st;
+    *symmetric = c->symmetric ? 1 : 0;
+    return DMOLP_OK;
+}
+
+int dmolp_set_symmetry_test(dmolp_ctx *c, int exact) {
+    if (!c) return fail(DMOLP_ERR_ARG, "null context");
+    if ((exact != 0) != c->symmetry_exact) {
+        c->symmetry_exact = exact != 0;
+        c->symmetry_known = false;  // the resident graph is tested again, the chosen way, when next needed
+        drop_graphs(c);
     }
     return DMOLP_OK;
 }
@@ -1261,9 +1233,10 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     }
     if (c->profiling) {
         // Algorithmic bytes per launch of the design (ids and labels are 4 B, offsets 8 B):
-        //  bnd    : record slot (ball id, stamp, selection flag) of every vertex with arcs, offsets +
-        //           boundary count of each candidate, id + window stamp per arc of a pull-mode walk, own
-        //           label per boundary record
+        //  bnd    : per record slot (every vertex with arcs) its id, own label, boundary count and the record
+        //           label written, from iteration 2 also its stamp (push) or window stamp (pull) and, on
+        //           graphs with hubs, its hub-window count; offsets per candidate; the key written per
+        //           boundary record; id + window stamp per arc of a pull-mode walk
         //  decide : list id + offsets + own label per selected vertex, id + label per arc, 8 B per mover;
         //           with kept counts 64 B of counts per selected vertex and no arcs
         //  mark   : list id + offsets per window vertex, id read + stamp write per arc of a walked row
@@ -1282,7 +1255,8 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
                 const double ncand = t == 1 ? nbk : (double)d.candidates;
                 double bytes = 0;
                 if (kind == 0)
-                bytes = (t > 1 ? 8.0 : 4.0) * nbk + 5.0 * nbk + 20.0 * ncand + 8.0 * (double)d.arcs_bnd + 8.0 * d.boundary;
+                    bytes = (16.0 + (t > 1 ? 4.0 : 0.0) + (t > 1 && c->nb[2] > 0 ? 4.0 : 0.0)) * nbk + 16.0 * ncand +
+                            8.0 * d.boundary + 8.0 * (double)d.arcs_bnd;
                 else if (kind == 1)
                     bytes = (c->counts_kept ? 88.0 : 24.0) * d.window + 8.0 * (double)d.arcs_dec + 8.0 * d.changes;
                 else if (kind == 2) bytes = (t > 1 ? 20.0 * recs[t - 2].window : 0.0) + 8.0 * (double)d.arcs_mark;

@@ -55,7 +55,7 @@ int caller_device() {
 
 void require_single_rank(int mpi_size, const char *fn) {
     if (mpi_size != 1)
-        throw std::runtime_error(std::string(fn) + ": this build runs one process on one GPU (mpi_size must be 1)");
+        throw std::runtime_error(std::string(fn) + ": this library runs one process on one GPU (mpi_size must be 1)");
 }
 
 // A context with a resident graph, remembered by the identity of the host arrays it was uploaded from.

@@ -587,6 +587,130 @@ __global__ void k_keep_compact(const uint32_t *__restrict__ tok, int64_t ntok, c
         if (kept(tok, t)) col[keptpos[t]] = (int)(tok[t] & kVal);
 }
 
+// ---- a binary CSR copied to the device as given (dmolp_graph_upload) ----
+
+struct CsrScal {
+    unsigned long long maxdeg, maxraw;
+    unsigned long long violations;  // arcs not above their predecessor in the same row
+    int bad;                        // 1: offsets, 2: an id outside [0, nv), 4: a negative raw degree
+};
+
+// Per vertex tile (kLineTile vertices): row bounds in [0, narcs] and non-decreasing, the degree classes'
+// counts, the largest degree and raw degree, and a bit at the first arc of every non-empty row.
+__global__ void __launch_bounds__(kTxtThreads) k_csr_rows(const int64_t *__restrict__ off,
+                                                          const int32_t *__restrict__ raw, int64_t nv, int64_t narcs,
+                                                          uint32_t *__restrict__ lcnt, uint32_t *__restrict__ rowbit,
+                                                          CsrScal *sc) {
+    __shared__ uint32_t s_w[kNW];
+    uint32_t cnt3 = 0;
+    unsigned long long md = 0, mr = 0;
+    int bad = 0;
+    for (int s = 0; s < kLineSteps; ++s) {
+        const int64_t l = blockIdx.x * kLineTile + s * kTxtThreads + threadIdx.x;
+        if (l >= nv) break;
+        const int64_t a = off[l], z = off[l + 1], d = z - a;
+        if (a < 0 || d < 0 || z > narcs || d > 0x7fffffff) {
+            bad |= 1;
+        } else if (d > 0) {
+            cnt3 += 1u << (10 * (d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2)));
+            md = max(md, (unsigned long long)d);
+            atomicOr(rowbit + (a >> 5), 1u << (a & 31));
+        }
+        if (raw) {
+            const int32_t r = raw[l];
+            if (r < 0) bad |= 4;
+            else mr = max(mr, (unsigned long long)r);
+        }
+    }
+    const uint32_t c0 = block_sum(cnt3 & 1023u, s_w), c1 = block_sum((cnt3 >> 10) & 1023u, s_w),
+                   c2 = block_sum(cnt3 >> 20, s_w);
+    for (int o = 16; o > 0; o >>= 1) {
+        md = max(md, __shfl_xor_sync(DMOLP_FULL_MASK, md, o));
+        mr = max(mr, __shfl_xor_sync(DMOLP_FULL_MASK, mr, o));
+    }
+    bad = __reduce_or_sync(DMOLP_FULL_MASK, bad);
+    if ((threadIdx.x & 31) == 0) {
+        if (md) atomicMax(&sc->maxdeg, md);
+        if (mr) atomicMax(&sc->maxraw, mr);
+        if (bad) atomicOr(&sc->bad, bad);
+    }
+    if (threadIdx.x == 0) {
+        lcnt[3 * blockIdx.x] = c0;
+        lcnt[3 * blockIdx.x + 1] = c1;
+        lcnt[3 * blockIdx.x + 2] = c2;
+    }
+}
+
+// Per 4 arcs (one 16-byte load): every id in [0, nv), and every arc that does not start its row above its
+// predecessor.  The rows' bits come from k_csr_rows; after bad offsets the order test is skipped (the upload
+// fails anyway).  Whole warps iterate, so the predecessor of a lane's first arc comes from the lane below.
+__global__ void __launch_bounds__(256) k_csr_arcs(const int32_t *__restrict__ col, int64_t narcs, int64_t nv,
+                                                  const uint32_t *__restrict__ rowbit, CsrScal *sc) {
+    const int lane = threadIdx.x & 31;
+    const bool order = (((volatile CsrScal *)sc)->bad & 1) == 0;
+    const int64_t n4 = narcs >> 2;
+    const int64_t nwarp = (int64_t)gridDim.x * (blockDim.x >> 5);
+    int bad = 0;
+    unsigned long long viol = 0;
+    for (int64_t w0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; w0 < n4; w0 += nwarp * 32) {
+        const int64_t i = w0 + lane;
+        int4 q = make_int4(0, 0, 0, 0);
+        uint32_t bits = 0xfu;
+        if (i < n4) {
+            q = __ldcs(reinterpret_cast<const int4 *>(col) + i);
+            bits = (__ldg(rowbit + (i >> 3)) >> ((i & 7) * 4)) & 0xfu;
+        }
+        int prev = __shfl_up_sync(DMOLP_FULL_MASK, q.w, 1);
+        if (lane == 0) prev = i > 0 && i < n4 ? __ldg(col + 4 * i - 1) : 0;
+        if (i < n4) {
+            const int x[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                if ((uint32_t)x[t] >= (uint64_t)nv) bad = 2;
+                if (order && !((bits >> t) & 1u) && (i > 0 || t > 0) && x[t] <= (t ? x[t - 1] : prev)) ++viol;
+            }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 4) {  // the last narcs % 4 arcs
+        const int64_t j = 4 * n4 + threadIdx.x;
+        if (j < narcs) {
+            const int x = col[j];
+            if ((uint32_t)x >= (uint64_t)nv) bad = 2;
+            if (order && !((rowbit[j >> 5] >> (j & 31)) & 1u) && j > 0 && x <= col[j - 1]) ++viol;
+        }
+    }
+    bad = __reduce_or_sync(DMOLP_FULL_MASK, bad);
+    viol = __reduce_add_sync(DMOLP_FULL_MASK, (unsigned)viol);
+    if (lane == 0) {
+        if (bad) atomicOr(&sc->bad, bad);
+        if (viol) atomicAdd(&sc->violations, viol);
+    }
+}
+
+// Degree-class lists in ascending id order (isolated vertices in none), at the tile prefixes loff.
+__global__ void __launch_bounds__(kTxtThreads) k_csr_classes(const int64_t *__restrict__ off, int64_t nv,
+                                                             const int64_t *__restrict__ loff, int32_t *b0, int32_t *b1,
+                                                             int32_t *b2) {
+    __shared__ uint32_t s_w[kNW];
+    int64_t base[3] = {loff[3 * blockIdx.x], loff[3 * blockIdx.x + 1], loff[3 * blockIdx.x + 2]};
+    for (int s = 0; s < kLineSteps; ++s) {
+        const int64_t l = blockIdx.x * kLineTile + s * kTxtThreads + threadIdx.x;
+        if (blockIdx.x * kLineTile + s * kTxtThreads >= nv) break;  // uniform across the block
+        int cls = 3;
+        if (l < nv) {
+            const int64_t d = off[l + 1] - off[l];
+            cls = d == 0 ? 3 : (d <= kSmallDeg ? 0 : (d <= kLargeDeg ? 1 : 2));
+        }
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan(cls < 3 ? 1u << (10 * cls) : 0u, &tot, s_w);
+        if (cls < 3) {
+            int32_t *b = cls == 0 ? b0 : (cls == 1 ? b1 : b2);
+            b[base[cls] + ((ex >> (10 * cls)) & 1023u)] = (int32_t)l;
+        }
+        for (int c = 0; c < 3; ++c) base[c] += (tot >> (10 * c)) & 1023u;
+    }
+}
+
 // ---- host side ----
 
 template <typename T>
@@ -778,6 +902,57 @@ int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t b
         err = "a line has more than 2^31-1 tokens";
         return 1;
     }
+    return 0;
+}
+
+int check_csr(cudaStream_t st, const int64_t *off, const int32_t *col, const int32_t *raw, int64_t nv, int64_t narcs,
+              Pool &pool, CsrInfo &out, std::string &err) {
+    out = CsrInfo();
+    CsrScal *sc = nullptr;
+    if (!pool_get(pool, kScal, &sc, 1, err)) return 1;
+    ING_CUDA(cudaMemsetAsync(sc, 0, sizeof(CsrScal), st));
+    const int64_t nlt = (nv + kLineTile - 1) / kLineTile;
+    const int64_t nwords = (narcs + 31) / 32;
+    uint32_t *lcnt = nullptr, *rowbit = nullptr;
+    int64_t *loff = nullptr;
+    if (!pool_get(pool, kLcnt, &lcnt, (size_t)3 * nlt, err) || !pool_get(pool, kLoff, &loff, (size_t)3 * (nlt + 1), err) ||
+        !pool_get(pool, kKeptpos, &rowbit, (size_t)nwords, err))
+        return 1;
+    if (nwords) ING_CUDA(cudaMemsetAsync(rowbit, 0, (size_t)nwords * sizeof(uint32_t), st));
+    int64_t nb[3] = {0, 0, 0};
+    if (nlt > 0) {
+        k_csr_rows<<<(unsigned)nlt, kTxtThreads, 0, st>>>(off, raw, nv, narcs, lcnt, rowbit, sc);
+        k_scan<3><<<1, 1024, 0, st>>>(lcnt, nlt, loff);
+        out.launches += 2;
+    }
+    if (narcs > 0) {
+        k_csr_arcs<<<grid_for(narcs / 4 + 1, 256), 256, 0, st>>>(col, narcs, nv, rowbit, sc);
+        ++out.launches;
+    }
+    CsrScal h{};
+    ING_CUDA(cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, st));
+    if (nlt > 0) ING_CUDA(cudaMemcpyAsync(nb, loff + 3 * nlt, sizeof(nb), cudaMemcpyDeviceToHost, st));
+    const cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        err = std::string("upload check: ") + cudaGetErrorString(e);
+        return 1;
+    }
+    ING_CUDA(cudaGetLastError());
+    out.bad = h.bad;
+    out.sorted = h.violations == 0;
+    out.maxdeg = (int64_t)h.maxdeg;
+    out.maxraw = (int64_t)h.maxraw;
+    for (int c = 0; c < 3; ++c) out.nb[c] = nb[c];
+    out.loff = loff;
+    return 0;
+}
+
+int csr_classes(cudaStream_t st, const int64_t *off, int64_t nv, const CsrInfo &info, int32_t *const bucket[3],
+                std::string &err) {
+    const int64_t nlt = (nv + kLineTile - 1) / kLineTile;
+    if (nlt > 0)
+        k_csr_classes<<<(unsigned)nlt, kTxtThreads, 0, st>>>(off, nv, info.loff, bucket[0], bucket[1], bucket[2]);
+    ING_CUDA(cudaGetLastError());
     return 0;
 }
 

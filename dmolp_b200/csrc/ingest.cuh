@@ -73,6 +73,24 @@ struct Parsed {
 int parse(cudaStream_t st, uint8_t *d_txt, int64_t len, int64_t body0, int64_t body1, Pool &pool, Parsed &p,
           std::string &err);
 
+// A binary CSR already on the device (off[nv+1] with off[0] = 0 and off[nv] = narcs checked by the caller,
+// col[narcs], raw[nv] or null): checks every row bound and id, whether every row is strictly increasing,
+// and sizes the degree classes.  Synchronises the stream.  Returns 0 with `out` filled (out.bad nonzero:
+// the CSR is invalid), or 1 with `err` set on a CUDA failure.
+struct CsrInfo {
+    int bad = 0;                // 1: offsets out of order or out of [0, narcs], 2: an id outside [0, nv), 4: raw < 0
+    int sorted = 1;             // every row strictly increasing
+    int64_t maxdeg = 0, maxraw = 0;
+    int64_t nb[3] = {0, 0, 0};  // vertices per degree class
+    int64_t *loff = nullptr;    // device per-tile class prefixes (pool scratch) for csr_classes
+    long long launches = 0;
+};
+int check_csr(cudaStream_t st, const int64_t *off, const int32_t *col, const int32_t *raw, int64_t nv, int64_t narcs,
+              Pool &pool, CsrInfo &out, std::string &err);
+// The degree-class lists of a checked CSR into bucket[c][nb[c]], ascending ids.
+int csr_classes(cudaStream_t st, const int64_t *off, int64_t nv, const CsrInfo &info, int32_t *const bucket[3],
+                std::string &err);
+
 // CSR build into the context's arrays: off[nv+1], col[narcs], raw[nv], and the degree-class lists
 // bucket[c][nb[c]] in ascending id order.
 int build(cudaStream_t st, Parsed &p, int64_t *off, int32_t *col, int32_t *raw, int32_t *const bucket[3],

@@ -54,7 +54,9 @@ struct LpLaunch {
     int mode;      // DMOLP_LP_MODE_*
 };
 void lp_check_symmetric(dmolp_ctx *c, unsigned long long *counts);  // *b.flag: a reverse is missing
+void lp_symmetry_hash(dmolp_ctx *c, unsigned long long *sum, unsigned long long key);  // *sum += the multiset sum
 void lp_fill(dmolp_ctx *c, int32_t *p, int64_t n, int32_t v);
+void lp_degrees(dmolp_ctx *c, const int64_t *off, int64_t nv, int32_t *deg);  // deg[v] = off[v+1] - off[v]
 void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped);
 // use_hot: the hot labels are current (lp_hot_refresh since the labels were last set outside the loop)
 // keep_eff > 0: also write the kept label counts vcnt (labels < keep_eff <= 32) of every non-hub vertex

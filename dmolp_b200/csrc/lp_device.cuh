@@ -103,6 +103,36 @@ __device__ __forceinline__ int64_t warp_row_wide(const int32_t *__restrict__ col
     return read;
 }
 
+// The same walk with f(u, value) called on every lane for every slot of a step, empty slots included
+// (u == kNoArc, value = none), so that f may take warp-wide votes.  No early stop.
+template <typename T, typename G, typename F>
+__device__ __forceinline__ void warp_row_wide_all(const int32_t *__restrict__ col, int64_t s, int64_t e, int lane,
+                                                  T none, G g, F f) {
+    int64_t a = (s + 3) & ~int64_t(3);
+    if (a > e) a = e;
+    const int64_t qe = e >> 2;
+    const int64_t t0 = a > (qe << 2) ? a : (qe << 2);
+    const int4 *c4 = reinterpret_cast<const int4 *>(col);
+    bool first = true;
+    for (int64_t q0 = a >> 2; first || q0 < qe; q0 += 64) {
+        int u[10];
+        u[8] = first && s + lane < a ? __ldg(col + s + lane) : kNoArc;
+        u[9] = first && t0 + lane < e ? __ldg(col + t0 + lane) : kNoArc;
+        const int64_t q = q0 + lane;
+        int4 x = make_int4(kNoArc, kNoArc, kNoArc, kNoArc), y = x;
+        if (q < qe) x = __ldcs(c4 + q);
+        if (q + 32 < qe) y = __ldcs(c4 + q + 32);
+        u[0] = x.x; u[1] = x.y; u[2] = x.z; u[3] = x.w;
+        u[4] = y.x; u[5] = y.y; u[6] = y.z; u[7] = y.w;
+        T v[10];
+#pragma unroll
+        for (int r = 0; r < 10; ++r) v[r] = u[r] != kNoArc ? g(u[r]) : none;
+#pragma unroll
+        for (int r = 0; r < 10; ++r) f(u[r], v[r]);
+        first = false;
+    }
+}
+
 // Lane-private label counters of one warp for labels < 32: lane L counts label c in
 // h[c*32 + ((L + c) & 31)].  Increments need no atomics and hit distinct banks for lanes sharing a label;
 // the sum over row c (lane c, rotated start) is bank-conflict free as well.

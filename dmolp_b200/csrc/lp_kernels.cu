@@ -546,47 +546,59 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
 
     if (a.kept) {
         // ---- every other selected vertex from its kept label counts (vcnt): thread per vertex, 32 per
-        //      item, the rule of warp_argmax over labels < eff in one thread ----
+        //      item, the rule of warp_argmax over labels < eff in one thread.  The items cost the same, so
+        //      warps stride over them (a shared claim counter would serialise one atomic per 32 vertices) ----
         const int n0 = cn->ndec[0], n = n0 + cn->ndec[1];
         const int ng = (n + 31) >> 5;
-        int pend = grab_issue(&cn->dgrab[0], lane);
-        for (;;) {
-            const int g = grab_take(pend);
-            if (g >= ng) break;
-            pend = grab_issue(&cn->dgrab[0], lane);
+        const int nw = (int)gridDim.x * (int)(blockDim.x >> 5);
+        for (int g = (int)blockIdx.x * (int)(blockDim.x >> 5) + wib; g < ng; g += nw) {  // warp-uniform
             const int i = g * 32 + lane;
-            if (i >= n) continue;
-            const int v = i < n0 ? b.dec[0][i] : b.dec[1][i - n0];
-            const int own = b.label[v];
-            const uint4 *src = reinterpret_cast<const uint4 *>(b.vcnt + (size_t)v * 32);
-            uint32_t w[16];
+            int v = 0, nl = 0;
+            bool mv = false;
+            if (i < n) {
+                v = i < n0 ? b.dec[0][i] : b.dec[1][i - n0];
+                const int own = b.label[v];
+                const uint4 *src = reinterpret_cast<const uint4 *>(b.vcnt + (size_t)v * 32);
+                uint32_t w[16];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint4 x = src[q];
-                w[4 * q] = x.x;
-                w[4 * q + 1] = x.y;
-                w[4 * q + 2] = x.z;
-                w[4 * q + 3] = x.w;
-            }
-            double best = -DBL_MAX;
-            int bkey = 0x7fffffff, blab = -1, own_cnt = 0;
+                for (int q = 0; q < 4; ++q) {
+                    const uint4 x = src[q];
+                    w[4 * q] = x.x;
+                    w[4 * q + 1] = x.y;
+                    w[4 * q + 2] = x.z;
+                    w[4 * q + 3] = x.w;
+                }
+                double best = -DBL_MAX;
+                int bkey = 0x7fffffff, blab = -1, own_cnt = 0;
 #pragma unroll
-            for (int c = 0; c < 32; ++c) {
-                if (c < eff) {
-                    const int cnt = (int)((w[c >> 1] >> ((c & 1) * 16)) & 0xFFFFu);
-                    const double sc = cnt > 0 ? __dmul_rn((double)cnt, __ldg(b.tpen + c)) : 0.0;
-                    const int key = tiekey(c);
-                    if (better(sc, key, best, bkey)) {
-                        best = sc;
-                        bkey = key;
-                        blab = c;
+                for (int c = 0; c < 32; ++c) {
+                    if (c < eff) {
+                        const int cnt = (int)((w[c >> 1] >> ((c & 1) * 16)) & 0xFFFFu);
+                        const double sc = cnt > 0 ? __dmul_rn((double)cnt, __ldg(b.tpen + c)) : 0.0;
+                        const int key = tiekey(c);
+                        if (better(sc, key, best, bkey)) {
+                            best = sc;
+                            bkey = key;
+                            blab = c;
+                        }
+                        if (c == own) own_cnt = cnt;
                     }
-                    if (c == own) own_cnt = cnt;
+                }
+                const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
+                nl = best > own_raw ? blab : own;
+                mv = nl != own;
+            }
+            // the warp's movers appended with one atomic (one per mover would serialise on the counter)
+            const unsigned mm = __ballot_sync(DMOLP_FULL_MASK, mv);
+            if (mm) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&b.cnt->nchanged, __popc(mm));
+                base = __shfl_sync(DMOLP_FULL_MASK, base, 0);
+                if (mv) {
+                    b.newlab[v] = nl;
+                    b.mov[base + __popc(mm & ((1u << lane) - 1))] = v;
                 }
             }
-            const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
-            const int nl = best > own_raw ? blab : own;
-            if (nl != own) park_move(b, v, nl);
         }
     } else {
         // ---- warp per vertex, groups of G consecutive list entries per item ----
@@ -849,7 +861,9 @@ struct StatsArgs {
     int keep_eff;  // > 0: write vcnt, the counts of labels < keep_eff (<= 32), of every non-hub vertex
 };
 
-__global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int *stopped, const int *skip) {
+constexpr int kStatsLaneRow = 64;  // k_stats: rows of at most this many arcs are walked by one lane
+
+__global__ void __launch_bounds__(256, 4) k_stats(Buffers b, StatsArgs a, const int *stopped, const int *skip) {
     if ((stopped && *stopped) || (skip && *skip)) return;
     extern __shared__ unsigned long long sacc[];  // [2k]: vertex counts, intra arcs; then the hot labels
     const int k = a.k;
@@ -863,33 +877,41 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
         s_hot = sh;
         col = b.colh;
     }
-    // kept counts: byte counters of the thread class (word w of thread t at s_kc[w * 256 + t]) and one
-    // 32-int histogram per warp of the warp class
+    // kept counts of the rows a lane walks alone: byte counters (word w of thread t at s_kc[w * 256 + t])
     uint32_t *s_kc = reinterpret_cast<uint32_t *>(reinterpret_cast<uint8_t *>(sacc + 2 * k) + (a.use_hot ? kHotMax : 0));
-    int *s_kw = reinterpret_cast<int *>(s_kc + 8 * kBlock);
-    if (a.keep_eff) {
+    if (a.keep_eff)
         for (int i = threadIdx.x; i < 8 * kBlock; i += blockDim.x) s_kc[i] = 0u;
-        for (int i = threadIdx.x; i < kWarpsPerBlock * 32; i += blockDim.x) s_kw[i] = 0;
-    }
     __syncthreads();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     unsigned long long cut = 0;
     bool bad = false;
-    const int bx = blockIdx.x;
-    if (bx < a.gv) {
-        for (int v = bx * blockDim.x + threadIdx.x; v < a.nv; v += a.gv * blockDim.x) {
-            const int lv = b.label[v];
-            if ((unsigned)lv < (unsigned)k) atomicAdd(&svc[lv], 1ull);
-            else bad = true;
+    // logical block ranges [vertex counts | thread class | warp class | hub rows], dispatched hub rows first
+    // so that the longest rows start in the first wave, then the warp class, the thread class, the counts
+    int bx;
+    {
+        const int r = blockIdx.x, g2 = (int)gridDim.x - a.gv - a.g0 - a.g1;
+        if (r < g2) bx = a.gv + a.g0 + a.g1 + r;
+        else if (r < g2 + a.g1) bx = a.gv + a.g0 + (r - g2);
+        else if (r < g2 + a.g1 + a.g0) bx = a.gv + (r - g2 - a.g1);
+        else bx = r - g2 - a.g1 - a.g0;
+    }
+    if (bx < a.gv) {  // whole warps iterate: the lanes sharing a label add once
+        for (int v0 = bx * blockDim.x + (threadIdx.x & ~31); v0 < a.nv; v0 += a.gv * blockDim.x) {
+            const int v = v0 + lane;
+            const int lv = v < a.nv ? b.label[v] : -1;
+            const bool ok = (unsigned)lv < (unsigned)k;
+            bad |= v < a.nv && !ok;
+            const unsigned m = __match_any_sync(DMOLP_FULL_MASK, ok ? lv : -1);
+            if (ok && lane == __ffs(m) - 1) atomicAdd(&svc[lv], (unsigned long long)__popc(m));
         }
-    } else if (bx < a.gv + a.g0) {
-        for (int i = (bx - a.gv) * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
-            const int v = b.bucket[0][i];
-            const int lv = b.label[v];
-            const int64_t s = b.off[v];
-            const int deg = (int)(b.off[v + 1] - s);
+    } else if (bx < a.gv + a.g0 + a.g1) {
+        // thread class: a lane per row; warp class: rows of at most kStatsLaneRow arcs a lane each too, longer
+        // rows by the whole warp (one after another)
+        const bool cls0 = bx < a.gv + a.g0;
+        // one lane's row: eight ids, then their eight labels, in flight; byte counters for the kept counts
+        auto lane_row = [&](int v, int64_t s, int deg, int lv) {
             unsigned int same = 0, diff = 0;
-            for (int j = 0; j < deg; j += 8) {  // eight ids, then their eight labels, in flight
+            for (int j = 0; j < deg; j += 8) {
                 int u[8], l[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) u[q] = j + q < deg ? __ldg(col + s + j + q) : kNoArc;
@@ -908,7 +930,7 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
             cut += diff;
             b.ndiff[v] = (int)diff;
             if (same && (unsigned)lv < (unsigned)k) atomicAdd(&sin[lv], (unsigned long long)same);
-            if (a.keep_eff) {  // the byte counters (deg <= 16) widened to 32 u16, cleared for the next vertex
+            if (a.keep_eff) {  // the byte counters (deg <= kStatsLaneRow) widened to 32 u16, cleared for the next row
                 uint32_t w[16];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
@@ -921,36 +943,69 @@ __global__ void __launch_bounds__(256) k_stats(Buffers b, StatsArgs a, const int
 #pragma unroll
                 for (int q = 0; q < 4; ++q) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
             }
-        }
-    } else if (bx < a.gv + a.g0 + a.g1) {
-        const int wpb = blockDim.x >> 5;
-        const int gw = (bx - a.gv - a.g0) * wpb + wib, nw = a.g1 * wpb;
-        for (int i = gw; i < a.nb1; i += nw) {
-            const int v = b.bucket[1][i];
-            const int lv = b.label[v];
-            unsigned int same = 0, diff = 0;
-            int *kw = s_kw + wib * 32;
-            warp_row_wide(col, b.off[v], b.off[v + 1], lane, [&](int u) { return nbr_label(b.label, s_hot, u); },
-                          [&](int, int lu) {
-                bad |= (unsigned)lu >= (unsigned)k;
-                same += (lu == lv);
-                diff += (lu != lv);
-                if ((unsigned)lu < (unsigned)a.keep_eff) atomicAdd(&kw[lu], 1);
-            }, [] { return false; });
-            if (a.keep_eff) {  // lane c writes the count of label c (deg <= kLargeDeg fits 16 bits)
-                __syncwarp();
-                b.vcnt[(size_t)v * 32 + lane] = (uint16_t)kw[lane];
-                kw[lane] = 0;
-                __syncwarp();
+        };
+        if (cls0) {
+            for (int i = (bx - a.gv) * blockDim.x + threadIdx.x; i < a.nb0; i += a.g0 * blockDim.x) {
+                const int v = b.bucket[0][i];
+                const int64_t s = b.off[v];
+                lane_row(v, s, (int)(b.off[v + 1] - s), b.label[v]);
             }
-            for (int o = 16; o > 0; o >>= 1) {
-                same += __shfl_xor_sync(DMOLP_FULL_MASK, same, o);
-                diff += __shfl_xor_sync(DMOLP_FULL_MASK, diff, o);
-            }
-            if (lane == 0) {
-                cut += diff;
-                b.ndiff[v] = (int)diff;
-                if (same && (unsigned)lv < (unsigned)k) atomicAdd(&sin[lv], (unsigned long long)same);
+        } else {
+            const int wpb = blockDim.x >> 5;
+            const int gw = (bx - a.gv - a.g0) * wpb + wib, nw = a.g1 * wpb;
+            for (int i0 = gw * 32; i0 < a.nb1; i0 += nw * 32) {
+                const int i = i0 + lane;
+                const bool valid = i < a.nb1;
+                int v = 0, lv = 0;
+                int64_t s = 0, e = 0;
+                if (valid) {
+                    v = b.bucket[1][i];
+                    lv = b.label[v];
+                    s = b.off[v];
+                    e = b.off[v + 1];
+                }
+                const bool mine = valid && e - s <= kStatsLaneRow;
+                if (mine) lane_row(v, s, (int)(e - s), lv);
+                for (unsigned m = __ballot_sync(DMOLP_FULL_MASK, valid && !mine); m; m &= m - 1) {
+                    const int jl = __ffs(m) - 1;
+                    const int vj = __shfl_sync(DMOLP_FULL_MASK, v, jl), lvj = __shfl_sync(DMOLP_FULL_MASK, lv, jl);
+                    const int64_t sj = __shfl_sync(DMOLP_FULL_MASK, s, jl), ej = __shfl_sync(DMOLP_FULL_MASK, e, jl);
+                    unsigned int same = 0, diff = 0;
+                    // kept counts: lane c counts label c.  Per slot of a step, five votes on the bits of the
+                    // lanes' labels select the lanes holding label c (bit-sliced compare), no shared atomics:
+                    // neighbours mostly share a label, which would serialise atomics on one counter.
+                    int mycnt = 0;
+                    warp_row_wide_all(col, sj, ej, lane, 0, [&](int u) { return nbr_label(b.label, s_hot, u); },
+                                      [&](int u, int lu) {
+                        if (u != kNoArc) {
+                            bad |= (unsigned)lu >= (unsigned)k;
+                            same += (lu == lvj);
+                            diff += (lu != lvj);
+                        }
+                        if (a.keep_eff) {  // kernel-uniform
+                            unsigned sel = __ballot_sync(DMOLP_FULL_MASK, u != kNoArc && (unsigned)lu < (unsigned)a.keep_eff);
+                            if (sel) {  // warp-uniform
+#pragma unroll
+                                for (int bit = 0; bit < 5; ++bit) {
+                                    const unsigned bb = __ballot_sync(DMOLP_FULL_MASK, (lu >> bit) & 1);
+                                    sel &= ((lane >> bit) & 1) ? bb : ~bb;
+                                }
+                                mycnt += __popc(sel);
+                            }
+                        }
+                    });
+                    if (a.keep_eff)  // lane c writes the count of label c (deg <= kLargeDeg fits 16 bits)
+                        b.vcnt[(size_t)vj * 32 + lane] = (uint16_t)mycnt;
+                    for (int o = 16; o > 0; o >>= 1) {
+                        same += __shfl_xor_sync(DMOLP_FULL_MASK, same, o);
+                        diff += __shfl_xor_sync(DMOLP_FULL_MASK, diff, o);
+                    }
+                    if (lane == 0) {
+                        cut += diff;
+                        b.ndiff[vj] = (int)diff;
+                        if (same && (unsigned)lvj < (unsigned)k) atomicAdd(&sin[lvj], (unsigned long long)same);
+                    }
+                }
             }
         }
     } else {
@@ -1340,6 +1395,68 @@ __global__ void __launch_bounds__(256) k_symcheck(Buffers b, int g0, int g1, int
     if (__any_sync(DMOLP_FULL_MASK, missing) && lane == 0) *b.flag = 1;
 }
 
+// Multiset symmetry test in one streaming pass.  For every arc (u, v), u != v, of the pair p = (min, max):
+//   S += s * F(p)   (mod 2^64),  s = +1 when u < v, -1 when u > v,  F(p) = mix(p ^ key),
+// mix the SplitMix64 finaliser (Steele, Lea, Flood, "Fast splittable pseudorandom number generators",
+// 2014).  Every pair contributes (arcs u->v minus arcs v->u) times F(p), so a graph whose every arc has its
+// reverse with the same multiplicity gives S = 0 exactly; any other graph gives a nonzero difference vector,
+// and with the key drawn at random per context the sum vanishes with probability about 2^-64 (2^-(64 - t)
+// when every multiplicity difference is a multiple of 2^t).  Self-loops are their own reverse and are skipped.
+__device__ __forceinline__ unsigned long long sym_mix(unsigned long long z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ void sym_hash_arc(unsigned u, unsigned v, unsigned long long key, unsigned long long &sum) {
+    if (u == v) return;
+    const unsigned long long p = u < v ? ((unsigned long long)u << 32 | v) : ((unsigned long long)v << 32 | u);
+    const unsigned long long f = sym_mix(p ^ key);
+    sum += u < v ? f : 0ull - f;
+}
+
+__global__ void __launch_bounds__(256) k_symhash(Buffers b, int g0, int g1, int nb0, int nb1, int nb2,
+                                                 unsigned long long key, unsigned long long *sum) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long acc = 0;
+    // logical blocks [thread class | warp class | block class], dispatched block class (hub rows) first
+    const int g2 = (int)gridDim.x - g0 - g1, r = blockIdx.x;
+    const int bx = r < g2 ? g0 + g1 + r : r - g2;
+    if (bx < g0) {  // thread per vertex (rows of at most 16 arcs)
+        for (int i = bx * blockDim.x + threadIdx.x; i < nb0; i += g0 * blockDim.x) {
+            const int u = b.bucket[0][i];
+            const int64_t s = b.off[u], e = b.off[u + 1];
+#pragma unroll 4
+            for (int64_t j = s; j < e; ++j) sym_hash_arc((unsigned)u, (unsigned)__ldcs(b.col + j), key, acc);
+        }
+    } else if (bx < g0 + g1) {  // warp per vertex
+        const int wpb = blockDim.x >> 5;
+        const int gw = (bx - g0) * wpb + (threadIdx.x >> 5), nw = g1 * wpb;
+        for (int i = gw; i < nb1; i += nw) {
+            const int u = b.bucket[1][i];
+            const int64_t s = b.off[u], e = b.off[u + 1];
+#pragma unroll 4
+            for (int64_t j = s + lane; j < e; j += 32) sym_hash_arc((unsigned)u, (unsigned)__ldcs(b.col + j), key, acc);
+        }
+    } else {  // block per vertex
+        const int gb = bx - g0 - g1, nbk = g2;
+        for (int i = gb; i < nb2; i += nbk) {
+            const int u = b.bucket[2][i];
+            const int64_t s = b.off[u], e = b.off[u + 1];
+#pragma unroll 4
+            for (int64_t j = s + threadIdx.x; j < e; j += blockDim.x)
+                sym_hash_arc((unsigned)u, (unsigned)__ldcs(b.col + j), key, acc);
+        }
+    }
+    acc = warp_sum_u64(acc);
+    if (lane == 0 && acc) atomicAdd(sum, acc);
+}
+
+__global__ void k_degrees(const int64_t *__restrict__ off, int64_t nv, int32_t *__restrict__ deg) {
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x)
+        deg[v] = (int32_t)(off[v + 1] - off[v]);
+}
+
 __global__ void k_fill_int(int32_t *p, int64_t n, int32_t v) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         p[i] = v;
@@ -1433,7 +1550,7 @@ int stats_grid(dmolp_ctx *c, const StatsArgs &a) { return a.gv + a.g0 + a.g1 + c
 
 size_t stats_smem(const StatsArgs &a) {
     return 2 * (size_t)a.k * sizeof(unsigned long long) + (a.use_hot ? (size_t)kHotMax : 0) +
-           (a.keep_eff ? (8 * kBlock + kWarpsPerBlock * 32) * sizeof(int) : 0);
+           (a.keep_eff ? 8 * kBlock * sizeof(int) : 0);
 }
 
 // The LP decisions of the selected window: hub row chunks queued, the classes counted / decided, hub
@@ -1490,6 +1607,20 @@ void lp_check_symmetric(dmolp_ctx *c, unsigned long long *counts) {
     const int g0 = clampi((c->nb[0] + 255) / 256, 1, cap), g1 = clampi((c->nb[1] + 7) / 8, 1, cap);
     const int g2 = clampi(c->nb[2], 1, c->num_sms * 2);
     k_symcheck<<<g0 + g1 + g2, kBlock, 0, c->stream>>>(c->b, g0, g1, c->nb[0], c->nb[1], c->nb[2], counts);
+    c->launches++;
+}
+
+void lp_symmetry_hash(dmolp_ctx *c, unsigned long long *sum, unsigned long long key) {
+    const int cap = c->num_sms * 8;
+    const int g0 = clampi((c->nb[0] + 255) / 256, 1, cap), g1 = clampi((c->nb[1] + 7) / 8, 1, cap);
+    const int g2 = clampi(c->nb[2], 1, c->num_sms * 2);
+    k_symhash<<<g0 + g1 + g2, kBlock, 0, c->stream>>>(c->b, g0, g1, c->nb[0], c->nb[1], c->nb[2], key, sum);
+    c->launches++;
+}
+
+void lp_degrees(dmolp_ctx *c, const int64_t *off, int64_t nv, int32_t *deg) {
+    if (nv <= 0) return;
+    k_degrees<<<grid_for(c), kBlock, 0, c->stream>>>(off, nv, deg);
     c->launches++;
 }
 

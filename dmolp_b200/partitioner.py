@@ -172,6 +172,17 @@ class Partitioner:
             raise ValueError("labels length != number of vertices")
         self._check(self.lib.dmolp_labels_set(self.ctx, _p(lab)))
 
+    def symmetric(self) -> bool:
+        """Whether the resident graph is symmetric with strictly increasing rows (the LP loop then updates cut
+        and balance from the movers alone); runs the symmetry test now if the loop has not yet."""
+        out = ctypes.c_int()
+        self._check(self.lib.dmolp_graph_symmetric(self.ctx, byref(out)))
+        return bool(out.value)
+
+    def set_symmetry_test(self, exact: bool) -> None:
+        """exact=False (default): keyed multiset sums in one pass; exact=True: every reverse arc looked up."""
+        self._check(self.lib.dmolp_set_symmetry_test(self.ctx, 1 if exact else 0))
+
     def kernel_launches(self) -> int:
         return int(self.lib.dmolp_kernel_launches(self.ctx))
 

@@ -1,8 +1,11 @@
 """Train the learned initial partition on runs of the plain method, then compare it with the plain method
 on held-out graphs.
 
-    python -m dmolp_b200.train_proposal --train 2048 --epochs 40 --out dmolp_b200/weights/proposal.npy \
-        --eval 256 --report report.json
+    python -m dmolp_b200.train_proposal --train 10240 --vmax 200000 --epochs 30 --lr 0.003 --pos-repeat 5 \
+        --eval 256 --out dmolp_b200/weights/proposal.npy --report report.json
+
+(the command that made the shipped weights, dmolp_b200/weights/proposal.npy, and its record
+proposal_training.json beside them).
 
 Training graphs and held-out graphs come from the batched workload's distribution (vertex counts
 log-uniform in [vmin, vmax], half k-NN 2-D/3-D, half preferential attachment, k uniform in 2..64) with
@@ -116,6 +119,8 @@ def main():
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--report", default=None)
     ap.add_argument("--chunk", type=int, default=1024, help="graphs per batch when computing the targets")
+    ap.add_argument("--pos-repeat", type=int, default=1,
+                    help="each graph whose target is 1 appears this many times in the training minibatches")
     a = ap.parse_args()
     rep = {"args": vars(a)}
     t0 = time.time()
@@ -125,7 +130,13 @@ def main():
     y, rep["target_stats"] = chunked_targets(tr, a.theta, a.chunk)
     rep["targets_s"] = time.time() - t0
     rep["train_targets_positive"] = float(y.mean())
-    sets = [(tr[i:i + a.minibatch], y[i:i + a.minibatch]) for i in range(0, len(tr), a.minibatch)]
+    idx = np.arange(len(tr))
+    if a.pos_repeat > 1:  # balance the classes by repeating the (rarer) positive graphs
+        idx = np.concatenate([idx] + [np.nonzero(y > 0.5)[0]] * (a.pos_repeat - 1))
+        np.random.default_rng(a.seed).shuffle(idx)
+    rep["train_samples"] = int(len(idx))
+    sets = [([tr[j] for j in idx[i:i + a.minibatch]], y[idx[i:i + a.minibatch]])
+            for i in range(0, len(idx), a.minibatch)]
     model = Proposal(0)
     t0 = time.time()
     losses = train_gate(model, sets, a.epochs, a.lr, log=lambda ep, l: print(f"epoch {ep} loss {l:.5f}", flush=True))

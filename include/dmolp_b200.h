@@ -230,6 +230,17 @@ int dmolp_kernel_profile(dmolp_ctx *ctx, int kernel, double *total_ms, int64_t *
  * No reference counterpart (the reference's kernel has no barrier).  Mainly for testing that path. */
 int dmolp_set_wait_limit(dmolp_ctx *ctx, uint32_t polls);
 
+/* How the LP loop tests whether the resident graph is symmetric (every arc's reverse present, with the same
+ * multiplicity), which lets it update cut and balance from the movers alone.  exact = 0 (default): one
+ * streaming pass forms a keyed 64-bit multiset sum, zero for every symmetric graph; an asymmetric graph
+ * passes with probability about 2^-64 (key drawn per context).  exact = 1: every reverse arc is looked up
+ * by binary search (a few ms per 10^8 arcs).  Either way the test runs once per uploaded graph, when the loop
+ * first needs it.  No reference counterpart (the reference always recounts). */
+int dmolp_set_symmetry_test(dmolp_ctx *ctx, int exact);
+/* The test's answer for the resident graph (runs it now if the loop has not yet): 1 = symmetric with rows
+ * strictly increasing (incremental statistics apply), else 0. */
+int dmolp_graph_symmetric(dmolp_ctx *ctx, int *symmetric);
+
 /* ---- phase-1 hubs on the host (no device work) ----
  * dmolp_find_hubs_pairs: find_hub_nodes (src/phase1/init.cpp:139-177) on n (id, degree) pairs given in the
  * reference's degree-map order: the pairs sorted by degree in exactly the order std::sort leaves them (ties

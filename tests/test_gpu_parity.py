@@ -203,7 +203,7 @@ def test_window_select_and_lp_apply_match_oracle(golden_cases, part):
 @pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built")
 def test_reference_gpu_kernel_agrees(part):
     """The reference's own CUDA path (boundaryLPKernel_unified built unmodified for sm_100a, driven by its
-    run_phase2 loop) against the oracle and this build, on the same graphs and phase-1 labels."""
+    run_phase2 loop) against the oracle and this library, on the same graphs and phase-1 labels."""
     import os
     import tempfile
 
