@@ -240,6 +240,8 @@ __device__ __forceinline__ void put_slot(const Buffers &b, int pos, bool isb, in
 // differently-labelled neighbour: ndiff[v] > 0, a count kept exact by the statistics pass and by k_update
 // (symmetric graphs) or by the full pass after every move (other graphs).  So only pull-mode candidacy
 // walks rows; at t = 1 and in push mode every record slot costs a handful of per-vertex reads.
+constexpr int kBndPushU = 4;  // k_bnd push mode: record slots per thread and step
+
 __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
     if (b.ctrl->stopped) return;
     // [k] boundary records per label in this block, then [k * 256] first-digit or [k * kDsBins] superbin counts
@@ -273,13 +275,33 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
         put_slot(b, pos, isb, own, key);
     };
     if (!pull) {
-        // ---- every record slot, thread per slot ----
+        // ---- every record slot, thread per slot; kBndPushU slots per thread with their loads in flight
+        //      together (the per-slot chain slot -> vertex state -> offsets is latency, not bandwidth) ----
         const int n = a.nb0 + a.nb1 + a.nb2;
-        for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += gridDim.x * blockDim.x) {
-            const int v = b.ball[pos];
-            const int st = b.stamp[v], hw = a.hubwin ? b.hubwin[v] : 0, nd = b.ndiff[v], lv = b.label[v];
-            const bool cand = a.all || st == a.t || hw > 0;
-            finish(pos, v, cand, cand ? (int)(b.off[v + 1] - b.off[v]) : 0, nd, lv);
+        const int nt = (int)gridDim.x * (int)blockDim.x;
+        for (int p0 = blockIdx.x * blockDim.x + threadIdx.x; p0 < n; p0 += kBndPushU * nt) {
+            int v[kBndPushU], st[kBndPushU], hw[kBndPushU], nd[kBndPushU], lv[kBndPushU], deg[kBndPushU];
+            bool cand[kBndPushU];
+#pragma unroll
+            for (int q = 0; q < kBndPushU; ++q) v[q] = p0 + q * nt < n ? b.ball[p0 + q * nt] : -1;
+#pragma unroll
+            for (int q = 0; q < kBndPushU; ++q) {
+                st[q] = hw[q] = nd[q] = lv[q] = 0;
+                if (v[q] >= 0) {
+                    st[q] = b.stamp[v[q]];
+                    hw[q] = a.hubwin ? b.hubwin[v[q]] : 0;
+                    nd[q] = b.ndiff[v[q]];
+                    lv[q] = b.label[v[q]];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kBndPushU; ++q) {
+                cand[q] = v[q] >= 0 && (a.all || st[q] == a.t || hw[q] > 0);
+                deg[q] = cand[q] ? (int)(b.off[v[q] + 1] - b.off[v[q]]) : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < kBndPushU; ++q)
+                if (v[q] >= 0) finish(p0 + q * nt, v[q], cand[q], deg[q], nd[q], lv[q]);
         }
     } else if ((int)blockIdx.x < a.g0) {
         // ---- pull, thread per vertex (deg <= kSmallDeg): window stamps of the row, 8 at a time ----
