@@ -652,22 +652,35 @@ __global__ void __launch_bounds__(256) k_csr_arcs(const int32_t *__restrict__ co
     const int64_t nwarp = (int64_t)gridDim.x * (blockDim.x >> 5);
     int bad = 0;
     unsigned long long viol = 0;
-    for (int64_t w0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; w0 < n4; w0 += nwarp * 32) {
-        const int64_t i = w0 + lane;
-        int4 q = make_int4(0, 0, 0, 0);
-        uint32_t bits = 0xfu;
-        if (i < n4) {
-            q = __ldcs(reinterpret_cast<const int4 *>(col) + i);
-            bits = (__ldg(rowbit + (i >> 3)) >> ((i & 7) * 4)) & 0xfu;
-        }
-        int prev = __shfl_up_sync(DMOLP_FULL_MASK, q.w, 1);
-        if (lane == 0) prev = i > 0 && i < n4 ? __ldg(col + 4 * i - 1) : 0;
-        if (i < n4) {
-            const int x[4] = {q.x, q.y, q.z, q.w};
+    // two 16-byte groups per lane and step (512 arcs per warp), their loads in flight together
+    for (int64_t w0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 64; w0 < n4; w0 += nwarp * 64) {
+        int4 q[2];
+        uint32_t bits[2];
+        int pre[2];
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                if ((uint32_t)x[t] >= (uint64_t)nv) bad = 2;
-                if (order && !((bits >> t) & 1u) && (i > 0 || t > 0) && x[t] <= (t ? x[t - 1] : prev)) ++viol;
+        for (int h = 0; h < 2; ++h) {
+            const int64_t i = w0 + h * 32 + lane;
+            q[h] = make_int4(0, 0, 0, 0);
+            bits[h] = 0xfu;
+            pre[h] = 0;
+            if (i < n4) {
+                q[h] = __ldcs(reinterpret_cast<const int4 *>(col) + i);
+                bits[h] = (__ldg(rowbit + (i >> 3)) >> ((i & 7) * 4)) & 0xfu;
+                if (lane == 0 && i > 0) pre[h] = __ldg(col + 4 * i - 1);
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t i = w0 + h * 32 + lane;
+            int prev = __shfl_up_sync(DMOLP_FULL_MASK, q[h].w, 1);
+            if (lane == 0) prev = pre[h];
+            if (i < n4) {
+                const int x[4] = {q[h].x, q[h].y, q[h].z, q[h].w};
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    if ((uint32_t)x[t] >= (uint64_t)nv) bad = 2;
+                    if (order && !((bits[h] >> t) & 1u) && (i > 0 || t > 0) && x[t] <= (t ? x[t - 1] : prev)) ++viol;
+                }
             }
         }
     }
@@ -926,7 +939,7 @@ int check_csr(cudaStream_t st, const int64_t *off, const int32_t *col, const int
         out.launches += 2;
     }
     if (narcs > 0) {
-        k_csr_arcs<<<grid_for(narcs / 4 + 1, 256), 256, 0, st>>>(col, narcs, nv, rowbit, sc);
+        k_csr_arcs<<<grid_for(narcs / 8 + 1, 256), 256, 0, st>>>(col, narcs, nv, rowbit, sc);
         ++out.launches;
     }
     CsrScal h{};
