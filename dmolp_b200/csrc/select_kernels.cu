@@ -620,7 +620,10 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
     int *s_wrun = s_wc + kDsWarps * nseg;                       // [kDsWarps * nseg] running rank per warp
     int *s_stage = s_wrun + kDsWarps * nseg;                    // [kDsWarps * 4 * kStage] window appends
     __shared__ int s_scnt[kDsWarps][4];
-    __shared__ int s_ntie, s_walk1;
+    __shared__ int s_ntie, s_walk1, s_bstar, s_before;
+    __shared__ unsigned int s_wsum[kDsWarps];
+    __shared__ int s_soff[kDsWarps][4], s_sbase[4];
+    __shared__ unsigned long long s_te[kDsWarps], s_ws[kDsWarps];
     int *w_stage = s_stage + wid * 4 * kStage, *w_scnt = s_scnt[wid];
     if (lane < 4) w_scnt[lane] = 0;
     for (int i = threadIdx.x; i < nseg * kDsFine; i += blockDim.x) s_f[i] = 0u;
@@ -850,16 +853,33 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         emit_window<1>(a.sp, &take, &key, &p, vmask, te, ws, w_stage, w_scnt);  // all lanes
     }
     // ---- block p (p, p + gridDim.x, ...): label p's records of a partial superbin of degree >= 2048 ----
+    // The partial fine bin spans 2^jw degrees (octave j, jw = j - 6).  Its records are counted per sub-bin of
+    // the label's order (one degree each while jw <= 10, else 2^(jw-10) degrees), a block scan finds the
+    // sub-bin where the rest of the need is reached, the sub-bins before it are taken, and only that
+    // sub-bin's records are sorted by key (degree, then id) -- at these degrees usually a handful.
     for (int p = blockIdx.x; p < nseg; p += gridDim.x) {
         if (s_kind[p] != 3) continue;  // block-uniform
         const int nt = __ldcg(a.tcnt + p);
         const uint64_t *seg_tail = a.tail + s_toff[p];
-        const int ftake = s_ftake[p], fpart = s_fpart[p], frem = s_frem[p];
+        const int ftake = s_ftake[p], fpart = s_fpart[p], frem = s_frem[p], dir = s_dir[p];
+        const int jw = ds_ord(s_opart[p], kDsBins, dir) - kDsCoarse0 + 5;  // superbin kDsCoarse0 + j - 11
+        const int sh = jw > 10 ? jw - 10 : 0;
+        const int nsub = 1 << (jw - sh);  // <= 1024 = blockDim.x
+        auto sub_of = [&](uint64_t key) {
+            const int dk = (int)(key >> ibits);
+            const int x = (dir ? maxdeg - dk : dk) & ((1 << jw) - 1);
+            return (dir ? (1 << jw) - 1 - x : x) >> sh;
+        };
+        unsigned int *s_sub = reinterpret_cast<unsigned int *>(s_tkey);  // counts first, the tied keys later
         __syncthreads();  // s_ntie and the shared tie keys are free
-        if (threadIdx.x == 0) s_ntie = 0;
+        for (int i = threadIdx.x; i < nsub; i += blockDim.x) s_sub[i] = 0u;
+        if (threadIdx.x == 0) {
+            s_ntie = 0;
+            s_bstar = -1;
+            s_before = 0;
+        }
         __syncthreads();
-        // the segment in chunks: records of fine bins before the partial one are taken, those of the partial
-        // fine bin are collected
+        // pass 1: records of fine bins before the partial one are taken; the partial one's counted per sub-bin
         for (int i0 = 0; i0 < nt; i0 += blockDim.x) {
             const int i = i0 + (int)threadIdx.x;
             bool take = false;
@@ -869,19 +889,66 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
                 key = __ldcg(seg_tail + i);
                 int o, fo;
                 bins_of(key, p, o, fo);
-                if (fo < ftake) {
-                    take = true;
-                } else if (fo == fpart) {
-                    const int q = atomicAdd(&s_ntie, 1);
-                    if (q < kDsTieCap) s_tkey[q] = key;
+                if (fo < ftake) take = true;
+                else if (fo == fpart) atomicAdd(&s_sub[sub_of(key)], 1u);
+            }
+            emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
+        }
+        __syncthreads();
+        {  // the sub-bin where the running count reaches frem (block scan, one sub-bin per thread)
+            const unsigned int c = (int)threadIdx.x < nsub ? s_sub[threadIdx.x] : 0u;
+            unsigned int incl = c;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned int y = __shfl_up_sync(DMOLP_FULL_MASK, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) s_wsum[wid] = incl;
+            __syncthreads();
+            if (wid == 0) {
+                unsigned int x = s_wsum[lane];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned int y = __shfl_up_sync(DMOLP_FULL_MASK, x, o);
+                    if (lane >= o) x += y;
+                }
+                s_wsum[lane] = x;
+            }
+            __syncthreads();
+            incl += wid ? s_wsum[wid - 1] : 0u;
+            if (c && incl - c < (unsigned)frem && (unsigned)frem <= incl) {
+                s_bstar = (int)threadIdx.x;
+                s_before = (int)(incl - c);
+            }
+        }
+        __syncthreads();
+        const int bstar = s_bstar, rem2 = frem - s_before;  // bstar < 0: inconsistent counts (never expected)
+        // pass 2: sub-bins before bstar are taken, bstar's records collected
+        for (int i0 = 0; i0 < nt; i0 += blockDim.x) {
+            const int i = i0 + (int)threadIdx.x;
+            bool take = false;
+            uint64_t key = 0;
+            int pp = p;
+            if (i < nt && bstar >= 0) {
+                key = __ldcg(seg_tail + i);
+                int o, fo;
+                bins_of(key, p, o, fo);
+                if (fo == fpart) {
+                    const int sb2 = sub_of(key);
+                    if (sb2 < bstar) {
+                        take = true;
+                    } else if (sb2 == bstar) {
+                        const int q = atomicAdd(&s_ntie, 1);
+                        if (q < kDsTieCap) s_tkey[q] = key;
+                    }
                 }
             }
             emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
         }
         __syncthreads();
         const int m = s_ntie;
-        if (m <= kDsTieCap) {
-            // the ties sorted by key (bitonic, padded to a power of two): the first frem are taken
+        if (bstar < 0) {
+            // nothing more from this label
+        } else if (m <= kDsTieCap) {
+            // the sub-bin's records sorted by key (bitonic, padded to a power of two): the first rem2 are taken
             int n2 = 1;
             while (n2 < m) n2 <<= 1;
             for (int i = m + (int)threadIdx.x; i < n2; i += blockDim.x) s_tkey[i] = ~0ull;
@@ -899,7 +966,7 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
                 }
             }
             __syncthreads();
-            const int nt2 = frem < m ? frem : m;
+            const int nt2 = rem2 < m ? rem2 : m;
             for (int i0 = 0; i0 < nt2; i0 += blockDim.x) {
                 const int i = i0 + (int)threadIdx.x;
                 bool take = i < nt2;
@@ -907,7 +974,7 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
                 int pp = p;
                 emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
             }
-        } else {  // more ties than the shared keys hold: each ranked against the segment in global memory
+        } else {  // more ties than the shared keys hold: each ranked against the sub-bin in global memory
             for (int i0 = 0; i0 < nt; i0 += blockDim.x) {
                 const int i = i0 + (int)threadIdx.x;
                 bool take = false;
@@ -917,26 +984,54 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
                     key = __ldcg(seg_tail + i);
                     int o, fo;
                     bins_of(key, p, o, fo);
-                    if (fo == fpart) {
+                    if (fo == fpart && sub_of(key) == bstar) {
                         int rank = 0;
                         for (int j = 0; j < nt; ++j) {
                             const uint64_t kj = __ldcg(seg_tail + j);
                             int oj, foj;
                             bins_of(kj, p, oj, foj);
-                            rank += foj == fpart && kj < key;
+                            rank += foj == fpart && sub_of(kj) == bstar && kj < key;
                         }
-                        take = rank < frem;
+                        take = rank < rem2;
                     }
                 }
                 emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
             }
         }
     }
-    stage_flush(a.sp, w_stage, w_scnt);
+    // ---- end: the warps' staged appends and the block's sums, one atomic per list and per sum for the block
+    //      (one per warp would queue ~4,700 atomics on each of six counters) ----
+    __syncthreads();  // every warp's stage and counts are final
+    if (threadIdx.x < 4) {
+        const int j = threadIdx.x;
+        int tot = 0;
+        for (int w = 0; w < kDsWarps; ++w) {
+            s_soff[w][j] = tot;
+            tot += s_scnt[w][j];
+        }
+        s_sbase[j] = tot ? atomicAdd(list_ctr(a.sp, j), tot) : 0;
+    }
     te = warp_sum_u64(te);
     ws = warp_sum_u64(ws);
-    if (lane == 0 && te) atomicAdd(a.sp.te, te);
-    if (lane == 0 && ws) atomicAdd(a.sp.wsum, ws);
+    if (lane == 0) {
+        s_te[wid] = te;
+        s_ws[wid] = ws;
+    }
+    __syncthreads();
+    for (int j = 0; j < 4; ++j) {
+        const int n = w_scnt[j];
+        int *dst = list_ptr(a.sp, j) + s_sbase[j] + s_soff[wid][j];
+        for (int i = lane; i < n; i += 32) dst[i] = w_stage[j * kStage + i];
+    }
+    if (threadIdx.x == 0) {
+        unsigned long long tt = 0, ww = 0;
+        for (int w = 0; w < kDsWarps; ++w) {
+            tt += s_te[w];
+            ww += s_ws[w];
+        }
+        if (tt) atomicAdd(a.sp.te, tt);
+        if (ww) atomicAdd(a.sp.wsum, ww);
+    }
 }
 
 }  // namespace
