@@ -58,6 +58,23 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x)
     return x;
 }
 
+// One value per thread summed over the block; thread 0 adds the sum to *dst.  One atomic per block instead
+// of one per warp: atomics on one address queue at one L2 slice, and the warps of a kernel finish together.
+// Every thread of the block must call it (two block barriers); blockDim.x <= 1024.
+template <typename T>
+__device__ __forceinline__ void block_atomic_add(unsigned long long v, T *dst) {
+    __shared__ unsigned long long s_w[32];
+    v = warp_sum_u64(v);
+    __syncthreads();  // s_w is free (an earlier call's sums were read)
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_w[w];
+        if (t) atomicAdd(dst, (T)t);
+    }
+}
+
 // Read-only, streaming load of a neighbour id (bypasses L1 allocation; CSR is read once per pass).
 __device__ __forceinline__ int32_t ld_stream(const int32_t *p) { return __ldcs(p); }
 

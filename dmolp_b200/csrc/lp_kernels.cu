@@ -104,8 +104,7 @@ __global__ void k_mark(Buffers b, int t) {
         warp_row(b.col, s, e1, lane, [&](int u) { stamp_once(b, u, t); }, [] { return false; });
         if (lane == 0) rd += (unsigned long long)(e1 - s);
     }
-    rd = warp_sum_u64(rd);
-    if (lane == 0 && rd) atomicAdd(&b.rec[t - 1].arcs_mark, rd);
+    block_atomic_add(rd, &b.rec[t - 1].arcs_mark);
 }
 
 __global__ void k_mark_chunks(Buffers b, int t) {
@@ -121,8 +120,7 @@ __global__ void k_mark_chunks(Buffers b, int t) {
         warp_row(b.col, s, e, lane, [&](int u) { stamp_once(b, u, t); }, [] { return false; });
         if (lane == 0) rd += (unsigned long long)(e - s);
     }
-    rd = warp_sum_u64(rd);
-    if (lane == 0 && rd) atomicAdd(&b.rec[t - 1].arcs_mark, rd);
+    block_atomic_add(rd, &b.rec[t - 1].arcs_mark);
 }
 
 // The loop's marking: the previous window by decision class (dec[c], ndec_prev[c]; the lists are rewritten
@@ -169,8 +167,7 @@ __global__ void __launch_bounds__(256, 5) k_mark_win(Buffers b, int t, int g0) {
                           [] { return false; });
         }
     }
-    rd = warp_sum_u64(rd);
-    if (lane == 0 && rd) atomicAdd(&b.rec[t - 1].arcs_mark, rd);
+    block_atomic_add(rd, &b.rec[t - 1].arcs_mark);
 }
 
 // hubwin[u] = hubs of the previous window whose rows hold u, kept across iterations: a hub that entered
@@ -206,8 +203,7 @@ __global__ void k_hubwin_apply(Buffers b, int t) {
         warp_row(b.col, s, e, lane, [&](int u) { atomicAdd(&b.hubwin[u], d); }, [] { return false; });
         if (lane == 0) rd += (unsigned long long)(e - s);
     }
-    rd = warp_sum_u64(rd);
-    if (lane == 0 && rd) atomicAdd(&b.rec[t - 1].arcs_mark, rd);
+    block_atomic_add(rd, &b.rec[t - 1].arcs_mark);
 }
 
 // ------------------------------------------------------------------------------------ bnd
@@ -409,16 +405,10 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
             __syncthreads();
         }
     }
-    te = warp_sum_u64(te);
-    rd = warp_sum_u64(rd);
-    nc = warp_sum_u64(nc);
-    nbd = warp_sum_u64(nbd);
-    if (lane == 0) {
-        if (te) atomicAdd(&b.rec[a.t - 1].te_cand, te);
-        if (rd) atomicAdd(&b.rec[a.t - 1].arcs_bnd, rd);
-        if (nc) atomicAdd(&b.cnt->ncand, (int)nc);
-        if (nbd) atomicAdd(&b.cnt->nbnd, (int)nbd);
-    }
+    block_atomic_add(te, &b.rec[a.t - 1].te_cand);
+    block_atomic_add(rd, &b.rec[a.t - 1].arcs_bnd);
+    block_atomic_add(nc, &b.cnt->ncand);
+    block_atomic_add(nbd, &b.cnt->nbnd);
     __syncthreads();
     for (int p = threadIdx.x; p < k; p += blockDim.x)
         if (s_npart[p]) atomicAdd(&b.npart[p], s_npart[p]);
@@ -725,6 +715,7 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
             }
         }
     }
+    // per warp (no block barrier: the decisions' dynamic shared memory already takes the whole 48 KB)
     rd = warp_sum_u64(rd);
     if (lane == 0 && rd) atomicAdd(&b.rec[a.t - 1].arcs_dec, rd);
 }
@@ -847,12 +838,8 @@ __global__ void __launch_bounds__(256, 2) k_update(Buffers b, int k, int eff, in
             if (out_a) atomicAdd(&sacc[k + a], (unsigned long long)(-out_a));
         }
     }
-    for (int o = 16; o > 0; o >>= 1) dcut += __shfl_xor_sync(DMOLP_FULL_MASK, dcut, o);
-    rd = warp_sum_u64(rd);
-    if (lane == 0) {
-        if (dcut) atomicAdd(&b.cnt->cut_arcs, (unsigned long long)dcut);
-        if (rd) atomicAdd(&b.rec[t - 1].arcs_upd, rd);
-    }
+    block_atomic_add((unsigned long long)dcut, &b.cnt->cut_arcs);  // the sum is taken mod 2^64: negative deltas add
+    block_atomic_add(rd, &b.rec[t - 1].arcs_upd);
     __syncthreads();
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
         if (sacc[p]) atomicAdd(&b.vc[p], sacc[p]);
@@ -1071,9 +1058,8 @@ __global__ void __launch_bounds__(256, 4) k_stats(Buffers b, StatsArgs a, const 
             __syncthreads();
         }
     }
-    cut = warp_sum_u64(cut);
-    if (lane == 0 && cut) atomicAdd(&b.cnt->cut_arcs, cut);
     if (__any_sync(DMOLP_FULL_MASK, bad) && lane == 0) b.ctrl->error = 1;
+    block_atomic_add(cut, &b.cnt->cut_arcs);
     __syncthreads();
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
         if (svc[p]) atomicAdd(&b.vc[p], svc[p]);
@@ -1470,8 +1456,7 @@ __global__ void __launch_bounds__(256) k_symhash(Buffers b, int g0, int g1, int 
                 sym_hash_arc((unsigned)u, (unsigned)__ldcs(b.col + j), key, acc);
         }
     }
-    acc = warp_sum_u64(acc);
-    if (lane == 0 && acc) atomicAdd(sum, acc);
+    block_atomic_add(acc, sum);
 }
 
 __global__ void k_degrees(const int64_t *__restrict__ off, int64_t nv, int32_t *__restrict__ deg) {
