@@ -1188,8 +1188,8 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
     lp_reset_stats(c, k, nullptr);
     // symmetric graphs with at most 32 scored labels decide from kept label counts (no label gathers)
     c->counts_kept = c->symmetric && L.eff <= 32;
-    lp_stats(c, k, nullptr, nullptr, true, c->counts_kept ? L.eff : 0);
-    if (c->symmetric) lp_hub_counts(c, L.eff);
+    // the run-start pass also counts every hub's row into hh on symmetric graphs (kept from the movers after)
+    lp_stats(c, k, nullptr, nullptr, true, c->counts_kept ? L.eff : 0, c->symmetric ? L.eff : 0);
     lp_init_end(c, cfg->mode);
     st = check_launch(c);
     if (st) return st;

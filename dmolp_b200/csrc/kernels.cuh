@@ -60,14 +60,13 @@ void lp_degrees(dmolp_ctx *c, const int64_t *off, int64_t nv, int32_t *deg);  //
 void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped);
 // use_hot: the hot labels are current (lp_hot_refresh since the labels were last set outside the loop)
 // keep_eff > 0: also write the kept label counts vcnt (labels < keep_eff <= 32) of every non-hub vertex
-void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot = false, int keep_eff = 0);
+void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot = false, int keep_eff = 0,
+              int hub_eff = 0);  // hub_eff > 0: also every hub's label counts (hh), labels < hub_eff
 void lp_hot_hist(dmolp_ctx *c);              // b.degh = histogram of min(degree, 65535), degree > 0
 void lp_hot_build(dmolp_ctx *c, int dstar);  // vertices of degree >= dstar ranked; colh; b.flag = their number
 void lp_hot_refresh(dmolp_ctx *c);           // hot labels from the resident labels
 void lp_init_end(dmolp_ctx *c, int mode);
 void lp_hub_index(dmolp_ctx *c);            // b.hidx from bucket[2] (once per graph)
-void lp_hub_counts(dmolp_ctx *c, int eff);  // label counts of every hub's row into b.hh (run start, symmetric)
-// One LP iteration.  On symmetric graphs the hub decisions read b.hh as lp_hub_counts left it and k_update
 // keeps it current; otherwise the selected hubs' rows are recounted.
 void lp_iteration(dmolp_ctx *c, const LpLaunch &L, int t, bool first, bool last);
 // one-off pieces used by dmolp_window_select / dmolp_lp_apply

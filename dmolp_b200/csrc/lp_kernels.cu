@@ -743,16 +743,6 @@ __global__ void k_hub_prep(Buffers b, int eff) {
     hub_queue(b, b.dec[2], b.cnt->ndec[2], eff);
 }
 
-// Run start on symmetric graphs: every hub's row counted once (k_hub_all_queue, then k_hub_all_count).
-__global__ void k_hub_all_queue(Buffers b, int nhub, int eff) { hub_queue(b, b.bucket[2], nhub, eff); }
-
-__global__ void __launch_bounds__(256, 4) k_hub_all_count(Buffers b, int eff, int wstride) {
-    extern __shared__ int shist[];
-    int *h = shist + (threadIdx.x >> 5) * wstride;
-    unsigned long long rd = 0;
-    hub_chunks(b, b.col, nullptr, b.bucket[2], eff, threadIdx.x & 31, h, rd);
-}
-
 __global__ void k_hub_index(Buffers b, int nhub) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nhub; i += gridDim.x * blockDim.x)
         b.hidx[b.bucket[2][i]] = i;
@@ -868,6 +858,7 @@ struct StatsArgs {
     int k, nv, gv, g0, g1, nb0, nb1, nb2;
     int use_hot;   // rows through colh and the block's copy of the hot labels (k <= 255)
     int keep_eff;  // > 0: write vcnt, the counts of labels < keep_eff (<= 32), of every non-hub vertex
+    int hub_eff;   // > 0: write hh, every hub's counts of labels < hub_eff (the run start on symmetric graphs)
 };
 
 constexpr int kStatsLaneRow = 64;  // k_stats: rows of at most this many arcs are walked by one lane
@@ -1019,12 +1010,20 @@ __global__ void __launch_bounds__(256, 4) k_stats(Buffers b, StatsArgs a, const 
         }
     } else {
         __shared__ unsigned int s_diff[8];
+        __shared__ int s_hcw[kWarpsPerBlock][32];  // hub label counts per warp (hub_eff <= 32)
+        int *s_hc = reinterpret_cast<int *>(s_kc);  // [hub_eff] block counts (hub_eff > 32; keep_eff is 0 then)
+        const int heff = a.hub_eff;
         const int gb = bx - a.gv - a.g0 - a.g1, nbk = (int)gridDim.x - a.gv - a.g0 - a.g1;
         for (int i = gb; i < a.nb2; i += nbk) {
             const int v = b.bucket[2][i];
             const int lv = b.label[v];
             const int64_t s = b.off[v], e = b.off[v + 1];
             unsigned int same = 0, diff = 0;
+            int mycnt = 0;  // hub_eff <= 32: lane c counts label c (bit-sliced votes per slot)
+            if (heff > 32) {
+                for (int c = threadIdx.x; c < heff; c += blockDim.x) s_hc[c] = 0;
+                __syncthreads();
+            }
             for (int64_t j0 = s; j0 < e; j0 += 4 * blockDim.x) {  // four ids per thread, then their labels
                 int u[4], l[4];
 #pragma unroll
@@ -1041,6 +1040,39 @@ __global__ void __launch_bounds__(256, 4) k_stats(Buffers b, StatsArgs a, const 
                         same += (l[q] == lv);
                         diff += (l[q] != lv);
                     }
+                if (heff > 32) {  // kernel-uniform
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (u[q] != kNoArc && (unsigned)l[q] < (unsigned)heff) atomicAdd(&s_hc[l[q]], 1);
+                } else if (heff > 0) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        unsigned sel = __ballot_sync(DMOLP_FULL_MASK, u[q] != kNoArc && (unsigned)l[q] < (unsigned)heff);
+                        if (sel) {  // warp-uniform
+#pragma unroll
+                            for (int bit = 0; bit < 5; ++bit) {
+                                const unsigned bb = __ballot_sync(DMOLP_FULL_MASK, (l[q] >> bit) & 1);
+                                sel &= ((lane >> bit) & 1) ? bb : ~bb;
+                            }
+                            mycnt += __popc(sel);
+                        }
+                    }
+                }
+            }
+            if (heff > 0) {  // the hub's row of label counts, written whole (labels < hub_eff)
+                int32_t *row = b.hh + (size_t)b.hidx[v] * DMOLP_MAX_K;
+                if (heff <= 32) s_hcw[wib][lane] = mycnt;
+                __syncthreads();
+                if (heff <= 32) {
+                    if ((int)threadIdx.x < heff) {
+                        int t = 0;
+                        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_hcw[w][threadIdx.x];
+                        row[threadIdx.x] = t;
+                    }
+                } else {
+                    for (int c = threadIdx.x; c < heff; c += blockDim.x) row[c] = s_hc[c];
+                }
+                __syncthreads();
             }
             cut += diff;
             for (int o = 16; o > 0; o >>= 1) {
@@ -1537,10 +1569,11 @@ int dec_grid(dmolp_ctx *c, int eff) {
 }
 
 // use_hot: the hot labels are current; applies when the graph has a hot set and k <= 255 (exact bytes).
-StatsArgs stats_args(dmolp_ctx *c, int k, bool use_hot, int keep_eff = 0) {
+StatsArgs stats_args(dmolp_ctx *c, int k, bool use_hot, int keep_eff = 0, int hub_eff = 0) {
     StatsArgs a;
     a.k = k;
     a.keep_eff = keep_eff;
+    a.hub_eff = c->nb[2] > 0 ? hub_eff : 0;
     a.use_hot = use_hot && c->nhot > 0 && k <= 255;
     a.nv = (int)c->nv;
     const int cap = c->num_sms * 8;
@@ -1556,8 +1589,8 @@ StatsArgs stats_args(dmolp_ctx *c, int k, bool use_hot, int keep_eff = 0) {
 int stats_grid(dmolp_ctx *c, const StatsArgs &a) { return a.gv + a.g0 + a.g1 + clampi(c->nb[2], 1, c->num_sms * 2); }
 
 size_t stats_smem(const StatsArgs &a) {
-    return 2 * (size_t)a.k * sizeof(unsigned long long) + (a.use_hot ? (size_t)kHotMax : 0) +
-           (a.keep_eff ? 8 * kBlock * sizeof(int) : 0);
+    const size_t kc = a.keep_eff ? 8 * kBlock * sizeof(int) : 0, hc = a.hub_eff > 32 ? (size_t)a.hub_eff * sizeof(int) : 0;
+    return 2 * (size_t)a.k * sizeof(unsigned long long) + (a.use_hot ? (size_t)kHotMax : 0) + (kc > hc ? kc : hc);
 }
 
 // The LP decisions of the selected window: hub row chunks queued, the classes counted / decided, hub
@@ -1641,8 +1674,8 @@ void lp_reset_stats(dmolp_ctx *c, int k, const int *stopped) {
     c->launches++;
 }
 
-void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot, int keep_eff) {
-    const StatsArgs a = stats_args(c, k, use_hot, keep_eff);
+void lp_stats(dmolp_ctx *c, int k, const int *stopped, const int *skip, bool use_hot, int keep_eff, int hub_eff) {
+    const StatsArgs a = stats_args(c, k, use_hot, keep_eff, hub_eff);
     k_stats<<<stats_grid(c, a), kBlock, stats_smem(a), c->stream>>>(c->b, a, stopped, skip);
     c->launches++;
 }
@@ -1671,16 +1704,6 @@ void lp_hub_index(dmolp_ctx *c) {
         k_hub_index<<<clampi((c->nb[2] + 255) / 256, 1, grid_for(c)), kBlock, 0, c->stream>>>(c->b, c->nb[2]);
         c->launches++;
     }
-}
-
-void lp_hub_counts(dmolp_ctx *c, int eff) {
-    if (c->nb[2] == 0) return;
-    Buffers &b = c->b;
-    cudaMemsetAsync(&b.cnt->nhubq, 0, sizeof(int), c->stream);
-    cudaMemsetAsync(&b.cnt->dgrab[2], 0, sizeof(int), c->stream);
-    k_hub_all_queue<<<clampi((c->nb[2] + 7) / 8, 1, grid_for(c)), kBlock, 0, c->stream>>>(b, c->nb[2], eff);
-    k_hub_all_count<<<c->num_sms * 4, kBlock, dec_smem(eff, false), c->stream>>>(b, eff, dec_wstride(eff));
-    c->launches += 2;
 }
 
 void lp_init_end(dmolp_ctx *c, int mode) {
