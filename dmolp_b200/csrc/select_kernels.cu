@@ -707,15 +707,26 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         fo = ds_ord(bf.y, kDsFine, dir);
         return bf;
     };
+    // the next step's slots are loaded while this step's are processed
+    int np_[kDsU];
+    uint64_t nkey[kDsU];
+#pragma unroll
+    for (int u = 0; u < kDsU; ++u) {
+        const int r = wlo + u * 32 + lane;
+        np_[u] = r < whi ? a.seg[r] : -1;
+        nkey[u] = r < whi ? a.key[r] : 0;
+    }
     for (int r0 = wlo; r0 < whi; r0 += 32 * kDsU) {
-        int r[kDsU], p[kDsU], fb[kDsU];
+        int p[kDsU], fb[kDsU];
         uint64_t key[kDsU];
         bool take[kDsU], part[kDsU];
 #pragma unroll
         for (int u = 0; u < kDsU; ++u) {
-            r[u] = r0 + u * 32 + lane;
-            p[u] = r[u] < whi ? a.seg[r[u]] : -1;
-            key[u] = r[u] < whi ? a.key[r[u]] : 0;
+            p[u] = np_[u];
+            key[u] = nkey[u];
+            const int r = r0 + 32 * kDsU + u * 32 + lane;
+            np_[u] = r < whi ? a.seg[r] : -1;
+            nkey[u] = r < whi ? a.key[r] : 0;
         }
 #pragma unroll
         for (int u = 0; u < kDsU; ++u) {
@@ -852,16 +863,39 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         __syncwarp();
         emit_window<1>(a.sp, &take, &key, &p, vmask, te, ws, w_stage, w_scnt);  // all lanes
     }
-    // ---- block p (p, p + gridDim.x, ...): label p's records of a partial superbin of degree >= 2048 ----
-    // The partial fine bin spans 2^jw degrees (octave j, jw = j - 6).  Its records are counted per sub-bin of
-    // the label's order (one degree each while jw <= 10, else 2^(jw-10) degrees), a block scan finds the
-    // sub-bin where the rest of the need is reached, the sub-bins before it are taken, and only that
-    // sub-bin's records are sorted by key (degree, then id) -- at these degrees usually a handful.
+    // ---- labels with a partial superbin of degree >= 2048: their tail segments ----
+    // Every block takes its slice of every such segment's records of fine bins before the partial one.
+    for (int p = 0; p < nseg; ++p) {
+        if (s_kind[p] != 3) continue;  // block-uniform
+        const int nt = __ldcg(a.tcnt + p);
+        const int ch = (nt + (int)gridDim.x - 1) / (int)gridDim.x;
+        const int lo = (int)blockIdx.x * ch, hi = min(nt, lo + ch);
+        const uint64_t *seg_tail = a.tail + s_toff[p];
+        const int ftake = s_ftake[p];
+        for (int i0 = lo; i0 < hi; i0 += blockDim.x) {  // block-uniform trip count
+            const int i = i0 + (int)threadIdx.x;
+            bool take = false;
+            uint64_t key = 0;
+            int pp = p;
+            if (i < hi) {
+                key = __ldcg(seg_tail + i);
+                int o, fo;
+                bins_of(key, p, o, fo);
+                take = fo < ftake;
+            }
+            emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
+        }
+    }
+    // Block p (p, p + gridDim.x, ...) takes label p's records of the partial fine bin.  It spans 2^jw degrees
+    // (octave j, jw = j - 6); its records are counted per sub-bin of the label's order (one degree each while
+    // jw <= 10, else 2^(jw-10) degrees), a block scan finds the sub-bin where the rest of the need is reached,
+    // the sub-bins before it are taken, and only that sub-bin's records are sorted by key (degree, then id)
+    // -- at these degrees usually a handful.
     for (int p = blockIdx.x; p < nseg; p += gridDim.x) {
         if (s_kind[p] != 3) continue;  // block-uniform
         const int nt = __ldcg(a.tcnt + p);
         const uint64_t *seg_tail = a.tail + s_toff[p];
-        const int ftake = s_ftake[p], fpart = s_fpart[p], frem = s_frem[p], dir = s_dir[p];
+        const int fpart = s_fpart[p], frem = s_frem[p], dir = s_dir[p];
         const int jw = ds_ord(s_opart[p], kDsBins, dir) - kDsCoarse0 + 5;  // superbin kDsCoarse0 + j - 11
         const int sh = jw > 10 ? jw - 10 : 0;
         const int nsub = 1 << (jw - sh);  // <= 1024 = blockDim.x
@@ -879,20 +913,21 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
             s_before = 0;
         }
         __syncthreads();
-        // pass 1: records of fine bins before the partial one are taken; the partial one's counted per sub-bin
-        for (int i0 = 0; i0 < nt; i0 += blockDim.x) {
-            const int i = i0 + (int)threadIdx.x;
-            bool take = false;
-            uint64_t key = 0;
-            int pp = p;
-            if (i < nt) {
-                key = __ldcg(seg_tail + i);
-                int o, fo;
-                bins_of(key, p, o, fo);
-                if (fo < ftake) take = true;
-                else if (fo == fpart) atomicAdd(&s_sub[sub_of(key)], 1u);
+        // pass 1: the partial fine bin's records counted per sub-bin (four keys per thread in flight)
+        for (int i0 = 0; i0 < nt; i0 += 4 * blockDim.x) {
+            uint64_t k4[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = i0 + q * (int)blockDim.x + (int)threadIdx.x;
+                k4[q] = i < nt ? __ldcg(seg_tail + i) : ~0ull;
             }
-            emit_window<1>(a.sp, &take, &key, &pp, vmask, te, ws, w_stage, w_scnt);  // all lanes
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (k4[q] == ~0ull) continue;
+                int o, fo;
+                bins_of(k4[q], p, o, fo);
+                if (fo == fpart) atomicAdd(&s_sub[sub_of(k4[q])], 1u);
+            }
         }
         __syncthreads();
         {  // the sub-bin where the running count reaches frem (block scan, one sub-bin per thread)
