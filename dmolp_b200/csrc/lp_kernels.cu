@@ -571,29 +571,49 @@ __global__ void __launch_bounds__(256, 4) k_decide(Buffers b, DecArgs a) {
                 v = i < n0 ? b.dec[0][i] : b.dec[1][i - n0];
                 const int own = b.label[v];
                 const uint4 *src = reinterpret_cast<const uint4 *>(b.vcnt + (size_t)v * 32);
-                uint32_t w[16];
+                // the 16 count words staged in the lane's row of the warp's shared counters (stride 17:
+                // no bank conflicts), the labels with a nonzero count as a mask
+                uint32_t *sw = reinterpret_cast<uint32_t *>(h) + lane * 17;
+                uint32_t nz = 0;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const uint4 x = src[q];
-                    w[4 * q] = x.x;
-                    w[4 * q + 1] = x.y;
-                    w[4 * q + 2] = x.z;
-                    w[4 * q + 3] = x.w;
+                    const uint32_t xw[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        sw[4 * q + r] = xw[r];
+                        const uint32_t m2 = __vcmpne2(xw[r], 0u);  // 0xFFFF per nonzero half
+                        nz |= ((m2 & 1u) | ((m2 >> 15) & 2u)) << (2 * (4 * q + r));
+                    }
                 }
+                const uint32_t effm = eff >= 32 ? ~0u : (1u << eff) - 1u;
+                nz &= effm;
+                // argmax of (score, tie key) over labels < eff: the labels with neighbours first; those with
+                // none score exactly 0 and can only win when nothing scored above 0
                 double best = -DBL_MAX;
                 int bkey = 0x7fffffff, blab = -1, own_cnt = 0;
-#pragma unroll
-                for (int c = 0; c < 32; ++c) {
-                    if (c < eff) {
-                        const int cnt = (int)((w[c >> 1] >> ((c & 1) * 16)) & 0xFFFFu);
-                        const double sc = cnt > 0 ? __dmul_rn((double)cnt, __ldg(b.tpen + c)) : 0.0;
+                for (uint32_t m = nz; m; m &= m - 1) {
+                    const int c = __ffs(m) - 1;
+                    const int cnt = (int)((sw[c >> 1] >> ((c & 1) * 16)) & 0xFFFFu);
+                    const double sc = __dmul_rn((double)cnt, __ldg(b.tpen + c));
+                    const int key = tiekey(c);
+                    if (better(sc, key, best, bkey)) {
+                        best = sc;
+                        bkey = key;
+                        blab = c;
+                    }
+                    if (c == own) own_cnt = cnt;
+                }
+                const uint32_t zm = ~nz & effm;
+                if (zm && !(best > 0.0)) {
+                    for (uint32_t m = zm; m; m &= m - 1) {
+                        const int c = __ffs(m) - 1;
                         const int key = tiekey(c);
-                        if (better(sc, key, best, bkey)) {
-                            best = sc;
+                        if (better(0.0, key, best, bkey)) {
+                            best = 0.0;
                             bkey = key;
                             blab = c;
                         }
-                        if (c == own) own_cnt = cnt;
                     }
                 }
                 const double own_raw = (unsigned)own < (unsigned)eff ? (double)own_cnt : -1e300;
@@ -764,6 +784,8 @@ __global__ void k_hub_final(Buffers b, int eff, int t) {
 // the reverse arc (u,v) changes the same way but is never visited; weight 1 when u moves (or u == v):
 // (u,v) is visited from u's side.  Vertex counts move by one.  A hub neighbour u sees v's label go from
 // a to c: its row of label counts (labels < eff) moves by one.
+constexpr int kUpdLaneRow = 32;  // k_update: rows of at most this many arcs are walked by one lane
+
 __global__ void __launch_bounds__(256, 2) k_update(Buffers b, int k, int eff, int t, int keep) {
     if (b.ctrl->stopped) return;
     extern __shared__ unsigned long long sacc[];  // [2k]: vertex-count deltas, intra-arc deltas
@@ -774,58 +796,98 @@ __global__ void __launch_bounds__(256, 2) k_update(Buffers b, int k, int eff, in
     const int n = b.cnt->nchanged;
     long long dcut = 0;
     unsigned long long rd = 0;
-    for (int i = gw; i < n; i += nw) {
-        const int v = b.mov[i];
-        const int a = b.label[v], c = b.newlab[v];
-        const int64_t s = b.off[v], e = b.off[v + 1];
-        long long in_c = 0, out_a = 0, dc = 0;
-        int dv = 0;
-        warp_row_wide(b.col, s, e, lane, [&](int u) { return make_int3(b.label[u], b.newlab[u], b.hidx[u]); },
-                      [&](int u, int3 g) {
-            const int lo = g.x;
-            const int nu = g.y;
-            const int ln = nu >= 0 ? nu : lo;
-            const int w = nu >= 0 ? 1 : 2;
-            dc += w * ((int)(c != ln) - (int)(a != lo));
-            in_c += w * (int)(c == ln);
-            out_a += w * (int)(a == lo);
-            // differently-labelled neighbour counts: arc (u,v) seen from u; arc (v,u) from v when u stays
-            // (a moving u updates v's count from its own row)
-            const int du = (int)(ln != c) - (int)(lo != a);
-            if (du) atomicAdd(&b.ndiff[u], du);
-            if (nu < 0) dv += (int)(c != lo) - (int)(a != lo);
-            const int hu = g.z;
-            if (hu >= 0) {
-                int32_t *row = b.hh + (size_t)hu * DMOLP_MAX_K;
-                if ((unsigned)a < (unsigned)eff) atomicAdd(&row[a], -1);
-                if ((unsigned)c < (unsigned)eff) atomicAdd(&row[c], 1);
-            } else if (keep) {
-                // u's 16-bit counts, two per word: a count leaves label a (it is >= 1: it counts v) and
-                // enters label c (it stays <= deg(u) <= kLargeDeg), so no carry or borrow crosses a half
-                uint32_t *w = reinterpret_cast<uint32_t *>(b.vcnt + (size_t)u * 32);
-                const bool ia = (unsigned)a < (unsigned)eff, ic = (unsigned)c < (unsigned)eff;
-                const uint32_t da = 1u << ((a & 1) * 16), dc = 1u << ((c & 1) * 16);
-                if (ia && ic && (a >> 1) == (c >> 1)) {
-                    atomicAdd(&w[a >> 1], dc - da);
-                } else {
-                    if (ia) atomicSub(&w[a >> 1], da);
-                    if (ic) atomicAdd(&w[c >> 1], dc);
-                }
+    // arc (v, u) of a mover v from label a to c, u's labels g = (old, pending or -1, hub index or -1)
+    auto arc = [&](int u, int3 g, int a, int c, long long &in_c, long long &out_a, int &dv) {
+        const int lo = g.x;
+        const int nu = g.y;
+        const int ln = nu >= 0 ? nu : lo;
+        const int w = nu >= 0 ? 1 : 2;
+        dcut += w * ((int)(c != ln) - (int)(a != lo));
+        in_c += w * (int)(c == ln);
+        out_a += w * (int)(a == lo);
+        // differently-labelled neighbour counts: arc (u,v) seen from u; arc (v,u) from v when u stays
+        // (a moving u updates v's count from its own row)
+        const int du = (int)(ln != c) - (int)(lo != a);
+        if (du) atomicAdd(&b.ndiff[u], du);
+        if (nu < 0) dv += (int)(c != lo) - (int)(a != lo);
+        const int hu = g.z;
+        if (hu >= 0) {
+            int32_t *row = b.hh + (size_t)hu * DMOLP_MAX_K;
+            if ((unsigned)a < (unsigned)eff) atomicAdd(&row[a], -1);
+            if ((unsigned)c < (unsigned)eff) atomicAdd(&row[c], 1);
+        } else if (keep) {
+            // u's 16-bit counts, two per word: a count leaves label a (it is >= 1: it counts v) and
+            // enters label c (it stays <= deg(u) <= kLargeDeg), so no carry or borrow crosses a half
+            uint32_t *wd = reinterpret_cast<uint32_t *>(b.vcnt + (size_t)u * 32);
+            const bool ia = (unsigned)a < (unsigned)eff, ic = (unsigned)c < (unsigned)eff;
+            const uint32_t da = 1u << ((a & 1) * 16), dcn = 1u << ((c & 1) * 16);
+            if (ia && ic && (a >> 1) == (c >> 1)) {
+                atomicAdd(&wd[a >> 1], dcn - da);
+            } else {
+                if (ia) atomicSub(&wd[a >> 1], da);
+                if (ic) atomicAdd(&wd[c >> 1], dcn);
             }
-        }, [] { return false; });
-        for (int o = 16; o > 0; o >>= 1) {
-            in_c += __shfl_xor_sync(DMOLP_FULL_MASK, in_c, o);
-            out_a += __shfl_xor_sync(DMOLP_FULL_MASK, out_a, o);
-            dv += __shfl_xor_sync(DMOLP_FULL_MASK, dv, o);
         }
-        if (lane == 0 && dv) atomicAdd(&b.ndiff[v], dv);
-        dcut += dc;
-        if (lane == 0) {
+    };
+    auto gather = [&](int u) { return make_int3(b.label[u], b.newlab[u], b.hidx[u]); };
+    // 32 movers per warp and step: a row of at most kUpdLaneRow arcs is walked by its lane alone (four arcs
+    // in flight), longer rows by the whole warp one after another
+    for (int i0 = gw * 32; i0 < n; i0 += nw * 32) {
+        const int i = i0 + lane;
+        const bool valid = i < n;
+        int v = 0, a = 0, c = 0;
+        int64_t s = 0, e = 0;
+        if (valid) {
+            v = b.mov[i];
+            a = b.label[v];
+            c = b.newlab[v];
+            s = b.off[v];
+            e = b.off[v + 1];
+        }
+        const bool mine = valid && e - s <= kUpdLaneRow;
+        if (mine) {
+            long long in_c = 0, out_a = 0;
+            int dv = 0;
+            for (int64_t j0 = s; j0 < e; j0 += 4) {
+                int u[4];
+                int3 g[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) u[q] = j0 + q < e ? __ldg(b.col + j0 + q) : -1;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) g[q] = u[q] >= 0 ? gather(u[q]) : make_int3(0, -1, -1);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (u[q] >= 0) arc(u[q], g[q], a, c, in_c, out_a, dv);
+            }
+            if (dv) atomicAdd(&b.ndiff[v], dv);
             rd += (unsigned long long)(e - s);
             atomicAdd(&sacc[a], (unsigned long long)(-1ll));
             atomicAdd(&sacc[c], 1ull);
             if (in_c) atomicAdd(&sacc[k + c], (unsigned long long)in_c);
             if (out_a) atomicAdd(&sacc[k + a], (unsigned long long)(-out_a));
+        }
+        for (unsigned m = __ballot_sync(DMOLP_FULL_MASK, valid && !mine); m; m &= m - 1) {
+            const int jl = __ffs(m) - 1;
+            const int vj = __shfl_sync(DMOLP_FULL_MASK, v, jl), aj = __shfl_sync(DMOLP_FULL_MASK, a, jl),
+                      cj = __shfl_sync(DMOLP_FULL_MASK, c, jl);
+            const int64_t sj = __shfl_sync(DMOLP_FULL_MASK, s, jl), ej = __shfl_sync(DMOLP_FULL_MASK, e, jl);
+            long long in_c = 0, out_a = 0;
+            int dv = 0;
+            warp_row_wide(b.col, sj, ej, lane, gather, [&](int u, int3 g) { arc(u, g, aj, cj, in_c, out_a, dv); },
+                          [] { return false; });
+            for (int o = 16; o > 0; o >>= 1) {
+                in_c += __shfl_xor_sync(DMOLP_FULL_MASK, in_c, o);
+                out_a += __shfl_xor_sync(DMOLP_FULL_MASK, out_a, o);
+                dv += __shfl_xor_sync(DMOLP_FULL_MASK, dv, o);
+            }
+            if (lane == 0) {
+                if (dv) atomicAdd(&b.ndiff[vj], dv);
+                rd += (unsigned long long)(ej - sj);
+                atomicAdd(&sacc[aj], (unsigned long long)(-1ll));
+                atomicAdd(&sacc[cj], 1ull);
+                if (in_c) atomicAdd(&sacc[k + cj], (unsigned long long)in_c);
+                if (out_a) atomicAdd(&sacc[k + aj], (unsigned long long)(-out_a));
+            }
         }
     }
     block_atomic_add((unsigned long long)dcut, &b.cnt->cut_arcs);  // the sum is taken mod 2^64: negative deltas add
