@@ -784,7 +784,8 @@ __global__ void k_hub_final(Buffers b, int eff, int t) {
 // the reverse arc (u,v) changes the same way but is never visited; weight 1 when u moves (or u == v):
 // (u,v) is visited from u's side.  Vertex counts move by one.  A hub neighbour u sees v's label go from
 // a to c: its row of label counts (labels < eff) moves by one.
-constexpr int kUpdLaneRow = 32;  // k_update: rows of at most this many arcs are walked by one lane
+constexpr int kUpdLaneRow = 32;  // k_update: rows of at most this many arcs are walked by one lane ...
+constexpr int kUpdLaneMin = 8;   // ... when there are at least this many movers per warp
 
 __global__ void __launch_bounds__(256, 2) k_update(Buffers b, int k, int eff, int t, int keep) {
     if (b.ctrl->stopped) return;
@@ -830,63 +831,74 @@ __global__ void __launch_bounds__(256, 2) k_update(Buffers b, int k, int eff, in
         }
     };
     auto gather = [&](int u) { return make_int3(b.label[u], b.newlab[u], b.hidx[u]); };
-    // 32 movers per warp and step: a row of at most kUpdLaneRow arcs is walked by its lane alone (four arcs
-    // in flight), longer rows by the whole warp one after another
-    for (int i0 = gw * 32; i0 < n; i0 += nw * 32) {
-        const int i = i0 + lane;
-        const bool valid = i < n;
-        int v = 0, a = 0, c = 0;
-        int64_t s = 0, e = 0;
-        if (valid) {
-            v = b.mov[i];
-            a = b.label[v];
-            c = b.newlab[v];
-            s = b.off[v];
-            e = b.off[v + 1];
+    // a mover's row walked by the whole warp (all lanes call it)
+    auto warp_mover = [&](int vj, int aj, int cj, int64_t sj, int64_t ej) {
+        long long in_c = 0, out_a = 0;
+        int dv = 0;
+        warp_row_wide(b.col, sj, ej, lane, gather, [&](int u, int3 g) { arc(u, g, aj, cj, in_c, out_a, dv); },
+                      [] { return false; });
+        for (int o = 16; o > 0; o >>= 1) {
+            in_c += __shfl_xor_sync(DMOLP_FULL_MASK, in_c, o);
+            out_a += __shfl_xor_sync(DMOLP_FULL_MASK, out_a, o);
+            dv += __shfl_xor_sync(DMOLP_FULL_MASK, dv, o);
         }
-        const bool mine = valid && e - s <= kUpdLaneRow;
-        if (mine) {
-            long long in_c = 0, out_a = 0;
-            int dv = 0;
-            for (int64_t j0 = s; j0 < e; j0 += 4) {
-                int u[4];
-                int3 g[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) u[q] = j0 + q < e ? __ldg(b.col + j0 + q) : -1;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) g[q] = u[q] >= 0 ? gather(u[q]) : make_int3(0, -1, -1);
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (u[q] >= 0) arc(u[q], g[q], a, c, in_c, out_a, dv);
-            }
-            if (dv) atomicAdd(&b.ndiff[v], dv);
-            rd += (unsigned long long)(e - s);
-            atomicAdd(&sacc[a], (unsigned long long)(-1ll));
-            atomicAdd(&sacc[c], 1ull);
-            if (in_c) atomicAdd(&sacc[k + c], (unsigned long long)in_c);
-            if (out_a) atomicAdd(&sacc[k + a], (unsigned long long)(-out_a));
+        if (lane == 0) {
+            if (dv) atomicAdd(&b.ndiff[vj], dv);
+            rd += (unsigned long long)(ej - sj);
+            atomicAdd(&sacc[aj], (unsigned long long)(-1ll));
+            atomicAdd(&sacc[cj], 1ull);
+            if (in_c) atomicAdd(&sacc[k + cj], (unsigned long long)in_c);
+            if (out_a) atomicAdd(&sacc[k + aj], (unsigned long long)(-out_a));
         }
-        for (unsigned m = __ballot_sync(DMOLP_FULL_MASK, valid && !mine); m; m &= m - 1) {
-            const int jl = __ffs(m) - 1;
-            const int vj = __shfl_sync(DMOLP_FULL_MASK, v, jl), aj = __shfl_sync(DMOLP_FULL_MASK, a, jl),
-                      cj = __shfl_sync(DMOLP_FULL_MASK, c, jl);
-            const int64_t sj = __shfl_sync(DMOLP_FULL_MASK, s, jl), ej = __shfl_sync(DMOLP_FULL_MASK, e, jl);
-            long long in_c = 0, out_a = 0;
-            int dv = 0;
-            warp_row_wide(b.col, sj, ej, lane, gather, [&](int u, int3 g) { arc(u, g, aj, cj, in_c, out_a, dv); },
-                          [] { return false; });
-            for (int o = 16; o > 0; o >>= 1) {
-                in_c += __shfl_xor_sync(DMOLP_FULL_MASK, in_c, o);
-                out_a += __shfl_xor_sync(DMOLP_FULL_MASK, out_a, o);
-                dv += __shfl_xor_sync(DMOLP_FULL_MASK, dv, o);
+    };
+    if (n < nw * kUpdLaneMin) {
+        // few movers: one per warp at a time, its row spread over the lanes
+        for (int i = gw; i < n; i += nw) {
+            const int v = b.mov[i];
+            warp_mover(v, b.label[v], b.newlab[v], b.off[v], b.off[v + 1]);
+        }
+    } else {
+        // many movers: 32 per warp and step; a row of at most kUpdLaneRow arcs is walked by its lane alone
+        // (four arcs in flight), longer rows by the whole warp one after another
+        for (int i0 = gw * 32; i0 < n; i0 += nw * 32) {
+            const int i = i0 + lane;
+            const bool valid = i < n;
+            int v = 0, a = 0, c = 0;
+            int64_t s = 0, e = 0;
+            if (valid) {
+                v = b.mov[i];
+                a = b.label[v];
+                c = b.newlab[v];
+                s = b.off[v];
+                e = b.off[v + 1];
             }
-            if (lane == 0) {
-                if (dv) atomicAdd(&b.ndiff[vj], dv);
-                rd += (unsigned long long)(ej - sj);
-                atomicAdd(&sacc[aj], (unsigned long long)(-1ll));
-                atomicAdd(&sacc[cj], 1ull);
-                if (in_c) atomicAdd(&sacc[k + cj], (unsigned long long)in_c);
-                if (out_a) atomicAdd(&sacc[k + aj], (unsigned long long)(-out_a));
+            const bool mine = valid && e - s <= kUpdLaneRow;
+            if (mine) {
+                long long in_c = 0, out_a = 0;
+                int dv = 0;
+                for (int64_t j0 = s; j0 < e; j0 += 4) {
+                    int u[4];
+                    int3 g[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) u[q] = j0 + q < e ? __ldg(b.col + j0 + q) : -1;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) g[q] = u[q] >= 0 ? gather(u[q]) : make_int3(0, -1, -1);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (u[q] >= 0) arc(u[q], g[q], a, c, in_c, out_a, dv);
+                }
+                if (dv) atomicAdd(&b.ndiff[v], dv);
+                rd += (unsigned long long)(e - s);
+                atomicAdd(&sacc[a], (unsigned long long)(-1ll));
+                atomicAdd(&sacc[c], 1ull);
+                if (in_c) atomicAdd(&sacc[k + c], (unsigned long long)in_c);
+                if (out_a) atomicAdd(&sacc[k + a], (unsigned long long)(-out_a));
+            }
+            for (unsigned m = __ballot_sync(DMOLP_FULL_MASK, valid && !mine); m; m &= m - 1) {
+                const int jl = __ffs(m) - 1;
+                warp_mover(__shfl_sync(DMOLP_FULL_MASK, v, jl), __shfl_sync(DMOLP_FULL_MASK, a, jl),
+                           __shfl_sync(DMOLP_FULL_MASK, c, jl), __shfl_sync(DMOLP_FULL_MASK, s, jl),
+                           __shfl_sync(DMOLP_FULL_MASK, e, jl));
             }
         }
     }
