@@ -40,7 +40,7 @@ constexpr int kGridPerSm = 4;
 
 // ------------------------------------------------------------------------------------ begin
 // Start of iteration t (one block): counters, the iteration record, penalties.
-__device__ void lp_begin(const Buffers &b, int k, int t, long long narcs) {
+__device__ void lp_begin(const Buffers &b, int k, int t, long long narcs, double *s_re, double *s_tp) {
     LpControl *ctl = b.ctrl;
     LpCounters *cn = b.cnt;
     for (int p = threadIdx.x; p < k; p += blockDim.x) b.npart[p] = 0;
@@ -70,9 +70,15 @@ __device__ void lp_begin(const Buffers &b, int k, int t, long long narcs) {
         r.win_sum = 0;
     }
     // ---- statistics -> expected values and calculatePenalties (phase2.cpp:110-115, 158-209) ----
-    if (threadIdx.x < 32)
+    // (RE and the penalties in shared memory while the serial sums read them, then out to global)
+    if (threadIdx.x < 32) {
         warp_penalties(k, [&](int p) { return sll(b.vc[p]); }, [&](int p) { return sll(b.intra[p]) / 2; },
-                       b.logtab[t], b.RE, b.tpen, b.penhist + (size_t)(t - 1) * DMOLP_MAX_K);
+                       b.logtab[t], s_re, s_tp, b.penhist + (size_t)(t - 1) * DMOLP_MAX_K);
+        for (int p = threadIdx.x; p < k; p += 32) {
+            b.RE[p] = s_re[p];
+            b.tpen[p] = s_tp[p];
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------ mark
@@ -1287,6 +1293,7 @@ __device__ void lp_end(const Buffers &b, int k, int t, long long narcs, int mode
 // loop, the start of iteration t_begin (when > 0).
 __global__ void k_lp_turn(Buffers b, int k, int t_end, int t_begin, long long narcs, int mode, int symmetric) {
     __shared__ int s_stopped;
+    __shared__ double s_re[DMOLP_MAX_K], s_tp[DMOLP_MAX_K];
     if (threadIdx.x == 0) s_stopped = b.ctrl->stopped;
     __syncthreads();
     if (s_stopped) return;
@@ -1297,7 +1304,7 @@ __global__ void k_lp_turn(Buffers b, int k, int t_end, int t_begin, long long na
         __syncthreads();
         if (s_stopped) return;
     }
-    if (t_begin > 0) lp_begin(b, k, t_begin, narcs);
+    if (t_begin > 0) lp_begin(b, k, t_begin, narcs, s_re, s_tp);
 }
 
 // Asymmetric graphs: decide whether the full statistics pass runs (the reference skips it on an empty
