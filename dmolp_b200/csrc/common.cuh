@@ -27,7 +27,6 @@ constexpr int kDsCoarse0 = kDsSingle + 31;            // first superbin of degre
 constexpr int kDsBins = kDsCoarse0 + 20;              // superbins per label (degrees < 2^31)
 constexpr int kDsFine = 64;                           // fine bins per superbin
 constexpr int kDsExactMax = 2048;                     // degrees below this have a fine bin of their own
-constexpr int kDsChunk = 4096;  // record slots per chunk of the boundary counts that balance the selection's walk
 
 __device__ __forceinline__ int2 dsel_bin(int d) {
     if (d < kDsSingle) return make_int2(d, 0);

@@ -125,7 +125,6 @@ struct Buffers {
     unsigned int *dsup = nullptr;        // [kDegSelMaxK * kDsBins]
     unsigned int *dfine[2] = {nullptr, nullptr};  // [kDegSelMaxK * kDsFine] each
     unsigned int *dcntb = nullptr;       // [num_sms * kDegSelMaxK * kDsFine]
-    unsigned int *dchunk = nullptr;      // [npos / kDsChunk + 1] boundary records per chunk of record slots
     int *dtcnt = nullptr;                // [2 * kDegSelMaxK] tail records per label (by iteration parity)
     uint64_t *dlkey = nullptr;           // [nv] keys of the selection warps' lists (labels in active[0])
     uint64_t *dtkey = nullptr;           // [nv] keys of the selection's tail segments

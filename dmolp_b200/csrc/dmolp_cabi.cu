@@ -96,7 +96,6 @@ int clear_select_bins(dmolp_ctx *c) {
     for (int i = 0; i < 2; ++i)
         DMOLP_CUDA(cudaMemsetAsync(b.dfine[i], 0, (size_t)kDegSelMaxK * kDsFine * sizeof(unsigned int), c->stream));
     DMOLP_CUDA(cudaMemsetAsync(b.dtcnt, 0, 2 * kDegSelMaxK * sizeof(int), c->stream));
-    DMOLP_CUDA(cudaMemsetAsync(b.dchunk, 0, ((size_t)c->nv / kDsChunk + 2) * sizeof(unsigned int), c->stream));
     return DMOLP_OK;
 }
 
@@ -267,7 +266,6 @@ size_t layout(dmolp_ctx *c, char *base, int64_t nv, int64_t narcs, const size_t 
     ALLOC(b.dfine[0], (size_t)kDegSelMaxK * kDsFine);
     ALLOC(b.dfine[1], (size_t)kDegSelMaxK * kDsFine);
     ALLOC(b.dcntb, (size_t)c->num_sms * kDegSelMaxK * kDsFine);
-    ALLOC(b.dchunk, (size_t)nv / kDsChunk + 2);
     ALLOC(b.dtcnt, 2 * kDegSelMaxK);
     ALLOC(b.dlkey, n);
     ALLOC(b.dtkey, n);

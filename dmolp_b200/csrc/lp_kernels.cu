@@ -219,7 +219,6 @@ struct BndArgs {
     unsigned int *hist;  // when set: first-digit histogram of the boundary records for the selection (k <= 32)
     int hshift;          // its digit: bits [hshift, hshift + 8) of the key
     unsigned int *dsup;  // when set: degree-superbin counts of the boundary records per label (k <= 64)
-    unsigned int *dchunk;  // with dsup: boundary records per kDsChunk record slots (the selection's balance)
     int nb0, nb1, nb2;
     int g0, g1;  // block split: [0,g0) thread class, [g0,g0+g1) warp class, rest block class
 };
@@ -276,11 +275,6 @@ __global__ void __launch_bounds__(256, 5) k_bnd(Buffers b, BndArgs a, int k) {
             else if (a.hist) atomicAdd(&s_hist[own * kRadix + (int)((key >> a.hshift) & (kRadix - 1))], 1u);
         }
         put_slot(b, pos, isb, own, key);
-        if (a.dchunk) {  // the lanes of a chunk add once (callers may be divergent: active lanes only)
-            const unsigned am = __activemask();
-            const unsigned grp = __match_any_sync(am, isb ? pos / kDsChunk : -1);
-            if (isb && (threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&a.dchunk[pos / kDsChunk], (unsigned)__popc(grp));
-        }
     };
     if (!pull) {
         // ---- every record slot, thread per slot; kBndPushU slots per thread with their loads in flight
@@ -1603,7 +1597,6 @@ BndArgs bnd_args(dmolp_ctx *c, int t, int all, int hubwin, int k, bool hist_for_
     a.all = all;
     a.hubwin = hubwin;
     a.dsup = deg_sel ? c->b.dsup : nullptr;
-    a.dchunk = deg_sel ? c->b.dchunk : nullptr;
     a.hist = !deg_sel && hist_for_select && k <= kBndHistMaxK ? c->b.hist : nullptr;
     a.hshift = select_first_shift(c->dbits + c->ibits);
     a.ibits = c->ibits;

@@ -550,7 +550,6 @@ struct DegSelArgs {
     unsigned int *dfine;       // [nseg * kDsFine] fine counts of this iteration's partial superbins
     unsigned int *dfine_next;  // the other parity's buffer, cleared here for the next iteration
     unsigned int *dcntb;       // [gridDim.x * nseg * kDsFine]
-    unsigned int *dchunk;      // [slots / kDsChunk + 1] boundary records per chunk (the boundary test); cleared here
     int nseg;
     unsigned int polls;
     LpControl *ctl;
@@ -689,60 +688,9 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
     __syncthreads();
     // ---- 1. each warp walks its own contiguous range of record slots ----
     const int n0 = *a.n_dev;
-    // the blocks' slot ranges: contiguous, in block order, split at chunk boundaries so that each block holds
-    // about the same number of boundary records (the walk's cost); equal slot counts when none were counted
-    int lo, my_n;
-    {
-        const int nch = (n0 + kDsChunk - 1) / kDsChunk;
-        const int per = (nch + kDsThreads - 1) / kDsThreads;
-        const int c0 = min(nch, (int)threadIdx.x * per), c1 = min(nch, c0 + per);
-        unsigned int mine = 0;
-        for (int c = c0; c < c1; ++c) mine += __ldcg(a.dchunk + c);
-        unsigned int incl = mine;
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned int y = __shfl_up_sync(DMOLP_FULL_MASK, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) s_wsum[wid] = incl;
-        if (threadIdx.x == 0) {
-            s_bstar = blockIdx.x == 0 ? 0 : nch;  // first chunk of this block (nch: none left)
-            s_before = nch;                       // first chunk of the next block
-        }
-        __syncthreads();
-        if (wid == 0) {
-            unsigned int x = s_wsum[lane];
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned int y = __shfl_up_sync(DMOLP_FULL_MASK, x, o);
-                if (lane >= o) x += y;
-            }
-            s_wsum[lane] = x;
-        }
-        __syncthreads();
-        const unsigned long long total = s_wsum[kDsWarps - 1];
-        if (total > 0) {
-            // chunk c starts block b when the records before it reach b * total / gridDim.x (first such c)
-            const unsigned long long tb = (unsigned long long)blockIdx.x * total / gridDim.x,
-                                     te = (unsigned long long)(blockIdx.x + 1) * total / gridDim.x;
-            unsigned long long ex = (wid ? s_wsum[wid - 1] : 0u) + incl - mine;  // records before chunk c0
-            for (int c = c0; c < c1; ++c) {
-                const unsigned int cnt = __ldcg(a.dchunk + c);
-                if (blockIdx.x > 0 && ex >= tb && (c == 0 || ex - __ldcg(a.dchunk + c - 1) < tb)) s_bstar = c;
-                if (blockIdx.x + 1 < gridDim.x && ex >= te && (c == 0 || ex - __ldcg(a.dchunk + c - 1) < te))
-                    s_before = c;
-                ex += cnt;
-            }
-        }
-        __syncthreads();
-        if (total > 0) {
-            lo = min(n0, s_bstar * kDsChunk);
-            my_n = max(0, min(n0, s_before * kDsChunk) - lo);
-        } else {
-            const int cap = (n0 + gridDim.x - 1) / gridDim.x;
-            lo = blockIdx.x * cap;
-            my_n = max(0, min(n0, lo + cap) - lo);
-        }
-        __syncthreads();  // s_bstar and s_before are free again
-    }
+    const int cap = (n0 + gridDim.x - 1) / gridDim.x;
+    const int lo = blockIdx.x * cap;
+    const int my_n = max(0, min(n0, lo + cap) - lo);
     const int wcap = (my_n + kDsWarps - 1) / kDsWarps;
     const int wlo = lo + min(my_n, wid * wcap), whi = lo + min(my_n, (wid + 1) * wcap);
     int32_t *wlist = a.lists + wlo;  // at most whi - wlo entries: label, and the key in lkeys
@@ -830,10 +778,8 @@ __global__ void __launch_bounds__(kDsThreads, 1) k_select_deg(DegSelArgs a) {
         if (v) atomicAdd(&a.dfine[i], v);
     }
     if (!grid_sync(a.ctl, a.polls, 0)) return;
-    // every block has read the superbin and chunk counts: clear them for the next boundary test
+    // every block has read the superbin counts: clear them for the next boundary test
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nseg * kDsBins; i += gridDim.x * blockDim.x) a.dsup[i] = 0u;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n0 + kDsChunk - 1) / kDsChunk; i += gridDim.x * blockDim.x)
-        a.dchunk[i] = 0u;
     // ---- 2. per label with a partial superbin: the fine bin where the rest of the need is reached ----
     for (int p = wid; p < nseg; p += kDsWarps) {
         int take = 0, part = -1, rem = 0, pre = 0;
@@ -1181,7 +1127,6 @@ bool select_window_deg(dmolp_ctx *c, int nseg, const SplitArgs &split, const int
     a.dfine = c->b.dfine[split.t & 1];
     a.dfine_next = c->b.dfine[(split.t + 1) & 1];
     a.dcntb = c->b.dcntb;
-    a.dchunk = c->b.dchunk;
     a.nseg = nseg;
     a.polls = c->wait_polls;
     a.ctl = c->b.ctrl;
