@@ -177,6 +177,7 @@ struct dmolp_ctx {
     bool counts_kept = false;             // the current LP run decides from vcnt / hh (no label gathers)
     unsigned int wait_polls = dmolp::kDefaultWaitPolls;  // polls of a grid barrier before it gives up
     int nhot = 0;                         // hot vertices
+    int lp_runs = 0;                      // dmolp_lp_run calls on the resident graph
     std::vector<int32_t> h_rawdeg;        // host copy for the hub sort
     bool h_rawdeg_valid = false;          // h_rawdeg mirrors the resident raw degrees
     dmolp::Buffers b;

@@ -376,6 +376,7 @@ int graph_finish(dmolp_ctx *c, bool rows_sorted) {
     lp_fill(c, b.hrank, (int64_t)n, -1);  // no hot set until the first LP run builds it
     c->hot_ready = false;
     c->nhot = 0;
+    c->lp_runs = 0;
     lp_hub_index(c);
     select_prepare();
     // whether every arc has its reverse is tested when the LP loop first needs it (ensure_symmetry)
@@ -1182,12 +1183,18 @@ int dmolp_lp_run(dmolp_ctx *c, int k, const dmolp_lp_config *cfg, dmolp_lp_resul
         DMOLP_CUDA(cudaMemsetAsync(b.hubwin, 0, (size_t)(c->nv + 1) * sizeof(int32_t), c->stream));
         DMOLP_CUDA(cudaMemsetAsync(b.hub_in, 0, (size_t)c->nb[2] * sizeof(int32_t), c->stream));
     }
-    st = lp_hot_prepare(c);
-    if (st) return st;
-    lp_hot_refresh(c);
-    lp_reset_stats(c, k, nullptr);
     // symmetric graphs with at most 32 scored labels decide from kept label counts (no label gathers)
     c->counts_kept = c->symmetric && L.eff <= 32;
+    // The hot set (the labels of the highest-degree vertices in shared memory, a full pass over the arcs to
+    // build) pays off when the decisions gather labels, or over several runs on the graph; the first run of
+    // a kept-count graph goes without it.
+    if (!c->counts_kept || c->lp_runs > 0) {
+        st = lp_hot_prepare(c);
+        if (st) return st;
+    }
+    ++c->lp_runs;
+    lp_hot_refresh(c);
+    lp_reset_stats(c, k, nullptr);
     // the run-start pass also counts every hub's row into hh on symmetric graphs (kept from the movers after)
     lp_stats(c, k, nullptr, nullptr, true, c->counts_kept ? L.eff : 0, c->symmetric ? L.eff : 0);
     lp_init_end(c, cfg->mode);
