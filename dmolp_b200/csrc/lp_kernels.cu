@@ -10,13 +10,15 @@
 //   bnd      degree-bucketed candidacy (stamp / hubwin, or a pull walk that stops at the first window
 //            neighbour) and the boundary test from the maintained count of differently-labelled neighbours
 //            (gpu_lp_boundary.cu:251-270); a boundary vertex becomes a selection record keyed (degree
-//            asc|desc by RE[label], id), and the first radix digit of the keys is histogrammed per label
-//   select   per label the ceil(e^(-t/5) n) smallest keys (gpu_lp_boundary.cu:244, 277-301); the
-//            selection's partition emits the next window and routes it to the decision classes
+//            asc|desc by RE[label], id), counted per label and degree superbin (k <= 64; else the first
+//            radix digit of the keys is histogrammed per label)
+//   select   per label the ceil(e^(-t/5) n) smallest keys (gpu_lp_boundary.cu:244, 277-301), from the
+//            degree bins (k <= 64, select_kernels.cu k_select_deg) or by radix select; the selection emits
+//            the next window and routes it to the decision classes
 //   decide   boundaryLPKernel_unified's rule (gpu_lp_boundary.cu:354-426) for the selected vertices only:
 //            persistent warps over hub row chunks, warp-class groups and thread-class groups; on symmetric
-//            graphs the hubs' label counts are kept current instead of recounted; a changed label is
-//            parked in newlab[] (Jacobi: nothing moves yet)
+//            graphs the hubs' label counts (and, with at most 32 scored labels, every vertex's) are kept
+//            current instead of recounted; a changed label is parked in newlab[] (Jacobi: nothing moves yet)
 //   update   (symmetric graphs) edge cut, per-part intra arcs and vertex counts change only through the
 //            movers' arcs: each arc is re-scored with both endpoints' old and new labels, weighted 2 when
 //            the neighbour stays (its reverse arc is not visited) and 1 when it moves too.  Asymmetric
