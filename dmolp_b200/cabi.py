@@ -37,7 +37,7 @@ EXPORTS = [
     "dmolp_mpnn_prepare_training", "dmolp_mpnn_backward", "dmolp_mpnn_train_step", "dmolp_mpnn_decode",
     "dmolp_batch_propose", "dmolp_mpnn_gate", "dmolp_mpnn_train_gate", "dmolp_batch_phase1",
     "dmolp_graph_upload_adjtext", "dmolp_graph_load_adjtext", "dmolp_graph_size", "dmolp_graph_get",
-    "dmolp_graph_upload_adjtext_device", "dmolp_find_hubs_pairs", "dmolp_degree_order",
+    "dmolp_graph_upload_adjtext_device", "dmolp_find_hubs_pairs", "dmolp_degree_order", "dmolp_find_hubs",
 ]
 BATCH_MAX_K = 64
 
@@ -103,6 +103,7 @@ def bind(lib: ctypes.CDLL) -> ctypes.CDLL:
     lib.dmolp_graph_size.argtypes = [vp, POINTER(c_int64), POINTER(c_int64)]
     lib.dmolp_find_hubs_pairs.argtypes = [c_int64, vp, vp, vp, POINTER(c_int64)]
     lib.dmolp_degree_order.argtypes = [c_int64, vp, vp]
+    lib.dmolp_find_hubs.argtypes = [c_int64, vp, vp, POINTER(c_int64), POINTER(c_int32), POINTER(c_int32)]
     lib.dmolp_graph_get.argtypes = [vp, vp, vp, vp]
     lib.dmolp_phase1.argtypes = [vp, c_int, c_int, vp, vp, vp, POINTER(Phase1Info)]
     lib.dmolp_lp_run.argtypes = [vp, c_int, POINTER(LpConfig), POINTER(LpResult), vp, c_int]

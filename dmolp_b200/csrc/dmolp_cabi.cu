@@ -178,10 +178,7 @@ int run_stats(dmolp_ctx *c, int k, unsigned long long *cut_arcs, std::vector<lon
 // src/phase1/init.cpp:139-177 (see the comment at the top of this file): pairs in the order the reference's
 // degree map iterates at one rank (V-1..0), sorted with std::sort's exact permutation on all host threads.
 std::vector<int> find_hubs(const std::vector<int32_t> &raw) {
-    const int64_t nv = (int64_t)raw.size();
-    std::vector<std::pair<int, int>> sd(nv);
-    for (int64_t i = 0; i < nv; ++i) sd[i] = std::make_pair((int)(nv - 1 - i), raw[nv - 1 - i]);
-    return dmolp::hubs_from_pairs(std::move(sd));
+    return dmolp::hubs_from_degrees(raw.data(), (int64_t)raw.size());
 }
 
 // Capture (once) and launch the iterations [t0, t0+cnt) of an LP run as one CUDA graph.
@@ -1090,11 +1087,8 @@ int dmolp_phase1(dmolp_ctx *c, int k, int theta, int32_t *seeds_out, int64_t *ve
     // ---- hubs and first seed on the host (order-dependent; see the top of this file) ----
     const auto th0 = std::chrono::steady_clock::now();
     std::vector<int> hubs = find_hubs(c->h_rawdeg);
-    std::pair<int, int> first(-1, -1);
-    for (int64_t v = nv - 1; v >= 0; --v) {  // init.cpp:179-187, including its id-vs-degree tie test
-        const int d = c->h_rawdeg[v];
-        if (d > first.second || (d == first.second && (int)v < first.second)) first = std::make_pair((int)v, d);
-    }
+    // init.cpp:179-187, including its id-vs-degree tie test
+    const std::pair<int, int> first = dmolp::first_seed_of(c->h_rawdeg.data(), nv);
     inf.num_hubs = (int64_t)hubs.size();
     DMOLP_CUDA(cudaMemsetAsync(b.p1te, 0, sizeof(unsigned long long), c->stream));
     const auto th1 = std::chrono::steady_clock::now();

@@ -15,7 +15,10 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <utility>
 #include <vector>
 
@@ -249,10 +252,9 @@ void sort_by_degree(Pair *a, int64_t n) {
     }
 }
 
-// find_hub_nodes on pairs in the reference's map order.
-std::vector<int> hubs_from_pairs(std::vector<Pair> sd) {
-    sort_by_degree(sd.data(), (int64_t)sd.size());
-    const int N = (int)sd.size();
+// The hub cut of find_hub_nodes on pairs already in std::sort's order.
+std::vector<int> hubs_of_sorted(const Pair *sd, int64_t n) {
+    const int N = (int)n;
     std::vector<int> hubs;
     if (N < 2) return hubs;
     // The reference accumulates the sorted degrees in a double, left to right (init.cpp:145-160).  Every
@@ -275,6 +277,50 @@ std::vector<int> hubs_from_pairs(std::vector<Pair> sd) {
     return hubs;
 }
 
+// find_hub_nodes on pairs in the reference's map order.
+std::vector<int> hubs_from_pairs(std::vector<Pair> sd) {
+    sort_by_degree(sd.data(), (int64_t)sd.size());
+    return hubs_of_sorted(sd.data(), (int64_t)sd.size());
+}
+
+// find_hub_nodes on the raw degrees of one rank: the pairs (v, degree[v]) in the order the reference's
+// degree map iterates, vertex V-1 down to 0, are written on all threads into storage that is not zeroed
+// first (building the 32 MB of pairs of 4 M vertices on one thread was mostly first-touch page faults), then
+// sorted and cut as above.
+std::vector<int> hubs_from_degrees(const int32_t *degree, int64_t nv) {
+    struct Release {
+        void operator()(Pair *p) const { ::operator delete(p); }
+    };
+    std::unique_ptr<Pair, Release> buf(static_cast<Pair *>(::operator new((size_t)std::max<int64_t>(nv, 1) * sizeof(Pair))));
+    Pair *sd = buf.get();
+#pragma omp parallel for schedule(static) if (nv >= kParallelMin && !omp_in_parallel())
+    for (int64_t i = 0; i < nv; ++i) new (sd + i) Pair((int32_t)(nv - 1 - i), degree[nv - 1 - i]);
+    sort_by_degree(sd, nv);
+    return hubs_of_sorted(sd, nv);  // Pair is trivially destructible: the storage is released as it is
+}
+
+// find_first_seed (init.cpp:179-187) over the same order, V-1 down to 0, from (-1, -1): the best pair is
+// replaced by a larger degree, or by an equal degree whose vertex id is below the best DEGREE (the
+// reference's tie test compares an id with a degree).  With D the largest degree and v1 the highest vertex of
+// degree D, the loop holds v1 from there on, then every later (lower) vertex of degree D with id < D: it ends
+// at the lowest vertex of degree D with id < D, or at v1 when there is none, and at (-1, -1) when D < 0 or
+// there are no vertices.  Both come from two parallel passes.
+std::pair<int, int> first_seed_of(const int32_t *degree, int64_t nv) {
+    const bool par = nv >= kParallelMin && !omp_in_parallel();
+    int32_t D = INT32_MIN;
+#pragma omp parallel for reduction(max : D) schedule(static) if (par)
+    for (int64_t v = 0; v < nv; ++v) D = std::max(D, degree[v]);
+    if (nv == 0 || D < 0) return std::make_pair(-1, -1);
+    int64_t v1 = -1, u = INT64_MAX;
+#pragma omp parallel for reduction(max : v1) reduction(min : u) schedule(static) if (par)
+    for (int64_t v = 0; v < nv; ++v)
+        if (degree[v] == D) {
+            v1 = std::max(v1, v);
+            if (v < (int64_t)D) u = std::min(u, v);
+        }
+    return std::make_pair((int)(u != INT64_MAX ? u : v1), (int)D);
+}
+
 }  // namespace dmolp
 
 extern "C" {
@@ -288,6 +334,20 @@ int dmolp_degree_order(int64_t n, int32_t *ids, int32_t *degrees) {
         ids[i] = a[i].first;
         degrees[i] = a[i].second;
     }
+    return DMOLP_OK;
+}
+
+int dmolp_find_hubs(int64_t nv, const int32_t *raw_degree, int32_t *hubs, int64_t *nhubs, int32_t *first_seed,
+                    int32_t *first_seed_degree) {
+    if (nv < 0 || nv > 0x7fffffff || (nv > 0 && (!raw_degree || !hubs)) || !nhubs || !first_seed ||
+        !first_seed_degree)
+        return DMOLP_ERR_ARG;
+    const std::vector<int> h = dmolp::hubs_from_degrees(raw_degree, nv);
+    std::copy(h.begin(), h.end(), hubs);
+    *nhubs = (int64_t)h.size();
+    const std::pair<int, int> f = dmolp::first_seed_of(raw_degree, nv);
+    *first_seed = f.first;
+    *first_seed_degree = f.second;
     return DMOLP_OK;
 }
 

@@ -11,6 +11,10 @@ namespace dmolp {
 // ---- host (hubsort.cpp) ----
 // find_hub_nodes on (vertex, degree) pairs in the reference's map order, std::sort's tie order kept.
 std::vector<int> hubs_from_pairs(std::vector<std::pair<int, int>> sd);
+// The same on the raw degrees of one rank (pairs in map order, vertex V-1 down to 0, built on all threads).
+std::vector<int> hubs_from_degrees(const int32_t *degree, int64_t nv);
+// find_first_seed's (vertex, degree) over that order, its id-vs-degree tie test included.
+std::pair<int, int> first_seed_of(const int32_t *degree, int64_t nv);
 
 // ---- segmented radix select (select_kernels.cu) ----
 // Records i < *n_dev carry a segment seg[i] in [0,nseg) (or -1: an empty slot, ignored) and a 64-bit key

@@ -249,6 +249,13 @@ int dmolp_graph_symmetric(dmolp_ctx *ctx, int *symmetric);
  * in place).  Both run on all host threads and give std::sort's permutation (checked against it). */
 int dmolp_find_hubs_pairs(int64_t n, const int32_t *ids, const int32_t *degrees, int32_t *hubs, int64_t *nhubs);
 int dmolp_degree_order(int64_t n, int32_t *ids, int32_t *degrees);
+/* find_hub_nodes and find_first_seed (src/phase1/init.cpp:139-187; init.hpp:10-11) on the raw degrees one
+ * rank gathers (raw_degree[v] for v < nv; the degree map iterates v = nv-1 down to 0): the hubs as
+ * dmolp_find_hubs_pairs gives them (hubs needs room for nv entries) and the first seed with its degree, by
+ * the reference's loop and its tie test, which compares a vertex id with the best degree ((-1, -1) when
+ * there is no vertex of degree >= 0).  The host step of dmolp_phase1. */
+int dmolp_find_hubs(int64_t nv, const int32_t *raw_degree, int32_t *hubs, int64_t *nhubs, int32_t *first_seed,
+                    int32_t *first_seed_degree);
 
 /* ---- host-side graph loading (no device work) ----
  * Parse the reference's adjacency text: first line V, line i+1 = neighbour ids of vertex i.  Produces the

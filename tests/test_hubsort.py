@@ -1,6 +1,8 @@
 """The hub sort of phase 1 (find_hub_nodes, src/phase1/init.cpp:139-177): the library's parallel restatement
 of introsort must leave exactly the permutation this toolchain's std::sort leaves (the oracle calls std::sort
 itself), ties included, on inputs that exercise every part of the algorithm; the hub lists must agree too."""
+import sys
+
 import numpy as np
 import pytest
 
@@ -104,3 +106,85 @@ def test_degree_order_inside_a_callers_parallel_loop(tmp_path):
                     "-Wl,-rpath," + lib], check=True, capture_output=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True, timeout=300)
     assert out.stdout.strip() == "0"
+
+
+def literal_first_seed(deg):
+    """find_first_seed (src/phase1/init.cpp:179-187) as the reference runs it at one rank: the degree map
+    iterated from vertex V-1 down to 0, starting from (-1, -1), with its tie test comparing an id with the best
+    degree."""
+    best_v, best_d = -1, -1
+    for v in range(len(deg) - 1, -1, -1):
+        d = int(deg[v])
+        if d > best_d or (d == best_d and v < best_d):
+            best_v, best_d = v, d
+    return best_v, best_d
+
+
+def lib_find_hubs(deg):
+    import ctypes
+
+    deg = np.ascontiguousarray(deg, np.int32)
+    n = deg.shape[0]
+    h = np.empty(max(n, 1), np.int32)
+    nh, f, fd = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()
+    assert core().dmolp_find_hubs(n, deg.ctypes.data, h.ctypes.data, ctypes.byref(nh), ctypes.byref(f),
+                                  ctypes.byref(fd)) == cabi.DMOLP_OK
+    return h[:nh.value].copy(), (f.value, fd.value)
+
+
+def degree_cases():
+    rng = np.random.default_rng(23)
+    out = [("empty", np.zeros(0, np.int32)), ("one", np.array([5], np.int32)),
+           ("zeros", np.zeros(1000, np.int32)), ("all-minus-one", np.full(50, -1, np.int32)),
+           ("negative", np.full(100, -3, np.int32))]
+    d = np.zeros(2000, np.int32)
+    d[[5, 40, 1500, 1900]] = 100  # the largest degree at ids below it (5, 40) and above it: the loop ends at 5
+    out.append(("tie-ids-below-degree", d))
+    d = np.zeros(2000, np.int32)
+    d[[300, 700]] = 50  # every id above the degree: the loop keeps the highest, 700
+    out.append(("tie-ids-above-degree", d))
+    d = np.ones(5000, np.int32)
+    d[[4999, 3, 1]] = 7  # the first one met (4999) is replaced by 3, then by 1
+    out.append(("tie-replaced-twice", d))
+    for n in (50_000, 300_000, 1_200_000):  # 300 K and up: the parallel paths
+        out.append(("powerlaw-%d" % n, np.minimum((rng.pareto(1.1, n) * 2).astype(np.int64), 200).astype(np.int32)))
+        out.append(("few-keys-%d" % n, rng.integers(0, 6, n).astype(np.int32)))
+    return out
+
+
+@pytest.mark.parametrize("name,deg", degree_cases(), ids=[c[0] for c in degree_cases()])
+def test_find_hubs_from_raw_degrees(name, deg):
+    """dmolp_find_hubs (the host step of phase 1): the hub list equals the oracle's (std::sort over the map
+    order) and the first seed equals the reference's loop, tie test included."""
+    hubs, first = lib_find_hubs(deg)
+    assert first == literal_first_seed(deg), name
+    if deg.shape[0] and deg.min() >= 0:
+        assert np.array_equal(hubs, oracle.find_hubs(deg)), name
+
+
+THREADS = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+from tests.test_hubsort import lib_find_hubs
+rng = np.random.default_rng(31)
+d = np.minimum((rng.pareto(1.1, 1_500_000) * 2).astype(np.int64), 300).astype(np.int32)
+h, f = lib_find_hubs(d)
+print(len(h), int((h.astype(np.int64) * np.arange(1, len(h) + 1)).sum()), f[0], f[1])
+"""
+
+
+def test_find_hubs_same_at_every_thread_count():
+    """The pairs are written and the first seed reduced on however many threads OpenMP gives: the answer must
+    not depend on it."""
+    import os
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = set()
+    for t in (1, 3, 16):
+        env = dict(os.environ, OMP_NUM_THREADS=str(t))
+        r = subprocess.run([sys.executable, "-c", THREADS, root], env=env, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.add(r.stdout.strip())
+    assert len(outs) == 1, outs
