@@ -198,21 +198,8 @@ int lg(int64_t n) {
     return b;
 }
 
-}  // namespace
-
-namespace dmolp {
-
-// The permutation std::sort(a, a + n, by degree) leaves, computed in parallel for large n.
-void sort_by_degree(Pair *a, int64_t n) {
-    if (n <= 1) return;
-    const int T = n >= kParallelMin && !omp_in_parallel() ? std::max(1, omp_get_max_threads()) : 1;
-    if (T > 1) {
-#pragma omp parallel num_threads(T)
-#pragma omp single
-        introsort_loop(a, a + n, 2 * (int64_t)lg(n), true);
-    } else {
-        introsort_loop(a, a + n, 2 * (int64_t)lg(n), false);
-    }
+// std::sort's final insertion pass over a[0..n) once the loop has run on all of it.
+void final_insertion(Pair *a, int64_t n, int T) {
     if (n <= kSmall) {
         guarded_insertion(a, a + n);
         return;
@@ -252,41 +239,122 @@ void sort_by_degree(Pair *a, int64_t n) {
     }
 }
 
-// The hub cut of find_hub_nodes on pairs already in std::sort's order.
-std::vector<int> hubs_of_sorted(const Pair *sd, int64_t n) {
+int threads_for(int64_t n) { return n >= kParallelMin && !omp_in_parallel() ? std::max(1, omp_get_max_threads()) : 1; }
+
+// Only the top of the order: the ranges of the loop that reach position t0 or beyond, none that end below
+// it.  The ranges of introsort are independent (a range is partitioned by the same steps whatever happens
+// beside it), and every range's left side holds no degree above its right side's, so skipping the ranges
+// that end at or below t0 changes nothing at or above t0.  [first, last) holds t0 on entry; on return
+// *leaf is the start of the last range that held t0 (a partition cut, or a heapsorted or short range).
+void top_loop(Pair *first, Pair *last, int64_t depth, const Pair *t0, Pair **leaf, bool spawn) {
+    while (last - first > kSmall) {
+        if (depth == 0) {
+            heapsort(first, last - first);
+            break;
+        }
+        --depth;
+        Pair *cut = partition_around_front(first, last);
+        if (cut <= t0) {  // t0 is in the right side: the left side [first, cut) lies below t0
+            first = cut;
+            continue;
+        }
+        if (spawn && last - cut >= kTaskMin) {  // the right side lies above t0: needed whole
+#pragma omp task firstprivate(cut, last, depth)
+            introsort_loop(cut, last, depth, true);
+        } else {
+            introsort_loop(cut, last, depth, spawn);
+        }
+        last = cut;
+    }
+    *leaf = first;
+}
+
+}  // namespace
+
+namespace dmolp {
+
+// The permutation std::sort(a, a + n, by degree) leaves, computed in parallel for large n.
+void sort_by_degree(Pair *a, int64_t n) {
+    if (n <= 1) return;
+    const int T = threads_for(n);
+    if (T > 1) {
+#pragma omp parallel num_threads(T)
+#pragma omp single
+        introsort_loop(a, a + n, 2 * (int64_t)lg(n), true);
+    } else {
+        introsort_loop(a, a + n, 2 * (int64_t)lg(n), false);
+    }
+    final_insertion(a, n, T);
+}
+
+// a[t0..n) as std::sort(a, a + n, by degree) leaves it; a[0..t0) holds the rest in some order.  From the
+// start of the last range that held t0 (a point no element crosses: nothing left of it is above anything
+// right of it) the final insertion pass runs as std::sort's does; when nothing was skipped it is the full one.
+void top_by_degree(Pair *a, int64_t n, int64_t t0) {
+    if (n <= 1 || t0 >= n) return;
+    if (t0 <= 0) {
+        sort_by_degree(a, n);
+        return;
+    }
+    const int T = threads_for(n);
+    Pair *leaf = a;
+    if (T > 1) {
+#pragma omp parallel num_threads(T)
+#pragma omp single
+        top_loop(a, a + n, 2 * (int64_t)lg(n), a + t0, &leaf, true);
+    } else {
+        top_loop(a, a + n, 2 * (int64_t)lg(n), a + t0, &leaf, false);
+    }
+    if (leaf == a) {
+        final_insertion(a, n, T);
+        return;
+    }
+    for (Pair *i = leaf; i != a + n; ++i) linear_insert(i);  // a[leaf-1] is not above anything right of it
+}
+
+// find_hub_nodes (init.cpp:139-177) on pairs in the reference's map order.  The reference sorts them all,
+// accumulates the sorted degrees in a double, left to right (init.cpp:145-160), and takes vertices from the
+// top down while (i + 1) / N is past the x-intercept of the Lorenz curve's last segment.  Every partial sum
+// of non-negative integers below 2^53 is exact in a double, so the integer total and the largest degree give
+// the same bits, and the number of hubs H follows from them before any sorting: only the top H places of
+// std::sort's order are computed (top_by_degree), not the whole order.
+std::vector<int> hubs_of_pairs(Pair *sd, int64_t n) {
     const int N = (int)n;
     std::vector<int> hubs;
     if (N < 2) return hubs;
-    // The reference accumulates the sorted degrees in a double, left to right (init.cpp:145-160).  Every
-    // partial sum of non-negative integers below 2^53 is exact in a double, so the integer sums give the same
-    // bits: only the total and the sum without the last element are needed.
     int64_t total_i = 0;
-#pragma omp parallel for reduction(+ : total_i) schedule(static) if (N >= kParallelMin)
-    for (int i = 0; i < N; ++i) total_i += sd[i].second;
+    int32_t dmax = INT32_MIN;
+#pragma omp parallel for reduction(+ : total_i) reduction(max : dmax) schedule(static) \
+    if (N >= kParallelMin && !omp_in_parallel())
+    for (int i = 0; i < N; ++i) {
+        total_i += sd[i].second;
+        dmax = std::max(dmax, sd[i].second);
+    }
     const double total = (double)total_i;
-    const double y1 = (double)total_i / total, y0 = (double)(total_i - sd[N - 1].second) / total;
+    const double y1 = (double)total_i / total, y0 = (double)(total_i - dmax) / total;
     const double inv_n = 1.0 / N;
     const double x1 = N * inv_n;
     const double x0 = (N - 1) * inv_n;
     const double slope = (y1 - y0) / (x1 - x0);
     const double x_int = x1 - y1 / slope;
+    int H = 0;
     for (int i = N - 1; i >= 0; --i) {
-        if ((i + 1) * inv_n > x_int) hubs.push_back(sd[i].first);
+        if ((i + 1) * inv_n > x_int) ++H;
         else break;
     }
+    if (H == 0) return hubs;
+    top_by_degree(sd, n, n - H);
+    for (int i = N - 1; i >= N - H; --i) hubs.push_back(sd[i].first);
     return hubs;
 }
 
 // find_hub_nodes on pairs in the reference's map order.
-std::vector<int> hubs_from_pairs(std::vector<Pair> sd) {
-    sort_by_degree(sd.data(), (int64_t)sd.size());
-    return hubs_of_sorted(sd.data(), (int64_t)sd.size());
-}
+std::vector<int> hubs_from_pairs(std::vector<Pair> sd) { return hubs_of_pairs(sd.data(), (int64_t)sd.size()); }
 
 // find_hub_nodes on the raw degrees of one rank: the pairs (v, degree[v]) in the order the reference's
 // degree map iterates, vertex V-1 down to 0, are written on all threads into storage that is not zeroed
 // first (building the 32 MB of pairs of 4 M vertices on one thread was mostly first-touch page faults), then
-// sorted and cut as above.
+// cut as above.
 std::vector<int> hubs_from_degrees(const int32_t *degree, int64_t nv) {
     struct Release {
         void operator()(Pair *p) const { ::operator delete(p); }
@@ -295,8 +363,7 @@ std::vector<int> hubs_from_degrees(const int32_t *degree, int64_t nv) {
     Pair *sd = buf.get();
 #pragma omp parallel for schedule(static) if (nv >= kParallelMin && !omp_in_parallel())
     for (int64_t i = 0; i < nv; ++i) new (sd + i) Pair((int32_t)(nv - 1 - i), degree[nv - 1 - i]);
-    sort_by_degree(sd, nv);
-    return hubs_of_sorted(sd, nv);  // Pair is trivially destructible: the storage is released as it is
+    return hubs_of_pairs(sd, nv);  // Pair is trivially destructible: the storage is released as it is
 }
 
 // find_first_seed (init.cpp:179-187) over the same order, V-1 down to 0, from (-1, -1): the best pair is

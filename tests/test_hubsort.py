@@ -149,6 +149,16 @@ def degree_cases():
     for n in (50_000, 300_000, 1_200_000):  # 300 K and up: the parallel paths
         out.append(("powerlaw-%d" % n, np.minimum((rng.pareto(1.1, n) * 2).astype(np.int64), 200).astype(np.int32)))
         out.append(("few-keys-%d" % n, rng.integers(0, 6, n).astype(np.int32)))
+    # structured orders (the hub count ranges from a few to every vertex; only the top is sorted)
+    n = 300_000
+    out.append(("sorted-%d" % n, np.sort(rng.integers(0, 1000, n)).astype(np.int32)))
+    out.append(("reverse-%d" % n, np.sort(rng.integers(0, 1000, n))[::-1].astype(np.int32)))
+    out.append(("constant-%d" % n, np.full(n, 7, np.int32)))
+    out.append(("sawtooth-%d" % n, (np.arange(n) % 977).astype(np.int32)))
+    out.append(("organ-pipe-%d" % n, np.concatenate([np.arange(n // 2), np.arange(n - n // 2)[::-1]]).astype(np.int32)))
+    d = np.minimum((rng.pareto(1.1, n) * 2).astype(np.int64), 60).astype(np.int32)
+    d[rng.integers(0, n, 40)] = 60  # many vertices tied at the largest degree, some of them hubs
+    out.append(("tied-top-%d" % n, d))
     return out
 
 
