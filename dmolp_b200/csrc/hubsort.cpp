@@ -11,7 +11,10 @@
 //     OpenMP tasks;
 //   * the final insertion pass never moves an element left of a position p with max(a[0..p)) <= min(a[p..n)),
 //     so the array is cut at such positions and the pieces are finished in parallel.
-// tests/test_hubsort.py checks the permutation against std::sort itself on tie-heavy and adversarial inputs.
+// The hub list needs only the top of that order (the number of hubs is known before sorting), so it sorts
+// only the ranges that reach the top; find_first_seed's loop is evaluated from its closed form.
+// tests/test_hubsort.py checks the permutation against std::sort itself on tie-heavy and adversarial inputs,
+// the hub lists against the oracle and the first seed against the reference's loop.
 #include <omp.h>
 
 #include <algorithm>
