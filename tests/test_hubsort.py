@@ -69,8 +69,30 @@ NESTED = r"""
 #include <algorithm>
 #include <cstdint>
 extern "C" int dmolp_degree_order(int64_t n, int32_t *ids, int32_t *degrees);
+extern "C" int dmolp_find_hubs(int64_t nv, const int32_t *raw_degree, int32_t *hubs, int64_t *nhubs,
+                               int32_t *first_seed, int32_t *first_seed_degree);
+// hubs and first seed of a skewed degree array (sizes past the parallel threshold when called alone)
+static std::vector<int32_t> hub_answer(const std::vector<int32_t> &deg) {
+    std::vector<int32_t> h(deg.size() + 2);
+    int64_t nh = 0;
+    int32_t f = 0, fd = 0;
+    if (dmolp_find_hubs((int64_t)deg.size(), deg.data(), h.data(), &nh, &f, &fd) != 0) return {};
+    h.resize(nh);
+    h.push_back(f);
+    h.push_back(fd);
+    return h;
+}
 int main() {
     int bad = 0;
+    std::vector<std::vector<int32_t>> degs(12), inside(12);
+    for (int g = 0; g < 12; ++g) {
+        std::mt19937_64 rng(100 + g);
+        degs[g].resize(300000 + rng() % 100000);
+        for (auto &d : degs[g]) d = (int32_t)(std::min<uint64_t>(rng() % 1000, rng() % 1000) % (5 + g * 7));
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int g = 0; g < 12; ++g) inside[g] = hub_answer(degs[g]);
+    for (int g = 0; g < 12; ++g) bad += hub_answer(degs[g]) != inside[g] || inside[g].empty();
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : bad)
     for (int g = 0; g < 48; ++g) {
         std::mt19937_64 rng(g);
@@ -92,7 +114,8 @@ int main() {
 
 def test_degree_order_inside_a_callers_parallel_loop(tmp_path):
     """The batched phase 1 computes many graphs' hubs from inside its own OpenMP loop: the sort must neither
-    leave work behind (tasks outliving the call) nor differ from std::sort there."""
+    leave work behind (tasks outliving the call) nor differ from std::sort there, and the hub list and first
+    seed found inside the loop must equal the ones found by a call on all threads."""
     import os
     import subprocess
 
